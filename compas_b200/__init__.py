@@ -1,0 +1,297 @@
+"""compas_b200: B200-native finite-volume right-hand side and TVD-RK3 level advance of the COMPAS
+five- and six-equation diffuse-interface models.
+
+The compute path is the CUDA library ``libcompas_b200.so`` (sm_100a) behind the C ABI declared in
+``include/compas_b200.h``; this module binds it with ctypes. There is no CPU fallback: importing the
+bindings without the built library raises.
+
+Names mirror the reference's plugin points (include/COMPAS.H, include/Classes_Physics/
+Class_Compressible_PhaseField.H): ``compute_dUdt_FV``, ``ThirdOrderSSPRK`` stages, ``FillPatch``
+(single-box physical boundaries), ``Relaxation``, and the inputs keys ``FiniteVolume.Scheme``,
+``Physics.RiemannSolver``, ``prob.EOS.*``, ``run.cfl``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+FIVEEQS = 555
+SIXEQS = 666
+
+OK = 0
+EARG, ECUDA, ENOMEM, ESTATE, EUNSUPPORTED = -1, -2, -3, -4, -5
+ERR_NAN, ERR_COVOLUME, ERR_RELAX_NOROOT, ERR_CFL = 0x1, 0x2, 0x4, 0x8
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcompas_b200.so")
+
+
+class CompasError(RuntimeError):
+    """A C-ABI call returned a non-zero status (the reference would have aborted)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"compas_b200 error {code}: {msg}")
+        self.code = code
+
+
+class Parm(ctypes.Structure):
+    """ctypes mirror of ``compas_b200_parm`` (include/compas_b200.h)."""
+
+    _fields_ = [
+        ("physics", ctypes.c_int),
+        ("dim", ctypes.c_int),
+        ("eos", ctypes.c_int),
+        ("gamma_1", ctypes.c_double), ("gamma_2", ctypes.c_double),
+        ("pinf_1", ctypes.c_double), ("pinf_2", ctypes.c_double),
+        ("b_1", ctypes.c_double), ("b_2", ctypes.c_double),
+        ("q_1", ctypes.c_double), ("q_2", ctypes.c_double),
+        ("A1", ctypes.c_double), ("A2", ctypes.c_double),
+        ("B1", ctypes.c_double), ("B2", ctypes.c_double),
+        ("C1", ctypes.c_double), ("C2", ctypes.c_double),
+        ("D1", ctypes.c_double), ("D2", ctypes.c_double),
+        ("id_limiter", ctypes.c_int),
+        ("num_grow", ctypes.c_int),
+        ("thinc", ctypes.c_int),
+        ("thinc_use_normal", ctypes.c_int),
+        ("thinc_eps", ctypes.c_double), ("thinc_beta", ctypes.c_double),
+        ("thinc_normal_threshold", ctypes.c_double),
+        ("id_riemann", ctypes.c_int),
+        ("source_term", ctypes.c_int),
+        ("relaxation", ctypes.c_int),
+        ("relax_trace", ctypes.c_double),
+        ("cfl", ctypes.c_double),
+        ("change_limiter", ctypes.c_int),
+        ("precision", ctypes.c_int),
+    ]
+
+
+class Geom(ctypes.Structure):
+    """ctypes mirror of ``compas_b200_geom``."""
+
+    _fields_ = [
+        ("n", ctypes.c_int * 3),
+        ("ng", ctypes.c_int),
+        ("dx", ctypes.c_double * 3),
+        ("lo_bc", ctypes.c_int * 3),
+        ("hi_bc", ctypes.c_int * 3),
+    ]
+
+
+_lib_handle = None
+
+_SIGS = {
+    "compas_b200_last_error": (ctypes.c_char_p, []),
+    "compas_b200_parm_init": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.c_int, ctypes.c_int]),
+    "compas_b200_parm_set": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.c_char_p, ctypes.c_char_p]),
+    "compas_b200_parm_finalize": (ctypes.c_int, [ctypes.POINTER(Parm)]),
+    "compas_b200_state_bytes": (ctypes.c_longlong, [ctypes.POINTER(Parm), ctypes.POINTER(Geom)]),
+    "compas_b200_fill_boundary": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_void_p,
+                                                 ctypes.c_void_p]),
+    "compas_b200_compute_dUdt": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_void_p,
+                                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "compas_b200_rk3_stage": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_int,
+                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "compas_b200_relaxation": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_void_p,
+                                              ctypes.c_void_p, ctypes.c_void_p]),
+    "compas_b200_level_create": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom),
+                                                ctypes.POINTER(ctypes.c_void_p)]),
+    "compas_b200_level_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "compas_b200_level_upload": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
+                                                ctypes.c_void_p]),
+    "compas_b200_level_download": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "compas_b200_level_state": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "compas_b200_level_advance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                                 ctypes.c_void_p]),
+    "compas_b200_level_sync": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_uint)]),
+    "compas_b200_level_dts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
+    "compas_b200_level_launches": (ctypes.c_longlong, [ctypes.c_void_p]),
+}
+
+EXPORTED_SYMBOLS = tuple(_SIGS)
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded CUDA library; raises if it was not built (there is no fallback path)."""
+    global _lib_handle
+    if _lib_handle is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'`")
+        h = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(h, name)
+            f.restype = res
+            f.argtypes = args
+        _lib_handle = h
+    return _lib_handle
+
+
+def _check(rc: int) -> None:
+    if rc != OK:
+        raise CompasError(rc, lib().compas_b200_last_error().decode())
+
+
+def nstate(physics: int, dim: int) -> int:
+    """NSTATE of the model (include/Macros.H:73, :114)."""
+    return (4 if physics == FIVEEQS else 5) + dim
+
+
+def make_parm(physics: int, dim: int, inputs: dict | None = None) -> Parm:
+    """A parameter block from reference defaults plus inputs keys, e.g.
+    {"FiniteVolume.Scheme": "WENO5", "prob.EOS.gamma_2": 4.4, "run.cfl": 0.5}."""
+    p = Parm()
+    _check(lib().compas_b200_parm_init(ctypes.byref(p), physics, dim))
+    for k, v in (inputs or {}).items():
+        _check(lib().compas_b200_parm_set(ctypes.byref(p), k.encode(), str(v).encode()))
+    _check(lib().compas_b200_parm_finalize(ctypes.byref(p)))
+    return p
+
+
+def make_geom(n, dx, ng=3, lo_bc=(0, 0, 0), hi_bc=(0, 0, 0)) -> Geom:
+    g = Geom()
+    n = list(n) + [1] * (3 - len(n))
+    dx = list(dx) + [1.0] * (3 - len(dx))
+    for d in range(3):
+        g.n[d] = int(n[d])
+        g.dx[d] = float(dx[d])
+        g.lo_bc[d] = int(lo_bc[d]) if d < len(lo_bc) else 0
+        g.hi_bc[d] = int(hi_bc[d]) if d < len(hi_bc) else 0
+    g.ng = int(ng)
+    return g
+
+
+def padded_shape(p: Parm, g: Geom) -> tuple:
+    """(N, PZ, PY, PX) of a state array with ghosts (no z ghosts in 2D)."""
+    gz = g.ng if p.dim == 3 else 0
+    nz = g.n[2] if p.dim == 3 else 1
+    return (nstate(p.physics, p.dim), nz + 2 * gz, g.n[1] + 2 * g.ng, g.n[0] + 2 * g.ng)
+
+
+def valid_view(a, p: Parm, g: Geom):
+    """The valid cells of a padded array (numpy or torch), shape (N, nz, ny, nx)."""
+    gz = g.ng if p.dim == 3 else 0
+    nz = g.n[2] if p.dim == 3 else 1
+    return a[:, gz:gz + nz, g.ng:g.ng + g.n[1], g.ng:g.ng + g.n[0]]
+
+
+def _ptr(x) -> int:
+    if x is None:
+        return 0
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    return int(x)
+
+
+def _stream_ptr(stream) -> int:
+    if stream is None:
+        return 0
+    if hasattr(stream, "cuda_stream"):
+        return stream.cuda_stream
+    return int(stream)
+
+
+# ---- drop-in kernels on caller-owned device arrays (torch CUDA tensors or raw pointers) ----------
+
+def FillPatch(p: Parm, g: Geom, U, stream=None) -> None:
+    """Physical and periodic ghost cells of a single-box level (COMPAS::FillPatch, source/COMPAS.cpp:1629-1732)."""
+    _check(lib().compas_b200_fill_boundary(ctypes.byref(p), ctypes.byref(g), _ptr(U), _stream_ptr(stream)))
+
+
+def compute_dUdt_FV(p: Parm, g: Geom, U, dUdt, cmax=None, err=None, stream=None) -> None:
+    """dUdt of the valid cells from U with filled ghosts
+    (Compressible_PhaseField::compute_dUdt_FV, source/Class_Compressible_PhaseField.cpp:3472-3537)."""
+    _check(lib().compas_b200_compute_dUdt(ctypes.byref(p), ctypes.byref(g), _ptr(U), _ptr(dUdt), _ptr(cmax),
+                                          _ptr(err), _stream_ptr(stream)))
+
+
+def ThirdOrderSSPRK_stage(p: Parm, g: Geom, stage: int, Us, Uold, Unew, dt_dev, cmax=None, err=None,
+                          stream=None) -> None:
+    """One fused stage of ThirdOrderSSPRK plus PostTimeStage (source/Class_Compressible_PhaseField.cpp:3937-4107)."""
+    _check(lib().compas_b200_rk3_stage(ctypes.byref(p), ctypes.byref(g), stage, _ptr(Us), _ptr(Uold), _ptr(Unew),
+                                       _ptr(dt_dev), _ptr(cmax), _ptr(err), _stream_ptr(stream)))
+
+
+def Relaxation(p: Parm, g: Geom, U, err=None, stream=None) -> None:
+    """SIXEQS pressure relaxation in place (source/Class_Compressible6Eq_PhaseField.cpp:437-474)."""
+    _check(lib().compas_b200_relaxation(ctypes.byref(p), ctypes.byref(g), _ptr(U), _ptr(err), _stream_ptr(stream)))
+
+
+@dataclass
+class SyncInfo:
+    t: float
+    steps: int
+    status: int
+
+
+class Level:
+    """One single-box level with device-resident state and the reference's time-step control."""
+
+    def __init__(self, p: Parm, g: Geom):
+        self.p, self.g = p, g
+        self._h = ctypes.c_void_p()
+        _check(lib().compas_b200_level_create(ctypes.byref(p), ctypes.byref(g), ctypes.byref(self._h)))
+        self.shape = padded_shape(p, g)
+        self.nbytes = int(lib().compas_b200_state_bytes(ctypes.byref(p), ctypes.byref(g)))
+
+    def close(self) -> None:
+        if self._h:
+            lib().compas_b200_level_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, U, t0: float = 0.0, stream=None) -> None:
+        """Copy a padded state in (numpy host array, or a torch tensor on host or device)."""
+        if isinstance(U, np.ndarray):
+            U = np.ascontiguousarray(U, dtype=np.float64)
+            assert U.nbytes == self.nbytes, (U.shape, self.shape)
+            _check(lib().compas_b200_level_upload(self._h, U.ctypes.data, 0, t0, _stream_ptr(stream)))
+            # the copy from pageable memory is staged before the call returns
+        else:
+            assert U.numel() * 8 == self.nbytes
+            _check(lib().compas_b200_level_upload(self._h, U.data_ptr(), 1 if U.is_cuda else 0, t0,
+                                                  _stream_ptr(stream)))
+
+    def download(self, out=None, stream=None):
+        """Copy the padded state out (into `out`, numpy or torch, or a new numpy array)."""
+        if out is None:
+            out = np.empty(self.shape, dtype=np.float64)
+        if isinstance(out, np.ndarray):
+            _check(lib().compas_b200_level_download(self._h, out.ctypes.data, 0, _stream_ptr(stream)))
+            self.sync(check=False)
+        else:
+            _check(lib().compas_b200_level_download(self._h, out.data_ptr(), 1 if out.is_cuda else 0,
+                                                    _stream_ptr(stream)))
+        return out
+
+    def state_ptr(self) -> int:
+        return int(lib().compas_b200_level_state(self._h))
+
+    def advance(self, nsteps: int, stop_time: float = 1.0e300, use_graph: bool = True, stream=None) -> None:
+        _check(lib().compas_b200_level_advance(self._h, int(nsteps), float(stop_time), 1 if use_graph else 0,
+                                               _stream_ptr(stream)))
+
+    def sync(self, check: bool = True) -> SyncInfo:
+        t = ctypes.c_double()
+        s = ctypes.c_int()
+        st = ctypes.c_uint()
+        rc = lib().compas_b200_level_sync(self._h, ctypes.byref(t), ctypes.byref(s), ctypes.byref(st))
+        if check:
+            _check(rc)
+        return SyncInfo(t.value, s.value, st.value)
+
+    def dts(self, n: int) -> np.ndarray:
+        out = (ctypes.c_double * n)()
+        _check(lib().compas_b200_level_dts(self._h, out, n))
+        return np.array(out[:], dtype=np.float64)
+
+    def launches(self) -> int:
+        return int(lib().compas_b200_level_launches(self._h))

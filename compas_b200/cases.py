@@ -1,0 +1,220 @@
+"""Initial data of the workloads: cell averages of the conserved state by 4-point Gauss-Legendre
+quadrature per direction (include/InitData.H:19-290, run.QuadratureIC = 1), or cell-centre samples.
+
+Every case returns (parm inputs, geometry kwargs, padded state) so that the CUDA path and the CPU
+oracles start from the same bits. Arrays follow the padded Array4 layout (N, PZ, PY, PX) with zero
+ghosts. `xp` may be numpy (default) or torch (then `device` places the arrays; FP64 throughout).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import FIVEEQS, SIXEQS, nstate
+
+# Gauss-Legendre nodes and weights on [-1, 1] (4 points, exact to degree 7)
+_GL_X, _GL_W = np.polynomial.legendre.leggauss(4)
+
+
+def eos_AB(gamma: float, pinf: float) -> tuple:
+    """Stiffened-gas partial-form coefficients A = 1/(gamma-1), B = gamma pinf/(gamma-1) (source/Parm.cpp:126-130)."""
+    return 1.0 / (gamma - 1.0), gamma * pinf / (gamma - 1.0)
+
+
+def shock_state(Ma: float, u0: float, p0: float, rho0: float, gamma: float, pinf: float) -> tuple:
+    """Post-shock (rho, u, p) behind a right-running normal shock of Mach Ma into a stiffened gas at
+    rest state (rho0, u0, p0): the Rankine-Hugoniot relations written in the shifted pressure
+    P = p + pinf, the same relations include/PhysicsFunctions.H:15-35 evaluates."""
+    P0 = p0 + pinf
+    c0 = math.sqrt(gamma * P0 / rho0)
+    P1 = P0 * (1.0 + 2.0 * gamma / (gamma + 1.0) * (Ma * Ma - 1.0))
+    r = P1 / P0
+    mu = (gamma + 1.0) / (gamma - 1.0)
+    rho1 = rho0 * (mu * r + 1.0) / (mu + r)
+    # jump in velocity from mass conservation across the shock moving at u0 + Ma c0
+    s = u0 + Ma * c0
+    u1 = s - rho0 * (s - u0) / rho1
+    return rho1, u1, P1 - pinf
+
+
+def _xp_of(xp):
+    if xp is None:
+        return np
+    return xp
+
+
+def _zeros(xp, shape, device):
+    if xp is np:
+        return np.zeros(shape, dtype=np.float64)
+    return xp.zeros(shape, dtype=xp.float64, device=device)
+
+
+def _cons_from_prims(physics, dim, ar1, ar2, vel, p, alpha1, A, B, xp):
+    """Conserved components from phase masses, velocity, a common pressure and alpha1 (stiffened gas)."""
+    alpha2 = 1.0 - alpha1
+    rho = ar1 + ar2
+    ke = 0.0
+    for v in vel:
+        ke = ke + v * v
+    out = [ar1, ar2] + [rho * v for v in vel]
+    if physics == FIVEEQS:
+        rho_e = alpha1 * (A[0] * p + B[0]) + alpha2 * (A[1] * p + B[1])
+        out += [rho_e + 0.5 * rho * ke, alpha1]
+    else:
+        e1 = alpha1 * (A[0] * p + B[0]) + 0.5 * ar1 * ke
+        e2 = alpha2 * (A[1] * p + B[1]) + 0.5 * ar2 * ke
+        out += [e1, e2, alpha1]
+    return out
+
+
+def _average(physics, dim, n, dx, lo, pointwise, ng, quadrature, xp, device):
+    """Padded state whose valid cells hold the cell averages of pointwise(x, y, z) -> list of N arrays."""
+    N = nstate(physics, dim)
+    gz = ng if dim == 3 else 0
+    nz = n[2] if dim == 3 else 1
+    shape = (N, nz + 2 * gz, n[1] + 2 * ng, n[0] + 2 * ng)
+    U = _zeros(xp, shape, device)
+
+    def ar(m, d):
+        a = np.arange(m, dtype=np.float64) if xp is np else xp.arange(m, dtype=xp.float64, device=device)
+        return lo[d] + (a + 0.5) * dx[d]
+
+    xc = ar(n[0], 0)[None, None, :]
+    yc = ar(n[1], 1)[None, :, None]
+    zc = ar(nz, 2)[:, None, None] if dim == 3 else (xc * 0.0 + 0.0)
+    if quadrature:
+        nodes = list(zip(_GL_X, _GL_W))
+        zn = nodes if dim == 3 else [(0.0, 2.0)]
+        acc = None
+        norm = 1.0 / (2 ** dim)
+        for rz, wz in zn:
+            for ry, wy in nodes:
+                for rx, wx in nodes:
+                    w = wx * wy * (wz if dim == 3 else 1.0)
+                    vals = pointwise(xc + 0.5 * dx[0] * rx, yc + 0.5 * dx[1] * ry,
+                                     zc + (0.5 * dx[2] * rz if dim == 3 else 0.0))
+                    if acc is None:
+                        acc = [w * v for v in vals]
+                    else:
+                        acc = [a + w * v for a, v in zip(acc, vals)]
+        vals = [a * norm for a in acc]
+    else:
+        vals = pointwise(xc, yc, zc)
+    for c in range(N):
+        v = vals[c]
+        if not hasattr(v, "shape") or v.shape != (nz, n[1], n[0]):
+            v = v + 0.0 * xc * yc * (zc if dim == 3 else 1.0)
+        U[c, gz:gz + nz, ng:ng + n[1], ng:ng + n[0]] = v
+    return U
+
+
+def _tanh(xp, x):
+    return np.tanh(x) if xp is np else xp.tanh(x)
+
+
+def _clip(xp, x, lo, hi):
+    return np.clip(x, lo, hi) if xp is np else xp.clamp(x, lo, hi)
+
+
+def _sqrt(xp, x):
+    return np.sqrt(x) if xp is np else xp.sqrt(x)
+
+
+def advected_disc(n=128, ng=3, quadrature=True, xp=None, device=None):
+    """2D FIVEEQS advected interface on the periodic unit square: phase-2 disc of radius 0.25 at
+    (0.5, 0.5), alpha2 = 0.5(1 + tanh((0.25 - r)/(2 dx))) clipped to [1e-6, 1 - 1e-6]; phase 1 ideal
+    gas (gamma 1.4, rho 1), phase 2 stiffened gas (gamma 4.4, pinf 6e8, rho 1000); p = 1e5, u = v = 1.
+    WENO5 + HLLC + TVD-RK3, cfl 0.5."""
+    xp = _xp_of(xp)
+    dim, physics = 2, FIVEEQS
+    dx = (1.0 / n, 1.0 / n, 1.0)
+    g1, g2, pinf2 = 1.4, 4.4, 6e8
+    A = (1.0 / (g1 - 1.0), 1.0 / (g2 - 1.0))
+    B = (0.0, g2 * pinf2 / (g2 - 1.0))
+
+    def pw(x, y, z):
+        r = _sqrt(xp, (x - 0.5) ** 2 + (y - 0.5) ** 2)
+        a2 = _clip(xp, 0.5 * (1.0 + _tanh(xp, (0.25 - r) / (2.0 * dx[0]))), 1e-6, 1.0 - 1e-6)
+        a1 = 1.0 - a2
+        return _cons_from_prims(physics, dim, a1 * 1.0, a2 * 1000.0, [x * 0 + 1.0, y * 0 + 1.0], 1e5, a1, A, B, xp)
+
+    inputs = {"FiniteVolume.Scheme": "WENO5", "Physics.RiemannSolver": "HLLC", "prob.EOS.EOS": 1,
+              "prob.EOS.gamma_1": g1, "prob.EOS.gamma_2": g2, "prob.EOS.pinf_1": 0.0, "prob.EOS.pinf_2": pinf2,
+              "run.cfl": 0.5}
+    geom = dict(n=(n, n, 1), dx=dx, ng=ng, lo_bc=(0, 0, 0), hi_bc=(0, 0, 0))
+    U = _average(physics, dim, (n, n, 1), dx, (0.0, 0.0, 0.0), pw, ng, quadrature, xp, device)
+    return physics, dim, inputs, geom, U
+
+
+def shock_bubble(nx=2048, ny=1024, ng=3, quadrature=True, xp=None, device=None, Ma=1.22, rho_b=0.138,
+                 gamma_b=1.648, radius=0.25, center=(0.6, 0.5), scheme="WENO5B"):
+    """2D FIVEEQS shock-helium-bubble on [0,2]x[0,1]: air (phase 1, gamma 1.4, rho 1, p 1), helium
+    bubble (phase 2) with a tanh interface of width 2 dx, a Mach-Ma shock at x = 0.2 with the
+    Rankine-Hugoniot post-shock state on its left; reflective top/bottom (code 4), outflow
+    left/right (code 2)."""
+    xp = _xp_of(xp)
+    dim, physics = 2, FIVEEQS
+    L = 2.0
+    dx = (L / nx, 1.0 / ny, 1.0)
+    g1, g2 = 1.4, gamma_b
+    A = (1.0 / (g1 - 1.0), 1.0 / (g2 - 1.0))
+    B = (0.0, 0.0)
+    rs, us, ps = shock_state(Ma, 0.0, 1.0, 1.0, g1, 0.0)
+    eps = 1e-6
+
+    def pw(x, y, z):
+        r = _sqrt(xp, (x - center[0]) ** 2 + (y - center[1]) ** 2)
+        a2 = _clip(xp, 0.5 * (1.0 + _tanh(xp, (radius - r) / (2.0 * dx[0]))), eps, 1.0 - eps)
+        a1 = 1.0 - a2
+        post = (x < 0.2) * 1.0
+        rho1 = 1.0 + post * (rs - 1.0)
+        u = post * us
+        p = 1.0 + post * (ps - 1.0)
+        return _cons_from_prims(physics, dim, a1 * rho1, a2 * rho_b, [u, y * 0.0], p, a1, A, B, xp)
+
+    inputs = {"FiniteVolume.Scheme": scheme, "Physics.RiemannSolver": "HLLC", "prob.EOS.EOS": 1,
+              "prob.EOS.gamma_1": g1, "prob.EOS.gamma_2": g2, "run.cfl": 0.5}
+    geom = dict(n=(nx, ny, 1), dx=dx, ng=ng, lo_bc=(2, 4, 0), hi_bc=(2, 4, 0))
+    U = _average(physics, dim, (nx, ny, 1), dx, (0.0, 0.0, 0.0), pw, ng, quadrature, xp, device)
+    return physics, dim, inputs, geom, U
+
+
+def shock_droplet(n=256, ng=3, quadrature=True, xp=None, device=None, Ma=2.4, relaxation=1):
+    """3D SIXEQS shock-droplet in the unit cube: water droplet (phase 2, stiffened gas gamma 6.12,
+    pinf 3.43e8, rho 1000) of radius 0.1 at the centre, air (phase 1, gamma 1.4, rho 1.2, p 1e5), a
+    Mach-Ma air shock at x = 0.2 with the Rankine-Hugoniot state on its left; tanh interface of
+    width 2 dx clipped to [1e-6, 1 - 1e-6]; outflow (code 2) on all faces; pressure relaxation
+    after every stage. WENO5 + HLLC + TVD-RK3."""
+    xp = _xp_of(xp)
+    dim, physics = 3, SIXEQS
+    dx = (1.0 / n, 1.0 / n, 1.0 / n)
+    g1, g2, pinf2 = 1.4, 6.12, 3.43e8
+    A = (1.0 / (g1 - 1.0), 1.0 / (g2 - 1.0))
+    B = (0.0, g2 * pinf2 / (g2 - 1.0))
+    p0, rho_air = 1e5, 1.2
+    rs, us, ps = shock_state(Ma, 0.0, p0, rho_air, g1, 0.0)
+    eps = 1e-6
+
+    def pw(x, y, z):
+        r = _sqrt(xp, (x - 0.5) ** 2 + (y - 0.5) ** 2 + (z - 0.5) ** 2)
+        a2 = _clip(xp, 0.5 * (1.0 + _tanh(xp, (0.1 - r) / (2.0 * dx[0]))), eps, 1.0 - eps)
+        a1 = 1.0 - a2
+        post = (x < 0.2) * 1.0
+        rho1 = rho_air + post * (rs - rho_air)
+        u = post * us
+        p = p0 + post * (ps - p0)
+        return _cons_from_prims(physics, dim, a1 * rho1, a2 * 1000.0, [u, y * 0.0, z * 0.0], p, a1, A, B, xp)
+
+    inputs = {"FiniteVolume.Scheme": "WENO5", "Physics.RiemannSolver": "HLLC", "prob.EOS.EOS": 1,
+              "prob.EOS.gamma_1": g1, "prob.EOS.gamma_2": g2, "prob.EOS.pinf_2": pinf2,
+              "Physics.pressure_relaxation": relaxation, "run.cfl": 0.5}
+    geom = dict(n=(n, n, n), dx=dx, ng=ng, lo_bc=(2, 2, 2), hi_bc=(2, 2, 2))
+    U = _average(physics, dim, (n, n, n), dx, (0.0, 0.0, 0.0), pw, ng, quadrature, xp, device)
+    return physics, dim, inputs, geom, U
+
+
+def algorithmic_bytes_per_cell_stage(physics: int, dim: int) -> float:
+    """(8/3) N 8 B: stage 1 reads U and writes U1 (2N doubles), stages 2 and 3 read U^(s), U^0 and
+    write (3N doubles); relaxation is fused and adds nothing."""
+    return (8.0 / 3.0) * nstate(physics, dim) * 8.0

@@ -1,0 +1,740 @@
+// C-ABI of the B200 right-hand-side engine: parameters (the reference's inputs keys), the drop-in
+// stage kernels on caller-owned device arrays, and a single-level advance whose time-step control
+// runs on the device (no host synchronisation inside a run, CUDA-graph replay per step).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "compas_b200.h"
+#include "physics.cuh"
+#include "relax.cuh"
+#include "stage_kernel.cuh"
+
+namespace compas {
+
+// ------------------------------------------------------------------------------------------------
+// error reporting
+// ------------------------------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define CUDA_TRY(call)                                                                          \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            return fail(COMPAS_B200_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// ------------------------------------------------------------------------------------------------
+// small kernels: boundary fill, stand-alone relaxation, step control
+// ------------------------------------------------------------------------------------------------
+
+// AMReX BCType of component n across a face normal to d for a COMPAS boundary code
+// (source/Class_Compressible6Eq_PhaseField.cpp:352-434, Class_Compressible5Eq_PhaseField.cpp:162-):
+// 0 int_dir (periodic), 2 foextrap, 3/4 reflect_even with the normal momentum reflect_odd,
+// 5 reflect_odd for every momentum component.
+enum { kBcPeriodic = 0, kBcExtrap = 1, kBcEven = 2, kBcOdd = 3 };
+
+__device__ __forceinline__ int bc_kind(int code, int n, int d, int D) {
+    const bool mom = (n >= 2 && n < 2 + D);
+    switch (code) {
+        case 0: return kBcPeriodic;
+        case 2: return kBcExtrap;
+        case 3:
+        case 4: return (mom && n - 2 == d) ? kBcOdd : kBcEven;
+        default: return mom ? kBcOdd : kBcEven;  // 5: no-slip wall
+    }
+}
+
+struct BcArgs {
+    double* U;
+    Grid g;
+    int N, D;
+    int lo[3], hi[3];
+};
+
+// Map one coordinate of a ghost cell to its source along d; returns the sign factor.
+__device__ __forceinline__ double bc_map(int& x, int len, int code_lo, int code_hi, int n, int d, int D) {
+    if (x < 0) {
+        const int kind = bc_kind(code_lo, n, d, D);
+        if (kind == kBcPeriodic) { x += len; return 1.0; }
+        if (kind == kBcExtrap) { x = 0; return 1.0; }
+        x = -1 - x;
+        return kind == kBcOdd ? -1.0 : 1.0;
+    }
+    if (x >= len) {
+        const int kind = bc_kind(code_hi, n, d, D);
+        if (kind == kBcPeriodic) { x -= len; return 1.0; }
+        if (kind == kBcExtrap) { x = len - 1; return 1.0; }
+        x = 2 * len - 1 - x;
+        return kind == kBcOdd ? -1.0 : 1.0;
+    }
+    return 1.0;
+}
+
+// One thread per ghost cell (all components). Ghost cells are enumerated as the z slabs (full
+// padded planes), then the y slabs of the valid z range, then the x slabs of the valid y, z range.
+// Filling x, then y, then z over the full extent of the other directions (the oracle's order)
+// gives at every ghost cell the valid cell found by mapping each coordinate independently, with
+// the product of the per-direction signs, which is what this kernel computes directly.
+__global__ void fill_boundary_kernel(BcArgs a) {
+    const Grid& g = a.g;
+    const long long PX = g.px, PY = g.pxy / g.px;
+    const long long nz_slab = 2LL * g.gz * PX * PY;
+    const long long ny_slab = 2LL * g.ng * PX * g.n[2];
+    const long long nx_slab = 2LL * g.ng * g.n[1] * g.n[2];
+    const long long total = nz_slab + ny_slab + nx_slab;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+         q += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        if (q < nz_slab) {
+            const long long plane = PX * PY;
+            const int s = (int)(q / plane);
+            const long long r = q % plane;
+            i = (int)(r % PX) - g.ng;
+            j = (int)(r / PX) - g.ng;
+            k = (s < g.gz) ? s - g.gz : g.n[2] + (s - g.gz);
+        } else if (q < nz_slab + ny_slab) {
+            const long long r0 = q - nz_slab;
+            const long long row = PX * g.n[2];
+            const int s = (int)(r0 / row);
+            const long long r = r0 % row;
+            i = (int)(r % PX) - g.ng;
+            k = (int)(r / PX);
+            j = (s < g.ng) ? s - g.ng : g.n[1] + (s - g.ng);
+        } else {
+            const long long r0 = q - nz_slab - ny_slab;
+            const long long col = (long long)g.n[1] * g.n[2];
+            const int s = (int)(r0 / col);
+            const long long r = r0 % col;
+            j = (int)(r % g.n[1]);
+            k = (int)(r / g.n[1]);
+            i = (s < g.ng) ? s - g.ng : g.n[0] + (s - g.ng);
+        }
+        const long long dst = g.at(i, j, k);
+        for (int n = 0; n < a.N; ++n) {
+            int si = i, sj = j, sk = k;
+            double sgn = bc_map(si, g.n[0], a.lo[0], a.hi[0], n, 0, a.D);
+            sgn *= bc_map(sj, g.n[1], a.lo[1], a.hi[1], n, 1, a.D);
+            if (a.D == 3) sgn *= bc_map(sk, g.n[2], a.lo[2], a.hi[2], n, 2, a.D);
+            a.U[n * g.S + dst] = sgn * a.U[n * g.S + g.at(si, sj, sk)];
+        }
+    }
+}
+
+template <int D>
+__global__ void relax_kernel(double* U, Grid g, Eos e, double trace, unsigned int* err) {
+    constexpr int N = SixEq<D>::N;
+    const long long cells = (long long)g.n[0] * g.n[1] * g.n[2];
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < cells;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % g.n[0]);
+        const int j = (int)((c / g.n[0]) % g.n[1]);
+        const int k = (int)(c / ((long long)g.n[0] * g.n[1]));
+        const long long q = g.at(i, j, k);
+        double v[N];
+        for (int n = 0; n < N; ++n) v[n] = U[n * g.S + q];
+        relax_pressure<D>(v, e, trace, err);
+        for (int n = 0; n < N; ++n) U[n * g.S + q] = v[n];
+    }
+}
+
+// Device-resident time-step control of one level (COMPAS::ComputeDt, source/COMPAS.cpp:2249-2303,
+// and the coarse-step loop of Compressible_PhaseField::Evolve, source/Class_Compressible_PhaseField.cpp:201).
+struct StepCtl {
+    double t;
+    double dt;
+    double dt_prev;             // COMPAS dt[lev], 1e100 before the first step (source/COMPAS.cpp:81)
+    double stop_time;
+    unsigned long long cmax;    // bits of the largest face speed of the last step's stages
+    int steps;
+    int done;
+    unsigned int err;
+    int pad;
+};
+
+struct StepParams {
+    double cfl;
+    double dx[3];
+    int D;
+    int limiter;
+    double* dts;
+    int dts_cap;
+};
+
+__global__ void step_begin_kernel(StepCtl* s, StepParams p) {
+    if (s->done) return;
+    if (!(s->t < s->stop_time)) {
+        s->done = 1;
+        return;
+    }
+    const double cmax = __longlong_as_double((long long)s->cmax);
+    double dt_est = DBL_MAX;
+    for (int d = 0; d < p.D; ++d) dt_est = dmin(dt_est, p.cfl * p.dx[d] / cmax);
+    if (s->t == 0.0) s->dt_prev = dt_est;
+    if (p.limiter && s->dt_prev > 0.0) dt_est = dmin(dt_est, 1.1 * s->dt_prev);
+    double dt0 = dt_est;
+    const double eps = 1.0e-3 * dt0;
+    if (s->t + dt0 > s->stop_time - eps) dt0 = s->stop_time - s->t;
+    if (!(dt0 > 0.0) || !(dt0 <= DBL_MAX)) {
+        s->err |= COMPAS_B200_ERR_CFL;
+        s->done = 1;
+        return;
+    }
+    s->dt = dt0;
+    s->dt_prev = dt0;
+    s->cmax = 0ull;  // stage 0 resets c_max (source/Class_Compressible_PhaseField.cpp:3162-3164)
+    if (p.dts && s->steps < p.dts_cap) p.dts[s->steps] = dt0;
+}
+
+__global__ void step_end_kernel(StepCtl* s) {
+    if (s->done) return;
+    s->t += s->dt;
+    s->steps += 1;
+}
+
+__global__ void set_time_kernel(StepCtl* s, double t0, double stop_time, int reset) {
+    if (reset) {
+        s->t = t0;
+        s->dt = 0.0;
+        s->dt_prev = 1.e100;
+        s->cmax = 0ull;
+        s->steps = 0;
+        s->err = 0u;
+    }
+    s->stop_time = stop_time;
+    s->done = 0;
+}
+
+// ------------------------------------------------------------------------------------------------
+// launch helpers
+// ------------------------------------------------------------------------------------------------
+static Grid make_grid(const compas_b200_parm* p, const compas_b200_geom* g) {
+    Grid G;
+    G.n[0] = g->n[0];
+    G.n[1] = g->n[1];
+    G.n[2] = (p->dim == 3) ? g->n[2] : 1;
+    G.ng = g->ng;
+    G.gz = (p->dim == 3) ? g->ng : 0;
+    G.px = G.n[0] + 2 * G.ng;
+    const long long py = G.n[1] + 2 * G.ng;
+    const long long pz = G.n[2] + 2 * G.gz;
+    G.pxy = G.px * py;
+    G.S = G.pxy * pz;
+    G.dx[0] = g->dx[0];
+    G.dx[1] = g->dx[1];
+    G.dx[2] = (p->dim == 3) ? g->dx[2] : 1.0;
+    return G;
+}
+
+static Eos make_eos(const compas_b200_parm* p) {
+    return Eos{p->A1, p->A2, p->B1, p->B2, p->C1, p->C2, p->D1, p->D2};
+}
+
+static int nstate(const compas_b200_parm* p) {
+    return (p->physics == COMPAS_B200_FIVEEQS ? 4 : 5) + p->dim;
+}
+
+static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
+    if (!p || !g) return fail(COMPAS_B200_EARG, "null parameter or geometry");
+    if (p->physics != COMPAS_B200_FIVEEQS && p->physics != COMPAS_B200_SIXEQS)
+        return fail(COMPAS_B200_EARG, "physics must be FIVEEQS (555) or SIXEQS (666)");
+    if (p->dim != 2 && p->dim != 3) return fail(COMPAS_B200_EARG, "dim must be 2 or 3");
+    if (p->id_limiter != 5)
+        return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.Scheme: this build runs WENO5");
+    if (p->thinc) return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.THINC = 1 is not available in this build");
+    if (p->id_riemann != 2) return fail(COMPAS_B200_EUNSUPPORTED, "Physics.RiemannSolver: this build runs HLLC");
+    if (p->precision != 0) return fail(COMPAS_B200_EUNSUPPORTED, "only the plain FP64 form is available");
+    if (g->ng < 3) return fail(COMPAS_B200_EARG, "WENO5 needs ng >= 3 ghost cells");
+    for (int d = 0; d < p->dim; ++d) {
+        if (g->n[d] < 1) return fail(COMPAS_B200_EARG, "empty box");
+        if (!(g->dx[d] > 0.0)) return fail(COMPAS_B200_EARG, "cell sizes must be positive");
+        for (int code : {g->lo_bc[d], g->hi_bc[d]})
+            if (code != 0 && code != 2 && code != 3 && code != 4 && code != 5)
+                return fail(COMPAS_B200_EARG, "boundary codes: 0 interior, 2 outflow, 3 symmetry, 4 slip wall, "
+                                              "5 no-slip wall (1 inflow needs a user function)");
+        if ((g->lo_bc[d] == 0) != (g->hi_bc[d] == 0))
+            return fail(COMPAS_B200_EARG, "a periodic direction needs code 0 on both sides");
+        if (g->lo_bc[d] == 0 && g->n[d] < g->ng)
+            return fail(COMPAS_B200_EARG, "a periodic direction needs at least ng cells");
+        if (g->lo_bc[d] != 0 && g->lo_bc[d] != 2 && g->n[d] < g->ng)
+            return fail(COMPAS_B200_EARG, "a reflecting boundary needs at least ng cells");
+    }
+    if (p->dim == 2 && g->n[2] != 1) return fail(COMPAS_B200_EARG, "n[2] must be 1 in 2D");
+    return COMPAS_B200_OK;
+}
+
+template <class M, int TX, int TY, int TZ, int NT, int MINB>
+static int launch_stage_t(const StageArgs& a, cudaStream_t st) {
+    using T = TileShape<M, TX, TY, TZ>;
+    auto kern = stage_kernel<M, TX, TY, TZ, NT, MINB>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
+        attr_set = true;
+    }
+    const long long tiles = (long long)((a.g.n[0] + TX - 1) / TX) * ((a.g.n[1] + TY - 1) / TY) *
+                            ((a.g.n[2] + TZ - 1) / TZ);
+    if (tiles > 0x7fffffffLL) return fail(COMPAS_B200_EARG, "box too large");
+    kern<<<(unsigned)tiles, NT, T::SMEM, st>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    return COMPAS_B200_OK;
+}
+
+static int launch_stage(const compas_b200_parm* p, const StageArgs& a, cudaStream_t st) {
+    if (p->physics == COMPAS_B200_FIVEEQS) {
+        if (p->dim == 2) return launch_stage_t<FiveEq<2>, 16, 16, 1, 272, 2>(a, st);
+        return launch_stage_t<FiveEq<3>, 8, 8, 8, 288, 2>(a, st);
+    }
+    if (p->dim == 2) return launch_stage_t<SixEq<2>, 16, 16, 1, 272, 2>(a, st);
+    return launch_stage_t<SixEq<3>, 8, 8, 8, 288, 2>(a, st);
+}
+
+static int launch_fill(const compas_b200_parm* p, const compas_b200_geom* geo, double* U, cudaStream_t st) {
+    BcArgs b;
+    b.U = U;
+    b.g = make_grid(p, geo);
+    b.N = nstate(p);
+    b.D = p->dim;
+    for (int d = 0; d < 3; ++d) {
+        b.lo[d] = geo->lo_bc[d];
+        b.hi[d] = geo->hi_bc[d];
+    }
+    const Grid& g = b.g;
+    const long long total = 2LL * g.gz * g.pxy + 2LL * g.ng * g.px * g.n[2] + 2LL * g.ng * g.n[1] * g.n[2];
+    const int threads = 256;
+    long long blocks = (total + threads - 1) / threads;
+    if (blocks > 148LL * 16) blocks = 148LL * 16;
+    if (blocks < 1) blocks = 1;
+    fill_boundary_kernel<<<(unsigned)blocks, threads, 0, st>>>(b);
+    CUDA_TRY(cudaGetLastError());
+    return COMPAS_B200_OK;
+}
+
+static StageArgs base_args(const compas_b200_parm* p, const compas_b200_geom* g) {
+    StageArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.g = make_grid(p, g);
+    a.e = make_eos(p);
+    a.id_k = p->source_term;
+    a.relax = (p->physics == COMPAS_B200_SIXEQS) ? p->relaxation : 0;
+    a.trace = p->relax_trace;
+    return a;
+}
+
+}  // namespace compas
+
+// ================================================================================================
+// C ABI
+// ================================================================================================
+using namespace compas;
+
+struct compas_b200_level {
+    compas_b200_parm p;
+    compas_b200_geom g;
+    double* U = nullptr;   // state U^n (in place across steps)
+    double* U1 = nullptr;  // stage buffers
+    double* U2 = nullptr;
+    StepCtl* ctl = nullptr;
+    double* dts = nullptr;
+    int dts_cap = 0;
+    long long bytes = 0;
+    long long launches = 0;
+    bool need_init = true;
+    cudaGraphExec_t graph = nullptr;
+    cudaStream_t graph_stream = nullptr;
+};
+
+extern "C" {
+
+const char* compas_b200_last_error(void) { return g_last_error.c_str(); }
+
+int compas_b200_parm_init(compas_b200_parm* p, int physics, int dim) {
+    if (!p) return fail(COMPAS_B200_EARG, "null parm");
+    std::memset(p, 0, sizeof(*p));
+    p->physics = physics;
+    p->dim = dim;
+    p->eos = 1;
+    p->gamma_1 = 1.4;
+    p->gamma_2 = 1.4;
+    p->id_limiter = 5;
+    p->num_grow = 3;
+    p->thinc = 0;
+    p->thinc_use_normal = 1;
+    p->thinc_eps = 1.0e-4;
+    p->thinc_beta = 2.3;
+    p->thinc_normal_threshold = 0.25;
+    p->id_riemann = 2;
+    p->cfl = 0.4;
+    p->change_limiter = 1;
+    if (physics != COMPAS_B200_FIVEEQS && physics != COMPAS_B200_SIXEQS)
+        return fail(COMPAS_B200_EARG, "physics must be FIVEEQS (555) or SIXEQS (666)");
+    if (dim != 2 && dim != 3) return fail(COMPAS_B200_EARG, "dim must be 2 or 3");
+    return compas_b200_parm_finalize(p);
+}
+
+static bool parse_double(const char* v, double* out) {
+    char* end = nullptr;
+    const double x = std::strtod(v, &end);
+    if (end == v) return false;
+    while (*end == ' ') ++end;
+    if (*end) return false;
+    *out = x;
+    return true;
+}
+
+static bool parse_int(const char* v, int* out) {
+    char* end = nullptr;
+    const long x = std::strtol(v, &end, 10);
+    if (end == v) return false;
+    while (*end == ' ') ++end;
+    if (*end) return false;
+    *out = (int)x;
+    return true;
+}
+
+int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value) {
+    if (!p || !key || !value) return fail(COMPAS_B200_EARG, "null argument");
+    const std::string k(key), v(value);
+    auto bad = [&](const std::string& valid) {
+        return fail(COMPAS_B200_EARG, k + " = '" + v + "' is not recognized. Valid values are " + valid + ".");
+    };
+    double x;
+    int ix;
+    if (k == "FiniteVolume.Scheme") {
+        // include/Operators_FV/FiniteVolume_Parameter.H:51-147
+        if (v == "WENO5") { p->id_limiter = 5; p->num_grow = 3; return 0; }
+        if (v == "WENO5B") { p->id_limiter = 6; p->num_grow = 3; return 0; }
+        if (v == "GODUNOV" || v == "MUSCL" || v == "MUSCL-Minmod" || v == "MUSCL-vanLeer" ||
+            v == "MUSCL-Superbee" || v == "MUSCL-MC" || v == "WENO3" || v == "WENO3B")
+            return fail(COMPAS_B200_EUNSUPPORTED, k + " = " + v + " is a valid reference scheme outside this engine's "
+                                                  "hot path (WENO5, WENO5B)");
+        return bad("GODUNOV, MUSCL, MUSCL-Minmod, MUSCL-vanLeer, MUSCL-Superbee, MUSCL-MC, WENO3, WENO3B, WENO5, WENO5B");
+    }
+    if (k == "FiniteVolume.THINC") { if (!parse_int(value, &ix) || ix < 0 || ix > 1) return bad("0, 1"); p->thinc = ix; return 0; }
+    if (k == "FiniteVolume.THINC.UseNormal") { if (!parse_int(value, &ix)) return bad("an integer"); p->thinc_use_normal = ix; return 0; }
+    if (k == "FiniteVolume.THINC.EPS") { if (!parse_double(value, &x)) return bad("a number"); p->thinc_eps = x; return 0; }
+    if (k == "FiniteVolume.THINC.Beta") { if (!parse_double(value, &x)) return bad("a number"); p->thinc_beta = x; return 0; }
+    if (k == "FiniteVolume.THINC.NormalThreshold") { if (!parse_double(value, &x)) return bad("a number"); p->thinc_normal_threshold = x; return 0; }
+    if (k == "FiniteVolume.ID_Bound") {
+        if (!parse_int(value, &ix) || ix < 0 || ix > 1) return bad("0, 1");
+        if (ix == 1) return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.ID_Bound = 1 is outside this engine's hot path");
+        return 0;
+    }
+    if (k == "Physics.RiemannSolver") {
+        // source/Class_Compressible_PhaseField.cpp:92-111
+        if (v == "HLLC") { p->id_riemann = 2; return 0; }
+        if (v == "LLF" || v == "HLL") { p->id_riemann = (v == "LLF") ? 0 : 1; return 0; }
+        return bad("LLF, HLL, HLLC");
+    }
+    if (k == "Physics.source_term") {
+        if (!parse_int(value, &ix) || ix < 0 || ix > 1) return fail(COMPAS_B200_EARG, "Physics.source_term must be 0 or 1.");
+        p->source_term = ix;
+        return 0;
+    }
+    if (k == "Physics.pressure_relaxation") { if (!parse_int(value, &ix)) return bad("0, 1"); p->relaxation = ix ? 1 : 0; return 0; }
+    if (k == "Physics.pressure_relaxation_trace") {
+        if (!parse_double(value, &x) || x < 0.0 || x >= 1.0)
+            return fail(COMPAS_B200_EARG, "Physics.pressure_relaxation_trace must be in [0, 1).");
+        p->relax_trace = x;
+        return 0;
+    }
+    if (k == "prob.EOS.EOS") {
+        if (!parse_int(value, &ix) || (ix != 0 && ix != 1 && ix != 3))
+            return fail(COMPAS_B200_EARG, "prob.EOS.EOS = " + v + " is not recognized. Valid values are 0 (ideal gas), "
+                                          "1 (stiffened gas), 3 (Noble-Abel stiffened gas); 2 (Mie-Gruneisen) is outside "
+                                          "this engine's hot path.");
+        p->eos = ix;
+        return 0;
+    }
+    struct DKey { const char* name; double* dst; };
+    const DKey dkeys[] = {{"prob.EOS.gamma_1", &p->gamma_1}, {"prob.EOS.gamma_2", &p->gamma_2},
+                          {"prob.EOS.pinf_1", &p->pinf_1},   {"prob.EOS.pinf_2", &p->pinf_2},
+                          {"prob.EOS.b_1", &p->b_1},         {"prob.EOS.b_2", &p->b_2},
+                          {"prob.EOS.q_1", &p->q_1},         {"prob.EOS.q_2", &p->q_2},
+                          {"run.cfl", &p->cfl}};
+    for (const auto& dk : dkeys)
+        if (k == dk.name) {
+            if (!parse_double(value, &x)) return bad("a number");
+            *dk.dst = x;
+            return 0;
+        }
+    if (k == "run.timestep_change_limiter") { if (!parse_int(value, &ix)) return bad("0, 1"); p->change_limiter = ix ? 1 : 0; return 0; }
+    return fail(COMPAS_B200_EARG, "unknown inputs key '" + k + "'");
+}
+
+int compas_b200_parm_finalize(compas_b200_parm* p) {
+    if (!p) return fail(COMPAS_B200_EARG, "null parm");
+    // source/Parm.cpp:101-188
+    if (!(p->gamma_1 > 1.0) || !(p->gamma_2 > 1.0))
+        return fail(COMPAS_B200_EARG, "prob.EOS.EOS requires gamma > 1 for both phases");
+    p->A1 = 1. / (p->gamma_1 - 1.);
+    p->A2 = 1. / (p->gamma_2 - 1.);
+    if (p->eos == 0) {
+        p->B1 = 0.; p->B2 = 0.; p->C1 = 0.; p->C2 = 0.; p->D1 = 0.; p->D2 = 0.;
+    } else if (p->eos == 1) {
+        p->B1 = p->gamma_1 * p->pinf_1 / (p->gamma_1 - 1.);
+        p->B2 = p->gamma_2 * p->pinf_2 / (p->gamma_2 - 1.);
+        p->C1 = 0.; p->C2 = 0.; p->D1 = 0.; p->D2 = 0.;
+    } else if (p->eos == 3) {
+        if (p->b_1 < 0.0 || p->b_2 < 0.0) return fail(COMPAS_B200_EARG, "prob.EOS.b_k must be >= 0");
+        p->B1 = p->gamma_1 * p->pinf_1 / (p->gamma_1 - 1.);
+        p->B2 = p->gamma_2 * p->pinf_2 / (p->gamma_2 - 1.);
+        p->C1 = p->b_1; p->C2 = p->b_2; p->D1 = p->q_1; p->D2 = p->q_2;
+    } else {
+        return fail(COMPAS_B200_EARG, "prob.EOS.EOS must be 0, 1 or 3");
+    }
+    return COMPAS_B200_OK;
+}
+
+long long compas_b200_state_bytes(const compas_b200_parm* p, const compas_b200_geom* g) {
+    if (!p || !g) return 0;
+    const Grid G = make_grid(p, g);
+    return G.S * (long long)nstate(p) * (long long)sizeof(double);
+}
+
+int compas_b200_fill_boundary(const compas_b200_parm* p, const compas_b200_geom* g, double* U, void* stream) {
+    int rc = check_args(p, g);
+    if (rc) return rc;
+    if (!U) return fail(COMPAS_B200_EARG, "null state");
+    return launch_fill(p, g, U, (cudaStream_t)stream);
+}
+
+int compas_b200_compute_dUdt(const compas_b200_parm* p, const compas_b200_geom* g, const double* U, double* dUdt,
+                             double* cmax_dev, unsigned int* err_dev, void* stream) {
+    int rc = check_args(p, g);
+    if (rc) return rc;
+    if (!U || !dUdt) return fail(COMPAS_B200_EARG, "null state");
+    StageArgs a = base_args(p, g);
+    a.Us = U;
+    a.Uout = dUdt;
+    a.mode = kModeDudt;
+    a.cmax = reinterpret_cast<unsigned long long*>(cmax_dev);
+    a.err = err_dev;
+    return launch_stage(p, a, (cudaStream_t)stream);
+}
+
+int compas_b200_rk3_stage(const compas_b200_parm* p, const compas_b200_geom* g, int stage, const double* Us,
+                          const double* Uold, double* Unew, const double* dt_dev, double* cmax_dev,
+                          unsigned int* err_dev, void* stream) {
+    int rc = check_args(p, g);
+    if (rc) return rc;
+    if (stage < 0 || stage > 2) return fail(COMPAS_B200_EARG, "stage must be 0, 1 or 2");
+    if (!Us || !Unew || !dt_dev || (stage > 0 && !Uold)) return fail(COMPAS_B200_EARG, "null argument");
+    if (Us == Unew) return fail(COMPAS_B200_EARG, "Unew may not alias Us");
+    StageArgs a = base_args(p, g);
+    a.Us = Us;
+    a.U0 = Uold;
+    a.Uout = Unew;
+    a.mode = kModeStage;
+    a.stage = stage;
+    a.dt = dt_dev;
+    a.cmax = reinterpret_cast<unsigned long long*>(cmax_dev);
+    a.err = err_dev;
+    return launch_stage(p, a, (cudaStream_t)stream);
+}
+
+int compas_b200_relaxation(const compas_b200_parm* p, const compas_b200_geom* g, double* U, unsigned int* err_dev,
+                           void* stream) {
+    int rc = check_args(p, g);
+    if (rc) return rc;
+    if (p->physics != COMPAS_B200_SIXEQS) return COMPAS_B200_OK;
+    const Grid G = make_grid(p, g);
+    const long long cells = (long long)G.n[0] * G.n[1] * G.n[2];
+    long long blocks = (cells + 127) / 128;
+    if (blocks > 148LL * 32) blocks = 148LL * 32;
+    if (p->dim == 2)
+        relax_kernel<2><<<(unsigned)blocks, 128, 0, (cudaStream_t)stream>>>(U, G, make_eos(p), p->relax_trace, err_dev);
+    else
+        relax_kernel<3><<<(unsigned)blocks, 128, 0, (cudaStream_t)stream>>>(U, G, make_eos(p), p->relax_trace, err_dev);
+    CUDA_TRY(cudaGetLastError());
+    return COMPAS_B200_OK;
+}
+
+int compas_b200_level_create(const compas_b200_parm* p, const compas_b200_geom* g, compas_b200_level** out) {
+    if (!out) return fail(COMPAS_B200_EARG, "null output");
+    *out = nullptr;
+    int rc = check_args(p, g);
+    if (rc) return rc;
+    auto* lv = new compas_b200_level();
+    lv->p = *p;
+    lv->g = *g;
+    if (p->dim == 2) lv->g.n[2] = 1;
+    lv->bytes = compas_b200_state_bytes(p, g);
+    lv->dts_cap = 1 << 16;
+    cudaError_t e = cudaMalloc(&lv->U, lv->bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&lv->U1, lv->bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&lv->U2, lv->bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&lv->ctl, sizeof(StepCtl));
+    if (e == cudaSuccess) e = cudaMalloc(&lv->dts, sizeof(double) * lv->dts_cap);
+    if (e == cudaSuccess) e = cudaMemset(lv->ctl, 0, sizeof(StepCtl));
+    if (e == cudaSuccess) e = cudaMemset(lv->U, 0, lv->bytes);
+    if (e == cudaSuccess) e = cudaMemset(lv->U1, 0, lv->bytes);
+    if (e == cudaSuccess) e = cudaMemset(lv->U2, 0, lv->bytes);
+    if (e != cudaSuccess) {
+        compas_b200_level_destroy(lv);
+        cudaGetLastError();
+        return fail(e == cudaErrorMemoryAllocation ? COMPAS_B200_ENOMEM : COMPAS_B200_ECUDA,
+                    std::string("level allocation: ") + cudaGetErrorString(e));
+    }
+    *out = lv;
+    return COMPAS_B200_OK;
+}
+
+int compas_b200_level_destroy(compas_b200_level* lv) {
+    if (!lv) return COMPAS_B200_OK;
+    if (lv->graph) cudaGraphExecDestroy(lv->graph);
+    cudaFree(lv->U);
+    cudaFree(lv->U1);
+    cudaFree(lv->U2);
+    cudaFree(lv->ctl);
+    cudaFree(lv->dts);
+    delete lv;
+    return COMPAS_B200_OK;
+}
+
+double* compas_b200_level_state(compas_b200_level* lv) { return lv ? lv->U : nullptr; }
+
+long long compas_b200_level_launches(compas_b200_level* lv) { return lv ? lv->launches : 0; }
+
+int compas_b200_level_upload(compas_b200_level* lv, const double* src, int is_device, double t0, void* stream) {
+    if (!lv || !src) return fail(COMPAS_B200_EARG, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    CUDA_TRY(cudaMemcpyAsync(lv->U, src, lv->bytes, is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    set_time_kernel<<<1, 1, 0, st>>>(lv->ctl, t0, 0.0, 1);
+    CUDA_TRY(cudaGetLastError());
+    lv->launches = 1;
+    lv->need_init = true;
+    return COMPAS_B200_OK;
+}
+
+int compas_b200_level_download(compas_b200_level* lv, double* dst, int is_device, void* stream) {
+    if (!lv || !dst) return fail(COMPAS_B200_EARG, "null argument");
+    CUDA_TRY(cudaMemcpyAsync(dst, lv->U, lv->bytes, is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                             (cudaStream_t)stream));
+    return COMPAS_B200_OK;
+}
+
+// The launches of one coarse step: ComputeDt, then three (fill, stage) pairs, then t += dt.
+static int enqueue_step(compas_b200_level* lv, cudaStream_t st) {
+    const compas_b200_parm* p = &lv->p;
+    const compas_b200_geom* g = &lv->g;
+    StepParams sp;
+    sp.cfl = p->cfl;
+    sp.dx[0] = g->dx[0];
+    sp.dx[1] = g->dx[1];
+    sp.dx[2] = g->dx[2];
+    sp.D = p->dim;
+    sp.limiter = p->change_limiter;
+    sp.dts = lv->dts;
+    sp.dts_cap = lv->dts_cap;
+    step_begin_kernel<<<1, 1, 0, st>>>(lv->ctl, sp);
+    CUDA_TRY(cudaGetLastError());
+    StageArgs a = base_args(p, g);
+    a.mode = kModeStage;
+    a.dt = &lv->ctl->dt;
+    a.done = &lv->ctl->done;
+    a.cmax = &lv->ctl->cmax;
+    a.err = &lv->ctl->err;
+    double* bufs_in[3] = {lv->U, lv->U1, lv->U2};
+    double* bufs_out[3] = {lv->U1, lv->U2, lv->U};
+    int rc;
+    for (int s = 0; s < 3; ++s) {
+        if ((rc = launch_fill(p, g, bufs_in[s], st))) return rc;
+        a.stage = s;
+        a.Us = bufs_in[s];
+        a.U0 = lv->U;
+        a.Uout = bufs_out[s];
+        if ((rc = launch_stage(p, a, st))) return rc;
+    }
+    step_end_kernel<<<1, 1, 0, st>>>(lv->ctl);
+    CUDA_TRY(cudaGetLastError());
+    return COMPAS_B200_OK;
+}
+
+int compas_b200_level_advance(compas_b200_level* lv, int nsteps, double stop_time, int use_graph, void* stream) {
+    if (!lv) return fail(COMPAS_B200_EARG, "null level");
+    if (nsteps < 0) return fail(COMPAS_B200_EARG, "nsteps must be >= 0");
+    cudaStream_t st = (cudaStream_t)stream;
+    set_time_kernel<<<1, 1, 0, st>>>(lv->ctl, 0.0, stop_time, 0);
+    CUDA_TRY(cudaGetLastError());
+    lv->launches += 1;
+    int rc;
+    if (lv->need_init) {
+        // CalculateInitialcmax (source/Class_Compressible_PhaseField.cpp:4501-4605)
+        if ((rc = launch_fill(&lv->p, &lv->g, lv->U, st))) return rc;
+        StageArgs a = base_args(&lv->p, &lv->g);
+        a.Us = lv->U;
+        a.mode = kModeCmax;
+        a.cmax = &lv->ctl->cmax;
+        a.err = &lv->ctl->err;
+        if ((rc = launch_stage(&lv->p, a, st))) return rc;
+        lv->launches += 2;
+        lv->need_init = false;
+    }
+    if (nsteps == 0) return COMPAS_B200_OK;
+    if (use_graph) {
+        if (!lv->graph || lv->graph_stream != st) {
+            if (lv->graph) {
+                cudaGraphExecDestroy(lv->graph);
+                lv->graph = nullptr;
+            }
+            // capture on a private stream so a legacy default stream can be used by the caller
+            cudaStream_t cap;
+            CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+            cudaGraph_t graph;
+            cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) {
+                cudaStreamDestroy(cap);
+                return fail(COMPAS_B200_ECUDA, std::string("begin capture: ") + cudaGetErrorString(e));
+            }
+            rc = enqueue_step(lv, cap);
+            e = cudaStreamEndCapture(cap, &graph);
+            cudaStreamDestroy(cap);
+            if (rc) return rc;
+            if (e != cudaSuccess) return fail(COMPAS_B200_ECUDA, std::string("end capture: ") + cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&lv->graph, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) return fail(COMPAS_B200_ECUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+            lv->graph_stream = st;
+        }
+        for (int s = 0; s < nsteps; ++s) CUDA_TRY(cudaGraphLaunch(lv->graph, st));
+    } else {
+        for (int s = 0; s < nsteps; ++s)
+            if ((rc = enqueue_step(lv, st))) return rc;
+    }
+    lv->launches += 8LL * nsteps;
+    return COMPAS_B200_OK;
+}
+
+int compas_b200_level_sync(compas_b200_level* lv, double* t, int* steps, unsigned int* status) {
+    if (!lv) return fail(COMPAS_B200_EARG, "null level");
+    StepCtl h;
+    CUDA_TRY(cudaDeviceSynchronize());
+    CUDA_TRY(cudaMemcpy(&h, lv->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost));
+    if (t) *t = h.t;
+    if (steps) *steps = h.steps;
+    if (status) *status = h.err;
+    const unsigned int fatal = COMPAS_B200_ERR_NAN | COMPAS_B200_ERR_COVOLUME | COMPAS_B200_ERR_CFL;
+    if (h.err & fatal) return fail(COMPAS_B200_ESTATE, "status word " + std::to_string(h.err));
+    return COMPAS_B200_OK;
+}
+
+int compas_b200_level_dts(compas_b200_level* lv, double* dts, int n) {
+    if (!lv || !dts) return fail(COMPAS_B200_EARG, "null argument");
+    if (n > lv->dts_cap) n = lv->dts_cap;
+    if (n <= 0) return COMPAS_B200_OK;
+    CUDA_TRY(cudaMemcpy(dts, lv->dts, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    return COMPAS_B200_OK;
+}
+
+}  // extern "C"

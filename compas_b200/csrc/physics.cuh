@@ -1,0 +1,417 @@
+// Pointwise physics of the two-phase diffuse-interface models on the device: state layout,
+// conservative <-> primitive conversion through the stiffened-gas / NASG EOS, sound speed, WENO5
+// face values, the HLLC flux and the six-equation pressure relaxation.
+//
+// The plain FP64 path must reproduce the reference arithmetic to the bit, so every formula below is
+// evaluated with the same operations in the same association as the reference (C++ evaluates a+b+c
+// as (a+b)+c and a*b*c as (a*b)*c), and the library is compiled with FMA contraction off. Where a
+// value is recomputed several times in the reference from the same inputs it is computed once here:
+// the result is the same double.
+//
+// Reference correspondence (file:line in the reference tree):
+//   state layout           include/Physics_Compressible5Eq/Variables_Compressible5Eq.H:16-25
+//                          include/Physics_Compressible6Eq/Variables_Compressible6Eq.H:16-26
+//   NASG covolume          include/EquationOfState_NASG.H:26-58
+//   5Eq C2P / P2C / EOS    include/Physics_Compressible5Eq/Conservative2Primitive_Compressible5Eq.H:15-61,
+//                          Primitive2Conservative_Compressible5Eq.H, EquationOfState_Mixture_Compressible5Eq.H:15-77
+//   5Eq sound speed        SoundSpeed_Compressible5Eq.H, rho_c2_Mixture_Compressible5Eq.H, rho_c2_Phase_Compressible5Eq.H
+//   6Eq C2P / P2C / EOS    include/Physics_Compressible6Eq/Conservative2Primitive_Compressible6Eq.H:15-80,
+//                          Primitive2Conservative_Compressible6Eq.H, EquationOfState_Phase_Compressible6Eq.H:15-73
+//   6Eq sound speed        SoundSpeed_Compressible6Eq.H, rho_c2_Phase_Compressible6Eq.H, rho_c2_Mixture_Compressible6Eq.H
+//   WENO5                  include/Operators_FV/WENO5.H:12-75, Reconstruction2Face_WENO.H
+//   HLLC                   include/Physics_Compressible5Eq/Riemann_HLLC_Compressible5Eq.H:16-194
+//                          include/Physics_Compressible6Eq/Riemann_HLLC_Compressible6Eq.H:16-255
+//   relaxation             include/Physics_Compressible6Eq/Relaxation_Pressure_Instantaneous_Compressible6Eq.H:32-220
+//                          include/RelaxationPressure_Safeguarded.H:17-256
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+
+#include "compas_b200.h"
+
+namespace compas {
+
+// Error bits of the per-run status word (compas_b200.h: COMPAS_B200_ERR_*).
+__device__ __forceinline__ void flag_error(unsigned int* err, unsigned int bit) {
+    if (err) atomicOr(err, bit);
+}
+
+// Reference semantics of std::min / std::max (first argument returned on ties and NaN second).
+__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ double sgn0(double x) { return x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : 0.0); }
+
+// EOS coefficients of the two phases, partial form alpha rho e = A Pi + B phi + alpha rho D, with
+// C the NASG covolume b (source/Parm.cpp:101-188).
+struct Eos {
+    double A1, A2, B1, B2, C1, C2, D1, D2;
+};
+
+// NASG: phi = alpha - b alpha rho (alpha when b = 0); covolume violation 1 - b rho <= 0 is reported
+// through the status word where the reference aborts.
+__device__ __forceinline__ double nasg_phi(double alpha, double alpha_rho, double b, unsigned int* err) {
+    if (b > 0.0 && alpha > 0.0) {
+        const double xi = 1.0 - b * (alpha_rho / alpha);
+        if (!(xi > 0.0)) flag_error(err, COMPAS_B200_ERR_COVOLUME);
+    }
+    return (b > 0.0) ? alpha - b * alpha_rho : alpha;
+}
+__device__ __forceinline__ double nasg_xi(double alpha, double alpha_rho, double b, unsigned int* err) {
+    if (b > 0.0 && alpha > 0.0) {
+        const double xi = 1.0 - b * (alpha_rho / alpha);
+        if (!(xi > 0.0)) flag_error(err, COMPAS_B200_ERR_COVOLUME);
+        return xi;
+    }
+    return 1.0;
+}
+
+template <int D>
+__device__ __forceinline__ double ksum(const double* u) {
+    // u*u + v*v (+ w*w), left to right
+    double s = u[0] * u[0] + u[1] * u[1];
+    if (D == 3) s = s + u[2] * u[2];
+    return s;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Five-equation model: U = (a1r1, a2r2, rho u_d, rho E, alpha1), W = (a1r1, a2r2, u_d, p, alpha1)
+// ------------------------------------------------------------------------------------------------
+template <int DIM>
+struct FiveEq {
+    static constexpr int D = DIM;
+    static constexpr int N = 4 + DIM;
+    static constexpr int NC = 1;       // face quantities of the non-conservative terms
+    static constexpr int IE = 2 + DIM;  // total energy
+    static constexpr int IA = 3 + DIM;  // alpha1
+
+    __device__ static __forceinline__ void cons2prim(double* W, const double* U, const Eos& e, unsigned int* err) {
+        const double a1r1 = U[0], a2r2 = U[1], alpha1 = U[IA];
+        const double rho = a1r1 + a2r2;
+        double u[3];
+        for (int d = 0; d < D; ++d) u[d] = U[2 + d] / rho;
+        const double rho_e = U[IE] - (0.5 * rho) * ksum<D>(u);
+        const double alpha2 = 1.0 - alpha1;
+        const double phi1 = nasg_phi(alpha1, a1r1, e.C1, err);
+        const double phi2 = nasg_phi(alpha2, a2r2, e.C2, err);
+        const double rho_D = a1r1 * e.D1 + a2r2 * e.D2;
+        const double AP = phi1 * e.A1 + phi2 * e.A2;
+        const double BP = phi1 * e.B1 + phi2 * e.B2;
+        W[0] = a1r1;
+        W[1] = a2r2;
+        for (int d = 0; d < D; ++d) W[2 + d] = u[d];
+        W[IE] = ((rho_e - rho_D) - BP) / AP;
+        W[IA] = alpha1;
+    }
+
+    __device__ static __forceinline__ void prim2cons(double* U, const double* W, const Eos& e, unsigned int* err) {
+        const double a1r1 = W[0], a2r2 = W[1], p = W[IE], alpha1 = W[IA];
+        const double rho = a1r1 + a2r2;
+        const double alpha2 = 1.0 - alpha1;
+        const double phi1 = nasg_phi(alpha1, a1r1, e.C1, err);
+        const double phi2 = nasg_phi(alpha2, a2r2, e.C2, err);
+        const double rho_D = a1r1 * e.D1 + a2r2 * e.D2;
+        const double AP = phi1 * e.A1 + phi2 * e.A2;
+        const double BP = phi1 * e.B1 + phi2 * e.B2;
+        const double rho_e = (AP * p + BP) + rho_D;
+        U[0] = a1r1;
+        U[1] = a2r2;
+        for (int d = 0; d < D; ++d) U[2 + d] = rho * W[2 + d];
+        U[IE] = rho_e + (0.5 * rho) * ksum<D>(W + 2);
+        U[IA] = alpha1;
+    }
+
+    // Mixture sound speed; source_term 0 (K = 0) or 1 (Wood).
+    __device__ static __forceinline__ double sound_speed(const double* W, const Eos& e, int id_k, unsigned int* err) {
+        const double a1r1 = W[0], a2r2 = W[1], p = W[IE], alpha1 = W[IA];
+        const double r1c1 = ((e.A1 + 1.0) * p + e.B1) / e.A1;
+        const double r2c2 = ((e.A2 + 1.0) * p + e.B2) / e.A2;
+        const double alpha2 = 1.0 - alpha1;
+        const double phi1 = nasg_phi(alpha1, a1r1, e.C1, err);
+        const double phi2 = nasg_phi(alpha2, a2r2, e.C2, err);
+        double rho_c2;
+        if (id_k == 0) {
+            const double ap_rc2 = (alpha1 * e.A1) * r1c1 + (alpha2 * e.A2) * r2c2;
+            const double AP = phi1 * e.A1 + phi2 * e.A2;
+            rho_c2 = ap_rc2 / AP;
+        } else {
+            rho_c2 = 1.0 / (phi1 / r1c1 + phi2 / r2c2);
+        }
+        const double rho = a1r1 + a2r2;
+        return sqrt(rho_c2 / rho);
+    }
+
+    // Kapila coefficient factor phi1 (1 + K1) of the alpha1 equation (FVM_SurfaceIntegralNC_Compressible5Eq.H:15-52).
+    __device__ static __forceinline__ double kapila_factor(const double* U, const double* W, const Eos& e, int id_k,
+                                                           unsigned int* err) {
+        const double alpha1 = U[IA];
+        double phi1 = (id_k == 1) ? nasg_phi(alpha1, U[0], e.C1, err) : alpha1;
+        double K1 = 0.0;
+        if (id_k == 1) {
+            const double p = W[IE];
+            const double r1c1 = ((e.A1 + 1.0) * p + e.B1) / e.A1;
+            const double r2c2 = ((e.A2 + 1.0) * p + e.B2) / e.A2;
+            const double alpha2 = 1.0 - alpha1;
+            const double ph1 = nasg_phi(alpha1, W[0], e.C1, err);
+            const double ph2 = nasg_phi(alpha2, W[1], e.C2, err);
+            const double rho_c2 = 1.0 / (ph1 / r1c1 + ph2 / r2c2);
+            K1 = rho_c2 / r1c1 - 1.0;
+        }
+        return phi1 * (1.0 + K1);
+    }
+
+    // Physical flux in direction d of the state U with primitives W (Conservative2Flux).
+    __device__ static __forceinline__ void flux(double* F, const double* U, const double* W, int d) {
+        const double V = W[2 + d];
+        const double p = W[IE];
+        F[0] = U[0] * V;
+        F[1] = U[1] * V;
+        for (int c = 0; c < D; ++c) F[2 + c] = U[2 + c] * V;
+        F[IE] = (U[IE] + p) * V;
+        F[IA] = U[IA] * V;
+        F[2 + d] = F[2 + d] + p;
+    }
+
+    // HLLC flux, the normal face velocity u* (FluxNC[0]) and the face wave speed.
+    __device__ static __forceinline__ void hllc(double* Fout, double* fnc, double& cmax, const double* UL,
+                                                const double* UR, const Eos& e, int d, int id_k, unsigned int* err) {
+        double WL[N], WR[N], FL[N], FR[N];
+        cons2prim(WL, UL, e, err);
+        cons2prim(WR, UR, e, err);
+        flux(FL, UL, WL, d);
+        flux(FR, UR, WR, d);
+        const double cL = sound_speed(WL, e, id_k, err);
+        const double cR = sound_speed(WR, e, id_k, err);
+        const double VL = WL[2 + d], VR = WR[2 + d];
+        const double pL = WL[IE], pR = WR[IE];
+        const double V_avg = 0.5 * (VL + VR);
+        const double c_avg = 0.5 * (cL + cR);
+        const double SL = dmin(V_avg - c_avg, VL - cL);
+        const double SR = dmax(V_avg + c_avg, VR + cR);
+        const double Sm = dmin(0.0, SL);
+        const double Sp = dmax(0.0, SR);
+        const double rhoL = WL[0] + WL[1];
+        const double rhoR = WR[0] + WR[1];
+        const double S_Star = (((pR - pL) + (rhoL * VL) * (SL - VL)) - (rhoR * VR) * (SR - VR)) /
+                              (rhoL * (SL - VL) - rhoR * (SR - VR));
+        const double s = sgn0(S_Star);
+        const double hp = 0.5 * (1.0 + s), hm = 0.5 * (1.0 - s);
+        const double fL = (SL - VL) / (SL - S_Star);
+        const double fR = (SR - VR) / (SR - S_Star);
+        // normal face velocity: Vel[d] = hp*uL_d + hm*uR_d, then += hp*Sm*(fL-1) + hm*Sp*(fR-1)
+        double vel = hp * VL + hm * VR;
+        vel = vel + ((hp * Sm) * (fL - 1.0) + (hm * Sp) * (fR - 1.0));
+        fnc[0] = vel;
+        for (int i = 0; i < N; ++i) {
+            double sL = fL * UL[i];
+            double sR = fR * UR[i];
+            if (i == 2 + d) {
+                sL = sL + (fL * rhoL) * (S_Star - VL);
+                sR = sR + (fR * rhoR) * (S_Star - VR);
+            } else if (i == IE) {
+                sL = sL + (fL * (S_Star - VL)) * (rhoL * S_Star + pL / (SL - VL));
+                sR = sR + (fR * (S_Star - VR)) * (rhoR * S_Star + pR / (SR - VR));
+            }
+            Fout[i] = hp * (FL[i] + Sm * (sL - UL[i])) + hm * (FR[i] + Sp * (sR - UR[i]));
+        }
+        const double qL = cL + sqrt(ksum<D>(WL + 2));
+        const double qR = cR + sqrt(ksum<D>(WR + 2));
+        cmax = dmax(qL, qR);
+    }
+};
+
+// ------------------------------------------------------------------------------------------------
+// Six-equation model: U = (a1r1, a2r2, rho u_d, a1r1E1, a2r2E2, alpha1),
+//                     W = (a1r1, a2r2, u_d, a1p1, a2p2, alpha1)
+// ------------------------------------------------------------------------------------------------
+template <int DIM>
+struct SixEq {
+    static constexpr int D = DIM;
+    static constexpr int N = 5 + DIM;
+    static constexpr int NC = 3;        // u_n, (u a1p1)_n, (u a2p2)_n
+    static constexpr int IE1 = 2 + DIM;
+    static constexpr int IE2 = 3 + DIM;
+    static constexpr int IA = 4 + DIM;
+
+    // alpha p of one phase from alpha rho e (EquationOfState_Phase, pressure base, e -> p)
+    __device__ static __forceinline__ double phase_p(double are, double alpha, double ar, double A, double B,
+                                                     double b, double Dq, unsigned int* err) {
+        const double xi = nasg_xi(alpha, ar, b, err);
+        const double phi = xi * alpha;
+        return ((are - ar * Dq) - phi * B) / (A * xi);
+    }
+    // alpha rho e of one phase from alpha p (p -> e)
+    __device__ static __forceinline__ double phase_e(double ap, double alpha, double ar, double A, double B,
+                                                     double b, double Dq, unsigned int* err) {
+        const double xi = nasg_xi(alpha, ar, b, err);
+        const double phi = xi * alpha;
+        return ((A * xi) * ap + phi * B) + ar * Dq;
+    }
+
+    __device__ static __forceinline__ void cons2prim(double* W, const double* U, const Eos& e, unsigned int* err) {
+        const double a1r1 = U[0], a2r2 = U[1], alpha1 = U[IA];
+        const double alpha2 = 1.0 - alpha1;
+        const double rho = a1r1 + a2r2;
+        double u[3];
+        for (int d = 0; d < D; ++d) u[d] = U[2 + d] / rho;
+        const double k = ksum<D>(u);
+        const double a1r1e1 = U[IE1] - (0.5 * a1r1) * k;
+        const double a2r2e2 = U[IE2] - (0.5 * a2r2) * k;
+        W[0] = a1r1;
+        W[1] = a2r2;
+        for (int d = 0; d < D; ++d) W[2 + d] = u[d];
+        W[IE1] = phase_p(a1r1e1, alpha1, a1r1, e.A1, e.B1, e.C1, e.D1, err);
+        W[IE2] = phase_p(a2r2e2, alpha2, a2r2, e.A2, e.B2, e.C2, e.D2, err);
+        W[IA] = alpha1;
+    }
+
+    __device__ static __forceinline__ void prim2cons(double* U, const double* W, const Eos& e, unsigned int* err) {
+        const double a1r1 = W[0], a2r2 = W[1], alpha1 = W[IA];
+        const double alpha2 = 1.0 - alpha1;
+        const double rho = a1r1 + a2r2;
+        U[0] = a1r1;
+        U[1] = a2r2;
+        for (int d = 0; d < D; ++d) U[2 + d] = rho * W[2 + d];
+        const double a1r1e1 = phase_e(W[IE1], alpha1, a1r1, e.A1, e.B1, e.C1, e.D1, err);
+        const double a2r2e2 = phase_e(W[IE2], alpha2, a2r2, e.A2, e.B2, e.C2, e.D2, err);
+        const double k = ksum<D>(W + 2);
+        U[IE1] = a1r1e1 + (0.5 * a1r1) * k;
+        U[IE2] = a2r2e2 + (0.5 * a2r2) * k;
+        U[IA] = alpha1;
+    }
+
+    // Frozen mixture sound speed: rho c^2 = sum alpha_k rho_k c_k^2.
+    __device__ static __forceinline__ double sound_speed(const double* W, const Eos& e, unsigned int* err) {
+        const double a1r1 = W[0], a2r2 = W[1], alpha1 = W[IA];
+        const double xi1 = nasg_xi(alpha1, a1r1, e.C1, err);
+        const double xi2 = nasg_xi(1.0 - alpha1, a2r2, e.C2, err);
+        const double r1c1 = ((e.A1 + 1.0) * W[IE1] + alpha1 * e.B1) / (e.A1 * xi1);
+        const double r2c2 = ((e.A2 + 1.0) * W[IE2] + (1.0 - alpha1) * e.B2) / (e.A2 * xi2);
+        const double rho_c2 = r1c1 + r2c2;
+        const double rho = a1r1 + a2r2;
+        return sqrt(rho_c2 / rho);
+    }
+
+    __device__ static __forceinline__ void flux(double* F, const double* U, const double* W, int d) {
+        const double V = W[2 + d];
+        F[0] = U[0] * V;
+        F[1] = U[1] * V;
+        for (int c = 0; c < D; ++c) F[2 + c] = U[2 + c] * V;
+        F[IE1] = (U[IE1] + W[IE1]) * V;
+        F[IE2] = (U[IE2] + W[IE2]) * V;
+        F[IA] = U[IA] * V;
+        F[2 + d] = F[2 + d] + (W[IE1] + W[IE2]);
+    }
+
+    // HLLC flux and the face quantities u_n, (u a1p1)_n, (u a2p2)_n of the non-conservative terms.
+    __device__ static __forceinline__ void hllc(double* Fout, double* fnc, double& cmax, const double* UL,
+                                                const double* UR, const Eos& e, int d, int /*id_k*/,
+                                                unsigned int* err) {
+        double WL[N], WR[N], FL[N], FR[N];
+        cons2prim(WL, UL, e, err);
+        cons2prim(WR, UR, e, err);
+        flux(FL, UL, WL, d);
+        flux(FR, UR, WR, d);
+        const double cL = sound_speed(WL, e, err);
+        const double cR = sound_speed(WR, e, err);
+        const double VL = WL[2 + d], VR = WR[2 + d];
+        const double SL = dmin(VL - cL, VR - cR);
+        const double SR = dmax(VL + cL, VR + cR);
+        const double Sm = dmin(0.0, SL);
+        const double Sp = dmax(0.0, SR);
+        const double a1r1L = WL[0], a2r2L = WL[1], a1r1R = WR[0], a2r2R = WR[1];
+        const double a1p1L = WL[IE1], a2p2L = WL[IE2], a1p1R = WR[IE1], a2p2R = WR[IE2];
+        const double rhoL = a1r1L + a2r2L;
+        const double rhoR = a1r1R + a2r2R;
+        const double pL = a1p1L + a2p2L;
+        const double pR = a1p1R + a2p2R;
+        const double S_Star = (((pR - pL) + (rhoL * VL) * (SL - VL)) - (rhoR * VR) * (SR - VR)) /
+                              (rhoL * (SL - VL) - rhoR * (SR - VR));
+        const double fL = (SL - VL) / (SL - S_Star);
+        const double fR = (SR - VR) / (SR - S_Star);
+        const double a1r1Ls = fL * a1r1L, a1r1Rs = fR * a1r1R;
+        const double a2r2Ls = fL * a2r2L, a2r2Rs = fR * a2r2R;
+        double UsL[N], UsR[N];
+        UsL[0] = a1r1Ls; UsL[1] = a2r2Ls;
+        UsR[0] = a1r1Rs; UsR[1] = a2r2Rs;
+        for (int c = 0; c < D; ++c) {
+            const double uLc = WL[2 + c], uRc = WR[2 + c];
+            const double nrm = (c == d) ? 1.0 : 0.0;
+            UsL[2 + c] = (fL * rhoL) * (uLc + nrm * (S_Star - uLc));
+            UsR[2 + c] = (fR * rhoR) * (uRc + nrm * (S_Star - uRc));
+        }
+        const double a1p1Ls = (a1p1L + ((VL - SL) * a1r1L) * VL) - ((S_Star - SL) * a1r1Ls) * S_Star;
+        const double a1p1Rs = (a1p1R + ((VR - SR) * a1r1R) * VR) - ((S_Star - SR) * a1r1Rs) * S_Star;
+        const double a2p2Ls = (a2p2L + ((VL - SL) * a2r2L) * VL) - ((S_Star - SL) * a2r2Ls) * S_Star;
+        const double a2p2Rs = (a2p2R + ((VR - SR) * a2r2R) * VR) - ((S_Star - SR) * a2r2Rs) * S_Star;
+        UsL[IE1] = (((VL - SL) * UL[IE1] + VL * a1p1L) - S_Star * a1p1Ls) / (S_Star - SL);
+        UsR[IE1] = (((VR - SR) * UR[IE1] + VR * a1p1R) - S_Star * a1p1Rs) / (S_Star - SR);
+        UsL[IE2] = (((VL - SL) * UL[IE2] + VL * a2p2L) - S_Star * a2p2Ls) / (S_Star - SL);
+        UsR[IE2] = (((VR - SR) * UR[IE2] + VR * a2p2R) - S_Star * a2p2Rs) / (S_Star - SR);
+        UsL[IA] = fL * WL[IA];
+        UsR[IA] = fR * WR[IA];
+        const double s = sgn0(S_Star);
+        const double hp = 0.5 * (1.0 + s), hm = 0.5 * (1.0 - s);
+        // normal components of Vel, Vel*a1p1, Vel*a2p2
+        const double uLd = WL[2 + d], uRd = WR[2 + d];
+        double vel = hp * uLd + hm * uRd;
+        vel = vel + ((hp * Sm) * (fL - 1.0) + (hm * Sp) * (fR - 1.0));
+        const double va1 = hp * (uLd * a1p1L + (1.0 * Sm) * (VL * a1p1L - S_Star * a1p1Ls) / (S_Star - SL)) +
+                           hm * (uRd * a1p1R + (1.0 * Sp) * (VR * a1p1R - S_Star * a1p1Rs) / (S_Star - SR));
+        const double va2 = hp * (uLd * a2p2L + (1.0 * Sm) * (VL * a2p2L - S_Star * a2p2Ls) / (S_Star - SL)) +
+                           hm * (uRd * a2p2R + (1.0 * Sp) * (VR * a2p2R - S_Star * a2p2Rs) / (S_Star - SR));
+        fnc[0] = vel;
+        fnc[1] = va1;
+        fnc[2] = va2;
+        for (int i = 0; i < N; ++i)
+            Fout[i] = hp * (FL[i] + Sm * (UsL[i] - UL[i])) + hm * (FR[i] + Sp * (UsR[i] - UR[i]));
+        const double qL = cL + sqrt(ksum<D>(WL + 2));
+        const double qR = cR + sqrt(ksum<D>(WR + 2));
+        cmax = dmax(qL, qR);
+    }
+};
+
+// ------------------------------------------------------------------------------------------------
+// WENO5 face value, epsilon-free weights from smoothness ratios with a NaN guard.
+// side = +1: value at the right face of the centre cell c; side = -1: at its left face.
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ double weno5(double f_mm, double f_m, double f_c, double f_p, double f_pp, int side) {
+    double q0, q1, q2, d0, d2;
+    if (side == 1) {
+        q0 = (f_c + (2.0 / 3.0) * (f_p - f_c)) - (1.0 / 6.0) * (f_pp - f_p);
+        q1 = (f_c + (1.0 / 6.0) * (f_c - f_m)) + (1.0 / 3.0) * (f_p - f_c);
+        q2 = (f_c - (1.0 / 3.0) * (f_m - f_mm)) + (5.0 / 6.0) * (f_c - f_m);
+        d0 = 3.0 / 10.0;
+        d2 = 1.0 / 10.0;
+    } else {
+        q0 = (f_c - (5.0 / 6.0) * (f_p - f_c)) + (1.0 / 3.0) * (f_pp - f_p);
+        q1 = (f_c - (1.0 / 3.0) * (f_c - f_m)) - (1.0 / 6.0) * (f_p - f_c);
+        q2 = (f_c + (1.0 / 6.0) * (f_m - f_mm)) - (2.0 / 3.0) * (f_c - f_m);
+        d0 = 1.0 / 10.0;
+        d2 = 3.0 / 10.0;
+    }
+    const double d1 = (1.0 - d0) - d2;
+    const double a = f_p - f_c, b = f_pp - f_p, c = f_c - f_m, g = f_m - f_mm;
+    const double IS0 = ((10.0 / 3.0) * a) * a - ((11.0 / 3.0) * a) * b + ((4.0 / 3.0) * b) * b;
+    const double IS1 = (-(5.0 / 3.0) * c) * a + ((4.0 / 3.0) * c) * c + ((4.0 / 3.0) * a) * a;
+    const double IS2 = ((10.0 / 3.0) * c) * c - ((11.0 / 3.0) * g) * c + ((4.0 / 3.0) * g) * g;
+    double IS01 = IS0 / IS1;
+    if (isnan(IS01)) IS01 = 1.0;
+    const double IS10 = 1.0 / IS01;
+    double IS02 = IS0 / IS2;
+    if (isnan(IS02)) IS02 = 1.0;
+    const double IS20 = 1.0 / IS02;
+    double IS12 = IS1 / IS2;
+    if (isnan(IS12)) IS12 = 1.0;
+    const double IS21 = 1.0 / IS12;
+    const double w0 = d0 / ((d0 + (IS01 * IS01) * d1) + (IS02 * IS02) * d2);
+    const double w1 = d1 / (((IS10 * IS10) * d0 + d1) + (IS12 * IS12) * d2);
+    const double w2 = d2 / (((IS20 * IS20) * d0 + (IS21 * IS21) * d1) + d2);
+    double f = 0.0;
+    f += w0 * q0;
+    f += w1 * q1;
+    f += w2 * q2;
+    return f;
+}
+
+}  // namespace compas

@@ -1,0 +1,259 @@
+// Instantaneous pressure relaxation of the six-equation model, applied after every RK stage.
+//
+// Closed form first (a quadratic for the relaxed pressure, then the volume fractions, then the
+// pressure again from E1 + E2), kept wherever it is admissible; otherwise the safeguarded
+// bracketed Newton/bisection solve of g(P) = sum_k alpha_k(P) - V on the active phases, and the
+// phase energies reset at the common pressure. Operation order follows
+//   include/Physics_Compressible6Eq/Relaxation_Pressure_Instantaneous_Compressible6Eq.H:32-220
+//   include/RelaxationPressure_Safeguarded.H:17-256 (constants :76-84)
+// so that the FP64 result is the reference's to the bit. Every loop is bounded (at most
+// kMaxBracket + kMaxIter evaluations), so no input can make a thread spin.
+#pragma once
+
+#include "physics.cuh"
+
+namespace compas {
+
+constexpr double kRelaxRelTol = 1.0e-14;
+constexpr double kRelaxResTol = 4.0e-15;
+constexpr int kRelaxMaxIter = 100;
+constexpr int kRelaxMaxBracket = 1100;
+constexpr int kPathModel = 0, kPathSolve = 1, kPathOneActive = 2, kPathNoActive = 3, kPathNoRoot = 4;
+
+__device__ __forceinline__ bool finite_d(double x) { return (x == x) && (fabs(x) <= DBL_MAX); }
+
+// Safeguarded relaxation of two phases: returns the path; AlphaR holds the relaxed volume fractions.
+__device__ __noinline__ int relax_safeguarded2(double AlphaR[2], const double Alpha[2], const double Alpha_rho[2],
+                                               const double Phi[2], const double Pi[2], const double A[2],
+                                               const double B[2], double trace) {
+    double c[2], dd[2], pinf[2], shift[2] = {0.0, 0.0};
+    bool active[2];
+    int n_active = 0;
+    double pinf_m = DBL_MAX;
+    for (int k = 0; k < 2; ++k) {
+        const double gamma = (A[k] + 1.0) / A[k];
+        pinf[k] = B[k] / (A[k] + 1.0);
+        c[k] = (Pi[k] + Phi[k] * pinf[k]) / gamma;
+        dd[k] = Phi[k] / gamma;
+        active[k] = (Alpha[k] > 0.0) && (Alpha[k] > trace) && (Alpha_rho[k] > 0.0) && (c[k] > 0.0) &&
+                    finite_d(c[k]) && finite_d(dd[k]);
+        if (active[k]) {
+            ++n_active;
+            pinf_m = dmin(pinf_m, pinf[k]);
+        }
+    }
+    double S_passive = 0.0;
+    for (int k = 0; k < 2; ++k) {
+        AlphaR[k] = Alpha[k];
+        if (!active[k]) S_passive += Alpha[k];
+    }
+    const double V = 1.0 - S_passive;
+    if (n_active == 0) return kPathNoActive;
+    if (n_active == 1) {
+        for (int k = 0; k < 2; ++k)
+            if (active[k]) AlphaR[k] = V;
+        return kPathOneActive;
+    }
+    double S = 0.0, Dsum = 0.0, S_Phi = 0.0, S_Pi = 0.0;
+    for (int k = 0; k < 2; ++k) {
+        if (active[k]) {
+            S += Alpha[k];
+            Dsum += dd[k];
+            S_Phi += Phi[k];
+            S_Pi += Pi[k];
+            shift[k] = pinf[k] - pinf_m;
+        }
+    }
+    const double g_inf = (S - V) - Dsum;
+    if (!(g_inf < 0.0)) return kPathNoRoot;
+
+    auto g = [&](double x) {
+        double r = g_inf;
+        for (int k = 0; k < 2; ++k)
+            if (active[k]) r += c[k] / (x + shift[k]);
+        return r;
+    };
+    auto g_scale = [&](double x) {
+        double r = fabs(g_inf);
+        for (int k = 0; k < 2; ++k)
+            if (active[k]) r += c[k] / (x + shift[k]);
+        return r;
+    };
+    auto dg = [&](double x) {
+        double r = 0.0;
+        for (int k = 0; k < 2; ++k)
+            if (active[k]) {
+                const double y = x + shift[k];
+                r -= (c[k] / y) / y;
+            }
+        return r;
+    };
+
+    double x = (S_Phi > 0.0) ? S_Pi / S_Phi + pinf_m : -1.0;
+    if (!(x > 0.0 && finite_d(x))) x = 1.0;
+    double gx = g(x);
+    double a = 0.0;
+    double b = DBL_MAX;
+    if (gx > 0.0) {
+        a = x;
+        for (int n = 0; n < kRelaxMaxBracket; ++n) {
+            const double x4 = 4.0 * x;
+            const double g4 = g(x4);
+            if (!(g4 > 0.0)) {
+                b = x4;
+                break;
+            }
+            x = x4;
+            gx = g4;
+            a = x;
+        }
+    } else if (gx < 0.0) {
+        b = x;
+        for (int n = 0; n < kRelaxMaxBracket; ++n) {
+            x *= 0.25;
+            gx = g(x);
+            if (gx > 0.0) {
+                a = x;
+                break;
+            }
+            b = x;
+            if (!(gx < 0.0)) break;
+        }
+    }
+    const bool bracketed = (gx == 0.0) || ((a > 0.0) && (b < DBL_MAX));
+    if (!bracketed) return kPathNoRoot;
+    if (gx != 0.0 && !(fabs(gx) <= kRelaxResTol * g_scale(x))) {
+        for (int it = 0; it < kRelaxMaxIter; ++it) {
+            double xn = x - gx / dg(x);
+            if (!(xn > a && xn < b)) xn = (b > 16.0 * a) ? sqrt(a) * sqrt(b) : 0.5 * (a + b);
+            const double step = fabs(xn - x);
+            x = xn;
+            gx = g(x);
+            if (gx > 0.0)
+                a = x;
+            else if (gx < 0.0)
+                b = x;
+            else
+                break;
+            if (step <= kRelaxRelTol * x || fabs(gx) <= kRelaxResTol * g_scale(x)) break;
+        }
+    }
+    for (int k = 0; k < 2; ++k)
+        if (active[k]) AlphaR[k] = (Alpha[k] - dd[k]) + c[k] / (x + shift[k]);
+    return kPathSolve;
+}
+
+// Relax the state U of one cell in place (SixEq<D> layout).
+template <int D>
+__device__ __forceinline__ void relax_pressure(double* U, const Eos& e, double trace, unsigned int* err) {
+    using M = SixEq<D>;
+    constexpr int N = M::N;
+    double W[N];
+    M::cons2prim(W, U, e, err);
+    const double a1r1 = W[0], a2r2 = W[1];
+    const double alpha1 = W[M::IA];
+    const double alpha2 = 1.0 - alpha1;
+    const double a1p1 = W[M::IE1], a2p2 = W[M::IE2];
+    const double A1 = e.A1, B1 = e.B1, A2 = e.A2, B2 = e.B2;
+    double alpha1R, alpha2R, a1p1R, a2p2R;
+    double Phi1_In = alpha1, Phi2_In = alpha2, Pi1_In = a1p1, Pi2_In = a2p2;
+    bool raw_nan;
+    double pQ;
+    if (e.C1 > 0.0 || e.C2 > 0.0) {
+        const double b1 = e.C1, b2 = e.C2;
+        const double KE = 0.5 * ksum<D>(W + 2);
+        const double E1 = (U[M::IE1] - a1r1 * KE) - a1r1 * e.D1;
+        const double E2 = (U[M::IE2] - a2r2 * KE) - a2r2 * e.D2;
+        const double Phi1 = alpha1 - b1 * a1r1;
+        const double Phi2 = alpha2 - b2 * a2r2;
+        const double Pi1 = (E1 - B1 * Phi1) / A1;
+        const double Pi2 = (E2 - B2 * Phi2) / A2;
+        Phi1_In = Phi1; Phi2_In = Phi2; Pi1_In = Pi1; Pi2_In = Pi2;
+        const double aP = ((A1 * A2) * (Phi1 + Phi2) + A1 * Phi1) + A2 * Phi2;
+        const double bP = (((A1 * B2) * Phi1 + (A2 * B1) * Phi2) - ((A2 + 1.0) * A1) * Pi1) - ((A1 + 1.0) * A2) * Pi2;
+        const double cP = ((-B2) * A1) * Pi1 - (B1 * A2) * Pi2;
+        double pR = (-bP + sqrt(bP * bP - (4.0 * aP) * cP)) / (2.0 * aP);
+        pQ = pR;
+        alpha1R = ((E1 + pR * alpha1) + (b1 * a1r1) * (A1 * pR + B1)) / ((A1 + 1.0) * pR + B1);
+        alpha2R = ((E2 + pR * alpha2) + (b2 * a2r2) * (A2 * pR + B2)) / ((A2 + 1.0) * pR + B2);
+        raw_nan = isnan(alpha1R) || isnan(alpha2R);
+        if (isnan(alpha1R) && !isnan(alpha2R))
+            alpha1R = 1.0 - alpha2R;
+        else if (!isnan(alpha1R) && isnan(alpha2R))
+            alpha2R = 1.0 - alpha1R;
+        const double sum = alpha1R + alpha2R;
+        alpha1R /= sum;
+        alpha2R /= sum;
+        const double Phi1R = nasg_xi(alpha1R, a1r1, b1, err) * alpha1R;
+        const double Phi2R = nasg_xi(alpha2R, a2r2, b2, err) * alpha2R;
+        pR = (((E1 + E2) - B1 * Phi1R) - B2 * Phi2R) / (A1 * Phi1R + A2 * Phi2R);
+        a1p1R = alpha1R * pR;
+        a2p2R = alpha2R * pR;
+    } else {
+        const double aP = ((A1 * A2) + A1 * alpha1) + A2 * alpha2;
+        const double bP = (((A1 * B2) * alpha1 + (A2 * B1) * alpha2) - ((A2 + 1.0) * A1) * a1p1) - ((A1 + 1.0) * A2) * a2p2;
+        const double cP = ((-B2) * A1) * a1p1 - (B1 * A2) * a2p2;
+        double pR = (-bP + sqrt(bP * bP - (4.0 * aP) * cP)) / (2.0 * aP);
+        pQ = pR;
+        alpha1R = ((A1 * a1p1 + B1 * alpha1) + pR * alpha1) / ((A1 + 1.0) * pR + B1);
+        alpha2R = ((A2 * a2p2 + B2 * alpha2) + pR * alpha2) / ((A2 + 1.0) * pR + B2);
+        raw_nan = isnan(alpha1R) || isnan(alpha2R);
+        if (isnan(alpha1R) && !isnan(alpha2R))
+            alpha1R = 1.0 - alpha2R;
+        else if (!isnan(alpha1R) && isnan(alpha2R))
+            alpha2R = 1.0 - alpha1R;
+        const double sum = alpha1R + alpha2R;
+        alpha1R /= sum;
+        alpha2R /= sum;
+        pR = (((A1 * a1p1 + A2 * a2p2) + B1 * (alpha1 - alpha1R)) + B2 * (alpha2 - alpha2R)) /
+             (A1 * alpha1R + A2 * alpha2R);
+        a1p1R = alpha1R * pR;
+        a2p2R = alpha2R * pR;
+    }
+    const double pinf_1 = B1 / (A1 + 1.0);
+    const double pinf_2 = B2 / (A2 + 1.0);
+    double pinf_m = DBL_MAX, pinf_scale = 0.0;
+    if (alpha1 > 0.0) { pinf_m = dmin(pinf_m, pinf_1); pinf_scale = dmax(pinf_scale, fabs(pinf_1)); }
+    if (alpha2 > 0.0) { pinf_m = dmin(pinf_m, pinf_2); pinf_scale = dmax(pinf_scale, fabs(pinf_2)); }
+    const bool well = fabs(pQ + pinf_m) > 1.0e-8 * (fabs(pQ) + pinf_scale);
+    const bool admissible = !raw_nan && well && finite_d(alpha1R) && finite_d(a1p1R) && finite_d(a2p2R) &&
+                            !(alpha1 > 0.0 && alpha1 <= trace) && !(alpha2 > 0.0 && alpha2 <= trace);
+    if (admissible) {
+        W[M::IE1] = a1p1R;
+        W[M::IE2] = a2p2R;
+        W[M::IA] = alpha1R;
+        M::prim2cons(U, W, e, err);
+        return;
+    }
+    double AlphaR[2];
+    const double Al[2] = {alpha1, alpha2}, Ar[2] = {a1r1, a2r2}, Ph[2] = {Phi1_In, Phi2_In}, Pi[2] = {Pi1_In, Pi2_In};
+    const double Av[2] = {A1, A2}, Bv[2] = {B1, B2};
+    const int path = relax_safeguarded2(AlphaR, Al, Ar, Ph, Pi, Av, Bv, trace);
+    if (path == kPathNoRoot) flag_error(err, COMPAS_B200_ERR_RELAX_NOROOT);
+    if (path != kPathSolve) AlphaR[0] = alpha1;
+    AlphaR[1] = 1.0 - AlphaR[0];
+    const double rho = a1r1 + a2r2;
+    double rho_KE = 0.0;
+    if (rho > 0.0) {
+        double m2 = U[2] * U[2] + U[3] * U[3];
+        if (D == 3) m2 = m2 + U[4] * U[4];
+        rho_KE = (0.5 * m2) / rho;
+    }
+    const double KE = (rho > 0.0) ? rho_KE / rho : 0.0;
+    const double E = U[M::IE1] + U[M::IE2];
+    const double Phi1R = nasg_xi(AlphaR[0], a1r1, e.C1, err) * AlphaR[0];
+    const double Phi2R = nasg_xi(AlphaR[1], a2r2, e.C2, err) * AlphaR[1];
+    const double pR = (((((E - rho_KE) - a1r1 * e.D1) - a2r2 * e.D2) - B1 * Phi1R) - B2 * Phi2R) /
+                      (A1 * Phi1R + A2 * Phi2R);
+    double E1R = ((A1 * Phi1R) * pR + B1 * Phi1R) + a1r1 * (e.D1 + KE);
+    double E2R = ((A2 * Phi2R) * pR + B2 * Phi2R) + a2r2 * (e.D2 + KE);
+    if (AlphaR[0] >= AlphaR[1])
+        E1R = E - E2R;
+    else
+        E2R = E - E1R;
+    U[M::IE1] = E1R;
+    U[M::IE2] = E2R;
+    U[M::IA] = AlphaR[0];
+}
+
+}  // namespace compas

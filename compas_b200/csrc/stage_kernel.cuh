@@ -1,0 +1,315 @@
+// Fused finite-volume right-hand side and TVD-RK3 stage of one level box on sm_100a.
+//
+// One CTA owns a tile of TX x TY x TZ cells. Per tile:
+//   1. the conserved state of the tile cells is read once and converted to primitives into shared
+//      memory (one Conservative2Primitive per cell instead of the reference's ~14 per face);
+//   2. per direction d: the 3-cell halo slabs on both sides of the tile in d are converted into a
+//      shared halo buffer; every face of the tile in d (T_d + 1 per line) is reconstructed (WENO5 in
+//      primitive variables on both sides, then Primitive2Conservative), solved by HLLC, and its flux
+//      and non-conservative face quantities are written to a shared face buffer; each cell then adds
+//      (F_hi - F_lo)/dx_d to its register accumulator, in the order x, y, z of the reference's
+//      divergence (include/Operators_FV/FVM_Divergence_D.H);
+//   3. the epilogue forms dUdt = -div F + NC terms, the RK3 stage combination and, for the
+//      six-equation model, the pressure relaxation, and writes the new state once.
+// Face fluxes never leave shared memory; the face wave speeds are max-reduced per CTA (warp
+// shuffles) into one atomic per CTA.
+//
+// The thread count NT is chosen so that the faces of one direction are an exact multiple of NT
+// (8^3 tile: 9*8*8 = 576 = 2 x 288 threads; 16^2 tile: 17*16 = 272 threads), which keeps every
+// face round full. Launch sites: source/Class_Compressible_PhaseField.cpp:3192-3250 (faces),
+// :3310-3386 (divergence and NC terms), :3937-4107 (stage combinations),
+// source/Class_Compressible6Eq_PhaseField.cpp:437-474 (relaxation).
+#pragma once
+
+#include "physics.cuh"
+#include "relax.cuh"
+
+namespace compas {
+
+// Geometry of one state array (Array4 with ghosts; no z ghosts in 2D).
+struct Grid {
+    int n[3];
+    int ng, gz;
+    long long px, pxy, S;
+    double dx[3];
+    __device__ __forceinline__ long long at(int i, int j, int k) const {
+        return (long long)(k + gz) * pxy + (long long)(j + ng) * px + (i + ng);
+    }
+    __device__ __forceinline__ bool padded(int i, int j, int k) const {
+        return i >= -ng && i < n[0] + ng && j >= -ng && j < n[1] + ng && k >= -gz && k < n[2] + gz;
+    }
+};
+
+enum StageMode { kModeStage = 0, kModeDudt = 1, kModeCmax = 2 };
+
+struct StageArgs {
+    const double* Us;   // stage state, ghosts filled
+    const double* U0;   // state at the start of the step (stages 1, 2)
+    double* Uout;       // new state (kModeStage) or dUdt (kModeDudt)
+    Grid g;
+    Eos e;
+    int mode;
+    int stage;
+    const double* dt;          // device scalar
+    const int* done;           // device flag: step is a no-op when set (may be null)
+    unsigned long long* cmax;  // device double bits, atomicMax (non-negative)
+    unsigned int* err;
+    int id_k;
+    int relax;
+    double trace;
+};
+
+template <class M, int TX, int TY, int TZ>
+struct TileShape {
+    static constexpr int D = M::D;
+    static constexpr int CELLS = TX * TY * TZ;
+    static constexpr int A0 = TY * TZ, A1 = TX * TZ, A2 = TX * TY;
+    static constexpr int AMAX = (D == 3) ? (A0 > A1 ? (A0 > A2 ? A0 : A2) : (A1 > A2 ? A1 : A2)) : (A0 > A1 ? A0 : A1);
+    static constexpr int HALO = 6 * AMAX;
+    static constexpr int F0 = (TX + 1) * A0, F1 = (TY + 1) * A1, F2 = (TZ + 1) * A2;
+    static constexpr int FMAX = (D == 3) ? (F0 > F1 ? (F0 > F2 ? F0 : F2) : (F1 > F2 ? F1 : F2)) : (F0 > F1 ? F0 : F1);
+    static constexpr int NB = M::N + M::NC;
+    static constexpr size_t SMEM = sizeof(double) * ((size_t)M::N * CELLS + (size_t)M::N * HALO + (size_t)NB * FMAX);
+};
+
+template <class M>
+__device__ __forceinline__ void load_cons(double* U, const double* base, const Grid& g, long long q) {
+#pragma unroll
+    for (int n = 0; n < M::N; ++n) U[n] = base[n * g.S + q];
+}
+
+template <class M, int TX, int TY, int TZ, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
+    using T = TileShape<M, TX, TY, TZ>;
+    constexpr int N = M::N, NC = M::NC, D = M::D, NB = T::NB;
+    constexpr int CELLS = T::CELLS, HALO = T::HALO, FMAX = T::FMAX;
+    constexpr int R = (CELLS + NT - 1) / NT;
+
+    if (a.done && *a.done) return;
+
+    extern __shared__ double smem[];
+    double* Pint = smem;
+    double* Phal = Pint + N * CELLS;
+    double* Fb = Phal + N * HALO;
+
+    const Grid& g = a.g;
+    const int ntx = (g.n[0] + TX - 1) / TX;
+    const int nty = (g.n[1] + TY - 1) / TY;
+    int b = blockIdx.x;
+    const int i0 = (b % ntx) * TX;
+    b /= ntx;
+    const int j0 = (b % nty) * TY;
+    const int k0 = (b / nty) * TZ;
+    const int tid = threadIdx.x;
+    unsigned int* err = a.err;
+
+    // 1. tile cells -> primitives
+    for (int l = tid; l < CELLS; l += NT) {
+        const int lx = l % TX, ly = (l / TX) % TY, lz = l / (TX * TY);
+        const int i = i0 + lx, j = j0 + ly, k = k0 + lz;
+        double U[N], W[N];
+        if (g.padded(i, j, k)) {
+            load_cons<M>(U, a.Us, g, g.at(i, j, k));
+            M::cons2prim(W, U, a.e, nullptr);
+        } else {
+#pragma unroll
+            for (int n = 0; n < N; ++n) W[n] = 0.0;
+        }
+#pragma unroll
+        for (int n = 0; n < N; ++n) Pint[n * CELLS + l] = W[n];
+    }
+
+    double acc[R][NB];
+    double cmax_local = 0.0;
+
+#pragma unroll 1
+    for (int d = 0; d < D; ++d) {
+        const int Td = (d == 0) ? TX : (d == 1 ? TY : TZ);
+        const int Ad = (d == 0) ? T::A0 : (d == 1 ? T::A1 : T::A2);
+        // transverse extents (a fastest) of direction d
+        const int Ta = (d == 0) ? TY : TX;
+        // 2a. halo slabs of direction d -> primitives
+        for (int h = tid; h < 6 * Ad; h += NT) {
+            const int slot = h / Ad, t = h % Ad;
+            const int pos = (slot < 3) ? slot - 3 : Td + slot - 3;
+            const int ta = t % Ta, tb = t / Ta;
+            int lx, ly, lz;
+            if (d == 0) { lx = pos; ly = ta; lz = tb; }
+            else if (d == 1) { lx = ta; ly = pos; lz = tb; }
+            else { lx = ta; ly = tb; lz = pos; }
+            const int i = i0 + lx, j = j0 + ly, k = k0 + lz;
+            double U[N], W[N];
+            if (g.padded(i, j, k)) {
+                load_cons<M>(U, a.Us, g, g.at(i, j, k));
+                M::cons2prim(W, U, a.e, nullptr);
+            } else {
+#pragma unroll
+                for (int n = 0; n < N; ++n) W[n] = 0.0;
+            }
+#pragma unroll
+            for (int n = 0; n < N; ++n) Phal[n * HALO + h] = W[n];
+        }
+        __syncthreads();
+
+        // 2b. faces of direction d (x fastest, so neighbouring threads read neighbouring cells)
+        const int Ex = TX + (d == 0), Ey = TY + (d == 1), Ez = TZ + (d == 2);
+        const int NF = Ex * Ey * Ez;
+        for (int f = tid; f < NF; f += NT) {
+            const int fx = f % Ex, fy = (f / Ex) % Ey, fz = f / (Ex * Ey);
+            const int gi = i0 + fx, gj = j0 + fy, gk = k0 + fz;
+            const bool valid = (d == 0 ? gi <= g.n[0] : gi < g.n[0]) && (d == 1 ? gj <= g.n[1] : gj < g.n[1]) &&
+                               (D == 2 || (d == 2 ? gk <= g.n[2] : gk < g.n[2]));
+            if (!valid) continue;
+            const int fd = (d == 0) ? fx : (d == 1 ? fy : fz);
+            // transverse index of this face line (same convention as the halo slots)
+            const int ta = (d == 0) ? fy : fx;
+            const int tb = (d == 2) ? fy : fz;
+            const int t = ta + Ta * tb;
+            // shared-memory offset and component stride of the six stencil cells f-3 .. f+2
+            int off[6], str[6];
+#pragma unroll
+            for (int s = 0; s < 6; ++s) {
+                const int pos = fd - 3 + s;
+                if (pos >= 0 && pos < Td) {
+                    int lx = fx, ly = fy, lz = fz;
+                    if (d == 0) lx = pos; else if (d == 1) ly = pos; else lz = pos;
+                    off[s] = lx + TX * (ly + TY * lz);
+                    str[s] = CELLS;
+                } else {
+                    const int slot = (pos < 0) ? pos + 3 : pos - Td + 3;
+                    off[s] = N * CELLS + slot * Ad + t;
+                    str[s] = HALO;
+                }
+            }
+            double WfL[N], WfR[N], UL[N], UR[N];
+#pragma unroll
+            for (int n = 0; n < N; ++n) {
+                const double w0 = smem[off[0] + n * str[0]], w1 = smem[off[1] + n * str[1]];
+                const double w2 = smem[off[2] + n * str[2]], w3 = smem[off[3] + n * str[3]];
+                const double w4 = smem[off[4] + n * str[4]], w5 = smem[off[5] + n * str[5]];
+                WfL[n] = weno5(w0, w1, w2, w3, w4, 1);
+                WfR[n] = weno5(w1, w2, w3, w4, w5, -1);
+            }
+            M::prim2cons(UL, WfL, a.e, err);
+            M::prim2cons(UR, WfR, a.e, err);
+            double F[N], fnc[NC], cm;
+            M::hllc(F, fnc, cm, UL, UR, a.e, d, a.id_k, err);
+#pragma unroll
+            for (int n = 0; n < N; ++n) Fb[n * FMAX + f] = F[n];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) Fb[(N + c) * FMAX + f] = fnc[c];
+            const int gd = (d == 0) ? gi : (d == 1 ? gj : gk);
+            const int nd = g.n[d];
+            if (fd < Td && gd < nd) cmax_local = dmax(cm, cmax_local);
+        }
+        __syncthreads();
+
+        // 2c. divergence contribution of direction d
+        const double dxd = g.dx[d];
+        const int fstride = (d == 0) ? 1 : (d == 1 ? TX : TX * TY);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int l = tid + r * NT;
+            if (l < CELLS) {
+                const int lx = l % TX, ly = (l / TX) % TY, lz = l / (TX * TY);
+                const int fl = lx + Ex * (ly + Ey * lz);
+                const int fh = fl + fstride;
+#pragma unroll
+                for (int c = 0; c < NB; ++c) {
+                    const double tt = (Fb[c * FMAX + fh] - Fb[c * FMAX + fl]) / dxd;
+                    acc[r][c] = (d == 0) ? tt : acc[r][c] + tt;
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    // 3. epilogue
+    if (a.mode != kModeCmax) {
+        double dt = 0.0, ca = 1.0, cb = 0.0, cd = 1.0;
+        if (a.mode == kModeStage) {
+            dt = *a.dt;
+            if (a.stage == 1) { ca = 0.25; cb = 0.75; cd = 0.25; }
+            else if (a.stage == 2) { ca = 2.0 / 3.0; cb = 1.0 / 3.0; cd = 2.0 / 3.0; }
+        }
+        const double sdt = cd * dt;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int l = tid + r * NT;
+            if (l >= CELLS) continue;
+            const int lx = l % TX, ly = (l / TX) % TY, lz = l / (TX * TY);
+            const int i = i0 + lx, j = j0 + ly, k = k0 + lz;
+            if (i >= g.n[0] || j >= g.n[1] || k >= g.n[2]) continue;
+            double W[N], L[N];
+#pragma unroll
+            for (int n = 0; n < N; ++n) W[n] = Pint[n * CELLS + l];
+#pragma unroll
+            for (int n = 0; n < N; ++n) L[n] = -acc[r][n];
+            if constexpr (M::NC == 1) {
+                // five-equation: alpha1 += phi1 (1 + K1) div u*
+                const double fac = M::kapila_factor(W, W, a.e, a.id_k, err);
+                L[M::IA] = L[M::IA] + fac * acc[r][N];
+            } else {
+                // six-equation: phase energy exchange and alpha1 div u (FVM_SurfaceIntegralNC_Compressible6Eq.H)
+                const double divv = acc[r][N], dva1 = acc[r][N + 1], dva2 = acc[r][N + 2];
+                const double a1r1 = W[0], a2r2 = W[1];
+                const double rho = a1r1 + a2r2;
+                const double vg1 = dva1 - W[M::IE1] * divv;
+                const double vg2 = dva2 - W[M::IE2] * divv;
+                const double x = (a2r2 / rho) * vg1 - (a1r1 / rho) * vg2;
+                L[M::IE1] = L[M::IE1] + x;
+                L[M::IE2] = L[M::IE2] + (-x);
+                L[M::IA] = L[M::IA] + W[M::IA] * divv;
+            }
+            const long long q = g.at(i, j, k);
+            double out[N];
+            if (a.mode == kModeDudt) {
+#pragma unroll
+                for (int n = 0; n < N; ++n) out[n] = L[n];
+            } else {
+                double Us[N];
+                load_cons<M>(Us, a.Us, g, q);
+                if (a.stage == 0) {
+#pragma unroll
+                    for (int n = 0; n < N; ++n) out[n] = 1.0 * Us[n] + sdt * L[n];
+                } else {
+                    double U0[N];
+                    load_cons<M>(U0, a.U0, g, q);
+#pragma unroll
+                    for (int n = 0; n < N; ++n) {
+                        double v = ca * Us[n] + cb * U0[n];
+                        out[n] = v + sdt * L[n];
+                    }
+                }
+                if constexpr (M::NC == 3) {
+                    if (a.relax) relax_pressure<D>(out, a.e, a.trace, err);
+                }
+                bool bad = false;
+#pragma unroll
+                for (int n = 0; n < N; ++n) bad |= isnan(out[n]);
+                if (bad) flag_error(err, COMPAS_B200_ERR_NAN);
+            }
+#pragma unroll
+            for (int n = 0; n < N; ++n) a.Uout[n * g.S + q] = out[n];
+        }
+    }
+
+    // CTA max of the face wave speeds -> one atomic
+    if (a.cmax) {
+        double v = cmax_local;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = dmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        __shared__ double wmax[32];
+        const int w = tid >> 5, lane = tid & 31;
+        if (lane == 0) wmax[w] = v;
+        __syncthreads();
+        if (tid == 0) {
+            double m = 0.0;
+            for (int q = 0; q < (NT + 31) / 32; ++q) m = dmax(m, wmax[q]);
+            // non-negative doubles order like their bit patterns; a NaN speed propagates as the max
+            atomicMax(a.cmax, (unsigned long long)__double_as_longlong(m));
+        }
+    }
+}
+
+}  // namespace compas

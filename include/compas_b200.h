@@ -1,0 +1,175 @@
+/* compas_b200: B200-native (sm_100a) finite-volume right-hand side and TVD-RK3 level advance of the
+ * COMPAS five- and six-equation diffuse-interface models, behind a plain C ABI.
+ *
+ * Data layout. A state array is one AMReX FArrayBox as Array4 sees it: double precision, SoA,
+ * component-major, x fastest, covering the valid box plus `ng` ghost cells on every side (no z
+ * ghosts in 2D). Component n of cell (i,j,k), 0 <= i < n[0] valid, sits at
+ *     n*S + (k+gz)*PY*PX + (j+ng)*PX + (i+ng),
+ *     PX = n[0]+2ng, PY = n[1]+2ng, PZ = n[2]+2gz, S = PX*PY*PZ, gz = ng in 3D and 0 in 2D.
+ * This is the layout of MultiFab::fabPtr(mfi)->dataPtr() for a box grown by ng, so an AMReX caller
+ * passes its device pointers unchanged.
+ *
+ * Errors. Functions return COMPAS_B200_OK (0) or a negative COMPAS_B200_E* code; the reference
+ * aborts the process instead (amrex::Abort). Device kernels never trap: conditions the reference
+ * aborts on inside device code (NASG covolume, NaN state) set bits of a device status word
+ * (COMPAS_B200_ERR_*), which the host reads after the step.
+ *
+ * Streams. Every device-side call is asynchronous on the cudaStream_t passed as `stream` (NULL =
+ * legacy default stream); calls on one level object must not overlap.
+ */
+#ifndef COMPAS_B200_H_
+#define COMPAS_B200_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes --------------------------------------------------------------------------- */
+#define COMPAS_B200_OK 0
+#define COMPAS_B200_EARG (-1)      /* invalid argument or unknown inputs key/value */
+#define COMPAS_B200_ECUDA (-2)     /* a CUDA runtime call failed */
+#define COMPAS_B200_ENOMEM (-3)    /* device allocation failed */
+#define COMPAS_B200_ESTATE (-4)    /* the status word reports an error (see compas_b200_level_status) */
+#define COMPAS_B200_EUNSUPPORTED (-5)
+
+/* ---- device status word bits (set by kernels, read by the host) ----------------------------- */
+#define COMPAS_B200_ERR_NAN 0x1u          /* a NaN in the updated state (reference: SumVar abort) */
+#define COMPAS_B200_ERR_COVOLUME 0x2u     /* NASG 1 - b rho <= 0 (include/EquationOfState_NASG.H:26-32) */
+#define COMPAS_B200_ERR_RELAX_NOROOT 0x4u /* safeguarded relaxation found no root */
+#define COMPAS_B200_ERR_CFL 0x8u          /* non-positive or non-finite time step */
+
+/* ---- models and schemes (the reference's compile-time PHYSICS and run-time keys) ------------ */
+#define COMPAS_B200_FIVEEQS 555 /* include/Macros.H:56 */
+#define COMPAS_B200_SIXEQS 666  /* include/Macros.H:57 */
+
+/* Parameters of the hot path: the fields of the reference's `struct Parm`
+ * (exec/_Tests/Advection/prob/Parm.H:33-117) that the right-hand side reads, plus the run keys of
+ * the level advance. Fill with compas_b200_parm_init, then compas_b200_parm_set per inputs key. */
+typedef struct compas_b200_parm {
+    int physics;          /* COMPAS_B200_FIVEEQS or COMPAS_B200_SIXEQS */
+    int dim;              /* 2 or 3 (AMREX_SPACEDIM) */
+    /* prob.EOS.* (source/Parm.cpp:101-188): raw inputs and the derived partial-form coefficients */
+    int eos;              /* 0 ideal gas, 1 stiffened gas, 3 NASG */
+    double gamma_1, gamma_2, pinf_1, pinf_2, b_1, b_2, q_1, q_2;
+    double A1, A2, B1, B2, C1, C2, D1, D2;
+    /* FiniteVolume.* (include/Operators_FV/FiniteVolume_Parameter.H:25-202) */
+    int id_limiter;       /* 5 WENO5, 6 WENO5B */
+    int num_grow;         /* ghost cells the scheme reads (3 for WENO5/WENO5B) */
+    int thinc;            /* FiniteVolume.THINC */
+    int thinc_use_normal;
+    double thinc_eps, thinc_beta, thinc_normal_threshold;
+    /* Physics.* */
+    int id_riemann;       /* Physics.RiemannSolver: 2 HLLC (source/Class_Compressible_PhaseField.cpp:92-111) */
+    int source_term;      /* FIVEEQS Physics.source_term (Kapila K term) */
+    int relaxation;       /* SIXEQS Physics.pressure_relaxation */
+    double relax_trace;   /* SIXEQS Physics.pressure_relaxation_trace */
+    /* run.* (source/COMPAS.cpp:1276-1314) */
+    double cfl;
+    int change_limiter;   /* run.timestep_change_limiter */
+    /* precision of the bulk arithmetic: 0 plain FP64 (bit-compatible with the reference) */
+    int precision;
+} compas_b200_parm;
+
+/* One box covering a single-level domain (the valid cells), its ghost width and its boundary codes
+ * (COMPAS codes, docs/user-guide/inputs.md:113-120: 0 interior/periodic, 2 outflow, 3 symmetry,
+ * 4 slip wall, 5 no-slip wall). */
+typedef struct compas_b200_geom {
+    int n[3];       /* valid cells per direction; n[2] = 1 in 2D */
+    int ng;         /* ghost cells of the arrays (>= parm.num_grow) */
+    double dx[3];   /* cell sizes */
+    int lo_bc[3];
+    int hi_bc[3];
+} compas_b200_geom;
+
+/* ---- parameters ------------------------------------------------------------------------------- */
+
+/* Reference defaults for the model (Parm, FiniteVolume_Parameter, Physics_Parameter and COMPAS run
+ * defaults: WENO5, HLLC, cfl 0.4, change limiter on). */
+int compas_b200_parm_init(compas_b200_parm* p, int physics, int dim);
+
+/* Set one inputs key, reference syntax and value set, e.g. ("FiniteVolume.Scheme", "WENO5B"),
+ * ("Physics.RiemannSolver", "HLLC"), ("prob.EOS.gamma_2", "4.4"), ("run.cfl", "0.5"). Unknown keys
+ * or values return COMPAS_B200_EARG with the valid values in compas_b200_last_error(), where the
+ * reference aborts (e.g. include/Operators_FV/FiniteVolume_Parameter.H:143-146). EOS keys take
+ * effect at compas_b200_parm_finalize. */
+int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value);
+
+/* Derive the EOS coefficients A, B, C, D from prob.EOS.* as Parm::Initialize does
+ * (source/Parm.cpp:101-188) and check the combination. */
+int compas_b200_parm_finalize(compas_b200_parm* p);
+
+/* Bytes of one state array (all components, with ghosts) of the geometry. */
+long long compas_b200_state_bytes(const compas_b200_parm* p, const compas_b200_geom* g);
+
+/* Last error message of the calling thread. */
+const char* compas_b200_last_error(void);
+
+/* ---- drop-in kernels on caller-owned device arrays ------------------------------------------- */
+
+/* Ghost cells of U from its valid cells by the boundary codes (single-box domain). Replaces the
+ * physical-boundary and periodic part of COMPAS::FillPatch (source/COMPAS.cpp:1629-1732). */
+int compas_b200_fill_boundary(const compas_b200_parm* p, const compas_b200_geom* g, double* U, void* stream);
+
+/* dUdt = -div F(U) + non-conservative terms of the valid cells (dUdt has U's layout), from U with
+ * its ghosts filled, in one fused launch (no face arrays in HBM). Replaces
+ * Compressible_PhaseField::compute_dUdt_FV / ComputeFaceFluxes + FluxDivergence
+ * (source/Class_Compressible_PhaseField.cpp:3151-3537; include/Classes_Physics/
+ * Class_Compressible_PhaseField.H:116-139). cmax_dev (device double, may be NULL) receives
+ * max(*cmax_dev, largest face wave speed over the low faces of the valid cells); err_dev (device
+ * unsigned, may be NULL) is OR-ed with status bits. */
+int compas_b200_compute_dUdt(const compas_b200_parm* p, const compas_b200_geom* g, const double* U, double* dUdt,
+                             double* cmax_dev, unsigned int* err_dev, void* stream);
+
+/* One fused TVD-RK3 stage (stage 0, 1, 2) of ThirdOrderSSPRK
+ * (source/Class_Compressible_PhaseField.cpp:3937-4107) followed by PostTimeStage (the SIXEQS
+ * pressure relaxation, source/Class_Compressible6Eq_PhaseField.cpp:46-59, 437-474):
+ *   stage 0: Unew = Us + dt L(Us)
+ *   stage 1: Unew = 0.25 Us + 0.75 Uold;  Unew += (0.25 dt) L(Us)
+ *   stage 2: Unew = 2/3 Us + 1/3 Uold;    Unew += (2/3 dt) L(Us)
+ * Us must have its ghosts filled. dt is read from device memory (dt_dev). Unew may not alias Us. */
+int compas_b200_rk3_stage(const compas_b200_parm* p, const compas_b200_geom* g, int stage, const double* Us,
+                          const double* Uold, double* Unew, const double* dt_dev, double* cmax_dev,
+                          unsigned int* err_dev, void* stream);
+
+/* Pressure relaxation of the valid cells of U in place (SIXEQS). Replaces
+ * Compressible6Eq_PhaseField::Relaxation (source/Class_Compressible6Eq_PhaseField.cpp:437-474). */
+int compas_b200_relaxation(const compas_b200_parm* p, const compas_b200_geom* g, double* U, unsigned int* err_dev,
+                           void* stream);
+
+/* ---- single-level advance with device-resident state and time-step control -------------------- */
+
+typedef struct compas_b200_level compas_b200_level;
+
+/* Allocate the state (two arrays with ghosts) and the step-control block on the current device. */
+int compas_b200_level_create(const compas_b200_parm* p, const compas_b200_geom* g, compas_b200_level** out);
+int compas_b200_level_destroy(compas_b200_level* lv);
+
+/* Copy a state (layout above, with ghosts; ghost values are ignored) in or out. `host` may be
+ * pageable or pinned host memory, or device memory when is_device != 0. Sets the time to t0. */
+int compas_b200_level_upload(compas_b200_level* lv, const double* src, int is_device, double t0, void* stream);
+int compas_b200_level_download(compas_b200_level* lv, double* dst, int is_device, void* stream);
+
+/* Device pointer of the current state (layout above) for callers that keep data on the GPU. */
+double* compas_b200_level_state(compas_b200_level* lv);
+
+/* Enqueue nsteps coarse steps: ComputeDt (cfl, 1.1x change limiter, stop-time clamp;
+ * source/COMPAS.cpp:2249-2303, CalculateInitialcmax at t = 0) then ThirdOrderSSPRK, all on the
+ * device with no host synchronisation; steps after the stop time do nothing. With use_graph != 0
+ * the launches of one step are captured once into a CUDA graph and replayed. */
+int compas_b200_level_advance(compas_b200_level* lv, int nsteps, double stop_time, int use_graph, void* stream);
+
+/* Wait for the level's work; report the time, the number of steps taken since upload and the status
+ * word. Returns COMPAS_B200_ESTATE when the status word is non-zero. */
+int compas_b200_level_sync(compas_b200_level* lv, double* t, int* steps, unsigned int* status);
+
+/* Step sizes of the steps taken since upload (up to n values). */
+int compas_b200_level_dts(compas_b200_level* lv, double* dts, int n);
+
+/* Kernel launches the library enqueued on this level since upload. */
+long long compas_b200_level_launches(compas_b200_level* lv);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

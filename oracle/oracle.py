@@ -1,0 +1,159 @@
+"""Test infrastructure: ctypes loader of the CPU oracles of the finite-volume RHS / TVD-RK3 path.
+
+Two libraries export the same C interface (oracle/oracle_api.h):
+  * ``oracle/liboracle.so``  - plain-C restatement of the reference algorithm (oracle/compas_oracle.c),
+    built from committed sources anywhere gcc is available;
+  * ``oracle/_ref/libref_<model>_<dim>d.so`` - the reference's own include/Physics_* and
+    include/Operators_* headers compiled against oracle/refshim (built only where the reference
+    tree is present; see oracle/Makefile).
+
+Only tests, __graft_entry__.smoke() and the CPU-baseline leg of bench.py use this module; the
+product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+PORT_LIB = os.path.join(HERE, "liboracle.so")
+
+FIVEEQS, SIXEQS = 555, 666
+
+
+class Case(ctypes.Structure):
+    _fields_ = [
+        ("physics", ctypes.c_int),
+        ("dim", ctypes.c_int),
+        ("n", ctypes.c_int * 3),
+        ("ng", ctypes.c_int),
+        ("dx", ctypes.c_double * 3),
+        ("lo_bc", ctypes.c_int * 3),
+        ("hi_bc", ctypes.c_int * 3),
+        ("A1", ctypes.c_double), ("A2", ctypes.c_double),
+        ("B1", ctypes.c_double), ("B2", ctypes.c_double),
+        ("C1", ctypes.c_double), ("C2", ctypes.c_double),
+        ("D1", ctypes.c_double), ("D2", ctypes.c_double),
+        ("id_limiter", ctypes.c_int),
+        ("id_riemann", ctypes.c_int),
+        ("source_term", ctypes.c_int),
+        ("relaxation", ctypes.c_int),
+        ("relax_trace", ctypes.c_double),
+        ("thinc", ctypes.c_int),
+        ("thinc_use_normal", ctypes.c_int),
+        ("thinc_eps", ctypes.c_double), ("thinc_beta", ctypes.c_double),
+        ("thinc_normal_threshold", ctypes.c_double),
+        ("cfl", ctypes.c_double),
+        ("change_limiter", ctypes.c_int),
+    ]
+
+
+_P = ctypes.POINTER(Case)
+_D = ctypes.c_void_p
+_SIGS = {
+    "cmp_nstate": (ctypes.c_int, [_P]),
+    "cmp_fill_ghosts": (ctypes.c_int, [_P, _D]),
+    "cmp_compute_dudt": (ctypes.c_int, [_P, _D, _D, ctypes.POINTER(ctypes.c_double)]),
+    "cmp_relax": (ctypes.c_int, [_P, _D]),
+    "cmp_rk3_step": (ctypes.c_int, [_P, _D, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
+    "cmp_advance": (ctypes.c_int, [_P, _D, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_double), _D]),
+    "cmp_threads": (ctypes.c_int, []),
+}
+
+_cache: dict = {}
+
+
+def ref_lib_path(physics: int, dim: int) -> str:
+    model = "5eq" if physics == FIVEEQS else "6eq"
+    return os.path.join(REF_DIR, f"libref_{model}_{dim}d.so")
+
+
+def have_ref(physics: int, dim: int) -> bool:
+    return os.path.exists(ref_lib_path(physics, dim))
+
+
+def build_port() -> str:
+    """Compile the plain-C restatement if needed (gcc, OpenMP)."""
+    src = os.path.join(HERE, "compas_oracle.c")
+    if not os.path.exists(PORT_LIB) or os.path.getmtime(PORT_LIB) < os.path.getmtime(src):
+        subprocess.check_call(["make", "-s", "-C", HERE, "port"])
+    return PORT_LIB
+
+
+def load(kind: str, physics: int, dim: int) -> ctypes.CDLL:
+    """kind 'reference' (reference headers) or 'port' (C restatement)."""
+    path = ref_lib_path(physics, dim) if kind == "reference" else build_port()
+    if path not in _cache:
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        h = ctypes.CDLL(path)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(h, name)
+            f.restype = res
+            f.argtypes = args
+        _cache[path] = h
+    return _cache[path]
+
+
+def case_from(parm, geom) -> Case:
+    """Oracle case from a compas_b200 Parm / Geom pair (same field meanings)."""
+    c = Case()
+    c.physics, c.dim = parm.physics, parm.dim
+    for d in range(3):
+        c.n[d] = geom.n[d]
+        c.dx[d] = geom.dx[d]
+        c.lo_bc[d] = geom.lo_bc[d]
+        c.hi_bc[d] = geom.hi_bc[d]
+    if parm.dim == 2:
+        c.n[2] = 1
+    c.ng = geom.ng
+    for k in ("A1", "A2", "B1", "B2", "C1", "C2", "D1", "D2", "id_limiter", "id_riemann", "source_term",
+              "relaxation", "relax_trace", "thinc", "thinc_use_normal", "thinc_eps", "thinc_beta",
+              "thinc_normal_threshold", "cfl", "change_limiter"):
+        setattr(c, k, getattr(parm, k))
+    return c
+
+
+class Oracle:
+    def __init__(self, kind: str, parm, geom):
+        self.kind = kind
+        self.case = case_from(parm, geom)
+        self.lib = load(kind, parm.physics, parm.dim)
+
+    def _call(self, rc):
+        if rc < 0:
+            raise RuntimeError(f"oracle ({self.kind}) failed: {rc}")
+        return rc
+
+    def fill_ghosts(self, U: np.ndarray) -> None:
+        assert U.flags.c_contiguous and U.dtype == np.float64
+        self._call(self.lib.cmp_fill_ghosts(ctypes.byref(self.case), U.ctypes.data))
+
+    def compute_dudt(self, U: np.ndarray):
+        dU = np.zeros_like(U)
+        cm = ctypes.c_double()
+        self._call(self.lib.cmp_compute_dudt(ctypes.byref(self.case), U.ctypes.data, dU.ctypes.data,
+                                             ctypes.byref(cm)))
+        return dU, cm.value
+
+    def relax(self, U: np.ndarray) -> None:
+        self._call(self.lib.cmp_relax(ctypes.byref(self.case), U.ctypes.data))
+
+    def rk3_step(self, U: np.ndarray, dt: float) -> float:
+        cm = ctypes.c_double()
+        self._call(self.lib.cmp_rk3_step(ctypes.byref(self.case), U.ctypes.data, dt, ctypes.byref(cm)))
+        return cm.value
+
+    def advance(self, U: np.ndarray, nsteps: int, stop_time: float = 1e300, t0: float = 0.0):
+        t = ctypes.c_double(t0)
+        dts = np.zeros(max(nsteps, 1), dtype=np.float64)
+        n = self._call(self.lib.cmp_advance(ctypes.byref(self.case), U.ctypes.data, nsteps, stop_time,
+                                            ctypes.byref(t), dts.ctypes.data))
+        return t.value, dts[:n]
+
+    def threads(self) -> int:
+        return int(self.lib.cmp_threads())

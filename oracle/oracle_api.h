@@ -1,0 +1,75 @@
+/* Test infrastructure (oracle): the C interface shared by the two CPU oracles of the finite-volume
+ * right-hand side and TVD-RK3 level advance.
+ *
+ *   oracle/compas_oracle.c        plain-C restatement of the reference's algorithm (liboracle.so)
+ *   oracle/ref_driver.cpp         the reference's own include/Physics_* and include/Operators_* headers,
+ *                                 compiled against oracle/refshim, driven by a loop that restates
+ *                                 source/Class_Compressible_PhaseField.cpp (oracle/_ref/libref_*.so)
+ *
+ * Both export the same symbols so a test can check one against the other and against the CUDA path.
+ * Only tests, smoke() and the CPU-baseline leg of bench.py load these libraries.
+ *
+ * Array layout (AMReX Array4 with ghosts, one box covering the domain): component n of cell
+ * (i,j,k), 0 <= i < n[0] valid, -ng <= i < n[0]+ng with ghosts, sits at
+ *   n*S + (k+ng)*PY*PX + (j+ng)*PX + (i+ng),  PX = n[0]+2ng, PY = n[1]+2ng, PZ = n[2]+2ng (1 in 2D),
+ *   S = PX*PY*PZ. In 2D there are no z ghosts (PZ = 1, k = 0).
+ */
+#ifndef COMPAS_ORACLE_API_H_
+#define COMPAS_ORACLE_API_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct cmp_case {
+    int physics;        /* 555 FIVEEQS, 666 SIXEQS (include/Macros.H:56-59) */
+    int dim;            /* 2 or 3 */
+    int n[3];           /* valid cells per direction (n[2] = 1 in 2D) */
+    int ng;             /* ghost cells (3 for WENO5/WENO5B) */
+    double dx[3];       /* cell sizes (dx[2] unused in 2D) */
+    int lo_bc[3];       /* COMPAS boundary codes: 0 interior/periodic, 2 outflow, 3 symmetry, */
+    int hi_bc[3];       /*   4 slip wall, 5 no-slip wall (docs/user-guide/inputs.md:113-120) */
+    double A1, A2, B1, B2, C1, C2, D1, D2;  /* EOS coefficients as source/Parm.cpp:101-188 */
+    int id_limiter;     /* FiniteVolume.Scheme: 5 WENO5, 6 WENO5B (FiniteVolume_Parameter.H:51-147) */
+    int id_riemann;     /* Physics.RiemannSolver: 0 LLF, 1 HLL, 2 HLLC */
+    int source_term;    /* FIVEEQS Physics.source_term (K term): 0 or 1 */
+    int relaxation;     /* SIXEQS Physics.pressure_relaxation: 0 or 1 */
+    double relax_trace; /* SIXEQS Physics.pressure_relaxation_trace */
+    int thinc;          /* FiniteVolume.THINC: 0 or 1 */
+    int thinc_use_normal;
+    double thinc_eps, thinc_beta, thinc_normal_threshold;
+    double cfl;         /* run.cfl */
+    int change_limiter; /* run.timestep_change_limiter */
+} cmp_case;
+
+/* Number of conserved components of the case (NSTATE). */
+int cmp_nstate(const cmp_case* c);
+
+/* Fill the ghost cells of U (all components) from the valid cells by the boundary codes, direction by
+ * direction (x, then y, then z), each over the full extent of the other directions. */
+int cmp_fill_ghosts(const cmp_case* c, double* U);
+
+/* dUdt (same layout as U; valid cells written) of the state U whose ghosts are filled, and the largest
+ * face wave speed over the low faces of the valid cells (the c_max norm of the reference). */
+int cmp_compute_dudt(const cmp_case* c, const double* U, double* dUdt, double* cmax);
+
+/* Pressure relaxation of the valid cells of U in place (SIXEQS; no-op otherwise). */
+int cmp_relax(const cmp_case* c, double* U);
+
+/* One TVD-RK3 step of size dt on U (valid cells in, valid cells out; ghosts are scratch).
+ * cmax receives the largest face wave speed over the three stages. */
+int cmp_rk3_step(const cmp_case* c, double* U, double dt, double* cmax);
+
+/* nsteps level steps with the reference's time-step control (ComputeDt: cfl, the 1.1x change limiter,
+ * the stop-time clamp). *t is the start time on entry and the end time on exit; dts[s] receives the
+ * step sizes (may be NULL). Returns the number of steps taken. */
+int cmp_advance(const cmp_case* c, double* U, int nsteps, double stop_time, double* t, double* dts);
+
+/* Threads the library uses (OpenMP builds); 1 otherwise. */
+int cmp_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,2 @@
+// Test infrastructure (oracle): forwards to the shared AMReX-compatible shim.
+#include "amrex_shim_core.H"

@@ -1,0 +1,55 @@
+"""CPU-side checks of the C ABI: the library loads, exports every declared symbol, and the inputs-key
+parser follows the reference's keys, values and error behaviour (no GPU calls)."""
+import os
+import re
+
+import pytest
+
+import compas_b200 as cb
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    txt = open(os.path.join(ROOT, "include", "compas_b200.h")).read()
+    return sorted(set(re.findall(r"\b(compas_b200_[A-Za-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = cb.lib()
+    names = declared_symbols()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(cb.EXPORTED_SYMBOLS)
+
+
+def test_parm_defaults_and_eos():
+    p = cb.make_parm(cb.FIVEEQS, 2, {"prob.EOS.gamma_2": 4.4, "prob.EOS.pinf_2": 6e8})
+    assert p.id_limiter == 5 and p.num_grow == 3 and p.id_riemann == 2
+    assert p.cfl == 0.4 and p.change_limiter == 1
+    assert p.A1 == 1.0 / (1.4 - 1.0) and p.A2 == 1.0 / (4.4 - 1.0)
+    assert p.B2 == 4.4 * 6e8 / (4.4 - 1.0) and p.B1 == 0.0
+
+
+@pytest.mark.parametrize("key,value", [("FiniteVolume.Scheme", "WENO7"), ("Physics.RiemannSolver", "Roe"),
+                                       ("prob.EOS.EOS", "7"), ("no.such.key", "1"),
+                                       ("Physics.pressure_relaxation_trace", "1.5")])
+def test_invalid_inputs_are_errors_not_aborts(key, value):
+    with pytest.raises(cb.CompasError) as e:
+        cb.make_parm(cb.FIVEEQS, 2, {key: value})
+    assert e.value.code == cb.EARG
+
+
+def test_scheme_keys():
+    assert cb.make_parm(cb.FIVEEQS, 2, {"FiniteVolume.Scheme": "WENO5B"}).id_limiter == 6
+    with pytest.raises(cb.CompasError) as e:
+        cb.make_parm(cb.FIVEEQS, 2, {"FiniteVolume.Scheme": "MUSCL"})
+    assert e.value.code == cb.EUNSUPPORTED
+
+
+def test_state_bytes_layout():
+    p = cb.make_parm(cb.SIXEQS, 3, {})
+    g = cb.make_geom((10, 12, 14), (1, 1, 1), 3)
+    assert cb.padded_shape(p, g) == (8, 20, 18, 16)
+    assert cb.lib().compas_b200_state_bytes(p, g) == 8 * 20 * 18 * 16 * 8

@@ -266,8 +266,9 @@ static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
             return fail(COMPAS_B200_EARG, "a periodic direction needs code 0 on both sides");
         if (g->lo_bc[d] == 0 && g->n[d] < g->ng)
             return fail(COMPAS_B200_EARG, "a periodic direction needs at least ng cells");
-        if (g->lo_bc[d] != 0 && g->lo_bc[d] != 2 && g->n[d] < g->ng)
-            return fail(COMPAS_B200_EARG, "a reflecting boundary needs at least ng cells");
+        for (int code : {g->lo_bc[d], g->hi_bc[d]})
+            if (code != 0 && code != 2 && g->n[d] < g->ng)
+                return fail(COMPAS_B200_EARG, "a reflecting boundary needs at least ng cells");
     }
     if (p->dim == 2 && g->n[2] != 1) return fail(COMPAS_B200_EARG, "n[2] must be 1 in 2D");
     return COMPAS_B200_OK;

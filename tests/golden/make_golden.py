@@ -1,0 +1,47 @@
+"""Generates the golden fixtures of tests/golden from the reference's OWN arithmetic: the
+reference's include/Physics_* and include/Operators_* headers compiled against the AMReX shim
+(oracle/_ref, built by `make -C oracle ref` where the reference tree is present).
+
+Each fixture holds the initial padded state, the step sizes and the valid cells after the steps,
+so the CPU restatement and the CUDA path can be pinned to the reference without the reference tree.
+Run from the repository root:  python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+import compas_b200 as cb  # noqa: E402
+from compas_b200 import cases  # noqa: E402
+from oracle.oracle import Oracle  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+CASES = {
+    # name: (case function, kwargs, steps)
+    "disc_5eq_2d_32": (cases.advected_disc, dict(n=32), 12),
+    "bubble_5eq_2d_29x17": (cases.shock_bubble, dict(nx=29, ny=17, scheme="WENO5"), 6),
+    "droplet_6eq_3d_12": (cases.shock_droplet, dict(n=12), 3),
+}
+
+
+def make(name):
+    fn, kw, steps = CASES[name]
+    phys, dim, inputs, geom, U = fn(**kw)
+    p = cb.make_parm(phys, dim, inputs)
+    g = cb.make_geom(**geom)
+    out = U.copy()
+    t, dts = Oracle("reference", p, g).advance(out, steps)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), U0=U, dts=dts, t=np.array([t]),
+                        valid=np.ascontiguousarray(cb.valid_view(out, p, g)),
+                        inputs=np.array(repr(inputs)), geom=np.array(repr(geom)),
+                        physics=np.array([phys, dim, steps]))
+
+
+if __name__ == "__main__":
+    for n in CASES:
+        make(n)
+        print("wrote", n)

@@ -1,0 +1,354 @@
+#!/usr/bin/env python
+"""Benchmark of the fused WENO5 + HLLC + TVD-RK3 level advance on one or more B200s.
+
+Workload (one rank): the 3D six-equation shock-droplet, 256^3 cells (16.8 M), water droplet of radius
+0.1 in air, Mach 2.4 shock, WENO5 + HLLC + TVD-RK3 with the pressure relaxation after every stage,
+plain FP64. A step is one coarse time step (ComputeDt + three RK stages) of the whole box; the
+metric is cell-updates per second per RK stage (cells x 3 x steps / time). Inputs are larger than L2
+(3 state arrays of 144 MB each), so no L2 flush is needed between steps.
+
+  value   device time (CUDA events on the launching stream), state resident in HBM, max over ranks
+  e2e     the same metric through the C ABI with host buffers: every step copies the state in from
+          pinned host memory, advances one step, and copies the result back
+  roofline  the stage kernel alone, timed live with CUDA events: algorithmic bytes per launch
+          ((8/3) N 8 B per cell on average over the three stages) / mean launch time, against the
+          measured HBM copy bandwidth
+  cpu_baseline  the reference's own hot-path arithmetic (the reference headers compiled for the CPU,
+          OpenMP over the host cores) on a bounded sample of the same case
+
+Multi-GPU: every rank runs its own independent case (weak scaling, no data-path collective).
+`--impl reference` times the reference CPU build alone (rank 0) on the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s per RK stage"
+UNIT = "cell-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256, help="cells per direction of the cube")
+    ap.add_argument("--cpu-n", type=int, default=96, help="cube side of the CPU sample")
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(n, extra=None):
+    cfg = {"workload": f"3D SIXEQS shock-droplet {n}^3, WENO5+HLLC+TVD-RK3, pressure relaxation every stage",
+           "cells": n ** 3, "nstate": 8, "precision": "fp64 plain (bit-compatible with the reference)",
+           "l2": "inputs larger than L2 (three 144 MB state arrays), no flush", "parallelism": "replicas"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.strip()]
+        os.unlink(self.path)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel_key):
+    """DRAM bytes per launch of the stage kernel from the committed ncu summary (None if absent)."""
+    path = os.path.join(ROOT, "profiles", "stage_kernel_sixeq3d_shock_droplet.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+def cpu_baseline(n, steps):
+    """The reference-header CPU build (or the C restatement) on an n^3 sample of the same case."""
+    import numpy as np
+
+    import compas_b200 as cb
+    from compas_b200 import cases
+    from oracle.oracle import Oracle, have_ref
+
+    kind = "reference" if have_ref(cb.SIXEQS, 3) else "port"
+    phys, dim, inputs, geom, U = cases.shock_droplet(n=n)
+    p = cb.make_parm(phys, dim, inputs)
+    g = cb.make_geom(**geom)
+    o = Oracle(kind, p, g)
+    _, dts = o.advance(U, 1)  # untimed: the first step (with the t = 0 wave-speed pass)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.rk3_step(U, float(dts[0]))
+    el = time.perf_counter() - t0
+    val = n ** 3 * 3 * steps / el
+    return {"value": val, "unit": UNIT, "cores": o.threads(), "kind": kind,
+            "sample": f"{n}^3 cells of the same shock-droplet case, {steps} coarse steps (3 RK stages each) "
+                      f"after one untimed step, OpenMP over {o.threads()} host threads, {el:.1f} s"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    import compas_b200 as cb
+    from compas_b200 import cases
+    from oracle.oracle import Oracle, have_ref
+
+    kind = "reference" if have_ref(cb.SIXEQS, 3) else "port"
+    n = args.cpu_n
+    phys, dim, inputs, geom, U = cases.shock_droplet(n=n)
+    p = cb.make_parm(phys, dim, inputs)
+    g = cb.make_geom(**geom)
+    o = Oracle(kind, p, g)
+    _, dts = o.advance(U, 1)
+    for _ in range(args.warmup):
+        o.rk3_step(U, float(dts[0]))
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.rk3_step(U, float(dts[0]))
+    el = time.perf_counter() - t0
+    val = n ** 3 * 3 * args.steps / el
+    sample = (f"each step one coarse step (3 RK stages) of the same shock-droplet case on a {n}^3 box "
+              f"(a bounded sample of the {args.n}^3 workload), OpenMP over {o.threads()} host threads")
+    line = {"metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference", "config": workload_config(args.n, {"parallelism": "CPU, rank 0 only"}),
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": o.threads(), "kind": kind, "sample": sample},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    return line
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+
+    import compas_b200 as cb
+    from compas_b200 import cases
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    n = args.n
+    phys, dim, inputs, geom, U = cases.shock_droplet(n=n, xp=torch, device="cuda")
+    p = cb.make_parm(phys, dim, inputs)
+    g = cb.make_geom(**geom)
+    cells = n ** 3
+    lv = cb.Level(p, g)
+    lv.upload(U, stream=stream)
+    # warm-up (includes the t = 0 wave-speed pass and the CUDA-graph capture)
+    lv.advance(args.warmup, use_graph=True, stream=stream)
+    torch.cuda.synchronize()
+    info0 = lv.sync()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- value: K steps, state resident in HBM ----
+    clocks = Clocks(local)
+    barrier()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    lv.advance(args.steps, use_graph=True, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    barrier()
+    info = lv.sync()
+    assert info.steps == info0.steps + args.steps, (info0, info)
+    launches_value = 8 * args.steps
+    ms_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = world * cells * 3 * args.steps / (ms_max / 1e3)
+
+    # ---- roofline: the stage kernel alone, CUDA events around each launch ----
+    N = cb.nstate(p.physics, p.dim)
+    shape = cb.padded_shape(p, g)
+    Us = torch.empty(shape, dtype=torch.float64, device="cuda")
+    lv.download(out=Us, stream=stream)
+    cb.FillPatch(p, g, Us, stream=stream)
+    U0 = Us.clone()
+    Un = torch.empty_like(Us)
+    dt_dev = torch.tensor([1e-9], dtype=torch.float64, device="cuda")
+    cmax = torch.zeros(1, dtype=torch.float64, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    for s in range(3):
+        cb.ThirdOrderSSPRK_stage(p, g, s, Us, U0, Un, dt_dev, cmax, err, stream=stream)
+    torch.cuda.synchronize()
+    reps = 2
+    durs, algo = [], []
+    for _ in range(reps):
+        for s in range(3):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            cb.ThirdOrderSSPRK_stage(p, g, s, Us, U0, Un, dt_dev, cmax, err, stream=stream)
+            b.record(stream)
+            b.synchronize()
+            durs.append(a.elapsed_time(b) / 1e3)
+            algo.append(cells * N * 8 * (2 if s == 0 else 3))
+    fa = torch.cuda.Event(enable_timing=True)
+    fb = torch.cuda.Event(enable_timing=True)
+    fa.record(stream)
+    cb.FillPatch(p, g, Us, stream=stream)
+    fb.record(stream)
+    fb.synchronize()
+    fill_ms = fa.elapsed_time(fb)
+    mean_dur = sum(durs) / len(durs)
+    bytes_per_launch = sum(algo) / len(algo)
+    achieved = bytes_per_launch / mean_dur / 1e9
+    peak, peak_kind = measured_peaks()
+    del Us, U0, Un
+
+    # ---- e2e: host state in, one step, result out, every step ----
+    host_in = torch.empty(shape, dtype=torch.float64, pin_memory=True)
+    host_out = torch.empty(shape, dtype=torch.float64, pin_memory=True)
+    lv.download(out=host_in, stream=stream)
+    torch.cuda.synchronize()
+    lv.set_state(host_in, stream=stream)
+    lv.advance(1, use_graph=True, stream=stream)
+    lv.download(out=host_out, stream=stream)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        lv.set_state(host_in, stream=stream)
+        lv.advance(1, use_graph=True, stream=stream)
+        lv.download(out=host_out, stream=stream)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * cells * 3 * args.steps / e2e_s
+    lv.sync()
+    lv.close()
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            cpu = cpu_baseline(args.cpu_n, args.cpu_steps)
+        traffic = profiled_traffic("stage")
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(n, {"parallelism": f"replicas x{world}" if world > 1 else "single GPU"}),
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(lv.nbytes),
+                    "d2h_bytes_per_step": int(lv.nbytes),
+                    "path": "C-ABI level: set_state from pinned host, advance(1), download to pinned host"},
+            "gpu_launches": launches_value,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "stage_kernel<SixEq<3>> (fused WENO5+HLLC+divergence+RK3+relaxation)",
+                         "bytes_per_launch": bytes_per_launch, "mean_launch_ms": mean_dur * 1e3,
+                         "peak_source": f"{peak_kind} HBM copy bandwidth (MEASURED_PEAKS.json)",
+                         "note": "plain FP64 is FP64-pipe bound, not HBM bound; see profiles/"},
+            "fill_boundary_ms": fill_ms,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+    return line
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if args.impl == "reference":
+        line = run_reference(args, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    try:
+        line = run_ours(args, rank, world, dist)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

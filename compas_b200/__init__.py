@@ -103,6 +103,7 @@ _SIGS = {
     "compas_b200_level_upload": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
                                                 ctypes.c_void_p]),
     "compas_b200_level_download": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "compas_b200_level_set_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "compas_b200_level_state": (ctypes.c_void_p, [ctypes.c_void_p]),
     "compas_b200_level_advance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                                  ctypes.c_void_p]),
@@ -259,6 +260,15 @@ class Level:
             assert U.numel() * 8 == self.nbytes
             _check(lib().compas_b200_level_upload(self._h, U.data_ptr(), 1 if U.is_cuda else 0, t0,
                                                   _stream_ptr(stream)))
+
+    def set_state(self, U, stream=None) -> None:
+        """Replace the state only (keeps the time and the time-step control)."""
+        if isinstance(U, np.ndarray):
+            U = np.ascontiguousarray(U, dtype=np.float64)
+            _check(lib().compas_b200_level_set_state(self._h, U.ctypes.data, 0, _stream_ptr(stream)))
+        else:
+            _check(lib().compas_b200_level_set_state(self._h, U.data_ptr(), 1 if U.is_cuda else 0,
+                                                     _stream_ptr(stream)))
 
     def download(self, out=None, stream=None):
         """Copy the padded state out (into `out`, numpy or torch, or a new numpy array)."""

@@ -618,6 +618,13 @@ int compas_b200_level_upload(compas_b200_level* lv, const double* src, int is_de
     return COMPAS_B200_OK;
 }
 
+int compas_b200_level_set_state(compas_b200_level* lv, const double* src, int is_device, void* stream) {
+    if (!lv || !src) return fail(COMPAS_B200_EARG, "null argument");
+    CUDA_TRY(cudaMemcpyAsync(lv->U, src, lv->bytes, is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                             (cudaStream_t)stream));
+    return COMPAS_B200_OK;
+}
+
 int compas_b200_level_download(compas_b200_level* lv, double* dst, int is_device, void* stream) {
     if (!lv || !dst) return fail(COMPAS_B200_EARG, "null argument");
     CUDA_TRY(cudaMemcpyAsync(dst, lv->U, lv->bytes, is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,

@@ -149,6 +149,10 @@ int compas_b200_level_destroy(compas_b200_level* lv);
 int compas_b200_level_upload(compas_b200_level* lv, const double* src, int is_device, double t0, void* stream);
 int compas_b200_level_download(compas_b200_level* lv, double* dst, int is_device, void* stream);
 
+/* Replace the state only (host or device source), keeping the time, the step count and the time-step
+ * control; for callers that hand the state over every step. */
+int compas_b200_level_set_state(compas_b200_level* lv, const double* src, int is_device, void* stream);
+
 /* Device pointer of the current state (layout above) for callers that keep data on the GPU. */
 double* compas_b200_level_state(compas_b200_level* lv);
 

@@ -174,7 +174,7 @@ def test_fiveeq_3d_and_sixeq_2d():
 def test_status_word_reports_nan_without_fault():
     p, g, U = build_case(cases.advected_disc, n=32)
     V = cb.valid_view(U, p, g)
-    V[4, 10, 10] = np.nan  # a NaN energy: the kernels must flag it and keep the context usable
+    V[4, 0, 10, 10] = np.nan  # a NaN energy: the kernels must flag it and keep the context usable
     lv = cb.Level(p, g)
     lv.upload(U)
     lv.advance(1, use_graph=False)

@@ -249,8 +249,8 @@ static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
     if (p->physics != COMPAS_B200_FIVEEQS && p->physics != COMPAS_B200_SIXEQS)
         return fail(COMPAS_B200_EARG, "physics must be FIVEEQS (555) or SIXEQS (666)");
     if (p->dim != 2 && p->dim != 3) return fail(COMPAS_B200_EARG, "dim must be 2 or 3");
-    if (p->id_limiter != 5)
-        return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.Scheme: this build runs WENO5");
+    if (p->id_limiter != 5 && p->id_limiter != 6)
+        return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.Scheme: this build runs WENO5 and WENO5B");
     if (p->thinc) return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.THINC = 1 is not available in this build");
     if (p->id_riemann != 2) return fail(COMPAS_B200_EUNSUPPORTED, "Physics.RiemannSolver: this build runs HLLC");
     if (p->precision != 0) return fail(COMPAS_B200_EUNSUPPORTED, "only the plain FP64 form is available");
@@ -274,10 +274,10 @@ static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
     return COMPAS_B200_OK;
 }
 
-template <class M, int TX, int TY, int TZ, int NT, int MINB>
+template <class M, int SCHEME, int TX, int TY, int TZ, int NT, int MINB>
 static int launch_stage_t(const StageArgs& a, cudaStream_t st) {
     using T = TileShape<M, TX, TY, TZ>;
-    auto kern = stage_kernel<M, TX, TY, TZ, NT, MINB>;
+    auto kern = stage_kernel<M, SCHEME, TX, TY, TZ, NT, MINB>;
     static bool attr_set = false;
     if (!attr_set) {
         CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
@@ -291,13 +291,19 @@ static int launch_stage_t(const StageArgs& a, cudaStream_t st) {
     return COMPAS_B200_OK;
 }
 
-static int launch_stage(const compas_b200_parm* p, const StageArgs& a, cudaStream_t st) {
+template <int SCHEME>
+static int launch_stage_s(const compas_b200_parm* p, const StageArgs& a, cudaStream_t st) {
     if (p->physics == COMPAS_B200_FIVEEQS) {
-        if (p->dim == 2) return launch_stage_t<FiveEq<2>, 16, 16, 1, 272, 2>(a, st);
-        return launch_stage_t<FiveEq<3>, 8, 8, 8, 288, 2>(a, st);
+        if (p->dim == 2) return launch_stage_t<FiveEq<2>, SCHEME, 16, 16, 1, 272, 2>(a, st);
+        return launch_stage_t<FiveEq<3>, SCHEME, 8, 8, 8, 288, 2>(a, st);
     }
-    if (p->dim == 2) return launch_stage_t<SixEq<2>, 16, 16, 1, 272, 2>(a, st);
-    return launch_stage_t<SixEq<3>, 8, 8, 8, 288, 2>(a, st);
+    if (p->dim == 2) return launch_stage_t<SixEq<2>, SCHEME, 16, 16, 1, 272, 2>(a, st);
+    return launch_stage_t<SixEq<3>, SCHEME, 8, 8, 8, 288, 2>(a, st);
+}
+
+static int launch_stage(const compas_b200_parm* p, const StageArgs& a, cudaStream_t st) {
+    if (p->id_limiter == 6) return launch_stage_s<6>(p, a, st);
+    return launch_stage_s<5>(p, a, st);
 }
 
 static int launch_fill(const compas_b200_parm* p, const compas_b200_geom* geo, double* U, cudaStream_t st) {

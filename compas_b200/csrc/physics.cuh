@@ -414,4 +414,121 @@ __device__ __forceinline__ double weno5(double f_mm, double f_m, double f_c, dou
     return f;
 }
 
+// WENO5 candidate values q and nonlinear weights w separately (WENO5.H:12-75), for the bounded
+// variant, which reconstructs the volume fractions with the weights of the partial densities.
+__device__ __forceinline__ void weno5_parts(double f_mm, double f_m, double f_c, double f_p, double f_pp, int side,
+                                            double q[3], double* w) {
+    double d0, d2;
+    if (side == 1) {
+        q[0] = (f_c + (2.0 / 3.0) * (f_p - f_c)) - (1.0 / 6.0) * (f_pp - f_p);
+        q[1] = (f_c + (1.0 / 6.0) * (f_c - f_m)) + (1.0 / 3.0) * (f_p - f_c);
+        q[2] = (f_c - (1.0 / 3.0) * (f_m - f_mm)) + (5.0 / 6.0) * (f_c - f_m);
+        d0 = 3.0 / 10.0;
+        d2 = 1.0 / 10.0;
+    } else {
+        q[0] = (f_c - (5.0 / 6.0) * (f_p - f_c)) + (1.0 / 3.0) * (f_pp - f_p);
+        q[1] = (f_c - (1.0 / 3.0) * (f_c - f_m)) - (1.0 / 6.0) * (f_p - f_c);
+        q[2] = (f_c + (1.0 / 6.0) * (f_m - f_mm)) - (2.0 / 3.0) * (f_c - f_m);
+        d0 = 1.0 / 10.0;
+        d2 = 3.0 / 10.0;
+    }
+    if (!w) return;
+    const double d1 = (1.0 - d0) - d2;
+    const double a = f_p - f_c, b = f_pp - f_p, c = f_c - f_m, g = f_m - f_mm;
+    const double IS0 = ((10.0 / 3.0) * a) * a - ((11.0 / 3.0) * a) * b + ((4.0 / 3.0) * b) * b;
+    const double IS1 = (-(5.0 / 3.0) * c) * a + ((4.0 / 3.0) * c) * c + ((4.0 / 3.0) * a) * a;
+    const double IS2 = ((10.0 / 3.0) * c) * c - ((11.0 / 3.0) * g) * c + ((4.0 / 3.0) * g) * g;
+    double IS01 = IS0 / IS1;
+    if (isnan(IS01)) IS01 = 1.0;
+    const double IS10 = 1.0 / IS01;
+    double IS02 = IS0 / IS2;
+    if (isnan(IS02)) IS02 = 1.0;
+    const double IS20 = 1.0 / IS02;
+    double IS12 = IS1 / IS2;
+    if (isnan(IS12)) IS12 = 1.0;
+    const double IS21 = 1.0 / IS12;
+    w[0] = d0 / ((d0 + (IS01 * IS01) * d1) + (IS02 * IS02) * d2);
+    w[1] = d1 / (((IS10 * IS10) * d0 + d1) + (IS12 * IS12) * d2);
+    w[2] = d2 / (((IS20 * IS20) * d0 + (IS21 * IS21) * d1) + d2);
+}
+
+__device__ __forceinline__ double weno_sum(const double q[3], const double w[3]) {
+    double f = 0.0;
+    f += w[0] * q[0];
+    f += w[1] * q[1];
+    f += w[2] * q[2];
+    return f;
+}
+
+// Positivity limiter of a cell with face values fL (right face) and fR (left face), lower bound 0
+// (Limiter_Bound with ID_BoundType = -1: Limiter_BoundMin.H, fC_QuadratureRule.H; weight 1/12 for
+// the fifth-order polynomial, FiniteVolume_Parameter.H:157-170).
+__device__ __forceinline__ double bound_min_theta(double f_c, double fL, double fR) {
+    const double W = 1.0 / 12.0;
+    const double fC = ((f_c - W * fL) - W * fR) / (1.0 - 2.0 * W);
+    double mn = fC;  // std::min({fC, fL, fR})
+    if (fL < mn) mn = fL;
+    if (fR < mn) mn = fR;
+    const double th = dmax(0.0, f_c - 0.0) / dmax(0.0, f_c - mn);
+    return dmin(1.0, th);
+}
+
+// Bounded WENO5 (WENO5B) face values of the masses and volume fractions of one cell (stencil values
+// ar1[5], ar2[5], al1[5] centred at index 2): positivity of alpha_k rho_k, alpha_k with consistent
+// weights, renormalisation of sum alpha_k = 1, a second limiting pass; returns the values at the
+// face `side` (+1 right, -1 left). include/Operators_Compressible5Eq/
+// FVM_Reconstruction2Face_Conservative_WENO5B_D_Compressible5Eq.H:15-320 and the six-equation
+// counterpart (same steps).
+__device__ __forceinline__ void weno5b_masses(const double* ar1, const double* ar2, const double* al1, int side,
+                                              double& a1r1_f, double& a2r2_f, double& alpha1_f) {
+    double rL[2], rR[2], aL[2], aR[2];
+    double sumL = 0.0, sumR = 0.0;
+    double ac[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const double* fr = (k == 0) ? ar1 : ar2;
+        double fa[5];
+#pragma unroll
+        for (int s = 0; s < 5; ++s) fa[s] = (k == 0) ? al1[s] : 1.0 - al1[s];
+        ac[k] = fa[2];
+        double q[3], w[3], qa[3];
+        weno5_parts(fr[0], fr[1], fr[2], fr[3], fr[4], 1, q, w);
+        rL[k] = weno_sum(q, w);
+        weno5_parts(fa[0], fa[1], fa[2], fa[3], fa[4], 1, qa, nullptr);
+        aL[k] = weno_sum(qa, w);
+        weno5_parts(fr[0], fr[1], fr[2], fr[3], fr[4], -1, q, w);
+        rR[k] = weno_sum(q, w);
+        weno5_parts(fa[0], fa[1], fa[2], fa[3], fa[4], -1, qa, nullptr);
+        aR[k] = weno_sum(qa, w);
+        const double th_r = bound_min_theta(fr[2], rL[k], rR[k]);
+        const double th_a = bound_min_theta(fa[2], aL[k], aR[k]);
+        const double th = dmin(th_r, th_a);
+        rL[k] = fr[2] + th * (rL[k] - fr[2]);
+        aL[k] = fa[2] + th * (aL[k] - fa[2]);
+        rR[k] = fr[2] + th * (rR[k] - fr[2]);
+        aR[k] = fa[2] + th * (aR[k] - fa[2]);
+        sumL += aL[k];
+        sumR += aR[k];
+    }
+    double Th = 1.0;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const double rc = (k == 0) ? ar1[2] : ar2[2];
+        rL[k] /= sumL;
+        aL[k] /= sumL;
+        rR[k] /= sumR;
+        aR[k] /= sumR;
+        const double th_r = bound_min_theta(rc, rL[k], rR[k]);
+        const double th_a = bound_min_theta(ac[k], aL[k], aR[k]);
+        if (th_r < Th) Th = th_r;  // std::min({Th, th_r, th_a})
+        if (th_a < Th) Th = th_a;
+    }
+    const double r1 = (side == 1) ? rL[0] : rR[0];
+    const double r2 = (side == 1) ? rL[1] : rR[1];
+    const double a1 = (side == 1) ? aL[0] : aR[0];
+    a1r1_f = ar1[2] + Th * (r1 - ar1[2]);
+    a2r2_f = ar2[2] + Th * (r2 - ar2[2]);
+    alpha1_f = al1[2] + Th * (a1 - al1[2]);
+}
+
 }  // namespace compas

@@ -78,7 +78,9 @@ __device__ __forceinline__ void load_cons(double* U, const double* base, const G
     for (int n = 0; n < M::N; ++n) U[n] = base[n * g.S + q];
 }
 
-template <class M, int TX, int TY, int TZ, int NT, int MINB>
+// SCHEME: 5 WENO5 on every primitive variable; 6 WENO5B (bounded masses and volume fractions,
+// plain WENO5 on the velocity and the pressure(s)).
+template <class M, int SCHEME, int TX, int TY, int TZ, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
     using T = TileShape<M, TX, TY, TZ>;
     constexpr int N = M::N, NC = M::NC, D = M::D, NB = T::NB;
@@ -182,8 +184,21 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
                 }
             }
             double WfL[N], WfR[N], UL[N], UR[N];
+            constexpr int NB0 = (SCHEME == 6) ? 2 : 0;        // first plainly reconstructed component
+            constexpr int NB1 = (SCHEME == 6) ? M::IA : N;    // one past the last
+            if constexpr (SCHEME == 6) {
+                double r1[6], r2[6], al[6];
 #pragma unroll
-            for (int n = 0; n < N; ++n) {
+                for (int s = 0; s < 6; ++s) {
+                    r1[s] = smem[off[s]];
+                    r2[s] = smem[off[s] + str[s]];
+                    al[s] = smem[off[s] + M::IA * str[s]];
+                }
+                weno5b_masses(r1, r2, al, 1, WfL[0], WfL[1], WfL[M::IA]);
+                weno5b_masses(r1 + 1, r2 + 1, al + 1, -1, WfR[0], WfR[1], WfR[M::IA]);
+            }
+#pragma unroll
+            for (int n = NB0; n < NB1; ++n) {
                 const double w0 = smem[off[0] + n * str[0]], w1 = smem[off[1] + n * str[1]];
                 const double w2 = smem[off[2] + n * str[2]], w3 = smem[off[3] + n * str[3]];
                 const double w4 = smem[off[4] + n * str[4]], w5 = smem[off[5] + n * str[5]];

@@ -218,6 +218,109 @@ static double weno5(double f_mm, double f_m, double f_c, double f_p, double f_pp
     return f;
 }
 
+/* WENO5 candidates q and weights w (w may be NULL) */
+static void weno5_parts(double f_mm, double f_m, double f_c, double f_p, double f_pp, int side, double* q, double* w) {
+    double d0, d2;
+    if (side == 1) {
+        q[0] = f_c + (2.0 / 3.0) * (f_p - f_c) - (1.0 / 6.0) * (f_pp - f_p);
+        q[1] = f_c + (1.0 / 6.0) * (f_c - f_m) + (1.0 / 3.0) * (f_p - f_c);
+        q[2] = f_c - (1.0 / 3.0) * (f_m - f_mm) + (5.0 / 6.0) * (f_c - f_m);
+        d0 = 3.0 / 10.0;
+        d2 = 1.0 / 10.0;
+    } else {
+        q[0] = f_c - (5.0 / 6.0) * (f_p - f_c) + (1.0 / 3.0) * (f_pp - f_p);
+        q[1] = f_c - (1.0 / 3.0) * (f_c - f_m) - (1.0 / 6.0) * (f_p - f_c);
+        q[2] = f_c + (1.0 / 6.0) * (f_m - f_mm) - (2.0 / 3.0) * (f_c - f_m);
+        d0 = 1.0 / 10.0;
+        d2 = 3.0 / 10.0;
+    }
+    if (!w) return;
+    const double d1 = 1.0 - d0 - d2;
+    const double IS0 = (10.0 / 3.0) * (f_p - f_c) * (f_p - f_c) - (11.0 / 3.0) * (f_p - f_c) * (f_pp - f_p) +
+                       (4.0 / 3.0) * (f_pp - f_p) * (f_pp - f_p);
+    const double IS1 = -(5.0 / 3.0) * (f_c - f_m) * (f_p - f_c) + (4.0 / 3.0) * (f_c - f_m) * (f_c - f_m) +
+                       (4.0 / 3.0) * (f_p - f_c) * (f_p - f_c);
+    const double IS2 = (10.0 / 3.0) * (f_c - f_m) * (f_c - f_m) - (11.0 / 3.0) * (f_m - f_mm) * (f_c - f_m) +
+                       (4.0 / 3.0) * (f_m - f_mm) * (f_m - f_mm);
+    double IS01 = IS0 / IS1;
+    if (isnan(IS01)) IS01 = 1.0;
+    const double IS10 = 1.0 / IS01;
+    double IS02 = IS0 / IS2;
+    if (isnan(IS02)) IS02 = 1.0;
+    const double IS20 = 1.0 / IS02;
+    double IS12 = IS1 / IS2;
+    if (isnan(IS12)) IS12 = 1.0;
+    const double IS21 = 1.0 / IS12;
+    w[0] = d0 / (d0 + (IS01 * IS01) * d1 + (IS02 * IS02) * d2);
+    w[1] = d1 / ((IS10 * IS10) * d0 + d1 + (IS12 * IS12) * d2);
+    w[2] = d2 / ((IS20 * IS20) * d0 + (IS21 * IS21) * d1 + d2);
+}
+
+static double wsum(const double* q, const double* w) {
+    double f = 0.0;
+    for (int i = 0; i < 3; ++i) f += w[i] * q[i];
+    return f;
+}
+
+/* Limiter_Bound, ID_BoundType -1, f_min 0, Weight 1/12 (include/Operators_FV/Limiter_Bound.H,
+ * Limiter_BoundMin.H, fC_QuadratureRule.H) */
+static double theta_min0(double f_c, double fL, double fR) {
+    const double Wt = 1.0 / 12.0;
+    const double fC = (f_c - Wt * fL - Wt * fR) / (1.0 - 2.0 * Wt);
+    double mn = fC;
+    if (fL < mn) mn = fL;
+    if (fR < mn) mn = fR;
+    return dmin(1.0, dmax(0.0, f_c - 0.0) / dmax(0.0, f_c - mn));
+}
+
+/* WENO5B masses and volume fraction of the cell at P[2] (P: primitive stencil of 5 cells) at face side
+ * (include/Operators_Compressible5Eq/FVM_Reconstruction2Face_Conservative_WENO5B_D_Compressible5Eq.H:15-320) */
+static void weno5b_bounded(const Model* m, double P[][MAXN], int side, double* WF) {
+    double Ar[2][5], Al[2][5], rL[2], rR[2], aL[2], aR[2], q[3], w[3], qa[3];
+    for (int s = 0; s < 5; ++s) {
+        Ar[0][s] = P[s][0];
+        Ar[1][s] = P[s][1];
+        Al[0][s] = P[s][m->IA];
+        Al[1][s] = 1.0 - P[s][m->IA];
+    }
+    const double inf_unused = 0.0;
+    (void)inf_unused;
+    double sumL = 0.0, sumR = 0.0;
+    for (int k = 0; k < 2; ++k) {
+        const double* fr = Ar[k];
+        const double* fa = Al[k];
+        weno5_parts(fr[0], fr[1], fr[2], fr[3], fr[4], 1, q, w);
+        rL[k] = wsum(q, w);
+        weno5_parts(fa[0], fa[1], fa[2], fa[3], fa[4], 1, qa, NULL);
+        aL[k] = wsum(qa, w);
+        weno5_parts(fr[0], fr[1], fr[2], fr[3], fr[4], -1, q, w);
+        rR[k] = wsum(q, w);
+        weno5_parts(fa[0], fa[1], fa[2], fa[3], fa[4], -1, qa, NULL);
+        aR[k] = wsum(qa, w);
+        const double th = dmin(theta_min0(fr[2], rL[k], rR[k]), theta_min0(fa[2], aL[k], aR[k]));
+        rL[k] = fr[2] + th * (rL[k] - fr[2]);
+        aL[k] = fa[2] + th * (aL[k] - fa[2]);
+        rR[k] = fr[2] + th * (rR[k] - fr[2]);
+        aR[k] = fa[2] + th * (aR[k] - fa[2]);
+        sumL += aL[k];
+        sumR += aR[k];
+    }
+    double Th = 1.0;
+    for (int k = 0; k < 2; ++k) {
+        rL[k] /= sumL;
+        aL[k] /= sumL;
+        rR[k] /= sumR;
+        aR[k] /= sumR;
+        const double tr = theta_min0(Ar[k][2], rL[k], rR[k]);
+        const double ta = theta_min0(Al[k][2], aL[k], aR[k]);
+        if (tr < Th) Th = tr;
+        if (ta < Th) Th = ta;
+    }
+    WF[0] = Ar[0][2] + Th * ((side == 1 ? rL[0] : rR[0]) - Ar[0][2]);
+    WF[1] = Ar[1][2] + Th * ((side == 1 ? rL[1] : rR[1]) - Ar[1][2]);
+    WF[m->IA] = Al[0][2] + Th * ((side == 1 ? aL[0] : aR[0]) - Al[0][2]);
+}
+
 /* ---- Riemann solver ------------------------------------------------------------------------------ */
 static void hllc(const Model* m, const double* UL, const double* UR, int d, double* Fo, double* fnc, double* cmax) {
     const int N = m->N, D = m->D;
@@ -605,11 +708,15 @@ static void face_flux(const Model* m, const Geo* g, const double* U, int i, int 
         load(m, g, U, ii, jj, kk, C[s]);
     }
     /* left state: stencil i-3..i+1 centred at i-1, right face; right state: i-2..i+2 centred at i, left face */
+    const int bounded = (m->c->id_limiter == 6);
+    const int n0 = bounded ? 2 : 0, n1 = bounded ? m->IA : N;
     for (int s = 0; s < 5; ++s) c2p(m, C[s], P[s]);
-    for (int n = 0; n < N; ++n) WL[n] = weno5(P[0][n], P[1][n], P[2][n], P[3][n], P[4][n], 1);
+    if (bounded) weno5b_bounded(m, P, 1, WL);
+    for (int n = n0; n < n1; ++n) WL[n] = weno5(P[0][n], P[1][n], P[2][n], P[3][n], P[4][n], 1);
     p2c(m, WL, UL);
     for (int s = 1; s < 6; ++s) c2p(m, C[s], P[s]);
-    for (int n = 0; n < N; ++n) WR[n] = weno5(P[1][n], P[2][n], P[3][n], P[4][n], P[5][n], -1);
+    if (bounded) weno5b_bounded(m, P + 1, -1, WR);
+    for (int n = n0; n < n1; ++n) WR[n] = weno5(P[1][n], P[2][n], P[3][n], P[4][n], P[5][n], -1);
     p2c(m, WR, UR);
     hllc(m, UL, UR, d, F, fnc, cmax);
 }

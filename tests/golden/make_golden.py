@@ -25,6 +25,7 @@ CASES = {
     "disc_5eq_2d_32": (cases.advected_disc, dict(n=32), 12),
     "bubble_5eq_2d_29x17": (cases.shock_bubble, dict(nx=29, ny=17, scheme="WENO5"), 6),
     "droplet_6eq_3d_12": (cases.shock_droplet, dict(n=12), 3),
+    "bubble_weno5b_5eq_2d_31x19": (cases.shock_bubble, dict(nx=31, ny=19, scheme="WENO5B"), 6),
 }
 
 

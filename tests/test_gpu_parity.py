@@ -185,3 +185,18 @@ def test_status_word_reports_nan_without_fault():
     p2, g2, U2 = build_case(cases.advected_disc, n=32)
     got, info2, _ = run_gpu(p2, g2, U2, 1)
     assert info2.status == 0
+
+
+def test_weno5b_fiveeq_2d_shock_bubble_walls_outflow():
+    """WENO5B (bounded masses and volume fractions) on the shock-bubble with reflective top/bottom
+    and outflow left/right, the configuration of the 2D shock-helium-bubble at reduced size."""
+    p, g, U = build_case(cases.shock_bubble, nx=96, ny=48, scheme="WENO5B")
+    _compare_steps(p, g, U, 10)
+
+
+def test_weno5b_sixeq_3d():
+    phys, dim, inputs, geom, U = cases.shock_droplet(n=20)
+    inputs["FiniteVolume.Scheme"] = "WENO5B"
+    p = cb.make_parm(phys, dim, inputs)
+    g = cb.make_geom(**geom)
+    _compare_steps(p, g, U, 3)

@@ -291,14 +291,30 @@ static int launch_stage_t(const StageArgs& a, cudaStream_t st) {
     return COMPAS_B200_OK;
 }
 
+// Launch shape of the stage kernel: threads per CTA and CTAs per SM of the 3D (8^3 tile) and 2D
+// (16^2 tile) kernels. The register budget is set per SM sub-partition (16384 registers each, warps
+// dealt round-robin), so a CTA of 6 warps at 2 CTAs/SM gets 168 registers per thread.
+#ifndef COMPAS_NT3
+#define COMPAS_NT3 192
+#endif
+#ifndef COMPAS_MINB3
+#define COMPAS_MINB3 2
+#endif
+#ifndef COMPAS_NT2
+#define COMPAS_NT2 272
+#endif
+#ifndef COMPAS_MINB2
+#define COMPAS_MINB2 2
+#endif
+
 template <int SCHEME>
 static int launch_stage_s(const compas_b200_parm* p, const StageArgs& a, cudaStream_t st) {
     if (p->physics == COMPAS_B200_FIVEEQS) {
-        if (p->dim == 2) return launch_stage_t<FiveEq<2>, SCHEME, 16, 16, 1, 272, 2>(a, st);
-        return launch_stage_t<FiveEq<3>, SCHEME, 8, 8, 8, 288, 2>(a, st);
+        if (p->dim == 2) return launch_stage_t<FiveEq<2>, SCHEME, 16, 16, 1, COMPAS_NT2, COMPAS_MINB2>(a, st);
+        return launch_stage_t<FiveEq<3>, SCHEME, 8, 8, 8, COMPAS_NT3, COMPAS_MINB3>(a, st);
     }
-    if (p->dim == 2) return launch_stage_t<SixEq<2>, SCHEME, 16, 16, 1, 272, 2>(a, st);
-    return launch_stage_t<SixEq<3>, SCHEME, 8, 8, 8, 288, 2>(a, st);
+    if (p->dim == 2) return launch_stage_t<SixEq<2>, SCHEME, 16, 16, 1, COMPAS_NT2, COMPAS_MINB2>(a, st);
+    return launch_stage_t<SixEq<3>, SCHEME, 8, 8, 8, COMPAS_NT3, COMPAS_MINB3>(a, st);
 }
 
 static int launch_stage(const compas_b200_parm* p, const StageArgs& a, cudaStream_t st) {

@@ -66,6 +66,14 @@ __device__ __forceinline__ double nasg_xi(double alpha, double alpha_rho, double
     return 1.0;
 }
 
+// v[d] for a run-time direction d without indexing a per-thread array by a run-time value (which
+// would place the array in local memory).
+template <int D>
+__device__ __forceinline__ double pick(const double* v, int d) {
+    if (D == 2) return (d == 0) ? v[0] : v[1];
+    return (d == 0) ? v[0] : ((d == 1) ? v[1] : v[2]);
+}
+
 template <int D>
 __device__ __forceinline__ double ksum(const double* u) {
     // u*u + v*v (+ w*w), left to right
@@ -162,14 +170,17 @@ struct FiveEq {
 
     // Physical flux in direction d of the state U with primitives W (Conservative2Flux).
     __device__ static __forceinline__ void flux(double* F, const double* U, const double* W, int d) {
-        const double V = W[2 + d];
+        const double V = pick<D>(W + 2, d);
         const double p = W[IE];
         F[0] = U[0] * V;
         F[1] = U[1] * V;
-        for (int c = 0; c < D; ++c) F[2 + c] = U[2 + c] * V;
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+            F[2 + c] = U[2 + c] * V;
+            if (c == d) F[2 + c] = F[2 + c] + p;
+        }
         F[IE] = (U[IE] + p) * V;
         F[IA] = U[IA] * V;
-        F[2 + d] = F[2 + d] + p;
     }
 
     // HLLC flux, the normal face velocity u* (FluxNC[0]) and the face wave speed.
@@ -182,7 +193,7 @@ struct FiveEq {
         flux(FR, UR, WR, d);
         const double cL = sound_speed(WL, e, id_k, err);
         const double cR = sound_speed(WR, e, id_k, err);
-        const double VL = WL[2 + d], VR = WR[2 + d];
+        const double VL = pick<D>(WL + 2, d), VR = pick<D>(WR + 2, d);
         const double pL = WL[IE], pR = WR[IE];
         const double V_avg = 0.5 * (VL + VR);
         const double c_avg = 0.5 * (cL + cR);
@@ -202,6 +213,7 @@ struct FiveEq {
         double vel = hp * VL + hm * VR;
         vel = vel + ((hp * Sm) * (fL - 1.0) + (hm * Sp) * (fR - 1.0));
         fnc[0] = vel;
+#pragma unroll
         for (int i = 0; i < N; ++i) {
             double sL = fL * UL[i];
             double sR = fR * UR[i];
@@ -293,14 +305,17 @@ struct SixEq {
     }
 
     __device__ static __forceinline__ void flux(double* F, const double* U, const double* W, int d) {
-        const double V = W[2 + d];
+        const double V = pick<D>(W + 2, d);
         F[0] = U[0] * V;
         F[1] = U[1] * V;
-        for (int c = 0; c < D; ++c) F[2 + c] = U[2 + c] * V;
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+            F[2 + c] = U[2 + c] * V;
+            if (c == d) F[2 + c] = F[2 + c] + (W[IE1] + W[IE2]);
+        }
         F[IE1] = (U[IE1] + W[IE1]) * V;
         F[IE2] = (U[IE2] + W[IE2]) * V;
         F[IA] = U[IA] * V;
-        F[2 + d] = F[2 + d] + (W[IE1] + W[IE2]);
     }
 
     // HLLC flux and the face quantities u_n, (u a1p1)_n, (u a2p2)_n of the non-conservative terms.
@@ -314,7 +329,7 @@ struct SixEq {
         flux(FR, UR, WR, d);
         const double cL = sound_speed(WL, e, err);
         const double cR = sound_speed(WR, e, err);
-        const double VL = WL[2 + d], VR = WR[2 + d];
+        const double VL = pick<D>(WL + 2, d), VR = pick<D>(WR + 2, d);
         const double SL = dmin(VL - cL, VR - cR);
         const double SR = dmax(VL + cL, VR + cR);
         const double Sm = dmin(0.0, SL);
@@ -334,6 +349,7 @@ struct SixEq {
         double UsL[N], UsR[N];
         UsL[0] = a1r1Ls; UsL[1] = a2r2Ls;
         UsR[0] = a1r1Rs; UsR[1] = a2r2Rs;
+#pragma unroll
         for (int c = 0; c < D; ++c) {
             const double uLc = WL[2 + c], uRc = WR[2 + c];
             const double nrm = (c == d) ? 1.0 : 0.0;
@@ -353,7 +369,7 @@ struct SixEq {
         const double s = sgn0(S_Star);
         const double hp = 0.5 * (1.0 + s), hm = 0.5 * (1.0 - s);
         // normal components of Vel, Vel*a1p1, Vel*a2p2
-        const double uLd = WL[2 + d], uRd = WR[2 + d];
+        const double uLd = VL, uRd = VR;
         double vel = hp * uLd + hm * uRd;
         vel = vel + ((hp * Sm) * (fL - 1.0) + (hm * Sp) * (fR - 1.0));
         const double va1 = hp * (uLd * a1p1L + (1.0 * Sm) * (VL * a1p1L - S_Star * a1p1Ls) / (S_Star - SL)) +
@@ -363,6 +379,7 @@ struct SixEq {
         fnc[0] = vel;
         fnc[1] = va1;
         fnc[2] = va2;
+#pragma unroll
         for (int i = 0; i < N; ++i)
             Fout[i] = hp * (FL[i] + Sm * (UsL[i] - UL[i])) + hm * (FR[i] + Sp * (UsR[i] - UR[i]));
         const double qL = cL + sqrt(ksum<D>(WL + 2));

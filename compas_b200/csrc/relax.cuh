@@ -23,7 +23,7 @@ constexpr int kPathModel = 0, kPathSolve = 1, kPathOneActive = 2, kPathNoActive 
 __device__ __forceinline__ bool finite_d(double x) { return (x == x) && (fabs(x) <= DBL_MAX); }
 
 // Safeguarded relaxation of two phases: returns the path; AlphaR holds the relaxed volume fractions.
-__device__ __noinline__ int relax_safeguarded2(double AlphaR[2], const double Alpha[2], const double Alpha_rho[2],
+__device__ __forceinline__ int relax_safeguarded2(double AlphaR[2], const double Alpha[2], const double Alpha_rho[2],
                                                const double Phi[2], const double Pi[2], const double A[2],
                                                const double B[2], double trace) {
     double c[2], dd[2], pinf[2], shift[2] = {0.0, 0.0};

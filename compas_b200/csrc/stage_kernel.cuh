@@ -214,13 +214,13 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
 #pragma unroll
             for (int c = 0; c < NC; ++c) Fb[(N + c) * FMAX + f] = fnc[c];
             const int gd = (d == 0) ? gi : (d == 1 ? gj : gk);
-            const int nd = g.n[d];
+            const int nd = (d == 0) ? g.n[0] : (d == 1 ? g.n[1] : g.n[2]);
             if (fd < Td && gd < nd) cmax_local = dmax(cm, cmax_local);
         }
         __syncthreads();
 
         // 2c. divergence contribution of direction d
-        const double dxd = g.dx[d];
+        const double dxd = (d == 0) ? g.dx[0] : (d == 1 ? g.dx[1] : g.dx[2]);
         const int fstride = (d == 0) ? 1 : (d == 1 ? TX : TX * TY);
 #pragma unroll
         for (int r = 0; r < R; ++r) {

@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "compas_b200.h"
@@ -253,7 +254,8 @@ static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
         return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.Scheme: this build runs WENO5 and WENO5B");
     if (p->thinc) return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.THINC = 1 is not available in this build");
     if (p->id_riemann != 2) return fail(COMPAS_B200_EUNSUPPORTED, "Physics.RiemannSolver: this build runs HLLC");
-    if (p->precision != 0) return fail(COMPAS_B200_EUNSUPPORTED, "only the plain FP64 form is available");
+    if (p->precision != 0 && p->precision != 1)
+        return fail(COMPAS_B200_EARG, "precision must be 0 (plain FP64) or 1 (mixed)");
     if (g->ng < 3) return fail(COMPAS_B200_EARG, "WENO5 needs ng >= 3 ghost cells");
     for (int d = 0; d < p->dim; ++d) {
         if (g->n[d] < 1) return fail(COMPAS_B200_EARG, "empty box");
@@ -274,10 +276,10 @@ static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
     return COMPAS_B200_OK;
 }
 
-template <class M, int SCHEME, int TX, int TY, int TZ, int NT, int MINB>
+template <class M, int SCHEME, bool MIX, int TX, int TY, int TZ, int NT, int MINB>
 static int launch_stage_t(const StageArgs& a, cudaStream_t st) {
-    using T = TileShape<M, TX, TY, TZ>;
-    auto kern = stage_kernel<M, SCHEME, TX, TY, TZ, NT, MINB>;
+    using T = TileShape<M, TX, TY, TZ, typename std::conditional<MIX, float, double>::type>;
+    auto kern = stage_kernel<M, SCHEME, MIX, TX, TY, TZ, NT, MINB>;
     static bool attr_set = false;
     if (!attr_set) {
         CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
@@ -307,19 +309,23 @@ static int launch_stage_t(const StageArgs& a, cudaStream_t st) {
 #define COMPAS_MINB2 2
 #endif
 
-template <int SCHEME>
+template <int SCHEME, bool MIX>
 static int launch_stage_s(const compas_b200_parm* p, const StageArgs& a, cudaStream_t st) {
     if (p->physics == COMPAS_B200_FIVEEQS) {
-        if (p->dim == 2) return launch_stage_t<FiveEq<2>, SCHEME, 16, 16, 1, COMPAS_NT2, COMPAS_MINB2>(a, st);
-        return launch_stage_t<FiveEq<3>, SCHEME, 8, 8, 8, COMPAS_NT3, COMPAS_MINB3>(a, st);
+        if (p->dim == 2) return launch_stage_t<FiveEq<2>, SCHEME, MIX, 16, 16, 1, COMPAS_NT2, COMPAS_MINB2>(a, st);
+        return launch_stage_t<FiveEq<3>, SCHEME, MIX, 8, 8, 8, COMPAS_NT3, COMPAS_MINB3>(a, st);
     }
-    if (p->dim == 2) return launch_stage_t<SixEq<2>, SCHEME, 16, 16, 1, COMPAS_NT2, COMPAS_MINB2>(a, st);
-    return launch_stage_t<SixEq<3>, SCHEME, 8, 8, 8, COMPAS_NT3, COMPAS_MINB3>(a, st);
+    if (p->dim == 2) return launch_stage_t<SixEq<2>, SCHEME, MIX, 16, 16, 1, COMPAS_NT2, COMPAS_MINB2>(a, st);
+    return launch_stage_t<SixEq<3>, SCHEME, MIX, 8, 8, 8, COMPAS_NT3, COMPAS_MINB3>(a, st);
 }
 
 static int launch_stage(const compas_b200_parm* p, const StageArgs& a, cudaStream_t st) {
-    if (p->id_limiter == 6) return launch_stage_s<6>(p, a, st);
-    return launch_stage_s<5>(p, a, st);
+    if (p->precision == 1) {
+        if (p->id_limiter == 6) return launch_stage_s<6, true>(p, a, st);
+        return launch_stage_s<5, true>(p, a, st);
+    }
+    if (p->id_limiter == 6) return launch_stage_s<6, false>(p, a, st);
+    return launch_stage_s<5, false>(p, a, st);
 }
 
 static int launch_fill(const compas_b200_parm* p, const compas_b200_geom* geo, double* U, cudaStream_t st) {
@@ -491,6 +497,12 @@ int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value
             *dk.dst = x;
             return 0;
         }
+    if (k == "compas_b200.precision") {
+        // this engine's own key (no reference counterpart): the arithmetic of the bulk of the RHS
+        if (v == "fp64") { p->precision = 0; return 0; }
+        if (v == "mixed") { p->precision = 1; return 0; }
+        return bad("fp64, mixed");
+    }
     if (k == "run.timestep_change_limiter") { if (!parse_int(value, &ix)) return bad("0, 1"); p->change_limiter = ix ? 1 : 0; return 0; }
     return fail(COMPAS_B200_EARG, "unknown inputs key '" + k + "'");
 }

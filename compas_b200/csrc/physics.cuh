@@ -183,12 +183,21 @@ struct FiveEq {
         F[IA] = U[IA] * V;
     }
 
-    // HLLC flux, the normal face velocity u* (FluxNC[0]) and the face wave speed.
+    // HLLC flux, the normal face velocity u* (FluxNC[0]) and the face wave speed, from the face
+    // states UL, UR (Riemann_HLLC converts them to primitives first).
     __device__ static __forceinline__ void hllc(double* Fout, double* fnc, double& cmax, const double* UL,
                                                 const double* UR, const Eos& e, int d, int id_k, unsigned int* err) {
-        double WL[N], WR[N], FL[N], FR[N];
+        double WL[N], WR[N];
         cons2prim(WL, UL, e, err);
         cons2prim(WR, UR, e, err);
+        hllc_uw(Fout, fnc, cmax, UL, WL, UR, WR, e, d, id_k, err);
+    }
+
+    // The same from face states given both as conserved (U) and primitive (W) variables.
+    __device__ static __forceinline__ void hllc_uw(double* Fout, double* fnc, double& cmax, const double* UL,
+                                                   const double* WL, const double* UR, const double* WR, const Eos& e,
+                                                   int d, int id_k, unsigned int* err) {
+        double FL[N], FR[N];
         flux(FL, UL, WL, d);
         flux(FR, UR, WR, d);
         const double cL = sound_speed(WL, e, id_k, err);
@@ -320,11 +329,17 @@ struct SixEq {
 
     // HLLC flux and the face quantities u_n, (u a1p1)_n, (u a2p2)_n of the non-conservative terms.
     __device__ static __forceinline__ void hllc(double* Fout, double* fnc, double& cmax, const double* UL,
-                                                const double* UR, const Eos& e, int d, int /*id_k*/,
-                                                unsigned int* err) {
-        double WL[N], WR[N], FL[N], FR[N];
+                                                const double* UR, const Eos& e, int d, int id_k, unsigned int* err) {
+        double WL[N], WR[N];
         cons2prim(WL, UL, e, err);
         cons2prim(WR, UR, e, err);
+        hllc_uw(Fout, fnc, cmax, UL, WL, UR, WR, e, d, id_k, err);
+    }
+
+    __device__ static __forceinline__ void hllc_uw(double* Fout, double* fnc, double& cmax, const double* UL,
+                                                   const double* WL, const double* UR, const double* WR, const Eos& e,
+                                                   int d, int /*id_k*/, unsigned int* err) {
+        double FL[N], FR[N];
         flux(FL, UL, WL, d);
         flux(FR, UR, WR, d);
         const double cL = sound_speed(WL, e, err);
@@ -546,6 +561,125 @@ __device__ __forceinline__ void weno5b_masses(const double* ar1, const double* a
     a1r1_f = ar1[2] + Th * (r1 - ar1[2]);
     a2r2_f = ar2[2] + Th * (r2 - ar2[2]);
     alpha1_f = al1[2] + Th * (a1 - al1[2]);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Mixed precision: WENO5 / WENO5B in FP32 on primitive variables.
+//
+// The face value is formed as f_c + sum_k w_k (q_k - f_c), with the candidate corrections q_k - f_c
+// built from the undivided differences, so a constant field is reconstructed exactly whatever the
+// rounding of the weights, and the FP32 error scales with the correction, not with |f|. The
+// weights are the reference's ratio-form weights (include/Operators_FV/WENO5.H:44-75) rewritten
+// with one reciprocal: with r01 = IS0/IS1 and r02 = IS0/IS2, D = d0 + r01^2 d1 + r02^2 d2 and
+// w0 = d0/D, w1 = d1 r01^2/D, w2 = d2 r02^2/D (the same weights in exact arithmetic); where a
+// smoothness indicator vanishes or a ratio is huge, the ratio form with its NaN guard is used.
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ void weno5_f32_parts(float f_mm, float f_m, float f_c, float f_p, float f_pp, int side,
+                                                float e[3], float* w) {
+    const float a = f_p - f_c, b = f_pp - f_p, c = f_c - f_m, g = f_m - f_mm;
+    float d0, d2;
+    if (side == 1) {
+        e[0] = __fmaf_rn(2.0f / 3.0f, a, -(1.0f / 6.0f) * b);
+        e[1] = __fmaf_rn(1.0f / 6.0f, c, (1.0f / 3.0f) * a);
+        e[2] = __fmaf_rn(-(1.0f / 3.0f), g, (5.0f / 6.0f) * c);
+        d0 = 0.3f;
+        d2 = 0.1f;
+    } else {
+        e[0] = __fmaf_rn(-(5.0f / 6.0f), a, (1.0f / 3.0f) * b);
+        e[1] = __fmaf_rn(-(1.0f / 3.0f), c, -(1.0f / 6.0f) * a);
+        e[2] = __fmaf_rn(1.0f / 6.0f, g, -(2.0f / 3.0f) * c);
+        d0 = 0.1f;
+        d2 = 0.3f;
+    }
+    if (!w) return;
+    const float d1 = 0.6f;
+    const float IS0 = __fmaf_rn((10.0f / 3.0f) * a, a, __fmaf_rn(-(11.0f / 3.0f) * a, b, (4.0f / 3.0f) * b * b));
+    const float IS1 = __fmaf_rn(-(5.0f / 3.0f) * c, a, (4.0f / 3.0f) * __fmaf_rn(c, c, a * a));
+    const float IS2 = __fmaf_rn((10.0f / 3.0f) * c, c, __fmaf_rn(-(11.0f / 3.0f) * g, c, (4.0f / 3.0f) * g * g));
+    const float r01 = __fdividef(IS0, IS1), r02 = __fdividef(IS0, IS2);
+    if (IS1 > 0.0f && IS2 > 0.0f && r01 < 1.0e15f && r02 < 1.0e15f) {
+        const float s01 = r01 * r01, s02 = r02 * r02;
+        const float inv = __fdividef(1.0f, __fmaf_rn(s01, d1, __fmaf_rn(s02, d2, d0)));
+        w[0] = d0 * inv;
+        w[1] = (d1 * s01) * inv;
+        w[2] = (d2 * s02) * inv;
+        return;
+    }
+    float IS01 = IS0 / IS1;
+    if (isnan(IS01)) IS01 = 1.0f;
+    const float IS10 = 1.0f / IS01;
+    float IS02 = IS0 / IS2;
+    if (isnan(IS02)) IS02 = 1.0f;
+    const float IS20 = 1.0f / IS02;
+    float IS12 = IS1 / IS2;
+    if (isnan(IS12)) IS12 = 1.0f;
+    const float IS21 = 1.0f / IS12;
+    w[0] = d0 / ((d0 + (IS01 * IS01) * d1) + (IS02 * IS02) * d2);
+    w[1] = d1 / (((IS10 * IS10) * d0 + d1) + (IS12 * IS12) * d2);
+    w[2] = d2 / (((IS20 * IS20) * d0 + (IS21 * IS21) * d1) + d2);
+}
+
+__device__ __forceinline__ float weno5_f32(float f_mm, float f_m, float f_c, float f_p, float f_pp, int side) {
+    float e[3], w[3];
+    weno5_f32_parts(f_mm, f_m, f_c, f_p, f_pp, side, e, w);
+    return f_c + __fmaf_rn(w[0], e[0], __fmaf_rn(w[1], e[1], w[2] * e[2]));
+}
+
+__device__ __forceinline__ float bound_min_theta_f32(float f_c, float fL, float fR) {
+    const float W = 1.0f / 12.0f;
+    const float fC = (f_c - W * fL - W * fR) * (1.0f / (1.0f - 2.0f * W));
+    float mn = fminf(fC, fminf(fL, fR));
+    const float den = f_c - mn;
+    if (!(den > 0.0f)) return 1.0f;
+    return fminf(1.0f, __fdividef(fmaxf(0.0f, f_c), den));
+}
+
+// WENO5B masses and volume fraction in FP32 (same steps as weno5b_masses).
+__device__ __forceinline__ void weno5b_masses_f32(const float* ar1, const float* ar2, const float* al1, int side,
+                                                  float& a1r1_f, float& a2r2_f, float& alpha1_f) {
+    float rL[2], rR[2], aL[2], aR[2], ac[2];
+    float sumL = 0.0f, sumR = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const float* fr = (k == 0) ? ar1 : ar2;
+        float fa[5];
+#pragma unroll
+        for (int s = 0; s < 5; ++s) fa[s] = (k == 0) ? al1[s] : 1.0f - al1[s];
+        ac[k] = fa[2];
+        float e[3], w[3], ea[3];
+        weno5_f32_parts(fr[0], fr[1], fr[2], fr[3], fr[4], 1, e, w);
+        weno5_f32_parts(fa[0], fa[1], fa[2], fa[3], fa[4], 1, ea, nullptr);
+        rL[k] = fr[2] + __fmaf_rn(w[0], e[0], __fmaf_rn(w[1], e[1], w[2] * e[2]));
+        aL[k] = fa[2] + __fmaf_rn(w[0], ea[0], __fmaf_rn(w[1], ea[1], w[2] * ea[2]));
+        weno5_f32_parts(fr[0], fr[1], fr[2], fr[3], fr[4], -1, e, w);
+        weno5_f32_parts(fa[0], fa[1], fa[2], fa[3], fa[4], -1, ea, nullptr);
+        rR[k] = fr[2] + __fmaf_rn(w[0], e[0], __fmaf_rn(w[1], e[1], w[2] * e[2]));
+        aR[k] = fa[2] + __fmaf_rn(w[0], ea[0], __fmaf_rn(w[1], ea[1], w[2] * ea[2]));
+        const float th = fminf(bound_min_theta_f32(fr[2], rL[k], rR[k]), bound_min_theta_f32(fa[2], aL[k], aR[k]));
+        rL[k] = __fmaf_rn(th, rL[k] - fr[2], fr[2]);
+        aL[k] = __fmaf_rn(th, aL[k] - fa[2], fa[2]);
+        rR[k] = __fmaf_rn(th, rR[k] - fr[2], fr[2]);
+        aR[k] = __fmaf_rn(th, aR[k] - fa[2], fa[2]);
+        sumL += aL[k];
+        sumR += aR[k];
+    }
+    const float iL = 1.0f / sumL, iR = 1.0f / sumR;
+    float Th = 1.0f;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const float rc = (k == 0) ? ar1[2] : ar2[2];
+        rL[k] *= iL;
+        aL[k] *= iL;
+        rR[k] *= iR;
+        aR[k] *= iR;
+        Th = fminf(Th, fminf(bound_min_theta_f32(rc, rL[k], rR[k]), bound_min_theta_f32(ac[k], aL[k], aR[k])));
+    }
+    const float r1 = (side == 1) ? rL[0] : rR[0];
+    const float r2 = (side == 1) ? rL[1] : rR[1];
+    const float a1 = (side == 1) ? aL[0] : aR[0];
+    a1r1_f = __fmaf_rn(Th, r1 - ar1[2], ar1[2]);
+    a2r2_f = __fmaf_rn(Th, r2 - ar2[2], ar2[2]);
+    alpha1_f = __fmaf_rn(Th, a1 - al1[2], al1[2]);
 }
 
 }  // namespace compas

@@ -24,6 +24,8 @@
 #include "physics.cuh"
 #include "relax.cuh"
 
+#include <type_traits>
+
 namespace compas {
 
 // Geometry of one state array (Array4 with ghosts; no z ghosts in 2D).
@@ -59,7 +61,7 @@ struct StageArgs {
     double trace;
 };
 
-template <class M, int TX, int TY, int TZ>
+template <class M, int TX, int TY, int TZ, class PT = double>
 struct TileShape {
     static constexpr int D = M::D;
     static constexpr int CELLS = TX * TY * TZ;
@@ -69,7 +71,10 @@ struct TileShape {
     static constexpr int F0 = (TX + 1) * A0, F1 = (TY + 1) * A1, F2 = (TZ + 1) * A2;
     static constexpr int FMAX = (D == 3) ? (F0 > F1 ? (F0 > F2 ? F0 : F2) : (F1 > F2 ? F1 : F2)) : (F0 > F1 ? F0 : F1);
     static constexpr int NB = M::N + M::NC;
-    static constexpr size_t SMEM = sizeof(double) * ((size_t)M::N * CELLS + (size_t)M::N * HALO + (size_t)NB * FMAX);
+    // primitives (type PT) of the tile and of one halo slab pair, then the face buffer (FP64)
+    static constexpr size_t PBYTES = sizeof(PT) * ((size_t)M::N * CELLS + (size_t)M::N * HALO);
+    static constexpr size_t FOFF = (PBYTES + 15) / 16 * 16;
+    static constexpr size_t SMEM = FOFF + sizeof(double) * (size_t)NB * FMAX;
 };
 
 template <class M>
@@ -80,19 +85,25 @@ __device__ __forceinline__ void load_cons(double* U, const double* base, const G
 
 // SCHEME: 5 WENO5 on every primitive variable; 6 WENO5B (bounded masses and volume fractions,
 // plain WENO5 on the velocity and the pressure(s)).
-template <class M, int SCHEME, int TX, int TY, int TZ, int NT, int MINB>
+// MIX: false - plain FP64, the reference's arithmetic to the bit; true - mixed precision: the cell
+// primitives are recovered in FP64 (pressure from total energy) and kept in shared memory as FP32,
+// the reconstruction runs in FP32, the Riemann solver, divergence, stage accumulation and
+// relaxation in FP64.
+template <class M, int SCHEME, bool MIX, int TX, int TY, int TZ, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
-    using T = TileShape<M, TX, TY, TZ>;
+    using PT = typename std::conditional<MIX, float, double>::type;
+    using T = TileShape<M, TX, TY, TZ, PT>;
     constexpr int N = M::N, NC = M::NC, D = M::D, NB = T::NB;
     constexpr int CELLS = T::CELLS, HALO = T::HALO, FMAX = T::FMAX;
     constexpr int R = (CELLS + NT - 1) / NT;
 
     if (a.done && *a.done) return;
 
-    extern __shared__ double smem[];
-    double* Pint = smem;
-    double* Phal = Pint + N * CELLS;
-    double* Fb = Phal + N * HALO;
+    extern __shared__ double smem_d[];
+    PT* smem = reinterpret_cast<PT*>(smem_d);
+    PT* Pint = smem;
+    PT* Phal = Pint + N * CELLS;
+    double* Fb = reinterpret_cast<double*>(reinterpret_cast<char*>(smem_d) + T::FOFF);
 
     const Grid& g = a.g;
     const int ntx = (g.n[0] + TX - 1) / TX;
@@ -118,7 +129,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
             for (int n = 0; n < N; ++n) W[n] = 0.0;
         }
 #pragma unroll
-        for (int n = 0; n < N; ++n) Pint[n * CELLS + l] = W[n];
+        for (int n = 0; n < N; ++n) Pint[n * CELLS + l] = (PT)W[n];
     }
 
     double acc[R][NB];
@@ -149,7 +160,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
                 for (int n = 0; n < N; ++n) W[n] = 0.0;
             }
 #pragma unroll
-            for (int n = 0; n < N; ++n) Phal[n * HALO + h] = W[n];
+            for (int n = 0; n < N; ++n) Phal[n * HALO + h] = (PT)W[n];
         }
         __syncthreads();
 
@@ -186,29 +197,57 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
             double WfL[N], WfR[N], UL[N], UR[N];
             constexpr int NB0 = (SCHEME == 6) ? 2 : 0;        // first plainly reconstructed component
             constexpr int NB1 = (SCHEME == 6) ? M::IA : N;    // one past the last
-            if constexpr (SCHEME == 6) {
-                double r1[6], r2[6], al[6];
-#pragma unroll
-                for (int s = 0; s < 6; ++s) {
-                    r1[s] = smem[off[s]];
-                    r2[s] = smem[off[s] + str[s]];
-                    al[s] = smem[off[s] + M::IA * str[s]];
-                }
-                weno5b_masses(r1, r2, al, 1, WfL[0], WfL[1], WfL[M::IA]);
-                weno5b_masses(r1 + 1, r2 + 1, al + 1, -1, WfR[0], WfR[1], WfR[M::IA]);
-            }
-#pragma unroll
-            for (int n = NB0; n < NB1; ++n) {
-                const double w0 = smem[off[0] + n * str[0]], w1 = smem[off[1] + n * str[1]];
-                const double w2 = smem[off[2] + n * str[2]], w3 = smem[off[3] + n * str[3]];
-                const double w4 = smem[off[4] + n * str[4]], w5 = smem[off[5] + n * str[5]];
-                WfL[n] = weno5(w0, w1, w2, w3, w4, 1);
-                WfR[n] = weno5(w1, w2, w3, w4, w5, -1);
-            }
-            M::prim2cons(UL, WfL, a.e, err);
-            M::prim2cons(UR, WfR, a.e, err);
             double F[N], fnc[NC], cm;
-            M::hllc(F, fnc, cm, UL, UR, a.e, d, a.id_k, err);
+            if constexpr (!MIX) {
+                if constexpr (SCHEME == 6) {
+                    double r1[6], r2[6], al[6];
+#pragma unroll
+                    for (int s = 0; s < 6; ++s) {
+                        r1[s] = smem[off[s]];
+                        r2[s] = smem[off[s] + str[s]];
+                        al[s] = smem[off[s] + M::IA * str[s]];
+                    }
+                    weno5b_masses(r1, r2, al, 1, WfL[0], WfL[1], WfL[M::IA]);
+                    weno5b_masses(r1 + 1, r2 + 1, al + 1, -1, WfR[0], WfR[1], WfR[M::IA]);
+                }
+#pragma unroll
+                for (int n = NB0; n < NB1; ++n) {
+                    const double w0 = smem[off[0] + n * str[0]], w1 = smem[off[1] + n * str[1]];
+                    const double w2 = smem[off[2] + n * str[2]], w3 = smem[off[3] + n * str[3]];
+                    const double w4 = smem[off[4] + n * str[4]], w5 = smem[off[5] + n * str[5]];
+                    WfL[n] = weno5(w0, w1, w2, w3, w4, 1);
+                    WfR[n] = weno5(w1, w2, w3, w4, w5, -1);
+                }
+                M::prim2cons(UL, WfL, a.e, err);
+                M::prim2cons(UR, WfR, a.e, err);
+                M::hllc(F, fnc, cm, UL, UR, a.e, d, a.id_k, err);
+            } else {
+                if constexpr (SCHEME == 6) {
+                    float r1[6], r2[6], al[6];
+#pragma unroll
+                    for (int s = 0; s < 6; ++s) {
+                        r1[s] = smem[off[s]];
+                        r2[s] = smem[off[s] + str[s]];
+                        al[s] = smem[off[s] + M::IA * str[s]];
+                    }
+                    float x0, x1, x2;
+                    weno5b_masses_f32(r1, r2, al, 1, x0, x1, x2);
+                    WfL[0] = x0; WfL[1] = x1; WfL[M::IA] = x2;
+                    weno5b_masses_f32(r1 + 1, r2 + 1, al + 1, -1, x0, x1, x2);
+                    WfR[0] = x0; WfR[1] = x1; WfR[M::IA] = x2;
+                }
+#pragma unroll
+                for (int n = NB0; n < NB1; ++n) {
+                    const float w0 = smem[off[0] + n * str[0]], w1 = smem[off[1] + n * str[1]];
+                    const float w2 = smem[off[2] + n * str[2]], w3 = smem[off[3] + n * str[3]];
+                    const float w4 = smem[off[4] + n * str[4]], w5 = smem[off[5] + n * str[5]];
+                    WfL[n] = (double)weno5_f32(w0, w1, w2, w3, w4, 1);
+                    WfR[n] = (double)weno5_f32(w1, w2, w3, w4, w5, -1);
+                }
+                M::prim2cons(UL, WfL, a.e, err);
+                M::prim2cons(UR, WfR, a.e, err);
+                M::hllc_uw(F, fnc, cm, UL, WfL, UR, WfR, a.e, d, a.id_k, err);
+            }
 #pragma unroll
             for (int n = 0; n < N; ++n) Fb[n * FMAX + f] = F[n];
 #pragma unroll
@@ -256,8 +295,15 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
             const int i = i0 + lx, j = j0 + ly, k = k0 + lz;
             if (i >= g.n[0] || j >= g.n[1] || k >= g.n[2]) continue;
             double W[N], L[N];
+            if constexpr (MIX) {
+                // the epilogue needs the FP64 primitives of the cell: recover them again
+                double Uc[N];
+                load_cons<M>(Uc, a.Us, g, g.at(i, j, k));
+                M::cons2prim(W, Uc, a.e, nullptr);
+            } else {
 #pragma unroll
-            for (int n = 0; n < N; ++n) W[n] = Pint[n * CELLS + l];
+                for (int n = 0; n < N; ++n) W[n] = Pint[n * CELLS + l];
+            }
 #pragma unroll
             for (int n = 0; n < N; ++n) L[n] = -acc[r][n];
             if constexpr (M::NC == 1) {

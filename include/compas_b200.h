@@ -66,7 +66,9 @@ typedef struct compas_b200_parm {
     /* run.* (source/COMPAS.cpp:1276-1314) */
     double cfl;
     int change_limiter;   /* run.timestep_change_limiter */
-    /* precision of the bulk arithmetic: 0 plain FP64 (bit-compatible with the reference) */
+    /* precision of the bulk arithmetic (inputs key compas_b200.precision): 0 plain FP64, bit-compatible
+     * with the reference; 1 mixed: FP32 reconstruction, FP64 pressure recovery, Riemann solver,
+     * stage accumulation and relaxation */
     int precision;
 } compas_b200_parm;
 

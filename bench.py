@@ -48,13 +48,15 @@ def parse():
     ap.add_argument("--cpu-n", type=int, default=96, help="cube side of the CPU sample")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
     return ap.parse_args()
 
 
 def workload_config(n, extra=None):
     cfg = {"workload": f"3D SIXEQS shock-droplet {n}^3, WENO5+HLLC+TVD-RK3, pressure relaxation every stage",
-           "cells": n ** 3, "nstate": 8, "precision": "fp64 plain (bit-compatible with the reference)",
-           "l2": "inputs larger than L2 (three 144 MB state arrays), no flush", "parallelism": "replicas"}
+           "cells": n ** 3, "nstate": 8,
+           "l2": f"inputs larger than L2 (three state arrays of {(n + 6) ** 3 * 64 / 1e9:.2f} GB), no flush",
+           "parallelism": "replicas"}
     if extra:
         cfg.update(extra)
     return cfg
@@ -183,6 +185,7 @@ def run_reference(args, rank):
 
 
 def run_ours(args, rank, world, dist):
+    import numpy as np
     import torch
 
     import compas_b200 as cb
@@ -193,69 +196,94 @@ def run_ours(args, rank, world, dist):
     stream = torch.cuda.current_stream()
     n = args.n
     phys, dim, inputs, geom, U = cases.shock_droplet(n=n, xp=torch, device="cuda")
-    p = cb.make_parm(phys, dim, inputs)
     g = cb.make_geom(**geom)
     cells = n ** 3
-    lv = cb.Level(p, g)
-    lv.upload(U, stream=stream)
-    # warm-up (includes the t = 0 wave-speed pass and the CUDA-graph capture)
-    lv.advance(args.warmup, use_graph=True, stream=stream)
-    torch.cuda.synchronize()
-    info0 = lv.sync()
+    forms = {"mixed": cb.make_parm(phys, dim, dict(inputs, **{"compas_b200.precision": "mixed"})),
+             "fp64": cb.make_parm(phys, dim, inputs)}
+    if args.precision != "both":
+        forms = {args.precision: forms[args.precision]}
 
     def barrier():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
 
-    # ---- value: K steps, state resident in HBM ----
-    clocks = Clocks(local)
-    barrier()
-    clocks.start()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    lv.advance(args.steps, use_graph=True, stream=stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    clk = clocks.stop()
-    barrier()
-    info = lv.sync()
-    assert info.steps == info0.steps + args.steps, (info0, info)
-    launches_value = 8 * args.steps
-    ms_max = ms
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = world * cells * 3 * args.steps / (ms_max / 1e3)
+        return float(t.item())
 
-    # ---- roofline: the stage kernel alone, CUDA events around each launch ----
+    levels, ms, clks = {}, {}, []
+    for name, p in forms.items():
+        lv = cb.Level(p, g)
+        lv.upload(U, stream=stream)
+        # warm-up (includes the t = 0 wave-speed pass and the CUDA-graph capture)
+        lv.advance(args.warmup, use_graph=True, stream=stream)
+        torch.cuda.synchronize()
+        info0 = lv.sync()
+        clocks = Clocks(local)
+        barrier()
+        clocks.start()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        lv.advance(args.steps, use_graph=True, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_ms = e0.elapsed_time(e1)
+        clks.append(clocks.stop())
+        barrier()
+        info = lv.sync()
+        assert info.steps == info0.steps + args.steps, (info0, info)
+        ms[name] = max_over_ranks(t_ms)
+        levels[name] = lv
+    head = "mixed" if "mixed" in forms else "fp64"
+    p = forms[head]
+    value = world * cells * 3 * args.steps / (ms[head] / 1e3)
+
+    # error of the mixed form against the FP64 form after the same warm-up + timed steps
+    err = None
+    if len(levels) == 2:
+        shape = cb.padded_shape(p, g)
+        a = torch.empty(shape, dtype=torch.float64, device="cuda")
+        b = torch.empty(shape, dtype=torch.float64, device="cuda")
+        levels["mixed"].download(out=a, stream=stream)
+        levels["fp64"].download(out=b, stream=stream)
+        torch.cuda.synchronize()
+        va, vb = cb.valid_view(a, p, g), cb.valid_view(b, p, g)
+        names = ["a1rho1", "a2rho2", "rho_u", "rho_v", "rho_w", "a1rho1E1", "a2rho2E2", "alpha1"]
+        err = {"norm": "relative L1 (sum|mixed - fp64| / sum|fp64|) per field after "
+                       f"{args.warmup + args.steps} steps of the {n}^3 workload",
+               "fields": {nm: float((va[c] - vb[c]).abs().sum() / vb[c].abs().sum()) for c, nm in enumerate(names)},
+               "bound": "<= 1e-5 in a1rho1, a2rho2, alpha1"}
+        del a, b
+
+    # ---- roofline: the headline stage kernel alone, CUDA events around each launch ----
     N = cb.nstate(p.physics, p.dim)
     shape = cb.padded_shape(p, g)
     Us = torch.empty(shape, dtype=torch.float64, device="cuda")
-    lv.download(out=Us, stream=stream)
+    levels[head].download(out=Us, stream=stream)
     cb.FillPatch(p, g, Us, stream=stream)
     U0 = Us.clone()
     Un = torch.empty_like(Us)
     dt_dev = torch.tensor([1e-9], dtype=torch.float64, device="cuda")
     cmax = torch.zeros(1, dtype=torch.float64, device="cuda")
-    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    errw = torch.zeros(1, dtype=torch.int32, device="cuda")
     for s in range(3):
-        cb.ThirdOrderSSPRK_stage(p, g, s, Us, U0, Un, dt_dev, cmax, err, stream=stream)
+        cb.ThirdOrderSSPRK_stage(p, g, s, Us, U0, Un, dt_dev, cmax, errw, stream=stream)
     torch.cuda.synchronize()
-    reps = 2
     durs, algo = [], []
-    for _ in range(reps):
+    for _ in range(2):
         for s in range(3):
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            cb.ThirdOrderSSPRK_stage(p, g, s, Us, U0, Un, dt_dev, cmax, err, stream=stream)
-            b.record(stream)
-            b.synchronize()
-            durs.append(a.elapsed_time(b) / 1e3)
+            ea = torch.cuda.Event(enable_timing=True)
+            eb = torch.cuda.Event(enable_timing=True)
+            ea.record(stream)
+            cb.ThirdOrderSSPRK_stage(p, g, s, Us, U0, Un, dt_dev, cmax, errw, stream=stream)
+            eb.record(stream)
+            eb.synchronize()
+            durs.append(ea.elapsed_time(eb) / 1e3)
             algo.append(cells * N * 8 * (2 if s == 0 else 3))
     fa = torch.cuda.Event(enable_timing=True)
     fb = torch.cuda.Event(enable_timing=True)
@@ -270,7 +298,8 @@ def run_ours(args, rank, world, dist):
     peak, peak_kind = measured_peaks()
     del Us, U0, Un
 
-    # ---- e2e: host state in, one step, result out, every step ----
+    # ---- e2e: host state in, one step, result out, every step (headline form) ----
+    lv = levels[head]
     host_in = torch.empty(shape, dtype=torch.float64, pin_memory=True)
     host_out = torch.empty(shape, dtype=torch.float64, pin_memory=True)
     lv.download(out=host_in, stream=stream)
@@ -285,36 +314,44 @@ def run_ours(args, rank, world, dist):
         lv.advance(1, use_graph=True, stream=stream)
         lv.download(out=host_out, stream=stream)
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e = world * cells * 3 * args.steps / e2e_s
     lv.sync()
-    lv.close()
+    nbytes = int(lv.nbytes)
+    for l in levels.values():
+        l.close()
 
+    clk = None
+    good = [c for c in clks if c]
+    if good:
+        clk = {"sm_mhz": statistics.median([c["sm_mhz"] for c in good]), "sm_max_mhz": good[0]["sm_max_mhz"],
+               "reasons": sorted(set(r for c in good for r in c["reasons"])),
+               "samples": sum(c["samples"] for c in good)}
     line = None
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu:
             cpu = cpu_baseline(args.cpu_n, args.cpu_steps)
-        traffic = profiled_traffic("stage")
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(n, {"parallelism": f"replicas x{world}" if world > 1 else "single GPU"}),
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(lv.nbytes),
-                    "d2h_bytes_per_step": int(lv.nbytes),
+            "warmup": args.warmup, "ms_per_step": ms[head] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 reconstruction, f64 state/EOS/Riemann/relaxation" if head == "mixed" else "f64",
+            "data": "synthetic",
+            "config": workload_config(n, {"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                                          "precision": head}),
+            "fp64_plain": ({"value": world * cells * 3 * args.steps / (ms["fp64"] / 1e3),
+                            "ms_per_step": ms["fp64"] / args.steps,
+                            "note": "bit-identical to the reference CPU arithmetic"} if "fp64" in ms else None),
+            "mixed_error_vs_fp64": err,
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                     "path": "C-ABI level: set_state from pinned host, advance(1), download to pinned host"},
-            "gpu_launches": launches_value,
+            "gpu_launches": 8 * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "stage_kernel<SixEq<3>> (fused WENO5+HLLC+divergence+RK3+relaxation)",
+                         "frac": achieved / peak, "traffic": profiled_traffic("stage"),
+                         "kernel": f"stage_kernel<SixEq<3>, WENO5, {head}> (fused WENO5+HLLC+divergence+RK3+relaxation)",
                          "bytes_per_launch": bytes_per_launch, "mean_launch_ms": mean_dur * 1e3,
-                         "peak_source": f"{peak_kind} HBM copy bandwidth (MEASURED_PEAKS.json)",
-                         "note": "plain FP64 is FP64-pipe bound, not HBM bound; see profiles/"},
+                         "peak_source": f"{peak_kind} HBM copy bandwidth (MEASURED_PEAKS.json)"},
             "fill_boundary_ms": fill_ms,
             "clocks": clk,
             "cpu_baseline": cpu,

@@ -241,6 +241,79 @@ struct FiveEq {
     }
 };
 
+// Mixed-precision HLLC of the five-equation model. The wave speeds, S*, the star ratios
+// f = (S - V)/(S - S*) and the divisions and square roots run in FP32 on the reconstructed face
+// primitives (w); the star states and fluxes are assembled in FP64 from the FP64 face states U, so
+// that the large energy (alpha B ~ 1e9) enters only through f*E and stays consistent with the
+// alpha flux f*alpha (the pressure recovered from E - sum alpha_k B_k is not polluted).
+template <int DIM>
+__device__ __forceinline__ void fiveeq_hllc_mixed(double* Fout, double* fnc, float& cmax, const double* UL,
+                                                  const double* UR, const float* wL, const float* wR,
+                                                  const Eos& e, int d, int id_k) {
+    using M = FiveEq<DIM>;
+    constexpr int N = M::N, IE = M::IE, IA = M::IA;
+    auto csound = [&](const float* w) {
+        const float p = w[IE], a1 = w[IA], a2 = 1.0f - a1;
+        const float A1 = (float)e.A1, A2 = (float)e.A2, B1 = (float)e.B1, B2 = (float)e.B2;
+        const float r1 = __fdividef(__fmaf_rn(A1 + 1.0f, p, B1), A1);
+        const float r2 = __fdividef(__fmaf_rn(A2 + 1.0f, p, B2), A2);
+        const float ph1 = (e.C1 > 0.0) ? a1 - (float)e.C1 * w[0] : a1;
+        const float ph2 = (e.C2 > 0.0) ? a2 - (float)e.C2 * w[1] : a2;
+        float rc2;
+        if (id_k == 0)
+            rc2 = __fdividef(__fmaf_rn(a1 * A1, r1, (a2 * A2) * r2), __fmaf_rn(ph1, A1, ph2 * A2));
+        else
+            rc2 = __fdividef(1.0f, __fdividef(ph1, r1) + __fdividef(ph2, r2));
+        return sqrtf(fmaxf(rc2, 0.0f) / (w[0] + w[1]));
+    };
+    const float cL = csound(wL), cR = csound(wR);
+    const float VL = (d == 0) ? wL[2] : ((d == 1 || DIM == 2) ? wL[3] : wL[DIM == 3 ? 4 : 3]);
+    const float VR = (d == 0) ? wR[2] : ((d == 1 || DIM == 2) ? wR[3] : wR[DIM == 3 ? 4 : 3]);
+    const float pL = wL[IE], pR = wR[IE];
+    const float rhoL = wL[0] + wL[1], rhoR = wR[0] + wR[1];
+    const float Va = 0.5f * (VL + VR), ca = 0.5f * (cL + cR);
+    const float SL = fminf(Va - ca, VL - cL), SR = fmaxf(Va + ca, VR + cR);
+    const float Sm = fminf(0.0f, SL), Sp = fmaxf(0.0f, SR);
+    // delta form: dS = S* - V and f - 1 from the jumps, exactly 0 where p and V are uniform
+    const float gL = SL - VL, gR = SR - VR;
+    const float aL = rhoL * gL, aR = rhoR * gR;
+    const float inv_den = __fdividef(1.0f, aL - aR);
+    const float dp = pR - pL, dV = VL - VR;
+    const float dSL = __fmaf_rn(aR, dV, dp) * inv_den, dSR = __fmaf_rn(aL, dV, dp) * inv_den;
+    const float S = VL + dSL;
+    const float fm1L = __fdividef(dSL, gL - dSL), fm1R = __fdividef(dSR, gR - dSR);
+    const float eL = (1.0f + fm1L) * dSL * (rhoL * S + __fdividef(pL, gL));
+    const float eR = (1.0f + fm1R) * dSR * (rhoR * S + __fdividef(pR, gR));
+    const float mL = (1.0f + fm1L) * rhoL * dSL, mR = (1.0f + fm1R) * rhoR * dSR;
+    const float s = (S > 0.0f) ? 1.0f : ((S < 0.0f) ? -1.0f : 0.0f);
+    // FP64 assembly: F = h+ (F_L + S- (U*_L - U_L)) + h- (F_R + S+ (U*_R - U_R))
+    const double hp = 0.5 * (1.0 + s), hm = 0.5 * (1.0 - s);
+    const double gmL = fm1L, gmR = fm1R, Smd = Sm, Spd = Sp;
+    const double VLd = VL, VRd = VR, pLd = pL, pRd = pR;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        double fl = UL[i] * VLd, fr = UR[i] * VRd;
+        double dL = gmL * UL[i], dR = gmR * UR[i];
+        if (i == IE) {
+            fl = (UL[IE] + pLd) * VLd;
+            fr = (UR[IE] + pRd) * VRd;
+            dL += (double)eL;
+            dR += (double)eR;
+        } else if (i >= 2 && i < 2 + DIM && i - 2 == d) {
+            fl += pLd;
+            fr += pRd;
+            dL += (double)mL;
+            dR += (double)mR;
+        }
+        Fout[i] = hp * (fl + Smd * dL) + hm * (fr + Spd * dR);
+    }
+    fnc[0] = (hp * VLd + hm * VRd) + ((hp * Smd) * gmL + (hm * Spd) * gmR);
+    float kL = wL[2] * wL[2] + wL[3] * wL[3], kR = wR[2] * wR[2] + wR[3] * wR[3];
+    if (DIM == 3) { kL += wL[4] * wL[4]; kR += wR[4] * wR[4]; }
+    cmax = fmaxf(cL + sqrtf(kL), cR + sqrtf(kR));
+    (void)IA;
+}
+
 // ------------------------------------------------------------------------------------------------
 // Six-equation model: U = (a1r1, a2r2, rho u_d, a1r1E1, a2r2E2, alpha1),
 //                     W = (a1r1, a2r2, u_d, a1p1, a2p2, alpha1)
@@ -402,6 +475,80 @@ struct SixEq {
         cmax = dmax(qL, qR);
     }
 };
+
+// Mixed-precision HLLC of the six-equation model (same split as fiveeq_hllc_mixed). The phase-energy
+// star states are written E* = f E + (V alpha p - S* (alpha p)*)/(S* - S), the identity of
+// Riemann_HLLC_Compressible6Eq.H:163-200 with (V - S)/(S* - S) = f, so that E enters only through f.
+template <int DIM>
+__device__ __forceinline__ void sixeq_hllc_mixed(double* Fout, double* fnc, float& cmax, const double* UL,
+                                                 const double* UR, const float* wL, const float* wR,
+                                                 const Eos& e, int d) {
+    using M = SixEq<DIM>;
+    constexpr int N = M::N, IE1 = M::IE1, IE2 = M::IE2, IA = M::IA;
+    auto csound = [&](const float* w) {
+        const float a1 = w[IA];
+        const float xi1 = (e.C1 > 0.0 && a1 > 0.0f) ? 1.0f - (float)e.C1 * __fdividef(w[0], a1) : 1.0f;
+        const float xi2 = (e.C2 > 0.0 && 1.0f - a1 > 0.0f) ? 1.0f - (float)e.C2 * __fdividef(w[1], 1.0f - a1) : 1.0f;
+        const float r1 = __fdividef(__fmaf_rn((float)e.A1 + 1.0f, w[IE1], a1 * (float)e.B1), (float)e.A1 * xi1);
+        const float r2 = __fdividef(__fmaf_rn((float)e.A2 + 1.0f, w[IE2], (1.0f - a1) * (float)e.B2), (float)e.A2 * xi2);
+        return sqrtf(fmaxf(r1 + r2, 0.0f) / (w[0] + w[1]));
+    };
+    const float cL = csound(wL), cR = csound(wR);
+    const float VL = (d == 0) ? wL[2] : ((d == 1 || DIM == 2) ? wL[3] : wL[DIM == 3 ? 4 : 3]);
+    const float VR = (d == 0) ? wR[2] : ((d == 1 || DIM == 2) ? wR[3] : wR[DIM == 3 ? 4 : 3]);
+    const float SL = fminf(VL - cL, VR - cR), SR = fmaxf(VL + cL, VR + cR);
+    const float Sm = fminf(0.0f, SL), Sp = fmaxf(0.0f, SR);
+    const float rhoL = wL[0] + wL[1], rhoR = wR[0] + wR[1];
+    const float pL = wL[IE1] + wL[IE2], pR = wR[IE1] + wR[IE2];
+    // delta form: dS = S* - V and f - 1 from the jumps, exactly 0 where p and V are uniform
+    const float gL = SL - VL, gR = SR - VR;
+    const float aL = rhoL * gL, aR = rhoR * gR;
+    const float inv_den = __fdividef(1.0f, aL - aR);
+    const float dp = pR - pL, dV = VL - VR;
+    const float dSL = __fmaf_rn(aR, dV, dp) * inv_den, dSR = __fmaf_rn(aL, dV, dp) * inv_den;
+    const float S = VL + dSL;
+    const float qL = __fdividef(dSL, gL - dSL), qR = __fdividef(dSR, gR - dSR);  // f - 1
+    const float fL = 1.0f + qL, fR = 1.0f + qR;
+    // phase pressures at the star state: (alpha p)* = alpha p + alpha rho (S - V) dS, and the
+    // pressure part t of the phase-energy star state E* = f E + t, t = dS ((alpha p) + S* alpha rho g)/(g - dS)
+    const float a1p1L = wL[IE1], a2p2L = wL[IE2], a1p1R = wR[IE1], a2p2R = wR[IE2];
+    const float tL1 = qL * __fmaf_rn(S * wL[0], gL, a1p1L), tR1 = qR * __fmaf_rn(S * wR[0], gR, a1p1R);
+    const float tL2 = qL * __fmaf_rn(S * wL[1], gL, a2p2L), tR2 = qR * __fmaf_rn(S * wR[1], gR, a2p2R);
+    const float mL = fL * rhoL * dSL, mR = fR * rhoR * dSR;
+    const float s = (S > 0.0f) ? 1.0f : ((S < 0.0f) ? -1.0f : 0.0f);
+    const double hp = 0.5 * (1.0 + s), hm = 0.5 * (1.0 - s);
+    const double gmL = qL, gmR = qR, Smd = Sm, Spd = Sp;
+    const double VLd = VL, VRd = VR;
+    const double p1L = a1p1L, p2L = a2p2L, p1R = a1p1R, p2R = a2p2R;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        double fl = UL[i] * VLd, fr = UR[i] * VRd;
+        double dL = gmL * UL[i], dR = gmR * UR[i];
+        if (i >= 2 && i < 2 + DIM && i - 2 == d) {
+            fl += p1L + p2L;
+            fr += p1R + p2R;
+            dL += (double)mL;
+            dR += (double)mR;
+        } else if (i == IE1) {
+            fl = (UL[IE1] + p1L) * VLd;
+            fr = (UR[IE1] + p1R) * VRd;
+            dL += (double)tL1;
+            dR += (double)tR1;
+        } else if (i == IE2) {
+            fl = (UL[IE2] + p2L) * VLd;
+            fr = (UR[IE2] + p2R) * VRd;
+            dL += (double)tL2;
+            dR += (double)tR2;
+        }
+        Fout[i] = hp * (fl + Smd * dL) + hm * (fr + Spd * dR);
+    }
+    fnc[0] = (hp * VLd + hm * VRd) + ((hp * Smd) * gmL + (hm * Spd) * gmR);
+    fnc[1] = hp * (VLd * p1L + Smd * (double)tL1) + hm * (VRd * p1R + Spd * (double)tR1);
+    fnc[2] = hp * (VLd * p2L + Smd * (double)tL2) + hm * (VRd * p2R + Spd * (double)tR2);
+    float kL = wL[2] * wL[2] + wL[3] * wL[3], kR = wR[2] * wR[2] + wR[3] * wR[3];
+    if (DIM == 3) { kL += wL[4] * wL[4]; kR += wR[4] * wR[4]; }
+    cmax = fmaxf(cL + sqrtf(kL), cR + sqrtf(kR));
+}
 
 // ------------------------------------------------------------------------------------------------
 // WENO5 face value, epsilon-free weights from smoothness ratios with a NaN guard.
@@ -596,6 +743,17 @@ __device__ __forceinline__ void weno5_f32_parts(float f_mm, float f_m, float f_c
     const float IS0 = __fmaf_rn((10.0f / 3.0f) * a, a, __fmaf_rn(-(11.0f / 3.0f) * a, b, (4.0f / 3.0f) * b * b));
     const float IS1 = __fmaf_rn(-(5.0f / 3.0f) * c, a, (4.0f / 3.0f) * __fmaf_rn(c, c, a * a));
     const float IS2 = __fmaf_rn((10.0f / 3.0f) * c, c, __fmaf_rn(-(11.0f / 3.0f) * g, c, (4.0f / 3.0f) * g * g));
+    const bool z0 = (IS0 == 0.0f), z1 = (IS1 == 0.0f), z2 = (IS2 == 0.0f);
+    if (z0 | z1 | z2) {
+        // the ratio-form weights where some indicators vanish: the stencils with IS = 0 share the
+        // weight in proportion to their linear weights, the others get none (uniform stencil: d_k)
+        const float s = (z0 ? d0 : 0.0f) + (z1 ? d1 : 0.0f) + (z2 ? d2 : 0.0f);
+        const float inv = __fdividef(1.0f, s);
+        w[0] = z0 ? d0 * inv : 0.0f;
+        w[1] = z1 ? d1 * inv : 0.0f;
+        w[2] = z2 ? d2 * inv : 0.0f;
+        return;
+    }
     const float r01 = __fdividef(IS0, IS1), r02 = __fdividef(IS0, IS2);
     if (IS1 > 0.0f && IS2 > 0.0f && r01 < 1.0e15f && r02 < 1.0e15f) {
         const float s01 = r01 * r01, s02 = r02 * r02;

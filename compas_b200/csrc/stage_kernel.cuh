@@ -91,6 +91,7 @@ __device__ __forceinline__ void load_cons(double* U, const double* base, const G
 // relaxation in FP64.
 template <class M, int SCHEME, bool MIX, int TX, int TY, int TZ, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
+    static_assert(TX == TY && (M::D == 2 ? TZ == 1 : TZ == TX), "tiles are cubes (squares in 2D)");
     using PT = typename std::conditional<MIX, float, double>::type;
     using T = TileShape<M, TX, TY, TZ, PT>;
     constexpr int N = M::N, NC = M::NC, D = M::D, NB = T::NB;
@@ -137,10 +138,10 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
 
 #pragma unroll 1
     for (int d = 0; d < D; ++d) {
-        const int Td = (d == 0) ? TX : (d == 1 ? TY : TZ);
-        const int Ad = (d == 0) ? T::A0 : (d == 1 ? T::A1 : T::A2);
-        // transverse extents (a fastest) of direction d
-        const int Ta = (d == 0) ? TY : TX;
+        // cube (square) tiles: every direction has the same line length, slab area and transverse side
+        constexpr int Td = TX;
+        constexpr int Ad = T::A0;
+        constexpr int Ta = TX;
         // 2a. halo slabs of direction d -> primitives
         for (int h = tid; h < 6 * Ad; h += NT) {
             const int slot = h / Ad, t = h % Ad;
@@ -164,33 +165,48 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
         }
         __syncthreads();
 
-        // 2b. faces of direction d (x fastest, so neighbouring threads read neighbouring cells)
-        const int Ex = TX + (d == 0), Ey = TY + (d == 1), Ez = TZ + (d == 2);
-        const int NF = Ex * Ey * Ez;
+        // 2b. faces of direction d. Tiles are cubes (squares in 2D) of side TS, so every direction has
+        // TS + 1 faces per line and the decode below divides by compile-time constants. For d = 0 the
+        // face position runs fastest, for d > 0 the x index does, so that neighbouring threads read
+        // neighbouring cells of the shared primitive arrays.
+        constexpr int TS = TX;
+        constexpr int EF = TS + 1;
+        const int NF = EF * T::A0;
         for (int f = tid; f < NF; f += NT) {
-            const int fx = f % Ex, fy = (f / Ex) % Ey, fz = f / (Ex * Ey);
+            int fd, ta, tb;
+            if (d == 0) {
+                fd = f % EF;
+                const int t0 = f / EF;
+                ta = t0 % TS;
+                tb = t0 / TS;
+            } else {
+                ta = f % TS;
+                const int r0 = f / TS;
+                fd = r0 % EF;
+                tb = r0 / EF;
+            }
+            int fx, fy, fz;
+            if (d == 0) { fx = fd; fy = ta; fz = tb; }
+            else if (d == 1) { fx = ta; fy = fd; fz = tb; }
+            else { fx = ta; fy = tb; fz = fd; }
             const int gi = i0 + fx, gj = j0 + fy, gk = k0 + fz;
             const bool valid = (d == 0 ? gi <= g.n[0] : gi < g.n[0]) && (d == 1 ? gj <= g.n[1] : gj < g.n[1]) &&
                                (D == 2 || (d == 2 ? gk <= g.n[2] : gk < g.n[2]));
             if (!valid) continue;
-            const int fd = (d == 0) ? fx : (d == 1 ? fy : fz);
-            // transverse index of this face line (same convention as the halo slots)
-            const int ta = (d == 0) ? fy : fx;
-            const int tb = (d == 2) ? fy : fz;
-            const int t = ta + Ta * tb;
+            const int t = ta + TS * tb;
             // shared-memory offset and component stride of the six stencil cells f-3 .. f+2
             int off[6], str[6];
 #pragma unroll
             for (int s = 0; s < 6; ++s) {
                 const int pos = fd - 3 + s;
-                if (pos >= 0 && pos < Td) {
+                if (pos >= 0 && pos < TS) {
                     int lx = fx, ly = fy, lz = fz;
                     if (d == 0) lx = pos; else if (d == 1) ly = pos; else lz = pos;
                     off[s] = lx + TX * (ly + TY * lz);
                     str[s] = CELLS;
                 } else {
-                    const int slot = (pos < 0) ? pos + 3 : pos - Td + 3;
-                    off[s] = N * CELLS + slot * Ad + t;
+                    const int slot = (pos < 0) ? pos + 3 : pos - TS + 3;
+                    off[s] = N * CELLS + slot * T::A0 + t;
                     str[s] = HALO;
                 }
             }
@@ -222,6 +238,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
                 M::prim2cons(UR, WfR, a.e, err);
                 M::hllc(F, fnc, cm, UL, UR, a.e, d, a.id_k, err);
             } else {
+                float wL[N], wR[N];
                 if constexpr (SCHEME == 6) {
                     float r1[6], r2[6], al[6];
 #pragma unroll
@@ -230,23 +247,30 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
                         r2[s] = smem[off[s] + str[s]];
                         al[s] = smem[off[s] + M::IA * str[s]];
                     }
-                    float x0, x1, x2;
-                    weno5b_masses_f32(r1, r2, al, 1, x0, x1, x2);
-                    WfL[0] = x0; WfL[1] = x1; WfL[M::IA] = x2;
-                    weno5b_masses_f32(r1 + 1, r2 + 1, al + 1, -1, x0, x1, x2);
-                    WfR[0] = x0; WfR[1] = x1; WfR[M::IA] = x2;
+                    weno5b_masses_f32(r1, r2, al, 1, wL[0], wL[1], wL[M::IA]);
+                    weno5b_masses_f32(r1 + 1, r2 + 1, al + 1, -1, wR[0], wR[1], wR[M::IA]);
                 }
 #pragma unroll
                 for (int n = NB0; n < NB1; ++n) {
                     const float w0 = smem[off[0] + n * str[0]], w1 = smem[off[1] + n * str[1]];
                     const float w2 = smem[off[2] + n * str[2]], w3 = smem[off[3] + n * str[3]];
                     const float w4 = smem[off[4] + n * str[4]], w5 = smem[off[5] + n * str[5]];
-                    WfL[n] = (double)weno5_f32(w0, w1, w2, w3, w4, 1);
-                    WfR[n] = (double)weno5_f32(w1, w2, w3, w4, w5, -1);
+                    wL[n] = weno5_f32(w0, w1, w2, w3, w4, 1);
+                    wR[n] = weno5_f32(w1, w2, w3, w4, w5, -1);
+                }
+#pragma unroll
+                for (int n = 0; n < N; ++n) {
+                    WfL[n] = wL[n];
+                    WfR[n] = wR[n];
                 }
                 M::prim2cons(UL, WfL, a.e, err);
                 M::prim2cons(UR, WfR, a.e, err);
-                M::hllc_uw(F, fnc, cm, UL, WfL, UR, WfR, a.e, d, a.id_k, err);
+                float cmf;
+                if constexpr (M::NC == 1)
+                    fiveeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, a.e, d, a.id_k);
+                else
+                    sixeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, a.e, d);
+                cm = cmf;
             }
 #pragma unroll
             for (int n = 0; n < N; ++n) Fb[n * FMAX + f] = F[n];
@@ -254,20 +278,22 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
             for (int c = 0; c < NC; ++c) Fb[(N + c) * FMAX + f] = fnc[c];
             const int gd = (d == 0) ? gi : (d == 1 ? gj : gk);
             const int nd = (d == 0) ? g.n[0] : (d == 1 ? g.n[1] : g.n[2]);
-            if (fd < Td && gd < nd) cmax_local = dmax(cm, cmax_local);
+            if (fd < TS && gd < nd) cmax_local = dmax(cm, cmax_local);
         }
         __syncthreads();
 
         // 2c. divergence contribution of direction d
         const double dxd = (d == 0) ? g.dx[0] : (d == 1 ? g.dx[1] : g.dx[2]);
-        const int fstride = (d == 0) ? 1 : (d == 1 ? TX : TX * TY);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int l = tid + r * NT;
             if (l < CELLS) {
                 const int lx = l % TX, ly = (l / TX) % TY, lz = l / (TX * TY);
-                const int fl = lx + Ex * (ly + Ey * lz);
-                const int fh = fl + fstride;
+                // low and high faces of the cell in the enumeration of 2b
+                int fl, fh;
+                if (d == 0) { fl = lx + EF * (ly + TS * lz); fh = fl + 1; }
+                else if (d == 1) { fl = lx + TS * (ly + EF * lz); fh = fl + TS; }
+                else { fl = lx + TS * (lz + EF * ly); fh = fl + TS; }
 #pragma unroll
                 for (int c = 0; c < NB; ++c) {
                     const double tt = (Fb[c * FMAX + fh] - Fb[c * FMAX + fl]) / dxd;

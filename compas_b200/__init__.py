@@ -111,6 +111,20 @@ _SIGS = {
                                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_uint)]),
     "compas_b200_level_dts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
     "compas_b200_level_launches": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "compas_b200_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                ctypes.POINTER(ctypes.c_void_p)]),
+    "compas_b200_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "compas_b200_batch_add": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Parm), ctypes.POINTER(Geom),
+                                             ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                             ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    "compas_b200_batch_remove": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "compas_b200_batch_advance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+    "compas_b200_batch_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    "compas_b200_batch_download": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                                  ctypes.c_void_p]),
+    "compas_b200_batch_bytes": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "compas_b200_batch_launches": (ctypes.c_longlong, [ctypes.c_void_p]),
 }
 
 EXPORTED_SYMBOLS = tuple(_SIGS)
@@ -305,3 +319,83 @@ class Level:
 
     def launches(self) -> int:
         return int(lib().compas_b200_level_launches(self._h))
+
+
+@dataclass
+class CaseInfo:
+    id: int
+    t: float
+    steps: int
+    done: bool
+    status: int
+
+
+class Batch:
+    """Many independent single-box cases (uneven sizes, own EOS and boundaries, own time-step control)
+    advanced together, one persistent launch per RK stage over a device-side box list."""
+
+    def __init__(self, physics: int, dim: int, id_limiter: int = 5, precision: int = 0, capacity: int = 1024):
+        self.physics, self.dim = physics, dim
+        self._h = ctypes.c_void_p()
+        _check(lib().compas_b200_batch_create(physics, dim, id_limiter, precision, capacity, ctypes.byref(self._h)))
+        self.capacity = capacity
+        self._shapes = {}
+
+    def close(self) -> None:
+        if self._h:
+            lib().compas_b200_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, p: Parm, g: Geom, U, stop_time: float = 1.0e300, max_steps: int = 2 ** 31 - 1,
+            stream=None) -> int:
+        cid = ctypes.c_int()
+        if isinstance(U, np.ndarray):
+            U = np.ascontiguousarray(U, dtype=np.float64)
+            ptr, dev = U.ctypes.data, 0
+        else:
+            ptr, dev = U.data_ptr(), 1 if U.is_cuda else 0
+        _check(lib().compas_b200_batch_add(self._h, ctypes.byref(p), ctypes.byref(g), ptr, dev, float(stop_time),
+                                           int(max_steps), _stream_ptr(stream), ctypes.byref(cid)))
+        self._shapes[cid.value] = padded_shape(p, g)
+        return cid.value
+
+    def remove(self, case_id: int, stream=None) -> None:
+        _check(lib().compas_b200_batch_remove(self._h, int(case_id), _stream_ptr(stream)))
+        self._shapes.pop(case_id, None)
+
+    def advance(self, nsteps: int, use_graph: bool = True, stream=None) -> None:
+        _check(lib().compas_b200_batch_advance(self._h, int(nsteps), 1 if use_graph else 0, _stream_ptr(stream)))
+
+    def poll(self) -> list:
+        cap = max(len(self._shapes), 1)
+        ids = (ctypes.c_int * cap)()
+        ts = (ctypes.c_double * cap)()
+        st = (ctypes.c_int * cap)()
+        dn = (ctypes.c_int * cap)()
+        er = (ctypes.c_uint * cap)()
+        n = lib().compas_b200_batch_poll(self._h, ids, ts, st, dn, er, cap)
+        if n < 0:
+            _check(n)
+        return [CaseInfo(ids[i], ts[i], st[i], bool(dn[i]), er[i]) for i in range(min(n, cap))]
+
+    def download(self, case_id: int, out=None, stream=None):
+        if out is None:
+            out = np.empty(self._shapes[case_id], dtype=np.float64)
+        if isinstance(out, np.ndarray):
+            _check(lib().compas_b200_batch_download(self._h, int(case_id), out.ctypes.data, 0, _stream_ptr(stream)))
+        else:
+            _check(lib().compas_b200_batch_download(self._h, int(case_id), out.data_ptr(), 1 if out.is_cuda else 0,
+                                                    _stream_ptr(stream)))
+        return out
+
+    def bytes(self) -> int:
+        return int(lib().compas_b200_batch_bytes(self._h))
+
+    def launches(self) -> int:
+        return int(lib().compas_b200_batch_launches(self._h))

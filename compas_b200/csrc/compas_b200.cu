@@ -87,15 +87,17 @@ __device__ __forceinline__ double bc_map(int& x, int len, int code_lo, int code_
 // Filling x, then y, then z over the full extent of the other directions (the oracle's order)
 // gives at every ghost cell the valid cell found by mapping each coordinate independently, with
 // the product of the per-direction signs, which is what this kernel computes directly.
-__global__ void fill_boundary_kernel(BcArgs a) {
-    const Grid& g = a.g;
+__host__ __device__ __forceinline__ long long ghost_count(const Grid& g) {
+    return 2LL * g.gz * g.pxy + 2LL * g.ng * g.px * g.n[2] + 2LL * g.ng * g.n[1] * g.n[2];
+}
+
+// Fill ghost cell number q (enumeration above) of U, all components.
+__device__ __forceinline__ void fill_ghost_cell(double* U, const Grid& g, int N, int D, const int* lo, const int* hi,
+                                                long long q) {
     const long long PX = g.px, PY = g.pxy / g.px;
     const long long nz_slab = 2LL * g.gz * PX * PY;
     const long long ny_slab = 2LL * g.ng * PX * g.n[2];
-    const long long nx_slab = 2LL * g.ng * g.n[1] * g.n[2];
-    const long long total = nz_slab + ny_slab + nx_slab;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-         q += (long long)gridDim.x * blockDim.x) {
+    {
         int i, j, k;
         if (q < nz_slab) {
             const long long plane = PX * PY;
@@ -122,14 +124,21 @@ __global__ void fill_boundary_kernel(BcArgs a) {
             i = (s < g.ng) ? s - g.ng : g.n[0] + (s - g.ng);
         }
         const long long dst = g.at(i, j, k);
-        for (int n = 0; n < a.N; ++n) {
+        for (int n = 0; n < N; ++n) {
             int si = i, sj = j, sk = k;
-            double sgn = bc_map(si, g.n[0], a.lo[0], a.hi[0], n, 0, a.D);
-            sgn *= bc_map(sj, g.n[1], a.lo[1], a.hi[1], n, 1, a.D);
-            if (a.D == 3) sgn *= bc_map(sk, g.n[2], a.lo[2], a.hi[2], n, 2, a.D);
-            a.U[n * g.S + dst] = sgn * a.U[n * g.S + g.at(si, sj, sk)];
+            double sgn = bc_map(si, g.n[0], lo[0], hi[0], n, 0, D);
+            sgn *= bc_map(sj, g.n[1], lo[1], hi[1], n, 1, D);
+            if (D == 3) sgn *= bc_map(sk, g.n[2], lo[2], hi[2], n, 2, D);
+            U[n * g.S + dst] = sgn * U[n * g.S + g.at(si, sj, sk)];
         }
     }
+}
+
+__global__ void fill_boundary_kernel(BcArgs a) {
+    const long long total = ghost_count(a.g);
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+         q += (long long)gridDim.x * blockDim.x)
+        fill_ghost_cell(a.U, a.g, a.N, a.D, a.lo, a.hi, q);
 }
 
 template <int D>
@@ -238,7 +247,7 @@ static Grid make_grid(const compas_b200_parm* p, const compas_b200_geom* g) {
 }
 
 static Eos make_eos(const compas_b200_parm* p) {
-    return Eos{p->A1, p->A2, p->B1, p->B2, p->C1, p->C2, p->D1, p->D2};
+    return Eos{p->A1, p->A2, p->B1, p->B2, p->C1, p->C2, p->D1, p->D2, 1.0 / p->A1, 1.0 / p->A2};
 }
 
 static int nstate(const compas_b200_parm* p) {
@@ -361,6 +370,8 @@ static StageArgs base_args(const compas_b200_parm* p, const compas_b200_geom* g)
 }
 
 }  // namespace compas
+
+#include "batch.cuh"
 
 // ================================================================================================
 // C ABI
@@ -778,5 +789,268 @@ int compas_b200_level_dts(compas_b200_level* lv, double* dts, int n) {
     CUDA_TRY(cudaMemcpy(dts, lv->dts, sizeof(double) * n, cudaMemcpyDeviceToHost));
     return COMPAS_B200_OK;
 }
+
+
+// ---- batched independent cases (box list) ------------------------------------------------------
+
+static int batch_sync_list(compas_b200_batch* b, cudaStream_t st) {
+    const int nb = (int)b->cases.size();
+    std::vector<BoxDesc> boxes(nb);
+    std::vector<int> tile_off(nb + 1, 0), slots(nb, 0);
+    std::vector<long long> ghost_off(nb + 1, 0);
+    for (int i = 0; i < nb; ++i) {
+        const BatchCase& c = b->cases[i];
+        BoxDesc& B = boxes[i];
+        std::memset(&B, 0, sizeof(B));
+        B.g = make_grid(&c.p, &c.g);
+        B.e = make_eos(&c.p);
+        for (int k = 0; k < 3; ++k) B.U[k] = c.U[k];
+        StepCtl* ctl = b->d_ctl + c.slot;
+        B.dt = &ctl->dt;
+        B.done = &ctl->done;
+        B.cmax = &ctl->cmax;
+        B.err = &ctl->err;
+        for (int d = 0; d < 3; ++d) {
+            B.lo_bc[d] = c.g.lo_bc[d];
+            B.hi_bc[d] = c.g.hi_bc[d];
+        }
+        B.id_k = c.p.source_term;
+        B.relax = (c.p.physics == COMPAS_B200_SIXEQS) ? c.p.relaxation : 0;
+        B.trace = c.p.relax_trace;
+        B.tiles = tile_count(b->dim, B.g);
+        B.ghosts = ghost_count(B.g);
+        tile_off[i + 1] = tile_off[i] + B.tiles;
+        ghost_off[i + 1] = ghost_off[i] + B.ghosts;
+        slots[i] = c.slot;
+    }
+    if (nb > 0) {
+        CUDA_TRY(cudaMemcpyAsync(b->d_boxes, boxes.data(), sizeof(BoxDesc) * nb, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(b->d_slots, slots.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, st));
+    }
+    CUDA_TRY(cudaMemcpyAsync(b->d_tile_off, tile_off.data(), sizeof(int) * (nb + 1), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(b->d_ghost_off, ghost_off.data(), sizeof(long long) * (nb + 1), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(b->d_nbox, &nb, sizeof(int), cudaMemcpyHostToDevice, st));
+    // pageable sources: make the copies complete before the vectors go out of scope
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return COMPAS_B200_OK;
+}
+
+int compas_b200_batch_create(int physics, int dim, int id_limiter, int precision, int capacity,
+                             compas_b200_batch** out) {
+    if (!out) return fail(COMPAS_B200_EARG, "null output");
+    *out = nullptr;
+    compas_b200_parm probe;
+    int rc = compas_b200_parm_init(&probe, physics, dim);
+    if (rc) return rc;
+    if (id_limiter != 5 && id_limiter != 6) return fail(COMPAS_B200_EUNSUPPORTED, "WENO5 (5) or WENO5B (6)");
+    if (precision != 0 && precision != 1) return fail(COMPAS_B200_EARG, "precision 0 or 1");
+    if (capacity < 1 || capacity > (1 << 20)) return fail(COMPAS_B200_EARG, "capacity out of range");
+    auto* b = new compas_b200_batch();
+    b->physics = physics;
+    b->dim = dim;
+    b->limiter = id_limiter;
+    b->precision = precision;
+    b->capacity = capacity;
+    for (int i = capacity - 1; i >= 0; --i) b->free_slots.push_back(i);
+    cudaError_t e = cudaMalloc(&b->d_boxes, sizeof(BoxDesc) * capacity);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_nbox, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_tile_off, sizeof(int) * (capacity + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_ghost_off, sizeof(long long) * (capacity + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_slots, sizeof(int) * capacity);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_ctl, sizeof(StepCtl) * capacity);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_cs, sizeof(CaseStep) * capacity);
+    if (e == cudaSuccess) e = cudaMemset(b->d_ctl, 0, sizeof(StepCtl) * capacity);
+    if (e == cudaSuccess) e = cudaMemset(b->d_nbox, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(b->d_tile_off, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(b->d_ghost_off, 0, sizeof(long long));
+    if (e != cudaSuccess) {
+        compas_b200_batch_destroy(b);
+        cudaGetLastError();
+        return fail(COMPAS_B200_ENOMEM, std::string("batch allocation: ") + cudaGetErrorString(e));
+    }
+    *out = b;
+    return COMPAS_B200_OK;
+}
+
+int compas_b200_batch_destroy(compas_b200_batch* b) {
+    if (!b) return COMPAS_B200_OK;
+    cudaDeviceSynchronize();
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (auto& c : b->cases)
+        for (int k = 0; k < 3; ++k) cudaFree(c.U[k]);
+    cudaFree(b->d_boxes);
+    cudaFree(b->d_nbox);
+    cudaFree(b->d_tile_off);
+    cudaFree(b->d_ghost_off);
+    cudaFree(b->d_slots);
+    cudaFree(b->d_ctl);
+    cudaFree(b->d_cs);
+    delete b;
+    return COMPAS_B200_OK;
+}
+
+int compas_b200_batch_add(compas_b200_batch* b, const compas_b200_parm* p, const compas_b200_geom* g,
+                          const double* U, int is_device, double stop_time, int max_steps, void* stream,
+                          int* case_id) {
+    if (!b || !U) return fail(COMPAS_B200_EARG, "null argument");
+    int rc = check_args(p, g);
+    if (rc) return rc;
+    if (p->physics != b->physics || p->dim != b->dim || p->id_limiter != b->limiter || p->precision != b->precision)
+        return fail(COMPAS_B200_EARG, "a batch holds cases of one model, dimension, scheme and precision");
+    if (b->free_slots.empty()) return fail(COMPAS_B200_ENOMEM, "batch capacity reached");
+    if (max_steps < 0) return fail(COMPAS_B200_EARG, "max_steps must be >= 0");
+    cudaStream_t st = (cudaStream_t)stream;
+    BatchCase c;
+    c.p = *p;
+    c.g = *g;
+    if (p->dim == 2) c.g.n[2] = 1;
+    c.bytes = compas_b200_state_bytes(p, g);
+    for (int k = 0; k < 3; ++k) {
+        cudaError_t e = cudaMalloc(&c.U[k], c.bytes);
+        if (e != cudaSuccess) {
+            for (int j = 0; j < k; ++j) cudaFree(c.U[j]);
+            cudaGetLastError();
+            return fail(COMPAS_B200_ENOMEM, std::string("case allocation: ") + cudaGetErrorString(e));
+        }
+    }
+    CUDA_TRY(cudaMemcpyAsync(c.U[0], U, c.bytes, is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    c.slot = b->free_slots.back();
+    b->free_slots.pop_back();
+    c.id = b->next_id++;
+    StepCtl h;
+    std::memset(&h, 0, sizeof(h));
+    h.dt_prev = 1.e100;
+    h.stop_time = stop_time;
+    CaseStep cs;
+    cs.cfl = p->cfl;
+    cs.dx[0] = g->dx[0];
+    cs.dx[1] = g->dx[1];
+    cs.dx[2] = g->dx[2];
+    cs.D = p->dim;
+    cs.limiter = p->change_limiter;
+    cs.max_steps = max_steps;
+    cs.stop_time = stop_time;
+    CUDA_TRY(cudaMemcpyAsync(b->d_ctl + c.slot, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(b->d_cs + c.slot, &cs, sizeof(cs), cudaMemcpyHostToDevice, st));
+    // CalculateInitialcmax of the new case
+    if ((rc = launch_fill(&c.p, &c.g, c.U[0], st))) return rc;
+    StageArgs a = base_args(&c.p, &c.g);
+    a.Us = c.U[0];
+    a.mode = kModeCmax;
+    a.cmax = &(b->d_ctl + c.slot)->cmax;
+    a.err = &(b->d_ctl + c.slot)->err;
+    if ((rc = launch_stage(&c.p, a, st))) return rc;
+    b->launches += 2;
+    b->cases.push_back(c);
+    b->bytes_in_use += 3 * c.bytes;
+    if (case_id) *case_id = c.id;
+    return batch_sync_list(b, st);
+}
+
+int compas_b200_batch_remove(compas_b200_batch* b, int case_id, void* stream) {
+    if (!b) return fail(COMPAS_B200_EARG, "null batch");
+    cudaStream_t st = (cudaStream_t)stream;
+    for (size_t i = 0; i < b->cases.size(); ++i) {
+        if (b->cases[i].id != case_id) continue;
+        BatchCase c = b->cases[i];
+        b->cases.erase(b->cases.begin() + i);
+        int rc = batch_sync_list(b, st);
+        CUDA_TRY(cudaStreamSynchronize(st));
+        for (int k = 0; k < 3; ++k) cudaFree(c.U[k]);
+        b->free_slots.push_back(c.slot);
+        b->bytes_in_use -= 3 * c.bytes;
+        return rc;
+    }
+    return fail(COMPAS_B200_EARG, "no case with id " + std::to_string(case_id));
+}
+
+static int batch_enqueue_step(compas_b200_batch* b, cudaStream_t st) {
+    step_begin_list_kernel<<<4, 256, 0, st>>>(b->d_ctl, b->d_cs, b->d_slots, b->d_nbox);
+    CUDA_TRY(cudaGetLastError());
+    const int N = (b->physics == COMPAS_B200_FIVEEQS ? 4 : 5) + b->dim;
+    int rc;
+    for (int s = 0; s < 3; ++s) {
+        FillListArgs F{b->d_boxes, b->d_nbox, b->d_ghost_off, N, b->dim, s};
+        fill_list_kernel<<<148 * 8, 256, 0, st>>>(F);
+        CUDA_TRY(cudaGetLastError());
+        ListArgs L{b->d_boxes, b->d_nbox, b->d_tile_off, kModeStage, s};
+        if ((rc = launch_list(b->physics, b->dim, b->limiter, b->precision, L, st))) return rc;
+    }
+    step_end_list_kernel<<<4, 256, 0, st>>>(b->d_ctl, b->d_slots, b->d_nbox);
+    CUDA_TRY(cudaGetLastError());
+    return COMPAS_B200_OK;
+}
+
+int compas_b200_batch_advance(compas_b200_batch* b, int nsteps, int use_graph, void* stream) {
+    if (!b) return fail(COMPAS_B200_EARG, "null batch");
+    if (nsteps < 0) return fail(COMPAS_B200_EARG, "nsteps must be >= 0");
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc;
+    if (use_graph) {
+        if (!b->graph || b->graph_stream != st) {
+            if (b->graph) {
+                cudaGraphExecDestroy(b->graph);
+                b->graph = nullptr;
+            }
+            cudaStream_t cap;
+            CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+            cudaGraph_t graph;
+            cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) {
+                cudaStreamDestroy(cap);
+                return fail(COMPAS_B200_ECUDA, std::string("begin capture: ") + cudaGetErrorString(e));
+            }
+            rc = batch_enqueue_step(b, cap);
+            e = cudaStreamEndCapture(cap, &graph);
+            cudaStreamDestroy(cap);
+            if (rc) return rc;
+            if (e != cudaSuccess) return fail(COMPAS_B200_ECUDA, std::string("end capture: ") + cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&b->graph, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) return fail(COMPAS_B200_ECUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+            b->graph_stream = st;
+        }
+        for (int s = 0; s < nsteps; ++s) CUDA_TRY(cudaGraphLaunch(b->graph, st));
+    } else {
+        for (int s = 0; s < nsteps; ++s)
+            if ((rc = batch_enqueue_step(b, st))) return rc;
+    }
+    b->launches += 8LL * nsteps;
+    return COMPAS_B200_OK;
+}
+
+int compas_b200_batch_poll(compas_b200_batch* b, int* ids, double* t, int* steps, int* done, unsigned int* status,
+                           int cap) {
+    if (!b) return fail(COMPAS_B200_EARG, "null batch");
+    CUDA_TRY(cudaDeviceSynchronize());
+    std::vector<StepCtl> h(b->capacity);
+    CUDA_TRY(cudaMemcpy(h.data(), b->d_ctl, sizeof(StepCtl) * b->capacity, cudaMemcpyDeviceToHost));
+    const int n = std::min<int>(cap, (int)b->cases.size());
+    for (int i = 0; i < n; ++i) {
+        const BatchCase& c = b->cases[i];
+        const StepCtl& s = h[c.slot];
+        if (ids) ids[i] = c.id;
+        if (t) t[i] = s.t;
+        if (steps) steps[i] = s.steps;
+        if (done) done[i] = s.done;
+        if (status) status[i] = s.err;
+    }
+    return (int)b->cases.size();
+}
+
+int compas_b200_batch_download(compas_b200_batch* b, int case_id, double* dst, int is_device, void* stream) {
+    if (!b || !dst) return fail(COMPAS_B200_EARG, "null argument");
+    for (const auto& c : b->cases)
+        if (c.id == case_id) {
+            CUDA_TRY(cudaMemcpyAsync(dst, c.U[0], c.bytes, is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                     (cudaStream_t)stream));
+            return COMPAS_B200_OK;
+        }
+    return fail(COMPAS_B200_EARG, "no case with id " + std::to_string(case_id));
+}
+
+long long compas_b200_batch_bytes(compas_b200_batch* b) { return b ? b->bytes_in_use : 0; }
+
+long long compas_b200_batch_launches(compas_b200_batch* b) { return b ? b->launches : 0; }
 
 }  // extern "C"

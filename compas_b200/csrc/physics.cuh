@@ -46,6 +46,7 @@ __device__ __forceinline__ double sgn0(double x) { return x > 0.0 ? 1.0 : (x < 0
 // C the NASG covolume b (source/Parm.cpp:101-188).
 struct Eos {
     double A1, A2, B1, B2, C1, C2, D1, D2;
+    double iA1, iA2;  // 1/A1, 1/A2 (mixed-precision pressure recovery)
 };
 
 // NASG: phi = alpha - b alpha rho (alpha when b = 0); covolume violation 1 - b rho <= 0 is reported
@@ -110,6 +111,28 @@ struct FiveEq {
         for (int d = 0; d < D; ++d) W[2 + d] = u[d];
         W[IE] = ((rho_e - rho_D) - BP) / AP;
         W[IA] = alpha1;
+    }
+
+    // Mixed precision: primitives rounded to FP32 for the reconstruction. The pressure numerator
+    // rho e - rho D - B_P, where the energy cancels against alpha B (~1e9), is formed in FP64; the
+    // divisions (velocities, the well-conditioned A_P) run in FP32.
+    __device__ static __forceinline__ void cons2prim_f32(float* W, const double* U, const Eos& e) {
+        const double a1r1 = U[0], a2r2 = U[1], alpha1 = U[IA];
+        const double rho = a1r1 + a2r2;
+        const double ir = 1.0 / rho;  // one FP64 reciprocal: u = fl32(rho u / rho) keeps uniform flow uniform
+        double m2 = U[2] * U[2] + U[3] * U[3];
+        if (D == 3) m2 += U[4] * U[4];
+        const double alpha2 = 1.0 - alpha1;
+        const double phi1 = (e.C1 > 0.0) ? alpha1 - e.C1 * a1r1 : alpha1;
+        const double phi2 = (e.C2 > 0.0) ? alpha2 - e.C2 * a2r2 : alpha2;
+        const double num = ((U[IE] - 0.5 * m2 * ir) - (a1r1 * e.D1 + a2r2 * e.D2)) - (phi1 * e.B1 + phi2 * e.B2);
+        const double AP = phi1 * e.A1 + phi2 * e.A2;
+        W[0] = (float)a1r1;
+        W[1] = (float)a2r2;
+#pragma unroll
+        for (int d = 0; d < D; ++d) W[2 + d] = (float)(U[2 + d] * ir);
+        W[IE] = (float)(num / AP);  // rounded once from FP64: a uniform pressure stays uniform
+        W[IA] = (float)alpha1;
     }
 
     __device__ static __forceinline__ void prim2cons(double* U, const double* W, const Eos& e, unsigned int* err) {
@@ -357,6 +380,29 @@ struct SixEq {
         W[IE1] = phase_p(a1r1e1, alpha1, a1r1, e.A1, e.B1, e.C1, e.D1, err);
         W[IE2] = phase_p(a2r2e2, alpha2, a2r2, e.A2, e.B2, e.C2, e.D2, err);
         W[IA] = alpha1;
+    }
+
+    // Mixed precision (see FiveEq::cons2prim_f32): phase-energy numerators in FP64, divisions in FP32.
+    __device__ static __forceinline__ void cons2prim_f32(float* W, const double* U, const Eos& e) {
+        const double a1r1 = U[0], a2r2 = U[1], alpha1 = U[IA];
+        const double alpha2 = 1.0 - alpha1;
+        const double rho = a1r1 + a2r2;
+        const double ir = 1.0 / rho;  // one FP64 reciprocal: u = fl32(rho u / rho) keeps uniform flow uniform
+        double m2 = U[2] * U[2] + U[3] * U[3];
+        if (D == 3) m2 += U[4] * U[4];
+        const double k = (m2 * ir) * ir;  // |u|^2
+        const float xi1 = (e.C1 > 0.0 && alpha1 > 0.0) ? (float)(1.0 - e.C1 * (a1r1 / alpha1)) : 1.0f;
+        const float xi2 = (e.C2 > 0.0 && alpha2 > 0.0) ? (float)(1.0 - e.C2 * (a2r2 / alpha2)) : 1.0f;
+        const double n1 = (U[IE1] - (0.5 * a1r1) * k - a1r1 * e.D1) - ((double)xi1 * alpha1) * e.B1;
+        const double n2 = (U[IE2] - (0.5 * a2r2) * k - a2r2 * e.D2) - ((double)xi2 * alpha2) * e.B2;
+        W[0] = (float)a1r1;
+        W[1] = (float)a2r2;
+#pragma unroll
+        for (int d = 0; d < D; ++d) W[2 + d] = (float)(U[2 + d] * ir);
+        // rounded once from FP64 (a uniform pressure stays uniform); the NASG factor 1/xi in FP32
+        W[IE1] = (float)(n1 * e.iA1) / xi1;
+        W[IE2] = (float)(n2 * e.iA2) / xi2;
+        W[IA] = (float)alpha1;
     }
 
     __device__ static __forceinline__ void prim2cons(double* U, const double* W, const Eos& e, unsigned int* err) {
@@ -743,38 +789,22 @@ __device__ __forceinline__ void weno5_f32_parts(float f_mm, float f_m, float f_c
     const float IS0 = __fmaf_rn((10.0f / 3.0f) * a, a, __fmaf_rn(-(11.0f / 3.0f) * a, b, (4.0f / 3.0f) * b * b));
     const float IS1 = __fmaf_rn(-(5.0f / 3.0f) * c, a, (4.0f / 3.0f) * __fmaf_rn(c, c, a * a));
     const float IS2 = __fmaf_rn((10.0f / 3.0f) * c, c, __fmaf_rn(-(11.0f / 3.0f) * g, c, (4.0f / 3.0f) * g * g));
+    // Where some indicators vanish the ratio form gives the stencils with IS = 0 the weight in
+    // proportion to their linear weights and the others none (a uniform stencil: d_k); otherwise the
+    // one-reciprocal form, with the ratios clamped at 1e18 where the weights are 0 or 1 to FP32
+    // precision anyway. Both are evaluated without branches.
     const bool z0 = (IS0 == 0.0f), z1 = (IS1 == 0.0f), z2 = (IS2 == 0.0f);
-    if (z0 | z1 | z2) {
-        // the ratio-form weights where some indicators vanish: the stencils with IS = 0 share the
-        // weight in proportion to their linear weights, the others get none (uniform stencil: d_k)
-        const float s = (z0 ? d0 : 0.0f) + (z1 ? d1 : 0.0f) + (z2 ? d2 : 0.0f);
-        const float inv = __fdividef(1.0f, s);
-        w[0] = z0 ? d0 * inv : 0.0f;
-        w[1] = z1 ? d1 * inv : 0.0f;
-        w[2] = z2 ? d2 * inv : 0.0f;
-        return;
-    }
-    const float r01 = __fdividef(IS0, IS1), r02 = __fdividef(IS0, IS2);
-    if (IS1 > 0.0f && IS2 > 0.0f && r01 < 1.0e15f && r02 < 1.0e15f) {
-        const float s01 = r01 * r01, s02 = r02 * r02;
-        const float inv = __fdividef(1.0f, __fmaf_rn(s01, d1, __fmaf_rn(s02, d2, d0)));
-        w[0] = d0 * inv;
-        w[1] = (d1 * s01) * inv;
-        w[2] = (d2 * s02) * inv;
-        return;
-    }
-    float IS01 = IS0 / IS1;
-    if (isnan(IS01)) IS01 = 1.0f;
-    const float IS10 = 1.0f / IS01;
-    float IS02 = IS0 / IS2;
-    if (isnan(IS02)) IS02 = 1.0f;
-    const float IS20 = 1.0f / IS02;
-    float IS12 = IS1 / IS2;
-    if (isnan(IS12)) IS12 = 1.0f;
-    const float IS21 = 1.0f / IS12;
-    w[0] = d0 / ((d0 + (IS01 * IS01) * d1) + (IS02 * IS02) * d2);
-    w[1] = d1 / (((IS10 * IS10) * d0 + d1) + (IS12 * IS12) * d2);
-    w[2] = d2 / (((IS20 * IS20) * d0 + (IS21 * IS21) * d1) + d2);
+    const bool anyz = z0 | z1 | z2;
+    const float szero = (z0 ? d0 : 0.0f) + (z1 ? d1 : 0.0f) + (z2 ? d2 : 0.0f);
+    // |ratio|: an indicator can round slightly below zero; the clamp then also bounds the square
+    const float r01 = fminf(fabsf(IS0 * __fdividef(1.0f, IS1)), 1.0e18f);
+    const float r02 = fminf(fabsf(IS0 * __fdividef(1.0f, IS2)), 1.0e18f);
+    const float s01 = anyz ? 0.0f : r01 * r01, s02 = anyz ? 0.0f : r02 * r02;
+    const float den = anyz ? szero : __fmaf_rn(s01, d1, __fmaf_rn(s02, d2, d0));
+    const float inv = __fdividef(1.0f, den);
+    w[0] = (anyz ? (z0 ? d0 : 0.0f) : d0) * inv;
+    w[1] = (anyz ? (z1 ? d1 : 0.0f) : d1 * s01) * inv;
+    w[2] = (anyz ? (z2 ? d2 : 0.0f) : d2 * s02) * inv;
 }
 
 __device__ __forceinline__ float weno5_f32(float f_mm, float f_m, float f_c, float f_p, float f_pp, int side) {

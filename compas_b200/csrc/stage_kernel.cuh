@@ -89,8 +89,9 @@ __device__ __forceinline__ void load_cons(double* U, const double* base, const G
 // primitives are recovered in FP64 (pressure from total energy) and kept in shared memory as FP32,
 // the reconstruction runs in FP32, the Riemann solver, divergence, stage accumulation and
 // relaxation in FP64.
-template <class M, int SCHEME, bool MIX, int TX, int TY, int TZ, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
+// The work of one CTA on tile `tile` of the box described by `a` (tiles numbered x fastest).
+template <class M, int SCHEME, bool MIX, int TX, int TY, int TZ, int NT>
+__device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double* smem_d) {
     static_assert(TX == TY && (M::D == 2 ? TZ == 1 : TZ == TX), "tiles are cubes (squares in 2D)");
     using PT = typename std::conditional<MIX, float, double>::type;
     using T = TileShape<M, TX, TY, TZ, PT>;
@@ -98,9 +99,6 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
     constexpr int CELLS = T::CELLS, HALO = T::HALO, FMAX = T::FMAX;
     constexpr int R = (CELLS + NT - 1) / NT;
 
-    if (a.done && *a.done) return;
-
-    extern __shared__ double smem_d[];
     PT* smem = reinterpret_cast<PT*>(smem_d);
     PT* Pint = smem;
     PT* Phal = Pint + N * CELLS;
@@ -109,7 +107,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
     const Grid& g = a.g;
     const int ntx = (g.n[0] + TX - 1) / TX;
     const int nty = (g.n[1] + TY - 1) / TY;
-    int b = blockIdx.x;
+    int b = tile;
     const int i0 = (b % ntx) * TX;
     b /= ntx;
     const int j0 = (b % nty) * TY;
@@ -121,16 +119,18 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
     for (int l = tid; l < CELLS; l += NT) {
         const int lx = l % TX, ly = (l / TX) % TY, lz = l / (TX * TY);
         const int i = i0 + lx, j = j0 + ly, k = k0 + lz;
-        double U[N], W[N];
+        double U[N];
+        PT W[N];
         if (g.padded(i, j, k)) {
             load_cons<M>(U, a.Us, g, g.at(i, j, k));
-            M::cons2prim(W, U, a.e, nullptr);
+            if constexpr (MIX) M::cons2prim_f32(W, U, a.e);
+            else M::cons2prim(W, U, a.e, nullptr);
         } else {
 #pragma unroll
-            for (int n = 0; n < N; ++n) W[n] = 0.0;
+            for (int n = 0; n < N; ++n) W[n] = 0;
         }
 #pragma unroll
-        for (int n = 0; n < N; ++n) Pint[n * CELLS + l] = (PT)W[n];
+        for (int n = 0; n < N; ++n) Pint[n * CELLS + l] = W[n];
     }
 
     double acc[R][NB];
@@ -152,16 +152,18 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
             else if (d == 1) { lx = ta; ly = pos; lz = tb; }
             else { lx = ta; ly = tb; lz = pos; }
             const int i = i0 + lx, j = j0 + ly, k = k0 + lz;
-            double U[N], W[N];
+            double U[N];
+            PT W[N];
             if (g.padded(i, j, k)) {
                 load_cons<M>(U, a.Us, g, g.at(i, j, k));
-                M::cons2prim(W, U, a.e, nullptr);
+                if constexpr (MIX) M::cons2prim_f32(W, U, a.e);
+                else M::cons2prim(W, U, a.e, nullptr);
             } else {
 #pragma unroll
-                for (int n = 0; n < N; ++n) W[n] = 0.0;
+                for (int n = 0; n < N; ++n) W[n] = 0;
             }
 #pragma unroll
-            for (int n = 0; n < N; ++n) Phal[n * HALO + h] = (PT)W[n];
+            for (int n = 0; n < N; ++n) Phal[n * HALO + h] = W[n];
         }
         __syncthreads();
 
@@ -321,11 +323,17 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
             const int i = i0 + lx, j = j0 + ly, k = k0 + lz;
             if (i >= g.n[0] || j >= g.n[1] || k >= g.n[2]) continue;
             double W[N], L[N];
+            const long long q = g.at(i, j, k);
+            double Us[N];
+            load_cons<M>(Us, a.Us, g, q);
             if constexpr (MIX) {
-                // the epilogue needs the FP64 primitives of the cell: recover them again
-                double Uc[N];
-                load_cons<M>(Uc, a.Us, g, g.at(i, j, k));
-                M::cons2prim(W, Uc, a.e, nullptr);
+                // masses and volume fraction exactly from the conserved state (FP64); the pressures
+                // of the non-conservative terms from the FP32 tile
+#pragma unroll
+                for (int n = 0; n < N; ++n) W[n] = Pint[n * CELLS + l];
+                W[0] = Us[0];
+                W[1] = Us[1];
+                W[M::IA] = Us[M::IA];
             } else {
 #pragma unroll
                 for (int n = 0; n < N; ++n) W[n] = Pint[n * CELLS + l];
@@ -348,14 +356,11 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
                 L[M::IE2] = L[M::IE2] + (-x);
                 L[M::IA] = L[M::IA] + W[M::IA] * divv;
             }
-            const long long q = g.at(i, j, k);
             double out[N];
             if (a.mode == kModeDudt) {
 #pragma unroll
                 for (int n = 0; n < N; ++n) out[n] = L[n];
             } else {
-                double Us[N];
-                load_cons<M>(Us, a.Us, g, q);
                 if (a.stage == 0) {
 #pragma unroll
                     for (int n = 0; n < N; ++n) out[n] = 1.0 * Us[n] + sdt * L[n];
@@ -396,6 +401,82 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
             // non-negative doubles order like their bit patterns; a NaN speed propagates as the max
             atomicMax(a.cmax, (unsigned long long)__double_as_longlong(m));
         }
+    }
+}
+
+// One box: one CTA per tile.
+template <class M, int SCHEME, bool MIX, int TX, int TY, int TZ, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
+    if (a.done && *a.done) return;
+    extern __shared__ double smem_d[];
+    stage_tile<M, SCHEME, MIX, TX, TY, TZ, NT>(a, blockIdx.x, smem_d);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Box list: many boxes (independent cases of uneven size, or the boxes of a level) in one
+// persistent launch. The list, its tile prefix sums and its length live in device memory, so a
+// captured CUDA graph stays valid while boxes are added or removed between launches.
+// ------------------------------------------------------------------------------------------------
+struct BoxDesc {
+    Grid g;
+    Eos e;
+    double* U[3];                 // U^n, U^(1), U^(2) of the box (stage s reads U[s], writes U[(s+1)%3])
+    const double* dt;             // the box's time step (device)
+    const int* done;              // the box's no-op flag (device)
+    unsigned long long* cmax;     // the box's wave-speed accumulator (device)
+    unsigned int* err;            // the box's status word (device)
+    int lo_bc[3], hi_bc[3];
+    int id_k;
+    int relax;
+    double trace;
+    int tiles;                    // tiles of the box for the kernel's tile shape
+    long long ghosts;             // ghost cells of one array of the box
+};
+
+struct ListArgs {
+    const BoxDesc* boxes;
+    const int* nbox;              // number of boxes (device)
+    const int* tile_off;          // exclusive prefix sums of BoxDesc::tiles, nbox + 1 entries
+    int mode;
+    int stage;
+};
+
+__device__ __forceinline__ int find_box(const int* off, int nb, int w) {
+    int lo = 0, hi = nb - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= w) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <class M, int SCHEME, bool MIX, int TX, int TY, int TZ, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) stage_list_kernel(ListArgs L) {
+    extern __shared__ double smem_d[];
+    const int nb = *L.nbox;
+    if (nb <= 0) return;
+    const int total = L.tile_off[nb];
+    for (int w = blockIdx.x; w < total; w += gridDim.x) {
+        const int b = find_box(L.tile_off, nb, w);
+        const BoxDesc& B = L.boxes[b];
+        if (*B.done) continue;
+        StageArgs a;
+        a.g = B.g;
+        a.e = B.e;
+        a.mode = L.mode;
+        a.stage = L.stage;
+        a.Us = B.U[L.stage];
+        a.U0 = B.U[0];
+        a.Uout = B.U[(L.stage + 1) % 3];
+        a.dt = B.dt;
+        a.done = B.done;
+        a.cmax = B.cmax;
+        a.err = B.err;
+        a.id_k = B.id_k;
+        a.relax = B.relax;
+        a.trace = B.trace;
+        __syncthreads();  // the previous tile's readers of shared memory are done
+        stage_tile<M, SCHEME, MIX, TX, TY, TZ, NT>(a, w - L.tile_off[b], smem_d);
     }
 }
 

@@ -174,6 +174,40 @@ int compas_b200_level_dts(compas_b200_level* lv, double* dts, int n);
 /* Kernel launches the library enqueued on this level since upload. */
 long long compas_b200_level_launches(compas_b200_level* lv);
 
+/* ---- batched independent cases ------------------------------------------------------------------
+ * Many single-box cases of uneven size (each with its own EOS, boundary codes, stop time, step budget
+ * and time-step control) advanced together: every RK stage of every case runs in ONE persistent
+ * launch over a device-side box list (the serving/batching form; no reference counterpart - the
+ * reference advances one problem per process). The launches of one coarse step are captured once in
+ * a CUDA graph; admitting and retiring cases between advances does not invalidate it. A case whose
+ * stop time or step budget is reached stays in place as a no-op until it is removed. All cases of a
+ * batch share the model, dimension, scheme and precision. */
+typedef struct compas_b200_batch compas_b200_batch;
+
+int compas_b200_batch_create(int physics, int dim, int id_limiter, int precision, int capacity,
+                             compas_b200_batch** out);
+int compas_b200_batch_destroy(compas_b200_batch* b);
+
+/* Admit a case: allocates its three state arrays, copies the state in (padded layout, time 0) and
+ * runs the t = 0 wave-speed pass. *case_id receives its id. */
+int compas_b200_batch_add(compas_b200_batch* b, const compas_b200_parm* p, const compas_b200_geom* g,
+                          const double* U, int is_device, double stop_time, int max_steps, void* stream,
+                          int* case_id);
+int compas_b200_batch_remove(compas_b200_batch* b, int case_id, void* stream);
+
+/* Enqueue nsteps coarse steps of every active case (no host synchronisation). */
+int compas_b200_batch_advance(compas_b200_batch* b, int nsteps, int use_graph, void* stream);
+
+/* Wait for the device and report, for up to `cap` cases in admission order, id, time, steps taken,
+ * the no-op flag and the status word. Returns the number of cases in the batch. */
+int compas_b200_batch_poll(compas_b200_batch* b, int* ids, double* t, int* steps, int* done, unsigned int* status,
+                           int cap);
+int compas_b200_batch_download(compas_b200_batch* b, int case_id, double* dst, int is_device, void* stream);
+
+/* Device bytes held by the cases' state arrays. */
+long long compas_b200_batch_bytes(compas_b200_batch* b);
+long long compas_b200_batch_launches(compas_b200_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

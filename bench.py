@@ -49,6 +49,11 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batch-steps", type=int, default=10)
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=16)
+    ap.add_argument("--serve-rate", type=float, default=16.0)
     return ap.parse_args()
 
 
@@ -150,6 +155,77 @@ def cpu_baseline(n, steps):
     return {"value": val, "unit": UNIT, "cores": o.threads(), "kind": kind,
             "sample": f"{n}^3 cells of the same shock-droplet case, {steps} coarse steps (3 RK stages each) "
                       f"after one untimed step, OpenMP over {o.threads()} host threads, {el:.1f} s"}
+
+
+def run_batched(args):
+    """48 independent 2D FIVEEQS shock-bubble cases (seeded, uneven sizes) in one persistent box-list
+    launch per RK stage (mixed precision, WENO5B, CUDA-graph steps), against the same cases run one
+    after the other on single-case levels."""
+    import torch
+
+    import compas_b200 as cb
+    from compas_b200 import cases
+
+    stream = torch.cuda.current_stream()
+    cs = cases.batch_shock_bubbles(count=48, seed=0, xp=torch, device="cuda")
+    cells = sum(c[3]["n"][0] * c[3]["n"][1] for c in cs)
+    K, W = args.batch_steps, 2
+    out = {"workload": "48 independent 2D FIVEEQS shock-bubble cases, numpy PCG64 seed 0: side U{64..768}, "
+                       "aspect U[1,2], Mach U[1.1,3], density ratio logU[0.01,1000], radius U[0.1,0.3]; WENO5B+HLLC",
+           "cases": len(cs), "cells": cells, "steps": K}
+    for prec in ("mixed", "fp64"):
+        b = cb.Batch(cb.FIVEEQS, 2, id_limiter=6, precision=1 if prec == "mixed" else 0)
+        for phys, dim, inputs, geom, U, _ in cs:
+            b.add(cb.make_parm(phys, dim, dict(inputs, **{"compas_b200.precision": prec})), cb.make_geom(**geom), U)
+        b.advance(W, stream=stream)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.advance(K, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        assert all(i.status == 0 for i in b.poll())
+        out[f"batched_{prec}"] = cells * 3 * K / (ms / 1e3)
+        b.close()
+        # the same cases one after the other
+        tot = 0.0
+        for phys, dim, inputs, geom, U, _ in cs:
+            lv = cb.Level(cb.make_parm(phys, dim, dict(inputs, **{"compas_b200.precision": prec})),
+                          cb.make_geom(**geom))
+            lv.upload(U, stream=stream)
+            lv.advance(W, stream=stream)
+            e0.record(stream)
+            lv.advance(K, stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1)
+            lv.close()
+        out[f"sequential_{prec}"] = cells * 3 * K / (tot / 1e3)
+    out["unit"] = UNIT + " per RK stage (aggregate over the cases)"
+    out["batched_mixed_vs_sequential_fp64"] = out["batched_mixed"] / out["sequential_fp64"]
+    return out
+
+
+def run_serving(args):
+    """Poisson arrivals of mixed 2D shock-bubble / 3D shock-droplet solves under an HBM budget,
+    continuous batching, against the same requests one at a time on the plain FP64 path."""
+    from compas_b200 import serving
+
+    reqs = serving.poisson_requests(args.serve_requests, args.serve_rate, seed=0, sides2d=(128, 512),
+                                    sides3d=(64, 96), steps=(100, 300))
+    srv = serving.Server(budget_bytes=150e9, precision="mixed", steps_per_iter=4)
+    t0 = time.perf_counter()
+    done = srv.run(reqs)
+    wall = time.perf_counter() - t0
+    srv.close()
+    summ = serving.summarize(done, wall)
+    seq = serving.sequential_baseline(reqs, precision="fp64")
+    return {"workload": f"{len(reqs)} requests, Poisson rate {args.serve_rate}/s (seed 0): 2D FIVEEQS shock-bubble "
+                        "128^2-512^2 and 3D SIXEQS shock-droplet 64^3-96^3, 100-300 steps each; budget 150 GB",
+            "continuous_batching_mixed": summ, "sequential_fp64": seq,
+            "throughput_ratio": summ["cell_updates_per_s_per_stage"] / seq["cell_updates_per_s_per_stage"]}
 
 
 def run_reference(args, rank):
@@ -332,6 +408,8 @@ def run_ours(args, rank, world, dist):
         cpu = None
         if world == 1 and not args.no_cpu:
             cpu = cpu_baseline(args.cpu_n, args.cpu_steps)
+        batched = None if args.no_batched else run_batched(args)
+        serving_res = None if args.no_serving else run_serving(args)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms[head] / args.steps, "higher_is_better": True,
@@ -355,6 +433,8 @@ def run_ours(args, rank, world, dist):
             "fill_boundary_ms": fill_ms,
             "clocks": clk,
             "cpu_baseline": cpu,
+            "batched": batched,
+            "serving": serving_res,
         }
     return line
 

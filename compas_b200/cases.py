@@ -148,14 +148,14 @@ def advected_disc(n=128, ng=3, quadrature=True, xp=None, device=None):
 
 
 def shock_bubble(nx=2048, ny=1024, ng=3, quadrature=True, xp=None, device=None, Ma=1.22, rho_b=0.138,
-                 gamma_b=1.648, radius=0.25, center=(0.6, 0.5), scheme="WENO5B"):
-    """2D FIVEEQS shock-helium-bubble on [0,2]x[0,1]: air (phase 1, gamma 1.4, rho 1, p 1), helium
-    bubble (phase 2) with a tanh interface of width 2 dx, a Mach-Ma shock at x = 0.2 with the
-    Rankine-Hugoniot post-shock state on its left; reflective top/bottom (code 4), outflow
-    left/right (code 2)."""
+                 gamma_b=1.648, radius=0.25, center=(0.6, 0.5), scheme="WENO5B", length=2.0):
+    """2D FIVEEQS shock-helium-bubble on [0,length]x[0,1] (default [0,2]x[0,1]): air (phase 1, gamma
+    1.4, rho 1, p 1), helium bubble (phase 2) with a tanh interface of width 2 dx, a Mach-Ma shock at
+    x = 0.2 with the Rankine-Hugoniot post-shock state on its left; reflective top/bottom (code 4),
+    outflow left/right (code 2)."""
     xp = _xp_of(xp)
     dim, physics = 2, FIVEEQS
-    L = 2.0
+    L = float(length)
     dx = (L / nx, 1.0 / ny, 1.0)
     g1, g2 = 1.4, gamma_b
     A = (1.0 / (g1 - 1.0), 1.0 / (g2 - 1.0))
@@ -218,3 +218,27 @@ def algorithmic_bytes_per_cell_stage(physics: int, dim: int) -> float:
     """(8/3) N 8 B: stage 1 reads U and writes U1 (2N doubles), stages 2 and 3 read U^(s), U^0 and
     write (3N doubles); relaxation is fused and adds nothing."""
     return (8.0 / 3.0) * nstate(physics, dim) * 8.0
+
+
+def batch_shock_bubbles(count=48, seed=0, xp=None, device=None, quadrature=True, scheme="WENO5B",
+                        sides=tuple(range(64, 769, 64))):
+    """Independent 2D FIVEEQS shock-bubble cases with parameters drawn from numpy's PCG64 with `seed`:
+    grid side (cells in y) uniform in `sides` (64, 128, ..., 768), aspect ratio U[1, 2] (cells in x =
+    side x aspect, square cells, domain [0, aspect] x [0, 1]), shock Mach U[1.1, 3], bubble/ambient
+    density ratio log-uniform in [0.01, 1000], radius U[0.1, 0.3] (centred at x = 0.3 + r + 0.05).
+    Returns a list of (physics, dim, inputs, geom, U, params)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for _ in range(count):
+        side = int(rng.choice(np.array(sides)))
+        aspect = float(rng.uniform(1.0, 2.0))
+        Ma = float(rng.uniform(1.1, 3.0))
+        ratio = float(np.exp(rng.uniform(np.log(0.01), np.log(1000.0))))
+        r = float(rng.uniform(0.1, 0.3))
+        nx = int(round(side * aspect))
+        length = nx / side
+        phys, dim, inputs, geom, U = shock_bubble(nx=nx, ny=side, Ma=Ma, rho_b=ratio, radius=r,
+                                                  center=(0.3 + r + 0.05, 0.5), scheme=scheme, length=length,
+                                                  xp=xp, device=device, quadrature=quadrature)
+        out.append((phys, dim, inputs, geom, U, dict(side=side, nx=nx, aspect=aspect, Ma=Ma, ratio=ratio, r=r)))
+    return out

@@ -73,3 +73,34 @@ def test_batch_sixeq_3d_two_sizes():
         alone, _, _ = run_gpu(p, g, U, 3)
         np.testing.assert_array_equal(cb.valid_view(b.download(cid), p, g), cb.valid_view(alone, p, g))
     b.close()
+
+
+def test_serving_results_identical_alone_and_in_the_mix():
+    """Continuous batching: requests admitted while others run give the same state as alone."""
+    from compas_b200 import serving
+
+    reqs = serving.poisson_requests(6, rate=200.0, seed=1, sides2d=(32, 64), sides3d=(16, 24), steps=(5, 12))
+    srv = serving.Server(budget_bytes=150e9, precision="mixed", keep_results=True, steps_per_iter=1)
+    done = srv.run(reqs)
+    srv.close()
+    assert len(done) == len(reqs)
+    overlap = sum(1 for a in done for b in done if a is not b and a.admitted < b.finished and b.admitted < a.finished)
+    assert overlap > 0, "no request overlapped another"
+    for r in done:
+        p, g, U = serving.make_case(r, "mixed")
+        alone, info, _ = run_gpu(p, g, U.cpu().numpy(), r.steps)
+        assert info.steps == r.steps
+        np.testing.assert_array_equal(cb.valid_view(r.result, p, g), cb.valid_view(alone, p, g))
+
+
+def test_serving_budget_admission_waits():
+    from compas_b200 import serving
+
+    reqs = serving.poisson_requests(4, rate=1000.0, seed=2, kinds=("bubble2d",), sides2d=(64, 64), steps=(4, 4))
+    one = 3 * 6 * (64 + 6) * (64 + 6) * 8
+    srv = serving.Server(budget_bytes=one * 1.5, precision="fp64", steps_per_iter=1)
+    done = srv.run(reqs)
+    srv.close()
+    # with room for one case at a time, no two requests overlap
+    spans = sorted((r.admitted, r.finished) for r in done)
+    assert all(spans[i][1] <= spans[i + 1][0] + 1e-9 for i in range(len(spans) - 1))

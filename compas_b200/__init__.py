@@ -97,6 +97,9 @@ _SIGS = {
                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "compas_b200_relaxation": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_void_p,
                                               ctypes.c_void_p, ctypes.c_void_p]),
+    "compas_b200_rk3_step_noalloc": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_void_p,
+                                                    ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                                                    ctypes.c_void_p]),
     "compas_b200_level_create": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom),
                                                 ctypes.POINTER(ctypes.c_void_p)]),
     "compas_b200_level_destroy": (ctypes.c_int, [ctypes.c_void_p]),
@@ -228,6 +231,13 @@ def ThirdOrderSSPRK_stage(p: Parm, g: Geom, stage: int, Us, Uold, Unew, dt_dev, 
     """One fused stage of ThirdOrderSSPRK plus PostTimeStage (source/Class_Compressible_PhaseField.cpp:3937-4107)."""
     _check(lib().compas_b200_rk3_stage(ctypes.byref(p), ctypes.byref(g), stage, _ptr(Us), _ptr(Uold), _ptr(Unew),
                                        _ptr(dt_dev), _ptr(cmax), _ptr(err), _stream_ptr(stream)))
+
+
+def ThirdOrderSSPRK_step_noalloc(p: Parm, g: Geom, U, dt: float, cmax=None, err=None, stream=None) -> None:
+    """One whole TVD-RK3 step in place on U (device) without allocating device memory: the stage
+    states live in the library's fixed scratch array (states up to 16 MiB; see compas_b200.h)."""
+    _check(lib().compas_b200_rk3_step_noalloc(ctypes.byref(p), ctypes.byref(g), _ptr(U), float(dt), _ptr(cmax),
+                                              _ptr(err), _stream_ptr(stream)))
 
 
 def Relaxation(p: Parm, g: Geom, U, err=None, stream=None) -> None:

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <string>
 #include <type_traits>
+#include <mutex>
 #include <vector>
 
 #include "compas_b200.h"
@@ -369,6 +370,38 @@ static StageArgs base_args(const compas_b200_parm* p, const compas_b200_geom* g)
     return a;
 }
 
+// ------------------------------------------------------------------------------------------------
+// Allocation-free RK3 step: the two intermediate stage states and the step's dt live in this
+// file-scope device array instead of memory the library or the caller allocates. It is created with
+// the module on every GPU that loads the library and held until the process exits.
+// ------------------------------------------------------------------------------------------------
+constexpr long long kNoAllocStateBytes = 16LL << 20;       // largest state array (with ghosts) accepted
+constexpr long long kNoAllocHeadBytes = 256;               // dt of the step
+constexpr long long kNoAllocBytes = kNoAllocHeadBytes + 2 * kNoAllocStateBytes;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+__global__ void noalloc_set_dt_kernel(double* dt_slot, double dt) { *dt_slot = dt; }
+
+// Device address of g_noalloc_scratch on the current device, looked up once per device.
+static int noalloc_scratch(unsigned char** out) {
+    static std::mutex mu;
+    static unsigned char* addr[128] = {nullptr};
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 128) return fail(COMPAS_B200_EARG, "device index out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr)
+            return fail(COMPAS_B200_ECUDA, std::string("cudaGetSymbolAddress of the scratch array: ") +
+                                               cudaGetErrorString(e));
+        addr[dev] = static_cast<unsigned char*>(ptr);
+    }
+    *out = addr[dev];
+    return COMPAS_B200_OK;
+}
+
 }  // namespace compas
 
 #include "batch.cuh"
@@ -603,6 +636,48 @@ int compas_b200_relaxation(const compas_b200_parm* p, const compas_b200_geom* g,
     else
         relax_kernel<3><<<(unsigned)blocks, 128, 0, (cudaStream_t)stream>>>(U, G, make_eos(p), p->relax_trace, err_dev);
     CUDA_TRY(cudaGetLastError());
+    return COMPAS_B200_OK;
+}
+
+// One TVD-RK3 step in place on the caller's state U without allocating device memory. The two
+// intermediate stage states and the device copy of dt live in g_noalloc_scratch; everything else is
+// the same launches as compas_b200_rk3_stage (boundary fill, then the fused stage kernel, three times).
+int compas_b200_rk3_step_noalloc(const compas_b200_parm* p, const compas_b200_geom* g, double* U, double dt,
+                                 double* cmax_dev, unsigned int* err_dev, void* stream) {
+    int rc = check_args(p, g);
+    if (rc) return rc;
+    if (!U) return fail(COMPAS_B200_EARG, "null state");
+    if (!(dt > 0.0) || !(dt <= DBL_MAX)) return fail(COMPAS_B200_EARG, "dt must be positive and finite");
+    const long long bytes = compas_b200_state_bytes(p, g);
+    if (bytes > kNoAllocStateBytes)
+        return fail(COMPAS_B200_EARG, "state of " + std::to_string(bytes) + " bytes exceeds the " +
+                                          std::to_string(kNoAllocStateBytes) +
+                                          "-byte limit of the allocation-free step; use the level API");
+    unsigned char* base = nullptr;
+    if ((rc = noalloc_scratch(&base))) return rc;
+    double* dt_dev = reinterpret_cast<double*>(base);
+    double* U1 = reinterpret_cast<double*>(base + kNoAllocHeadBytes);
+    double* U2 = reinterpret_cast<double*>(base + kNoAllocHeadBytes + kNoAllocStateBytes);
+    cudaStream_t st = (cudaStream_t)stream;
+    // the scratch keeps the previous call's contents: dt is rewritten here, U1 and U2 are fully
+    // written (valid cells by the stage kernels, ghosts by the boundary fill) before they are read
+    noalloc_set_dt_kernel<<<1, 1, 0, st>>>(dt_dev, dt);
+    CUDA_TRY(cudaGetLastError());
+    StageArgs a = base_args(p, g);
+    a.mode = kModeStage;
+    a.dt = dt_dev;
+    a.cmax = reinterpret_cast<unsigned long long*>(cmax_dev);
+    a.err = err_dev;
+    double* ins[3] = {U, U1, U2};
+    double* outs[3] = {U1, U2, U};
+    for (int s = 0; s < 3; ++s) {
+        if ((rc = launch_fill(p, g, ins[s], st))) return rc;
+        a.stage = s;
+        a.Us = ins[s];
+        a.U0 = U;
+        a.Uout = outs[s];
+        if ((rc = launch_stage(p, a, st))) return rc;
+    }
     return COMPAS_B200_OK;
 }
 

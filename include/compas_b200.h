@@ -138,6 +138,26 @@ int compas_b200_rk3_stage(const compas_b200_parm* p, const compas_b200_geom* g, 
 int compas_b200_relaxation(const compas_b200_parm* p, const compas_b200_geom* g, double* U, unsigned int* err_dev,
                            void* stream);
 
+/* One TVD-RK3 step of size dt (stages 0-2 with their boundary fills and, for SIXEQS, the pressure
+ * relaxation) in place on the caller-owned state U, WITHOUT ALLOCATING ANY DEVICE MEMORY. This entry
+ * point has no counterpart in the reference. It is for callers that cannot call cudaMalloc - code
+ * running while a CUDA graph is being captured, callers whose memory is owned by another allocator
+ * (an AMReX arena, a framework's caching allocator) that must stay the only allocator, or hosts with
+ * a fixed memory reservation - which still want a whole step from one call.
+ *   - The two intermediate stage states live in a file-scope device array of this library,
+ *     2 x 16 MiB plus 256 bytes, created on every GPU that loads the library and held until the
+ *     process exits. A state (compas_b200_state_bytes) larger than 16 MiB is rejected with
+ *     COMPAS_B200_EARG; use compas_b200_level_* for larger boxes.
+ *   - The first call on a device looks up that array's device address (cudaGetSymbolAddress) and
+ *     caches it, so make the first call on each device before any stream capture.
+ *   - Every call on a device shares the one array and leaves its contents behind; the call rewrites
+ *     everything it reads. Calls that overlap on the GPU (other streams, other host threads) race on
+ *     it: serialize them.
+ *   - cmax_dev and err_dev as in compas_b200_rk3_stage (device pointers, may be NULL; cmax is
+ *     max-accumulated, so clear it first if the step's own maximum is wanted). */
+int compas_b200_rk3_step_noalloc(const compas_b200_parm* p, const compas_b200_geom* g, double* U, double dt,
+                                 double* cmax_dev, unsigned int* err_dev, void* stream);
+
 /* ---- single-level advance with device-resident state and time-step control -------------------- */
 
 typedef struct compas_b200_level compas_b200_level;

@@ -147,6 +147,34 @@ def advected_disc(n=128, ng=3, quadrature=True, xp=None, device=None):
     return physics, dim, inputs, geom, U
 
 
+def advected_interface(n=32, dim=3, physics=SIXEQS, ng=3, quadrature=True, xp=None, device=None, relaxation=1):
+    """The advected interface of advected_disc for either model in 2D or 3D: phase-2 disc / sphere of
+    radius 0.25 at the centre of the periodic unit square / cube, the same phases, p = 1e5 and
+    velocity 1 along every axis; for SIXEQS the pressure relaxation after every stage."""
+    xp = _xp_of(xp)
+    dx = (1.0 / n, 1.0 / n, 1.0 / n if dim == 3 else 1.0)
+    g1, g2, pinf2 = 1.4, 4.4, 6e8
+    A = (1.0 / (g1 - 1.0), 1.0 / (g2 - 1.0))
+    B = (0.0, g2 * pinf2 / (g2 - 1.0))
+
+    def pw(x, y, z):
+        r2 = (x - 0.5) ** 2 + (y - 0.5) ** 2 + ((z - 0.5) ** 2 if dim == 3 else 0.0)
+        a2 = _clip(xp, 0.5 * (1.0 + _tanh(xp, (0.25 - _sqrt(xp, r2)) / (2.0 * dx[0]))), 1e-6, 1.0 - 1e-6)
+        a1 = 1.0 - a2
+        vel = [x * 0 + 1.0, y * 0 + 1.0] + ([z * 0 + 1.0] if dim == 3 else [])
+        return _cons_from_prims(physics, dim, a1 * 1.0, a2 * 1000.0, vel, 1e5, a1, A, B, xp)
+
+    inputs = {"FiniteVolume.Scheme": "WENO5", "Physics.RiemannSolver": "HLLC", "prob.EOS.EOS": 1,
+              "prob.EOS.gamma_1": g1, "prob.EOS.gamma_2": g2, "prob.EOS.pinf_1": 0.0, "prob.EOS.pinf_2": pinf2,
+              "run.cfl": 0.5}
+    if physics == SIXEQS:
+        inputs["Physics.pressure_relaxation"] = relaxation
+    nz = n if dim == 3 else 1
+    geom = dict(n=(n, n, nz), dx=dx, ng=ng, lo_bc=(0, 0, 0), hi_bc=(0, 0, 0))
+    U = _average(physics, dim, (n, n, nz), dx, (0.0, 0.0, 0.0), pw, ng, quadrature, xp, device)
+    return physics, dim, inputs, geom, U
+
+
 def shock_bubble(nx=2048, ny=1024, ng=3, quadrature=True, xp=None, device=None, Ma=1.22, rho_b=0.138,
                  gamma_b=1.648, radius=0.25, center=(0.6, 0.5), scheme="WENO5B", length=2.0):
     """2D FIVEEQS shock-helium-bubble on [0,length]x[0,1] (default [0,2]x[0,1]): air (phase 1, gamma

@@ -93,45 +93,8 @@ __global__ void step_end_list_kernel(StepCtl* ctl, const int* slots, const int* 
     }
 }
 
-template <class M, int SCHEME, bool MIX, int TX, int TY, int TZ, int NT, int MINB>
-static int launch_list_t(const ListArgs& L, cudaStream_t st) {
-    using T = TileShape<M, TX, TY, TZ, typename std::conditional<MIX, float, double>::type>;
-    auto kern = stage_list_kernel<M, SCHEME, MIX, TX, TY, TZ, NT, MINB>;
-    static int grid = 0;
-    if (!grid) {
-        CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
-        int dev = 0, sms = 0, per = 0;
-        CUDA_TRY(cudaGetDevice(&dev));
-        CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, NT, T::SMEM));
-        grid = sms * std::max(per, 1);
-    }
-    kern<<<grid, NT, T::SMEM, st>>>(L);
-    CUDA_TRY(cudaGetLastError());
-    return COMPAS_B200_OK;
-}
-
-template <int SCHEME, bool MIX>
-static int launch_list_s(int physics, int dim, const ListArgs& L, cudaStream_t st) {
-    if (physics == COMPAS_B200_FIVEEQS) {
-        if (dim == 2) return launch_list_t<FiveEq<2>, SCHEME, MIX, 16, 16, 1, COMPAS_NT2, COMPAS_MINB2>(L, st);
-        return launch_list_t<FiveEq<3>, SCHEME, MIX, 8, 8, 8, COMPAS_NT3, COMPAS_MINB3>(L, st);
-    }
-    if (dim == 2) return launch_list_t<SixEq<2>, SCHEME, MIX, 16, 16, 1, COMPAS_NT2, COMPAS_MINB2>(L, st);
-    return launch_list_t<SixEq<3>, SCHEME, MIX, 8, 8, 8, COMPAS_NT3, COMPAS_MINB3>(L, st);
-}
-
-static int launch_list(int physics, int dim, int limiter, int precision, const ListArgs& L, cudaStream_t st) {
-    if (precision == 1) {
-        if (limiter == 6) return launch_list_s<6, true>(physics, dim, L, st);
-        return launch_list_s<5, true>(physics, dim, L, st);
-    }
-    if (limiter == 6) return launch_list_s<6, false>(physics, dim, L, st);
-    return launch_list_s<5, false>(physics, dim, L, st);
-}
-
 static int tile_count(int dim, const Grid& g) {
-    const int T = (dim == 2) ? 16 : 8;
+    const int T = (dim == 2) ? kTile2 : kTile3;
     const long long t = (long long)((g.n[0] + T - 1) / T) * ((g.n[1] + T - 1) / T) * ((g.n[2] + (dim == 2 ? 1 : T) - 1) /
                                                                                      (dim == 2 ? 1 : T));
     return (int)t;

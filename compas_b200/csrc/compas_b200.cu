@@ -15,6 +15,7 @@
 #include "compas_b200.h"
 #include "physics.cuh"
 #include "relax.cuh"
+#include "launch.h"
 #include "stage_kernel.cuh"
 
 namespace compas {
@@ -262,7 +263,6 @@ static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
     if (p->dim != 2 && p->dim != 3) return fail(COMPAS_B200_EARG, "dim must be 2 or 3");
     if (p->id_limiter != 5 && p->id_limiter != 6)
         return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.Scheme: this build runs WENO5 and WENO5B");
-    if (p->thinc) return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.THINC = 1 is not available in this build");
     if (p->id_riemann != 2) return fail(COMPAS_B200_EUNSUPPORTED, "Physics.RiemannSolver: this build runs HLLC");
     if (p->precision != 0 && p->precision != 1)
         return fail(COMPAS_B200_EARG, "precision must be 0 (plain FP64) or 1 (mixed)");
@@ -286,56 +286,38 @@ static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
     return COMPAS_B200_OK;
 }
 
-template <class M, int SCHEME, bool MIX, int TX, int TY, int TZ, int NT, int MINB>
-static int launch_stage_t(const StageArgs& a, cudaStream_t st) {
-    using T = TileShape<M, TX, TY, TZ, typename std::conditional<MIX, float, double>::type>;
-    auto kern = stage_kernel<M, SCHEME, MIX, TX, TY, TZ, NT, MINB>;
-    static bool attr_set = false;
-    if (!attr_set) {
-        CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
-        attr_set = true;
-    }
-    const long long tiles = (long long)((a.g.n[0] + TX - 1) / TX) * ((a.g.n[1] + TY - 1) / TY) *
-                            ((a.g.n[2] + TZ - 1) / TZ);
-    if (tiles > 0x7fffffffLL) return fail(COMPAS_B200_EARG, "box too large");
-    kern<<<(unsigned)tiles, NT, T::SMEM, st>>>(a);
-    CUDA_TRY(cudaGetLastError());
-    return COMPAS_B200_OK;
-}
-
-// Launch shape of the stage kernel: threads per CTA and CTAs per SM of the 3D (8^3 tile) and 2D
-// (16^2 tile) kernels. The register budget is set per SM sub-partition (16384 registers each, warps
-// dealt round-robin), so a CTA of 6 warps at 2 CTAs/SM gets 168 registers per thread.
-#ifndef COMPAS_NT3
-#define COMPAS_NT3 192
-#endif
-#ifndef COMPAS_MINB3
-#define COMPAS_MINB3 2
-#endif
-#ifndef COMPAS_NT2
-#define COMPAS_NT2 272
-#endif
-#ifndef COMPAS_MINB2
-#define COMPAS_MINB2 2
-#endif
-
-template <int SCHEME, bool MIX>
-static int launch_stage_s(const compas_b200_parm* p, const StageArgs& a, cudaStream_t st) {
-    if (p->physics == COMPAS_B200_FIVEEQS) {
-        if (p->dim == 2) return launch_stage_t<FiveEq<2>, SCHEME, MIX, 16, 16, 1, COMPAS_NT2, COMPAS_MINB2>(a, st);
-        return launch_stage_t<FiveEq<3>, SCHEME, MIX, 8, 8, 8, COMPAS_NT3, COMPAS_MINB3>(a, st);
-    }
-    if (p->dim == 2) return launch_stage_t<SixEq<2>, SCHEME, MIX, 16, 16, 1, COMPAS_NT2, COMPAS_MINB2>(a, st);
-    return launch_stage_t<SixEq<3>, SCHEME, MIX, 8, 8, 8, COMPAS_NT3, COMPAS_MINB3>(a, st);
+// The stage kernel of the model, dimension and scheme of p (kernels live in kern_*.cu).
+static KernelChoice choice_of(const compas_b200_parm* p) {
+    KernelChoice k;
+    k.limiter = p->id_limiter;
+    k.precision = p->precision;
+    k.thinc = p->thinc;
+    return k;
 }
 
 static int launch_stage(const compas_b200_parm* p, const StageArgs& a, cudaStream_t st) {
-    if (p->precision == 1) {
-        if (p->id_limiter == 6) return launch_stage_s<6, true>(p, a, st);
-        return launch_stage_s<5, true>(p, a, st);
-    }
-    if (p->id_limiter == 6) return launch_stage_s<6, false>(p, a, st);
-    return launch_stage_s<5, false>(p, a, st);
+    const int ts = (p->dim == 2) ? kTile2 : kTile3;
+    const long long tiles = (long long)((a.g.n[0] + ts - 1) / ts) * ((a.g.n[1] + ts - 1) / ts) *
+                            ((a.g.n[2] + (p->dim == 2 ? 1 : ts) - 1) / (p->dim == 2 ? 1 : ts));
+    if (tiles > 0x7fffffffLL) return fail(COMPAS_B200_EARG, "box too large");
+    const KernelChoice k = choice_of(p);
+    cudaError_t e;
+    if (p->physics == COMPAS_B200_FIVEEQS) e = (p->dim == 2) ? launch_stage_fiveeq2(k, a, st) : launch_stage_fiveeq3(k, a, st);
+    else e = (p->dim == 2) ? launch_stage_sixeq2(k, a, st) : launch_stage_sixeq3(k, a, st);
+    if (e != cudaSuccess) return fail(COMPAS_B200_ECUDA, std::string("stage kernel launch: ") + cudaGetErrorString(e));
+    return COMPAS_B200_OK;
+}
+
+static int launch_list(int physics, int dim, int limiter, int precision, const ListArgs& L, cudaStream_t st) {
+    KernelChoice k;
+    k.limiter = limiter;
+    k.precision = precision;
+    k.thinc = 0;
+    cudaError_t e;
+    if (physics == COMPAS_B200_FIVEEQS) e = (dim == 2) ? launch_list_fiveeq2(k, L, st) : launch_list_fiveeq3(k, L, st);
+    else e = (dim == 2) ? launch_list_sixeq2(k, L, st) : launch_list_sixeq3(k, L, st);
+    if (e != cudaSuccess) return fail(COMPAS_B200_ECUDA, std::string("box-list kernel launch: ") + cudaGetErrorString(e));
+    return COMPAS_B200_OK;
 }
 
 static int launch_fill(const compas_b200_parm* p, const compas_b200_geom* geo, double* U, cudaStream_t st) {
@@ -367,6 +349,10 @@ static StageArgs base_args(const compas_b200_parm* p, const compas_b200_geom* g)
     a.id_k = p->source_term;
     a.relax = (p->physics == COMPAS_B200_SIXEQS) ? p->relaxation : 0;
     a.trace = p->relax_trace;
+    a.thinc.use_normal = p->thinc_use_normal;
+    a.thinc.eps = p->thinc_eps;
+    a.thinc.beta = p->thinc_beta;
+    a.thinc.thr = p->thinc_normal_threshold;
     return a;
 }
 
@@ -972,6 +958,7 @@ int compas_b200_batch_add(compas_b200_batch* b, const compas_b200_parm* p, const
     if (rc) return rc;
     if (p->physics != b->physics || p->dim != b->dim || p->id_limiter != b->limiter || p->precision != b->precision)
         return fail(COMPAS_B200_EARG, "a batch holds cases of one model, dimension, scheme and precision");
+    if (p->thinc) return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.THINC = 1 runs on the level API, not in a batch");
     if (b->free_slots.empty()) return fail(COMPAS_B200_ENOMEM, "batch capacity reached");
     if (max_steps < 0) return fail(COMPAS_B200_EARG, "max_steps must be >= 0");
     cudaStream_t st = (cudaStream_t)stream;

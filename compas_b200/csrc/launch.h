@@ -1,0 +1,34 @@
+// Launchers of the stage kernels. The kernels are compiled in one translation unit per model and
+// dimension (kern_*.cu, built in parallel); the C-ABI translation unit calls them through these
+// declarations. Each returns the CUDA error of its launch.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace compas {
+
+struct StageArgs;
+struct ListArgs;
+
+// Variant of the stage kernel: FiniteVolume.Scheme (5 WENO5, 6 WENO5B), precision (0 FP64, 1 mixed),
+// FiniteVolume.THINC (single-box kernel only).
+struct KernelChoice {
+    int limiter;
+    int precision;
+    int thinc;
+};
+
+// Tile side of the stage kernels (cells per direction): 16^2 tiles in 2D, 8^3 in 3D.
+constexpr int kTile2 = 16;
+constexpr int kTile3 = 8;
+
+#define COMPAS_DECLARE_LAUNCHERS(name)                                                          \
+    cudaError_t launch_stage_##name(const KernelChoice& k, const StageArgs& a, cudaStream_t st); \
+    cudaError_t launch_list_##name(const KernelChoice& k, const ListArgs& L, cudaStream_t st);
+COMPAS_DECLARE_LAUNCHERS(fiveeq2)
+COMPAS_DECLARE_LAUNCHERS(fiveeq3)
+COMPAS_DECLARE_LAUNCHERS(sixeq2)
+COMPAS_DECLARE_LAUNCHERS(sixeq3)
+#undef COMPAS_DECLARE_LAUNCHERS
+
+}  // namespace compas

@@ -67,6 +67,25 @@ __device__ __forceinline__ double nasg_xi(double alpha, double alpha_rho, double
     return 1.0;
 }
 
+// NASG covolume factor from a phase density (THINC face states): 1 - b rho, 1 when b = 0
+// (include/EquationOfState_NASG.H:52-57).
+__device__ __forceinline__ double nasg_xi_rho(double rho, double b, unsigned int* err) {
+    if (b > 0.0) {
+        const double xi = 1.0 - b * rho;
+        if (!(xi > 0.0)) flag_error(err, COMPAS_B200_ERR_COVOLUME);
+        return xi;
+    }
+    return 1.0;
+}
+
+// FiniteVolume.THINC parameters (include/Operators_FV/FiniteVolume_Parameter.H:34-38, 175-180).
+struct Thinc {
+    int use_normal;   // FiniteVolume.THINC.UseNormal
+    double eps;       // FiniteVolume.THINC.EPS
+    double beta;      // FiniteVolume.THINC.Beta
+    double thr;       // FiniteVolume.THINC.NormalThreshold
+};
+
 // v[d] for a run-time direction d without indexing a per-thread array by a run-time value (which
 // would place the array in local memory).
 template <int D>
@@ -150,6 +169,33 @@ struct FiveEq {
         for (int d = 0; d < D; ++d) U[2 + d] = rho * W[2 + d];
         U[IE] = rho_e + (0.5 * rho) * ksum<D>(W + 2);
         U[IA] = alpha1;
+    }
+
+    // THINC side of a face: the face state Uf (MUSCL-minmod) with its volume fraction replaced by the
+    // THINC value af; phase densities, velocity and pressure are kept, masses, momentum and energy
+    // rebuilt (Reconstruct_State_From_VolumeFraction,
+    // include/Operators_Compressible5Eq/FVM_Reconstruction2Face_Conservative_THINC_K_Compressible5Eq.H:15-63).
+    __device__ static __forceinline__ void thinc_rebuild(double* Uo, const double* Uf, double af, const Eos& e,
+                                                         unsigned int* err) {
+        double W[N];
+        cons2prim(W, Uf, e, err);
+        const double al = W[IA], p = W[IE];
+        const double rho1 = W[0] / al;
+        const double rho2 = W[1] / (1.0 - al);
+        const double m1 = af * rho1;
+        const double m2 = (1.0 - af) * rho2;
+        const double rr = m1 + m2;
+        const double K = 0.5 * ksum<D>(W + 2);
+        const double r1e1 = (e.C1 > 0.0) ? nasg_xi_rho(rho1, e.C1, err) * (e.A1 * p + e.B1) + rho1 * e.D1
+                                         : e.A1 * p + e.B1 + rho1 * e.D1;
+        const double r2e2 = (e.C2 > 0.0) ? nasg_xi_rho(rho2, e.C2, err) * (e.A2 * p + e.B2) + rho2 * e.D2
+                                         : e.A2 * p + e.B2 + rho2 * e.D2;
+        Uo[0] = m1;
+        Uo[1] = m2;
+#pragma unroll
+        for (int c = 0; c < D; ++c) Uo[2 + c] = W[2 + c] * rr;
+        Uo[IE] = K * rr + r1e1 * af + r2e2 * (1.0 - af);
+        Uo[IA] = af;
     }
 
     // Mixture sound speed; source_term 0 (K = 0) or 1 (Wood).
@@ -418,6 +464,34 @@ struct SixEq {
         U[IE1] = a1r1e1 + (0.5 * a1r1) * k;
         U[IE2] = a2r2e2 + (0.5 * a2r2) * k;
         U[IA] = alpha1;
+    }
+
+    // THINC side of a face (include/Operators_Compressible6Eq/FVM_Reconstruction2Face_Conservative_THINC_K_Compressible6Eq.H:14-62):
+    // phase densities, velocity and phase pressures of the face state are kept.
+    __device__ static __forceinline__ void thinc_rebuild(double* Uo, const double* Uf, double af, const Eos& e,
+                                                         unsigned int* err) {
+        double W[N];
+        cons2prim(W, Uf, e, err);
+        const double al = W[IA];
+        const double rho1 = W[0] / al;
+        const double rho2 = W[1] / (1.0 - al);
+        const double m1 = af * rho1;
+        const double m2 = (1.0 - af) * rho2;
+        const double rr = m1 + m2;
+        const double p1 = W[IE1] / al;
+        const double p2 = W[IE2] / (1.0 - al);
+        const double K = 0.5 * ksum<D>(W + 2);
+        const double r1e1 = (e.C1 > 0.0) ? nasg_xi_rho(rho1, e.C1, err) * (e.A1 * p1 + e.B1) + rho1 * e.D1
+                                         : e.A1 * p1 + e.B1 + rho1 * e.D1;
+        const double r2e2 = (e.C2 > 0.0) ? nasg_xi_rho(rho2, e.C2, err) * (e.A2 * p2 + e.B2) + rho2 * e.D2
+                                         : e.A2 * p2 + e.B2 + rho2 * e.D2;
+        Uo[0] = m1;
+        Uo[1] = m2;
+#pragma unroll
+        for (int c = 0; c < D; ++c) Uo[2 + c] = W[2 + c] * rr;
+        Uo[IE1] = K * m1 + r1e1 * af;
+        Uo[IE2] = K * m2 + r2e2 * (1.0 - af);
+        Uo[IA] = af;
     }
 
     // Frozen mixture sound speed: rho c^2 = sum alpha_k rho_k c_k^2.

@@ -59,7 +59,14 @@ struct StageArgs {
     int id_k;
     int relax;
     double trace;
+    Thinc thinc;               // used by the THINC kernels only
 };
+
+}  // namespace compas
+
+#include "thinc.cuh"
+
+namespace compas {
 
 template <class M, int TX, int TY, int TZ, class PT = double>
 struct TileShape {
@@ -89,8 +96,9 @@ __device__ __forceinline__ void load_cons(double* U, const double* base, const G
 // primitives are recovered in FP64 (pressure from total energy) and kept in shared memory as FP32,
 // the reconstruction runs in FP32, the Riemann solver, divergence, stage accumulation and
 // relaxation in FP64.
+// TH: THINC interface reconstruction on top of the scheme (FiniteVolume.THINC = 1).
 // The work of one CTA on tile `tile` of the box described by `a` (tiles numbered x fastest).
-template <class M, int SCHEME, bool MIX, int TX, int TY, int TZ, int NT>
+template <class M, int SCHEME, bool MIX, bool TH, int TX, int TY, int TZ, int NT>
 __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double* smem_d) {
     static_assert(TX == TY && (M::D == 2 ? TZ == 1 : TZ == TX), "tiles are cubes (squares in 2D)");
     using PT = typename std::conditional<MIX, float, double>::type;
@@ -216,57 +224,68 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
             constexpr int NB0 = (SCHEME == 6) ? 2 : 0;        // first plainly reconstructed component
             constexpr int NB1 = (SCHEME == 6) ? M::IA : N;    // one past the last
             double F[N], fnc[NC], cm;
+            bool thinc_face = false;
+            if constexpr (TH)
+                thinc_face = thinc_face_states<M, PT>(a.thinc, a.Us, g, a.e, smem, off + 1, str + 1, d, gi, gj, gk, UL,
+                                                      UR, err);
             if constexpr (!MIX) {
-                if constexpr (SCHEME == 6) {
-                    double r1[6], r2[6], al[6];
+                if (!thinc_face) {
+                    if constexpr (SCHEME == 6) {
+                        double r1[6], r2[6], al[6];
 #pragma unroll
-                    for (int s = 0; s < 6; ++s) {
-                        r1[s] = smem[off[s]];
-                        r2[s] = smem[off[s] + str[s]];
-                        al[s] = smem[off[s] + M::IA * str[s]];
+                        for (int s = 0; s < 6; ++s) {
+                            r1[s] = smem[off[s]];
+                            r2[s] = smem[off[s] + str[s]];
+                            al[s] = smem[off[s] + M::IA * str[s]];
+                        }
+                        weno5b_masses(r1, r2, al, 1, WfL[0], WfL[1], WfL[M::IA]);
+                        weno5b_masses(r1 + 1, r2 + 1, al + 1, -1, WfR[0], WfR[1], WfR[M::IA]);
                     }
-                    weno5b_masses(r1, r2, al, 1, WfL[0], WfL[1], WfL[M::IA]);
-                    weno5b_masses(r1 + 1, r2 + 1, al + 1, -1, WfR[0], WfR[1], WfR[M::IA]);
-                }
 #pragma unroll
-                for (int n = NB0; n < NB1; ++n) {
-                    const double w0 = smem[off[0] + n * str[0]], w1 = smem[off[1] + n * str[1]];
-                    const double w2 = smem[off[2] + n * str[2]], w3 = smem[off[3] + n * str[3]];
-                    const double w4 = smem[off[4] + n * str[4]], w5 = smem[off[5] + n * str[5]];
-                    WfL[n] = weno5(w0, w1, w2, w3, w4, 1);
-                    WfR[n] = weno5(w1, w2, w3, w4, w5, -1);
+                    for (int n = NB0; n < NB1; ++n) {
+                        const double w0 = smem[off[0] + n * str[0]], w1 = smem[off[1] + n * str[1]];
+                        const double w2 = smem[off[2] + n * str[2]], w3 = smem[off[3] + n * str[3]];
+                        const double w4 = smem[off[4] + n * str[4]], w5 = smem[off[5] + n * str[5]];
+                        WfL[n] = weno5(w0, w1, w2, w3, w4, 1);
+                        WfR[n] = weno5(w1, w2, w3, w4, w5, -1);
+                    }
+                    M::prim2cons(UL, WfL, a.e, err);
+                    M::prim2cons(UR, WfR, a.e, err);
                 }
-                M::prim2cons(UL, WfL, a.e, err);
-                M::prim2cons(UR, WfR, a.e, err);
                 M::hllc(F, fnc, cm, UL, UR, a.e, d, a.id_k, err);
             } else {
                 float wL[N], wR[N];
-                if constexpr (SCHEME == 6) {
-                    float r1[6], r2[6], al[6];
+                if (thinc_face) {
+                    M::cons2prim_f32(wL, UL, a.e);
+                    M::cons2prim_f32(wR, UR, a.e);
+                } else {
+                    if constexpr (SCHEME == 6) {
+                        float r1[6], r2[6], al[6];
 #pragma unroll
-                    for (int s = 0; s < 6; ++s) {
-                        r1[s] = smem[off[s]];
-                        r2[s] = smem[off[s] + str[s]];
-                        al[s] = smem[off[s] + M::IA * str[s]];
+                        for (int s = 0; s < 6; ++s) {
+                            r1[s] = smem[off[s]];
+                            r2[s] = smem[off[s] + str[s]];
+                            al[s] = smem[off[s] + M::IA * str[s]];
+                        }
+                        weno5b_masses_f32(r1, r2, al, 1, wL[0], wL[1], wL[M::IA]);
+                        weno5b_masses_f32(r1 + 1, r2 + 1, al + 1, -1, wR[0], wR[1], wR[M::IA]);
                     }
-                    weno5b_masses_f32(r1, r2, al, 1, wL[0], wL[1], wL[M::IA]);
-                    weno5b_masses_f32(r1 + 1, r2 + 1, al + 1, -1, wR[0], wR[1], wR[M::IA]);
-                }
 #pragma unroll
-                for (int n = NB0; n < NB1; ++n) {
-                    const float w0 = smem[off[0] + n * str[0]], w1 = smem[off[1] + n * str[1]];
-                    const float w2 = smem[off[2] + n * str[2]], w3 = smem[off[3] + n * str[3]];
-                    const float w4 = smem[off[4] + n * str[4]], w5 = smem[off[5] + n * str[5]];
-                    wL[n] = weno5_f32(w0, w1, w2, w3, w4, 1);
-                    wR[n] = weno5_f32(w1, w2, w3, w4, w5, -1);
-                }
+                    for (int n = NB0; n < NB1; ++n) {
+                        const float w0 = smem[off[0] + n * str[0]], w1 = smem[off[1] + n * str[1]];
+                        const float w2 = smem[off[2] + n * str[2]], w3 = smem[off[3] + n * str[3]];
+                        const float w4 = smem[off[4] + n * str[4]], w5 = smem[off[5] + n * str[5]];
+                        wL[n] = weno5_f32(w0, w1, w2, w3, w4, 1);
+                        wR[n] = weno5_f32(w1, w2, w3, w4, w5, -1);
+                    }
 #pragma unroll
-                for (int n = 0; n < N; ++n) {
-                    WfL[n] = wL[n];
-                    WfR[n] = wR[n];
+                    for (int n = 0; n < N; ++n) {
+                        WfL[n] = wL[n];
+                        WfR[n] = wR[n];
+                    }
+                    M::prim2cons(UL, WfL, a.e, err);
+                    M::prim2cons(UR, WfR, a.e, err);
                 }
-                M::prim2cons(UL, WfL, a.e, err);
-                M::prim2cons(UR, WfR, a.e, err);
                 float cmf;
                 if constexpr (M::NC == 1)
                     fiveeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, a.e, d, a.id_k);
@@ -405,11 +424,11 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
 }
 
 // One box: one CTA per tile.
-template <class M, int SCHEME, bool MIX, int TX, int TY, int TZ, int NT, int MINB>
+template <class M, int SCHEME, bool MIX, bool TH, int TX, int TY, int TZ, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
     if (a.done && *a.done) return;
     extern __shared__ double smem_d[];
-    stage_tile<M, SCHEME, MIX, TX, TY, TZ, NT>(a, blockIdx.x, smem_d);
+    stage_tile<M, SCHEME, MIX, TH, TX, TY, TZ, NT>(a, blockIdx.x, smem_d);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -476,7 +495,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_list_kernel(ListArgs L) {
         a.relax = B.relax;
         a.trace = B.trace;
         __syncthreads();  // the previous tile's readers of shared memory are done
-        stage_tile<M, SCHEME, MIX, TX, TY, TZ, NT>(a, w - L.tile_off[b], smem_d);
+        stage_tile<M, SCHEME, MIX, false, TX, TY, TZ, NT>(a, w - L.tile_off[b], smem_d);
     }
 }
 

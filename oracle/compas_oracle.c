@@ -16,6 +16,10 @@
  *   WENO5                include/Operators_FV/WENO5.H:12-75, Reconstruction2Face_WENO.H
  *   face reconstruction  include/Operators_Compressible5Eq/FVM_Reconstruction2Face_Conservative_WENO5_D_Compressible5Eq.H,
  *                        FVM_Reconstruction2FaceLR_Conservative_WENO5_{D,K}_Compressible5Eq.H (6Eq alike)
+ *   THINC                include/Operators_Compressible5Eq/FVM_Reconstruction2Face_Conservative_THINC_K_Compressible5Eq.H:15-190,
+ *                        include/Operators_Compressible6Eq/FVM_Reconstruction2Face_Conservative_THINC_K_Compressible6Eq.H:14-188,
+ *                        include/Operators_FV/Reconstruction2Face_THINC_D.H, Reconstruction2Face_MUSCL_D.H, Limiter_Minmod.H,
+ *                        include/Operators_FD/FDM_Normal_{X,Y,Z}FaceFromCenter_{K,D}.H, FDM_Gradient*FaceFromCenter_D.H
  *   HLLC                 include/Physics_Compressible5Eq/Riemann_HLLC_Compressible5Eq.H:16-194,
  *                        include/Physics_Compressible6Eq/Riemann_HLLC_Compressible6Eq.H:16-255
  *   face functor         include/Operators_Compressible5Eq/FVM_Conservative2FluxHyperbolic_K_Compressible5Eq.H:15-170,
@@ -697,6 +701,148 @@ int cmp_fill_ghosts(const cmp_case* c, double* U) {
     return 0;
 }
 
+/* ---- THINC ------------------------------------------------------------------------------------- */
+static double signnz(double x) { return x > 0.0 ? 1.0 : -1.0; }
+
+/* Test control (not part of the reference algorithm): when on, every THINC face value is moved up
+ * by one ulp. Tests use it to measure how strongly a case amplifies a last-bit difference in
+ * exp / log / tanh between two math libraries, which bounds what a correct implementation on
+ * another library can be held to. */
+static int g_thinc_ulp = 0;
+void cmp_set_thinc_ulp(int on) { g_thinc_ulp = on; }
+
+/* Reconstruction2Face_THINC_D: id_face 1 = high face of the cell, 0 = low face */
+static double thinc_face_alpha(double beta, double sigma, double abar, int id_face) {
+    const double a = (id_face == 1) ? 0.0 : 1.0;
+    const double b = (id_face == 1) ? 1.0 : -1.0;
+    const double arg_ln = (exp(2.0 * beta * abar) - 1.0) / (exp(2.0 * beta) - exp(2.0 * beta * abar));
+    const double cc = 0.5 / beta * log(arg_ln);
+    const double arg = beta * (a + 0.5 * b * (sigma + 1.0) + cc);
+    const double af = 0.5 * (1.0 + tanh(arg));
+    const double r = dmin(1.0, dmax(0.0, af));
+    return g_thinc_ulp ? nextafter(r, 2.0) : r;
+}
+
+/* Reconstruction2Face_MUSCL_D with the minmod slope (ID_Limiter 1) */
+static double muscl_minmod(double fm, double fc, double fp, double dx, int id_face) {
+    const double sm = (fc - fm) / dx;
+    const double sp = (fp - fc) / dx;
+    const double slope = dmin(dmax(sm, 0.0), dmax(sp, 0.0)) + dmax(dmin(sm, 0.0), dmin(sp, 0.0));
+    return fc + (double)id_face * 0.5 * slope * dx;
+}
+
+/* Interpolation2Edge_Linear_D */
+static double edge4(double c, double a1, double a2, double a12) { return 0.25 * c + 0.25 * a1 + 0.25 * a2 + 0.25 * a12; }
+
+/* Component d of FDM_Normal_{X,Y,Z}FaceFromCenter at face (i,j,k) of direction d, written out per
+ * direction as the reference does (the argument order of the edge averages differs per direction). */
+static double face_normal_d(const Model* m, const Geo* g, const double* U, int i, int j, int k, int d) {
+    const double* A = U + (long long)m->IA * g->S;
+#define F(ii, jj, kk) A[at(g, (ii), (jj), (kk))]
+    const double* dx = m->c->dx;
+    double n[3] = {0.0, 0.0, 0.0};
+    const double fc = F(i, j, k);
+    if (d == 0) {
+        const double xm = F(i - 1, j, k);
+        n[0] = (fc - xm) / dx[0];
+        n[1] = (edge4(fc, xm, F(i, j + 1, k), F(i - 1, j + 1, k)) - edge4(fc, xm, F(i, j - 1, k), F(i - 1, j - 1, k))) / dx[1];
+        if (m->D == 3)
+            n[2] = (edge4(fc, xm, F(i, j, k + 1), F(i - 1, j, k + 1)) - edge4(fc, xm, F(i, j, k - 1), F(i - 1, j, k - 1))) / dx[2];
+    } else if (d == 1) {
+        const double ym = F(i, j - 1, k);
+        n[0] = (edge4(fc, F(i + 1, j, k), ym, F(i + 1, j - 1, k)) - edge4(fc, F(i - 1, j, k), ym, F(i - 1, j - 1, k))) / dx[0];
+        n[1] = (fc - ym) / dx[1];
+        if (m->D == 3)
+            n[2] = (edge4(fc, ym, F(i, j, k + 1), F(i, j - 1, k + 1)) - edge4(fc, ym, F(i, j, k - 1), F(i, j - 1, k - 1))) / dx[2];
+    } else {
+        const double zm = F(i, j, k - 1);
+        n[0] = (edge4(fc, F(i + 1, j, k), zm, F(i + 1, j, k - 1)) - edge4(fc, F(i - 1, j, k), zm, F(i - 1, j, k - 1))) / dx[0];
+        n[1] = (edge4(fc, F(i, j + 1, k), zm, F(i, j + 1, k - 1)) - edge4(fc, F(i, j - 1, k), zm, F(i, j - 1, k - 1))) / dx[1];
+        n[2] = (fc - zm) / dx[2];
+    }
+#undef F
+    double sum = 0.0;
+    for (int t = 0; t < m->D; ++t) sum += n[t] * n[t];
+    if (sum == 0.0) return 0.0;
+    return n[d] / sqrt(sum);
+}
+
+static double xi_rho(double rho, double b) { return (b > 0.0) ? 1.0 - b * rho : 1.0; }
+
+/* Reconstruct_State_From_VolumeFraction (5Eq :15-63, 6Eq :14-62) */
+static void thinc_rebuild(const Model* m, const double* Uf, double af, double* Uo) {
+    const cmp_case* c = m->c;
+    double W[MAXN];
+    c2p(m, Uf, W);
+    const double al = W[m->IA];
+    const double rho1 = W[0] / al;
+    const double rho2 = W[1] / (1.0 - al);
+    const double m1 = af * rho1;
+    const double m2 = (1.0 - af) * rho2;
+    const double rr = m1 + m2;
+    const double K = 0.5 * ksum(W + 2, m->D);
+    double p1, p2;
+    if (!m->six) {
+        p1 = W[m->IE];
+        p2 = W[m->IE];
+    } else {
+        p1 = W[m->IE1] / al;
+        p2 = W[m->IE2] / (1.0 - al);
+    }
+    double r1e1 = c->A1 * p1 + c->B1 + rho1 * c->D1;
+    double r2e2 = c->A2 * p2 + c->B2 + rho2 * c->D2;
+    if (c->C1 > 0.0) r1e1 = xi_rho(rho1, c->C1) * (c->A1 * p1 + c->B1) + rho1 * c->D1;
+    if (c->C2 > 0.0) r2e2 = xi_rho(rho2, c->C2) * (c->A2 * p2 + c->B2) + rho2 * c->D2;
+    Uo[0] = m1;
+    Uo[1] = m2;
+    for (int d = 0; d < m->D; ++d) Uo[2 + d] = W[2 + d] * rr;
+    if (!m->six) {
+        Uo[m->IE] = K * rr + r1e1 * af + r2e2 * (1.0 - af);
+    } else {
+        Uo[m->IE1] = K * m1 + r1e1 * af;
+        Uo[m->IE2] = K * m2 + r2e2 * (1.0 - af);
+    }
+    Uo[m->IA] = af;
+}
+
+/* FVM_Reconstruction2Face_Conservative_THINC_K: C[0..3] are the cells i-2 .. i+1 of the face (i,j,k)
+ * of direction d. Returns 0 when the face keeps the base scheme. */
+static int thinc_states(const Model* m, const Geo* g, const double* U, int i, int j, int k, int d, double C[][MAXN],
+                        double* UL, double* UR) {
+    const cmp_case* c = m->c;
+    const int N = m->N, IA = m->IA;
+    const double nd = face_normal_d(m, g, U, i, j, k, d);
+    const double amm = C[0][IA], am = C[1][IA], ac = C[2][IA], ap = C[3][IA];
+    const int grad_l = (ac - am) * (am - amm) > 0.0;
+    const int grad_r = (ap - ac) * (ac - am) > 0.0;
+    const int sym = (amm == ap) && (am == ac) && (am != amm);
+    const int gate = (!c->thinc_use_normal) || (fabs(nd) > c->thinc_normal_threshold);
+    const double eps = c->thinc_eps;
+    const int int_l = (am > eps && am < 1.0 - eps) && (grad_l || sym) && gate;
+    const int int_r = (ac > eps && ac < 1.0 - eps) && (grad_r || sym) && gate;
+    if (!(int_l || int_r)) return 0;
+    double P[4][MAXN], WL[MAXN], WR[MAXN];
+    for (int s = 0; s < 4; ++s) c2p(m, C[s], P[s]);
+    const double dxd = c->dx[d];
+    for (int n = 0; n < N; ++n) {
+        WL[n] = muscl_minmod(P[0][n], P[1][n], P[2][n], dxd, 1);
+        WR[n] = muscl_minmod(P[1][n], P[2][n], P[3][n], dxd, -1);
+    }
+    p2c(m, WL, UL);
+    p2c(m, WR, UR);
+    const double beta = c->thinc_use_normal ? (c->thinc_beta * fabs(nd) + 0.01) : c->thinc_beta;
+    double Uf[MAXN];
+    if (int_l) {
+        memcpy(Uf, UL, sizeof(double) * N);
+        thinc_rebuild(m, Uf, thinc_face_alpha(beta, signnz(ac - amm), am, 1), UL);
+    }
+    if (int_r) {
+        memcpy(Uf, UR, sizeof(double) * N);
+        thinc_rebuild(m, Uf, thinc_face_alpha(beta, signnz(ap - am), ac, 0), UR);
+    }
+    return 1;
+}
+
 /* face (i,j,k) of direction d lies between cells (i,j,k) - e_d and (i,j,k) */
 static void face_flux(const Model* m, const Geo* g, const double* U, int i, int j, int k, int d, double* F,
                       double* fnc, double* cmax) {
@@ -708,6 +854,10 @@ static void face_flux(const Model* m, const Geo* g, const double* U, int i, int 
         load(m, g, U, ii, jj, kk, C[s]);
     }
     /* left state: stencil i-3..i+1 centred at i-1, right face; right state: i-2..i+2 centred at i, left face */
+    if (m->c->thinc && thinc_states(m, g, U, i, j, k, d, C + 1, UL, UR)) {
+        hllc(m, UL, UR, d, F, fnc, cmax);
+        return;
+    }
     const int bounded = (m->c->id_limiter == 6);
     const int n0 = bounded ? 2 : 0, n1 = bounded ? m->IA : N;
     for (int s = 0; s < 5; ++s) c2p(m, C[s], P[s]);

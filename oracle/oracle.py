@@ -119,39 +119,54 @@ def case_from(parm, geom) -> Case:
 
 
 class Oracle:
-    def __init__(self, kind: str, parm, geom):
+    def __init__(self, kind: str, parm, geom, thinc_ulp: bool = False):
+        """thinc_ulp (port only): move every THINC face value up by one ulp, to measure how strongly
+        a case amplifies last-bit differences of exp/log/tanh between math libraries."""
         self.kind = kind
         self.case = case_from(parm, geom)
         self.lib = load(kind, parm.physics, parm.dim)
+        self.thinc_ulp = bool(thinc_ulp)
+        if self.thinc_ulp and kind != "port":
+            raise ValueError("the one-ulp THINC control exists in the port only")
+        if kind == "port":
+            self.lib.cmp_set_thinc_ulp.argtypes = [ctypes.c_int]
+            self.lib.cmp_set_thinc_ulp.restype = None
 
     def _call(self, rc):
         if rc < 0:
             raise RuntimeError(f"oracle ({self.kind}) failed: {rc}")
         return rc
 
+    @property
+    def _c(self):
+        # the one-ulp control is process-wide in the port: set it for this instance before each call
+        if self.kind == "port":
+            self.lib.cmp_set_thinc_ulp(int(self.thinc_ulp))
+        return ctypes.byref(self.case)
+
     def fill_ghosts(self, U: np.ndarray) -> None:
         assert U.flags.c_contiguous and U.dtype == np.float64
-        self._call(self.lib.cmp_fill_ghosts(ctypes.byref(self.case), U.ctypes.data))
+        self._call(self.lib.cmp_fill_ghosts(self._c, U.ctypes.data))
 
     def compute_dudt(self, U: np.ndarray):
         dU = np.zeros_like(U)
         cm = ctypes.c_double()
-        self._call(self.lib.cmp_compute_dudt(ctypes.byref(self.case), U.ctypes.data, dU.ctypes.data,
+        self._call(self.lib.cmp_compute_dudt(self._c, U.ctypes.data, dU.ctypes.data,
                                              ctypes.byref(cm)))
         return dU, cm.value
 
     def relax(self, U: np.ndarray) -> None:
-        self._call(self.lib.cmp_relax(ctypes.byref(self.case), U.ctypes.data))
+        self._call(self.lib.cmp_relax(self._c, U.ctypes.data))
 
     def rk3_step(self, U: np.ndarray, dt: float) -> float:
         cm = ctypes.c_double()
-        self._call(self.lib.cmp_rk3_step(ctypes.byref(self.case), U.ctypes.data, dt, ctypes.byref(cm)))
+        self._call(self.lib.cmp_rk3_step(self._c, U.ctypes.data, dt, ctypes.byref(cm)))
         return cm.value
 
     def advance(self, U: np.ndarray, nsteps: int, stop_time: float = 1e300, t0: float = 0.0):
         t = ctypes.c_double(t0)
         dts = np.zeros(max(nsteps, 1), dtype=np.float64)
-        n = self._call(self.lib.cmp_advance(ctypes.byref(self.case), U.ctypes.data, nsteps, stop_time,
+        n = self._call(self.lib.cmp_advance(self._c, U.ctypes.data, nsteps, stop_time,
                                             ctypes.byref(t), dts.ctypes.data))
         return t.value, dts[:n]
 

@@ -21,17 +21,22 @@ from oracle.oracle import Oracle  # noqa: E402
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 CASES = {
-    # name: (case function, kwargs, steps)
+    # name: (case function, kwargs, steps[, extra inputs keys])
     "disc_5eq_2d_32": (cases.advected_disc, dict(n=32), 12),
     "bubble_5eq_2d_29x17": (cases.shock_bubble, dict(nx=29, ny=17, scheme="WENO5"), 6),
     "droplet_6eq_3d_12": (cases.shock_droplet, dict(n=12), 3),
     "bubble_weno5b_5eq_2d_31x19": (cases.shock_bubble, dict(nx=31, ny=19, scheme="WENO5B"), 6),
+    "disc_thinc_5eq_2d_32": (cases.advected_disc, dict(n=32), 12, {"FiniteVolume.THINC": "1"}),
+    "bubble_thinc_weno5b_5eq_2d_31x19": (cases.shock_bubble, dict(nx=31, ny=19, scheme="WENO5B"), 6,
+                                         {"FiniteVolume.THINC": "1", "FiniteVolume.THINC.UseNormal": "0"}),
+    "droplet_thinc_6eq_3d_12": (cases.shock_droplet, dict(n=12), 3, {"FiniteVolume.THINC": "1"}),
 }
 
 
 def make(name):
-    fn, kw, steps = CASES[name]
+    fn, kw, steps = CASES[name][:3]
     phys, dim, inputs, geom, U = fn(**kw)
+    inputs = dict(inputs, **(CASES[name][3] if len(CASES[name]) > 3 else {}))
     p = cb.make_parm(phys, dim, inputs)
     g = cb.make_geom(**geom)
     out = U.copy()
@@ -43,6 +48,6 @@ def make(name):
 
 
 if __name__ == "__main__":
-    for n in CASES:
+    for n in (sys.argv[1:] or CASES):
         make(n)
         print("wrote", n)

@@ -33,13 +33,18 @@ def test_port_matches_reference_golden(path):
 
 
 @pytest.mark.skipif(not have_ref(cb.FIVEEQS, 2), reason="reference-header oracle not built here")
-@pytest.mark.parametrize("case,kw,steps", [
-    (cases.advected_disc, dict(n=40), 8),
-    (cases.shock_bubble, dict(nx=33, ny=21, scheme="WENO5"), 8),
-    (cases.shock_droplet, dict(n=14), 2),
+@pytest.mark.parametrize("case,kw,steps,extra", [
+    (cases.advected_disc, dict(n=40), 8, {}),
+    (cases.shock_bubble, dict(nx=33, ny=21, scheme="WENO5"), 8, {}),
+    (cases.shock_droplet, dict(n=14), 2, {}),
+    (cases.advected_disc, dict(n=40), 8, {"FiniteVolume.THINC": "1"}),
+    (cases.advected_disc, dict(n=36), 8, {"FiniteVolume.THINC": "1", "FiniteVolume.THINC.UseNormal": "0"}),
+    (cases.shock_bubble, dict(nx=33, ny=21, scheme="WENO5B"), 8, {"FiniteVolume.THINC": "1"}),
+    (cases.shock_droplet, dict(n=14), 2, {"FiniteVolume.THINC": "1"}),
 ])
-def test_port_matches_reference_build(case, kw, steps):
+def test_port_matches_reference_build(case, kw, steps, extra):
     phys, dim, inputs, geom, U = case(**kw)
+    inputs = dict(inputs, **extra)
     p, g = _parm_geom(phys, dim, inputs, geom)
     a, b = U.copy(), U.copy()
     ta, da = Oracle("reference", p, g).advance(a, steps)

@@ -65,6 +65,14 @@ class Parm(ctypes.Structure):
         ("cfl", ctypes.c_double),
         ("change_limiter", ctypes.c_int),
         ("precision", ctypes.c_int),
+        ("phase_field", ctypes.c_int),
+        ("pf_mechanism", ctypes.c_int),
+        ("pf_explicit_rc", ctypes.c_int),
+        ("pf_lambda", ctypes.c_double), ("pf_eta", ctypes.c_double),
+        ("pf_eta_factor", ctypes.c_double), ("pf_eta_multiplier", ctypes.c_double),
+        ("pf_cfl", ctypes.c_double),
+        ("pf_max_step", ctypes.c_int),
+        ("pf_tol_rel", ctypes.c_double),
     ]
 
 
@@ -114,6 +122,17 @@ _SIGS = {
                                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_uint)]),
     "compas_b200_level_dts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
     "compas_b200_level_launches": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "compas_b200_level_pf_substeps": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "compas_b200_pf_grad_q": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_void_p,
+                                             ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_void_p]),
+    "compas_b200_pf_compute_dUdt": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_void_p,
+                                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "compas_b200_pf_rk3_stage": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_int,
+                                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                ctypes.c_void_p]),
     "compas_b200_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                 ctypes.POINTER(ctypes.c_void_p)]),
     "compas_b200_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
@@ -240,6 +259,34 @@ def ThirdOrderSSPRK_step_noalloc(p: Parm, g: Geom, U, dt: float, cmax=None, err=
                                               _ptr(err), _stream_ptr(stream)))
 
 
+def PhaseField_GradQPF(p: Parm, g: Geom, U, dt: float, gq, stream=None) -> np.ndarray:
+    """Mechanism evolution over dt and the face gradients of the regularisation potential Q into the
+    device arrays gq[d] (PhaseFieldMechanism_Evolve + PhaseField_GradQPF,
+    source/Class_Compressible_PhaseField.cpp:596-711, :2132-2401). Returns the info vector
+    (max|u|, mobility, eta, mechanism sub-steps, solver iterations, max|grad Q|, relative residual)."""
+    info = (ctypes.c_double * 7)()
+    ptrs = [_ptr(gq[d]) if d < len(gq) else None for d in range(3)]
+    _check(lib().compas_b200_pf_grad_q(ctypes.byref(p), ctypes.byref(g), _ptr(U), float(dt), ptrs[0], ptrs[1],
+                                       ptrs[2], info, _stream_ptr(stream)))
+    return np.array(info[:])
+
+
+def PhaseField_compute_dUdt_FV(p: Parm, g: Geom, U, dUdt, gq, err=None, stream=None) -> None:
+    """Phase-Field right-hand side (source/Class_Compressible_PhaseField.cpp:950-1004)."""
+    ptrs = [_ptr(gq[d]) if d < len(gq) else None for d in range(3)]
+    _check(lib().compas_b200_pf_compute_dUdt(ctypes.byref(p), ctypes.byref(g), _ptr(U), _ptr(dUdt), ptrs[0],
+                                             ptrs[1], ptrs[2], _ptr(err), _stream_ptr(stream)))
+
+
+def PhaseField_ThirdOrderSSPRK_stage(p: Parm, g: Geom, stage: int, Us, Uold, Unew, dt_dev, gq, err=None,
+                                     stream=None) -> None:
+    """One stage of PhaseField_ThirdOrderSSPRK (source/Class_Compressible_PhaseField.cpp:2619-2752)."""
+    ptrs = [_ptr(gq[d]) if d < len(gq) else None for d in range(3)]
+    _check(lib().compas_b200_pf_rk3_stage(ctypes.byref(p), ctypes.byref(g), int(stage), _ptr(Us), _ptr(Uold),
+                                          _ptr(Unew), _ptr(dt_dev), ptrs[0], ptrs[1], ptrs[2], _ptr(err),
+                                          _stream_ptr(stream)))
+
+
 def Relaxation(p: Parm, g: Geom, U, err=None, stream=None) -> None:
     """SIXEQS pressure relaxation in place (source/Class_Compressible6Eq_PhaseField.cpp:437-474)."""
     _check(lib().compas_b200_relaxation(ctypes.byref(p), ctypes.byref(g), _ptr(U), _ptr(err), _stream_ptr(stream)))
@@ -329,6 +376,10 @@ class Level:
 
     def launches(self) -> int:
         return int(lib().compas_b200_level_launches(self._h))
+
+    def pf_substeps(self) -> int:
+        """Phase-Field sub-steps taken so far (PhaseField.phase_field = 1)."""
+        return int(lib().compas_b200_level_pf_substeps(self._h))
 
 
 @dataclass

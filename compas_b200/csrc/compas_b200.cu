@@ -3,6 +3,7 @@
 // runs on the device (no host synchronisation inside a run, CUDA-graph replay per step).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -16,6 +17,7 @@
 #include "physics.cuh"
 #include "relax.cuh"
 #include "launch.h"
+#include "phasefield.h"
 #include "stage_kernel.cuh"
 
 namespace compas {
@@ -264,6 +266,12 @@ static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
     if (p->id_limiter != 5 && p->id_limiter != 6)
         return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.Scheme: this build runs WENO5 and WENO5B");
     if (p->id_riemann != 2) return fail(COMPAS_B200_EUNSUPPORTED, "Physics.RiemannSolver: this build runs HLLC");
+    if (p->phase_field && p->physics != COMPAS_B200_FIVEEQS)
+        return fail(COMPAS_B200_EUNSUPPORTED, "PhaseField.phase_field = 1: this engine runs the FIVEEQS Phase-Field step");
+    if (p->phase_field && p->pf_mechanism != 1 && p->pf_mechanism != 3)
+        return fail(COMPAS_B200_EUNSUPPORTED, "PhaseField.Mechanism: this engine runs CAC-Adv and ACDI");
+    if (p->phase_field && p->pf_explicit_rc && p->pf_mechanism == 1)
+        return fail(COMPAS_B200_EARG, "non flux-based mechanism can not use the explicit RC approach");
     if (p->precision != 0 && p->precision != 1)
         return fail(COMPAS_B200_EARG, "precision must be 0 (plain FP64) or 1 (mixed)");
     if (g->ng < 3) return fail(COMPAS_B200_EARG, "WENO5 needs ng >= 3 ghost cells");
@@ -292,15 +300,20 @@ static KernelChoice choice_of(const compas_b200_parm* p) {
     k.limiter = p->id_limiter;
     k.precision = p->precision;
     k.thinc = p->thinc;
+    k.phase_field = 0;
     return k;
 }
 
-static int launch_stage(const compas_b200_parm* p, const StageArgs& a, cudaStream_t st) {
+static int launch_stage(const compas_b200_parm* p, const StageArgs& a, cudaStream_t st, int phase_field = 0) {
     const int ts = (p->dim == 2) ? kTile2 : kTile3;
     const long long tiles = (long long)((a.g.n[0] + ts - 1) / ts) * ((a.g.n[1] + ts - 1) / ts) *
                             ((a.g.n[2] + (p->dim == 2 ? 1 : ts) - 1) / (p->dim == 2 ? 1 : ts));
     if (tiles > 0x7fffffffLL) return fail(COMPAS_B200_EARG, "box too large");
-    const KernelChoice k = choice_of(p);
+    KernelChoice k = choice_of(p);
+    if (phase_field) {
+        k.thinc = 0;
+        k.phase_field = 1;
+    }
     cudaError_t e;
     if (p->physics == COMPAS_B200_FIVEEQS) e = (p->dim == 2) ? launch_stage_fiveeq2(k, a, st) : launch_stage_fiveeq3(k, a, st);
     else e = (p->dim == 2) ? launch_stage_sixeq2(k, a, st) : launch_stage_sixeq3(k, a, st);
@@ -313,6 +326,7 @@ static int launch_list(int physics, int dim, int limiter, int precision, const L
     k.limiter = limiter;
     k.precision = precision;
     k.thinc = 0;
+    k.phase_field = 0;
     cudaError_t e;
     if (physics == COMPAS_B200_FIVEEQS) e = (dim == 2) ? launch_list_fiveeq2(k, L, st) : launch_list_fiveeq3(k, L, st);
     else e = (dim == 2) ? launch_list_sixeq2(k, L, st) : launch_list_sixeq3(k, L, st);
@@ -411,7 +425,63 @@ struct compas_b200_level {
     bool need_init = true;
     cudaGraphExec_t graph = nullptr;
     cudaStream_t graph_stream = nullptr;
+    compas::PfLevel* pf = nullptr;  // Phase-Field work arrays (PhaseField.phase_field = 1)
+    long long pf_substeps = 0;
 };
+
+namespace compas {
+
+static void set_pf_args(StageArgs& a, const double* const* gq) {
+    for (int d = 0; d < 3; ++d) a.gq[d] = gq[d];
+}
+
+__global__ void set_scalar_kernel(double* slot, double v) { *slot = v; }
+
+// The sub-stepped Phase-Field TVD-RK3 advance over dt with fixed face gradients
+// (PhaseField_Evolve :546-592, PhaseField_ComputeDt :2036-2098, PhaseField_ThirdOrderSSPRK :2619-2752).
+// U is advanced in place with U1, U2 as stage buffers. Returns the sub-steps through *steps.
+static int pf_advance(const compas_b200_parm* p, const compas_b200_geom* g, double* U, double* U1, double* U2,
+                      const double* const* gq, double* dt_slot, double dt, double gmax, unsigned int* err_dev,
+                      cudaStream_t st, int* steps, long long* launches) {
+    double dxmin = g->dx[0];
+    for (int d = 1; d < p->dim; ++d) dxmin = std::min(dxmin, g->dx[d]);
+    StageArgs a = base_args(p, g);
+    a.mode = kModeStage;
+    a.dt = dt_slot;
+    a.err = err_dev;
+    set_pf_args(a, gq);
+    double* bufs_in[3] = {U, U1, U2};
+    double* bufs_out[3] = {U1, U2, U};
+    double pft = 0.0, pfdt = 0.0;
+    int n = 0, rc;
+    for (int s = 0; s < p->pf_max_step && pft < dt; ++s) {
+        double tmp = p->pf_cfl * dxmin / (gmax + 1.0e-14);
+        if (pft == 0.0) pfdt = tmp;
+        if (p->change_limiter && pfdt > 0.0) tmp = std::min(tmp, 1.1 * pfdt);
+        double d0 = tmp;
+        const double eps = 1.0e-3 * d0;
+        if (pft + d0 > dt - eps) d0 = dt - pft;
+        pfdt = d0;
+        set_scalar_kernel<<<1, 1, 0, st>>>(dt_slot, pfdt);
+        CUDA_TRY(cudaGetLastError());
+        for (int k = 0; k < 3; ++k) {
+            if ((rc = launch_fill(p, g, bufs_in[k], st))) return rc;
+            a.stage = k;
+            a.Us = bufs_in[k];
+            a.U0 = U;
+            a.Uout = bufs_out[k];
+            if ((rc = launch_stage(p, a, st, 1))) return rc;
+        }
+        *launches += 7;
+        pft += pfdt;
+        ++n;
+        if (pft >= dt - 1.0e-6 * dt) break;
+    }
+    *steps = n;
+    return COMPAS_B200_OK;
+}
+
+}  // namespace compas
 
 extern "C" {
 
@@ -435,6 +505,14 @@ int compas_b200_parm_init(compas_b200_parm* p, int physics, int dim) {
     p->id_riemann = 2;
     p->cfl = 0.4;
     p->change_limiter = 1;
+    // PhaseField_Parameter defaults (include/Physics_PhaseField/PhaseField_Parameter.H:27-50): the
+    // inputs default mechanism is CAC-Adv (:52)
+    p->pf_mechanism = 1;
+    p->pf_eta_factor = 2.0;
+    p->pf_eta_multiplier = 1.0;
+    p->pf_cfl = 0.4;
+    p->pf_max_step = 1000000;
+    p->pf_tol_rel = 1.0e-10;
     if (physics != COMPAS_B200_FIVEEQS && physics != COMPAS_B200_SIXEQS)
         return fail(COMPAS_B200_EARG, "physics must be FIVEEQS (555) or SIXEQS (666)");
     if (dim != 2 && dim != 3) return fail(COMPAS_B200_EARG, "dim must be 2 or 3");
@@ -533,6 +611,50 @@ int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value
         if (v == "mixed") { p->precision = 1; return 0; }
         return bad("fp64, mixed");
     }
+    if (k == "PhaseField.Mechanism") {
+        // include/Physics_PhaseField/PhaseField_Parameter.H:66-115
+        if (v == "CAC-Adv") { p->pf_mechanism = 1; return 0; }
+        if (v == "ACDI") { p->pf_mechanism = 3; return 0; }
+        if (v == "CAC-Adv-NormalFace" || v == "CAC-VanDerWaals" || v == "CDI" || v == "CDI-NormalFace" ||
+            v == "CDI-CompressionInterpolation" || v == "ACDI-NormalFace" || v == "CH-Adv" || v == "CH-Adv-NormalFace" ||
+            v == "CH-VanDerWaals")
+            return fail(COMPAS_B200_EUNSUPPORTED, k + " = " + v + " is a valid reference mechanism outside this engine "
+                                                  "(CAC-Adv, ACDI)");
+        return bad("CAC-Adv, CAC-Adv-NormalFace, CAC-VanDerWaals, CDI, CDI-NormalFace, CDI-CompressionInterpolation, "
+                   "ACDI, ACDI-NormalFace, CH-Adv, CH-Adv-NormalFace, CH-VanDerWaals");
+    }
+    if (k == "PhaseField.phase_field") { if (!parse_int(value, &ix)) return bad("0, 1"); p->phase_field = ix ? 1 : 0; return 0; }
+    if (k == "PhaseField.ID_ExplicitRC") { if (!parse_int(value, &ix) || ix < 0 || ix > 1) return bad("0, 1"); p->pf_explicit_rc = ix; return 0; }
+    if (k == "PhaseField.max_step") { if (!parse_int(value, &ix)) return bad("an integer"); p->pf_max_step = ix; return 0; }
+    {
+        struct PKey { const char* name; double* dst; };
+        const PKey pkeys[] = {{"PhaseField.Lambda", &p->pf_lambda}, {"PhaseField.Eta", &p->pf_eta},
+                              {"PhaseField.Eta_Factor", &p->pf_eta_factor},
+                              {"PhaseField.Eta_Multiplier", &p->pf_eta_multiplier},
+                              {"PhaseField.cfl", &p->pf_cfl}, {"LinearSystem.tol_rel", &p->pf_tol_rel}};
+        for (const auto& pk : pkeys)
+            if (k == pk.name) {
+                if (!parse_double(value, &x)) return bad("a number");
+                *pk.dst = x;
+                return 0;
+            }
+    }
+    // options the engine runs only at their reference defaults (PhaseField_Parameter.H:40-48)
+    {
+        struct OKey { const char* name; int only; };
+        const OKey okeys[] = {{"PhaseField.ID_Flux", 0}, {"PhaseField.ID_FluxPhase2Flux", 1},
+                              {"PhaseField.ID_Weight", 0}, {"PhaseField.ID_Potential", 0},
+                              {"PhaseField.ID_DegenerateMobility", 0}, {"PhaseField.ID_Formulation", 1},
+                              {"PhaseField.Switch_Step", 0}};
+        for (const auto& ok : okeys)
+            if (k == ok.name) {
+                if (!parse_int(value, &ix)) return bad("an integer");
+                if (ix != ok.only)
+                    return fail(COMPAS_B200_EUNSUPPORTED, k + " = " + v + ": this engine runs the reference default " +
+                                                              std::to_string(ok.only));
+                return 0;
+            }
+    }
     if (k == "run.timestep_change_limiter") { if (!parse_int(value, &ix)) return bad("0, 1"); p->change_limiter = ix ? 1 : 0; return 0; }
     return fail(COMPAS_B200_EARG, "unknown inputs key '" + k + "'");
 }
@@ -607,6 +729,95 @@ int compas_b200_rk3_stage(const compas_b200_parm* p, const compas_b200_geom* g, 
     a.err = err_dev;
     return launch_stage(p, a, (cudaStream_t)stream);
 }
+
+int compas_b200_pf_compute_dUdt(const compas_b200_parm* p, const compas_b200_geom* g, const double* U, double* dUdt,
+                                const double* gq0, const double* gq1, const double* gq2, unsigned int* err_dev,
+                                void* stream) {
+    int rc = check_args(p, g);
+    if (rc) return rc;
+    if (p->physics != COMPAS_B200_FIVEEQS)
+        return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field right-hand side is the FIVEEQS model's");
+    if (!U || !dUdt || !gq0 || !gq1 || (p->dim == 3 && !gq2)) return fail(COMPAS_B200_EARG, "null argument");
+    StageArgs a = base_args(p, g);
+    a.Us = U;
+    a.Uout = dUdt;
+    a.mode = kModeDudt;
+    a.err = err_dev;
+    const double* gq[3] = {gq0, gq1, gq2};
+    set_pf_args(a, gq);
+    return launch_stage(p, a, (cudaStream_t)stream, 1);
+}
+
+int compas_b200_pf_rk3_stage(const compas_b200_parm* p, const compas_b200_geom* g, int stage, const double* Us,
+                             const double* Uold, double* Unew, const double* dt_dev, const double* gq0,
+                             const double* gq1, const double* gq2, unsigned int* err_dev, void* stream) {
+    int rc = check_args(p, g);
+    if (rc) return rc;
+    if (p->physics != COMPAS_B200_FIVEEQS)
+        return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field right-hand side is the FIVEEQS model's");
+    if (stage < 0 || stage > 2) return fail(COMPAS_B200_EARG, "stage must be 0, 1 or 2");
+    if (!Us || !Unew || !dt_dev || (stage > 0 && !Uold) || !gq0 || !gq1 || (p->dim == 3 && !gq2))
+        return fail(COMPAS_B200_EARG, "null argument");
+    if (Us == Unew) return fail(COMPAS_B200_EARG, "Unew may not alias Us");
+    StageArgs a = base_args(p, g);
+    a.Us = Us;
+    a.U0 = Uold;
+    a.Uout = Unew;
+    a.mode = kModeStage;
+    a.stage = stage;
+    a.dt = dt_dev;
+    a.err = err_dev;
+    const double* gq[3] = {gq0, gq1, gq2};
+    set_pf_args(a, gq);
+    return launch_stage(p, a, (cudaStream_t)stream, 1);
+}
+
+int compas_b200_pf_grad_q(const compas_b200_parm* p, const compas_b200_geom* g, const double* U, double dt,
+                          double* gq0, double* gq1, double* gq2, double* info, void* stream) {
+    int rc = check_args(p, g);
+    if (rc) return rc;
+    if (p->physics != COMPAS_B200_FIVEEQS)
+        return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field step is the FIVEEQS model's");
+    if (!U || !gq0 || !gq1 || (p->dim == 3 && !gq2)) return fail(COMPAS_B200_EARG, "null argument");
+    if (!(dt > 0.0)) return fail(COMPAS_B200_EARG, "dt must be positive");
+    compas_b200_geom gg = *g;
+    if (p->dim == 2) gg.n[2] = 1;
+    PfLevel* pf = nullptr;
+    std::string msg;
+    if ((rc = pf_create(p, &gg, &pf, &msg))) return fail(rc, msg);
+    cudaStream_t st = (cudaStream_t)stream;
+    PfInfo pi;
+    rc = pf_grad_q(pf, p, U, dt, st, &pi, &msg);
+    if (!rc) {
+        double* out[3] = {gq0, gq1, gq2};
+        for (int d = 0; d < p->dim && !rc; ++d) {
+            const long long nf = (long long)(gg.n[0] + (d == 0)) * (gg.n[1] + (d == 1)) * (gg.n[2] + (d == 2));
+            cudaError_t e = cudaMemcpyAsync(out[d], pf_gq(pf, d), sizeof(double) * nf, cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) {
+                rc = COMPAS_B200_ECUDA;
+                msg = std::string("copy of grad Q: ") + cudaGetErrorString(e);
+            }
+        }
+        if (!rc && cudaStreamSynchronize(st) != cudaSuccess) {
+            rc = COMPAS_B200_ECUDA;
+            msg = "stream synchronisation";
+        }
+    }
+    pf_destroy(pf);
+    if (rc) return fail(rc, msg);
+    if (info) {
+        info[0] = pi.max_v;
+        info[1] = pi.mobility;
+        info[2] = pi.eta;
+        info[3] = pi.mech_steps;
+        info[4] = pi.solve_iters;
+        info[5] = pi.gmax;
+        info[6] = pi.solve_res;
+    }
+    return COMPAS_B200_OK;
+}
+
+long long compas_b200_level_pf_substeps(const compas_b200_level* lv) { return lv ? lv->pf_substeps : 0; }
 
 int compas_b200_relaxation(const compas_b200_parm* p, const compas_b200_geom* g, double* U, unsigned int* err_dev,
                            void* stream) {
@@ -693,6 +904,14 @@ int compas_b200_level_create(const compas_b200_parm* p, const compas_b200_geom* 
         return fail(e == cudaErrorMemoryAllocation ? COMPAS_B200_ENOMEM : COMPAS_B200_ECUDA,
                     std::string("level allocation: ") + cudaGetErrorString(e));
     }
+    if (p->phase_field) {
+        std::string msg;
+        if ((rc = pf_create(p, &lv->g, &lv->pf, &msg))) {
+            compas_b200_level_destroy(lv);
+            cudaGetLastError();
+            return fail(rc, msg);
+        }
+    }
     *out = lv;
     return COMPAS_B200_OK;
 }
@@ -705,6 +924,7 @@ int compas_b200_level_destroy(compas_b200_level* lv) {
     cudaFree(lv->U2);
     cudaFree(lv->ctl);
     cudaFree(lv->dts);
+    pf_destroy(lv->pf);
     delete lv;
     return COMPAS_B200_OK;
 }
@@ -796,6 +1016,28 @@ int compas_b200_level_advance(compas_b200_level* lv, int nsteps, double stop_tim
         lv->need_init = false;
     }
     if (nsteps == 0) return COMPAS_B200_OK;
+    if (lv->pf) {
+        // Evolve (source/Class_Compressible_PhaseField.cpp:171-330): each hyperbolic step is followed by
+        // a Phase-Field step of the same dt; its host loop reads dt, max|u| and max|grad Q|.
+        for (int s = 0; s < nsteps; ++s) {
+            if ((rc = enqueue_step(lv, st))) return rc;
+            lv->launches += 8;
+            StepCtl h;
+            CUDA_TRY(cudaMemcpyAsync(&h, lv->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, st));
+            CUDA_TRY(cudaStreamSynchronize(st));
+            if (h.done || h.err) break;
+            PfInfo info;
+            std::string msg;
+            if ((rc = pf_grad_q(lv->pf, &lv->p, lv->U, h.dt, st, &info, &msg))) return fail(rc, msg);
+            const double* gq[3] = {pf_gq(lv->pf, 0), pf_gq(lv->pf, 1), lv->p.dim == 3 ? pf_gq(lv->pf, 2) : nullptr};
+            int sub = 0;
+            if ((rc = pf_advance(&lv->p, &lv->g, lv->U, lv->U1, lv->U2, gq, pf_dt_slot(lv->pf), h.dt, info.gmax,
+                                 &lv->ctl->err, st, &sub, &lv->launches)))
+                return rc;
+            lv->pf_substeps += sub;
+        }
+        return COMPAS_B200_OK;
+    }
     if (use_graph) {
         if (!lv->graph || lv->graph_stream != st) {
             if (lv->graph) {

@@ -35,11 +35,11 @@ struct LaunchShape {
 };
 
 // One CTA per tile of the box.
-template <class M, int SCHEME, bool MIX, bool TH>
+template <class M, int SCHEME, bool MIX, int VAR>
 static cudaError_t launch_stage_v(const StageArgs& a, cudaStream_t st) {
     using S = LaunchShape<M>;
     using T = TileShape<M, S::TS, S::TS, S::TZ, typename std::conditional<MIX, float, double>::type>;
-    auto kern = stage_kernel<M, SCHEME, MIX, TH, S::TS, S::TS, S::TZ, S::NT, S::MINB>;
+    auto kern = stage_kernel<M, SCHEME, MIX, VAR, S::TS, S::TS, S::TZ, S::NT, S::MINB>;
     static bool attr_set = false;
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
@@ -52,15 +52,21 @@ static cudaError_t launch_stage_v(const StageArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+template <class M, int SCHEME, bool MIX>
+static cudaError_t launch_stage_var(const KernelChoice& k, const StageArgs& a, cudaStream_t st) {
+    if (k.phase_field) {
+        if constexpr (M::NC == 1) return launch_stage_v<M, SCHEME, MIX, kVarPhaseField>(a, st);
+        else return cudaErrorNotSupported;
+    }
+    if (k.thinc) return launch_stage_v<M, SCHEME, MIX, kVarThinc>(a, st);
+    return launch_stage_v<M, SCHEME, MIX, kVarPlain>(a, st);
+}
+
 template <class M>
 static cudaError_t launch_stage_m(const KernelChoice& k, const StageArgs& a, cudaStream_t st) {
-    const bool mix = (k.precision == 1), bounded = (k.limiter == 6), th = (k.thinc != 0);
-    if (mix) {
-        if (bounded) return th ? launch_stage_v<M, 6, true, true>(a, st) : launch_stage_v<M, 6, true, false>(a, st);
-        return th ? launch_stage_v<M, 5, true, true>(a, st) : launch_stage_v<M, 5, true, false>(a, st);
-    }
-    if (bounded) return th ? launch_stage_v<M, 6, false, true>(a, st) : launch_stage_v<M, 6, false, false>(a, st);
-    return th ? launch_stage_v<M, 5, false, true>(a, st) : launch_stage_v<M, 5, false, false>(a, st);
+    const bool mix = (k.precision == 1), bounded = (k.limiter == 6);
+    if (mix) return bounded ? launch_stage_var<M, 6, true>(k, a, st) : launch_stage_var<M, 5, true>(k, a, st);
+    return bounded ? launch_stage_var<M, 6, false>(k, a, st) : launch_stage_var<M, 5, false>(k, a, st);
 }
 
 // Persistent box-list launch: one resident wave of CTAs walks the tiles of every box.

@@ -11,11 +11,13 @@ struct StageArgs;
 struct ListArgs;
 
 // Variant of the stage kernel: FiniteVolume.Scheme (5 WENO5, 6 WENO5B), precision (0 FP64, 1 mixed),
-// FiniteVolume.THINC (single-box kernel only).
+// FiniteVolume.THINC (single-box kernel only), and the Phase-Field regularisation right-hand side
+// instead of the hyperbolic one (FIVEEQS, single-box kernel only).
 struct KernelChoice {
     int limiter;
     int precision;
     int thinc;
+    int phase_field;
 };
 
 // Tile side of the stage kernels (cells per direction): 16^2 tiles in 2D, 8^3 in 3D.

@@ -1,0 +1,891 @@
+// Phase-Field regularisation step of the five-equation model on the device (see phasefield.h).
+//
+// Reference (orchestration in source/Class_Compressible_PhaseField.cpp):
+//   PhaseField_Evolve            :424-595   mobility 0.5 eta max|u|, eta = Eta_Multiplier x max dx
+//   PhaseFieldMechanism_Evolve   :596-711   explicit pseudo-time steps of the mechanism over dt
+//   PhaseField_Mechanism (CAC)   :1006-1152 Allen-Cahn with the advective chemical potential and the
+//                                           conservative Lagrange multiplier -int(mech)/int(W)
+//   PhaseField_Mechanism (flux)  :1155-1232, PhaseField_ACDI :1494-1645
+//   PhaseField_Normal            :1957-2033
+//   PhaseField_GradQPF           :2132-2310 (implicit: div(beta grad Q) = Div_Jhat, beta = W(phi~)+1e-3,
+//                                           AMReX MLMG ABecLaplacian), :2314-2401 (explicit)
+// and the device functions of include/Physics_PhaseField and include/Operators_PhaseField cited at
+// each kernel. The elliptic solve is this engine's own: conjugate gradients preconditioned by one
+// geometric multigrid V-cycle (red-black Gauss-Seidel, or weighted Jacobi where a periodic side has
+// an odd cell count), stopped at the reference's criterion max|r| <= LinearSystem.tol_rel max|rhs|.
+// All arithmetic is FP64; sums are reduced in a fixed order (block partials, then one block), so a
+// step is deterministic.
+#include "phasefield.h"
+
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "physics.cuh"
+
+namespace compas {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kRedBlocks = 592;  // 4 x 148 SMs: partial sums of the reductions
+constexpr int kMaxLevels = 24;
+
+struct PfDims {
+    int n[3];
+    int D;
+    double dx[3];
+    int periodic[3];
+    long long nv;            // valid cells
+    int px, py, pz, gz;      // padded scalar layout: one ghost layer (none in z in 2D)
+    long long ps;            // padded cells per component
+    long long nf[3];         // faces per direction
+};
+
+PfDims make_dims(int D, const int* n, const double* dx, const int* periodic) {
+    PfDims m;
+    m.D = D;
+    for (int d = 0; d < 3; ++d) {
+        m.n[d] = (d < D) ? n[d] : 1;
+        m.dx[d] = (d < D) ? dx[d] : 1.0;
+        m.periodic[d] = (d < D) ? periodic[d] : 0;
+    }
+    m.nv = (long long)m.n[0] * m.n[1] * m.n[2];
+    m.gz = (D == 3) ? 1 : 0;
+    m.px = m.n[0] + 2;
+    m.py = m.n[1] + 2;
+    m.pz = m.n[2] + 2 * m.gz;
+    m.ps = (long long)m.px * m.py * m.pz;
+    for (int d = 0; d < 3; ++d)
+        m.nf[d] = (d < D) ? (long long)(m.n[0] + (d == 0)) * (m.n[1] + (d == 1)) * (m.n[2] + (d == 2)) : 0;
+    return m;
+}
+
+__device__ __forceinline__ long long pidx(const PfDims& m, int i, int j, int k) {
+    return (long long)(i + 1) + m.px * ((long long)(j + 1) + (long long)m.py * (k + m.gz));
+}
+__device__ __forceinline__ long long vidx(const PfDims& m, int i, int j, int k) {
+    return (long long)i + m.n[0] * ((long long)j + (long long)m.n[1] * k);
+}
+__device__ __forceinline__ long long fidx(const PfDims& m, int d, int i, int j, int k) {
+    const int fx = m.n[0] + (d == 0), fy = m.n[1] + (d == 1);
+    return (long long)i + fx * ((long long)j + (long long)fy * k);
+}
+__device__ __forceinline__ void vcoord(const PfDims& m, long long q, int& i, int& j, int& k) {
+    i = (int)(q % m.n[0]);
+    const long long r = q / m.n[0];
+    j = (int)(r % m.n[1]);
+    k = (int)(r / m.n[1]);
+}
+__device__ __forceinline__ void fcoord(const PfDims& m, int d, long long q, int& i, int& j, int& k) {
+    const int fx = m.n[0] + (d == 0), fy = m.n[1] + (d == 1);
+    i = (int)(q % fx);
+    const long long r = q / fx;
+    j = (int)(r % fy);
+    k = (int)(r / fy);
+}
+
+#define GRID_STRIDE(q, total) \
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < (total); q += (long long)gridDim.x * blockDim.x)
+
+unsigned blocks_for(long long n) {
+    long long b = (n + kThreads - 1) / kThreads;
+    if (b > 148LL * 32) b = 148LL * 32;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+
+// ---- Phase-Field device functions (include/Physics_PhaseField) --------------------------------------
+// Mapping_Backward.H: psi = sqrt(2) eta atanh(2 phi - 1), phi clipped to [1e-12, 1 - 1e-12]
+__device__ __forceinline__ double map_backward(double phi, double eta) {
+    const double ep = 1.0e-12;
+    double t = phi;
+    if (t < ep) t = ep;
+    else if (t > 1.0 - ep) t = 1.0 - ep;
+    return sqrt(2.0) * eta * atanh(2.0 * t - 1.0);
+}
+// Mapping_Forward.H (ID_Derivative 0 and 1)
+__device__ __forceinline__ double map_forward(double psi, double eta) {
+    return 0.5 + 0.5 * tanh(psi / (sqrt(2.0) * eta));
+}
+__device__ __forceinline__ double map_forward_d1(double psi, double eta) {
+    return 0.5 / (sqrt(2.0) * eta) / cosh(psi / (sqrt(2.0) * eta)) / cosh(psi / (sqrt(2.0) * eta));
+}
+// face value of the mapped phase field (PhaseField_GradQPF :2218-2241 / :2357-2381)
+__device__ __forceinline__ double face_mapped(double pc, double pm, double eta, double eta_f) {
+    const double psic = map_backward(pc, eta), psim = map_backward(pm, eta);
+    const double fc = map_forward(psic, eta_f * eta), fm = map_forward(psim, eta_f * eta);
+    return 0.5 * fm + 0.5 * fc;
+}
+
+// ---- small kernels ----------------------------------------------------------------------------------
+// volume fraction (component ia of the padded state) into a padded scalar field
+__global__ void k_extract(const double* U, long long S, long long upx, long long upxy, int ung, int ugz, int ia,
+                          PfDims m, double* dst) {
+    GRID_STRIDE(q, m.nv) {
+        int i, j, k;
+        vcoord(m, q, i, j, k);
+        const long long uq = (long long)(k + ugz) * upxy + (long long)(j + ung) * upx + (i + ung);
+        dst[pidx(m, i, j, k)] = U[(long long)ia * S + uq];
+    }
+}
+
+// ghost layer of a padded scalar field: int_dir on periodic directions, foextrap otherwise
+__global__ void k_fill(double* f, int ncomp, PfDims m) {
+    GRID_STRIDE(q, m.ps * ncomp) {
+        const int c = (int)(q / m.ps);
+        const long long r = q % m.ps;
+        int i = (int)(r % m.px) - 1;
+        const long long r2 = r / m.px;
+        int j = (int)(r2 % m.py) - 1;
+        int k = (int)(r2 / m.py) - m.gz;
+        const bool ghost = i < 0 || i >= m.n[0] || j < 0 || j >= m.n[1] || (m.D == 3 && (k < 0 || k >= m.n[2]));
+        if (!ghost) continue;
+        int x[3] = {i, j, k};
+        for (int d = 0; d < m.D; ++d) {
+            if (x[d] < 0) x[d] = m.periodic[d] ? x[d] + m.n[d] : 0;
+            else if (x[d] >= m.n[d]) x[d] = m.periodic[d] ? x[d] - m.n[d] : m.n[d] - 1;
+        }
+        f[c * m.ps + r] = f[c * m.ps + pidx(m, x[0], x[1], x[2])];
+    }
+}
+
+// FDM_Normal_CenterFromCenter_{K,D}: normalised centred gradient of f at the valid cells
+__global__ void k_normal(const double* f, double* nrm, PfDims m) {
+    GRID_STRIDE(q, m.nv) {
+        int i, j, k;
+        vcoord(m, q, i, j, k);
+        const double fc = f[pidx(m, i, j, k)];
+        double gr[3] = {0.0, 0.0, 0.0};
+        double sum = 0.0;
+        for (int d = 0; d < m.D; ++d) {
+            const int ei = (d == 0), ej = (d == 1), ek = (d == 2);
+            const double fm = f[pidx(m, i - ei, j - ej, k - ek)], fp = f[pidx(m, i + ei, j + ej, k + ek)];
+            const double gm = (fc - fm) / m.dx[d], gp = (fp - fc) / m.dx[d];
+            gr[d] = 0.5 * gm + 0.5 * gp;
+            sum += gr[d] * gr[d];
+        }
+        const long long pq = pidx(m, i, j, k);
+        for (int d = 0; d < m.D; ++d) nrm[d * m.ps + pq] = (sum == 0.0) ? 0.0 : gr[d] / sqrt(sum);
+    }
+}
+
+// fixed-order block reduction of two sums into partial[blockIdx] (2 per block)
+__device__ __forceinline__ void block_sum2(double a, double b, double* partial) {
+    __shared__ double sa[kThreads], sb[kThreads];
+    sa[threadIdx.x] = a;
+    sb[threadIdx.x] = b;
+    __syncthreads();
+    for (int s = kThreads / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            sa[threadIdx.x] += sa[threadIdx.x + s];
+            sb[threadIdx.x] += sb[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partial[2 * blockIdx.x] = sa[0];
+        partial[2 * blockIdx.x + 1] = sb[0];
+    }
+}
+
+__global__ void k_reduce2(const double* partial, int nb, double* out) {
+    __shared__ double sa[kThreads], sb[kThreads];
+    double a = 0.0, b = 0.0;
+    for (int t = threadIdx.x; t < nb; t += kThreads) {
+        a += partial[2 * t];
+        b += partial[2 * t + 1];
+    }
+    sa[threadIdx.x] = a;
+    sb[threadIdx.x] = b;
+    __syncthreads();
+    for (int s = kThreads / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            sa[threadIdx.x] += sa[threadIdx.x + s];
+            sb[threadIdx.x] += sb[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = sa[0];
+        out[1] = sb[0];
+    }
+}
+
+// CAC-Adv mechanism and weight at the valid cells, with their sums
+// (FDM_PhaseFieldMechanism_ACAdv_{K,D}, FDM_ChemicalPotential_Adv_D, ChemicalPotential_Adv,
+//  PotentialFunction_DoubleWell (first derivative), PhaseFieldMechanism_AC, WeightFunction_Quadratic)
+__global__ void k_cac_mech(const double* pf, const double* nrm, PfDims m, double mob, double lam, double eta,
+                           double* mech, double* wgt, double* partial) {
+    double sm = 0.0, sw = 0.0;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < m.nv; q += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        vcoord(m, q, i, j, k);
+        const long long c = pidx(m, i, j, k);
+        const double fc = pf[c];
+        double lap = 0.0, divn = 0.0, ag = 0.0;
+        for (int d = 0; d < m.D; ++d) {
+            const int ei = (d == 0), ej = (d == 1), ek = (d == 2);
+            const long long cm = pidx(m, i - ei, j - ej, k - ek), cp = pidx(m, i + ei, j + ej, k + ek);
+            const double fm = pf[cm], fp = pf[cp];
+            const double h = m.dx[d];
+            const double gfp = (fp - fc) / h, gfm = (fc - fm) / h;
+            const double tl = (gfp - gfm) / h;
+            lap = (d == 0) ? tl : lap + tl;
+            const double nc = nrm[d * m.ps + c], nm = nrm[d * m.ps + cm], np = nrm[d * m.ps + cp];
+            const double nfp = 0.5 * nc + 0.5 * np, nfm = 0.5 * nm + 0.5 * nc;
+            const double tn = (nfp - nfm) / h;
+            divn = (d == 0) ? tn : divn + tn;
+            const double g = 0.5 * gfm + 0.5 * gfp;
+            ag += g * g;
+        }
+        const double curv = -divn;
+        ag = sqrt(ag);
+        const double g1 = 2.0 * fc * (1.0 - fc) * (1.0 - 2.0 * fc);
+        const double mu = lam * ((1.0 / eta / eta) * g1 - lap - ag * curv);
+        const double me = -mob * mu;
+        const double w = fc * (1.0 - fc);
+        mech[q] = me;
+        wgt[q] = w;
+        sm += me;
+        sw += w;
+    }
+    block_sum2(sm, sw, partial);
+}
+
+// PhaseFieldMechanism_CAC and the explicit pseudo-time update phi = phi_old + dt Div_J
+__global__ void k_cac_update(const double* mech, const double* wgt, const double* tot, const double* pfo, double* pf,
+                             PfDims m, double dtm) {
+    const double im = tot[0], iw = tot[1];
+    const double L = (iw == 0.0) ? 0.0 : -im / iw;
+    GRID_STRIDE(q, m.nv) {
+        int i, j, k;
+        vcoord(m, q, i, j, k);
+        const double dj = mech[q] + wgt[q] * L;
+        pf[pidx(m, i, j, k)] = 1.0 * pfo[q] + dtm * dj;
+    }
+}
+
+__global__ void k_copy_valid(const double* pf, double* dst, PfDims m) {
+    GRID_STRIDE(q, m.nv) {
+        int i, j, k;
+        vcoord(m, q, i, j, k);
+        dst[q] = pf[pidx(m, i, j, k)];
+    }
+}
+
+// level-set of ACDI (Mapping_Backward at the valid cells)
+__global__ void k_ls(const double* pf, double* ls, PfDims m, double eta) {
+    GRID_STRIDE(q, m.nv) {
+        int i, j, k;
+        vcoord(m, q, i, j, k);
+        const long long c = pidx(m, i, j, k);
+        ls[c] = map_backward(pf[c], eta);
+    }
+}
+
+// ACDI face flux of direction d (FDM_PhaseFieldFlux_ACDI_{K,D}, PhaseFieldFlux_ACDI); with the
+// explicit approach also Jhat += dt J (MultiFab::Saxpy)
+__global__ void k_acdi_flux(const double* pf, const double* nrm, PfDims m, int d, double mob, double eta, double* J,
+                            double* Jhat, double dtm) {
+    GRID_STRIDE(q, m.nf[d]) {
+        int i, j, k;
+        fcoord(m, d, q, i, j, k);
+        const int ei = (d == 0), ej = (d == 1), ek = (d == 2);
+        const long long c = pidx(m, i, j, k), cm = pidx(m, i - ei, j - ej, k - ek);
+        const double pc = pf[c], pm = pf[cm];
+        const double psic = map_backward(pc, eta), psim = map_backward(pm, eta);
+        const double grad = (pc - pm) / m.dx[d];
+        const double psi = 0.5 * psim + 0.5 * psic;
+        const double nf = 0.5 * nrm[d * m.ps + cm] + 0.5 * nrm[d * m.ps + c];
+        const double mobf = 0.5 * mob + 0.5 * mob;
+        const double f1 = map_forward_d1(psi, eta);
+        const double flux = mobf * (grad - f1 * nf);
+        J[q] = flux;
+        if (Jhat) Jhat[q] = Jhat[q] + dtm * flux;
+    }
+}
+
+// FVM_Divergence_K of the face fluxes and the pseudo-time update
+__global__ void k_div_update(const double* J0, const double* J1, const double* J2, const double* pfo, double* pf,
+                             PfDims m, double dtm) {
+    GRID_STRIDE(q, m.nv) {
+        int i, j, k;
+        vcoord(m, q, i, j, k);
+        const double* J[3] = {J0, J1, J2};
+        double dv = 0.0;
+        for (int d = 0; d < m.D; ++d) {
+            const int ei = (d == 0), ej = (d == 1), ek = (d == 2);
+            const double t = (J[d][fidx(m, d, i + ei, j + ej, k + ek)] - J[d][fidx(m, d, i, j, k)]) / m.dx[d];
+            dv = (d == 0) ? t : dv + t;
+        }
+        pf[pidx(m, i, j, k)] = 1.0 * pfo[q] + dtm * dv;
+    }
+}
+
+// Div_Jhat = (1/dt) phi_new + (-1/dt) phi (MultiFab::LinComb), and its sum
+__global__ void k_djhat(const double* pfn, const double* pf0, PfDims m, double inv, double* rhs, double* partial) {
+    double s = 0.0;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < m.nv; q += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        vcoord(m, q, i, j, k);
+        const long long c = pidx(m, i, j, k);
+        const double v = inv * pfn[c] + (-inv) * pf0[c];
+        rhs[q] = v;
+        s += v;
+    }
+    block_sum2(s, 0.0, partial);
+}
+
+// face coefficient beta = W(phi~_face) + 1e-3 of direction d
+__global__ void k_beta(const double* pf0, PfDims m, int d, double eta, double eta_f, double* beta) {
+    GRID_STRIDE(q, m.nf[d]) {
+        int i, j, k;
+        fcoord(m, d, q, i, j, k);
+        const int ei = (d == 0), ej = (d == 1), ek = (d == 2);
+        const double face = face_mapped(pf0[pidx(m, i, j, k)], pf0[pidx(m, i - ei, j - ej, k - ek)], eta, eta_f);
+        beta[q] = face * (1.0 - face) + 1.0e-3;
+    }
+}
+
+// explicit approach: grad Q = J / (W(phi~_face) + eps), J = Jhat (1/dt) (PhaseFieldFlux2GradQPF)
+__global__ void k_gq_explicit(const double* pf0, const double* Jhat, PfDims m, int d, double inv, double eta,
+                              double eta_f, double* gq) {
+    GRID_STRIDE(q, m.nf[d]) {
+        int i, j, k;
+        fcoord(m, d, q, i, j, k);
+        const int ei = (d == 0), ej = (d == 1), ek = (d == 2);
+        const double face = face_mapped(pf0[pidx(m, i, j, k)], pf0[pidx(m, i - ei, j - ej, k - ek)], eta, eta_f);
+        const double J = Jhat[q] * inv;
+        const double eps = 1.0e-3;
+        const double flux = (face < eps || face > 1.0 - eps) ? 0.0 : J;
+        gq[q] = flux / (face * (1.0 - face) + eps);
+    }
+}
+
+// face gradient of the solution (MLMG getGradSolution): (Q_c - Q_m)/dx, zero on Neumann sides
+__global__ void k_gq_from_q(const double* Q, PfDims m, int d, double* gq) {
+    GRID_STRIDE(q, m.nf[d]) {
+        int x[3];
+        fcoord(m, d, q, x[0], x[1], x[2]);
+        int mm[3] = {x[0], x[1], x[2]};
+        mm[d] -= 1;
+        if (x[d] == 0 || x[d] == m.n[d]) {
+            if (!m.periodic[d]) {
+                gq[q] = 0.0;
+                continue;
+            }
+            x[d] = (x[d] + m.n[d]) % m.n[d];
+            mm[d] = (mm[d] + m.n[d]) % m.n[d];
+        }
+        gq[q] = (Q[vidx(m, x[0], x[1], x[2])] - Q[vidx(m, mm[0], mm[1], mm[2])]) / m.dx[d];
+    }
+}
+
+// max |u| over the valid cells of the padded state (MaxVelocity, Conservative2Velocity)
+__global__ void k_maxv(const double* U, long long S, long long upx, long long upxy, int ung, int ugz, PfDims m,
+                       unsigned long long* out) {
+    double v = 0.0;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < m.nv; q += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        vcoord(m, q, i, j, k);
+        const long long uq = (long long)(k + ugz) * upxy + (long long)(j + ung) * upx + (i + ung);
+        const double rho = U[uq] + U[S + uq];
+        double s = 0.0;
+        for (int d = 0; d < m.D; ++d) {
+            const double u = U[(2 + d) * S + uq] / rho;
+            s = (d == 0) ? u * u : s + u * u;
+        }
+        v = dmax(v, fabs(sqrt(s)));
+    }
+    for (int o = 16; o > 0; o >>= 1) v = dmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(v));
+}
+
+__global__ void k_maxabs(const double* a, long long n, unsigned long long* out) {
+    double v = 0.0;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        v = dmax(v, fabs(a[q]));
+    for (int o = 16; o > 0; o >>= 1) v = dmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(v));
+}
+
+// ---- multigrid -----------------------------------------------------------------------------------------
+// A x = -div(beta grad x) on the valid cells (no flux through Neumann sides, wrap on periodic ones).
+struct MgLevel {
+    PfDims m;
+    double* beta[3] = {nullptr, nullptr, nullptr};
+    double* x = nullptr;
+    double* b = nullptr;
+    double* r = nullptr;
+    bool rb = true;  // red-black colouring is a proper two-colouring (no odd periodic side)
+};
+
+__device__ __forceinline__ void mg_row(const MgLevel& L, const double* x, long long q, double& off, double& diag) {
+    const PfDims& m = L.m;
+    int c[3];
+    vcoord(m, q, c[0], c[1], c[2]);
+    off = 0.0;
+    diag = 0.0;
+    for (int d = 0; d < m.D; ++d) {
+        const double h2 = m.dx[d] * m.dx[d];
+        for (int s = 0; s < 2; ++s) {
+            int nb[3] = {c[0], c[1], c[2]};
+            nb[d] += s ? 1 : -1;
+            if (nb[d] < 0 || nb[d] >= m.n[d]) {
+                if (!m.periodic[d]) continue;
+                nb[d] = (nb[d] + m.n[d]) % m.n[d];
+            }
+            int f[3] = {c[0], c[1], c[2]};
+            if (s) f[d] += 1;
+            const double bf = L.beta[d][fidx(m, d, f[0], f[1], f[2])] / h2;
+            diag += bf;
+            off += bf * x[vidx(m, nb[0], nb[1], nb[2])];
+        }
+    }
+}
+
+__global__ void k_mg_apply(MgLevel L, const double* x, double* y) {
+    GRID_STRIDE(q, L.m.nv) {
+        double off, diag;
+        mg_row(L, x, q, off, diag);
+        y[q] = diag * x[q] - off;
+    }
+}
+
+__global__ void k_mg_residual(MgLevel L) {
+    GRID_STRIDE(q, L.m.nv) {
+        double off, diag;
+        mg_row(L, L.x, q, off, diag);
+        L.r[q] = L.b[q] - (diag * L.x[q] - off);
+    }
+}
+
+// red-black Gauss-Seidel half sweep on cells of colour `color`
+__global__ void k_mg_rb(MgLevel L, int color) {
+    GRID_STRIDE(q, L.m.nv) {
+        int i, j, k;
+        vcoord(L.m, q, i, j, k);
+        if (((i + j + k) & 1) != color) continue;
+        double off, diag;
+        mg_row(L, L.x, q, off, diag);
+        L.x[q] = (L.b[q] + off) / diag;
+    }
+}
+
+// weighted Jacobi sweep (x_new into r, then copied back)
+__global__ void k_mg_jacobi(MgLevel L) {
+    GRID_STRIDE(q, L.m.nv) {
+        double off, diag;
+        mg_row(L, L.x, q, off, diag);
+        L.r[q] = L.x[q] + 0.8 * ((L.b[q] + off) / diag - L.x[q]);
+    }
+}
+__global__ void k_copy(const double* a, double* b, long long n) {
+    GRID_STRIDE(q, n) b[q] = a[q];
+}
+__global__ void k_zero(double* a, long long n) {
+    GRID_STRIDE(q, n) a[q] = 0.0;
+}
+
+// coarse rhs = average of the fine residuals of the 2^D children
+__global__ void k_mg_restrict(const double* rf, PfDims f, double* bc, PfDims c) {
+    GRID_STRIDE(q, c.nv) {
+        int I, J, K;
+        vcoord(c, q, I, J, K);
+        double s = 0.0;
+        const int kz = (c.D == 3) ? 2 : 1;
+        for (int dk = 0; dk < kz; ++dk)
+            for (int dj = 0; dj < 2; ++dj)
+                for (int di = 0; di < 2; ++di) s += rf[vidx(f, 2 * I + di, 2 * J + dj, (c.D == 3 ? 2 * K + dk : 0))];
+        bc[q] = s / (double)(c.D == 3 ? 8 : 4);
+    }
+}
+
+// fine x += coarse x of the parent (piecewise-constant prolongation)
+__global__ void k_mg_prolong(const double* xc, PfDims c, double* xf, PfDims f) {
+    GRID_STRIDE(q, f.nv) {
+        int i, j, k;
+        vcoord(f, q, i, j, k);
+        xf[q] += xc[vidx(c, i / 2, j / 2, (f.D == 3 ? k / 2 : 0))];
+    }
+}
+
+// coarse face coefficient = average of the fine faces it covers
+__global__ void k_mg_beta(const double* bf, PfDims f, double* bc, PfDims c, int d) {
+    GRID_STRIDE(q, c.nf[d]) {
+        int x[3];
+        fcoord(c, d, q, x[0], x[1], x[2]);
+        double s = 0.0;
+        int cnt = 0;
+        const int t0 = (d == 0) ? 1 : 0, t1 = (d == 2) ? 1 : 2;  // transverse directions
+        const int r0 = (t0 < c.D) ? 2 : 1, r1 = (t1 < c.D && t1 != d) ? 2 : 1;
+        for (int a = 0; a < r0; ++a)
+            for (int b = 0; b < r1; ++b) {
+                int y[3] = {2 * x[0], 2 * x[1], (c.D == 3) ? 2 * x[2] : 0};
+                y[t0] += a;
+                if (t1 < 3) y[t1] += b;
+                s += bf[fidx(f, d, y[0], y[1], y[2])];
+                ++cnt;
+            }
+        bc[q] = s / (double)cnt;
+    }
+}
+
+// dot product partials (fixed order); b == nullptr sums a
+__global__ void k_dot(const double* a, const double* b, long long n, double* partial) {
+    double s = 0.0;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        s += b ? a[q] * b[q] : a[q];
+    block_sum2(s, 0.0, partial);
+}
+__global__ void k_add_const(double* a, long long n, const double* tot, double scale) {
+    const double c = -tot[0] * scale;
+    GRID_STRIDE(q, n) a[q] += c;
+}
+__global__ void k_axpy2(double* x, double* r, const double* p, const double* Ap, long long n, double al,
+                        unsigned long long* rmax) {
+    double v = 0.0;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        x[q] += al * p[q];
+        r[q] -= al * Ap[q];
+        v = dmax(v, fabs(r[q]));
+    }
+    for (int o = 16; o > 0; o >>= 1) v = dmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(rmax, (unsigned long long)__double_as_longlong(v));
+}
+__global__ void k_xpby(const double* z, double* p, long long n, double be) {
+    GRID_STRIDE(q, n) p[q] = z[q] + be * p[q];
+}
+__global__ void k_neg(double* a, long long n) {
+    GRID_STRIDE(q, n) a[q] = -a[q];
+}
+
+}  // namespace
+
+struct PfLevel {
+    PfDims m;
+    int ia;                                  // component of alpha1 in the state
+    long long S, upx, upxy;                  // padded state layout
+    int ung, ugz;
+    double* pfb0 = nullptr;                  // phase field at the step start (padded)
+    double* pfb = nullptr;                   // mechanism iterate (padded)
+    double* pfo = nullptr;                   // previous iterate (valid)
+    double* nrm = nullptr;                   // normals (padded, D components)
+    double* ls = nullptr;                    // ACDI level set (padded)
+    double* mech = nullptr;
+    double* wgt = nullptr;
+    double* J[3] = {nullptr, nullptr, nullptr};
+    double* Jhat[3] = {nullptr, nullptr, nullptr};
+    double* gq[3] = {nullptr, nullptr, nullptr};
+    double* partial = nullptr;               // 2 x kRedBlocks
+    double* tot = nullptr;                   // 2 doubles
+    unsigned long long* umax = nullptr;      // max reductions (bits)
+    double* dt_slot = nullptr;
+    // multigrid levels and the conjugate-gradient vectors of the finest one
+    std::vector<MgLevel> mg;
+    double *z = nullptr, *p = nullptr, *Ap = nullptr;
+    long long bytes = 0;
+    std::vector<void*> allocs;
+};
+
+namespace {
+
+cudaError_t dalloc(PfLevel* pf, double** ptr, long long n) {
+    if (n < 1) n = 1;
+    cudaError_t e = cudaMalloc((void**)ptr, sizeof(double) * n);
+    if (e != cudaSuccess) return e;
+    pf->allocs.push_back(*ptr);
+    pf->bytes += sizeof(double) * n;
+    return cudaMemset(*ptr, 0, sizeof(double) * n);
+}
+
+bool coarsenable(const PfDims& m) {
+    for (int d = 0; d < m.D; ++d)
+        if (m.n[d] % 2 != 0 || m.n[d] < 4) return false;
+    return true;
+}
+
+#define PF_TRY(call)                                                                          \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) {                                                              \
+            if (err) *err = std::string(#call) + ": " + cudaGetErrorString(e_);               \
+            return COMPAS_B200_ECUDA;                                                         \
+        }                                                                                     \
+    } while (0)
+
+double read_max(unsigned long long* dev, cudaStream_t st) {
+    unsigned long long h = 0;
+    cudaMemcpyAsync(&h, dev, sizeof(h), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    double v;
+    std::memcpy(&v, &h, sizeof(v));
+    return v;
+}
+
+// one V-cycle on level l (x_l from its current value, b_l given)
+cudaError_t vcycle(PfLevel* pf, int l, cudaStream_t st) {
+    MgLevel& L = pf->mg[l];
+    const unsigned nb = blocks_for(L.m.nv);
+    auto smooth = [&](int sweeps, bool reverse) {
+        for (int s = 0; s < sweeps; ++s) {
+            if (L.rb) {
+                k_mg_rb<<<nb, kThreads, 0, st>>>(L, reverse ? 1 : 0);
+                k_mg_rb<<<nb, kThreads, 0, st>>>(L, reverse ? 0 : 1);
+            } else {
+                k_mg_jacobi<<<nb, kThreads, 0, st>>>(L);
+                k_copy<<<nb, kThreads, 0, st>>>(L.r, L.x, L.m.nv);
+            }
+        }
+    };
+    if (l + 1 == (int)pf->mg.size()) {
+        smooth(L.m.nv <= 64 ? 64 : 16, false);
+        smooth(L.m.nv <= 64 ? 64 : 16, true);
+        return cudaGetLastError();
+    }
+    smooth(2, false);
+    k_mg_residual<<<nb, kThreads, 0, st>>>(L);
+    MgLevel& C = pf->mg[l + 1];
+    k_mg_restrict<<<blocks_for(C.m.nv), kThreads, 0, st>>>(L.r, L.m, C.b, C.m);
+    k_zero<<<blocks_for(C.m.nv), kThreads, 0, st>>>(C.x, C.m.nv);
+    cudaError_t e = vcycle(pf, l + 1, st);
+    if (e != cudaSuccess) return e;
+    k_mg_prolong<<<nb, kThreads, 0, st>>>(C.x, C.m, L.x, L.m);
+    smooth(2, true);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+int pf_create(const compas_b200_parm* p, const compas_b200_geom* g, PfLevel** out, std::string* err) {
+    PfLevel* pf = new PfLevel();
+    int per[3] = {0, 0, 0};
+    for (int d = 0; d < p->dim; ++d) per[d] = (g->lo_bc[d] == 0);
+    pf->m = make_dims(p->dim, g->n, g->dx, per);
+    const PfDims& m = pf->m;
+    pf->ia = 3 + p->dim;
+    pf->ung = g->ng;
+    pf->ugz = (p->dim == 3) ? g->ng : 0;
+    pf->upx = g->n[0] + 2LL * g->ng;
+    pf->upxy = pf->upx * (g->n[1] + 2LL * g->ng);
+    pf->S = pf->upxy * ((p->dim == 3 ? g->n[2] : 1) + 2LL * pf->ugz);
+    auto fail_out = [&](cudaError_t e) {
+        if (err) *err = std::string("Phase-Field work arrays: ") + cudaGetErrorString(e);
+        pf_destroy(pf);
+        return COMPAS_B200_ENOMEM;
+    };
+    cudaError_t e;
+    if ((e = dalloc(pf, &pf->pfb0, m.ps)) || (e = dalloc(pf, &pf->pfb, m.ps)) || (e = dalloc(pf, &pf->pfo, m.nv)) ||
+        (e = dalloc(pf, &pf->nrm, m.ps * m.D)) || (e = dalloc(pf, &pf->ls, m.ps)) || (e = dalloc(pf, &pf->mech, m.nv)) ||
+        (e = dalloc(pf, &pf->wgt, m.nv)) || (e = dalloc(pf, &pf->partial, 2 * kRedBlocks)) ||
+        (e = dalloc(pf, &pf->tot, 2)) || (e = dalloc(pf, &pf->dt_slot, 1)))
+        return fail_out(e);
+    if ((e = dalloc(pf, (double**)&pf->umax, 1))) return fail_out(e);
+    for (int d = 0; d < m.D; ++d)
+        if ((e = dalloc(pf, &pf->J[d], m.nf[d])) || (e = dalloc(pf, &pf->Jhat[d], m.nf[d])) ||
+            (e = dalloc(pf, &pf->gq[d], m.nf[d])))
+            return fail_out(e);
+    // multigrid hierarchy
+    PfDims lm = m;
+    for (int l = 0; l < kMaxLevels; ++l) {
+        MgLevel L;
+        L.m = lm;
+        L.rb = true;
+        for (int d = 0; d < lm.D; ++d)
+            if (lm.periodic[d] && (lm.n[d] % 2)) L.rb = false;
+        for (int d = 0; d < lm.D; ++d)
+            if ((e = dalloc(pf, &L.beta[d], lm.nf[d]))) return fail_out(e);
+        if ((e = dalloc(pf, &L.x, lm.nv)) || (e = dalloc(pf, &L.b, lm.nv)) || (e = dalloc(pf, &L.r, lm.nv)))
+            return fail_out(e);
+        pf->mg.push_back(L);
+        if (!coarsenable(lm) || lm.nv <= 16) break;
+        int nc[3] = {lm.n[0] / 2, lm.n[1] / 2, lm.D == 3 ? lm.n[2] / 2 : 1};
+        double dc[3] = {2 * lm.dx[0], 2 * lm.dx[1], lm.D == 3 ? 2 * lm.dx[2] : 1.0};
+        lm = make_dims(lm.D, nc, dc, lm.periodic);
+    }
+    if ((e = dalloc(pf, &pf->z, m.nv)) || (e = dalloc(pf, &pf->p, m.nv)) || (e = dalloc(pf, &pf->Ap, m.nv)))
+        return fail_out(e);
+    *out = pf;
+    return COMPAS_B200_OK;
+}
+
+void pf_destroy(PfLevel* pf) {
+    if (!pf) return;
+    for (void* a : pf->allocs) cudaFree(a);
+    delete pf;
+}
+
+const double* pf_gq(const PfLevel* pf, int d) { return pf->gq[d]; }
+double* pf_dt_slot(PfLevel* pf) { return pf->dt_slot; }
+long long pf_bytes(const PfLevel* pf) { return pf ? pf->bytes : 0; }
+
+namespace {
+
+// sum of a finest-level vector (fixed order) into pf->tot[0]
+cudaError_t vsum(PfLevel* pf, const double* a, cudaStream_t st) {
+    const PfDims& m = pf->mg[0].m;
+    k_dot<<<kRedBlocks, kThreads, 0, st>>>(a, nullptr, m.nv, pf->partial);
+    k_reduce2<<<1, kThreads, 0, st>>>(pf->partial, kRedBlocks, pf->tot);
+    return cudaGetLastError();
+}
+
+double dot_host(PfLevel* pf, const double* a, const double* b, cudaStream_t st) {
+    const PfDims& m = pf->mg[0].m;
+    k_dot<<<kRedBlocks, kThreads, 0, st>>>(a, b, m.nv, pf->partial);
+    k_reduce2<<<1, kThreads, 0, st>>>(pf->partial, kRedBlocks, pf->tot);
+    double h[2];
+    cudaMemcpyAsync(h, pf->tot, sizeof(h), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    return h[0];
+}
+
+}  // namespace
+
+int pf_grad_q(PfLevel* pf, const compas_b200_parm* p, const double* U, double dt, cudaStream_t st, PfInfo* info,
+              std::string* err) {
+    const PfDims& m = pf->m;
+    const unsigned nbv = blocks_for(m.nv), nbp = blocks_for(m.ps);
+    // MaxVelocity and the parameters PhaseField_Evolve derives (:426-463)
+    PF_TRY(cudaMemsetAsync(pf->umax, 0, sizeof(unsigned long long), st));
+    k_maxv<<<nbv, kThreads, 0, st>>>(U, pf->S, pf->upx, pf->upxy, pf->ung, pf->ugz, m, pf->umax);
+    PF_TRY(cudaGetLastError());
+    const double vmax = read_max(pf->umax, st);
+    const double lam = (p->pf_lambda <= 0.0) ? 1.0 : p->pf_lambda;
+    double eta = p->pf_eta;
+    if (eta <= 0.0) {
+        double dxm = m.dx[0];
+        for (int d = 1; d < m.D; ++d) dxm = std::max(dxm, m.dx[d]);
+        eta = p->pf_eta_multiplier * dxm;
+    }
+    double mob = 1.0;
+    mob *= 0.5 * eta * vmax;
+    // PFBorder of the state
+    k_extract<<<nbv, kThreads, 0, st>>>(U, pf->S, pf->upx, pf->upxy, pf->ung, pf->ugz, pf->ia, m, pf->pfb0);
+    k_fill<<<nbp, kThreads, 0, st>>>(pf->pfb0, 1, m);
+    PF_TRY(cudaMemcpyAsync(pf->pfb, pf->pfb0, sizeof(double) * m.ps, cudaMemcpyDeviceToDevice, st));
+    const bool acdi = (p->pf_mechanism == 3);
+    const bool explicit_rc = acdi && p->pf_explicit_rc;
+    if (explicit_rc)
+        for (int d = 0; d < m.D; ++d) PF_TRY(cudaMemsetAsync(pf->Jhat[d], 0, sizeof(double) * m.nf[d], st));
+    // PhaseFieldMechanism_Evolve (:596-711)
+    double mdt = 0.9 / (2.0 * mob * lam);
+    {
+        double s = 0.0;
+        for (int d = 0; d < m.D; ++d) s = (d == 0) ? 1.0 / m.dx[d] / m.dx[d] : s + 1.0 / m.dx[d] / m.dx[d];
+        mdt = mdt / (s + 1.0 / eta / eta);
+    }
+    double mt = 0.0;
+    const double T = dt;
+    int msteps = 0;
+    while (mt < T) {
+        if (mt + mdt > T) mdt = T - mt;
+        k_copy_valid<<<nbv, kThreads, 0, st>>>(pf->pfb, pf->pfo, m);
+        k_fill<<<nbp, kThreads, 0, st>>>(pf->pfb, 1, m);
+        if (!acdi) {
+            k_normal<<<nbv, kThreads, 0, st>>>(pf->pfb, pf->nrm, m);
+            k_fill<<<nbp, kThreads, 0, st>>>(pf->nrm, m.D, m);
+            k_cac_mech<<<kRedBlocks, kThreads, 0, st>>>(pf->pfb, pf->nrm, m, mob, lam, eta, pf->mech, pf->wgt, pf->partial);
+            k_reduce2<<<1, kThreads, 0, st>>>(pf->partial, kRedBlocks, pf->tot);
+            k_cac_update<<<nbv, kThreads, 0, st>>>(pf->mech, pf->wgt, pf->tot, pf->pfo, pf->pfb, m, mdt);
+        } else {
+            k_ls<<<nbv, kThreads, 0, st>>>(pf->pfb, pf->ls, m, eta);
+            k_fill<<<nbp, kThreads, 0, st>>>(pf->ls, 1, m);
+            k_normal<<<nbv, kThreads, 0, st>>>(pf->ls, pf->nrm, m);
+            k_fill<<<nbp, kThreads, 0, st>>>(pf->nrm, m.D, m);
+            for (int d = 0; d < m.D; ++d)
+                k_acdi_flux<<<blocks_for(m.nf[d]), kThreads, 0, st>>>(pf->pfb, pf->nrm, m, d, mob, eta, pf->J[d],
+                                                                      explicit_rc ? pf->Jhat[d] : nullptr, mdt);
+            k_div_update<<<nbv, kThreads, 0, st>>>(pf->J[0], pf->J[1], pf->J[2], pf->pfo, pf->pfb, m, mdt);
+        }
+        PF_TRY(cudaGetLastError());
+        mt += mdt;
+        ++msteps;
+    }
+    int iters = 0;
+    double res = 0.0;
+    const double eta_f = p->pf_eta_factor;
+    if (explicit_rc) {
+        for (int d = 0; d < m.D; ++d)
+            k_gq_explicit<<<blocks_for(m.nf[d]), kThreads, 0, st>>>(pf->pfb0, pf->Jhat[d], m, d, 1.0 / dt, eta, eta_f,
+                                                                    pf->gq[d]);
+        PF_TRY(cudaGetLastError());
+    } else {
+        // PhaseField_GradQPF, implicit (:2132-2310): div(beta grad Q) = Div_Jhat
+        MgLevel& F = pf->mg[0];
+        k_djhat<<<kRedBlocks, kThreads, 0, st>>>(pf->pfb, pf->pfb0, m, 1.0 / dt, F.b, pf->partial);
+        k_reduce2<<<1, kThreads, 0, st>>>(pf->partial, kRedBlocks, pf->tot);
+        k_add_const<<<nbv, kThreads, 0, st>>>(F.b, m.nv, pf->tot, 1.0 / (double)m.nv);  // solvable (zero mean)
+        k_neg<<<nbv, kThreads, 0, st>>>(F.b, m.nv);  // A = -div(beta grad): A Q = -Div_Jhat
+        for (int d = 0; d < m.D; ++d)
+            k_beta<<<blocks_for(m.nf[d]), kThreads, 0, st>>>(pf->pfb0, m, d, eta, eta_f, F.beta[d]);
+        for (size_t l = 1; l < pf->mg.size(); ++l)
+            for (int d = 0; d < m.D; ++d)
+                k_mg_beta<<<blocks_for(pf->mg[l].m.nf[d]), kThreads, 0, st>>>(pf->mg[l - 1].beta[d], pf->mg[l - 1].m,
+                                                                               pf->mg[l].beta[d], pf->mg[l].m, d);
+        PF_TRY(cudaGetLastError());
+        // preconditioned conjugate gradients on the mean-free space; r lives in F.r, the solution in Q
+        double* x = pf->pfo;      // the mechanism iterate is no longer needed: hold the solution here
+        double* r = pf->mech;     // residual
+        k_zero<<<nbv, kThreads, 0, st>>>(x, m.nv);
+        k_copy<<<nbv, kThreads, 0, st>>>(F.b, r, m.nv);
+        PF_TRY(cudaMemsetAsync(pf->umax, 0, sizeof(unsigned long long), st));
+        k_maxabs<<<nbv, kThreads, 0, st>>>(r, m.nv, pf->umax);
+        const double bnorm = read_max(pf->umax, st);
+        auto precond = [&](const double* in, double* outz) -> cudaError_t {
+            // z = V(in) with a zero start, made mean-free
+            k_copy<<<nbv, kThreads, 0, st>>>(in, F.b, m.nv);
+            k_zero<<<nbv, kThreads, 0, st>>>(F.x, m.nv);
+            cudaError_t e = vcycle(pf, 0, st);
+            if (e != cudaSuccess) return e;
+            k_copy<<<nbv, kThreads, 0, st>>>(F.x, outz, m.nv);
+            vsum(pf, outz, st);
+            k_add_const<<<nbv, kThreads, 0, st>>>(outz, m.nv, pf->tot, 1.0 / (double)m.nv);
+            return cudaGetLastError();
+        };
+        const double tol = p->pf_tol_rel;
+        if (bnorm > 0.0) {
+            PF_TRY(precond(r, pf->z));
+            k_copy<<<nbv, kThreads, 0, st>>>(pf->z, pf->p, m.nv);
+            double rz = dot_host(pf, r, pf->z, st);
+            res = 1.0;
+            for (iters = 0; iters < 1000;) {
+                k_mg_apply<<<nbv, kThreads, 0, st>>>(F, pf->p, pf->Ap);
+                const double pAp = dot_host(pf, pf->p, pf->Ap, st);
+                if (!(pAp > 0.0)) break;
+                const double al = rz / pAp;
+                PF_TRY(cudaMemsetAsync(pf->umax, 0, sizeof(unsigned long long), st));
+                k_axpy2<<<nbv, kThreads, 0, st>>>(x, r, pf->p, pf->Ap, m.nv, al, pf->umax);
+                ++iters;
+                res = read_max(pf->umax, st) / bnorm;
+                if (res <= tol) break;
+                PF_TRY(precond(r, pf->z));
+                const double rz2 = dot_host(pf, r, pf->z, st);
+                const double be = rz2 / rz;
+                rz = rz2;
+                k_xpby<<<nbv, kThreads, 0, st>>>(pf->z, pf->p, m.nv, be);
+            }
+        } else {
+            res = 0.0;
+        }
+        for (int d = 0; d < m.D; ++d) k_gq_from_q<<<blocks_for(m.nf[d]), kThreads, 0, st>>>(x, m, d, pf->gq[d]);
+        PF_TRY(cudaGetLastError());
+    }
+    // max |grad Q| (PhaseField_ComputeDt)
+    PF_TRY(cudaMemsetAsync(pf->umax, 0, sizeof(unsigned long long), st));
+    for (int d = 0; d < m.D; ++d) k_maxabs<<<blocks_for(m.nf[d]), kThreads, 0, st>>>(pf->gq[d], m.nf[d], pf->umax);
+    PF_TRY(cudaGetLastError());
+    const double gmax = read_max(pf->umax, st);
+    if (info) {
+        info->max_v = vmax;
+        info->mobility = mob;
+        info->eta = eta;
+        info->mech_steps = msteps;
+        info->solve_iters = iters;
+        info->solve_res = res;
+        info->gmax = gmax;
+    }
+    return COMPAS_B200_OK;
+}
+
+}  // namespace compas

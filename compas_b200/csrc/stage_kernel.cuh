@@ -60,11 +60,16 @@ struct StageArgs {
     int relax;
     double trace;
     Thinc thinc;               // used by the THINC kernels only
+    const double* gq[3];       // Phase-Field kernels: face gradients of the potential Q per direction
 };
+
+// Variants of the stage kernel (the VAR template argument of stage_tile).
+enum { kVarPlain = 0, kVarThinc = 1, kVarPhaseField = 2 };
 
 }  // namespace compas
 
 #include "thinc.cuh"
+#include "pf_flux.cuh"
 
 namespace compas {
 
@@ -96,11 +101,17 @@ __device__ __forceinline__ void load_cons(double* U, const double* base, const G
 // primitives are recovered in FP64 (pressure from total energy) and kept in shared memory as FP32,
 // the reconstruction runs in FP32, the Riemann solver, divergence, stage accumulation and
 // relaxation in FP64.
-// TH: THINC interface reconstruction on top of the scheme (FiniteVolume.THINC = 1).
+// VAR: kVarPlain - the hyperbolic right-hand side; kVarThinc - with THINC interface reconstruction
+// (FiniteVolume.THINC = 1); kVarPhaseField - the Phase-Field regularisation right-hand side (the
+// same face states, the regularisation flux of the face gradient a.gq instead of the Riemann flux,
+// no non-conservative terms; FIVEEQS).
 // The work of one CTA on tile `tile` of the box described by `a` (tiles numbered x fastest).
-template <class M, int SCHEME, bool MIX, bool TH, int TX, int TY, int TZ, int NT>
+template <class M, int SCHEME, bool MIX, int VAR, int TX, int TY, int TZ, int NT>
 __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double* smem_d) {
     static_assert(TX == TY && (M::D == 2 ? TZ == 1 : TZ == TX), "tiles are cubes (squares in 2D)");
+    constexpr bool TH = (VAR == kVarThinc);
+    constexpr bool PFX = (VAR == kVarPhaseField);
+    static_assert(!PFX || M::NC == 1, "the Phase-Field kernel is the five-equation model's");
     using PT = typename std::conditional<MIX, float, double>::type;
     using T = TileShape<M, TX, TY, TZ, PT>;
     constexpr int N = M::N, NC = M::NC, D = M::D, NB = T::NB;
@@ -252,7 +263,13 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                     M::prim2cons(UL, WfL, a.e, err);
                     M::prim2cons(UR, WfR, a.e, err);
                 }
-                M::hllc(F, fnc, cm, UL, UR, a.e, d, a.id_k, err);
+                if constexpr (PFX) {
+                    pf_face_flux<D>(F, UL, UR, pf_face_gq(a, d, gi, gj, gk), a.e, err);
+                    fnc[0] = 0.0;
+                    cm = 0.0;
+                } else {
+                    M::hllc(F, fnc, cm, UL, UR, a.e, d, a.id_k, err);
+                }
             } else {
                 float wL[N], wR[N];
                 if (thinc_face) {
@@ -287,10 +304,15 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                     M::prim2cons(UR, WfR, a.e, err);
                 }
                 float cmf;
-                if constexpr (M::NC == 1)
+                if constexpr (PFX) {
+                    pf_face_flux<D>(F, UL, UR, pf_face_gq(a, d, gi, gj, gk), a.e, err);
+                    fnc[0] = 0.0;
+                    cmf = 0.0f;
+                } else if constexpr (M::NC == 1) {
                     fiveeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, a.e, d, a.id_k);
-                else
+                } else {
                     sixeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, a.e, d);
+                }
                 cm = cmf;
             }
 #pragma unroll
@@ -359,7 +381,10 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
             }
 #pragma unroll
             for (int n = 0; n < N; ++n) L[n] = -acc[r][n];
-            if constexpr (M::NC == 1) {
+            if constexpr (PFX) {
+                // the Phase-Field step has no non-conservative terms in the five-equation model
+                // (include/Operators_Compressible5Eq_PhaseField/FVM_PhaseField_SurfaceIntegralNC_Compressible5Eq_PhaseField.H)
+            } else if constexpr (M::NC == 1) {
                 // five-equation: alpha1 += phi1 (1 + K1) div u*
                 const double fac = M::kapila_factor(W, W, a.e, a.id_k, err);
                 L[M::IA] = L[M::IA] + fac * acc[r][N];
@@ -424,11 +449,11 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
 }
 
 // One box: one CTA per tile.
-template <class M, int SCHEME, bool MIX, bool TH, int TX, int TY, int TZ, int NT, int MINB>
+template <class M, int SCHEME, bool MIX, int VAR, int TX, int TY, int TZ, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
     if (a.done && *a.done) return;
     extern __shared__ double smem_d[];
-    stage_tile<M, SCHEME, MIX, TH, TX, TY, TZ, NT>(a, blockIdx.x, smem_d);
+    stage_tile<M, SCHEME, MIX, VAR, TX, TY, TZ, NT>(a, blockIdx.x, smem_d);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -495,7 +520,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_list_kernel(ListArgs L) {
         a.relax = B.relax;
         a.trace = B.trace;
         __syncthreads();  // the previous tile's readers of shared memory are done
-        stage_tile<M, SCHEME, MIX, false, TX, TY, TZ, NT>(a, w - L.tile_off[b], smem_d);
+        stage_tile<M, SCHEME, MIX, kVarPlain, TX, TY, TZ, NT>(a, w - L.tile_off[b], smem_d);
     }
 }
 

@@ -70,6 +70,19 @@ typedef struct compas_b200_parm {
      * with the reference; 1 mixed: FP32 reconstruction, FP64 pressure recovery, Riemann solver,
      * stage accumulation and relaxation */
     int precision;
+    /* PhaseField.* (include/Physics_PhaseField/PhaseField_Parameter.H:25-117) and LinearSystem.tol_rel
+     * (include/Operators_LinearSystem/LinearSystem_Parameter.H:27): the regularisation step after
+     * every hyperbolic step (FIVEEQS) */
+    int phase_field;          /* PhaseField.phase_field */
+    int pf_mechanism;         /* PhaseField.Mechanism: 1 CAC-Adv, 3 ACDI (the reference's ID_Mechanism) */
+    int pf_explicit_rc;       /* PhaseField.ID_ExplicitRC: 0 elliptic solve, 1 explicit (flux-based only) */
+    double pf_lambda;         /* PhaseField.Lambda (<= 0: 1) */
+    double pf_eta;            /* PhaseField.Eta (<= 0: Eta_Multiplier x the largest cell size) */
+    double pf_eta_factor;     /* PhaseField.Eta_Factor */
+    double pf_eta_multiplier; /* PhaseField.Eta_Multiplier */
+    double pf_cfl;            /* PhaseField.cfl */
+    int pf_max_step;          /* PhaseField.max_step */
+    double pf_tol_rel;        /* LinearSystem.tol_rel */
 } compas_b200_parm;
 
 /* One box covering a single-level domain (the valid cells), its ghost width and its boundary codes
@@ -138,6 +151,34 @@ int compas_b200_rk3_stage(const compas_b200_parm* p, const compas_b200_geom* g, 
 int compas_b200_relaxation(const compas_b200_parm* p, const compas_b200_geom* g, double* U, unsigned int* err_dev,
                            void* stream);
 
+/* ---- Phase-Field regularisation (FIVEEQS; PhaseField.phase_field = 1) ---------------------------
+ * The level advance runs the Phase-Field step after every hyperbolic step by itself. The entry
+ * points below expose its pieces to a host that keeps the reference's Phase-Field loop. Face arrays
+ * gq_d are nodal in direction d: (n[0]+(d==0)) x (n[1]+(d==1)) x (n[2]+(d==2)) doubles, x fastest. */
+
+/* Mechanism pseudo-time evolution over dt and the face gradients of the regularisation potential Q
+ * for the padded state U: replaces PhaseFieldMechanism_Evolve + PhaseField_GradQPF
+ * (source/Class_Compressible_PhaseField.cpp:596-711, :2132-2401) as PhaseField_Evolve (:424-545) calls
+ * them. The implicit approach solves div(beta grad Q) = Div_Jhat with this engine's multigrid-
+ * preconditioned conjugate gradients to LinearSystem.tol_rel (the reference uses AMReX MLMG).
+ * Synchronous (the reference's loop reads the same scalars on the host); allocates work arrays.
+ * info (host, 7 doubles, may be NULL): max|u|, mobility, eta, mechanism sub-steps, solver iterations,
+ * max|grad Q|, final relative residual. */
+int compas_b200_pf_grad_q(const compas_b200_parm* p, const compas_b200_geom* g, const double* U, double dt,
+                          double* gq0, double* gq1, double* gq2, double* info, void* stream);
+
+/* Phase-Field right-hand side of the padded state U (ghosts filled) into dUdt: replaces
+ * PhaseField_compute_dUdt_FV (source/Class_Compressible_PhaseField.cpp:950-1004). */
+int compas_b200_pf_compute_dUdt(const compas_b200_parm* p, const compas_b200_geom* g, const double* U, double* dUdt,
+                                const double* gq0, const double* gq1, const double* gq2, unsigned int* err_dev,
+                                void* stream);
+
+/* One stage of PhaseField_ThirdOrderSSPRK (source/Class_Compressible_PhaseField.cpp:2619-2752): the
+ * Phase-Field right-hand side of Us and the stage combination with Uold, dt read from device memory. */
+int compas_b200_pf_rk3_stage(const compas_b200_parm* p, const compas_b200_geom* g, int stage, const double* Us,
+                             const double* Uold, double* Unew, const double* dt_dev, const double* gq0,
+                             const double* gq1, const double* gq2, unsigned int* err_dev, void* stream);
+
 /* One TVD-RK3 step of size dt (stages 0-2 with their boundary fills and, for SIXEQS, the pressure
  * relaxation) in place on the caller-owned state U, WITHOUT ALLOCATING ANY DEVICE MEMORY. This entry
  * point has no counterpart in the reference. It is for callers that cannot call cudaMalloc - code
@@ -193,6 +234,9 @@ int compas_b200_level_dts(compas_b200_level* lv, double* dts, int n);
 
 /* Kernel launches the library enqueued on this level since upload. */
 long long compas_b200_level_launches(compas_b200_level* lv);
+
+/* Phase-Field sub-steps taken by the level so far (0 without PhaseField.phase_field). */
+long long compas_b200_level_pf_substeps(const compas_b200_level* lv);
 
 /* ---- batched independent cases ------------------------------------------------------------------
  * Many single-box cases of uneven size (each with its own EOS, boundary codes, stop time, step budget

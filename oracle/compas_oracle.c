@@ -1049,3 +1049,19 @@ int cmp_advance(const cmp_case* c, double* U, int nsteps, double stop_time, doub
     *t = time;
     return taken;
 }
+
+/* The Phase-Field step is in the reference-header build (oracle/ref_driver.cpp) only. */
+int cmp_pf_step(const cmp_case* c, const cmp_pf* pf, double* U, double dt, double* info) {
+    (void)c; (void)pf; (void)U; (void)dt; (void)info;
+    return -2;
+}
+int cmp_pf_grad_q(const cmp_case* c, const cmp_pf* pf, const double* U, double dt, double* gq0, double* gq1,
+                  double* gq2, double* info) {
+    (void)c; (void)pf; (void)U; (void)dt; (void)gq0; (void)gq1; (void)gq2; (void)info;
+    return -2;
+}
+int cmp_advance_pf(const cmp_case* c, const cmp_pf* pf, double* U, int nsteps, double stop_time, double* t,
+                   double* dts) {
+    (void)c; (void)pf; (void)U; (void)nsteps; (void)stop_time; (void)t; (void)dts;
+    return -2;
+}

@@ -62,7 +62,32 @@ _SIGS = {
     "cmp_rk3_step": (ctypes.c_int, [_P, _D, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
     "cmp_advance": (ctypes.c_int, [_P, _D, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_double), _D]),
     "cmp_threads": (ctypes.c_int, []),
+    "cmp_pf_step": (ctypes.c_int, [_P, ctypes.c_void_p, _D, ctypes.c_double, _D]),
+    "cmp_pf_grad_q": (ctypes.c_int, [_P, ctypes.c_void_p, _D, ctypes.c_double, _D, _D, _D, _D]),
+    "cmp_advance_pf": (ctypes.c_int, [_P, ctypes.c_void_p, _D, ctypes.c_int, ctypes.c_double,
+                                      ctypes.POINTER(ctypes.c_double), _D]),
 }
+
+
+class PfCase(ctypes.Structure):
+    """ctypes mirror of ``cmp_pf`` (oracle/oracle_api.h)."""
+
+    _fields_ = [
+        ("mechanism", ctypes.c_int), ("explicit_rc", ctypes.c_int),
+        ("lambda_", ctypes.c_double), ("eta", ctypes.c_double), ("eta_factor", ctypes.c_double),
+        ("eta_multiplier", ctypes.c_double), ("cfl", ctypes.c_double), ("max_step", ctypes.c_int),
+        ("tol_rel", ctypes.c_double),
+    ]
+
+
+def pf_from(parm, tol_rel=None) -> PfCase:
+    """Oracle Phase-Field parameters from a compas_b200 Parm (tol_rel overrides LinearSystem.tol_rel)."""
+    q = PfCase()
+    q.mechanism, q.explicit_rc = parm.pf_mechanism, parm.pf_explicit_rc
+    q.lambda_, q.eta, q.eta_factor = parm.pf_lambda, parm.pf_eta, parm.pf_eta_factor
+    q.eta_multiplier, q.cfl, q.max_step = parm.pf_eta_multiplier, parm.pf_cfl, parm.pf_max_step
+    q.tol_rel = parm.pf_tol_rel if tol_rel is None else tol_rel
+    return q
 
 _cache: dict = {}
 
@@ -168,6 +193,41 @@ class Oracle:
         dts = np.zeros(max(nsteps, 1), dtype=np.float64)
         n = self._call(self.lib.cmp_advance(self._c, U.ctypes.data, nsteps, stop_time,
                                             ctypes.byref(t), dts.ctypes.data))
+        return t.value, dts[:n]
+
+    # ---- Phase-Field step (reference-header build only) ----------------------------------------
+    def _pf(self, pf):
+        if self.kind != "reference":
+            raise RuntimeError("the Phase-Field step is in the reference-header oracle only")
+        return ctypes.byref(pf)
+
+    def pf_step(self, U: np.ndarray, pf, dt: float):
+        info = np.zeros(6)
+        self._call(self.lib.cmp_pf_step(self._c, self._pf(pf), U.ctypes.data, dt, info.ctypes.data))
+        return info
+
+    def pf_grad_q(self, U: np.ndarray, pf, dt: float):
+        c = self.case
+        dim = c.dim
+        n = [c.n[0], c.n[1], c.n[2] if dim == 3 else 1]
+        out = []
+        for d in range(3):
+            if d < dim:
+                shp = [n[2] + (d == 2), n[1] + (d == 1), n[0] + (d == 0)]
+                out.append(np.zeros(shp))
+            else:
+                out.append(None)
+        info = np.zeros(6)
+        ptr = [o.ctypes.data if o is not None else None for o in out]
+        self._call(self.lib.cmp_pf_grad_q(self._c, self._pf(pf), U.ctypes.data, dt, ptr[0], ptr[1], ptr[2],
+                                          info.ctypes.data))
+        return out[:dim], info
+
+    def advance_pf(self, U: np.ndarray, pf, nsteps: int, stop_time: float = 1e300, t0: float = 0.0):
+        t = ctypes.c_double(t0)
+        dts = np.zeros(max(nsteps, 1), dtype=np.float64)
+        n = self._call(self.lib.cmp_advance_pf(self._c, self._pf(pf), U.ctypes.data, nsteps, stop_time,
+                                               ctypes.byref(t), dts.ctypes.data))
         return t.value, dts[:n]
 
     def threads(self) -> int:

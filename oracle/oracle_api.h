@@ -68,6 +68,36 @@ int cmp_advance(const cmp_case* c, double* U, int nsteps, double stop_time, doub
 /* Threads the library uses (OpenMP builds); 1 otherwise. */
 int cmp_threads(void);
 
+/* Phase-Field regularisation step (FIVEEQS; PhaseField_Evolve, source/Class_Compressible_PhaseField.cpp:
+ * 424-595). The reference-header build implements it; the plain-C port returns -2. */
+typedef struct cmp_pf {
+    int mechanism;          /* PhaseField ID_Mechanism: 1 CAC-Adv, 3 ACDI (PhaseField_Parameter.H:66-110) */
+    int explicit_rc;        /* PhaseField.ID_ExplicitRC: 0 implicit (elliptic solve), 1 explicit */
+    double lambda;          /* PhaseField.Lambda (<= 0: 1) */
+    double eta;             /* PhaseField.Eta (<= 0: Eta_Multiplier x the largest cell size) */
+    double eta_factor;      /* PhaseField.Eta_Factor */
+    double eta_multiplier;  /* PhaseField.Eta_Multiplier */
+    double cfl;             /* PhaseField.cfl */
+    int max_step;           /* PhaseField.max_step */
+    double tol_rel;         /* LinearSystem.tol_rel of the elliptic solve */
+} cmp_pf;
+
+/* One Phase-Field step after a hyperbolic step of size dt: mechanism pseudo-time evolution, the
+ * regularisation potential gradient on faces, and the sub-stepped TVD-RK3 advance of U over dt.
+ * info (may be NULL) receives {max |u|, mobility, eta, mechanism sub-steps, Phase-Field sub-steps,
+ * max |grad Q|}. */
+int cmp_pf_step(const cmp_case* c, const cmp_pf* pf, double* U, double dt, double* info);
+
+/* The face gradients grad Q (component d in gq[d], nodal in direction d, (n[d]+1) faces, x fastest)
+ * that cmp_pf_step computes for U and dt, without advancing U. */
+int cmp_pf_grad_q(const cmp_case* c, const cmp_pf* pf, const double* U, double dt, double* gq0, double* gq1,
+                  double* gq2, double* info);
+
+/* cmp_advance with a Phase-Field step after every hyperbolic step (Evolve, source/
+ * Class_Compressible_PhaseField.cpp:171-330). */
+int cmp_advance_pf(const cmp_case* c, const cmp_pf* pf, double* U, int nsteps, double stop_time, double* t,
+                   double* dts);
+
 #ifdef __cplusplus
 }
 #endif

@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-steps", type=int, default=10)
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-phase-field", action="store_true")
+    ap.add_argument("--pf-steps", type=int, default=10)
     ap.add_argument("--serve-requests", type=int, default=16)
     ap.add_argument("--serve-rate", type=float, default=16.0)
     return ap.parse_args()
@@ -205,6 +207,55 @@ def run_batched(args):
         out[f"sequential_{prec}"] = cells * 3 * K / (tot / 1e3)
     out["unit"] = UNIT + " per RK stage (aggregate over the cases)"
     out["batched_mixed_vs_sequential_fp64"] = out["batched_mixed"] / out["sequential_fp64"]
+    return out
+
+
+def run_phase_field(args):
+    """2D shock-helium-bubble with the CAC Phase-Field regularisation (the reference's configuration:
+    2048 x 1024 cells on [0,2]x[0,1], WENO5B + HLLC, CAC-Adv with the implicit regularisation
+    potential, eta = dx): hyperbolic step + Phase-Field step per coarse step, both precisions, against
+    the same steps without the Phase-Field step. Timed with CUDA events around whole steps (the
+    Phase-Field host loop reads dt, max|u| and max|grad Q| each step, as the reference's does)."""
+    import torch
+
+    import compas_b200 as cb
+    from compas_b200 import cases
+
+    stream = torch.cuda.current_stream()
+    phys, dim, inputs, geom, U = cases.shock_bubble(nx=2048, ny=1024, xp=torch, device="cuda")
+    g = cb.make_geom(**geom)
+    cells = geom["n"][0] * geom["n"][1]
+    K, W = args.pf_steps, 2
+    out = {"workload": "2D FIVEEQS shock-helium-bubble 2048x1024, WENO5B+HLLC+TVD-RK3, CAC-Adv Phase-Field "
+                       "(implicit regularisation potential, Eta_Multiplier 1), reflective top/bottom, outflow left/right",
+           "cells": cells, "steps": K, "unit": UNIT + " per hyperbolic RK stage (Phase-Field step included)"}
+    for prec in ("mixed", "fp64"):
+        for pf_on in (True, False):
+            extra = {"compas_b200.precision": prec}
+            if pf_on:
+                extra.update({"PhaseField.phase_field": "1", "PhaseField.Mechanism": "CAC-Adv"})
+            p = cb.make_parm(phys, dim, dict(inputs, **extra))
+            lv = cb.Level(p, g)
+            lv.upload(U, stream=stream)
+            lv.advance(W, stream=stream)
+            torch.cuda.synchronize()
+            sub0 = lv.pf_substeps()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            lv.advance(K, stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            info = lv.sync()
+            assert info.status == 0
+            key = f"{prec}_{'with_phase_field' if pf_on else 'hyperbolic_only'}"
+            out[key] = cells * 3 * K / (ms / 1e3)
+            if pf_on:
+                out[f"{prec}_pf_substeps_per_step"] = (lv.pf_substeps() - sub0) / K
+                out[f"{prec}_ms_per_step"] = ms / K
+            lv.close()
+    out["mixed_vs_fp64_with_phase_field"] = out["mixed_with_phase_field"] / out["fp64_with_phase_field"]
     return out
 
 
@@ -410,6 +461,7 @@ def run_ours(args, rank, world, dist):
             cpu = cpu_baseline(args.cpu_n, args.cpu_steps)
         batched = None if args.no_batched else run_batched(args)
         serving_res = None if args.no_serving else run_serving(args)
+        pf_res = None if args.no_phase_field else run_phase_field(args)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms[head] / args.steps, "higher_is_better": True,
@@ -435,6 +487,7 @@ def run_ours(args, rank, world, dist):
             "cpu_baseline": cpu,
             "batched": batched,
             "serving": serving_res,
+            "phase_field": pf_res,
         }
     return line
 

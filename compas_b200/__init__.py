@@ -123,6 +123,7 @@ _SIGS = {
     "compas_b200_level_dts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
     "compas_b200_level_launches": (ctypes.c_longlong, [ctypes.c_void_p]),
     "compas_b200_level_pf_substeps": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "compas_b200_level_pf_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "compas_b200_pf_grad_q": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_void_p,
                                              ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_void_p, ctypes.c_void_p]),
@@ -380,6 +381,13 @@ class Level:
     def pf_substeps(self) -> int:
         """Phase-Field sub-steps taken so far (PhaseField.phase_field = 1)."""
         return int(lib().compas_b200_level_pf_substeps(self._h))
+
+    def pf_info(self) -> dict:
+        """Counters of the last Phase-Field step."""
+        v = (ctypes.c_double * 7)()
+        _check(lib().compas_b200_level_pf_info(self._h, v))
+        keys = ("max_v", "mobility", "eta", "mechanism_steps", "solver_iterations", "max_grad_q", "residual")
+        return dict(zip(keys, v[:]))
 
 
 @dataclass

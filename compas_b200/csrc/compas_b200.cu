@@ -427,6 +427,7 @@ struct compas_b200_level {
     cudaStream_t graph_stream = nullptr;
     compas::PfLevel* pf = nullptr;  // Phase-Field work arrays (PhaseField.phase_field = 1)
     long long pf_substeps = 0;
+    compas::PfInfo pf_last{};       // counters of the last Phase-Field step
 };
 
 namespace compas {
@@ -819,6 +820,19 @@ int compas_b200_pf_grad_q(const compas_b200_parm* p, const compas_b200_geom* g, 
 
 long long compas_b200_level_pf_substeps(const compas_b200_level* lv) { return lv ? lv->pf_substeps : 0; }
 
+int compas_b200_level_pf_info(const compas_b200_level* lv, double* info) {
+    if (!lv || !info) return fail(COMPAS_B200_EARG, "null argument");
+    const PfInfo& i = lv->pf_last;
+    info[0] = i.max_v;
+    info[1] = i.mobility;
+    info[2] = i.eta;
+    info[3] = i.mech_steps;
+    info[4] = i.solve_iters;
+    info[5] = i.gmax;
+    info[6] = i.solve_res;
+    return COMPAS_B200_OK;
+}
+
 int compas_b200_relaxation(const compas_b200_parm* p, const compas_b200_geom* g, double* U, unsigned int* err_dev,
                            void* stream) {
     int rc = check_args(p, g);
@@ -1029,6 +1043,7 @@ int compas_b200_level_advance(compas_b200_level* lv, int nsteps, double stop_tim
             PfInfo info;
             std::string msg;
             if ((rc = pf_grad_q(lv->pf, &lv->p, lv->U, h.dt, st, &info, &msg))) return fail(rc, msg);
+            lv->pf_last = info;
             const double* gq[3] = {pf_gq(lv->pf, 0), pf_gq(lv->pf, 1), lv->p.dim == 3 ? pf_gq(lv->pf, 2) : nullptr};
             int sub = 0;
             if ((rc = pf_advance(&lv->p, &lv->g, lv->U, lv->U1, lv->U2, gq, pf_dt_slot(lv->pf), h.dt, info.gmax,

@@ -382,6 +382,19 @@ __global__ void k_gq_from_q(const double* Q, PfDims m, int d, double* gq) {
     }
 }
 
+// largest non-negative value of the block into *out (bits of a double; one atomic per block)
+__device__ __forceinline__ void block_max_atomic(double v, unsigned long long* out) {
+    __shared__ double wm[kThreads / 32];
+    for (int o = 16; o > 0; o >>= 1) v = dmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = dmax(m, wm[w]);
+        atomicMax(out, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
 // max |u| over the valid cells of the padded state (MaxVelocity, Conservative2Velocity)
 __global__ void k_maxv(const double* U, long long S, long long upx, long long upxy, int ung, int ugz, PfDims m,
                        unsigned long long* out) {
@@ -398,16 +411,14 @@ __global__ void k_maxv(const double* U, long long S, long long upx, long long up
         }
         v = dmax(v, fabs(sqrt(s)));
     }
-    for (int o = 16; o > 0; o >>= 1) v = dmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(v));
+    block_max_atomic(v, out);
 }
 
 __global__ void k_maxabs(const double* a, long long n, unsigned long long* out) {
     double v = 0.0;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
         v = dmax(v, fabs(a[q]));
-    for (int o = 16; o > 0; o >>= 1) v = dmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(v));
+    block_max_atomic(v, out);
 }
 
 // ---- multigrid -----------------------------------------------------------------------------------------
@@ -418,69 +429,116 @@ struct MgLevel {
     double* x = nullptr;
     double* b = nullptr;
     double* r = nullptr;
+    double* idiag = nullptr;  // 1 / diagonal of A (set once per solve)
+    double ih2[3] = {1.0, 1.0, 1.0};
     bool rb = true;  // red-black colouring is a proper two-colouring (no odd periodic side)
 };
 
-__device__ __forceinline__ void mg_row(const MgLevel& L, const double* x, long long q, double& off, double& diag) {
+// off-diagonal part sum_f beta_f x_nb / h^2 of row (i,j,k) (32-bit indices: cells < 2^31)
+__device__ __forceinline__ double mg_off(const MgLevel& L, const double* x, int i, int j, int k) {
     const PfDims& m = L.m;
-    int c[3];
-    vcoord(m, q, c[0], c[1], c[2]);
-    off = 0.0;
-    diag = 0.0;
+    const int c[3] = {i, j, k};
+    const int n0 = m.n[0], n1 = m.n[1];
+    double off = 0.0;
     for (int d = 0; d < m.D; ++d) {
-        const double h2 = m.dx[d] * m.dx[d];
+        const int fx = n0 + (d == 0), fy = n1 + (d == 1);
         for (int s = 0; s < 2; ++s) {
             int nb[3] = {c[0], c[1], c[2]};
             nb[d] += s ? 1 : -1;
             if (nb[d] < 0 || nb[d] >= m.n[d]) {
                 if (!m.periodic[d]) continue;
-                nb[d] = (nb[d] + m.n[d]) % m.n[d];
+                nb[d] = (nb[d] < 0) ? nb[d] + m.n[d] : nb[d] - m.n[d];
             }
             int f[3] = {c[0], c[1], c[2]};
             if (s) f[d] += 1;
-            const double bf = L.beta[d][fidx(m, d, f[0], f[1], f[2])] / h2;
-            diag += bf;
-            off += bf * x[vidx(m, nb[0], nb[1], nb[2])];
+            const double bf = L.beta[d][f[0] + fx * (f[1] + fy * f[2])] * L.ih2[d];
+            off += bf * x[nb[0] + n0 * (nb[1] + n1 * nb[2])];
         }
     }
+    return off;
 }
 
-__global__ void k_mg_apply(MgLevel L, const double* x, double* y) {
-    GRID_STRIDE(q, L.m.nv) {
-        double off, diag;
-        mg_row(L, x, q, off, diag);
-        y[q] = diag * x[q] - off;
+// the same with the dimension known at compile time (the per-level kernels below)
+template <int D>
+__device__ __forceinline__ double mg_off_t(const MgLevel& L, const double* __restrict__ x, int i, int j, int k) {
+    const PfDims& m = L.m;
+    const int n0 = m.n[0], n1 = m.n[1];
+    const int c[3] = {i, j, k};
+    double off = 0.0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        const int fx = n0 + (d == 0), fy = n1 + (d == 1);
+        const double* __restrict__ bt = L.beta[d];
+        const double ih = L.ih2[d];
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            int nb[3] = {c[0], c[1], c[2]};
+            nb[d] += s ? 1 : -1;
+            bool ok = true;
+            if (nb[d] < 0 || nb[d] >= m.n[d]) {
+                if (m.periodic[d]) nb[d] = (nb[d] < 0) ? nb[d] + m.n[d] : nb[d] - m.n[d];
+                else ok = false;
+            }
+            if (ok) {
+                int f[3] = {c[0], c[1], c[2]};
+                if (s) f[d] += 1;
+                off += (bt[f[0] + fx * (f[1] + fy * f[2])] * ih) * x[nb[0] + n0 * (nb[1] + n1 * nb[2])];
+            }
+        }
+    }
+    return off;
+}
+
+// grid-shaped launches: x blocks along i, one grid row per (j, k) - no index division
+#define MG_CELL(m)                                              \
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;         \
+    const int j = blockIdx.y, k = blockIdx.z;                    \
+    if (i >= (m).n[0]) return;                                   \
+    const int q = i + (m).n[0] * (j + (m).n[1] * k);
+
+template <int D>
+__global__ void k_mg_rb_t(MgLevel L, int color) {
+    MG_CELL(L.m)
+    if (((i + j + k) & 1) != color) return;
+    L.x[q] = (L.b[q] + mg_off_t<D>(L, L.x, i, j, k)) * L.idiag[q];
+}
+template <int D>
+__global__ void k_mg_residual_t(MgLevel L) {
+    MG_CELL(L.m)
+    L.r[q] = L.b[q] - (L.x[q] / L.idiag[q] - mg_off_t<D>(L, L.x, i, j, k));
+}
+template <int D>
+__global__ void k_mg_apply_t(MgLevel L, const double* __restrict__ x, double* __restrict__ y) {
+    MG_CELL(L.m)
+    y[q] = x[q] / L.idiag[q] - mg_off_t<D>(L, x, i, j, k);
+}
+template <int D>
+__global__ void k_mg_jacobi_t(MgLevel L) {
+    MG_CELL(L.m)
+    L.r[q] = L.x[q] + 0.8 * ((L.b[q] + mg_off_t<D>(L, L.x, i, j, k)) * L.idiag[q] - L.x[q]);
+}
+
+constexpr int kRowThreads = 128;
+dim3 mg_grid(const PfDims& m) { return dim3((unsigned)((m.n[0] + kRowThreads - 1) / kRowThreads), (unsigned)m.n[1], (unsigned)m.n[2]); }
+
+__global__ void k_mg_idiag(MgLevel L) {
+    const PfDims& m = L.m;
+    GRID_STRIDE(q, m.nv) {
+        int c[3];
+        vcoord(m, q, c[0], c[1], c[2]);
+        double diag = 0.0;
+        for (int d = 0; d < m.D; ++d)
+            for (int s = 0; s < 2; ++s) {
+                const int nb = c[d] + (s ? 1 : -1);
+                if ((nb < 0 || nb >= m.n[d]) && !m.periodic[d]) continue;
+                int f[3] = {c[0], c[1], c[2]};
+                if (s) f[d] += 1;
+                diag += L.beta[d][fidx(m, d, f[0], f[1], f[2])] * L.ih2[d];
+            }
+        L.idiag[q] = 1.0 / diag;
     }
 }
 
-__global__ void k_mg_residual(MgLevel L) {
-    GRID_STRIDE(q, L.m.nv) {
-        double off, diag;
-        mg_row(L, L.x, q, off, diag);
-        L.r[q] = L.b[q] - (diag * L.x[q] - off);
-    }
-}
-
-// red-black Gauss-Seidel half sweep on cells of colour `color`
-__global__ void k_mg_rb(MgLevel L, int color) {
-    GRID_STRIDE(q, L.m.nv) {
-        int i, j, k;
-        vcoord(L.m, q, i, j, k);
-        if (((i + j + k) & 1) != color) continue;
-        double off, diag;
-        mg_row(L, L.x, q, off, diag);
-        L.x[q] = (L.b[q] + off) / diag;
-    }
-}
-
-// weighted Jacobi sweep (x_new into r, then copied back)
-__global__ void k_mg_jacobi(MgLevel L) {
-    GRID_STRIDE(q, L.m.nv) {
-        double off, diag;
-        mg_row(L, L.x, q, off, diag);
-        L.r[q] = L.x[q] + 0.8 * ((L.b[q] + off) / diag - L.x[q]);
-    }
-}
 __global__ void k_copy(const double* a, double* b, long long n) {
     GRID_STRIDE(q, n) b[q] = a[q];
 }
@@ -543,19 +601,159 @@ __global__ void k_add_const(double* a, long long n, const double* tot, double sc
     const double c = -tot[0] * scale;
     GRID_STRIDE(q, n) a[q] += c;
 }
-__global__ void k_axpy2(double* x, double* r, const double* p, const double* Ap, long long n, double al,
+// the coarsest level: all sweeps in one single-block launch (colours separated by block barriers)
+__global__ void k_mg_coarse(MgLevel L, int sweeps) {
+    const PfDims& m = L.m;
+    const int n = (int)m.nv;
+    for (int s = 0; s < sweeps; ++s) {
+        if (L.rb) {
+            for (int c = 0; c < 2; ++c) {
+                const int color = (s & 1) ? 1 - c : c;
+                for (int q = threadIdx.x; q < n; q += blockDim.x) {
+                    const int i = q % m.n[0], r = q / m.n[0];
+                    const int j = r % m.n[1], k = r / m.n[1];
+                    if (((i + j + k) & 1) != color) continue;
+                    L.x[q] = (L.b[q] + mg_off(L, L.x, i, j, k)) * L.idiag[q];
+                }
+                __syncthreads();
+            }
+        } else {
+            for (int q = threadIdx.x; q < n; q += blockDim.x) {
+                const int i = q % m.n[0], r = q / m.n[0];
+                const int j = r % m.n[1], k = r / m.n[1];
+                L.r[q] = L.x[q] + 0.8 * ((L.b[q] + mg_off(L, L.x, i, j, k)) * L.idiag[q] - L.x[q]);
+            }
+            __syncthreads();
+            for (int q = threadIdx.x; q < n; q += blockDim.x) L.x[q] = L.r[q];
+            __syncthreads();
+        }
+    }
+}
+
+// The coarse part of a V-cycle, levels l0 .. nl-1 (each of at most kBlockCells cells), in one
+// single-block launch: the same smoothing, restriction and prolongation as the per-level kernels,
+// with block barriers between the steps.
+constexpr int kBlockCells = 4096;
+constexpr int kBlockThreads = 1024;
+
+__device__ void blk_smooth(const MgLevel& L, int sweeps, bool reverse) {
+    const PfDims& m = L.m;
+    const int n = (int)m.nv;
+    for (int s = 0; s < sweeps; ++s) {
+        if (L.rb) {
+            for (int c = 0; c < 2; ++c) {
+                const int color = reverse ? 1 - c : c;
+                for (int q = threadIdx.x; q < n; q += blockDim.x) {
+                    const int i = q % m.n[0], r = q / m.n[0];
+                    const int j = r % m.n[1], k = r / m.n[1];
+                    if (((i + j + k) & 1) != color) continue;
+                    L.x[q] = (L.b[q] + mg_off(L, L.x, i, j, k)) * L.idiag[q];
+                }
+                __syncthreads();
+            }
+        } else {
+            for (int q = threadIdx.x; q < n; q += blockDim.x) {
+                const int i = q % m.n[0], r = q / m.n[0];
+                const int j = r % m.n[1], k = r / m.n[1];
+                L.r[q] = L.x[q] + 0.8 * ((L.b[q] + mg_off(L, L.x, i, j, k)) * L.idiag[q] - L.x[q]);
+            }
+            __syncthreads();
+            for (int q = threadIdx.x; q < n; q += blockDim.x) L.x[q] = L.r[q];
+            __syncthreads();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBlockThreads) k_mg_vcycle_block(const MgLevel* levels, int l0, int nl) {
+    // down
+    for (int l = l0; l < nl - 1; ++l) {
+        const MgLevel& L = levels[l];
+        const MgLevel& C = levels[l + 1];
+        blk_smooth(L, 2, false);
+        const PfDims& m = L.m;
+        for (int q = threadIdx.x; q < (int)m.nv; q += blockDim.x) {
+            const int i = q % m.n[0], r = q / m.n[0];
+            const int j = r % m.n[1], k = r / m.n[1];
+            L.r[q] = L.b[q] - (L.x[q] / L.idiag[q] - mg_off(L, L.x, i, j, k));
+        }
+        __syncthreads();
+        const PfDims& c = C.m;
+        for (int q = threadIdx.x; q < (int)c.nv; q += blockDim.x) {
+            const int I = q % c.n[0], r = q / c.n[0];
+            const int J = r % c.n[1], K = r / c.n[1];
+            double sacc = 0.0;
+            const int kz = (c.D == 3) ? 2 : 1;
+            for (int dk = 0; dk < kz; ++dk)
+                for (int dj = 0; dj < 2; ++dj)
+                    for (int di = 0; di < 2; ++di)
+                        sacc += L.r[(2 * I + di) + m.n[0] * ((2 * J + dj) + m.n[1] * (c.D == 3 ? 2 * K + dk : 0))];
+            C.b[q] = sacc / (double)(c.D == 3 ? 8 : 4);
+            C.x[q] = 0.0;
+        }
+        __syncthreads();
+    }
+    // coarsest: an even number of sweeps alternating the colour order (symmetric)
+    {
+        const MgLevel& L = levels[nl - 1];
+        for (int s = 0; s < 8; ++s) {
+            blk_smooth(L, 1, false);
+            blk_smooth(L, 1, true);
+        }
+    }
+    // up
+    for (int l = nl - 2; l >= l0; --l) {
+        const MgLevel& L = levels[l];
+        const MgLevel& C = levels[l + 1];
+        const PfDims& m = L.m;
+        const PfDims& c = C.m;
+        for (int q = threadIdx.x; q < (int)m.nv; q += blockDim.x) {
+            const int i = q % m.n[0], r = q / m.n[0];
+            const int j = r % m.n[1], k = r / m.n[1];
+            L.x[q] += C.x[(i / 2) + c.n[0] * ((j / 2) + c.n[1] * (m.D == 3 ? k / 2 : 0))];
+        }
+        __syncthreads();
+        blk_smooth(L, 2, true);
+    }
+}
+
+// one reduced sum (the first of block_sum2's pair) into *out
+__global__ void k_reduce1(const double* partial, int nb, double* out) {
+    __shared__ double sa[kThreads];
+    double a = 0.0;
+    for (int t = threadIdx.x; t < nb; t += kThreads) a += partial[2 * t];
+    sa[threadIdx.x] = a;
+    __syncthreads();
+    for (int s = kThreads / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) sa[threadIdx.x] += sa[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sa[0];
+}
+
+// conjugate-gradient scalars kept on the device: cg[0] rz, [1] pAp, [2] alpha, [3] rz_new, [4] beta
+__global__ void k_cg_alpha(double* cg) { cg[2] = (cg[1] > 0.0) ? cg[0] / cg[1] : 0.0; }
+__global__ void k_cg_beta(double* cg) {
+    cg[4] = (cg[0] != 0.0) ? cg[3] / cg[0] : 0.0;
+    cg[0] = cg[3];
+}
+
+__global__ void k_axpy2(double* x, double* r, const double* p, const double* Ap, long long n, const double* alp,
                         unsigned long long* rmax) {
+    const double al = *alp;
     double v = 0.0;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
         x[q] += al * p[q];
         r[q] -= al * Ap[q];
         v = dmax(v, fabs(r[q]));
     }
-    for (int o = 16; o > 0; o >>= 1) v = dmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(rmax, (unsigned long long)__double_as_longlong(v));
+    block_max_atomic(v, rmax);
 }
-__global__ void k_xpby(const double* z, double* p, long long n, double be) {
+__global__ void k_xpby(const double* z, double* p, long long n, const double* bep) {
+    const double be = *bep;
     GRID_STRIDE(q, n) p[q] = z[q] + be * p[q];
+}
+__global__ void k_sub(const double* a, const double* b, double* c, long long n) {
+    GRID_STRIDE(q, n) c[q] = a[q] - b[q];
 }
 __global__ void k_neg(double* a, long long n) {
     GRID_STRIDE(q, n) a[q] = -a[q];
@@ -584,7 +782,12 @@ struct PfLevel {
     double* dt_slot = nullptr;
     // multigrid levels and the conjugate-gradient vectors of the finest one
     std::vector<MgLevel> mg;
+    MgLevel* mg_dev = nullptr;               // the level descriptors on the device (block V-cycle)
+    int mg_block0 = -1;                      // first level of the single-block coarse cycle
     double *z = nullptr, *p = nullptr, *Ap = nullptr;
+    double* cg = nullptr;                    // device scalars of the conjugate gradients
+    double* qsol = nullptr;                  // solution Q, kept as the next step's starting iterate
+    cudaGraphExec_t cg_iter = nullptr;       // one captured iteration (fixed pointers)
     long long bytes = 0;
     std::vector<void*> allocs;
 };
@@ -628,24 +831,37 @@ double read_max(unsigned long long* dev, cudaStream_t st) {
 cudaError_t vcycle(PfLevel* pf, int l, cudaStream_t st) {
     MgLevel& L = pf->mg[l];
     const unsigned nb = blocks_for(L.m.nv);
+    const unsigned nbh = blocks_for((long long)L.m.n[1] * L.m.n[2] * ((L.m.n[0] + 1) / 2));
+    const dim3 gg = mg_grid(L.m);
+    const bool d3 = (L.m.D == 3);
     auto smooth = [&](int sweeps, bool reverse) {
         for (int s = 0; s < sweeps; ++s) {
             if (L.rb) {
-                k_mg_rb<<<nb, kThreads, 0, st>>>(L, reverse ? 1 : 0);
-                k_mg_rb<<<nb, kThreads, 0, st>>>(L, reverse ? 0 : 1);
+                for (int c = 0; c < 2; ++c) {
+                    const int color = reverse ? 1 - c : c;
+                    if (d3) k_mg_rb_t<3><<<gg, kRowThreads, 0, st>>>(L, color);
+                    else k_mg_rb_t<2><<<gg, kRowThreads, 0, st>>>(L, color);
+                }
             } else {
-                k_mg_jacobi<<<nb, kThreads, 0, st>>>(L);
+                if (d3) k_mg_jacobi_t<3><<<gg, kRowThreads, 0, st>>>(L);
+                else k_mg_jacobi_t<2><<<gg, kRowThreads, 0, st>>>(L);
                 k_copy<<<nb, kThreads, 0, st>>>(L.r, L.x, L.m.nv);
             }
         }
     };
+    (void)nbh;
+    if (l == pf->mg_block0) {
+        k_mg_vcycle_block<<<1, kBlockThreads, 0, st>>>(pf->mg_dev, l, (int)pf->mg.size());
+        return cudaGetLastError();
+    }
     if (l + 1 == (int)pf->mg.size()) {
-        smooth(L.m.nv <= 64 ? 64 : 16, false);
-        smooth(L.m.nv <= 64 ? 64 : 16, true);
+        // an even number of sweeps alternating the colour order keeps the cycle symmetric
+        k_mg_coarse<<<1, kThreads, 0, st>>>(L, 16);
         return cudaGetLastError();
     }
     smooth(2, false);
-    k_mg_residual<<<nb, kThreads, 0, st>>>(L);
+    if (d3) k_mg_residual_t<3><<<gg, kRowThreads, 0, st>>>(L);
+    else k_mg_residual_t<2><<<gg, kRowThreads, 0, st>>>(L);
     MgLevel& C = pf->mg[l + 1];
     k_mg_restrict<<<blocks_for(C.m.nv), kThreads, 0, st>>>(L.r, L.m, C.b, C.m);
     k_zero<<<blocks_for(C.m.nv), kThreads, 0, st>>>(C.x, C.m.nv);
@@ -659,6 +875,10 @@ cudaError_t vcycle(PfLevel* pf, int l, cudaStream_t st) {
 }  // namespace
 
 int pf_create(const compas_b200_parm* p, const compas_b200_geom* g, PfLevel** out, std::string* err) {
+    if ((long long)g->n[0] * g->n[1] * (p->dim == 3 ? g->n[2] : 1) >= (1LL << 31)) {
+        if (err) *err = "the Phase-Field step supports boxes of fewer than 2^31 cells";
+        return COMPAS_B200_EARG;
+    }
     PfLevel* pf = new PfLevel();
     int per[3] = {0, 0, 0};
     for (int d = 0; d < p->dim; ++d) per[d] = (g->lo_bc[d] == 0);
@@ -696,15 +916,29 @@ int pf_create(const compas_b200_parm* p, const compas_b200_geom* g, PfLevel** ou
             if (lm.periodic[d] && (lm.n[d] % 2)) L.rb = false;
         for (int d = 0; d < lm.D; ++d)
             if ((e = dalloc(pf, &L.beta[d], lm.nf[d]))) return fail_out(e);
-        if ((e = dalloc(pf, &L.x, lm.nv)) || (e = dalloc(pf, &L.b, lm.nv)) || (e = dalloc(pf, &L.r, lm.nv)))
+        if ((e = dalloc(pf, &L.x, lm.nv)) || (e = dalloc(pf, &L.b, lm.nv)) || (e = dalloc(pf, &L.r, lm.nv)) ||
+            (e = dalloc(pf, &L.idiag, lm.nv)))
             return fail_out(e);
+        for (int d = 0; d < lm.D; ++d) L.ih2[d] = 1.0 / (lm.dx[d] * lm.dx[d]);
         pf->mg.push_back(L);
         if (!coarsenable(lm) || lm.nv <= 16) break;
         int nc[3] = {lm.n[0] / 2, lm.n[1] / 2, lm.D == 3 ? lm.n[2] / 2 : 1};
         double dc[3] = {2 * lm.dx[0], 2 * lm.dx[1], lm.D == 3 ? 2 * lm.dx[2] : 1.0};
         lm = make_dims(lm.D, nc, dc, lm.periodic);
     }
-    if ((e = dalloc(pf, &pf->z, m.nv)) || (e = dalloc(pf, &pf->p, m.nv)) || (e = dalloc(pf, &pf->Ap, m.nv)))
+    for (size_t l = 0; l < pf->mg.size(); ++l)
+        if (pf->mg[l].m.nv <= kBlockCells) {
+            pf->mg_block0 = (int)l;
+            break;
+        }
+    {
+        const long long nbytes = (long long)(sizeof(MgLevel) * pf->mg.size() + 7) / 8;
+        if ((e = dalloc(pf, (double**)&pf->mg_dev, nbytes))) return fail_out(e);
+        if ((e = cudaMemcpy(pf->mg_dev, pf->mg.data(), sizeof(MgLevel) * pf->mg.size(), cudaMemcpyHostToDevice)))
+            return fail_out(e);
+    }
+    if ((e = dalloc(pf, &pf->z, m.nv)) || (e = dalloc(pf, &pf->p, m.nv)) || (e = dalloc(pf, &pf->Ap, m.nv)) ||
+        (e = dalloc(pf, &pf->cg, 8)) || (e = dalloc(pf, &pf->qsol, m.nv)))
         return fail_out(e);
     *out = pf;
     return COMPAS_B200_OK;
@@ -712,6 +946,7 @@ int pf_create(const compas_b200_parm* p, const compas_b200_geom* g, PfLevel** ou
 
 void pf_destroy(PfLevel* pf) {
     if (!pf) return;
+    if (pf->cg_iter) cudaGraphExecDestroy(pf->cg_iter);
     for (void* a : pf->allocs) cudaFree(a);
     delete pf;
 }
@@ -719,28 +954,6 @@ void pf_destroy(PfLevel* pf) {
 const double* pf_gq(const PfLevel* pf, int d) { return pf->gq[d]; }
 double* pf_dt_slot(PfLevel* pf) { return pf->dt_slot; }
 long long pf_bytes(const PfLevel* pf) { return pf ? pf->bytes : 0; }
-
-namespace {
-
-// sum of a finest-level vector (fixed order) into pf->tot[0]
-cudaError_t vsum(PfLevel* pf, const double* a, cudaStream_t st) {
-    const PfDims& m = pf->mg[0].m;
-    k_dot<<<kRedBlocks, kThreads, 0, st>>>(a, nullptr, m.nv, pf->partial);
-    k_reduce2<<<1, kThreads, 0, st>>>(pf->partial, kRedBlocks, pf->tot);
-    return cudaGetLastError();
-}
-
-double dot_host(PfLevel* pf, const double* a, const double* b, cudaStream_t st) {
-    const PfDims& m = pf->mg[0].m;
-    k_dot<<<kRedBlocks, kThreads, 0, st>>>(a, b, m.nv, pf->partial);
-    k_reduce2<<<1, kThreads, 0, st>>>(pf->partial, kRedBlocks, pf->tot);
-    double h[2];
-    cudaMemcpyAsync(h, pf->tot, sizeof(h), cudaMemcpyDeviceToHost, st);
-    cudaStreamSynchronize(st);
-    return h[0];
-}
-
-}  // namespace
 
 int pf_grad_q(PfLevel* pf, const compas_b200_parm* p, const double* U, double dt, cudaStream_t st, PfInfo* info,
               std::string* err) {
@@ -823,50 +1036,86 @@ int pf_grad_q(PfLevel* pf, const compas_b200_parm* p, const double* U, double dt
             for (int d = 0; d < m.D; ++d)
                 k_mg_beta<<<blocks_for(pf->mg[l].m.nf[d]), kThreads, 0, st>>>(pf->mg[l - 1].beta[d], pf->mg[l - 1].m,
                                                                                pf->mg[l].beta[d], pf->mg[l].m, d);
+        for (size_t l = 0; l < pf->mg.size(); ++l)
+            k_mg_idiag<<<blocks_for(pf->mg[l].m.nv), kThreads, 0, st>>>(pf->mg[l]);
         PF_TRY(cudaGetLastError());
-        // preconditioned conjugate gradients on the mean-free space; r lives in F.r, the solution in Q
-        double* x = pf->pfo;      // the mechanism iterate is no longer needed: hold the solution here
-        double* r = pf->mech;     // residual
-        k_zero<<<nbv, kThreads, 0, st>>>(x, m.nv);
-        k_copy<<<nbv, kThreads, 0, st>>>(F.b, r, m.nv);
+        // preconditioned conjugate gradients on the mean-free space; the scalars stay on the device and
+        // one iteration is a captured graph, so an iteration costs one host read (the residual norm)
+        // The iterate starts from the previous step's solution (the problem changes little from one
+        // step to the next); the stopping test is the reference's absolute one, max|r| <= tol max|rhs|,
+        // so the warm start changes only the number of iterations.
+        double* x = pf->qsol;
+        double* r = pf->mech;     // residual (the mechanism's scratch is free here)
+        if (m.D == 3) k_mg_apply_t<3><<<mg_grid(F.m), kRowThreads, 0, st>>>(F, x, pf->Ap);
+        else k_mg_apply_t<2><<<mg_grid(F.m), kRowThreads, 0, st>>>(F, x, pf->Ap);
+        k_sub<<<nbv, kThreads, 0, st>>>(F.b, pf->Ap, r, m.nv);
+        PF_TRY(cudaMemsetAsync(pf->umax, 0, sizeof(unsigned long long), st));
+        k_maxabs<<<nbv, kThreads, 0, st>>>(F.b, m.nv, pf->umax);
+        const double bnorm = read_max(pf->umax, st);
         PF_TRY(cudaMemsetAsync(pf->umax, 0, sizeof(unsigned long long), st));
         k_maxabs<<<nbv, kThreads, 0, st>>>(r, m.nv, pf->umax);
-        const double bnorm = read_max(pf->umax, st);
-        auto precond = [&](const double* in, double* outz) -> cudaError_t {
+        const double rnorm0 = read_max(pf->umax, st);
+        auto dot_dev = [&](const double* a, const double* b, double* slot, cudaStream_t s2) {
+            k_dot<<<kRedBlocks, kThreads, 0, s2>>>(a, b, m.nv, pf->partial);
+            k_reduce1<<<1, kThreads, 0, s2>>>(pf->partial, kRedBlocks, slot);
+        };
+        auto precond = [&](const double* in, double* outz, cudaStream_t s2) -> cudaError_t {
             // z = V(in) with a zero start, made mean-free
-            k_copy<<<nbv, kThreads, 0, st>>>(in, F.b, m.nv);
-            k_zero<<<nbv, kThreads, 0, st>>>(F.x, m.nv);
-            cudaError_t e = vcycle(pf, 0, st);
+            k_copy<<<nbv, kThreads, 0, s2>>>(in, F.b, m.nv);
+            k_zero<<<nbv, kThreads, 0, s2>>>(F.x, m.nv);
+            cudaError_t e = vcycle(pf, 0, s2);
             if (e != cudaSuccess) return e;
-            k_copy<<<nbv, kThreads, 0, st>>>(F.x, outz, m.nv);
-            vsum(pf, outz, st);
-            k_add_const<<<nbv, kThreads, 0, st>>>(outz, m.nv, pf->tot, 1.0 / (double)m.nv);
+            k_copy<<<nbv, kThreads, 0, s2>>>(F.x, outz, m.nv);
+            dot_dev(outz, nullptr, pf->cg + 5, s2);
+            k_add_const<<<nbv, kThreads, 0, s2>>>(outz, m.nv, pf->cg + 5, 1.0 / (double)m.nv);
+            return cudaGetLastError();
+        };
+        auto iteration = [&](cudaStream_t s2) -> cudaError_t {
+            if (m.D == 3) k_mg_apply_t<3><<<mg_grid(F.m), kRowThreads, 0, s2>>>(F, pf->p, pf->Ap);
+            else k_mg_apply_t<2><<<mg_grid(F.m), kRowThreads, 0, s2>>>(F, pf->p, pf->Ap);
+            dot_dev(pf->p, pf->Ap, pf->cg + 1, s2);
+            k_cg_alpha<<<1, 1, 0, s2>>>(pf->cg);
+            cudaError_t e = cudaMemsetAsync(pf->umax, 0, sizeof(unsigned long long), s2);
+            if (e != cudaSuccess) return e;
+            k_axpy2<<<nbv, kThreads, 0, s2>>>(x, r, pf->p, pf->Ap, m.nv, pf->cg + 2, pf->umax);
+            if ((e = precond(r, pf->z, s2)) != cudaSuccess) return e;
+            dot_dev(r, pf->z, pf->cg + 3, s2);
+            k_cg_beta<<<1, 1, 0, s2>>>(pf->cg);
+            k_xpby<<<nbv, kThreads, 0, s2>>>(pf->z, pf->p, m.nv, pf->cg + 4);
             return cudaGetLastError();
         };
         const double tol = p->pf_tol_rel;
-        if (bnorm > 0.0) {
-            PF_TRY(precond(r, pf->z));
+        if (bnorm > 0.0 && rnorm0 > tol * bnorm) {
+            PF_TRY(precond(r, pf->z, st));
             k_copy<<<nbv, kThreads, 0, st>>>(pf->z, pf->p, m.nv);
-            double rz = dot_host(pf, r, pf->z, st);
+            dot_dev(r, pf->z, pf->cg + 0, st);
+            PF_TRY(cudaGetLastError());
+            if (!pf->cg_iter) {
+                cudaStream_t cap;
+                PF_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+                cudaGraph_t graph;
+                cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+                if (e == cudaSuccess) {
+                    cudaError_t e2 = iteration(cap);
+                    e = cudaStreamEndCapture(cap, &graph);
+                    if (e == cudaSuccess && e2 != cudaSuccess) e = e2;
+                    if (e == cudaSuccess) {
+                        e = cudaGraphInstantiate(&pf->cg_iter, graph, 0);
+                        cudaGraphDestroy(graph);
+                    }
+                }
+                cudaStreamDestroy(cap);
+                PF_TRY(e);
+            }
             res = 1.0;
             for (iters = 0; iters < 1000;) {
-                k_mg_apply<<<nbv, kThreads, 0, st>>>(F, pf->p, pf->Ap);
-                const double pAp = dot_host(pf, pf->p, pf->Ap, st);
-                if (!(pAp > 0.0)) break;
-                const double al = rz / pAp;
-                PF_TRY(cudaMemsetAsync(pf->umax, 0, sizeof(unsigned long long), st));
-                k_axpy2<<<nbv, kThreads, 0, st>>>(x, r, pf->p, pf->Ap, m.nv, al, pf->umax);
+                PF_TRY(cudaGraphLaunch(pf->cg_iter, st));
                 ++iters;
                 res = read_max(pf->umax, st) / bnorm;
-                if (res <= tol) break;
-                PF_TRY(precond(r, pf->z));
-                const double rz2 = dot_host(pf, r, pf->z, st);
-                const double be = rz2 / rz;
-                rz = rz2;
-                k_xpby<<<nbv, kThreads, 0, st>>>(pf->z, pf->p, m.nv, be);
+                if (!(res > tol)) break;
             }
         } else {
-            res = 0.0;
+            res = (bnorm > 0.0) ? rnorm0 / bnorm : 0.0;
         }
         for (int d = 0; d < m.D; ++d) k_gq_from_q<<<blocks_for(m.nf[d]), kThreads, 0, st>>>(x, m, d, pf->gq[d]);
         PF_TRY(cudaGetLastError());

@@ -238,6 +238,11 @@ long long compas_b200_level_launches(compas_b200_level* lv);
 /* Phase-Field sub-steps taken by the level so far (0 without PhaseField.phase_field). */
 long long compas_b200_level_pf_substeps(const compas_b200_level* lv);
 
+/* Counters of the level's last Phase-Field step, the quantities PhaseField_Evolve prints
+ * (source/Class_Compressible_PhaseField.cpp:424-595) into info (host, 7 doubles) as
+ * compas_b200_pf_grad_q returns them. */
+int compas_b200_level_pf_info(const compas_b200_level* lv, double* info);
+
 /* ---- batched independent cases ------------------------------------------------------------------
  * Many single-box cases of uneven size (each with its own EOS, boundary codes, stop time, step budget
  * and time-step control) advanced together: every RK stage of every case runs in ONE persistent

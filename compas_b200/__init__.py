@@ -123,6 +123,18 @@ _SIGS = {
     "compas_b200_level_dts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
     "compas_b200_level_launches": (ctypes.c_longlong, [ctypes.c_void_p]),
     "compas_b200_level_pf_substeps": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "compas_b200_amr_create": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_int, ctypes.c_void_p,
+                                              ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "compas_b200_amr_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "compas_b200_amr_upload": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                              ctypes.c_void_p]),
+    "compas_b200_amr_download": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                                ctypes.c_void_p]),
+    "compas_b200_amr_advance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_void_p]),
+    "compas_b200_amr_sync": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_uint)]),
+    "compas_b200_amr_dts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
+    "compas_b200_amr_launches": (ctypes.c_longlong, [ctypes.c_void_p]),
     "compas_b200_level_pf_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "compas_b200_pf_grad_q": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_void_p,
                                              ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
@@ -388,6 +400,83 @@ class Level:
         _check(lib().compas_b200_level_pf_info(self._h, v))
         keys = ("max_v", "mobility", "eta", "mechanism_steps", "solver_iterations", "max_grad_q", "residual")
         return dict(zip(keys, v[:]))
+
+
+class AmrBox(ctypes.Structure):
+    """ctypes mirror of ``compas_b200_amr_box``."""
+
+    _fields_ = [("lev", ctypes.c_int), ("lo", ctypes.c_int * 3), ("hi", ctypes.c_int * 3)]
+
+
+class Amr:
+    """Multi-level advance of a fixed box hierarchy (refinement ratio 2, subcycling, refluxing):
+    boxes = [(lev, lo, hi), ...] with inclusive corners in each level's index space; g0 is level 0."""
+
+    def __init__(self, p: Parm, g0: Geom, boxes):
+        self._h = None
+        arr = (AmrBox * len(boxes))()
+        for b, (lev, lo, hi) in enumerate(boxes):
+            arr[b].lev = lev
+            for d in range(3):
+                arr[b].lo[d] = lo[d]
+                arr[b].hi[d] = hi[d]
+        self.boxes = list(boxes)
+        self.p, self.g0 = p, g0
+        h = ctypes.c_void_p()
+        nlev = 1 + max(b[0] for b in boxes)
+        _check(lib().compas_b200_amr_create(ctypes.byref(p), ctypes.byref(g0), nlev, arr, len(boxes), ctypes.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if self._h is not None:
+            lib().compas_b200_amr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, box: int, U, stream=None) -> None:
+        """Padded state of box `box` (numpy host array, or a torch tensor on host or device)."""
+        if isinstance(U, np.ndarray):
+            U = np.ascontiguousarray(U, dtype=np.float64)
+            _check(lib().compas_b200_amr_upload(self._h, box, U.ctypes.data, 0, _stream_ptr(stream)))
+        else:
+            _check(lib().compas_b200_amr_upload(self._h, box, U.data_ptr(), 1 if U.is_cuda else 0, _stream_ptr(stream)))
+
+    def download(self, box: int, out=None, stream=None):
+        lev, lo, hi = self.boxes[box]
+        n = [hi[d] - lo[d] + 1 for d in range(3)]
+        ng = self.g0.ng
+        dim = self.p.dim
+        shape = (nstate(self.p.physics, dim), (n[2] + 2 * ng) if dim == 3 else 1, n[1] + 2 * ng, n[0] + 2 * ng)
+        if out is None:
+            out = np.empty(shape, dtype=np.float64)
+        if isinstance(out, np.ndarray):
+            _check(lib().compas_b200_amr_download(self._h, box, out.ctypes.data, 0, _stream_ptr(stream)))
+            self.sync(check=False)
+        else:
+            _check(lib().compas_b200_amr_download(self._h, box, out.data_ptr(), 1 if out.is_cuda else 0,
+                                                  _stream_ptr(stream)))
+        return out
+
+    def advance(self, nsteps: int, stop_time: float = 1.0e300, stream=None) -> None:
+        _check(lib().compas_b200_amr_advance(self._h, int(nsteps), float(stop_time), _stream_ptr(stream)))
+
+    def sync(self, check: bool = True):
+        t, s, st = ctypes.c_double(), ctypes.c_int(), ctypes.c_uint()
+        _check(lib().compas_b200_amr_sync(self._h, ctypes.byref(t), ctypes.byref(s), ctypes.byref(st)))
+        return SyncInfo(t.value, s.value, st.value)
+
+    def dts(self, n: int) -> np.ndarray:
+        out = (ctypes.c_double * n)()
+        _check(lib().compas_b200_amr_dts(self._h, out, n))
+        return np.array(out[:], dtype=np.float64)
+
+    def launches(self) -> int:
+        return int(lib().compas_b200_amr_launches(self._h))
 
 
 @dataclass

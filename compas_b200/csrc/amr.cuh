@@ -1,0 +1,330 @@
+// Multi-level (AMR) advance of a fixed box hierarchy on the device: refinement ratio 2, subcycling,
+// TVD-RK3 per level through the persistent box-list stage kernel, coarse-fine ghost cells by linear
+// time interpolation and cell-conservative linear interpolation, conservative refluxing (with the
+// five-equation non-conservative alpha1 source) and average-down.
+//
+// Reference orchestration (source/): timeStepWithSubcycling Class_Compressible_PhaseField.cpp:4359-4451,
+// ThirdOrderSSPRK with flux registers :3937-4107 and :3472-3537, ComputeDt COMPAS.cpp:2249-2303,
+// FillPatch / FillPatchStage COMPAS.cpp:1598-1799 with GetData :1953-1985, AverageDownTo :1549-1558,
+// RefluxLev Class_Compressible5Eq_PhaseField.cpp:77-160. The AMReX operations (FillPatchTwoLevels,
+// lincc_interp, FluxRegister, average_down) follow their documented semantics; lincc_interp is the
+// monotonized-central limited linear interpolation per direction (fine value u_c + sum_d off_d s_d,
+// off_d = -1/4 or +1/4).
+//
+// Layout: every box keeps four padded arrays (two alternating time levels, two stage states); the
+// host builds, once per hierarchy, the tables of where every ghost cell, coarse-fine face and
+// covered coarse cell takes its data from, so a level fill is three table-driven launches.
+#pragma once
+
+#include <vector>
+
+namespace compas {
+
+// ghost cell copied from a valid cell of a box of the same level (periodic images included)
+struct AmrSame {
+    int db, sb;
+    long long dq, sq;
+};
+// ghost cell interpolated from the coarse level: stencil cells C, C-e0, C+e0, C-e1, C+e1 (, C-e2, C+e2)
+// with, per stencil cell, the coarse box, the padded index and the components whose value changes
+// sign through a reflecting boundary
+struct AmrInterp {
+    int db;
+    long long dq;
+    int cb[7];
+    long long cq[7];
+    unsigned odd[7];
+    int par;  // bit d set: the fine cell is the upper child along d (offset +1/4)
+};
+// ghost cell outside the domain along one direction: mirror / extrapolation within the same box
+struct AmrBc {
+    int b;
+    long long dq, sq;
+    unsigned odd;
+};
+// coarse-fine face between an uncovered coarse cell and the fine region
+struct AmrCf {
+    int cbox;                  // coarse box of the uncovered coarse cell
+    long long cq;              // its padded index
+    int cface[3];              // face index in the coarse box (local, nodal along d)
+    int d, hi_side;
+    int fbox[4];               // fine boxes and local face indices of the 2^(D-1) fine faces
+    int fface[4][3];
+};
+// covered coarse cell and its 2^D fine children
+struct AmrAvg {
+    int cb;
+    long long cq;
+    int fb[8];
+    long long fq[8];
+};
+
+struct AmrBoxH {
+    int lev;
+    int lo[3], hi[3], n[3];
+    Grid g;
+    double* buf[4] = {nullptr, nullptr, nullptr, nullptr};  // time levels 0/1, stage states 1/2
+    long long S;
+};
+
+struct AmrLevelH {
+    std::vector<int> boxes;
+    int dom[3];
+    double dx[3];
+    int parity = 0;  // buf[parity] is U_new, buf[1-parity] U_old
+    double t_old = 0.0, t_new = 0.0, dt = 1.e100;
+    double cmax = 0.0;
+    // box-list launch of the level: descriptors for both parities
+    BoxDesc* d_desc[2] = {nullptr, nullptr};
+    int* d_nbox = nullptr;
+    int* d_tile_off = nullptr;
+    // step control of the level on the device
+    double* d_dt = nullptr;
+    unsigned long long* d_cmax = nullptr;
+    int* d_done = nullptr;
+    // tables
+    AmrSame* d_same = nullptr;
+    long long n_same = 0;
+    AmrInterp* d_interp = nullptr;
+    long long n_interp = 0;
+    AmrBc* d_bc[3] = {nullptr, nullptr, nullptr};
+    long long n_bc[3] = {0, 0, 0};
+    // as the fine level of the pair (l-1, l): coarse-fine faces, registers, reflux groups
+    AmrCf* d_cf = nullptr;
+    int n_cf = 0;
+    double* d_reg = nullptr;
+    double* d_reg_nc = nullptr;
+    int* d_groups = nullptr;  // start of each coarse-cell group in the face list, n_groups + 1 entries
+    int n_groups = 0;
+    AmrAvg* d_avg = nullptr;  // covered cells of level l-1
+    long long n_avg = 0;
+};
+
+// ---- kernels -------------------------------------------------------------------------------------------
+struct AmrBufs {
+    double* const* p;          // p[box * 4 + k]
+    const long long* S;        // component stride of each box
+};
+
+__global__ void amr_same_kernel(const AmrSame* t, long long n, AmrBufs B, int dk, int sk, int N) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const AmrSame e = t[q];
+        double* dst = B.p[e.db * 4 + dk];
+        const double* src = B.p[e.sb * 4 + sk];
+        const long long Sd = B.S[e.db], Ss = B.S[e.sb];
+        for (int c = 0; c < N; ++c) dst[c * Sd + e.dq] = src[c * Ss + e.sq];
+    }
+}
+
+// mode 0: coarse new data, 1: coarse old data, 2: alpha old + beta new
+__device__ __forceinline__ double amr_coarse(const AmrBufs& B, int cb, long long cq, int c, int knew, int kold, int mode,
+                                             double alpha, double beta) {
+    const long long S = B.S[cb];
+    if (mode == 0) return B.p[cb * 4 + knew][c * S + cq];
+    if (mode == 1) return B.p[cb * 4 + kold][c * S + cq];
+    return alpha * B.p[cb * 4 + kold][c * S + cq] + beta * B.p[cb * 4 + knew][c * S + cq];
+}
+
+__global__ void amr_interp_kernel(const AmrInterp* t, long long n, AmrBufs B, int dk, int knew, int kold, int mode,
+                                  double alpha, double beta, int N, int D) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const AmrInterp& e = t[q];
+        double* dst = B.p[e.db * 4 + dk];
+        const long long Sd = B.S[e.db];
+        for (int c = 0; c < N; ++c) {
+            auto val = [&](int s) {
+                const double v = amr_coarse(B, e.cb[s], e.cq[s], c, knew, kold, mode, alpha, beta);
+                return ((e.odd[s] >> c) & 1u) ? -1.0 * v : 1.0 * v;
+            };
+            const double uc = val(0);
+            double u = uc;
+            for (int d = 0; d < D; ++d) {
+                const double um = val(1 + 2 * d), up = val(2 + 2 * d);
+                const double dc = 0.5 * (up - um), df = 2.0 * (up - uc), db = 2.0 * (uc - um);
+                double s = 0.0;
+                if (df * db >= 0.0) {
+                    const double m = dmin(fabs(dc), dmin(fabs(df), fabs(db)));
+                    s = (dc >= 0.0) ? m : -m;
+                }
+                const double off = ((e.par >> d) & 1) ? 0.25 : -0.25;
+                u = u + off * s;
+            }
+            dst[c * Sd + e.dq] = u;
+        }
+    }
+}
+
+__global__ void amr_bc_kernel(const AmrBc* t, long long n, AmrBufs B, int k, int N) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const AmrBc e = t[q];
+        double* a = B.p[e.b * 4 + k];
+        const long long S = B.S[e.b];
+        for (int c = 0; c < N; ++c) {
+            const double v = a[c * S + e.sq];
+            a[c * S + e.dq] = ((e.odd >> c) & 1u) ? -1.0 * v : 1.0 * v;
+        }
+    }
+}
+
+// face flux of face (i,j,k) (between cells i-1 and i along d) of a box with ghost-filled data U,
+// by the same sequence of device functions as the stage kernel (stage_kernel.cuh, step 2b)
+template <class M, int SCHEME, bool MIX>
+__device__ void amr_face_flux(const double* U, const Grid& g, int d, int i, int j, int k, const Eos& e, int id_k,
+                              double* F, double* fnc, unsigned int* err) {
+    using PT = typename std::conditional<MIX, float, double>::type;
+    constexpr int N = M::N, D = M::D;
+    PT P[6][N];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        int x = i, y = j, z = k;
+        if (d == 0) x += s - 3; else if (d == 1) y += s - 3; else z += s - 3;
+        double Uc[N];
+        const long long q = g.at(x, y, z);
+#pragma unroll
+        for (int c = 0; c < N; ++c) Uc[c] = U[c * g.S + q];
+        if constexpr (MIX) M::cons2prim_f32(P[s], Uc, e);
+        else M::cons2prim(P[s], Uc, e, nullptr);
+    }
+    double WfL[N], WfR[N], UL[N], UR[N];
+    constexpr int NB0 = (SCHEME == 6) ? 2 : 0;
+    constexpr int NB1 = (SCHEME == 6) ? M::IA : N;
+    double cm;
+    if constexpr (!MIX) {
+        if constexpr (SCHEME == 6) {
+            double r1[6], r2[6], al[6];
+#pragma unroll
+            for (int s = 0; s < 6; ++s) {
+                r1[s] = P[s][0];
+                r2[s] = P[s][1];
+                al[s] = P[s][M::IA];
+            }
+            weno5b_masses(r1, r2, al, 1, WfL[0], WfL[1], WfL[M::IA]);
+            weno5b_masses(r1 + 1, r2 + 1, al + 1, -1, WfR[0], WfR[1], WfR[M::IA]);
+        }
+#pragma unroll
+        for (int n = NB0; n < NB1; ++n) {
+            WfL[n] = weno5(P[0][n], P[1][n], P[2][n], P[3][n], P[4][n], 1);
+            WfR[n] = weno5(P[1][n], P[2][n], P[3][n], P[4][n], P[5][n], -1);
+        }
+        M::prim2cons(UL, WfL, e, err);
+        M::prim2cons(UR, WfR, e, err);
+        M::hllc(F, fnc, cm, UL, UR, e, d, id_k, err);
+    } else {
+        float wL[N], wR[N];
+        if constexpr (SCHEME == 6) {
+            float r1[6], r2[6], al[6];
+#pragma unroll
+            for (int s = 0; s < 6; ++s) {
+                r1[s] = P[s][0];
+                r2[s] = P[s][1];
+                al[s] = P[s][M::IA];
+            }
+            weno5b_masses_f32(r1, r2, al, 1, wL[0], wL[1], wL[M::IA]);
+            weno5b_masses_f32(r1 + 1, r2 + 1, al + 1, -1, wR[0], wR[1], wR[M::IA]);
+        }
+#pragma unroll
+        for (int n = NB0; n < NB1; ++n) {
+            wL[n] = weno5_f32(P[0][n], P[1][n], P[2][n], P[3][n], P[4][n], 1);
+            wR[n] = weno5_f32(P[1][n], P[2][n], P[3][n], P[4][n], P[5][n], -1);
+        }
+#pragma unroll
+        for (int n = 0; n < N; ++n) {
+            WfL[n] = wL[n];
+            WfR[n] = wR[n];
+        }
+        M::prim2cons(UL, WfL, e, err);
+        M::prim2cons(UR, WfR, e, err);
+        float cmf;
+        if constexpr (M::NC == 1) fiveeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, e, d, id_k);
+        else sixeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, e, d);
+    }
+}
+
+struct AmrCfArgs {
+    const AmrCf* cf;
+    int n;
+    double* reg;
+    double* reg_nc;
+    AmrBufs B;
+    const Grid* grids;  // per box
+    int k;              // array of the stage input
+    double w;           // the stage's dt share
+    double dA[3];       // face areas of the level computing the fluxes
+    Eos e;
+    int id_k;
+    int role;           // 0: coarse (CrseInit, scale -w), 1: fine (FineAdd, scale w)
+};
+
+template <class M, int SCHEME, bool MIX>
+__global__ void amr_cf_kernel(AmrCfArgs A) {
+    constexpr int N = M::N, NC = M::NC;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < A.n; t += gridDim.x * blockDim.x) {
+        const AmrCf& f = A.cf[t];
+        const double dA = (f.d == 0) ? A.dA[0] : (f.d == 1 ? A.dA[1] : A.dA[2]);
+        double F[N], fnc[NC];
+        if (A.role == 0) {
+            amr_face_flux<M, SCHEME, MIX>(A.B.p[f.cbox * 4 + A.k], A.grids[f.cbox], f.d, f.cface[0], f.cface[1],
+                                          f.cface[2], A.e, A.id_k, F, fnc, nullptr);
+            for (int c = 0; c < N; ++c) A.reg[(long long)t * N + c] += (-A.w) * (F[c] * dA);
+            for (int c = 0; c < NC; ++c) A.reg_nc[(long long)t * NC + c] += (-A.w) * (fnc[c] * dA);
+        } else {
+            const int nf = (M::D == 3) ? 4 : 2;
+            for (int a = 0; a < nf; ++a) {
+                amr_face_flux<M, SCHEME, MIX>(A.B.p[f.fbox[a] * 4 + A.k], A.grids[f.fbox[a]], f.d, f.fface[a][0],
+                                              f.fface[a][1], f.fface[a][2], A.e, A.id_k, F, fnc, nullptr);
+                for (int c = 0; c < N; ++c) A.reg[(long long)t * N + c] += A.w * (F[c] * dA);
+                for (int c = 0; c < NC; ++c) A.reg_nc[(long long)t * NC + c] += A.w * (fnc[c] * dA);
+            }
+        }
+    }
+}
+
+// FluxRegister::Reflux and, for the five-equation model, RefluxSourceTerms: one thread per coarse cell,
+// its faces in list order
+template <class M>
+__global__ void amr_reflux_kernel(const AmrCf* cf, const int* groups, int ngroups, const double* reg,
+                                  const double* reg_nc, AmrBufs B, int knew, double vol, Eos e, int id_k) {
+    constexpr int N = M::N, NC = M::NC;
+    for (int gi = blockIdx.x * blockDim.x + threadIdx.x; gi < ngroups; gi += gridDim.x * blockDim.x) {
+        const int t0 = groups[gi], t1 = groups[gi + 1];
+        const AmrCf& f0 = cf[t0];
+        double* U = B.p[f0.cbox * 4 + knew];
+        const long long S = B.S[f0.cbox];
+        double src = 0.0;
+        if constexpr (NC == 1) {
+            double Uc[N], W[N];
+            for (int c = 0; c < N; ++c) Uc[c] = U[c * S + f0.cq];
+            M::cons2prim(W, Uc, e, nullptr);
+            src = M::kapila_factor(Uc, W, e, id_k, nullptr);
+        }
+        double xs = 0.0;
+        for (int t = t0; t < t1; ++t) {
+            const double mult = cf[t].hi_side ? -1.0 : 1.0;
+            for (int c = 0; c < N; ++c) U[c * S + f0.cq] += mult * reg[(long long)t * N + c] / vol;
+            const double xi = mult * reg_nc[(long long)t * NC] / vol;
+            xs = (t == t0) ? xi : xs + xi;
+        }
+        if constexpr (NC == 1) U[M::IA * S + f0.cq] += -1.0 * (xs * src);
+    }
+}
+
+__global__ void amr_avg_kernel(const AmrAvg* t, long long n, AmrBufs B, int kc, int kf, int N, int nchild,
+                               double volfrac) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const AmrAvg& e = t[q];
+        double* C = B.p[e.cb * 4 + kc];
+        const long long Sc = B.S[e.cb];
+        for (int c = 0; c < N; ++c) {
+            double s = 0.0;
+            for (int h = 0; h < nchild; ++h) s += B.p[e.fb[h] * 4 + kf][c * B.S[e.fb[h]] + e.fq[h]];
+            C[c * Sc + e.cq] = volfrac * s;
+        }
+    }
+}
+
+__global__ void amr_set_kernel(double* dt, double v, unsigned long long* cmax) {
+    *dt = v;
+    if (cmax) *cmax = 0ull;
+}
+
+}  // namespace compas

@@ -405,6 +405,7 @@ static int noalloc_scratch(unsigned char** out) {
 }  // namespace compas
 
 #include "batch.cuh"
+#include "amr.cuh"
 
 // ================================================================================================
 // C ABI
@@ -1373,3 +1374,5 @@ long long compas_b200_batch_bytes(compas_b200_batch* b) { return b ? b->bytes_in
 long long compas_b200_batch_launches(compas_b200_batch* b) { return b ? b->launches : 0; }
 
 }  // extern "C"
+
+#include "amr_api.inc"

@@ -475,6 +475,7 @@ struct BoxDesc {
     double trace;
     int tiles;                    // tiles of the box for the kernel's tile shape
     long long ghosts;             // ghost cells of one array of the box
+    double* out_last;             // output of the last stage (nullptr: in place over U[0])
 };
 
 struct ListArgs {
@@ -511,7 +512,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_list_kernel(ListArgs L) {
         a.stage = L.stage;
         a.Us = B.U[L.stage];
         a.U0 = B.U[0];
-        a.Uout = B.U[(L.stage + 1) % 3];
+        a.Uout = (L.stage == 2 && B.out_last) ? B.out_last : B.U[(L.stage + 1) % 3];
         a.dt = B.dt;
         a.done = B.done;
         a.cmax = B.cmax;

@@ -277,6 +277,37 @@ int compas_b200_batch_download(compas_b200_batch* b, int case_id, double* dst, i
 long long compas_b200_batch_bytes(compas_b200_batch* b);
 long long compas_b200_batch_launches(compas_b200_batch* b);
 
+/* ---- multi-level (AMR) advance of a fixed box hierarchy ------------------------------------------
+ * Replaces timeStepWithSubcycling with its per-level ThirdOrderSSPRK, FillPatch / FillPatchStage,
+ * flux registers, RefluxLev and AverageDownTo (source/Class_Compressible_PhaseField.cpp:4359-4451,
+ * :3937-4107, :3472-3537; source/COMPAS.cpp:1549-1558, 1598-1799, 2249-2303;
+ * source/Class_Compressible5Eq_PhaseField.cpp:77-160) for a hierarchy that does not regrid:
+ * refinement ratio 2, subcycling, TVD-RK3 (FIVEEQS, WENO5 / WENO5B). Every level's boxes advance
+ * together in one persistent box-list launch per RK stage. g0 describes level 0 (domain cells,
+ * cell size, ghost width, boundary codes); box b lives on level boxes[b].lev with inclusive corners
+ * lo / hi in that level's index space. Level 0 must tile the domain; every finer level must be
+ * properly nested (its ghost cells and their interpolation stencil reach valid coarser cells). */
+typedef struct compas_b200_amr compas_b200_amr;
+typedef struct compas_b200_amr_box {
+    int lev;
+    int lo[3];
+    int hi[3];
+} compas_b200_amr_box;
+
+int compas_b200_amr_create(const compas_b200_parm* p, const compas_b200_geom* g0, int nlev,
+                           const compas_b200_amr_box* boxes, int nbox, compas_b200_amr** out);
+int compas_b200_amr_destroy(compas_b200_amr* A);
+/* State of box b (padded Array4 layout of a single box of the box's size and ghost width). */
+int compas_b200_amr_upload(compas_b200_amr* A, int box, const double* src, int is_device, void* stream);
+int compas_b200_amr_download(compas_b200_amr* A, int box, double* dst, int is_device, void* stream);
+/* nsteps level-0 steps (each with its subcycled finer steps); the host computes dt from the levels'
+ * wave speeds (ComputeDt), so every step synchronises the stream once. */
+int compas_b200_amr_advance(compas_b200_amr* A, int nsteps, double stop_time, void* stream);
+int compas_b200_amr_sync(compas_b200_amr* A, double* t, int* steps, unsigned int* status);
+/* Level-0 step sizes taken so far (the first n). */
+int compas_b200_amr_dts(const compas_b200_amr* A, double* dts, int n);
+long long compas_b200_amr_launches(const compas_b200_amr* A);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1065,3 +1065,8 @@ int cmp_advance_pf(const cmp_case* c, const cmp_pf* pf, double* U, int nsteps, d
     (void)c; (void)pf; (void)U; (void)nsteps; (void)stop_time; (void)t; (void)dts;
     return -2;
 }
+int cmp_amr_advance(const cmp_case* c, int nlev, const cmp_amr_box* boxes, int nbox, double** U, int nsteps,
+                    double stop_time, double* t, double* dts) {
+    (void)c; (void)nlev; (void)boxes; (void)nbox; (void)U; (void)nsteps; (void)stop_time; (void)t; (void)dts;
+    return -2;
+}

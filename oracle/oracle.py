@@ -66,7 +66,15 @@ _SIGS = {
     "cmp_pf_grad_q": (ctypes.c_int, [_P, ctypes.c_void_p, _D, ctypes.c_double, _D, _D, _D, _D]),
     "cmp_advance_pf": (ctypes.c_int, [_P, ctypes.c_void_p, _D, ctypes.c_int, ctypes.c_double,
                                       ctypes.POINTER(ctypes.c_double), _D]),
+    "cmp_amr_advance": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                       ctypes.c_double, ctypes.POINTER(ctypes.c_double), _D]),
 }
+
+
+class AmrBox(ctypes.Structure):
+    """ctypes mirror of ``cmp_amr_box`` (oracle/oracle_api.h)."""
+
+    _fields_ = [("lev", ctypes.c_int), ("lo", ctypes.c_int * 3), ("hi", ctypes.c_int * 3)]
 
 
 class PfCase(ctypes.Structure):
@@ -228,6 +236,28 @@ class Oracle:
         dts = np.zeros(max(nsteps, 1), dtype=np.float64)
         n = self._call(self.lib.cmp_advance_pf(self._c, self._pf(pf), U.ctypes.data, nsteps, stop_time,
                                                ctypes.byref(t), dts.ctypes.data))
+        return t.value, dts[:n]
+
+    # ---- multi-level advance (reference-header build only) ---------------------------------------
+    def amr_advance(self, boxes, states, nsteps: int, stop_time: float = 1e300, t0: float = 0.0):
+        """boxes: [(lev, lo, hi)], states: padded float64 arrays (advanced in place); self's case is
+        level 0."""
+        if self.kind != "reference":
+            raise RuntimeError("the multi-level advance is in the reference-header oracle only")
+        arr = (AmrBox * len(boxes))()
+        for b, (lev, lo, hi) in enumerate(boxes):
+            arr[b].lev = lev
+            for d in range(3):
+                arr[b].lo[d] = lo[d]
+                arr[b].hi[d] = hi[d]
+        for U in states:
+            assert U.flags.c_contiguous and U.dtype == np.float64
+        ptrs = (ctypes.c_void_p * len(states))(*[U.ctypes.data for U in states])
+        t = ctypes.c_double(t0)
+        dts = np.zeros(max(nsteps, 1), dtype=np.float64)
+        nlev = 1 + max(b[0] for b in boxes)
+        n = self._call(self.lib.cmp_amr_advance(self._c, nlev, arr, len(boxes), ptrs, nsteps, stop_time,
+                                                ctypes.byref(t), dts.ctypes.data))
         return t.value, dts[:n]
 
     def threads(self) -> int:

@@ -98,6 +98,22 @@ int cmp_pf_grad_q(const cmp_case* c, const cmp_pf* pf, const double* U, double d
 int cmp_advance_pf(const cmp_case* c, const cmp_pf* pf, double* U, int nsteps, double stop_time, double* t,
                    double* dts);
 
+/* Multi-level (AMR) advance of a fixed box hierarchy, refinement ratio 2, with subcycling, flux
+ * registers, reflux and average-down (timeStepWithSubcycling, source/Class_Compressible_PhaseField.cpp:
+ * 4359-4451). c describes level 0 (domain cells, cell size, boundary codes, scheme); box b lives on
+ * level boxes[b].lev with inclusive corners lo/hi in that level's index space, and U[b] is its
+ * padded state (the Array4 layout of a single-box case of the box's size). Level 0 must cover the
+ * domain and every level must be properly nested in the one below. The reference-header build
+ * implements it; the plain-C port returns -2. Returns the number of level-0 steps. */
+typedef struct cmp_amr_box {
+    int lev;
+    int lo[3];
+    int hi[3];
+} cmp_amr_box;
+
+int cmp_amr_advance(const cmp_case* c, int nlev, const cmp_amr_box* boxes, int nbox, double** U, int nsteps,
+                    double stop_time, double* t, double* dts);
+
 #ifdef __cplusplus
 }
 #endif

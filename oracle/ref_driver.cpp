@@ -160,7 +160,9 @@ void fill_ghosts(const cmp_case* c, double* U) {
 
 // ComputeFaceFluxes + FluxDivergence of one level state (ghosts filled). cmax: largest face wave
 // speed over the faces (i,j,k) with (i,j,k) a valid cell (the low faces), as c_max.norminf(0,0,true).
-void compute_dudt(const cmp_case* c, const Parm& parm, const double* U, double* dUdt, double* cmax_out) {
+void compute_dudt(const cmp_case* c, const Parm& parm, const double* U, double* dUdt, double* cmax_out,
+                  std::vector<std::vector<double>>* faces_out = nullptr,
+                  std::vector<std::vector<double>>* faces_nc_out = nullptr) {
     Geo g(c);
     const int nc = NSTATE;
     auto statein = g.view(U, nc);
@@ -225,6 +227,8 @@ void compute_dudt(const cmp_case* c, const Parm& parm, const double* U, double* 
                                AMREX_D_DECL(dx, dy, dz), parm, parm.Physics_Parm);
     }
     if (cmax_out) *cmax_out = cmax_all;
+    if (faces_out) *faces_out = F;
+    if (faces_nc_out) *faces_nc_out = FNC;
 }
 
 void relax(const cmp_case* c, const Parm& parm, double* U) {
@@ -857,6 +861,8 @@ void pf_step(const cmp_case* c, const cmp_pf* pf, double* U, double dt, double* 
 }
 #endif  // PHYSICS == FIVEEQS
 
+#include "ref_amr.inc"
+
 template <class Fn>
 int guarded(Fn&& fn) {
     try {
@@ -1001,6 +1007,13 @@ int cmp_advance_pf(const cmp_case* c, const cmp_pf* pf, double* U, int nsteps, d
     (void)c; (void)pf; (void)U; (void)nsteps; (void)stop_time; (void)t; (void)dts;
     return -2;
 #endif
+}
+
+int cmp_amr_advance(const cmp_case* c, int nlev, const cmp_amr_box* boxes, int nbox, double** U, int nsteps,
+                    double stop_time, double* t, double* dts) {
+    int taken = 0;
+    int rc = guarded([&] { taken = amr_advance(c, nlev, boxes, nbox, U, nsteps, stop_time, t, dts); });
+    return rc == 0 ? taken : rc;
 }
 
 }  // extern "C"

@@ -100,3 +100,48 @@ def test_mirror_symmetry_of_the_droplet():
     V = cb.valid_view(U, p, g)
     for c in (0, 1, 2, 5, 6, 7):
         np.testing.assert_allclose(V[c], V[c][:, ::-1, :], rtol=1e-8, atol=1e-8 * np.abs(V[c]).max())
+
+
+def _amr_run(max_grid_size, steps=3):
+    from compas_b200 import amr
+
+    kw = dict(nx=64, ny=32, scheme="WENO5B")
+    phys, dim, inputs, geom, _ = cases.shock_bubble(**kw)
+    p, g = _parm_geom(phys, dim, inputs, geom)
+    regions = [((40, 16, 0), (95, 47, 0)), ((96, 48, 0), (175, 79, 0))]
+    boxes = amr.hierarchy((64, 32), dim, regions, max_grid_size)
+    states = amr.box_states(cases.shock_bubble, kw, (64, 32), dim, boxes)
+    _, dts = Oracle("reference", p, g).amr_advance(boxes, states, steps)
+    # each level as one array
+    out = {}
+    for (lev, lo, hi), S in zip(boxes, states):
+        scale = 1 << lev
+        a = out.setdefault(lev, np.full((S.shape[0], 32 * scale, 64 * scale), np.nan))
+        a[:, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1] = S[:, 0, 3:3 + hi[1] - lo[1] + 1, 3:3 + hi[0] - lo[0] + 1]
+    return dts, out
+
+
+@pytest.mark.skipif(not have_ref(cb.FIVEEQS, 2), reason="reference-header oracle not built here")
+def test_amr_oracle_independent_of_box_decomposition():
+    dts_a, a = _amr_run(32)
+    dts_b, b = _amr_run(8)
+    np.testing.assert_array_equal(dts_a, dts_b)
+    for lev in a:
+        np.testing.assert_array_equal(a[lev], b[lev])
+
+
+@pytest.mark.skipif(not have_ref(cb.FIVEEQS, 2), reason="reference-header oracle not built here")
+def test_amr_oracle_conserves_composite_totals_periodic():
+    from compas_b200 import amr
+
+    kw = dict(n=32)
+    phys, dim, inputs, geom, _ = cases.advected_disc(**kw)
+    p, g = _parm_geom(phys, dim, inputs, geom)
+    boxes = amr.hierarchy((32, 32), 2, [((16, 16, 0), (47, 47, 0)), ((40, 40, 0), (87, 87, 0))], 16)
+    states = amr.box_states(cases.advected_disc, kw, (32, 32), 2, boxes)
+    cov = amr.covered_mask_fn(boxes, 2)
+    s0 = [amr.composite_sum(states, boxes, 2, 3, c, cov) for c in range(5)]
+    Oracle("reference", p, g).amr_advance(boxes, states, 6)
+    s1 = [amr.composite_sum(states, boxes, 2, 3, c, cov) for c in range(5)]
+    for a, b in zip(s0, s1):
+        assert abs(a - b) <= 1e-13 * abs(a)

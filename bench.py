@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--batch-steps", type=int, default=10)
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-phase-field", action="store_true")
+    ap.add_argument("--no-amr", action="store_true")
+    ap.add_argument("--amr-steps", type=int, default=5)
     ap.add_argument("--pf-steps", type=int, default=10)
     ap.add_argument("--serve-requests", type=int, default=16)
     ap.add_argument("--serve-rate", type=float, default=16.0)
@@ -259,6 +261,58 @@ def run_phase_field(args):
     return out
 
 
+def run_amr(args):
+    """3-level AMR shock-helium-bubble (refinement ratio 2, max_grid_size drawn with numpy PCG64 seed 0
+    from {32, 64, 128}): level 0 512 x 256 on [0,2]x[0,1], level 1 around the shock and the bubble,
+    level 2 around the bubble; every level's boxes advance through the persistent box-list stage
+    kernel, one launch per RK stage, subcycled, with refluxing and average-down. Rate: composite
+    cell-updates per RK stage (each level's cells x its substeps x 3) per second."""
+    import numpy as np
+    import torch
+
+    import compas_b200 as cb
+    from compas_b200 import amr, cases
+
+    rng = np.random.Generator(np.random.PCG64(0))
+    mgs = int(rng.choice([32, 64, 128]))
+    kw = dict(nx=512, ny=256, scheme="WENO5B")
+    phys, dim, inputs, geom, _ = cases.shock_bubble(**kw, quadrature=False)
+    regions = [((64, 96, 0), (895, 415, 0)), ((512, 256, 0), (1407, 767, 0))]
+    boxes = amr.hierarchy((512, 256), dim, regions, mgs)
+    states = amr.box_states(cases.shock_bubble, kw, (512, 256), dim, boxes, xp=torch, device="cuda")
+    cells = [0, 0, 0]
+    for lev, lo, hi in boxes:
+        cells[lev] += (hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1)
+    per_step = sum(c * (1 << lev) for lev, c in enumerate(cells)) * 3
+    out = {"workload": f"3-level AMR 2D FIVEEQS shock-helium-bubble, level 0 512x256, max_grid_size {mgs} (seed 0), "
+                       f"WENO5B+HLLC, subcycled TVD-RK3 with refluxing", "boxes": len(boxes),
+           "cells_per_level": cells, "steps": args.amr_steps,
+           "unit": UNIT + " per RK stage (composite: each level's cells x substeps)"}
+    stream = torch.cuda.current_stream()
+    for prec in ("mixed", "fp64"):
+        p = cb.make_parm(phys, dim, dict(inputs, **{"compas_b200.precision": prec}))
+        A = cb.Amr(p, cb.make_geom(**geom), boxes)
+        for b, U in enumerate(states):
+            A.upload(b, U, stream=stream)
+        A.advance(2, stream=stream)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        l0 = A.launches()
+        e0.record(stream)
+        A.advance(args.amr_steps, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        assert A.sync().status == 0
+        out[prec] = per_step * args.amr_steps / (ms / 1e3)
+        out[f"{prec}_ms_per_coarse_step"] = ms / args.amr_steps
+        out[f"{prec}_launches_per_coarse_step"] = (A.launches() - l0) / args.amr_steps
+        A.close()
+    out["mixed_vs_fp64"] = out["mixed"] / out["fp64"]
+    return out
+
+
 def run_serving(args):
     """Poisson arrivals of mixed 2D shock-bubble / 3D shock-droplet solves under an HBM budget,
     continuous batching, against the same requests one at a time on the plain FP64 path."""
@@ -462,6 +516,7 @@ def run_ours(args, rank, world, dist):
         batched = None if args.no_batched else run_batched(args)
         serving_res = None if args.no_serving else run_serving(args)
         pf_res = None if args.no_phase_field else run_phase_field(args)
+        amr_res = None if args.no_amr else run_amr(args)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms[head] / args.steps, "higher_is_better": True,
@@ -488,6 +543,7 @@ def run_ours(args, rank, world, dist):
             "batched": batched,
             "serving": serving_res,
             "phase_field": pf_res,
+            "amr": amr_res,
         }
     return line
 

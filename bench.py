@@ -45,8 +45,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256, help="cells per direction of the cube")
-    ap.add_argument("--cpu-n", type=int, default=96, help="cube side of the CPU sample")
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-n", type=int, default=128, help="cube side of the CPU sample")
+    ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
     ap.add_argument("--no-batched", action="store_true")
@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--no-amr", action="store_true")
     ap.add_argument("--amr-steps", type=int, default=5)
     ap.add_argument("--pf-steps", type=int, default=10)
+    ap.add_argument("--no-triple", action="store_true")
+    ap.add_argument("--triple-m", type=int, default=256, help="triple point side: 7m x 3m cells")
+    ap.add_argument("--triple-steps", type=int, default=20)
     ap.add_argument("--serve-requests", type=int, default=16)
     ap.add_argument("--serve-rate", type=float, default=16.0)
     return ap.parse_args()
@@ -313,13 +316,58 @@ def run_amr(args):
     return out
 
 
+def run_triple_point(args):
+    """2D FIVEEQS_NPHASE (NPHASE = 3) triple point on [0,7]x[0,3] at 1792 x 768 cells (sharp
+    interfaces, reflecting walls, WENO5 with the consistent limiter + HLLC + TVD-RK3, cfl 0.4), both
+    precisions, single-box level advance timed with CUDA events."""
+    import torch
+
+    import compas_b200 as cb
+    from compas_b200 import cases
+
+    stream = torch.cuda.current_stream()
+    m = args.triple_m
+    phys, dim, inputs, geom, U = cases.triple_point(m=m, xp=torch, device="cuda")
+    g = cb.make_geom(**geom)
+    cells = geom["n"][0] * geom["n"][1]
+    K, W = args.triple_steps, 3
+    bytes_cs = cases.algorithmic_bytes_per_cell_stage(phys, dim, 3)
+    peak = measured_peaks()[0]
+    out = {"workload": f"2D FIVEEQS_NPHASE (NPHASE 3) triple point {7 * m}x{3 * m} on [0,7]x[0,3], WENO5 "
+                       "(consistent limiter)+HLLC+TVD-RK3, reflecting walls", "cells": cells, "steps": K,
+           "unit": UNIT, "algorithmic_bytes_per_cell_stage": bytes_cs}
+    for prec in ("mixed", "fp64"):
+        p = cb.make_parm(phys, dim, dict(inputs, **{"compas_b200.precision": prec}))
+        lv = cb.Level(p, g)
+        lv.upload(U, stream=stream)
+        lv.advance(W, stream=stream)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        lv.advance(K, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        info = lv.sync()
+        assert info.status == 0
+        rate = cells * 3 * K / (ms / 1e3)
+        out[prec] = rate
+        out[f"{prec}_ms_per_step"] = ms / K
+        out[f"{prec}_hbm_frac_of_measured"] = rate * bytes_cs / 1e9 / peak if peak else None
+        lv.close()
+    out["mixed_vs_fp64"] = out["mixed"] / out["fp64"]
+    return out
+
+
 def run_serving(args):
-    """Poisson arrivals of mixed 2D shock-bubble / 3D shock-droplet solves under an HBM budget,
-    continuous batching, against the same requests one at a time on the plain FP64 path."""
+    """Poisson arrivals of mixed 2D shock-bubble / 3D shock-droplet / 2D three-material triple-point
+    solves under an HBM budget, continuous batching, against the same requests one at a time on the
+    plain FP64 path."""
     from compas_b200 import serving
 
     reqs = serving.poisson_requests(args.serve_requests, args.serve_rate, seed=0, sides2d=(128, 512),
-                                    sides3d=(64, 96), steps=(100, 300))
+                                    sides3d=(64, 96), sides_triple=(32, 96), steps=(100, 300))
     srv = serving.Server(budget_bytes=150e9, precision="mixed", steps_per_iter=4)
     t0 = time.perf_counter()
     done = srv.run(reqs)
@@ -327,8 +375,10 @@ def run_serving(args):
     srv.close()
     summ = serving.summarize(done, wall)
     seq = serving.sequential_baseline(reqs, precision="fp64")
-    return {"workload": f"{len(reqs)} requests, Poisson rate {args.serve_rate}/s (seed 0): 2D FIVEEQS shock-bubble "
-                        "128^2-512^2 and 3D SIXEQS shock-droplet 64^3-96^3, 100-300 steps each; budget 150 GB",
+    kinds = {k: sum(1 for r in reqs if r.kind == k) for k in serving.KINDS}
+    return {"workload": f"{len(reqs)} requests {kinds}, Poisson rate {args.serve_rate}/s (seed 0): 2D FIVEEQS "
+                        "shock-bubble 128^2-512^2, 3D SIXEQS shock-droplet 64^3-96^3 and 2D FIVEEQS_NPHASE (NPHASE 3) "
+                        "triple point 224x96-672x288, 100-300 steps each; budget 150 GB",
             "continuous_batching_mixed": summ, "sequential_fp64": seq,
             "throughput_ratio": summ["cell_updates_per_s_per_stage"] / seq["cell_updates_per_s_per_stage"]}
 
@@ -517,6 +567,7 @@ def run_ours(args, rank, world, dist):
         serving_res = None if args.no_serving else run_serving(args)
         pf_res = None if args.no_phase_field else run_phase_field(args)
         amr_res = None if args.no_amr else run_amr(args)
+        triple_res = None if args.no_triple else run_triple_point(args)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms[head] / args.steps, "higher_is_better": True,
@@ -544,6 +595,7 @@ def run_ours(args, rank, world, dist):
             "serving": serving_res,
             "phase_field": pf_res,
             "amr": amr_res,
+            "triple_point": triple_res,
         }
     return line
 

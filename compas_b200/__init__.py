@@ -20,6 +20,8 @@ import numpy as np
 
 FIVEEQS = 555
 SIXEQS = 666
+FIVEEQS_NPHASE = 55501
+MAX_PHASES = 4
 
 OK = 0
 EARG, ECUDA, ENOMEM, ESTATE, EUNSUPPORTED = -1, -2, -3, -4, -5
@@ -73,6 +75,11 @@ class Parm(ctypes.Structure):
         ("pf_cfl", ctypes.c_double),
         ("pf_max_step", ctypes.c_int),
         ("pf_tol_rel", ctypes.c_double),
+        ("nphase", ctypes.c_int),
+        ("gamma_k", ctypes.c_double * MAX_PHASES), ("pinf_k", ctypes.c_double * MAX_PHASES),
+        ("b_k", ctypes.c_double * MAX_PHASES), ("q_k", ctypes.c_double * MAX_PHASES),
+        ("Ak", ctypes.c_double * MAX_PHASES), ("Bk", ctypes.c_double * MAX_PHASES),
+        ("Ck", ctypes.c_double * MAX_PHASES), ("Dk", ctypes.c_double * MAX_PHASES),
     ]
 
 
@@ -93,6 +100,7 @@ _lib_handle = None
 _SIGS = {
     "compas_b200_last_error": (ctypes.c_char_p, []),
     "compas_b200_parm_init": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.c_int, ctypes.c_int]),
+    "compas_b200_parm_init_nphase": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "compas_b200_parm_set": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.c_char_p, ctypes.c_char_p]),
     "compas_b200_parm_finalize": (ctypes.c_int, [ctypes.POINTER(Parm)]),
     "compas_b200_state_bytes": (ctypes.c_longlong, [ctypes.POINTER(Parm), ctypes.POINTER(Geom)]),
@@ -148,6 +156,8 @@ _SIGS = {
                                                 ctypes.c_void_p]),
     "compas_b200_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                 ctypes.POINTER(ctypes.c_void_p)]),
+    "compas_b200_batch_create_nphase": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                       ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "compas_b200_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "compas_b200_batch_add": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Parm), ctypes.POINTER(Geom),
                                              ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int,
@@ -185,18 +195,34 @@ def _check(rc: int) -> None:
         raise CompasError(rc, lib().compas_b200_last_error().decode())
 
 
-def nstate(physics: int, dim: int) -> int:
-    """NSTATE of the model (include/Macros.H:73, :114)."""
+def nstate(physics: int, dim: int, nphase: int = 2) -> int:
+    """NSTATE of the model (include/Macros.H:73, :89, :114)."""
+    if physics == FIVEEQS_NPHASE:
+        return 2 * nphase + dim + 1
     return (4 if physics == FIVEEQS else 5) + dim
 
 
-def make_parm(physics: int, dim: int, inputs: dict | None = None) -> Parm:
+def parm_nstate(p: Parm) -> int:
+    return nstate(p.physics, p.dim, p.nphase)
+
+
+def _inputs_value(v) -> str:
+    if isinstance(v, (list, tuple)):
+        return " ".join(str(x) for x in v)
+    return str(v)
+
+
+def make_parm(physics: int, dim: int, inputs: dict | None = None, nphase: int | None = None) -> Parm:
     """A parameter block from reference defaults plus inputs keys, e.g.
-    {"FiniteVolume.Scheme": "WENO5", "prob.EOS.gamma_2": 4.4, "run.cfl": 0.5}."""
+    {"FiniteVolume.Scheme": "WENO5", "prob.EOS.gamma_2": 4.4, "run.cfl": 0.5}; for FIVEEQS_NPHASE the
+    per-phase lists {"prob.EOS.gamma": [1.4, 1.5, 1.5]} and `nphase` (the compile-time NPHASE)."""
     p = Parm()
-    _check(lib().compas_b200_parm_init(ctypes.byref(p), physics, dim))
+    if nphase is None:
+        g = (inputs or {}).get("prob.EOS.gamma")
+        nphase = len(g) if physics == FIVEEQS_NPHASE and isinstance(g, (list, tuple)) else 2
+    _check(lib().compas_b200_parm_init_nphase(ctypes.byref(p), physics, dim, int(nphase)))
     for k, v in (inputs or {}).items():
-        _check(lib().compas_b200_parm_set(ctypes.byref(p), k.encode(), str(v).encode()))
+        _check(lib().compas_b200_parm_set(ctypes.byref(p), k.encode(), _inputs_value(v).encode()))
     _check(lib().compas_b200_parm_finalize(ctypes.byref(p)))
     return p
 
@@ -218,7 +244,7 @@ def padded_shape(p: Parm, g: Geom) -> tuple:
     """(N, PZ, PY, PX) of a state array with ghosts (no z ghosts in 2D)."""
     gz = g.ng if p.dim == 3 else 0
     nz = g.n[2] if p.dim == 3 else 1
-    return (nstate(p.physics, p.dim), nz + 2 * gz, g.n[1] + 2 * g.ng, g.n[0] + 2 * g.ng)
+    return (parm_nstate(p), nz + 2 * gz, g.n[1] + 2 * g.ng, g.n[0] + 2 * g.ng)
 
 
 def valid_view(a, p: Parm, g: Geom):
@@ -451,7 +477,7 @@ class Amr:
         n = [hi[d] - lo[d] + 1 for d in range(3)]
         ng = self.g0.ng
         dim = self.p.dim
-        shape = (nstate(self.p.physics, dim), (n[2] + 2 * ng) if dim == 3 else 1, n[1] + 2 * ng, n[0] + 2 * ng)
+        shape = (parm_nstate(self.p), (n[2] + 2 * ng) if dim == 3 else 1, n[1] + 2 * ng, n[0] + 2 * ng)
         if out is None:
             out = np.empty(shape, dtype=np.float64)
         if isinstance(out, np.ndarray):
@@ -492,10 +518,12 @@ class Batch:
     """Many independent single-box cases (uneven sizes, own EOS and boundaries, own time-step control)
     advanced together, one persistent launch per RK stage over a device-side box list."""
 
-    def __init__(self, physics: int, dim: int, id_limiter: int = 5, precision: int = 0, capacity: int = 1024):
-        self.physics, self.dim = physics, dim
+    def __init__(self, physics: int, dim: int, id_limiter: int = 5, precision: int = 0, capacity: int = 1024,
+                 nphase: int = 2):
+        self.physics, self.dim, self.nphase = physics, dim, nphase
         self._h = ctypes.c_void_p()
-        _check(lib().compas_b200_batch_create(physics, dim, id_limiter, precision, capacity, ctypes.byref(self._h)))
+        _check(lib().compas_b200_batch_create_nphase(physics, dim, nphase, id_limiter, precision, capacity,
+                                                     ctypes.byref(self._h)))
         self.capacity = capacity
         self._shapes = {}
 

@@ -11,7 +11,7 @@ import math
 
 import numpy as np
 
-from . import FIVEEQS, SIXEQS, nstate
+from . import FIVEEQS, FIVEEQS_NPHASE, SIXEQS, nstate
 
 # Gauss-Legendre nodes and weights on [-1, 1] (4 points, exact to degree 7)
 _GL_X, _GL_W = np.polynomial.legendre.leggauss(4)
@@ -68,9 +68,9 @@ def _cons_from_prims(physics, dim, ar1, ar2, vel, p, alpha1, A, B, xp):
     return out
 
 
-def _average(physics, dim, n, dx, lo, pointwise, ng, quadrature, xp, device):
+def _average(physics, dim, n, dx, lo, pointwise, ng, quadrature, xp, device, nphase=2):
     """Padded state whose valid cells hold the cell averages of pointwise(x, y, z) -> list of N arrays."""
-    N = nstate(physics, dim)
+    N = nstate(physics, dim, nphase)
     gz = ng if dim == 3 else 0
     nz = n[2] if dim == 3 else 1
     shape = (N, nz + 2 * gz, n[1] + 2 * ng, n[0] + 2 * ng)
@@ -208,6 +208,141 @@ def shock_bubble(nx=2048, ny=1024, ng=3, quadrature=True, xp=None, device=None, 
     return physics, dim, inputs, geom, U
 
 
+def _box_level_set_2d(xp, x, y, xmin, ymin, xmax, ymax):
+    """Signed distance to the rectangle [xmin, xmax] x [ymin, ymax], negative inside (the triple-point
+    problem's boxLevelSet2D, exec/TriplePoint-5Eq-N/prob/ProblemICBC.H:15-34)."""
+    cx, cy = 0.5 * (xmin + xmax), 0.5 * (ymin + ymax)
+    hx, hy = 0.5 * (xmax - xmin), 0.5 * (ymax - ymin)
+    ax = xp.abs(x - cx) if xp is not np else np.abs(x - cx)
+    ay = xp.abs(y - cy) if xp is not np else np.abs(y - cy)
+    dx_, dy_ = ax - hx, ay - hy
+    mx = (dx_ > 0.0) * dx_
+    my = (dy_ > 0.0) * dy_
+    outside = _sqrt(xp, mx * mx + my * my)
+    big = xp.maximum(dx_, dy_) if xp is not np else np.maximum(dx_, dy_)
+    inside = (big < 0.0) * big
+    return outside + inside
+
+
+# Triple-point material states (x < 1: driver; x > 1, y < 1.5: lower right; x > 1, y > 1.5: upper
+# right), phase order of exec/TriplePoint-5Eq-N/prob/ProblemICBC.H (phase 1 lower right, phase 2
+# driver, phase 3 upper right). TRIPLE_POINT_GAMMAS is the workload's gamma of each phase (driver and
+# lower right 1.5, upper right 1.4); the reference example's inputs use (1.4, 1.5, 1.5).
+TRIPLE_POINT_RHO = (1.0, 1.0, 0.125)
+TRIPLE_POINT_P = (0.1, 1.0, 0.1)
+TRIPLE_POINT_GAMMAS = (1.5, 1.5, 1.4)
+TRIPLE_POINT_REFERENCE_GAMMAS = (1.4, 1.5, 1.5)
+
+
+def triple_point(m=32, ng=3, quadrature=True, xp=None, device=None, gammas=TRIPLE_POINT_GAMMAS, eta=0.0,
+                 scheme="WENO5"):
+    """2D FIVEEQS_NPHASE (NPHASE = 3) triple point on [0,7] x [0,3] with 7m x 3m square cells, gases at
+    rest, reflecting walls (code 4) on every side, HLLC, source term 0, cfl 0.4, no change limiter
+    (the reference example's run keys). Volume fractions 0.5(1 + tanh(psi/(sqrt(2) eta))(1 - 1e-12))
+    of the two rectangle level sets, material 3 the remainder, normalised; eta = 0 gives the sharp
+    interfaces of the example (they lie on cell faces when m is a multiple of 2), pressure mixed by
+    volume fraction; the reference's initial_condition (ProblemICBC.H:36-105)."""
+    xp = _xp_of(xp)
+    dim, physics, nphase = 2, FIVEEQS_NPHASE, 3
+    nx, ny = 7 * m, 3 * m
+    dx = (7.0 / nx, 3.0 / ny, 1.0)
+    A = [1.0 / (g - 1.0) for g in gammas]
+    eps = 1.0e-12
+
+    def tanh_scaled(psi):
+        if eta == 0.0:
+            return (psi > 0.0) * 1.0 - (psi < 0.0) * 1.0
+        return _tanh(xp, psi / (math.sqrt(2.0) * eta))
+
+    def pw(x, y, z):
+        psi0 = -_box_level_set_2d(xp, x, y, 1.0, -1.0, 8.0, 1.5)
+        psi1 = -_box_level_set_2d(xp, x, y, -1.0, -1.0, 1.0, 4.0)
+        a0 = 0.5 * (1.0 + tanh_scaled(psi0) * (1.0 - eps))
+        a1 = 0.5 * (1.0 + tanh_scaled(psi1) * (1.0 - eps))
+        a2 = 1 - a0 - a1
+        ssum = (0.0 + a0) + a1
+        ssum = ssum + a2
+        al = [a0 / ssum, a1 / ssum, a2 / ssum]
+        P = 0.0
+        for k in range(nphase):
+            P = P + al[k] * TRIPLE_POINT_P[k]
+        ar = [al[k] * TRIPLE_POINT_RHO[k] for k in range(nphase)]
+        rho = 0.0
+        for k in range(nphase):
+            rho = rho + ar[k]
+        AP = 0.0
+        for k in range(nphase):
+            AP = AP + al[k] * A[k]
+        rho_e = (AP * P + 0.0) + 0.0  # ideal gases: B_k = D_k = 0
+        zero = x * 0.0 + y * 0.0
+        return ar + [rho * zero, rho * zero, rho_e + (0.5 * rho) * (zero * zero + zero * zero)] + al
+
+    inputs = {"FiniteVolume.Scheme": scheme, "Physics.RiemannSolver": "HLLC", "Physics.source_term": 0,
+              "prob.EOS.EOS": 1, "prob.EOS.gamma": list(gammas), "prob.EOS.pinf": [0.0] * nphase,
+              "run.cfl": 0.4, "run.timestep_change_limiter": 0}
+    geom = dict(n=(nx, ny, 1), dx=dx, ng=ng, lo_bc=(4, 4, 0), hi_bc=(4, 4, 0))
+    U = _average(physics, dim, (nx, ny, 1), dx, (0.0, 0.0, 0.0), pw, ng, quadrature, xp, device, nphase=nphase)
+    return physics, dim, inputs, geom, U
+
+
+def nphase_bubbles(n=32, nphase=3, dim=2, ng=3, quadrature=True, xp=None, device=None, source_term=0,
+                   eos=1, velocity=1.0):
+    """FIVEEQS_NPHASE advected interfaces on the periodic unit square / cube: phase k < nphase - 1
+    fills a disc (sphere) of radius 0.15 centred at (0.3 + 0.4 (k % 2), 0.3 + 0.4 (k // 2 % 2), 0.5)
+    with a tanh profile of width 2 dx, the last phase takes the remainder; volume fractions clipped
+    to [1e-6, 1] and normalised. Phases alternate between an ideal gas (gamma 1.4, rho 1) and a
+    stiffened liquid (gamma 4.4, pinf 6e8, rho 1000; with eos = 3 also NASG covolume 1e-4 and q 0);
+    uniform pressure 1e5 and velocity `velocity` along every axis. WENO5 + HLLC, cfl 0.5."""
+    xp = _xp_of(xp)
+    physics = FIVEEQS_NPHASE
+    dx = (1.0 / n, 1.0 / n, 1.0 / n if dim == 3 else 1.0)
+    gam = [1.4 if k % 2 == 0 else 4.4 for k in range(nphase)]
+    pinf = [0.0 if k % 2 == 0 else 6e8 for k in range(nphase)]
+    rho0 = [1.0 if k % 2 == 0 else 1000.0 for k in range(nphase)]
+    bcov = [0.0 if k % 2 == 0 else 1e-4 for k in range(nphase)] if eos == 3 else [0.0] * nphase
+    A = [1.0 / (g - 1.0) for g in gam]
+    B = [gam[k] * pinf[k] / (gam[k] - 1.0) for k in range(nphase)]
+    p0 = 1e5
+
+    def pw(x, y, z):
+        al = []
+        rest = 1.0
+        for k in range(nphase - 1):
+            cx, cy = 0.3 + 0.4 * (k % 2), 0.3 + 0.4 * ((k // 2) % 2)
+            r2 = (x - cx) ** 2 + (y - cy) ** 2 + ((z - 0.5) ** 2 if dim == 3 else 0.0)
+            a = _clip(xp, 0.5 * (1.0 + _tanh(xp, (0.15 - _sqrt(xp, r2)) / (2.0 * dx[0]))), 1e-6, 1.0)
+            al.append(a)
+            rest = rest - a
+        al.append(_clip(xp, rest, 1e-6, 1.0))
+        ssum = 0.0
+        for a in al:
+            ssum = ssum + a
+        al = [a / ssum for a in al]
+        ar = [al[k] * rho0[k] for k in range(nphase)]
+        rho = 0.0
+        for v in ar:
+            rho = rho + v
+        rho_e = 0.0
+        for k in range(nphase):
+            phi = al[k] - bcov[k] * ar[k]
+            rho_e = rho_e + phi * (A[k] * p0 + B[k])
+        vel = [x * 0 + velocity, y * 0 + velocity] + ([z * 0 + velocity] if dim == 3 else [])
+        ke = 0.0
+        for v in vel:
+            ke = ke + v * v
+        return ar + [rho * v for v in vel] + [rho_e + 0.5 * rho * ke] + al
+
+    inputs = {"FiniteVolume.Scheme": "WENO5", "Physics.RiemannSolver": "HLLC", "Physics.source_term": source_term,
+              "prob.EOS.EOS": eos, "prob.EOS.gamma": gam, "prob.EOS.pinf": pinf, "run.cfl": 0.5}
+    if eos == 3:
+        inputs["prob.EOS.b"] = bcov
+        inputs["prob.EOS.q"] = [0.0] * nphase
+    nz = n if dim == 3 else 1
+    geom = dict(n=(n, n, nz), dx=dx, ng=ng, lo_bc=(0, 0, 0), hi_bc=(0, 0, 0))
+    U = _average(physics, dim, (n, n, nz), dx, (0.0, 0.0, 0.0), pw, ng, quadrature, xp, device, nphase=nphase)
+    return physics, dim, inputs, geom, U
+
+
 def shock_droplet(n=256, ng=3, quadrature=True, xp=None, device=None, Ma=2.4, relaxation=1):
     """3D SIXEQS shock-droplet in the unit cube: water droplet (phase 2, stiffened gas gamma 6.12,
     pinf 3.43e8, rho 1000) of radius 0.1 at the centre, air (phase 1, gamma 1.4, rho 1.2, p 1e5), a
@@ -242,10 +377,10 @@ def shock_droplet(n=256, ng=3, quadrature=True, xp=None, device=None, Ma=2.4, re
     return physics, dim, inputs, geom, U
 
 
-def algorithmic_bytes_per_cell_stage(physics: int, dim: int) -> float:
+def algorithmic_bytes_per_cell_stage(physics: int, dim: int, nphase: int = 2) -> float:
     """(8/3) N 8 B: stage 1 reads U and writes U1 (2N doubles), stages 2 and 3 read U^(s), U^0 and
     write (3N doubles); relaxation is fused and adds nothing."""
-    return (8.0 / 3.0) * nstate(physics, dim) * 8.0
+    return (8.0 / 3.0) * nstate(physics, dim, nphase) * 8.0
 
 
 def batch_shock_bubbles(count=48, seed=0, xp=None, device=None, quadrature=True, scheme="WENO5B",

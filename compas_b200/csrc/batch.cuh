@@ -17,7 +17,7 @@ struct FillListArgs {
     const BoxDesc* boxes;
     const int* nbox;
     const long long* ghost_off;  // exclusive prefix sums of BoxDesc::ghosts, nbox + 1 entries
-    int N, D;
+    int N, D, m0;                // components, dimension, first momentum component
     int stage;                   // fills BoxDesc::U[stage]
 };
 
@@ -39,7 +39,7 @@ __global__ void fill_list_kernel(FillListArgs F) {
         const int b = find_box_ll(F.ghost_off, nb, q);
         const BoxDesc& B = F.boxes[b];
         if (*B.done) continue;
-        fill_ghost_cell(B.U[F.stage], B.g, F.N, F.D, B.lo_bc, B.hi_bc, q - F.ghost_off[b]);
+        fill_ghost_cell(B.U[F.stage], B.g, F.N, F.D, F.m0, B.lo_bc, B.hi_bc, q - F.ghost_off[b]);
     }
 }
 
@@ -112,7 +112,7 @@ struct BatchCase {
 }  // namespace compas
 
 struct compas_b200_batch {
-    int physics, dim, limiter, precision;
+    int physics, dim, nphase, limiter, precision;
     int capacity;
     std::vector<compas::BatchCase> cases;  // active cases, in box-list order
     std::vector<int> free_slots;

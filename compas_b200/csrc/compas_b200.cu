@@ -46,16 +46,18 @@ static int fail(int code, const std::string& msg) {
 // AMReX BCType of component n across a face normal to d for a COMPAS boundary code
 // (source/Class_Compressible6Eq_PhaseField.cpp:352-434, Class_Compressible5Eq_PhaseField.cpp:162-):
 // 0 int_dir (periodic), 2 foextrap, 3/4 reflect_even with the normal momentum reflect_odd,
-// 5 reflect_odd for every momentum component.
+// 5 reflect_odd for every momentum component. The momentum components are m0 .. m0 + D - 1 (m0 = 2
+// for the two-phase models, NPHASE for FIVEEQS_NPHASE,
+// source/Class_Compressible5Eq_NPhase_PhaseField.cpp:133-205).
 enum { kBcPeriodic = 0, kBcExtrap = 1, kBcEven = 2, kBcOdd = 3 };
 
-__device__ __forceinline__ int bc_kind(int code, int n, int d, int D) {
-    const bool mom = (n >= 2 && n < 2 + D);
+__device__ __forceinline__ int bc_kind(int code, int n, int d, int D, int m0) {
+    const bool mom = (n >= m0 && n < m0 + D);
     switch (code) {
         case 0: return kBcPeriodic;
         case 2: return kBcExtrap;
         case 3:
-        case 4: return (mom && n - 2 == d) ? kBcOdd : kBcEven;
+        case 4: return (mom && n - m0 == d) ? kBcOdd : kBcEven;
         default: return mom ? kBcOdd : kBcEven;  // 5: no-slip wall
     }
 }
@@ -63,21 +65,21 @@ __device__ __forceinline__ int bc_kind(int code, int n, int d, int D) {
 struct BcArgs {
     double* U;
     Grid g;
-    int N, D;
+    int N, D, m0;
     int lo[3], hi[3];
 };
 
 // Map one coordinate of a ghost cell to its source along d; returns the sign factor.
-__device__ __forceinline__ double bc_map(int& x, int len, int code_lo, int code_hi, int n, int d, int D) {
+__device__ __forceinline__ double bc_map(int& x, int len, int code_lo, int code_hi, int n, int d, int D, int m0) {
     if (x < 0) {
-        const int kind = bc_kind(code_lo, n, d, D);
+        const int kind = bc_kind(code_lo, n, d, D, m0);
         if (kind == kBcPeriodic) { x += len; return 1.0; }
         if (kind == kBcExtrap) { x = 0; return 1.0; }
         x = -1 - x;
         return kind == kBcOdd ? -1.0 : 1.0;
     }
     if (x >= len) {
-        const int kind = bc_kind(code_hi, n, d, D);
+        const int kind = bc_kind(code_hi, n, d, D, m0);
         if (kind == kBcPeriodic) { x -= len; return 1.0; }
         if (kind == kBcExtrap) { x = len - 1; return 1.0; }
         x = 2 * len - 1 - x;
@@ -96,8 +98,8 @@ __host__ __device__ __forceinline__ long long ghost_count(const Grid& g) {
 }
 
 // Fill ghost cell number q (enumeration above) of U, all components.
-__device__ __forceinline__ void fill_ghost_cell(double* U, const Grid& g, int N, int D, const int* lo, const int* hi,
-                                                long long q) {
+__device__ __forceinline__ void fill_ghost_cell(double* U, const Grid& g, int N, int D, int m0, const int* lo,
+                                                const int* hi, long long q) {
     const long long PX = g.px, PY = g.pxy / g.px;
     const long long nz_slab = 2LL * g.gz * PX * PY;
     const long long ny_slab = 2LL * g.ng * PX * g.n[2];
@@ -130,9 +132,9 @@ __device__ __forceinline__ void fill_ghost_cell(double* U, const Grid& g, int N,
         const long long dst = g.at(i, j, k);
         for (int n = 0; n < N; ++n) {
             int si = i, sj = j, sk = k;
-            double sgn = bc_map(si, g.n[0], lo[0], hi[0], n, 0, D);
-            sgn *= bc_map(sj, g.n[1], lo[1], hi[1], n, 1, D);
-            if (D == 3) sgn *= bc_map(sk, g.n[2], lo[2], hi[2], n, 2, D);
+            double sgn = bc_map(si, g.n[0], lo[0], hi[0], n, 0, D, m0);
+            sgn *= bc_map(sj, g.n[1], lo[1], hi[1], n, 1, D, m0);
+            if (D == 3) sgn *= bc_map(sk, g.n[2], lo[2], hi[2], n, 2, D, m0);
             U[n * g.S + dst] = sgn * U[n * g.S + g.at(si, sj, sk)];
         }
     }
@@ -142,7 +144,7 @@ __global__ void fill_boundary_kernel(BcArgs a) {
     const long long total = ghost_count(a.g);
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
          q += (long long)gridDim.x * blockDim.x)
-        fill_ghost_cell(a.U, a.g, a.N, a.D, a.lo, a.hi, q);
+        fill_ghost_cell(a.U, a.g, a.N, a.D, a.m0, a.lo, a.hi, q);
 }
 
 template <int D>
@@ -251,18 +253,49 @@ static Grid make_grid(const compas_b200_parm* p, const compas_b200_geom* g) {
 }
 
 static Eos make_eos(const compas_b200_parm* p) {
-    return Eos{p->A1, p->A2, p->B1, p->B2, p->C1, p->C2, p->D1, p->D2, 1.0 / p->A1, 1.0 / p->A2};
+    Eos e;
+    std::memset(&e, 0, sizeof(e));
+    e.A1 = p->A1; e.A2 = p->A2; e.B1 = p->B1; e.B2 = p->B2;
+    e.C1 = p->C1; e.C2 = p->C2; e.D1 = p->D1; e.D2 = p->D2;
+    e.iA1 = 1.0 / p->A1;
+    e.iA2 = 1.0 / p->A2;
+    for (int k = 0; k < kMaxPhases; ++k) {
+        e.Ak[k] = p->Ak[k];
+        e.Bk[k] = p->Bk[k];
+        e.Ck[k] = p->Ck[k];
+        e.Dk[k] = p->Dk[k];
+    }
+    return e;
 }
 
-static int nstate(const compas_b200_parm* p) {
-    return (p->physics == COMPAS_B200_FIVEEQS ? 4 : 5) + p->dim;
+// NSTATE (include/Macros.H:73, :89, :114).
+static int nstate_of(int physics, int dim, int nphase) {
+    if (physics == COMPAS_B200_FIVEEQS_NPHASE) return 2 * nphase + dim + 1;
+    return (physics == COMPAS_B200_FIVEEQS ? 4 : 5) + dim;
+}
+static int nstate(const compas_b200_parm* p) { return nstate_of(p->physics, p->dim, p->nphase); }
+
+// First momentum component (INDEX_MomentumX).
+static int mom0_of(int physics, int nphase) { return physics == COMPAS_B200_FIVEEQS_NPHASE ? nphase : 2; }
+
+// The N-phase kernels this build instantiates.
+static bool nphase_built(int dim, int nphase) {
+    return (dim == 2 && nphase >= 2 && nphase <= 4) || (dim == 3 && nphase == 3);
 }
 
 static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
     if (!p || !g) return fail(COMPAS_B200_EARG, "null parameter or geometry");
-    if (p->physics != COMPAS_B200_FIVEEQS && p->physics != COMPAS_B200_SIXEQS)
-        return fail(COMPAS_B200_EARG, "physics must be FIVEEQS (555) or SIXEQS (666)");
+    if (p->physics != COMPAS_B200_FIVEEQS && p->physics != COMPAS_B200_SIXEQS &&
+        p->physics != COMPAS_B200_FIVEEQS_NPHASE)
+        return fail(COMPAS_B200_EARG, "physics must be FIVEEQS (555), SIXEQS (666) or FIVEEQS_NPHASE (55501)");
     if (p->dim != 2 && p->dim != 3) return fail(COMPAS_B200_EARG, "dim must be 2 or 3");
+    if (p->physics == COMPAS_B200_FIVEEQS_NPHASE) {
+        if (!nphase_built(p->dim, p->nphase))
+            return fail(COMPAS_B200_EUNSUPPORTED, "FIVEEQS_NPHASE: this build runs NPHASE 2, 3, 4 in 2D and 3 in 3D");
+        if (p->id_limiter != 5)
+            return fail(COMPAS_B200_EUNSUPPORTED, "FIVEEQS_NPHASE: this engine runs FiniteVolume.Scheme = WENO5");
+        if (p->thinc) return fail(COMPAS_B200_EUNSUPPORTED, "FIVEEQS_NPHASE: FiniteVolume.THINC is not in this engine");
+    }
     if (p->id_limiter != 5 && p->id_limiter != 6)
         return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.Scheme: this build runs WENO5 and WENO5B");
     if (p->id_riemann != 2) return fail(COMPAS_B200_EUNSUPPORTED, "Physics.RiemannSolver: this build runs HLLC");
@@ -316,12 +349,16 @@ static int launch_stage(const compas_b200_parm* p, const StageArgs& a, cudaStrea
     }
     cudaError_t e;
     if (p->physics == COMPAS_B200_FIVEEQS) e = (p->dim == 2) ? launch_stage_fiveeq2(k, a, st) : launch_stage_fiveeq3(k, a, st);
-    else e = (p->dim == 2) ? launch_stage_sixeq2(k, a, st) : launch_stage_sixeq3(k, a, st);
+    else if (p->physics == COMPAS_B200_SIXEQS) e = (p->dim == 2) ? launch_stage_sixeq2(k, a, st) : launch_stage_sixeq3(k, a, st);
+    else if (p->dim == 3) e = launch_stage_fiveeqn3_3(k, a, st);
+    else e = (p->nphase == 2) ? launch_stage_fiveeqn2_2(k, a, st)
+           : (p->nphase == 3) ? launch_stage_fiveeqn2_3(k, a, st) : launch_stage_fiveeqn2_4(k, a, st);
     if (e != cudaSuccess) return fail(COMPAS_B200_ECUDA, std::string("stage kernel launch: ") + cudaGetErrorString(e));
     return COMPAS_B200_OK;
 }
 
-static int launch_list(int physics, int dim, int limiter, int precision, const ListArgs& L, cudaStream_t st) {
+static int launch_list(int physics, int dim, int nphase, int limiter, int precision, const ListArgs& L,
+                       cudaStream_t st) {
     KernelChoice k;
     k.limiter = limiter;
     k.precision = precision;
@@ -329,7 +366,10 @@ static int launch_list(int physics, int dim, int limiter, int precision, const L
     k.phase_field = 0;
     cudaError_t e;
     if (physics == COMPAS_B200_FIVEEQS) e = (dim == 2) ? launch_list_fiveeq2(k, L, st) : launch_list_fiveeq3(k, L, st);
-    else e = (dim == 2) ? launch_list_sixeq2(k, L, st) : launch_list_sixeq3(k, L, st);
+    else if (physics == COMPAS_B200_SIXEQS) e = (dim == 2) ? launch_list_sixeq2(k, L, st) : launch_list_sixeq3(k, L, st);
+    else if (dim == 3) e = launch_list_fiveeqn3_3(k, L, st);
+    else e = (nphase == 2) ? launch_list_fiveeqn2_2(k, L, st)
+           : (nphase == 3) ? launch_list_fiveeqn2_3(k, L, st) : launch_list_fiveeqn2_4(k, L, st);
     if (e != cudaSuccess) return fail(COMPAS_B200_ECUDA, std::string("box-list kernel launch: ") + cudaGetErrorString(e));
     return COMPAS_B200_OK;
 }
@@ -340,6 +380,7 @@ static int launch_fill(const compas_b200_parm* p, const compas_b200_geom* geo, d
     b.g = make_grid(p, geo);
     b.N = nstate(p);
     b.D = p->dim;
+    b.m0 = mom0_of(p->physics, p->nphase);
     for (int d = 0; d < 3; ++d) {
         b.lo[d] = geo->lo_bc[d];
         b.hi[d] = geo->hi_bc[d];
@@ -490,13 +531,19 @@ extern "C" {
 const char* compas_b200_last_error(void) { return g_last_error.c_str(); }
 
 int compas_b200_parm_init(compas_b200_parm* p, int physics, int dim) {
+    return compas_b200_parm_init_nphase(p, physics, dim, 2);
+}
+
+int compas_b200_parm_init_nphase(compas_b200_parm* p, int physics, int dim, int nphase) {
     if (!p) return fail(COMPAS_B200_EARG, "null parm");
     std::memset(p, 0, sizeof(*p));
     p->physics = physics;
     p->dim = dim;
+    p->nphase = nphase;
     p->eos = 1;
     p->gamma_1 = 1.4;
     p->gamma_2 = 1.4;
+    for (int k = 0; k < kMaxPhases; ++k) p->gamma_k[k] = 1.4;
     p->id_limiter = 5;
     p->num_grow = 3;
     p->thinc = 0;
@@ -515,9 +562,13 @@ int compas_b200_parm_init(compas_b200_parm* p, int physics, int dim) {
     p->pf_cfl = 0.4;
     p->pf_max_step = 1000000;
     p->pf_tol_rel = 1.0e-10;
-    if (physics != COMPAS_B200_FIVEEQS && physics != COMPAS_B200_SIXEQS)
-        return fail(COMPAS_B200_EARG, "physics must be FIVEEQS (555) or SIXEQS (666)");
+    if (physics != COMPAS_B200_FIVEEQS && physics != COMPAS_B200_SIXEQS && physics != COMPAS_B200_FIVEEQS_NPHASE)
+        return fail(COMPAS_B200_EARG, "physics must be FIVEEQS (555), SIXEQS (666) or FIVEEQS_NPHASE (55501)");
     if (dim != 2 && dim != 3) return fail(COMPAS_B200_EARG, "dim must be 2 or 3");
+    if (physics == COMPAS_B200_FIVEEQS_NPHASE && (nphase < 2 || nphase > kMaxPhases))
+        return fail(COMPAS_B200_EARG, "FIVEEQS_NPHASE: nphase must be in [2, " + std::to_string(kMaxPhases) + "]");
+    if (physics != COMPAS_B200_FIVEEQS_NPHASE && nphase != 2)
+        return fail(COMPAS_B200_EARG, "the two-phase models have nphase = 2");
     return compas_b200_parm_finalize(p);
 }
 
@@ -595,6 +646,33 @@ int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value
         p->eos = ix;
         return 0;
     }
+    if (p->physics == COMPAS_B200_FIVEEQS_NPHASE) {
+        // per-phase lists (source/Parm.cpp:66-92): exactly NPHASE values
+        struct LKey { const char* name; double* dst; };
+        const LKey lkeys[] = {{"prob.EOS.gamma", p->gamma_k}, {"prob.EOS.pinf", p->pinf_k},
+                              {"prob.EOS.b", p->b_k}, {"prob.EOS.q", p->q_k}};
+        for (const auto& lk : lkeys)
+            if (k == lk.name) {
+                double vals[kMaxPhases];
+                int cnt = 0;
+                const char* c = value;
+                while (true) {
+                    while (*c == ' ' || *c == '\t' || *c == ',') ++c;
+                    if (!*c) break;
+                    char* end = nullptr;
+                    const double x1 = std::strtod(c, &end);
+                    if (end == c) return bad("a list of numbers");
+                    if (cnt < kMaxPhases) vals[cnt] = x1;
+                    ++cnt;
+                    c = end;
+                }
+                if (cnt != p->nphase)
+                    return fail(COMPAS_B200_EARG, k + " has " + std::to_string(cnt) + " values, but NPHASE = " +
+                                                      std::to_string(p->nphase) + " needs one value per phase.");
+                for (int i = 0; i < cnt; ++i) lk.dst[i] = vals[i];
+                return 0;
+            }
+    }
     struct DKey { const char* name; double* dst; };
     const DKey dkeys[] = {{"prob.EOS.gamma_1", &p->gamma_1}, {"prob.EOS.gamma_2", &p->gamma_2},
                           {"prob.EOS.pinf_1", &p->pinf_1},   {"prob.EOS.pinf_2", &p->pinf_2},
@@ -663,6 +741,37 @@ int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value
 
 int compas_b200_parm_finalize(compas_b200_parm* p) {
     if (!p) return fail(COMPAS_B200_EARG, "null parm");
+    if (p->physics == COMPAS_B200_FIVEEQS_NPHASE) {
+        // source/Parm.cpp:185-253
+        const int np = p->nphase;
+        if (np < 2 || np > kMaxPhases) return fail(COMPAS_B200_EARG, "FIVEEQS_NPHASE: nphase out of range");
+        for (int k = 0; k < np; ++k) {
+            if (!(p->gamma_k[k] > 1.0))
+                return fail(COMPAS_B200_EARG, "prob.EOS.EOS requires gamma > 1, but prob.EOS.gamma[" +
+                                                  std::to_string(k) + "] is " + std::to_string(p->gamma_k[k]));
+            const double g = p->gamma_k[k];
+            p->Ak[k] = 1. / (g - 1.);
+            if (p->eos == 0) {
+                p->Bk[k] = 0.0; p->Ck[k] = 0.0; p->Dk[k] = 0.0;
+            } else if (p->eos == 1) {
+                p->Bk[k] = g * p->pinf_k[k] / (g - 1.);
+                p->Ck[k] = 0.0; p->Dk[k] = 0.0;
+            } else if (p->eos == 3) {
+                if (p->b_k[k] < 0.0) return fail(COMPAS_B200_EARG, "prob.EOS.b must be >= 0");
+                p->Bk[k] = g * p->pinf_k[k] / (g - 1.);
+                p->Ck[k] = p->b_k[k];
+                p->Dk[k] = p->q_k[k];
+            } else {
+                return fail(COMPAS_B200_EARG, "prob.EOS.EOS must be 0, 1 or 3");
+            }
+        }
+        for (int k = np; k < kMaxPhases; ++k) {
+            p->Ak[k] = 1.0; p->Bk[k] = 0.0; p->Ck[k] = 0.0; p->Dk[k] = 0.0;
+        }
+        // the two-phase fields stay valid (A = 1/(1.4 - 1)) so that shared code never divides by 0
+        p->A1 = p->Ak[0]; p->A2 = p->Ak[1];
+        return COMPAS_B200_OK;
+    }
     // source/Parm.cpp:101-188
     if (!(p->gamma_1 > 1.0) || !(p->gamma_2 > 1.0))
         return fail(COMPAS_B200_EARG, "prob.EOS.EOS requires gamma > 1 for both phases");
@@ -1156,17 +1265,25 @@ static int batch_sync_list(compas_b200_batch* b, cudaStream_t st) {
 
 int compas_b200_batch_create(int physics, int dim, int id_limiter, int precision, int capacity,
                              compas_b200_batch** out) {
+    return compas_b200_batch_create_nphase(physics, dim, 2, id_limiter, precision, capacity, out);
+}
+
+int compas_b200_batch_create_nphase(int physics, int dim, int nphase, int id_limiter, int precision, int capacity,
+                                    compas_b200_batch** out) {
     if (!out) return fail(COMPAS_B200_EARG, "null output");
     *out = nullptr;
     compas_b200_parm probe;
-    int rc = compas_b200_parm_init(&probe, physics, dim);
+    int rc = compas_b200_parm_init_nphase(&probe, physics, dim, nphase);
     if (rc) return rc;
+    if (physics == COMPAS_B200_FIVEEQS_NPHASE && (!nphase_built(dim, nphase) || id_limiter != 5))
+        return fail(COMPAS_B200_EUNSUPPORTED, "FIVEEQS_NPHASE batches: WENO5, NPHASE 2, 3, 4 in 2D and 3 in 3D");
     if (id_limiter != 5 && id_limiter != 6) return fail(COMPAS_B200_EUNSUPPORTED, "WENO5 (5) or WENO5B (6)");
     if (precision != 0 && precision != 1) return fail(COMPAS_B200_EARG, "precision 0 or 1");
     if (capacity < 1 || capacity > (1 << 20)) return fail(COMPAS_B200_EARG, "capacity out of range");
     auto* b = new compas_b200_batch();
     b->physics = physics;
     b->dim = dim;
+    b->nphase = nphase;
     b->limiter = id_limiter;
     b->precision = precision;
     b->capacity = capacity;
@@ -1214,8 +1331,9 @@ int compas_b200_batch_add(compas_b200_batch* b, const compas_b200_parm* p, const
     if (!b || !U) return fail(COMPAS_B200_EARG, "null argument");
     int rc = check_args(p, g);
     if (rc) return rc;
-    if (p->physics != b->physics || p->dim != b->dim || p->id_limiter != b->limiter || p->precision != b->precision)
-        return fail(COMPAS_B200_EARG, "a batch holds cases of one model, dimension, scheme and precision");
+    if (p->physics != b->physics || p->dim != b->dim || p->id_limiter != b->limiter || p->precision != b->precision ||
+        (p->physics == COMPAS_B200_FIVEEQS_NPHASE && p->nphase != b->nphase))
+        return fail(COMPAS_B200_EARG, "a batch holds cases of one model, dimension, number of phases, scheme and precision");
     if (p->thinc) return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.THINC = 1 runs on the level API, not in a batch");
     if (b->free_slots.empty()) return fail(COMPAS_B200_ENOMEM, "batch capacity reached");
     if (max_steps < 0) return fail(COMPAS_B200_EARG, "max_steps must be >= 0");
@@ -1287,14 +1405,14 @@ int compas_b200_batch_remove(compas_b200_batch* b, int case_id, void* stream) {
 static int batch_enqueue_step(compas_b200_batch* b, cudaStream_t st) {
     step_begin_list_kernel<<<4, 256, 0, st>>>(b->d_ctl, b->d_cs, b->d_slots, b->d_nbox);
     CUDA_TRY(cudaGetLastError());
-    const int N = (b->physics == COMPAS_B200_FIVEEQS ? 4 : 5) + b->dim;
+    const int N = nstate_of(b->physics, b->dim, b->nphase);
     int rc;
     for (int s = 0; s < 3; ++s) {
-        FillListArgs F{b->d_boxes, b->d_nbox, b->d_ghost_off, N, b->dim, s};
+        FillListArgs F{b->d_boxes, b->d_nbox, b->d_ghost_off, N, b->dim, mom0_of(b->physics, b->nphase), s};
         fill_list_kernel<<<148 * 8, 256, 0, st>>>(F);
         CUDA_TRY(cudaGetLastError());
         ListArgs L{b->d_boxes, b->d_nbox, b->d_tile_off, kModeStage, s};
-        if ((rc = launch_list(b->physics, b->dim, b->limiter, b->precision, L, st))) return rc;
+        if ((rc = launch_list(b->physics, b->dim, b->nphase, b->limiter, b->precision, L, st))) return rc;
     }
     step_end_list_kernel<<<4, 256, 0, st>>>(b->d_ctl, b->d_slots, b->d_nbox);
     CUDA_TRY(cudaGetLastError());

@@ -54,19 +54,30 @@ static cudaError_t launch_stage_v(const StageArgs& a, cudaStream_t st) {
 
 template <class M, int SCHEME, bool MIX>
 static cudaError_t launch_stage_var(const KernelChoice& k, const StageArgs& a, cudaStream_t st) {
-    if (k.phase_field) {
-        if constexpr (M::NC == 1) return launch_stage_v<M, SCHEME, MIX, kVarPhaseField>(a, st);
-        else return cudaErrorNotSupported;
+    if constexpr (M::KIND == kModelFiveN) {
+        // FIVEEQS_NPHASE: the plain hyperbolic right-hand side only
+        if (k.phase_field || k.thinc) return cudaErrorNotSupported;
+        return launch_stage_v<M, SCHEME, MIX, kVarPlain>(a, st);
+    } else {
+        if (k.phase_field) {
+            if constexpr (M::KIND == kModelFive) return launch_stage_v<M, SCHEME, MIX, kVarPhaseField>(a, st);
+            else return cudaErrorNotSupported;
+        }
+        if (k.thinc) return launch_stage_v<M, SCHEME, MIX, kVarThinc>(a, st);
+        return launch_stage_v<M, SCHEME, MIX, kVarPlain>(a, st);
     }
-    if (k.thinc) return launch_stage_v<M, SCHEME, MIX, kVarThinc>(a, st);
-    return launch_stage_v<M, SCHEME, MIX, kVarPlain>(a, st);
 }
 
 template <class M>
 static cudaError_t launch_stage_m(const KernelChoice& k, const StageArgs& a, cudaStream_t st) {
     const bool mix = (k.precision == 1), bounded = (k.limiter == 6);
-    if (mix) return bounded ? launch_stage_var<M, 6, true>(k, a, st) : launch_stage_var<M, 5, true>(k, a, st);
-    return bounded ? launch_stage_var<M, 6, false>(k, a, st) : launch_stage_var<M, 5, false>(k, a, st);
+    if constexpr (M::KIND == kModelFiveN) {
+        if (bounded) return cudaErrorNotSupported;
+        return mix ? launch_stage_var<M, 5, true>(k, a, st) : launch_stage_var<M, 5, false>(k, a, st);
+    } else {
+        if (mix) return bounded ? launch_stage_var<M, 6, true>(k, a, st) : launch_stage_var<M, 5, true>(k, a, st);
+        return bounded ? launch_stage_var<M, 6, false>(k, a, st) : launch_stage_var<M, 5, false>(k, a, st);
+    }
 }
 
 // Persistent box-list launch: one resident wave of CTAs walks the tiles of every box.
@@ -91,8 +102,13 @@ static cudaError_t launch_list_v(const ListArgs& L, cudaStream_t st) {
 
 template <class M>
 static cudaError_t launch_list_m(const KernelChoice& k, const ListArgs& L, cudaStream_t st) {
-    if (k.precision == 1) return (k.limiter == 6) ? launch_list_v<M, 6, true>(L, st) : launch_list_v<M, 5, true>(L, st);
-    return (k.limiter == 6) ? launch_list_v<M, 6, false>(L, st) : launch_list_v<M, 5, false>(L, st);
+    if constexpr (M::KIND == kModelFiveN) {
+        if (k.limiter == 6) return cudaErrorNotSupported;
+        return (k.precision == 1) ? launch_list_v<M, 5, true>(L, st) : launch_list_v<M, 5, false>(L, st);
+    } else {
+        if (k.precision == 1) return (k.limiter == 6) ? launch_list_v<M, 6, true>(L, st) : launch_list_v<M, 5, true>(L, st);
+        return (k.limiter == 6) ? launch_list_v<M, 6, false>(L, st) : launch_list_v<M, 5, false>(L, st);
+    }
 }
 
 }  // namespace compas

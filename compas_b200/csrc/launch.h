@@ -12,7 +12,8 @@ struct ListArgs;
 
 // Variant of the stage kernel: FiniteVolume.Scheme (5 WENO5, 6 WENO5B), precision (0 FP64, 1 mixed),
 // FiniteVolume.THINC (single-box kernel only), and the Phase-Field regularisation right-hand side
-// instead of the hyperbolic one (FIVEEQS, single-box kernel only).
+// instead of the hyperbolic one (FIVEEQS, single-box kernel only). The N-phase model
+// (fiveeqn<dim>_<nphase>) runs WENO5 only.
 struct KernelChoice {
     int limiter;
     int precision;
@@ -31,6 +32,10 @@ COMPAS_DECLARE_LAUNCHERS(fiveeq2)
 COMPAS_DECLARE_LAUNCHERS(fiveeq3)
 COMPAS_DECLARE_LAUNCHERS(sixeq2)
 COMPAS_DECLARE_LAUNCHERS(sixeq3)
+COMPAS_DECLARE_LAUNCHERS(fiveeqn2_2)
+COMPAS_DECLARE_LAUNCHERS(fiveeqn2_3)
+COMPAS_DECLARE_LAUNCHERS(fiveeqn2_4)
+COMPAS_DECLARE_LAUNCHERS(fiveeqn3_3)
 #undef COMPAS_DECLARE_LAUNCHERS
 
 }  // namespace compas

@@ -42,12 +42,18 @@ __device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b 
 __device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }
 __device__ __forceinline__ double sgn0(double x) { return x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : 0.0); }
 
-// EOS coefficients of the two phases, partial form alpha rho e = A Pi + B phi + alpha rho D, with
-// C the NASG covolume b (source/Parm.cpp:101-188).
+// EOS coefficients, partial form alpha rho e = A Pi + B phi + alpha rho D, with C the NASG covolume b
+// (source/Parm.cpp:101-188): the two phases of FIVEEQS / SIXEQS, and the per-phase lists of
+// FIVEEQS_NPHASE (source/Parm.cpp:185-262).
+constexpr int kMaxPhases = COMPAS_B200_MAX_PHASES;
 struct Eos {
     double A1, A2, B1, B2, C1, C2, D1, D2;
     double iA1, iA2;  // 1/A1, 1/A2 (mixed-precision pressure recovery)
+    double Ak[kMaxPhases], Bk[kMaxPhases], Ck[kMaxPhases], Dk[kMaxPhases];
 };
+
+// Model families of the stage kernel (the M::KIND of each model struct).
+enum { kModelFive = 0, kModelSix = 1, kModelFiveN = 2 };
 
 // NASG: phi = alpha - b alpha rho (alpha when b = 0); covolume violation 1 - b rho <= 0 is reported
 // through the status word where the reference aborts.
@@ -107,6 +113,7 @@ __device__ __forceinline__ double ksum(const double* u) {
 // ------------------------------------------------------------------------------------------------
 template <int DIM>
 struct FiveEq {
+    static constexpr int KIND = kModelFive;
     static constexpr int D = DIM;
     static constexpr int N = 4 + DIM;
     static constexpr int NC = 1;       // face quantities of the non-conservative terms
@@ -389,6 +396,7 @@ __device__ __forceinline__ void fiveeq_hllc_mixed(double* Fout, double* fnc, flo
 // ------------------------------------------------------------------------------------------------
 template <int DIM>
 struct SixEq {
+    static constexpr int KIND = kModelSix;
     static constexpr int D = DIM;
     static constexpr int N = 5 + DIM;
     static constexpr int NC = 3;        // u_n, (u a1p1)_n, (u a2p2)_n

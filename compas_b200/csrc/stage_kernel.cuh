@@ -22,6 +22,7 @@
 #pragma once
 
 #include "physics.cuh"
+#include "physics_nphase.cuh"
 #include "relax.cuh"
 
 #include <type_traits>
@@ -111,7 +112,9 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
     static_assert(TX == TY && (M::D == 2 ? TZ == 1 : TZ == TX), "tiles are cubes (squares in 2D)");
     constexpr bool TH = (VAR == kVarThinc);
     constexpr bool PFX = (VAR == kVarPhaseField);
-    static_assert(!PFX || M::NC == 1, "the Phase-Field kernel is the five-equation model's");
+    static_assert(!PFX || M::KIND == kModelFive, "the Phase-Field kernel is the five-equation model's");
+    static_assert(M::KIND != kModelFiveN || (SCHEME == 5 && !TH), "FIVEEQS_NPHASE runs WENO5 without THINC");
+    constexpr bool NPH = (M::KIND == kModelFiveN);
     using PT = typename std::conditional<MIX, float, double>::type;
     using T = TileShape<M, TX, TY, TZ, PT>;
     constexpr int N = M::N, NC = M::NC, D = M::D, NB = T::NB;
@@ -193,6 +196,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
         constexpr int TS = TX;
         constexpr int EF = TS + 1;
         const int NF = EF * T::A0;
+        const double dxd = (d == 0) ? g.dx[0] : (d == 1 ? g.dx[1] : g.dx[2]);
         for (int f = tid; f < NF; f += NT) {
             int fd, ta, tb;
             if (d == 0) {
@@ -262,6 +266,11 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                     }
                     M::prim2cons(UL, WfL, a.e, err);
                     M::prim2cons(UR, WfR, a.e, err);
+                    if constexpr (NPH) {
+                        // N-phase WENO5: the consistent limiter about the stencil centres f-1 and f
+                        M::consistent_limit(UL, smem + off[2], str[2], dxd, 1, a.e, err);
+                        M::consistent_limit(UR, smem + off[3], str[3], dxd, -1, a.e, err);
+                    }
                 }
                 if constexpr (PFX) {
                     pf_face_flux<D>(F, UL, UR, pf_face_gq(a, d, gi, gj, gk), a.e, err);
@@ -302,18 +311,27 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                     }
                     M::prim2cons(UL, WfL, a.e, err);
                     M::prim2cons(UR, WfR, a.e, err);
+                    if constexpr (NPH) {
+                        M::consistent_limit(UL, smem + off[2], str[2], dxd, 1, a.e, err);
+                        M::consistent_limit(UR, smem + off[3], str[3], dxd, -1, a.e, err);
+                    }
                 }
-                float cmf;
-                if constexpr (PFX) {
-                    pf_face_flux<D>(F, UL, UR, pf_face_gq(a, d, gi, gj, gk), a.e, err);
-                    fnc[0] = 0.0;
-                    cmf = 0.0f;
-                } else if constexpr (M::NC == 1) {
-                    fiveeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, a.e, d, a.id_k);
+                if constexpr (NPH) {
+                    // N-phase: FP32 reconstruction, FP64 limiter and Riemann solver
+                    M::hllc(F, fnc, cm, UL, UR, a.e, d, a.id_k, err);
                 } else {
-                    sixeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, a.e, d);
+                    float cmf;
+                    if constexpr (PFX) {
+                        pf_face_flux<D>(F, UL, UR, pf_face_gq(a, d, gi, gj, gk), a.e, err);
+                        fnc[0] = 0.0;
+                        cmf = 0.0f;
+                    } else if constexpr (M::KIND == kModelFive) {
+                        fiveeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, a.e, d, a.id_k);
+                    } else {
+                        sixeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, a.e, d);
+                    }
+                    cm = cmf;
                 }
-                cm = cmf;
             }
 #pragma unroll
             for (int n = 0; n < N; ++n) Fb[n * FMAX + f] = F[n];
@@ -326,7 +344,6 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
         __syncthreads();
 
         // 2c. divergence contribution of direction d
-        const double dxd = (d == 0) ? g.dx[0] : (d == 1 ? g.dx[1] : g.dx[2]);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int l = tid + r * NT;
@@ -372,9 +389,17 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                 // of the non-conservative terms from the FP32 tile
 #pragma unroll
                 for (int n = 0; n < N; ++n) W[n] = Pint[n * CELLS + l];
-                W[0] = Us[0];
-                W[1] = Us[1];
-                W[M::IA] = Us[M::IA];
+                if constexpr (NPH) {
+#pragma unroll
+                    for (int k = 0; k < M::NP; ++k) {
+                        W[k] = Us[k];
+                        W[M::IA + k] = Us[M::IA + k];
+                    }
+                } else {
+                    W[0] = Us[0];
+                    W[1] = Us[1];
+                    W[M::IA] = Us[M::IA];
+                }
             } else {
 #pragma unroll
                 for (int n = 0; n < N; ++n) W[n] = Pint[n * CELLS + l];
@@ -384,10 +409,16 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
             if constexpr (PFX) {
                 // the Phase-Field step has no non-conservative terms in the five-equation model
                 // (include/Operators_Compressible5Eq_PhaseField/FVM_PhaseField_SurfaceIntegralNC_Compressible5Eq_PhaseField.H)
-            } else if constexpr (M::NC == 1) {
+            } else if constexpr (M::KIND == kModelFive) {
                 // five-equation: alpha1 += phi1 (1 + K1) div u*
                 const double fac = M::kapila_factor(W, W, a.e, a.id_k, err);
                 L[M::IA] = L[M::IA] + fac * acc[r][N];
+            } else if constexpr (NPH) {
+                // N-phase five-equation: alpha_k += phi_k (1 + K_k) div u*
+                double fac[M::NP];
+                M::kapila_factors(fac, W, a.e, a.id_k, err);
+#pragma unroll
+                for (int k = 0; k < M::NP; ++k) L[M::IA + k] = L[M::IA + k] + fac[k] * acc[r][N];
             } else {
                 // six-equation: phase energy exchange and alpha1 div u (FVM_SurfaceIntegralNC_Compressible6Eq.H)
                 const double divv = acc[r][N], dva1 = acc[r][N + 1], dva2 = acc[r][N + 2];
@@ -417,7 +448,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                         out[n] = v + sdt * L[n];
                     }
                 }
-                if constexpr (M::NC == 3) {
+                if constexpr (M::KIND == kModelSix) {
                     if (a.relax) relax_pressure<D>(out, a.e, a.trace, err);
                 }
                 bool bad = false;

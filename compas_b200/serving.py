@@ -7,10 +7,10 @@ the budget - while others are running - and retires cases when their step count 
 reports time-to-solution (arrival to completion) percentiles and the aggregate cell-update rate, and
 can replay the same requests one at a time on a single-case level for comparison.
 
-Request types (configuration 5 of the north star):
+Request types:
   bubble2d   2D FIVEEQS shock-bubble (WENO5B), side^2 cells
   droplet3d  3D SIXEQS shock-droplet (WENO5, relaxation), side^3 cells
-The FIVEEQS_NPHASE triple point is not a model of this engine.
+  triple2d   2D FIVEEQS_NPHASE (NPHASE = 3) triple point on [0,7] x [0,3] (WENO5), 7 side x 3 side cells
 """
 from __future__ import annotations
 
@@ -19,10 +19,11 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import FIVEEQS, SIXEQS, Batch, Level, make_geom, make_parm, padded_shape, valid_view
+from . import FIVEEQS, FIVEEQS_NPHASE, SIXEQS, Batch, Level, make_geom, make_parm, padded_shape, valid_view
 from . import cases as _cases
 
-KINDS = {"bubble2d": (FIVEEQS, 2, 6), "droplet3d": (SIXEQS, 3, 5)}
+# kind: (physics, dim, FiniteVolume.Scheme id, NPHASE)
+KINDS = {"bubble2d": (FIVEEQS, 2, 6, 2), "droplet3d": (SIXEQS, 3, 5, 2), "triple2d": (FIVEEQS_NPHASE, 2, 5, 3)}
 
 
 @dataclass
@@ -52,22 +53,25 @@ def make_case(req: Request, precision: str, device="cuda", xp=None):
                                                          Ma=req.params.get("Ma", 1.5),
                                                          rho_b=req.params.get("ratio", 0.138),
                                                          xp=xp, device=device)
+    elif req.kind == "triple2d":
+        phys, dim, inputs, geom, U = _cases.triple_point(m=req.side, xp=xp, device=device)
     else:
         phys, dim, inputs, geom, U = _cases.shock_droplet(n=req.side, xp=xp, device=device)
     inputs = dict(inputs, **{"compas_b200.precision": precision})
     return make_parm(phys, dim, inputs), make_geom(**geom), U
 
 
-def poisson_requests(n, rate, seed=0, kinds=("bubble2d", "droplet3d"), sides2d=(128, 1024), sides3d=(64, 192),
-                     steps=(100, 2000)):
-    """n requests with exponential inter-arrival times of mean 1/rate (seeded)."""
+def poisson_requests(n, rate, seed=0, kinds=("bubble2d", "droplet3d", "triple2d"), sides2d=(128, 1024),
+                     sides3d=(64, 192), sides_triple=(32, 128), steps=(100, 2000)):
+    """n requests with exponential inter-arrival times of mean 1/rate (seeded). The side of a request
+    is a multiple of 16 in the kind's range (the triple point's side m gives 7m x 3m cells)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     t = 0.0
     out = []
     for i in range(n):
         t += float(rng.exponential(1.0 / rate))
         kind = kinds[int(rng.integers(len(kinds)))]
-        lo, hi = sides2d if kind == "bubble2d" else sides3d
+        lo, hi = {"bubble2d": sides2d, "droplet3d": sides3d, "triple2d": sides_triple}[kind]
         side = int(rng.integers(lo // 16, hi // 16 + 1)) * 16
         st = int(rng.integers(steps[0], steps[1] + 1))
         params = {"Ma": float(rng.uniform(1.1, 3.0)), "ratio": float(np.exp(rng.uniform(np.log(0.01), np.log(1000))))}
@@ -76,6 +80,8 @@ def poisson_requests(n, rate, seed=0, kinds=("bubble2d", "droplet3d"), sides2d=(
 
 
 def _cells(req):
+    if req.kind == "triple2d":
+        return 21 * req.side * req.side
     return req.side ** (2 if req.kind == "bubble2d" else 3)
 
 
@@ -87,8 +93,8 @@ class Server:
         self.budget = float(budget_bytes)
         self.precision = precision
         prec = 1 if precision == "mixed" else 0
-        self.batches = {k: Batch(ph, d, id_limiter=lim, precision=prec, capacity=capacity)
-                        for k, (ph, d, lim) in KINDS.items()}
+        self.batches = {k: Batch(ph, d, id_limiter=lim, precision=prec, capacity=capacity, nphase=nph)
+                        for k, (ph, d, lim, nph) in KINDS.items()}
         self.steps_per_iter = steps_per_iter
         self.keep_results = keep_results
         self.in_use = 0

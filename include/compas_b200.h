@@ -41,12 +41,14 @@ extern "C" {
 /* ---- models and schemes (the reference's compile-time PHYSICS and run-time keys) ------------ */
 #define COMPAS_B200_FIVEEQS 555 /* include/Macros.H:56 */
 #define COMPAS_B200_SIXEQS 666  /* include/Macros.H:57 */
+#define COMPAS_B200_FIVEEQS_NPHASE 55501 /* include/Macros.H:58: N-phase five-equation model */
+#define COMPAS_B200_MAX_PHASES 4         /* largest NPHASE this build instantiates */
 
 /* Parameters of the hot path: the fields of the reference's `struct Parm`
  * (exec/_Tests/Advection/prob/Parm.H:33-117) that the right-hand side reads, plus the run keys of
  * the level advance. Fill with compas_b200_parm_init, then compas_b200_parm_set per inputs key. */
 typedef struct compas_b200_parm {
-    int physics;          /* COMPAS_B200_FIVEEQS or COMPAS_B200_SIXEQS */
+    int physics;          /* COMPAS_B200_FIVEEQS, COMPAS_B200_SIXEQS or COMPAS_B200_FIVEEQS_NPHASE */
     int dim;              /* 2 or 3 (AMREX_SPACEDIM) */
     /* prob.EOS.* (source/Parm.cpp:101-188): raw inputs and the derived partial-form coefficients */
     int eos;              /* 0 ideal gas, 1 stiffened gas, 3 NASG */
@@ -83,6 +85,14 @@ typedef struct compas_b200_parm {
     double pf_cfl;            /* PhaseField.cfl */
     int pf_max_step;          /* PhaseField.max_step */
     double pf_tol_rel;        /* LinearSystem.tol_rel */
+    /* FIVEEQS_NPHASE: the number of phases (the reference's compile-time NPHASE; 2 for the two-phase
+     * models) and the per-phase lists prob.EOS.gamma/pinf/b/q with their partial-form coefficients
+     * (source/Parm.cpp:185-262); the A1..D2 fields above are not used by this model */
+    int nphase;
+    double gamma_k[COMPAS_B200_MAX_PHASES], pinf_k[COMPAS_B200_MAX_PHASES];
+    double b_k[COMPAS_B200_MAX_PHASES], q_k[COMPAS_B200_MAX_PHASES];
+    double Ak[COMPAS_B200_MAX_PHASES], Bk[COMPAS_B200_MAX_PHASES];
+    double Ck[COMPAS_B200_MAX_PHASES], Dk[COMPAS_B200_MAX_PHASES];
 } compas_b200_parm;
 
 /* One box covering a single-level domain (the valid cells), its ghost width and its boundary codes
@@ -99,14 +109,22 @@ typedef struct compas_b200_geom {
 /* ---- parameters ------------------------------------------------------------------------------- */
 
 /* Reference defaults for the model (Parm, FiniteVolume_Parameter, Physics_Parameter and COMPAS run
- * defaults: WENO5, HLLC, cfl 0.4, change limiter on). */
+ * defaults: WENO5, HLLC, cfl 0.4, change limiter on). FIVEEQS_NPHASE gets NPHASE = 2, the
+ * reference's default (include/Macros.H:83-85). */
 int compas_b200_parm_init(compas_b200_parm* p, int physics, int dim);
+
+/* The same with the number of phases of FIVEEQS_NPHASE (2 <= nphase <= COMPAS_B200_MAX_PHASES; this
+ * build instantiates the N-phase kernels for nphase 2, 3, 4 in 2D and 3 in 3D). For the two-phase
+ * models nphase must be 2. */
+int compas_b200_parm_init_nphase(compas_b200_parm* p, int physics, int dim, int nphase);
 
 /* Set one inputs key, reference syntax and value set, e.g. ("FiniteVolume.Scheme", "WENO5B"),
  * ("Physics.RiemannSolver", "HLLC"), ("prob.EOS.gamma_2", "4.4"), ("run.cfl", "0.5"). Unknown keys
  * or values return COMPAS_B200_EARG with the valid values in compas_b200_last_error(), where the
  * reference aborts (e.g. include/Operators_FV/FiniteVolume_Parameter.H:143-146). EOS keys take
- * effect at compas_b200_parm_finalize. */
+ * effect at compas_b200_parm_finalize. FIVEEQS_NPHASE takes the per-phase lists
+ * ("prob.EOS.gamma", "1.4 1.5 1.5"), "prob.EOS.pinf", "prob.EOS.b", "prob.EOS.q" with exactly
+ * nphase values each (source/Parm.cpp:82-92). */
 int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value);
 
 /* Derive the EOS coefficients A, B, C, D from prob.EOS.* as Parm::Initialize does
@@ -255,6 +273,9 @@ typedef struct compas_b200_batch compas_b200_batch;
 
 int compas_b200_batch_create(int physics, int dim, int id_limiter, int precision, int capacity,
                              compas_b200_batch** out);
+/* The same for FIVEEQS_NPHASE cases with nphase phases (compas_b200_batch_create takes nphase = 2). */
+int compas_b200_batch_create_nphase(int physics, int dim, int nphase, int id_limiter, int precision, int capacity,
+                                    compas_b200_batch** out);
 int compas_b200_batch_destroy(compas_b200_batch* b);
 
 /* Admit a case: allocates its three state arrays, copies the state in (padded layout, time 0) and

@@ -1,6 +1,7 @@
 /* Test infrastructure (oracle): plain-C restatement of the reference's finite-volume right-hand side
  * and TVD-RK3 level advance for the two-phase five- and six-equation models (WENO5 + HLLC, the
- * stiffened-gas / NASG EOS, the six-equation pressure relaxation). It follows the reference's own
+ * stiffened-gas / NASG EOS, the six-equation pressure relaxation) and the N-phase five-equation model
+ * (FIVEEQS_NPHASE: WENO5 with the consistent limiter + HLLC). It follows the reference's own
  * per-face structure - every face converts its six stencil cells to primitives, reconstructs both
  * sides, converts back and calls the Riemann solver - with the same operations in the same order,
  * so that it agrees with the reference-header build (oracle/_ref) to the bit.
@@ -27,6 +28,14 @@
  *   divergence / NC      include/Operators_FV/FVM_SurfaceIntegral.H:17-28, FVM_Divergence_D.H,
  *                        include/Operators_Compressible5Eq/FVM_SurfaceIntegralNC_Compressible5Eq.H:15-52,
  *                        include/Operators_Compressible6Eq/FVM_SurfaceIntegralNC_Compressible6Eq.H:15-122
+ *   N-phase model        include/Physics_Compressible5Eq_NPhase/{Conservative2Primitive,Primitive2Conservative,
+ *                        EquationOfState_Mixture,SoundSpeed,rho_c2_Mixture,rho_c2_Phase,Conservative2Flux,
+ *                        Riemann_HLLC,NonConservative}_Compressible5Eq_NPhase.H;
+ *                        include/Operators_Compressible5Eq_NPhase/FVM_Reconstruction2Face_Conservative_WENO5_D_Compressible5Eq_NPhase.H,
+ *                        FVM_Reconstruction2Face_Conservative_LimiterConsistent_Compressible5Eq_NPhase.H,
+ *                        FVM_Reconstruction2Face_LimiterConsistent_Compressible5Eq_NPhase.H,
+ *                        FVM_SurfaceIntegralNC_Compressible5Eq_NPhase.H; include/Operators_FV/Limiter_Consistent.H,
+ *                        Reconstruction2Face_Linear.H
  *   relaxation           include/Physics_Compressible6Eq/Relaxation_Pressure_Instantaneous_Compressible6Eq.H:32-220,
  *                        include/RelaxationPressure_Safeguarded.H:17-256
  *   launch sites         source/Class_Compressible_PhaseField.cpp:3151-3391 (faces, divergence),
@@ -44,11 +53,14 @@
 
 #include "oracle_api.h"
 
-#define MAXN 8
+#define MAXN 12
+#define MAXP 4
 
 typedef struct {
     int six, D, N, NC;
     int IE, IE1, IE2, IA; /* IE: 5Eq energy; IE1/IE2: 6Eq phase energies */
+    int np;               /* FIVEEQS_NPHASE: phases (0 for the two-phase models) */
+    int IM;               /* first momentum component */
     const cmp_case* c;
 } Model;
 
@@ -57,6 +69,17 @@ static Model model_of(const cmp_case* c) {
     m.c = c;
     m.D = c->dim;
     m.six = (c->physics == 666);
+    m.np = (c->physics == 55501) ? c->nphase : 0;
+    if (m.np) {
+        m.N = 2 * m.np + m.D + 1;
+        m.NC = 1;
+        m.IM = m.np;
+        m.IE = m.np + m.D;
+        m.IE1 = m.IE2 = m.IE;
+        m.IA = m.np + m.D + 1;
+        return m;
+    }
+    m.IM = 2;
     m.N = (m.six ? 5 : 4) + m.D;
     m.NC = m.six ? 3 : 1;
     m.IE = 2 + m.D;
@@ -81,10 +104,127 @@ static double ksum(const double* u, int D) {
     return s;
 }
 
+/* ---- N-phase five-equation model -------------------------------------------------------------- */
+/* EquationOfState_Mixture sums over the phases, each from 0.0 */
+static void np_sums(const Model* m, const double* ar, const double* al, double* rho_D, double* AP, double* BP) {
+    const cmp_case* c = m->c;
+    *rho_D = 0.0;
+    for (int k = 0; k < m->np; ++k) *rho_D += ar[k] * c->Dk[k];
+    *AP = 0.0;
+    *BP = 0.0;
+    for (int k = 0; k < m->np; ++k) {
+        const double Phi = nasg_phi(al[k], ar[k], c->Ck[k]);
+        *AP += Phi * c->Ak[k];
+        *BP += Phi * c->Bk[k];
+    }
+}
+
+static void np_c2p(const Model* m, const double* U, double* W) {
+    const int D = m->D, NP = m->np;
+    double rho = 0.0, u[3], rho_D, AP, BP;
+    for (int k = 0; k < NP; ++k) rho += U[k];
+    for (int d = 0; d < D; ++d) u[d] = U[m->IM + d] / rho;
+    const double rho_e = U[m->IE] - (0.5) * rho * ksum(u, D);
+    np_sums(m, U, U + m->IA, &rho_D, &AP, &BP);
+    for (int k = 0; k < NP; ++k) {
+        W[k] = U[k];
+        W[m->IA + k] = U[m->IA + k];
+    }
+    for (int d = 0; d < D; ++d) W[m->IM + d] = u[d];
+    W[m->IE] = (rho_e - rho_D - BP) / AP;
+}
+
+static void np_p2c(const Model* m, const double* W, double* U) {
+    const int D = m->D, NP = m->np;
+    double rho = 0.0, rho_D, AP, BP;
+    for (int k = 0; k < NP; ++k) rho += W[k];
+    np_sums(m, W, W + m->IA, &rho_D, &AP, &BP);
+    const double rho_e = AP * W[m->IE] + BP + rho_D;
+    for (int k = 0; k < NP; ++k) {
+        U[k] = W[k];
+        U[m->IA + k] = W[m->IA + k];
+    }
+    for (int d = 0; d < D; ++d) U[m->IM + d] = rho * W[m->IM + d];
+    U[m->IE] = rho_e + (0.5) * rho * ksum(W + m->IM, D);
+}
+
+/* rho c^2 of the mixture from the phase values rhop_cp2 (rho_c2_Mixture) */
+static double np_rho_c2(const Model* m, const double* W, const double* rc2, int id_k) {
+    const cmp_case* c = m->c;
+    if (id_k == 0) {
+        double AP_rho_c2 = 0.0, AP = 0.0;
+        for (int k = 0; k < m->np; ++k) {
+            const double Phi = nasg_phi(W[m->IA + k], W[k], c->Ck[k]);
+            AP_rho_c2 += W[m->IA + k] * c->Ak[k] * rc2[k];
+            AP += Phi * c->Ak[k];
+        }
+        return AP_rho_c2 / AP;
+    }
+    double inv = 0.0;
+    for (int k = 0; k < m->np; ++k) inv += nasg_phi(W[m->IA + k], W[k], c->Ck[k]) / rc2[k];
+    return 1.0 / inv;
+}
+
+static void np_rc2_phases(const Model* m, double p, double* rc2) {
+    const cmp_case* c = m->c;
+    for (int k = 0; k < m->np; ++k) rc2[k] = ((c->Ak[k] + 1.0) * p + c->Bk[k]) / c->Ak[k];
+}
+
+static double np_sound_speed(const Model* m, const double* W) {
+    double rc2[MAXP], rho = 0.0;
+    np_rc2_phases(m, W[m->IE], rc2);
+    const double rho_c2 = np_rho_c2(m, W, rc2, m->c->source_term);
+    for (int k = 0; k < m->np; ++k) rho += W[k];
+    return sqrt(rho_c2 / rho);
+}
+
+/* Limiter_Consistent (include/Operators_FV/Limiter_Consistent.H) */
+static void np_limiter_consistent(int np, const double* slope, double* theta) {
+    const double ep = 1.0e-10;
+    double sum = 0.0, absv[MAXP];
+    for (int k = 0; k < np; ++k) {
+        sum += slope[k];
+        absv[k] = fabs(slope[k]);
+    }
+    int imax = 0; /* std::max_element: the first largest */
+    for (int k = 1; k < np; ++k)
+        if (absv[imax] < absv[k]) imax = k;
+    const double smax = slope[imax];
+    if (fabs(smax) < ep || fabs(sum) < ep) {
+        for (int k = 0; k < np; ++k) theta[k] = 1.0;
+    } else {
+        const double smaxS = smax - sum;
+        for (int k = 0; k < np; ++k) theta[k] = dmax(dmin(smax / smaxS, 1.0), 0.0);
+        theta[imax] = dmax(dmin(smaxS / smax, 1.0), 0.0);
+    }
+}
+
+/* FVM_Reconstruction2Face_Conservative_LimiterConsistent: Uf in/out, Uc the stencil centre */
+static void np_consistent(const Model* m, double* Uf, const double* Uc, double dx, int id_face) {
+    const int NP = m->np;
+    double Wf[MAXN], Wc[MAXN], s_ar[MAXP], s_al[MAXP], th[MAXP];
+    np_c2p(m, Uf, Wf);
+    np_c2p(m, Uc, Wc);
+    for (int k = 0; k < NP; ++k) {
+        s_ar[k] = (Wf[k] - Wc[k]) / ((double)id_face * 0.5 * dx);
+        s_al[k] = (Wf[m->IA + k] - Wc[m->IA + k]) / ((double)id_face * 0.5 * dx);
+    }
+    np_limiter_consistent(NP, s_al, th);
+    for (int k = 0; k < NP; ++k) {
+        Wf[k] = Wc[k] + (double)id_face * 0.5 * (th[k] * s_ar[k]) * dx;
+        Wf[m->IA + k] = Wc[m->IA + k] + (double)id_face * 0.5 * (th[k] * s_al[k]) * dx;
+    }
+    np_p2c(m, Wf, Uf);
+}
+
 /* ---- conversions ------------------------------------------------------------------------------ */
 static void c2p(const Model* m, const double* U, double* W) {
     const cmp_case* c = m->c;
     const int D = m->D;
+    if (m->np) {
+        np_c2p(m, U, W);
+        return;
+    }
     double u[3];
     const double a1r1 = U[0], a2r2 = U[1], alpha1 = U[m->IA];
     const double rho = a1r1 + a2r2;
@@ -115,6 +255,10 @@ static void c2p(const Model* m, const double* U, double* W) {
 static void p2c(const Model* m, const double* W, double* U) {
     const cmp_case* c = m->c;
     const int D = m->D;
+    if (m->np) {
+        np_p2c(m, W, U);
+        return;
+    }
     const double a1r1 = W[0], a2r2 = W[1], alpha1 = W[m->IA];
     const double alpha2 = 1.0 - alpha1;
     const double rho = a1r1 + a2r2;
@@ -141,6 +285,7 @@ static void p2c(const Model* m, const double* W, double* U) {
 
 static double sound_speed(const Model* m, const double* W) {
     const cmp_case* c = m->c;
+    if (m->np) return np_sound_speed(m, W);
     const double a1r1 = W[0], a2r2 = W[1], alpha1 = W[m->IA];
     double rho_c2;
     if (!m->six) {
@@ -165,6 +310,17 @@ static double sound_speed(const Model* m, const double* W) {
 }
 
 static void phys_flux(const Model* m, const double* U, const double* W, int d, double* F) {
+    if (m->np) {
+        const double V = W[m->IM + d], p = W[m->IE];
+        for (int k = 0; k < m->np; ++k) {
+            F[k] = U[k] * V;
+            F[m->IA + k] = U[m->IA + k] * V;
+        }
+        for (int k = 0; k < m->D; ++k) F[m->IM + k] = U[m->IM + k] * V;
+        F[m->IE] = (U[m->IE] + p) * V;
+        F[m->IM + d] += p;
+        return;
+    }
     const double V = W[2 + d];
     F[0] = U[0] * V;
     F[1] = U[1] * V;
@@ -334,8 +490,16 @@ static void hllc(const Model* m, const double* UL, const double* UR, int d, doub
     phys_flux(m, UL, WL, d, FL);
     phys_flux(m, UR, WR, d, FR);
     const double cL = sound_speed(m, WL), cR = sound_speed(m, WR);
-    const double VL = WL[2 + d], VR = WR[2 + d];
-    const double rhoL = WL[0] + WL[1], rhoR = WR[0] + WR[1];
+    const double VL = WL[m->IM + d], VR = WR[m->IM + d];
+    double rhoL = WL[0] + WL[1], rhoR = WR[0] + WR[1];
+    if (m->np) {
+        rhoL = 0.0;
+        rhoR = 0.0;
+        for (int k = 0; k < m->np; ++k) {
+            rhoL += WL[k];
+            rhoR += WR[k];
+        }
+    }
     double SL, SR, pL, pR;
     if (!m->six) {
         pL = WL[m->IE];
@@ -357,7 +521,7 @@ static void hllc(const Model* m, const double* UL, const double* UR, int d, doub
         for (int i = 0; i < N; ++i) {
             UsL[i] = (SL - VL) / (SL - S) * UL[i];
             UsR[i] = (SR - VR) / (SR - S) * UR[i];
-            if (i == 2 + d) {
+            if (i == m->IM + d) {
                 UsL[i] += (SL - VL) / (SL - S) * rhoL * (S - VL);
                 UsR[i] += (SR - VR) / (SR - S) * rhoR * (S - VR);
             } else if (i == m->IE) {
@@ -365,7 +529,7 @@ static void hllc(const Model* m, const double* UL, const double* UR, int d, doub
                 UsR[i] += (SR - VR) / (SR - S) * (S - VR) * (rhoR * S + pR / (SR - VR));
             }
         }
-        double vel = 0.5 * (1.0 + s) * WL[2 + d] + 0.5 * (1.0 - s) * WR[2 + d];
+        double vel = 0.5 * (1.0 + s) * WL[m->IM + d] + 0.5 * (1.0 - s) * WR[m->IM + d];
         vel += 0.5 * (1.0 + s) * Sm * ((SL - VL) / (SL - S) - 1.0) + 0.5 * (1.0 - s) * Sp * ((SR - VR) / (SR - S) - 1.0);
         fnc[0] = vel;
     } else {
@@ -399,7 +563,7 @@ static void hllc(const Model* m, const double* UL, const double* UR, int d, doub
     }
     for (int i = 0; i < N; ++i)
         Fo[i] = 0.5 * (1.0 + s) * (FL[i] + Sm * (UsL[i] - UL[i])) + 0.5 * (1.0 - s) * (FR[i] + Sp * (UsR[i] - UR[i]));
-    *cmax = dmax(cL + sqrt(ksum(WL + 2, D)), cR + sqrt(ksum(WR + 2, D)));
+    *cmax = dmax(cL + sqrt(ksum(WL + m->IM, D)), cR + sqrt(ksum(WR + m->IM, D)));
 }
 
 /* ---- six-equation pressure relaxation -------------------------------------------------------------- */
@@ -651,11 +815,11 @@ static void load(const Model* m, const Geo* g, const double* U, int i, int j, in
 }
 
 /* BCType of component n across a boundary normal to d (0 periodic, 1 extrap, 2 even, 3 odd) */
-static int bc_kind(int code, int n, int d, int D) {
-    const int mom = (n >= 2 && n < 2 + D);
+static int bc_kind(int code, int n, int d, int D, int m0) {
+    const int mom = (n >= m0 && n < m0 + D);
     if (code == 0) return 0;
     if (code == 2) return 1;
-    if (code == 3 || code == 4) return (mom && n - 2 == d) ? 3 : 2;
+    if (code == 3 || code == 4) return (mom && n - m0 == d) ? 3 : 2;
     return mom ? 3 : 2;
 }
 
@@ -679,7 +843,7 @@ int cmp_fill_ghosts(const cmp_case* c, double* U) {
             for (int side = 0; side < 2; ++side) {
                 const int code = side == 0 ? c->lo_bc[d] : c->hi_bc[d];
                 if (code != 0 && code != 2 && code != 3 && code != 4 && code != 5) return -1;
-                const int kind = bc_kind(code, n, d, m.D);
+                const int kind = bc_kind(code, n, d, m.D, m.IM);
                 for (int k = -g.gz; k < g.n[2] + g.gz; ++k)
                     for (int j = -g.ng; j < g.n[1] + g.ng; ++j)
                         for (int i = -g.ng; i < g.n[0] + g.ng; ++i) {
@@ -864,10 +1028,12 @@ static void face_flux(const Model* m, const Geo* g, const double* U, int i, int 
     if (bounded) weno5b_bounded(m, P, 1, WL);
     for (int n = n0; n < n1; ++n) WL[n] = weno5(P[0][n], P[1][n], P[2][n], P[3][n], P[4][n], 1);
     p2c(m, WL, UL);
+    if (m->np) np_consistent(m, UL, C[2], m->c->dx[d], 1);
     for (int s = 1; s < 6; ++s) c2p(m, C[s], P[s]);
     if (bounded) weno5b_bounded(m, P + 1, -1, WR);
     for (int n = n0; n < n1; ++n) WR[n] = weno5(P[1][n], P[2][n], P[3][n], P[4][n], P[5][n], -1);
     p2c(m, WR, UR);
+    if (m->np) np_consistent(m, UR, C[3], m->c->dx[d], -1);
     hllc(m, UL, UR, d, F, fnc, cmax);
 }
 
@@ -927,7 +1093,21 @@ int cmp_compute_dudt(const cmp_case* c, const double* U, double* dUdt, double* c
                 for (int n = 0; n < N; ++n) dUdt[n * g.S + q] = -div[n];
                 load(&m, &g, U, i, j, k, Uc);
                 c2p(&m, Uc, W);
-                if (!m.six) {
+                if (m.np) {
+                    /* alpha_k += phi_k (1 + K_k) div u* (FVM_SurfaceIntegralNC_Compressible5Eq_NPhase.H) */
+                    double K[MAXP], rc2[MAXP];
+                    for (int kk = 0; kk < m.np; ++kk) K[kk] = 0.0;
+                    if (c->source_term == 1) {
+                        np_rc2_phases(&m, W[m.IE], rc2);
+                        const double rho_c2 = np_rho_c2(&m, W, rc2, 1);
+                        for (int kk = 0; kk < m.np; ++kk) K[kk] = (rho_c2 / rc2[kk] - 1.0);
+                    }
+                    for (int kk = 0; kk < m.np; ++kk) {
+                        const double al = Uc[m.IA + kk];
+                        const double Phi = (c->source_term == 1) ? nasg_phi(al, Uc[kk], c->Ck[kk]) : al;
+                        dUdt[(m.IA + kk) * g.S + q] += Phi * (1.0 + K[kk]) * div[N];
+                    }
+                } else if (!m.six) {
                     double K1 = 0.0;
                     double phi1 = Uc[m.IA];
                     if (c->source_term == 1) {

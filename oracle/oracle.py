@@ -22,7 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 PORT_LIB = os.path.join(HERE, "liboracle.so")
 
-FIVEEQS, SIXEQS = 555, 666
+FIVEEQS, SIXEQS, FIVEEQS_NPHASE = 555, 666, 55501
 
 
 class Case(ctypes.Structure):
@@ -49,6 +49,9 @@ class Case(ctypes.Structure):
         ("thinc_normal_threshold", ctypes.c_double),
         ("cfl", ctypes.c_double),
         ("change_limiter", ctypes.c_int),
+        ("nphase", ctypes.c_int),
+        ("Ak", ctypes.c_double * 4), ("Bk", ctypes.c_double * 4),
+        ("Ck", ctypes.c_double * 4), ("Dk", ctypes.c_double * 4),
     ]
 
 
@@ -100,13 +103,15 @@ def pf_from(parm, tol_rel=None) -> PfCase:
 _cache: dict = {}
 
 
-def ref_lib_path(physics: int, dim: int) -> str:
+def ref_lib_path(physics: int, dim: int, nphase: int = 2) -> str:
+    if physics == FIVEEQS_NPHASE:
+        return os.path.join(REF_DIR, f"libref_5eqn{nphase}_{dim}d.so")
     model = "5eq" if physics == FIVEEQS else "6eq"
     return os.path.join(REF_DIR, f"libref_{model}_{dim}d.so")
 
 
-def have_ref(physics: int, dim: int) -> bool:
-    return os.path.exists(ref_lib_path(physics, dim))
+def have_ref(physics: int, dim: int, nphase: int = 2) -> bool:
+    return os.path.exists(ref_lib_path(physics, dim, nphase))
 
 
 def build_port() -> str:
@@ -117,9 +122,9 @@ def build_port() -> str:
     return PORT_LIB
 
 
-def load(kind: str, physics: int, dim: int) -> ctypes.CDLL:
+def load(kind: str, physics: int, dim: int, nphase: int = 2) -> ctypes.CDLL:
     """kind 'reference' (reference headers) or 'port' (C restatement)."""
-    path = ref_lib_path(physics, dim) if kind == "reference" else build_port()
+    path = ref_lib_path(physics, dim, nphase) if kind == "reference" else build_port()
     if path not in _cache:
         if not os.path.exists(path):
             raise FileNotFoundError(path)
@@ -148,6 +153,10 @@ def case_from(parm, geom) -> Case:
               "relaxation", "relax_trace", "thinc", "thinc_use_normal", "thinc_eps", "thinc_beta",
               "thinc_normal_threshold", "cfl", "change_limiter"):
         setattr(c, k, getattr(parm, k))
+    c.nphase = getattr(parm, "nphase", 2)
+    if parm.physics == FIVEEQS_NPHASE:
+        for k in range(4):
+            c.Ak[k], c.Bk[k], c.Ck[k], c.Dk[k] = parm.Ak[k], parm.Bk[k], parm.Ck[k], parm.Dk[k]
     return c
 
 
@@ -157,7 +166,7 @@ class Oracle:
         a case amplifies last-bit differences of exp/log/tanh between math libraries."""
         self.kind = kind
         self.case = case_from(parm, geom)
-        self.lib = load(kind, parm.physics, parm.dim)
+        self.lib = load(kind, parm.physics, parm.dim, getattr(parm, "nphase", 2))
         self.thinc_ulp = bool(thinc_ulp)
         if self.thinc_ulp and kind != "port":
             raise ValueError("the one-ulp THINC control exists in the port only")

@@ -22,7 +22,7 @@ extern "C" {
 #endif
 
 typedef struct cmp_case {
-    int physics;        /* 555 FIVEEQS, 666 SIXEQS (include/Macros.H:56-59) */
+    int physics;        /* 555 FIVEEQS, 666 SIXEQS, 55501 FIVEEQS_NPHASE (include/Macros.H:56-59) */
     int dim;            /* 2 or 3 */
     int n[3];           /* valid cells per direction (n[2] = 1 in 2D) */
     int ng;             /* ghost cells (3 for WENO5/WENO5B) */
@@ -40,6 +40,8 @@ typedef struct cmp_case {
     double thinc_eps, thinc_beta, thinc_normal_threshold;
     double cfl;         /* run.cfl */
     int change_limiter; /* run.timestep_change_limiter */
+    int nphase;         /* FIVEEQS_NPHASE (55501): phases (the build's NPHASE); 2 otherwise */
+    double Ak[4], Bk[4], Ck[4], Dk[4];  /* FIVEEQS_NPHASE EOS coefficients per phase (source/Parm.cpp:185-253) */
 } cmp_case;
 
 /* Number of conserved components of the case (NSTATE). */

@@ -22,7 +22,15 @@
 
 #include <Parm.H>
 
+#if (PHYSICS == FIVEEQS_NPHASE)
+#include <Physics_Compressible_NPhase.H>
+#include <Physics_Compressible5Eq_NPhase.H>
+#include <Operators_FV.H>
+#include <Operators_FD.H>
+#include <Operators_Compressible5Eq_NPhase.H>
+#else
 #include <Physics_Compressible_TwoPhase.H>
+#endif
 #if (PHYSICS == FIVEEQS)
 #include <Physics_Compressible5Eq.H>
 #include <Operators_FV.H>
@@ -76,8 +84,17 @@ struct Geo {
 Parm make_parm(const cmp_case* c) {
     Parm p;
     p.EOS = 1;
+#if (PHYSICS == FIVEEQS_NPHASE)
+    if (c->nphase != NPHASE) amrex::Abort("the case's nphase differs from this build's NPHASE");
+    for (int k = 0; k < NPHASE; ++k) {
+        p.A[k] = c->Ak[k]; p.B[k] = c->Bk[k]; p.C[k] = c->Ck[k]; p.D[k] = c->Dk[k];
+        p.p_min[k] = 0.0;
+    }
+#else
     p.A1 = c->A1; p.A2 = c->A2; p.B1 = c->B1; p.B2 = c->B2;
     p.C1 = c->C1; p.C2 = c->C2; p.D1 = c->D1; p.D2 = c->D2;
+    p.p_min = {0.0, 0.0};
+#endif
     auto& fv = p.FiniteVolume_Parm;
     fv.ID_WENO = 1;
     fv.ID_Limiter = c->id_limiter;
@@ -90,9 +107,8 @@ Parm make_parm(const cmp_case* c) {
     fv.THINC_EPS = c->thinc_eps;
     fv.THINC_Beta = c->thinc_beta;
     fv.THINC_NormalThreshold = c->thinc_normal_threshold;
-    p.p_min = {0.0, 0.0};
     p.Physics_Parm.ID_Riemann = c->id_riemann;
-#if (PHYSICS == FIVEEQS)
+#if (PHYSICS == FIVEEQS || PHYSICS == FIVEEQS_NPHASE)
     p.Physics_Parm.source_term = c->source_term;
 #elif (PHYSICS == SIXEQS)
     p.Physics_Parm.pressure_relaxation = c->relaxation;
@@ -103,12 +119,18 @@ Parm make_parm(const cmp_case* c) {
 }
 
 // AMReX BCType for component n in direction d at code `code`
-// (source/Class_Compressible6Eq_PhaseField.cpp:362-431): 0 int_dir, 2 foextrap, 3/4 reflect_even
-// (normal momentum reflect_odd), 5 reflect_odd for every momentum component.
+// (source/Class_Compressible6Eq_PhaseField.cpp:362-431, Class_Compressible5Eq_NPhase_PhaseField.cpp:
+// 133-205): 0 int_dir, 2 foextrap, 3/4 reflect_even (normal momentum reflect_odd), 5 reflect_odd for
+// every momentum component.
 enum { BC_INT = 0, BC_FOEXTRAP = 1, BC_EVEN = 2, BC_ODD = 3 };
 int bc_kind(int code, int n, int d) {
-    const bool mom = (n >= 2 && n < 2 + AMREX_SPACEDIM);
-    const bool normal = mom && (n - 2 == d);
+#if (PHYSICS == FIVEEQS_NPHASE)
+    const int m0 = NPHASE;
+#else
+    const int m0 = 2;
+#endif
+    const bool mom = (n >= m0 && n < m0 + AMREX_SPACEDIM);
+    const bool normal = mom && (n - m0 == d);
     switch (code) {
         case 0: return BC_INT;
         case 2: return BC_FOEXTRAP;
@@ -861,7 +883,9 @@ void pf_step(const cmp_case* c, const cmp_pf* pf, double* U, double dt, double* 
 }
 #endif  // PHYSICS == FIVEEQS
 
+#if (PHYSICS != FIVEEQS_NPHASE)
 #include "ref_amr.inc"
+#endif
 
 template <class Fn>
 int guarded(Fn&& fn) {
@@ -1011,9 +1035,14 @@ int cmp_advance_pf(const cmp_case* c, const cmp_pf* pf, double* U, int nsteps, d
 
 int cmp_amr_advance(const cmp_case* c, int nlev, const cmp_amr_box* boxes, int nbox, double** U, int nsteps,
                     double stop_time, double* t, double* dts) {
+#if (PHYSICS != FIVEEQS_NPHASE)
     int taken = 0;
     int rc = guarded([&] { taken = amr_advance(c, nlev, boxes, nbox, U, nsteps, stop_time, t, dts); });
     return rc == 0 ? taken : rc;
+#else
+    (void)c; (void)nlev; (void)boxes; (void)nbox; (void)U; (void)nsteps; (void)stop_time; (void)t; (void)dts;
+    return -2;
+#endif
 }
 
 }  // extern "C"

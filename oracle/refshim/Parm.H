@@ -1,6 +1,6 @@
 // Test infrastructure (oracle): the per-case parameter struct that the reference's physics headers
 // take as `Parm const&`. Field names and meanings mirror exec/_Tests/Advection/prob/Parm.H:33-117
-// (the two-phase models); the linear-solver block is left out because no hyperbolic-path function
+// (the two-phase models) and exec/TriplePoint-5Eq-N/prob/Parm.H (FIVEEQS_NPHASE); the linear-solver block is left out because no hyperbolic-path function
 // reads it. The oracle driver fills the fields directly (the EOS coefficients as source/Parm.cpp:
 // 101-188 computes them), so no ParmParse input is read.
 #ifndef PARM_H_
@@ -14,12 +14,34 @@
 #include <Physics_Parameter_Compressible5Eq.H>
 #elif (PHYSICS == SIXEQS)
 #include <Physics_Parameter_Compressible6Eq.H>
+#elif (PHYSICS == FIVEEQS_NPHASE)
+#include <Physics_Parameter_Compressible5Eq_NPhase.H>
 #else
-#error "the oracle build covers the two-phase models FIVEEQS and SIXEQS"
+#error "the oracle build covers FIVEEQS, SIXEQS and FIVEEQS_NPHASE"
 #endif
 #include <FiniteVolume_Parameter.H>
 #include <PhaseField_Parameter.H>
 
+#if (PHYSICS == FIVEEQS_NPHASE)
+// The N-phase model's Parm (exec/TriplePoint-5Eq-N/prob/Parm.H): per-phase EOS arrays.
+struct Parm
+{
+    Physics_Parameter Physics_Parm;
+    FiniteVolume_Parameter FiniteVolume_Parm;
+    PhaseField_Parameter PhaseField_Parm;
+
+    int EOS = 1;
+    amrex::Array<amrex::Real, NPHASE> A, B, C, D;
+    amrex::Array<amrex::Real, NPHASE> gamma, pinf, gGamma, pref, eref, cv, mu, muB, kappa;
+
+    amrex::Real K = 0.0;
+    amrex::Array<amrex::Real, NSTATE> UpperBound;
+    amrex::Array<amrex::Real, NSTATE> LowerBound;
+    amrex::Array<int, NSTATE> ID_BoundType;
+    amrex::Array<amrex::Real, NPHASE> p_min;
+    int interface_thickness = 0;
+};
+#else
 struct Parm
 {
     Physics_Parameter Physics_Parm;
@@ -44,5 +66,6 @@ struct Parm
     amrex::Array<amrex::Real, 2> p_min;
     int interface_thickness = 0;
 };
+#endif
 
 #endif

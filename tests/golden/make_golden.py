@@ -30,6 +30,10 @@ CASES = {
     "bubble_thinc_weno5b_5eq_2d_31x19": (cases.shock_bubble, dict(nx=31, ny=19, scheme="WENO5B"), 6,
                                          {"FiniteVolume.THINC": "1", "FiniteVolume.THINC.UseNormal": "0"}),
     "droplet_thinc_6eq_3d_12": (cases.shock_droplet, dict(n=12), 3, {"FiniteVolume.THINC": "1"}),
+    "triple_5eqn3_2d_42x18": (cases.triple_point, dict(m=6), 10),
+    "bubbles_nasg_k_5eqn4_2d_24": (cases.nphase_bubbles, dict(n=24, nphase=4, eos=3, source_term=1), 6),
+    "bubbles_5eqn2_2d_24": (cases.nphase_bubbles, dict(n=24, nphase=2), 6),
+    "bubbles_5eqn3_3d_10": (cases.nphase_bubbles, dict(n=10, nphase=3, dim=3), 3),
 }
 
 

@@ -5,8 +5,8 @@ import compas_b200 as cb
 from oracle.oracle import Oracle, have_ref
 
 
-def oracle_kind(physics, dim):
-    return "reference" if have_ref(physics, dim) else "port"
+def oracle_kind(physics, dim, nphase=2):
+    return "reference" if have_ref(physics, dim, nphase) else "port"
 
 
 def rel_linf(a, b):
@@ -20,7 +20,7 @@ def rel_linf(a, b):
 
 def build_case(case_fn, **kw):
     phys, dim, inputs, geom, U = case_fn(**kw)
-    p = cb.make_parm(phys, dim, inputs)
+    p = cb.make_parm(phys, dim, inputs)  # FIVEEQS_NPHASE: nphase from the per-phase lists
     g = cb.make_geom(**geom)
     return p, g, U
 
@@ -38,6 +38,6 @@ def run_gpu(p, g, U, nsteps, use_graph=True, stop_time=1e300):
 
 def run_oracle(p, g, U, nsteps, kind=None, stop_time=1e300):
     ref = U.copy()
-    o = Oracle(kind or oracle_kind(p.physics, p.dim), p, g)
+    o = Oracle(kind or oracle_kind(p.physics, p.dim, p.nphase), p, g)
     t, dts = o.advance(ref, nsteps, stop_time=stop_time)
     return ref, t, dts

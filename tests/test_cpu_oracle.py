@@ -53,6 +53,42 @@ def test_port_matches_reference_build(case, kw, steps, extra):
     np.testing.assert_array_equal(a, b)
 
 
+@pytest.mark.parametrize("case,kw,steps", [
+    (cases.triple_point, dict(m=8), 12),
+    (cases.nphase_bubbles, dict(n=20, nphase=2), 6),
+    (cases.nphase_bubbles, dict(n=20, nphase=3, source_term=1), 6),
+    (cases.nphase_bubbles, dict(n=20, nphase=4, eos=3, source_term=1), 6),
+    (cases.nphase_bubbles, dict(n=10, nphase=3, dim=3), 2),
+], ids=["triple8", "bubbles2", "bubbles3_K", "bubbles4_nasg_K", "bubbles3_3d"])
+def test_port_matches_reference_build_nphase(case, kw, steps):
+    """The N-phase restatement (WENO5 with the consistent limiter, HLLC, Kapila terms) equals the
+    reference's own N-phase headers to the bit."""
+    phys, dim, inputs, geom, U = case(**kw)
+    p, g = _parm_geom(phys, dim, inputs, geom)
+    if not have_ref(phys, dim, p.nphase):
+        pytest.skip("reference-header oracle not built here")
+    a, b = U.copy(), U.copy()
+    ta, da = Oracle("reference", p, g).advance(a, steps)
+    tb, db = Oracle("port", p, g).advance(b, steps)
+    np.testing.assert_array_equal(da, db)
+    np.testing.assert_array_equal(a, b)
+
+
+def test_nphase_parm_lists_follow_the_reference_rules():
+    """prob.EOS.gamma and the other per-phase lists need exactly NPHASE values (source/Parm.cpp:82-92);
+    A_k = 1/(gamma_k - 1), B_k = gamma_k pinf_k/(gamma_k - 1)."""
+    p = cb.make_parm(cb.FIVEEQS_NPHASE, 2, {"prob.EOS.gamma": [1.4, 1.5, 4.4], "prob.EOS.pinf": [0, 0, 6e8]})
+    assert p.nphase == 3 and cb.parm_nstate(p) == 9
+    assert list(p.Ak[:3]) == [1.0 / (1.4 - 1.0), 1.0 / (1.5 - 1.0), 1.0 / (4.4 - 1.0)]
+    assert p.Bk[2] == 4.4 * 6e8 / (4.4 - 1.0)
+    with pytest.raises(cb.CompasError):
+        cb.make_parm(cb.FIVEEQS_NPHASE, 2, {"prob.EOS.gamma": [1.4, 1.5]}, nphase=3)
+    with pytest.raises(cb.CompasError):
+        cb.make_parm(cb.FIVEEQS_NPHASE, 2, {"prob.EOS.gamma": [1.4, 0.9, 1.5]})
+    with pytest.raises(cb.CompasError):
+        cb.make_parm(cb.FIVEEQS_NPHASE, 2, {"prob.EOS.gamma": [1.4] * 5}, nphase=5)
+
+
 def test_conservation_periodic_round_off():
     phys, dim, inputs, geom, U = cases.advected_disc(n=32)
     p, g = _parm_geom(phys, dim, inputs, geom)

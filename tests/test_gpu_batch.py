@@ -79,7 +79,9 @@ def test_serving_results_identical_alone_and_in_the_mix():
     """Continuous batching: requests admitted while others run give the same state as alone."""
     from compas_b200 import serving
 
-    reqs = serving.poisson_requests(6, rate=200.0, seed=1, sides2d=(32, 64), sides3d=(16, 24), steps=(5, 12))
+    reqs = serving.poisson_requests(9, rate=200.0, seed=1, sides2d=(32, 64), sides3d=(16, 24), sides_triple=(16, 32),
+                                    steps=(5, 12))
+    assert {r.kind for r in reqs} == set(serving.KINDS)
     srv = serving.Server(budget_bytes=150e9, precision="mixed", keep_results=True, steps_per_iter=1)
     done = srv.run(reqs)
     srv.close()

@@ -42,6 +42,16 @@ __device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b 
 __device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }
 __device__ __forceinline__ double sgn0(double x) { return x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : 0.0); }
 
+// Reciprocal for the mixed-precision form: an FP32 estimate refined by one Newton-Raphson step for
+// 1/x, r1 = r0 (2 - x r0), evaluated in FP64 (Newton's method; the relative error squares, from
+// about 2^-22 to below 2^-43). For x of FP32 range (densities, A_P). The quantities scaled by it are
+// rounded to FP32 afterwards, so the result matches the IEEE FP64 quotient except within 2^-43 of a
+// rounding boundary, at a fraction of the cost of an FP64 division.
+__device__ __forceinline__ double rcp_mixed(double x) {
+    const double r0 = (double)__fdividef(1.0f, (float)x);
+    return r0 * (2.0 - x * r0);
+}
+
 // EOS coefficients, partial form alpha rho e = A Pi + B phi + alpha rho D, with C the NASG covolume b
 // (source/Parm.cpp:101-188): the two phases of FIVEEQS / SIXEQS, and the per-phase lists of
 // FIVEEQS_NPHASE (source/Parm.cpp:185-262).
@@ -145,7 +155,7 @@ struct FiveEq {
     __device__ static __forceinline__ void cons2prim_f32(float* W, const double* U, const Eos& e) {
         const double a1r1 = U[0], a2r2 = U[1], alpha1 = U[IA];
         const double rho = a1r1 + a2r2;
-        const double ir = 1.0 / rho;  // one FP64 reciprocal: u = fl32(rho u / rho) keeps uniform flow uniform
+        const double ir = rcp_mixed(rho);  // near-FP64 reciprocal: u = fl32(rho u / rho) keeps uniform flow uniform
         double m2 = U[2] * U[2] + U[3] * U[3];
         if (D == 3) m2 += U[4] * U[4];
         const double alpha2 = 1.0 - alpha1;
@@ -157,7 +167,7 @@ struct FiveEq {
         W[1] = (float)a2r2;
 #pragma unroll
         for (int d = 0; d < D; ++d) W[2 + d] = (float)(U[2 + d] * ir);
-        W[IE] = (float)(num / AP);  // rounded once from FP64: a uniform pressure stays uniform
+        W[IE] = (float)(num * rcp_mixed(AP));  // rounded once from near-FP64: a uniform pressure stays uniform
         W[IA] = (float)alpha1;
     }
 
@@ -441,7 +451,7 @@ struct SixEq {
         const double a1r1 = U[0], a2r2 = U[1], alpha1 = U[IA];
         const double alpha2 = 1.0 - alpha1;
         const double rho = a1r1 + a2r2;
-        const double ir = 1.0 / rho;  // one FP64 reciprocal: u = fl32(rho u / rho) keeps uniform flow uniform
+        const double ir = rcp_mixed(rho);  // near-FP64 reciprocal: u = fl32(rho u / rho) keeps uniform flow uniform
         double m2 = U[2] * U[2] + U[3] * U[3];
         if (D == 3) m2 += U[4] * U[4];
         const double k = (m2 * ir) * ir;  // |u|^2
@@ -454,8 +464,8 @@ struct SixEq {
 #pragma unroll
         for (int d = 0; d < D; ++d) W[2 + d] = (float)(U[2 + d] * ir);
         // rounded once from FP64 (a uniform pressure stays uniform); the NASG factor 1/xi in FP32
-        W[IE1] = (float)(n1 * e.iA1) / xi1;
-        W[IE2] = (float)(n2 * e.iA2) / xi2;
+        W[IE1] = (e.C1 > 0.0) ? (float)(n1 * e.iA1) / xi1 : (float)(n1 * e.iA1);
+        W[IE2] = (e.C2 > 0.0) ? (float)(n2 * e.iA2) / xi2 : (float)(n2 * e.iA2);
         W[IA] = (float)alpha1;
     }
 

@@ -73,12 +73,12 @@ struct FiveEqN {
     }
 
     // Mixed precision: the pressure numerator rho e - rho D - B_P (where the energy cancels against
-    // the B_k terms) and A_P in FP64, one FP64 reciprocal of rho, the primitives rounded once to FP32.
+    // the B_k terms) and A_P in FP64, near-FP64 reciprocals (rcp_mixed), the primitives rounded once to FP32.
     __device__ static __forceinline__ void cons2prim_f32(float* W, const double* U, const Eos& e) {
         double rho = 0.0;
 #pragma unroll
         for (int k = 0; k < NP; ++k) rho += U[k];
-        const double ir = 1.0 / rho;
+        const double ir = rcp_mixed(rho);
         double m2 = U[IM] * U[IM] + U[IM + 1] * U[IM + 1];
         if (D == 3) m2 += U[IM + 2] * U[IM + 2];
         double rho_D = 0.0, AP = 0.0, BP = 0.0;
@@ -95,7 +95,7 @@ struct FiveEqN {
         for (int k = 0; k < NP; ++k) W[k] = (float)U[k];
 #pragma unroll
         for (int d = 0; d < D; ++d) W[IM + d] = (float)(U[IM + d] * ir);
-        W[IE] = (float)(num / AP);
+        W[IE] = (float)(num * rcp_mixed(AP));
 #pragma unroll
         for (int k = 0; k < NP; ++k) W[IA + k] = (float)U[IA + k];
     }

@@ -137,9 +137,11 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
     const int tid = threadIdx.x;
     unsigned int* err = a.err;
 
-    // 1. tile cells -> primitives
-    for (int l = tid; l < CELLS; l += NT) {
-        const int lx = l % TX, ly = (l / TX) % TY, lz = l / (TX * TY);
+    // 1. tile cells and the x-direction halo slabs -> primitives, read as whole rows of TX + 6 cells
+    // (coalesced), the tile cells into Pint and the halo cells into the x slabs of Phal
+    constexpr int RX = TX + 6;
+    for (int l = tid; l < RX * TY * TZ; l += NT) {
+        const int lx = l % RX - 3, ly = (l / RX) % TY, lz = l / (RX * TY);
         const int i = i0 + lx, j = j0 + ly, k = k0 + lz;
         double U[N];
         PT W[N];
@@ -151,8 +153,17 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
 #pragma unroll
             for (int n = 0; n < N; ++n) W[n] = 0;
         }
+        int dst;
+        if (lx >= 0 && lx < TX) {
+            dst = lx + TX * (ly + TY * lz);
+        } else {
+            const int slot = (lx < 0) ? lx + 3 : lx - TX + 3;
+            dst = N * CELLS + slot * T::A0 + (ly + TX * lz);
+        }
+        PT* out = (dst < N * CELLS) ? Pint + dst : Phal + (dst - N * CELLS);
+        const int stride = (dst < N * CELLS) ? CELLS : HALO;
 #pragma unroll
-        for (int n = 0; n < N; ++n) Pint[n * CELLS + l] = W[n];
+        for (int n = 0; n < N; ++n) out[n * stride] = W[n];
     }
 
     double acc[R][NB];
@@ -164,8 +175,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
         constexpr int Td = TX;
         constexpr int Ad = T::A0;
         constexpr int Ta = TX;
-        // 2a. halo slabs of direction d -> primitives
-        for (int h = tid; h < 6 * Ad; h += NT) {
+        // 2a. halo slabs of direction d -> primitives (the x slabs came with the rows of step 1)
+        for (int h = (d == 0) ? 6 * Ad : tid; h < 6 * Ad; h += NT) {
             const int slot = h / Ad, t = h % Ad;
             const int pos = (slot < 3) ? slot - 3 : Td + slot - 3;
             const int ta = t % Ta, tb = t / Ta;
@@ -343,7 +354,9 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
         }
         __syncthreads();
 
-        // 2c. divergence contribution of direction d
+        // 2c. divergence contribution of direction d: (F+ - F-)/dx as the reference divides (FP64 form);
+        // times the reciprocal of dx in the mixed form (an FP64 division per term dominates otherwise)
+        const double idxd = 1.0 / dxd;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int l = tid + r * NT;
@@ -356,7 +369,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                 else { fl = lx + TS * (lz + EF * ly); fh = fl + TS; }
 #pragma unroll
                 for (int c = 0; c < NB; ++c) {
-                    const double tt = (Fb[c * FMAX + fh] - Fb[c * FMAX + fl]) / dxd;
+                    const double df = Fb[c * FMAX + fh] - Fb[c * FMAX + fl];
+                    const double tt = MIX ? df * idxd : df / dxd;
                     acc[r][c] = (d == 0) ? tt : acc[r][c] + tt;
                 }
             }

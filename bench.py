@@ -446,7 +446,7 @@ def run_ours(args, rank, world, dist):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    levels, ms, clks = {}, {}, []
+    levels, ms, clks, tuned = {}, {}, [], {}
     for name, p in forms.items():
         lv = cb.Level(p, g)
         lv.upload(U, stream=stream)
@@ -470,6 +470,7 @@ def run_ours(args, rank, world, dist):
         assert info.steps == info0.steps + args.steps, (info0, info)
         ms[name] = max_over_ranks(t_ms)
         levels[name] = lv
+        tuned[name] = lv.kernel()
     head = "mixed" if "mixed" in forms else "fp64"
     p = forms[head]
     value = world * cells * 3 * args.steps / (ms[head] / 1e3)
@@ -575,7 +576,10 @@ def run_ours(args, rank, world, dist):
             "dtype": "f32 reconstruction, f64 state/EOS/Riemann/relaxation" if head == "mixed" else "f64",
             "data": "synthetic",
             "config": workload_config(n, {"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                                          "precision": head}),
+                                          "precision": head,
+                                          "stage_kernel_autotuned": {
+                                              k: {"launch_shape": v[0], "tile_order": ("x fastest", "bricks")[v[1]]}
+                                              for k, v in tuned.items()}}),
             "fp64_plain": ({"value": world * cells * 3 * args.steps / (ms["fp64"] / 1e3),
                             "ms_per_step": ms["fp64"] / args.steps,
                             "note": "bit-identical to the reference CPU arithmetic"} if "fp64" in ms else None),

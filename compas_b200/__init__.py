@@ -80,6 +80,7 @@ class Parm(ctypes.Structure):
         ("b_k", ctypes.c_double * MAX_PHASES), ("q_k", ctypes.c_double * MAX_PHASES),
         ("Ak", ctypes.c_double * MAX_PHASES), ("Bk", ctypes.c_double * MAX_PHASES),
         ("Ck", ctypes.c_double * MAX_PHASES), ("Dk", ctypes.c_double * MAX_PHASES),
+        ("autotune", ctypes.c_int),
     ]
 
 
@@ -131,6 +132,12 @@ _SIGS = {
     "compas_b200_level_dts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
     "compas_b200_level_launches": (ctypes.c_longlong, [ctypes.c_void_p]),
     "compas_b200_level_pf_substeps": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "compas_b200_level_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                                ctypes.POINTER(ctypes.c_int)]),
+    "compas_b200_level_set_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "compas_b200_batch_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                                ctypes.POINTER(ctypes.c_int)]),
+    "compas_b200_batch_set_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "compas_b200_amr_create": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_int, ctypes.c_void_p,
                                               ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "compas_b200_amr_destroy": (ctypes.c_int, [ctypes.c_void_p]),
@@ -416,6 +423,16 @@ class Level:
     def launches(self) -> int:
         return int(lib().compas_b200_level_launches(self._h))
 
+    def kernel(self) -> tuple:
+        """(launch shape, tile order) of the stage kernel: the autotuner's pick after the first advance."""
+        sh, od = ctypes.c_int(), ctypes.c_int()
+        _check(lib().compas_b200_level_kernel(self._h, ctypes.byref(sh), ctypes.byref(od)))
+        return sh.value, od.value
+
+    def set_kernel(self, shape: int, order: int) -> None:
+        """Force a launch shape and tile order (no tuning for this level)."""
+        _check(lib().compas_b200_level_set_kernel(self._h, int(shape), int(order)))
+
     def pf_substeps(self) -> int:
         """Phase-Field sub-steps taken so far (PhaseField.phase_field = 1)."""
         return int(lib().compas_b200_level_pf_substeps(self._h))
@@ -585,3 +602,11 @@ class Batch:
 
     def launches(self) -> int:
         return int(lib().compas_b200_batch_launches(self._h))
+
+    def kernel(self) -> tuple:
+        sh, od = ctypes.c_int(), ctypes.c_int()
+        _check(lib().compas_b200_batch_kernel(self._h, ctypes.byref(sh), ctypes.byref(od)))
+        return sh.value, od.value
+
+    def set_kernel(self, shape: int, order: int) -> None:
+        _check(lib().compas_b200_batch_set_kernel(self._h, int(shape), int(order)))

@@ -128,4 +128,6 @@ struct compas_b200_batch {
     long long launches = 0;
     cudaGraphExec_t graph = nullptr;
     cudaStream_t graph_stream = nullptr;
+    int shape = 0, order = 0;   // box-list kernel launch shape and tile order (autotuner or forced)
+    bool tuned = false, forced = false;
 };

@@ -10,6 +10,7 @@
 #include <cstring>
 #include <string>
 #include <type_traits>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -334,15 +335,18 @@ static KernelChoice choice_of(const compas_b200_parm* p) {
     k.precision = p->precision;
     k.thinc = p->thinc;
     k.phase_field = 0;
+    k.shape = 0;
     return k;
 }
 
-static int launch_stage(const compas_b200_parm* p, const StageArgs& a, cudaStream_t st, int phase_field = 0) {
+static int launch_stage(const compas_b200_parm* p, const StageArgs& a, cudaStream_t st, int phase_field = 0,
+                        int shape = 0) {
     const int ts = (p->dim == 2) ? kTile2 : kTile3;
     const long long tiles = (long long)((a.g.n[0] + ts - 1) / ts) * ((a.g.n[1] + ts - 1) / ts) *
                             ((a.g.n[2] + (p->dim == 2 ? 1 : ts) - 1) / (p->dim == 2 ? 1 : ts));
     if (tiles > 0x7fffffffLL) return fail(COMPAS_B200_EARG, "box too large");
     KernelChoice k = choice_of(p);
+    k.shape = shape;
     if (phase_field) {
         k.thinc = 0;
         k.phase_field = 1;
@@ -358,12 +362,13 @@ static int launch_stage(const compas_b200_parm* p, const StageArgs& a, cudaStrea
 }
 
 static int launch_list(int physics, int dim, int nphase, int limiter, int precision, const ListArgs& L,
-                       cudaStream_t st) {
+                       cudaStream_t st, int shape = 0) {
     KernelChoice k;
     k.limiter = limiter;
     k.precision = precision;
     k.thinc = 0;
     k.phase_field = 0;
+    k.shape = shape;
     cudaError_t e;
     if (physics == COMPAS_B200_FIVEEQS) e = (dim == 2) ? launch_list_fiveeq2(k, L, st) : launch_list_fiveeq3(k, L, st);
     else if (physics == COMPAS_B200_SIXEQS) e = (dim == 2) ? launch_list_sixeq2(k, L, st) : launch_list_sixeq3(k, L, st);
@@ -394,6 +399,90 @@ static int launch_fill(const compas_b200_parm* p, const compas_b200_geom* geo, d
     fill_boundary_kernel<<<(unsigned)blocks, threads, 0, st>>>(b);
     CUDA_TRY(cudaGetLastError());
     return COMPAS_B200_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Autotuner: the launch shape (threads per CTA, CTAs per SM; kern_impl.cuh) and the tile traversal
+// order (tile_coords) of the plain stage kernels, picked per model, precision and box size by timing
+// every candidate on the caller's own data (one RK stage each, CUDA events, after one warm-up
+// launch) the first time a level or batch advances. Every candidate computes the same faces with
+// the same arithmetic, so the choice changes the time, never the result. Choices are cached for the
+// process, keyed by model, scheme, precision, kind (single box / box list) and size.
+// ------------------------------------------------------------------------------------------------
+struct TuneChoice {
+    int shape = 0, order = 0;
+    float ms = 0.f;
+};
+static std::mutex g_tune_mu;
+static std::map<std::string, TuneChoice> g_tune_cache;
+
+static std::string tune_key(const compas_b200_parm* p, const char* kind, long long s0, long long s1, long long s2) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return std::to_string(dev) + "/" + std::to_string(p->physics) + "/" + std::to_string(p->dim) + "/" +
+           std::to_string(p->nphase) + "/" + std::to_string(p->id_limiter) + "/" + std::to_string(p->precision) +
+           "/" + kind + "/" + std::to_string(s0) + "x" + std::to_string(s1) + "x" + std::to_string(s2);
+}
+
+static bool tune_lookup(const std::string& key, TuneChoice* c) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it == g_tune_cache.end()) return false;
+    *c = it->second;
+    return true;
+}
+
+static void tune_store(const std::string& key, const TuneChoice& c) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_cache[key] = c;
+}
+
+// Times launch(shape, order) for every candidate (one warm-up, then `reps` timed launches) on st and
+// returns the fastest. Synchronises st.
+template <class F>
+static int tune_candidates(F&& launch, cudaStream_t st, int reps, TuneChoice* best) {
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(COMPAS_B200_ECUDA, "event create");
+    }
+    int rc = COMPAS_B200_OK;
+    best->ms = 3.0e38f;
+    for (int sh = 0; sh < kShapes && !rc; ++sh)
+        for (int od = 0; od < kOrders && !rc; ++od) {
+            if ((rc = launch(sh, od))) break;
+            cudaEventRecord(e0, st);
+            for (int r = 0; r < reps && !rc; ++r) rc = launch(sh, od);
+            cudaEventRecord(e1, st);
+            if (rc) break;
+            cudaError_t e = cudaEventSynchronize(e1);
+            float ms = 0.f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (e != cudaSuccess) {
+                rc = fail(COMPAS_B200_ECUDA, std::string("autotune timing: ") + cudaGetErrorString(e));
+                break;
+            }
+            ms /= reps;
+            if (ms < best->ms) {
+                best->shape = sh;
+                best->order = od;
+                best->ms = ms;
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
+
+// The tuned launch shape / tile order of a single box of this size, if a level has tuned it in this
+// process (the drop-in entry points reuse it; they never time anything themselves).
+static int cached_shape(const compas_b200_parm* p, const compas_b200_geom* g, StageArgs& a) {
+    if (!p->autotune) return 0;
+    TuneChoice c;
+    if (!tune_lookup(tune_key(p, "box", g->n[0], g->n[1], p->dim == 3 ? g->n[2] : 1), &c)) return 0;
+    a.order = c.order;
+    return c.shape;
 }
 
 static StageArgs base_args(const compas_b200_parm* p, const compas_b200_geom* g) {
@@ -470,6 +559,8 @@ struct compas_b200_level {
     compas::PfLevel* pf = nullptr;  // Phase-Field work arrays (PhaseField.phase_field = 1)
     long long pf_substeps = 0;
     compas::PfInfo pf_last{};       // counters of the last Phase-Field step
+    int shape = 0, order = 0;       // stage-kernel launch shape and tile order (autotuner or forced)
+    bool tuned = false, forced = false;
 };
 
 namespace compas {
@@ -562,6 +653,7 @@ int compas_b200_parm_init_nphase(compas_b200_parm* p, int physics, int dim, int 
     p->pf_cfl = 0.4;
     p->pf_max_step = 1000000;
     p->pf_tol_rel = 1.0e-10;
+    p->autotune = 1;
     if (physics != COMPAS_B200_FIVEEQS && physics != COMPAS_B200_SIXEQS && physics != COMPAS_B200_FIVEEQS_NPHASE)
         return fail(COMPAS_B200_EARG, "physics must be FIVEEQS (555), SIXEQS (666) or FIVEEQS_NPHASE (55501)");
     if (dim != 2 && dim != 3) return fail(COMPAS_B200_EARG, "dim must be 2 or 3");
@@ -685,6 +777,12 @@ int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value
             *dk.dst = x;
             return 0;
         }
+    if (k == "compas_b200.autotune") {
+        // this engine's own key: pick the stage kernel's launch shape and tile order by timing
+        if (!parse_int(value, &ix) || ix < 0 || ix > 1) return bad("0, 1");
+        p->autotune = ix;
+        return 0;
+    }
     if (k == "compas_b200.precision") {
         // this engine's own key (no reference counterpart): the arithmetic of the bulk of the RHS
         if (v == "fp64") { p->precision = 0; return 0; }
@@ -818,7 +916,8 @@ int compas_b200_compute_dUdt(const compas_b200_parm* p, const compas_b200_geom* 
     a.mode = kModeDudt;
     a.cmax = reinterpret_cast<unsigned long long*>(cmax_dev);
     a.err = err_dev;
-    return launch_stage(p, a, (cudaStream_t)stream);
+    const int shape = cached_shape(p, g, a);
+    return launch_stage(p, a, (cudaStream_t)stream, 0, shape);
 }
 
 int compas_b200_rk3_stage(const compas_b200_parm* p, const compas_b200_geom* g, int stage, const double* Us,
@@ -838,7 +937,8 @@ int compas_b200_rk3_stage(const compas_b200_parm* p, const compas_b200_geom* g, 
     a.dt = dt_dev;
     a.cmax = reinterpret_cast<unsigned long long*>(cmax_dev);
     a.err = err_dev;
-    return launch_stage(p, a, (cudaStream_t)stream);
+    const int shape = cached_shape(p, g, a);
+    return launch_stage(p, a, (cudaStream_t)stream, 0, shape);
 }
 
 int compas_b200_pf_compute_dUdt(const compas_b200_parm* p, const compas_b200_geom* g, const double* U, double* dUdt,
@@ -1082,6 +1182,44 @@ int compas_b200_level_download(compas_b200_level* lv, double* dst, int is_device
     return COMPAS_B200_OK;
 }
 
+// Autotune the level's stage kernel on its own state (ghosts filled): a stage-0 launch with dt = 0
+// into the stage buffer U1 per candidate, wave speeds and status into a scratch block.
+static int tune_level(compas_b200_level* lv, cudaStream_t st) {
+    const std::string key = tune_key(&lv->p, "box", lv->g.n[0], lv->g.n[1], lv->p.dim == 3 ? lv->g.n[2] : 1);
+    TuneChoice c;
+    if (!tune_lookup(key, &c)) {
+        double* scratch = nullptr;
+        CUDA_TRY(cudaMalloc(&scratch, 64));
+        cudaError_t e = cudaMemsetAsync(scratch, 0, 64, st);
+        if (e != cudaSuccess) {
+            cudaFree(scratch);
+            return fail(COMPAS_B200_ECUDA, std::string("autotune scratch: ") + cudaGetErrorString(e));
+        }
+        StageArgs a = base_args(&lv->p, &lv->g);
+        a.mode = kModeStage;
+        a.stage = 0;
+        a.Us = lv->U;
+        a.U0 = lv->U;
+        a.Uout = lv->U1;
+        a.dt = scratch;
+        a.cmax = reinterpret_cast<unsigned long long*>(scratch + 1);
+        a.err = reinterpret_cast<unsigned int*>(scratch + 2);
+        auto launch = [&](int sh, int od) {
+            a.order = od;
+            return launch_stage(&lv->p, a, st, 0, sh);
+        };
+        const int rc = tune_candidates(launch, st, 2, &c);
+        cudaStreamSynchronize(st);
+        cudaFree(scratch);
+        if (rc) return rc;
+        tune_store(key, c);
+    }
+    lv->shape = c.shape;
+    lv->order = c.order;
+    lv->tuned = true;
+    return COMPAS_B200_OK;
+}
+
 // The launches of one coarse step: ComputeDt, then three (fill, stage) pairs, then t += dt.
 static int enqueue_step(compas_b200_level* lv, cudaStream_t st) {
     const compas_b200_parm* p = &lv->p;
@@ -1106,13 +1244,14 @@ static int enqueue_step(compas_b200_level* lv, cudaStream_t st) {
     double* bufs_in[3] = {lv->U, lv->U1, lv->U2};
     double* bufs_out[3] = {lv->U1, lv->U2, lv->U};
     int rc;
+    a.order = lv->order;
     for (int s = 0; s < 3; ++s) {
         if ((rc = launch_fill(p, g, bufs_in[s], st))) return rc;
         a.stage = s;
         a.Us = bufs_in[s];
         a.U0 = lv->U;
         a.Uout = bufs_out[s];
-        if ((rc = launch_stage(p, a, st))) return rc;
+        if ((rc = launch_stage(p, a, st, 0, lv->shape))) return rc;
     }
     step_end_kernel<<<1, 1, 0, st>>>(lv->ctl);
     CUDA_TRY(cudaGetLastError());
@@ -1140,6 +1279,13 @@ int compas_b200_level_advance(compas_b200_level* lv, int nsteps, double stop_tim
         lv->need_init = false;
     }
     if (nsteps == 0) return COMPAS_B200_OK;
+    if (lv->p.autotune && !lv->tuned && !lv->forced && !lv->p.thinc) {
+        if ((rc = tune_level(lv, st))) return rc;
+        if (lv->graph) {
+            cudaGraphExecDestroy(lv->graph);
+            lv->graph = nullptr;
+        }
+    }
     if (lv->pf) {
         // Evolve (source/Class_Compressible_PhaseField.cpp:171-330): each hyperbolic step is followed by
         // a Phase-Field step of the same dt; its host loop reads dt, max|u| and max|grad Q|.
@@ -1194,6 +1340,28 @@ int compas_b200_level_advance(compas_b200_level* lv, int nsteps, double stop_tim
             if ((rc = enqueue_step(lv, st))) return rc;
     }
     lv->launches += 8LL * nsteps;
+    return COMPAS_B200_OK;
+}
+
+int compas_b200_level_kernel(const compas_b200_level* lv, int* shape, int* order) {
+    if (!lv) return fail(COMPAS_B200_EARG, "null level");
+    if (shape) *shape = lv->shape;
+    if (order) *order = lv->order;
+    return COMPAS_B200_OK;
+}
+
+int compas_b200_level_set_kernel(compas_b200_level* lv, int shape, int order) {
+    if (!lv) return fail(COMPAS_B200_EARG, "null level");
+    if (shape < 0 || shape >= kShapes || order < 0 || order >= kOrders)
+        return fail(COMPAS_B200_EARG, "shape in [0, " + std::to_string(kShapes) + "), order in [0, " +
+                                          std::to_string(kOrders) + ")");
+    lv->shape = shape;
+    lv->order = order;
+    lv->forced = true;
+    if (lv->graph) {
+        cudaGraphExecDestroy(lv->graph);
+        lv->graph = nullptr;
+    }
     return COMPAS_B200_OK;
 }
 
@@ -1402,6 +1570,32 @@ int compas_b200_batch_remove(compas_b200_batch* b, int case_id, void* stream) {
     return fail(COMPAS_B200_EARG, "no case with id " + std::to_string(case_id));
 }
 
+// Autotune the batch's box-list kernel on the cases admitted so far (all at t = 0 when the batch first
+// advances): a stage-0 launch per candidate with each case's dt still 0, into each case's stage
+// buffer; the wave speeds it adds equal the t = 0 pass's, so the step control is unchanged.
+static int tune_batch(compas_b200_batch* b, cudaStream_t st) {
+    long long tiles = 0;
+    for (auto& c : b->cases) tiles += tile_count(b->dim, make_grid(&c.p, &c.g));
+    long long tb = 1, nb = 1;
+    while (tb < tiles) tb <<= 1;
+    while (nb < (long long)b->cases.size()) nb <<= 1;
+    const std::string key = tune_key(&b->cases[0].p, "list", tb, nb, 0);
+    TuneChoice c;
+    if (!tune_lookup(key, &c)) {
+        auto launch = [&](int sh, int od) {
+            ListArgs L{b->d_boxes, b->d_nbox, b->d_tile_off, kModeStage, 0, od};
+            return launch_list(b->physics, b->dim, b->nphase, b->limiter, b->precision, L, st, sh);
+        };
+        int rc = tune_candidates(launch, st, 2, &c);
+        if (rc) return rc;
+        tune_store(key, c);
+    }
+    b->shape = c.shape;
+    b->order = c.order;
+    b->tuned = true;
+    return COMPAS_B200_OK;
+}
+
 static int batch_enqueue_step(compas_b200_batch* b, cudaStream_t st) {
     step_begin_list_kernel<<<4, 256, 0, st>>>(b->d_ctl, b->d_cs, b->d_slots, b->d_nbox);
     CUDA_TRY(cudaGetLastError());
@@ -1411,8 +1605,8 @@ static int batch_enqueue_step(compas_b200_batch* b, cudaStream_t st) {
         FillListArgs F{b->d_boxes, b->d_nbox, b->d_ghost_off, N, b->dim, mom0_of(b->physics, b->nphase), s};
         fill_list_kernel<<<148 * 8, 256, 0, st>>>(F);
         CUDA_TRY(cudaGetLastError());
-        ListArgs L{b->d_boxes, b->d_nbox, b->d_tile_off, kModeStage, s};
-        if ((rc = launch_list(b->physics, b->dim, b->nphase, b->limiter, b->precision, L, st))) return rc;
+        ListArgs L{b->d_boxes, b->d_nbox, b->d_tile_off, kModeStage, s, b->order};
+        if ((rc = launch_list(b->physics, b->dim, b->nphase, b->limiter, b->precision, L, st, b->shape))) return rc;
     }
     step_end_list_kernel<<<4, 256, 0, st>>>(b->d_ctl, b->d_slots, b->d_nbox);
     CUDA_TRY(cudaGetLastError());
@@ -1424,6 +1618,13 @@ int compas_b200_batch_advance(compas_b200_batch* b, int nsteps, int use_graph, v
     if (nsteps < 0) return fail(COMPAS_B200_EARG, "nsteps must be >= 0");
     cudaStream_t st = (cudaStream_t)stream;
     int rc;
+    if (!b->tuned && !b->forced && !b->cases.empty() && b->cases[0].p.autotune && nsteps > 0) {
+        if ((rc = tune_batch(b, st))) return rc;
+        if (b->graph) {
+            cudaGraphExecDestroy(b->graph);
+            b->graph = nullptr;
+        }
+    }
     if (use_graph) {
         if (!b->graph || b->graph_stream != st) {
             if (b->graph) {
@@ -1454,6 +1655,28 @@ int compas_b200_batch_advance(compas_b200_batch* b, int nsteps, int use_graph, v
             if ((rc = batch_enqueue_step(b, st))) return rc;
     }
     b->launches += 8LL * nsteps;
+    return COMPAS_B200_OK;
+}
+
+int compas_b200_batch_kernel(const compas_b200_batch* b, int* shape, int* order) {
+    if (!b) return fail(COMPAS_B200_EARG, "null batch");
+    if (shape) *shape = b->shape;
+    if (order) *order = b->order;
+    return COMPAS_B200_OK;
+}
+
+int compas_b200_batch_set_kernel(compas_b200_batch* b, int shape, int order) {
+    if (!b) return fail(COMPAS_B200_EARG, "null batch");
+    if (shape < 0 || shape >= kShapes || order < 0 || order >= kOrders)
+        return fail(COMPAS_B200_EARG, "shape in [0, " + std::to_string(kShapes) + "), order in [0, " +
+                                          std::to_string(kOrders) + ")");
+    b->shape = shape;
+    b->order = order;
+    b->forced = true;
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
     return COMPAS_B200_OK;
 }
 

@@ -8,36 +8,35 @@
 #include "launch.h"
 #include "stage_kernel.cuh"
 
-// Launch shape of the stage kernel: threads per CTA and CTAs per SM of the 3D (8^3 tile) and 2D
-// (16^2 tile) kernels. The register budget is set per SM sub-partition (16384 registers each, warps
-// dealt round-robin), so a CTA of 6 warps at 2 CTAs/SM gets 168 registers per thread.
-#ifndef COMPAS_NT3
-#define COMPAS_NT3 192
-#endif
-#ifndef COMPAS_MINB3
-#define COMPAS_MINB3 2
-#endif
-#ifndef COMPAS_NT2
-#define COMPAS_NT2 272
-#endif
-#ifndef COMPAS_MINB2
-#define COMPAS_MINB2 2
-#endif
-
 namespace compas {
 
-template <class M>
+// Launch shapes of the stage kernel (threads per CTA, CTAs per SM) among which the autotuner picks;
+// the tile is 8^3 in 3D and 16^2 in 2D for every shape. The register budget is set per SM
+// sub-partition (16384 registers each, warps dealt round-robin): in 3D, 6 warps at 2 CTAs/SM get
+// 168 registers per thread, 8 warps 128, 9 warps 112; in 2D, 272 threads at 2 CTAs/SM get 96, at 1
+// CTA/SM 232, 136 threads at 4 CTAs/SM 120. Every shape covers the 576 (3D) or 272 (2D) faces of a
+// direction in whole rounds or nearly so. Shape 0 is the default when tuning is off.
+template <int D, int S>
+struct ShapeParams;
+template <> struct ShapeParams<3, 0> { static constexpr int NT = 192, MINB = 2; };
+template <> struct ShapeParams<3, 1> { static constexpr int NT = 256, MINB = 2; };
+template <> struct ShapeParams<3, 2> { static constexpr int NT = 288, MINB = 2; };
+template <> struct ShapeParams<2, 0> { static constexpr int NT = 272, MINB = 2; };
+template <> struct ShapeParams<2, 1> { static constexpr int NT = 272, MINB = 1; };
+template <> struct ShapeParams<2, 2> { static constexpr int NT = 136, MINB = 4; };
+
+template <class M, int S = 0>
 struct LaunchShape {
     static constexpr int TS = (M::D == 2) ? kTile2 : kTile3;
     static constexpr int TZ = (M::D == 2) ? 1 : TS;
-    static constexpr int NT = (M::D == 2) ? COMPAS_NT2 : COMPAS_NT3;
-    static constexpr int MINB = (M::D == 2) ? COMPAS_MINB2 : COMPAS_MINB3;
+    static constexpr int NT = ShapeParams<M::D, S>::NT;
+    static constexpr int MINB = ShapeParams<M::D, S>::MINB;
 };
 
 // One CTA per tile of the box.
-template <class M, int SCHEME, bool MIX, int VAR>
+template <class M, int SCHEME, bool MIX, int VAR, int SH>
 static cudaError_t launch_stage_v(const StageArgs& a, cudaStream_t st) {
-    using S = LaunchShape<M>;
+    using S = LaunchShape<M, SH>;
     using T = TileShape<M, S::TS, S::TS, S::TZ, typename std::conditional<MIX, float, double>::type>;
     auto kern = stage_kernel<M, SCHEME, MIX, VAR, S::TS, S::TS, S::TZ, S::NT, S::MINB>;
     static bool attr_set = false;
@@ -57,14 +56,18 @@ static cudaError_t launch_stage_var(const KernelChoice& k, const StageArgs& a, c
     if constexpr (M::KIND == kModelFiveN) {
         // FIVEEQS_NPHASE: the plain hyperbolic right-hand side only
         if (k.phase_field || k.thinc) return cudaErrorNotSupported;
-        return launch_stage_v<M, SCHEME, MIX, kVarPlain>(a, st);
     } else {
+        // the THINC and Phase-Field variants run at shape 0
         if (k.phase_field) {
-            if constexpr (M::KIND == kModelFive) return launch_stage_v<M, SCHEME, MIX, kVarPhaseField>(a, st);
+            if constexpr (M::KIND == kModelFive) return launch_stage_v<M, SCHEME, MIX, kVarPhaseField, 0>(a, st);
             else return cudaErrorNotSupported;
         }
-        if (k.thinc) return launch_stage_v<M, SCHEME, MIX, kVarThinc>(a, st);
-        return launch_stage_v<M, SCHEME, MIX, kVarPlain>(a, st);
+        if (k.thinc) return launch_stage_v<M, SCHEME, MIX, kVarThinc, 0>(a, st);
+    }
+    switch (k.shape) {
+        case 1: return launch_stage_v<M, SCHEME, MIX, kVarPlain, 1>(a, st);
+        case 2: return launch_stage_v<M, SCHEME, MIX, kVarPlain, 2>(a, st);
+        default: return launch_stage_v<M, SCHEME, MIX, kVarPlain, 0>(a, st);
     }
 }
 
@@ -81,9 +84,9 @@ static cudaError_t launch_stage_m(const KernelChoice& k, const StageArgs& a, cud
 }
 
 // Persistent box-list launch: one resident wave of CTAs walks the tiles of every box.
-template <class M, int SCHEME, bool MIX>
+template <class M, int SCHEME, bool MIX, int SH>
 static cudaError_t launch_list_v(const ListArgs& L, cudaStream_t st) {
-    using S = LaunchShape<M>;
+    using S = LaunchShape<M, SH>;
     using T = TileShape<M, S::TS, S::TS, S::TZ, typename std::conditional<MIX, float, double>::type>;
     auto kern = stage_list_kernel<M, SCHEME, MIX, S::TS, S::TS, S::TZ, S::NT, S::MINB>;
     static int grid = 0;
@@ -100,14 +103,24 @@ static cudaError_t launch_list_v(const ListArgs& L, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+template <class M, int SCHEME, bool MIX>
+static cudaError_t launch_list_s(const KernelChoice& k, const ListArgs& L, cudaStream_t st) {
+    switch (k.shape) {
+        case 1: return launch_list_v<M, SCHEME, MIX, 1>(L, st);
+        case 2: return launch_list_v<M, SCHEME, MIX, 2>(L, st);
+        default: return launch_list_v<M, SCHEME, MIX, 0>(L, st);
+    }
+}
+
 template <class M>
 static cudaError_t launch_list_m(const KernelChoice& k, const ListArgs& L, cudaStream_t st) {
     if constexpr (M::KIND == kModelFiveN) {
         if (k.limiter == 6) return cudaErrorNotSupported;
-        return (k.precision == 1) ? launch_list_v<M, 5, true>(L, st) : launch_list_v<M, 5, false>(L, st);
+        return (k.precision == 1) ? launch_list_s<M, 5, true>(k, L, st) : launch_list_s<M, 5, false>(k, L, st);
     } else {
-        if (k.precision == 1) return (k.limiter == 6) ? launch_list_v<M, 6, true>(L, st) : launch_list_v<M, 5, true>(L, st);
-        return (k.limiter == 6) ? launch_list_v<M, 6, false>(L, st) : launch_list_v<M, 5, false>(L, st);
+        if (k.precision == 1)
+            return (k.limiter == 6) ? launch_list_s<M, 6, true>(k, L, st) : launch_list_s<M, 5, true>(k, L, st);
+        return (k.limiter == 6) ? launch_list_s<M, 6, false>(k, L, st) : launch_list_s<M, 5, false>(k, L, st);
     }
 }
 

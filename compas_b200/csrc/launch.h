@@ -19,7 +19,12 @@ struct KernelChoice {
     int precision;
     int thinc;
     int phase_field;
+    int shape;  // launch shape (kern_impl.cuh ShapeParams; 0..kShapes-1), chosen by the autotuner
 };
+
+// Launch shapes compiled per kernel variant, and tile traversal orders (tile_coords).
+constexpr int kShapes = 3;
+constexpr int kOrders = 2;
 
 // Tile side of the stage kernels (cells per direction): 16^2 tiles in 2D, 8^3 in 3D.
 constexpr int kTile2 = 16;

@@ -62,7 +62,35 @@ struct StageArgs {
     double trace;
     Thinc thinc;               // used by the THINC kernels only
     const double* gq[3];       // Phase-Field kernels: face gradients of the potential Q per direction
+    int order;                 // tile traversal order (tile_coords): 0 x fastest, 1 bricks of tiles
 };
+
+// Tile coordinates (in tiles) of the w-th CTA of a box of ntx x nty x ntz tiles. order 0: x fastest.
+// order 1: bricks of BX x BY x BZ tiles (4^3 in 3D, 8^2 in 2D) walked x fastest, tiles inside a
+// brick x fastest, so that the tiles resident at one time are close in every direction and their
+// halo reads hit L2. The mapping is a bijection on [0, ntx*nty*ntz) (edge bricks are smaller).
+__device__ __forceinline__ void tile_coords(int w, int ntx, int nty, int ntz, int order, int D, int& tx, int& ty,
+                                            int& tz) {
+    if (order == 0) {
+        tx = w % ntx;
+        ty = (w / ntx) % nty;
+        tz = w / (ntx * nty);
+        return;
+    }
+    const int BX = (D == 3) ? 4 : 8, BY = BX, BZ = (D == 3) ? 4 : 1;
+    const int gz = w / (BZ * nty * ntx);
+    int r = w - gz * BZ * nty * ntx;
+    const int nz = min(BZ, ntz - gz * BZ);
+    const int gy = r / (BY * nz * ntx);
+    r -= gy * BY * nz * ntx;
+    const int ny = min(BY, nty - gy * BY);
+    const int gx = r / (BX * ny * nz);
+    r -= gx * BX * ny * nz;
+    const int nx = min(BX, ntx - gx * BX);
+    tx = gx * BX + r % nx;
+    ty = gy * BY + (r / nx) % ny;
+    tz = gz * BZ + r / (nx * ny);
+}
 
 // Variants of the stage kernel (the VAR template argument of stage_tile).
 enum { kVarPlain = 0, kVarThinc = 1, kVarPhaseField = 2 };
@@ -129,11 +157,12 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
     const Grid& g = a.g;
     const int ntx = (g.n[0] + TX - 1) / TX;
     const int nty = (g.n[1] + TY - 1) / TY;
-    int b = tile;
-    const int i0 = (b % ntx) * TX;
-    b /= ntx;
-    const int j0 = (b % nty) * TY;
-    const int k0 = (b / nty) * TZ;
+    const int ntz = (g.n[2] + TZ - 1) / TZ;
+    int tix, tiy, tiz;
+    tile_coords(tile, ntx, nty, ntz, a.order, D, tix, tiy, tiz);
+    const int i0 = tix * TX;
+    const int j0 = tiy * TY;
+    const int k0 = tiz * TZ;
     const int tid = threadIdx.x;
     unsigned int* err = a.err;
 
@@ -529,6 +558,7 @@ struct ListArgs {
     const int* tile_off;          // exclusive prefix sums of BoxDesc::tiles, nbox + 1 entries
     int mode;
     int stage;
+    int order;                    // tile traversal order inside each box (tile_coords)
 };
 
 __device__ __forceinline__ int find_box(const int* off, int nb, int w) {
@@ -565,6 +595,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_list_kernel(ListArgs L) {
         a.id_k = B.id_k;
         a.relax = B.relax;
         a.trace = B.trace;
+        a.order = L.order;
         __syncthreads();  // the previous tile's readers of shared memory are done
         stage_tile<M, SCHEME, MIX, kVarPlain, TX, TY, TZ, NT>(a, w - L.tile_off[b], smem_d);
     }

@@ -93,6 +93,10 @@ typedef struct compas_b200_parm {
     double b_k[COMPAS_B200_MAX_PHASES], q_k[COMPAS_B200_MAX_PHASES];
     double Ak[COMPAS_B200_MAX_PHASES], Bk[COMPAS_B200_MAX_PHASES];
     double Ck[COMPAS_B200_MAX_PHASES], Dk[COMPAS_B200_MAX_PHASES];
+    /* compas_b200.autotune (this engine's key, default 1): levels and batches pick the stage kernel's
+     * launch shape and tile traversal order by timing the candidates on their own data the first
+     * time they advance (the result is the same for every candidate) */
+    int autotune;
 } compas_b200_parm;
 
 /* One box covering a single-level domain (the valid cells), its ghost width and its boundary codes
@@ -138,6 +142,9 @@ long long compas_b200_state_bytes(const compas_b200_parm* p, const compas_b200_g
 const char* compas_b200_last_error(void);
 
 /* ---- drop-in kernels on caller-owned device arrays ------------------------------------------- */
+/* With compas_b200.autotune = 1 the stage-kernel entry points below run the launch shape and tile
+ * order that a level of the same model and box size has tuned in this process (they never time
+ * anything themselves); the results do not depend on it. */
 
 /* Ghost cells of U from its valid cells by the boundary codes (single-box domain). Replaces the
  * physical-boundary and periodic part of COMPAS::FillPatch (source/COMPAS.cpp:1629-1732). */
@@ -250,6 +257,12 @@ int compas_b200_level_sync(compas_b200_level* lv, double* t, int* steps, unsigne
 /* Step sizes of the steps taken since upload (up to n values). */
 int compas_b200_level_dts(compas_b200_level* lv, double* dts, int n);
 
+/* The stage kernel's launch shape (0..2: threads per CTA and CTAs per SM) and tile traversal order
+ * (0 x fastest, 1 bricks of tiles) the level runs: the autotuner's choice after the first advance
+ * (compas_b200.autotune = 1), else shape 0 / order 0 or what set_kernel forced. */
+int compas_b200_level_kernel(const compas_b200_level* lv, int* shape, int* order);
+int compas_b200_level_set_kernel(compas_b200_level* lv, int shape, int order);
+
 /* Kernel launches the library enqueued on this level since upload. */
 long long compas_b200_level_launches(compas_b200_level* lv);
 
@@ -284,6 +297,11 @@ int compas_b200_batch_add(compas_b200_batch* b, const compas_b200_parm* p, const
                           const double* U, int is_device, double stop_time, int max_steps, void* stream,
                           int* case_id);
 int compas_b200_batch_remove(compas_b200_batch* b, int case_id, void* stream);
+
+/* The box-list kernel's launch shape and tile order (as compas_b200_level_kernel; a batch is tuned on
+ * the cases it holds at its first advance, when the first case's parm has compas_b200.autotune = 1). */
+int compas_b200_batch_kernel(const compas_b200_batch* b, int* shape, int* order);
+int compas_b200_batch_set_kernel(compas_b200_batch* b, int shape, int order);
 
 /* Enqueue nsteps coarse steps of every active case (no host synchronisation). */
 int compas_b200_batch_advance(compas_b200_batch* b, int nsteps, int use_graph, void* stream);

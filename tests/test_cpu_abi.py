@@ -53,3 +53,10 @@ def test_state_bytes_layout():
     g = cb.make_geom((10, 12, 14), (1, 1, 1), 3)
     assert cb.padded_shape(p, g) == (8, 20, 18, 16)
     assert cb.lib().compas_b200_state_bytes(p, g) == 8 * 20 * 18 * 16 * 8
+
+
+def test_autotune_key():
+    assert cb.make_parm(cb.FIVEEQS, 2).autotune == 1
+    assert cb.make_parm(cb.FIVEEQS, 2, {"compas_b200.autotune": 0}).autotune == 0
+    with pytest.raises(cb.CompasError):
+        cb.make_parm(cb.FIVEEQS, 2, {"compas_b200.autotune": 2})

@@ -108,7 +108,10 @@ struct TileShape {
     static constexpr int CELLS = TX * TY * TZ;
     static constexpr int A0 = TY * TZ, A1 = TX * TZ, A2 = TX * TY;
     static constexpr int AMAX = (D == 3) ? (A0 > A1 ? (A0 > A2 ? A0 : A2) : (A1 > A2 ? A1 : A2)) : (A0 > A1 ? A0 : A1);
-    static constexpr int HALO = 6 * AMAX;
+    // halo slab slot stride: padded by 8 cells in 3D so that the 4 slots a warp touches in one
+    // face round fall in different shared-memory banks
+    static constexpr int HS = (D == 3) ? AMAX + 8 : AMAX;
+    static constexpr int HALO = 6 * HS;
     static constexpr int F0 = (TX + 1) * A0, F1 = (TY + 1) * A1, F2 = (TZ + 1) * A2;
     static constexpr int FMAX = (D == 3) ? (F0 > F1 ? (F0 > F2 ? F0 : F2) : (F1 > F2 ? F1 : F2)) : (F0 > F1 ? F0 : F1);
     static constexpr int NB = M::N + M::NC;
@@ -187,7 +190,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
             dst = lx + TX * (ly + TY * lz);
         } else {
             const int slot = (lx < 0) ? lx + 3 : lx - TX + 3;
-            dst = N * CELLS + slot * T::A0 + (ly + TX * lz);
+            dst = N * CELLS + slot * T::HS + (ly + TX * lz);
         }
         PT* out = (dst < N * CELLS) ? Pint + dst : Phal + (dst - N * CELLS);
         const int stride = (dst < N * CELLS) ? CELLS : HALO;
@@ -225,7 +228,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                 for (int n = 0; n < N; ++n) W[n] = 0;
             }
 #pragma unroll
-            for (int n = 0; n < N; ++n) Phal[n * HALO + h] = W[n];
+            for (int n = 0; n < N; ++n) Phal[n * HALO + slot * T::HS + t] = W[n];
         }
         __syncthreads();
 
@@ -244,11 +247,16 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                 const int t0 = f / EF;
                 ta = t0 % TS;
                 tb = t0 / TS;
-            } else {
+            } else if (d == 1) {
                 ta = f % TS;
                 const int r0 = f / TS;
                 fd = r0 % EF;
                 tb = r0 / EF;
+            } else {
+                // z faces: x, then y, then the face position, so that a warp reads one z plane
+                ta = f % TS;
+                tb = (f / TS) % TS;
+                fd = f / (TS * TS);
             }
             int fx, fy, fz;
             if (d == 0) { fx = fd; fy = ta; fz = tb; }
@@ -271,7 +279,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                     str[s] = CELLS;
                 } else {
                     const int slot = (pos < 0) ? pos + 3 : pos - TS + 3;
-                    off[s] = N * CELLS + slot * T::A0 + t;
+                    off[s] = N * CELLS + slot * T::HS + t;
                     str[s] = HALO;
                 }
             }
@@ -395,7 +403,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                 int fl, fh;
                 if (d == 0) { fl = lx + EF * (ly + TS * lz); fh = fl + 1; }
                 else if (d == 1) { fl = lx + TS * (ly + EF * lz); fh = fl + TS; }
-                else { fl = lx + TS * (lz + EF * ly); fh = fl + TS; }
+                else { fl = lx + TS * (ly + TS * lz); fh = fl + TS * TS; }
 #pragma unroll
                 for (int c = 0; c < NB; ++c) {
                     const double df = Fb[c * FMAX + fh] - Fb[c * FMAX + fl];
@@ -404,7 +412,9 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                 }
             }
         }
-        __syncthreads();
+        // no barrier here: the next direction's halo pass writes only the halo slabs, which this
+        // direction's faces finished reading before the barrier above, and its faces overwrite the
+        // face buffer only after the barrier that follows that halo pass
     }
 
     // 3. epilogue

@@ -521,6 +521,94 @@ __global__ void k_mg_jacobi_t(MgLevel L) {
 constexpr int kRowThreads = 128;
 dim3 mg_grid(const PfDims& m) { return dim3((unsigned)((m.n[0] + kRowThreads - 1) / kRowThreads), (unsigned)m.n[1], (unsigned)m.n[2]); }
 
+// Two red-black Gauss-Seidel sweeps (four colour passes) of a 2D level in ONE launch, by temporal
+// blocking: each CTA loads its kRbTX x kRbTY tile with a halo of kRbH = 4 cells (x, b, 1/diag and
+// the four face coefficients beta_f / h^2 of every cell, periodic sides wrapped) into shared memory
+// and runs the passes there; pass p updates the cells of its colour within kRbH - 1 - p rings of
+// the tile, so after the fourth pass the tile holds exactly what four global passes give (a
+// colour's update reads only the other colour), and only the tile is written back. This replaces
+// four launches and four passes over the level by one.
+constexpr int kRbTX = 32, kRbTY = 16, kRbH = 4, kRbPasses = kRbH;
+constexpr int kRbW = kRbTX + 2 * kRbH, kRbHt = kRbTY + 2 * kRbH, kRbCells = kRbW * kRbHt;
+constexpr int kRbThreads = 256;
+constexpr size_t kRbSmem = sizeof(double) * 7 * (size_t)kRbCells + sizeof(unsigned char) * kRbCells;
+
+__global__ void __launch_bounds__(kRbThreads) k_mg_rb4_2d(MgLevel L, int first_color) {
+    extern __shared__ double rbs[];
+    double* sx = rbs;
+    double* sb = sx + kRbCells;
+    double* sd = sb + kRbCells;
+    double* cw = sd + kRbCells;  // coefficient of the -x neighbour (beta of the cell's low x face / h^2)
+    double* ce = cw + kRbCells;
+    double* cs = ce + kRbCells;
+    double* cn = cs + kRbCells;
+    unsigned char* flag = reinterpret_cast<unsigned char*>(cn + kRbCells);  // bit0 in domain, bits1-4 nb valid, bit5 colour
+    const PfDims& m = L.m;
+    const int n0 = m.n[0], n1 = m.n[1];
+    const int i0 = blockIdx.x * kRbTX - kRbH, j0 = blockIdx.y * kRbTY - kRbH;
+    const double ih0 = L.ih2[0], ih1 = L.ih2[1];
+    for (int c = threadIdx.x; c < kRbCells; c += kRbThreads) {
+        const int lx = c % kRbW, ly = c / kRbW;
+        int i = i0 + lx, j = j0 + ly;
+        bool in = true;
+        // periodic sides wrap (as often as the tile and its halo need); a cell beyond a
+        // non-periodic side is left out
+        if (i < 0 || i >= n0) {
+            if (m.periodic[0]) i = ((i % n0) + n0) % n0;
+            else in = false;
+        }
+        if (j < 0 || j >= n1) {
+            if (m.periodic[1]) j = ((j % n1) + n1) % n1;
+            else in = false;
+        }
+        unsigned char f = 0;
+        if (in) {
+            const int q = i + n0 * j;
+            sx[c] = L.x[q];
+            sb[c] = L.b[q];
+            sd[c] = L.idiag[q];
+            const int fx = n0 + 1;
+            f = 1;
+            if (i > 0 || m.periodic[0]) f |= 2;
+            if (i < n0 - 1 || m.periodic[0]) f |= 4;
+            if (j > 0 || m.periodic[1]) f |= 8;
+            if (j < n1 - 1 || m.periodic[1]) f |= 16;
+            if ((i + j) & 1) f |= 32;
+            cw[c] = L.beta[0][i + fx * j] * ih0;
+            ce[c] = L.beta[0][(i + 1) + fx * j] * ih0;
+            cs[c] = L.beta[1][i + n0 * j] * ih1;
+            cn[c] = L.beta[1][i + n0 * (j + 1)] * ih1;
+        }
+        flag[c] = f;
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int p = 0; p < kRbPasses; ++p) {
+        const int color = first_color ^ (p & 1);
+        const int reach = kRbH - 1 - p;  // rings of the tile this pass updates
+        for (int c = threadIdx.x; c < kRbCells; c += kRbThreads) {
+            const int lx = c % kRbW - kRbH, ly = c / kRbW - kRbH;
+            const int rx = lx < 0 ? -lx : (lx >= kRbTX ? lx - kRbTX + 1 : 0);
+            const int ry = ly < 0 ? -ly : (ly >= kRbTY ? ly - kRbTY + 1 : 0);
+            const unsigned char f = flag[c];
+            if ((rx > ry ? rx : ry) > reach || !(f & 1) || ((f >> 5) & 1) != color) continue;
+            // the neighbours in mg_off_t's order: -x, +x, -y, +y
+            double off = 0.0;
+            if (f & 2) off += cw[c] * sx[c - 1];
+            if (f & 4) off += ce[c] * sx[c + 1];
+            if (f & 8) off += cs[c] * sx[c - kRbW];
+            if (f & 16) off += cn[c] * sx[c + kRbW];
+            sx[c] = (sb[c] + off) * sd[c];
+        }
+        __syncthreads();
+    }
+    for (int c = threadIdx.x; c < kRbTX * kRbTY; c += kRbThreads) {
+        const int lx = c % kRbTX, ly = c / kRbTX;
+        const int i = blockIdx.x * kRbTX + lx, j = blockIdx.y * kRbTY + ly;
+        if (i < n0 && j < n1) L.x[i + n0 * j] = sx[(lx + kRbH) + kRbW * (ly + kRbH)];
+    }
+}
+
 __global__ void k_mg_idiag(MgLevel L) {
     const PfDims& m = L.m;
     GRID_STRIDE(q, m.nv) {
@@ -635,12 +723,41 @@ __global__ void k_mg_coarse(MgLevel L, int sweeps) {
 // with block barriers between the steps.
 constexpr int kBlockCells = 4096;
 constexpr int kBlockThreads = 1024;
+constexpr size_t kBlockSmemMax = 200 * 1024;  // shared memory of the single-block cycle
+
+// One red-black colour pass of a 2D level with an even number of columns: each thread takes cells of
+// the colour only (the t-th cell of the colour in row-major order), and the neighbour sum is written
+// out in mg_off's order (-x, +x, -y, +y) with its boundary rules, so the values are mg_off's.
+__device__ void blk_rb_pass_2d(const MgLevel& L, int color) {
+    const PfDims& m = L.m;
+    const int n0 = m.n[0], n1 = m.n[1], hw = n0 / 2;
+    const int ncol = hw * n1;
+    const double ih0 = L.ih2[0], ih1 = L.ih2[1];
+    const bool p0 = m.periodic[0], p1 = m.periodic[1];
+    for (int t = threadIdx.x; t < ncol; t += blockDim.x) {
+        const int j = t / hw;
+        const int i = 2 * (t - j * hw) + ((j + color) & 1);
+        const int q = i + n0 * j;
+        double off = 0.0;
+        if (i > 0 || p0) off += (L.beta[0][i + (n0 + 1) * j] * ih0) * L.x[i > 0 ? q - 1 : q + n0 - 1];
+        if (i < n0 - 1 || p0) off += (L.beta[0][(i + 1) + (n0 + 1) * j] * ih0) * L.x[i < n0 - 1 ? q + 1 : q - n0 + 1];
+        if (j > 0 || p1) off += (L.beta[1][i + n0 * j] * ih1) * L.x[j > 0 ? q - n0 : q + n0 * (n1 - 1)];
+        if (j < n1 - 1 || p1) off += (L.beta[1][i + n0 * (j + 1)] * ih1) * L.x[j < n1 - 1 ? q + n0 : q - n0 * (n1 - 1)];
+        L.x[q] = (L.b[q] + off) * L.idiag[q];
+    }
+}
 
 __device__ void blk_smooth(const MgLevel& L, int sweeps, bool reverse) {
     const PfDims& m = L.m;
     const int n = (int)m.nv;
+    const bool fast2d = (m.D == 2 && L.rb && (m.n[0] % 2) == 0);
     for (int s = 0; s < sweeps; ++s) {
-        if (L.rb) {
+        if (fast2d) {
+            for (int c = 0; c < 2; ++c) {
+                blk_rb_pass_2d(L, reverse ? 1 - c : c);
+                __syncthreads();
+            }
+        } else if (L.rb) {
             for (int c = 0; c < 2; ++c) {
                 const int color = reverse ? 1 - c : c;
                 for (int q = threadIdx.x; q < n; q += blockDim.x) {
@@ -664,11 +781,55 @@ __device__ void blk_smooth(const MgLevel& L, int sweeps, bool reverse) {
     }
 }
 
+// Shared memory of the single-block cycle over levels l0 .. nl-1: x, b, r, 1/diag and the face
+// coefficients of every level.
+__host__ __device__ inline long long block_cycle_doubles(const PfDims& m) {
+    long long s = 4 * m.nv;
+    for (int d = 0; d < m.D; ++d) s += m.nf[d];
+    return s;
+}
+
+// The whole cycle runs in shared memory: every level's x, b, r, 1/diag and face coefficients (the
+// last two copied in at the start, constant during a solve), level l0's x and b read at the start
+// and its x written back at the end. Every step is the same arithmetic as the global-memory form,
+// so the result is the same.
 __global__ void __launch_bounds__(kBlockThreads) k_mg_vcycle_block(const MgLevel* levels, int l0, int nl) {
+    extern __shared__ double bsm[];
+    __shared__ MgLevel sl[kMaxLevels];
+    if (threadIdx.x == 0) {
+        long long off = 0;
+        for (int l = l0; l < nl; ++l) {
+            MgLevel L = levels[l];
+            const long long n = L.m.nv;
+            L.x = bsm + off;
+            L.b = bsm + off + n;
+            L.r = bsm + off + 2 * n;
+            L.idiag = bsm + off + 3 * n;
+            off += 4 * n;
+            for (int d = 0; d < L.m.D; ++d) {
+                L.beta[d] = bsm + off;
+                off += L.m.nf[d];
+            }
+            sl[l] = L;
+        }
+    }
+    __syncthreads();
+    for (int l = l0; l < nl; ++l) {
+        const MgLevel& G = levels[l];
+        const MgLevel& L = sl[l];
+        for (int q = threadIdx.x; q < (int)G.m.nv; q += blockDim.x) L.idiag[q] = G.idiag[q];
+        for (int d = 0; d < G.m.D; ++d)
+            for (int q = threadIdx.x; q < (int)G.m.nf[d]; q += blockDim.x) L.beta[d][q] = G.beta[d][q];
+    }
+    for (int q = threadIdx.x; q < (int)levels[l0].m.nv; q += blockDim.x) {
+        sl[l0].x[q] = levels[l0].x[q];
+        sl[l0].b[q] = levels[l0].b[q];
+    }
+    __syncthreads();
     // down
     for (int l = l0; l < nl - 1; ++l) {
-        const MgLevel& L = levels[l];
-        const MgLevel& C = levels[l + 1];
+        const MgLevel& L = sl[l];
+        const MgLevel& C = sl[l + 1];
         blk_smooth(L, 2, false);
         const PfDims& m = L.m;
         for (int q = threadIdx.x; q < (int)m.nv; q += blockDim.x) {
@@ -694,7 +855,7 @@ __global__ void __launch_bounds__(kBlockThreads) k_mg_vcycle_block(const MgLevel
     }
     // coarsest: an even number of sweeps alternating the colour order (symmetric)
     {
-        const MgLevel& L = levels[nl - 1];
+        const MgLevel& L = sl[nl - 1];
         for (int s = 0; s < 8; ++s) {
             blk_smooth(L, 1, false);
             blk_smooth(L, 1, true);
@@ -702,8 +863,8 @@ __global__ void __launch_bounds__(kBlockThreads) k_mg_vcycle_block(const MgLevel
     }
     // up
     for (int l = nl - 2; l >= l0; --l) {
-        const MgLevel& L = levels[l];
-        const MgLevel& C = levels[l + 1];
+        const MgLevel& L = sl[l];
+        const MgLevel& C = sl[l + 1];
         const PfDims& m = L.m;
         const PfDims& c = C.m;
         for (int q = threadIdx.x; q < (int)m.nv; q += blockDim.x) {
@@ -714,6 +875,7 @@ __global__ void __launch_bounds__(kBlockThreads) k_mg_vcycle_block(const MgLevel
         __syncthreads();
         blk_smooth(L, 2, true);
     }
+    for (int q = threadIdx.x; q < (int)levels[l0].m.nv; q += blockDim.x) levels[l0].x[q] = sl[l0].x[q];
 }
 
 // one reduced sum (the first of block_sum2's pair) into *out
@@ -784,6 +946,7 @@ struct PfLevel {
     std::vector<MgLevel> mg;
     MgLevel* mg_dev = nullptr;               // the level descriptors on the device (block V-cycle)
     int mg_block0 = -1;                      // first level of the single-block coarse cycle
+    size_t mg_block_smem = 0;                // its shared memory: x, b, r of every level it covers
     double *z = nullptr, *p = nullptr, *Ap = nullptr;
     double* cg = nullptr;                    // device scalars of the conjugate gradients
     double* qsol = nullptr;                  // solution Q, kept as the next step's starting iterate
@@ -834,7 +997,19 @@ cudaError_t vcycle(PfLevel* pf, int l, cudaStream_t st) {
     const unsigned nbh = blocks_for((long long)L.m.n[1] * L.m.n[2] * ((L.m.n[0] + 1) / 2));
     const dim3 gg = mg_grid(L.m);
     const bool d3 = (L.m.D == 3);
+    // 2D levels of at least 2 halo widths per side: two sweeps per temporally blocked launch
+    const bool fused = !d3 && L.rb && L.m.n[0] >= 2 * kRbH && L.m.n[1] >= 2 * kRbH;
     auto smooth = [&](int sweeps, bool reverse) {
+        if (fused && sweeps == 2) {
+            static bool attr = false;
+            if (!attr) {
+                cudaFuncSetAttribute(k_mg_rb4_2d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRbSmem);
+                attr = true;
+            }
+            const dim3 grid((unsigned)((L.m.n[0] + kRbTX - 1) / kRbTX), (unsigned)((L.m.n[1] + kRbTY - 1) / kRbTY));
+            k_mg_rb4_2d<<<grid, kRbThreads, kRbSmem, st>>>(L, reverse ? 1 : 0);
+            return;
+        }
         for (int s = 0; s < sweeps; ++s) {
             if (L.rb) {
                 for (int c = 0; c < 2; ++c) {
@@ -851,7 +1026,12 @@ cudaError_t vcycle(PfLevel* pf, int l, cudaStream_t st) {
     };
     (void)nbh;
     if (l == pf->mg_block0) {
-        k_mg_vcycle_block<<<1, kBlockThreads, 0, st>>>(pf->mg_dev, l, (int)pf->mg.size());
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_mg_vcycle_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBlockSmemMax);
+            attr = true;
+        }
+        k_mg_vcycle_block<<<1, kBlockThreads, pf->mg_block_smem, st>>>(pf->mg_dev, l, (int)pf->mg.size());
         return cudaGetLastError();
     }
     if (l + 1 == (int)pf->mg.size()) {
@@ -926,11 +1106,17 @@ int pf_create(const compas_b200_parm* p, const compas_b200_geom* g, PfLevel** ou
         double dc[3] = {2 * lm.dx[0], 2 * lm.dx[1], lm.D == 3 ? 2 * lm.dx[2] : 1.0};
         lm = make_dims(lm.D, nc, dc, lm.periodic);
     }
-    for (size_t l = 0; l < pf->mg.size(); ++l)
-        if (pf->mg[l].m.nv <= kBlockCells) {
+    // the single-block cycle starts at the first level of at most kBlockCells cells whose levels fit
+    // in shared memory together
+    for (size_t l = 0; l < pf->mg.size() && pf->mg_block0 < 0; ++l) {
+        if (pf->mg[l].m.nv > kBlockCells) continue;
+        long long dbl = 0;
+        for (size_t k = l; k < pf->mg.size(); ++k) dbl += block_cycle_doubles(pf->mg[k].m);
+        if ((size_t)dbl * sizeof(double) <= kBlockSmemMax) {
             pf->mg_block0 = (int)l;
-            break;
+            pf->mg_block_smem = (size_t)dbl * sizeof(double);
         }
+    }
     {
         const long long nbytes = (long long)(sizeof(MgLevel) * pf->mg.size() + 7) / 8;
         if ((e = dalloc(pf, (double**)&pf->mg_dev, nbytes))) return fail_out(e);

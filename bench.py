@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--no-amr", action="store_true")
     ap.add_argument("--amr-steps", type=int, default=5)
     ap.add_argument("--pf-steps", type=int, default=10)
+    ap.add_argument("--force-kernel", default=None,
+                    help="shape,order of the stage kernel instead of the autotuner's pick (profiling)")
     ap.add_argument("--no-triple", action="store_true")
     ap.add_argument("--triple-m", type=int, default=256, help="triple point side: 7m x 3m cells")
     ap.add_argument("--triple-steps", type=int, default=20)
@@ -449,6 +451,8 @@ def run_ours(args, rank, world, dist):
     levels, ms, clks, tuned = {}, {}, [], {}
     for name, p in forms.items():
         lv = cb.Level(p, g)
+        if args.force_kernel:
+            lv.set_kernel(*(int(x) for x in args.force_kernel.split(",")))
         lv.upload(U, stream=stream)
         # warm-up (includes the t = 0 wave-speed pass and the CUDA-graph capture)
         lv.advance(args.warmup, use_graph=True, stream=stream)

@@ -62,7 +62,8 @@ def parse():
     ap.add_argument("--triple-m", type=int, default=256, help="triple point side: 7m x 3m cells")
     ap.add_argument("--triple-steps", type=int, default=20)
     ap.add_argument("--serve-requests", type=int, default=16)
-    ap.add_argument("--serve-rate", type=float, default=16.0)
+    ap.add_argument("--serve-rate", type=float, default=16.0, help="headline arrival rate (one of --serve-rates)")
+    ap.add_argument("--serve-rates", default="4,16,64", help="arrival rates swept (requests/s)")
     return ap.parse_args()
 
 
@@ -364,25 +365,40 @@ def run_triple_point(args):
 
 def run_serving(args):
     """Poisson arrivals of mixed 2D shock-bubble / 3D shock-droplet / 2D three-material triple-point
-    solves under an HBM budget, continuous batching, against the same requests one at a time on the
-    plain FP64 path."""
+    solves under an HBM budget, continuous batching, at several arrival rates, against the same
+    requests one at a time on the plain FP64 path. The request set (kinds, sizes, steps) is the same at
+    every rate (the seeded draws do not depend on the rate); only the arrival times scale."""
     from compas_b200 import serving
 
-    reqs = serving.poisson_requests(args.serve_requests, args.serve_rate, seed=0, sides2d=(128, 512),
-                                    sides3d=(64, 96), sides_triple=(32, 96), steps=(100, 300))
-    srv = serving.Server(budget_bytes=150e9, precision="mixed", steps_per_iter=4)
-    t0 = time.perf_counter()
-    done = srv.run(reqs)
-    wall = time.perf_counter() - t0
-    srv.close()
-    summ = serving.summarize(done, wall)
-    seq = serving.sequential_baseline(reqs, precision="fp64")
-    kinds = {k: sum(1 for r in reqs if r.kind == k) for k in serving.KINDS}
-    return {"workload": f"{len(reqs)} requests {kinds}, Poisson rate {args.serve_rate}/s (seed 0): 2D FIVEEQS "
-                        "shock-bubble 128^2-512^2, 3D SIXEQS shock-droplet 64^3-96^3 and 2D FIVEEQS_NPHASE (NPHASE 3) "
-                        "triple point 224x96-672x288, 100-300 steps each; budget 150 GB",
+    def reqs_at(rate):
+        return serving.poisson_requests(args.serve_requests, rate, seed=0, sides2d=(128, 512), sides3d=(64, 96),
+                                        sides_triple=(32, 96), steps=(100, 300))
+
+    rates = [float(x) for x in args.serve_rates.split(",")]
+    base = reqs_at(rates[0])
+    service = serving.sequential_service(base, precision="fp64")
+    kinds = {k: sum(1 for r in base if r.kind == k) for k in serving.KINDS}
+    out = {"workload": f"{len(base)} requests {kinds}, Poisson arrivals at each rate (seed 0): 2D FIVEEQS "
+                       "shock-bubble 128^2-512^2, 3D SIXEQS shock-droplet 64^3-96^3 and 2D FIVEEQS_NPHASE (NPHASE 3) "
+                       "triple point 224x96-672x288, 100-300 steps each; budget 150 GB; continuous batching in the "
+                       "mixed form vs the same requests one at a time on the plain FP64 path",
+           "rates": {}}
+    for rate in rates:
+        reqs = reqs_at(rate)
+        srv = serving.Server(budget_bytes=150e9, precision="mixed", steps_per_iter=4)
+        t0 = time.perf_counter()
+        done = srv.run(reqs)
+        wall = time.perf_counter() - t0
+        srv.close()
+        summ = serving.summarize(done, wall)
+        seq = serving.sequential_baseline(reqs, service=service)
+        out["rates"][f"{rate:g}/s"] = {
             "continuous_batching_mixed": summ, "sequential_fp64": seq,
             "throughput_ratio": summ["cell_updates_per_s_per_stage"] / seq["cell_updates_per_s_per_stage"]}
+    head = out["rates"][f"{args.serve_rate:g}/s"] if f"{args.serve_rate:g}/s" in out["rates"] else \
+        next(iter(out["rates"].values()))
+    out.update(head)  # the headline rate's figures at the top level
+    return out
 
 
 def run_reference(args, rank):

@@ -167,9 +167,9 @@ def summarize(done, wall_s):
             "mean_tts_s": float(tts.mean()), "cell_updates_per_s_per_stage": work / wall_s, "wall_s": wall_s}
 
 
-def sequential_baseline(requests, precision="fp64"):
-    """The same requests one at a time on a single-case level (FIFO, no overlap): per-request service
-    times measured on the GPU, time-to-solution from the arrival times."""
+def sequential_service(requests, precision="fp64"):
+    """Service time of each request alone on a single-case level (device work, after one warm-up
+    step on a separate level), keyed by request id."""
     import torch
 
     service = {}
@@ -187,6 +187,14 @@ def sequential_baseline(requests, precision="fp64"):
         service[r.rid] = time.perf_counter() - t0
         lv.close()
         lv2.close()
+    return service
+
+
+def sequential_baseline(requests, precision="fp64", service=None):
+    """The same requests one at a time on a single-case level (FIFO, no overlap): per-request service
+    times measured on the GPU (or given), time-to-solution from the arrival times."""
+    if service is None:
+        service = sequential_service(requests, precision)
     t = 0.0
     tts = []
     for r in sorted(requests, key=lambda x: x.arrival):

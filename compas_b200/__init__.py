@@ -25,7 +25,7 @@ MAX_PHASES = 4
 
 OK = 0
 EARG, ECUDA, ENOMEM, ESTATE, EUNSUPPORTED = -1, -2, -3, -4, -5
-ERR_NAN, ERR_COVOLUME, ERR_RELAX_NOROOT, ERR_CFL = 0x1, 0x2, 0x4, 0x8
+ERR_NAN, ERR_COVOLUME, ERR_RELAX_NOROOT, ERR_CFL, ERR_TIMEOUT = 0x1, 0x2, 0x4, 0x8, 0x10
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libcompas_b200.so")
@@ -81,6 +81,7 @@ class Parm(ctypes.Structure):
         ("Ak", ctypes.c_double * MAX_PHASES), ("Bk", ctypes.c_double * MAX_PHASES),
         ("Ck", ctypes.c_double * MAX_PHASES), ("Dk", ctypes.c_double * MAX_PHASES),
         ("autotune", ctypes.c_int),
+        ("tma", ctypes.c_int),
     ]
 
 
@@ -135,6 +136,7 @@ _SIGS = {
     "compas_b200_level_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                                 ctypes.POINTER(ctypes.c_int)]),
     "compas_b200_level_set_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "compas_b200_level_tma": (ctypes.c_int, [ctypes.c_void_p]),
     "compas_b200_batch_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                                 ctypes.POINTER(ctypes.c_int)]),
     "compas_b200_batch_set_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
@@ -432,6 +434,10 @@ class Level:
     def set_kernel(self, shape: int, order: int) -> None:
         """Force a launch shape and tile order (no tuning for this level)."""
         _check(lib().compas_b200_level_set_kernel(self._h, int(shape), int(order)))
+
+    def tma(self) -> bool:
+        """Whether the stage kernel stages its halo slabs by TMA (3D mixed form)."""
+        return bool(lib().compas_b200_level_tma(self._h))
 
     def pf_substeps(self) -> int:
         """Phase-Field sub-steps taken so far (PhaseField.phase_field = 1)."""

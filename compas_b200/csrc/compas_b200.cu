@@ -2,6 +2,7 @@
 // stage kernels on caller-owned device arrays, and a single-level advance whose time-step control
 // runs on the device (no host synchronisation inside a run, CUDA-graph replay per step).
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -340,7 +341,7 @@ static KernelChoice choice_of(const compas_b200_parm* p) {
 }
 
 static int launch_stage(const compas_b200_parm* p, const StageArgs& a, cudaStream_t st, int phase_field = 0,
-                        int shape = 0) {
+                        int shape = 0, const TmaMaps* tm = nullptr) {
     const int ts = (p->dim == 2) ? kTile2 : kTile3;
     const long long tiles = (long long)((a.g.n[0] + ts - 1) / ts) * ((a.g.n[1] + ts - 1) / ts) *
                             ((a.g.n[2] + (p->dim == 2 ? 1 : ts) - 1) / (p->dim == 2 ? 1 : ts));
@@ -352,11 +353,13 @@ static int launch_stage(const compas_b200_parm* p, const StageArgs& a, cudaStrea
         k.phase_field = 1;
     }
     cudaError_t e;
-    if (p->physics == COMPAS_B200_FIVEEQS) e = (p->dim == 2) ? launch_stage_fiveeq2(k, a, st) : launch_stage_fiveeq3(k, a, st);
-    else if (p->physics == COMPAS_B200_SIXEQS) e = (p->dim == 2) ? launch_stage_sixeq2(k, a, st) : launch_stage_sixeq3(k, a, st);
-    else if (p->dim == 3) e = launch_stage_fiveeqn3_3(k, a, st);
-    else e = (p->nphase == 2) ? launch_stage_fiveeqn2_2(k, a, st)
-           : (p->nphase == 3) ? launch_stage_fiveeqn2_3(k, a, st) : launch_stage_fiveeqn2_4(k, a, st);
+    if (p->physics == COMPAS_B200_FIVEEQS)
+        e = (p->dim == 2) ? launch_stage_fiveeq2(k, a, st, tm) : launch_stage_fiveeq3(k, a, st, tm);
+    else if (p->physics == COMPAS_B200_SIXEQS)
+        e = (p->dim == 2) ? launch_stage_sixeq2(k, a, st, tm) : launch_stage_sixeq3(k, a, st, tm);
+    else if (p->dim == 3) e = launch_stage_fiveeqn3_3(k, a, st, tm);
+    else e = (p->nphase == 2) ? launch_stage_fiveeqn2_2(k, a, st, tm)
+           : (p->nphase == 3) ? launch_stage_fiveeqn2_3(k, a, st, tm) : launch_stage_fiveeqn2_4(k, a, st, tm);
     if (e != cudaSuccess) return fail(COMPAS_B200_ECUDA, std::string("stage kernel launch: ") + cudaGetErrorString(e));
     return COMPAS_B200_OK;
 }
@@ -411,6 +414,7 @@ static int launch_fill(const compas_b200_parm* p, const compas_b200_geom* geo, d
 // ------------------------------------------------------------------------------------------------
 struct TuneChoice {
     int shape = 0, order = 0;
+    int tma = 0;  // halo slabs staged by TMA (single-box 3D mixed kernels that have tensor maps)
     float ms = 0.f;
 };
 static std::mutex g_tune_mu;
@@ -437,10 +441,10 @@ static void tune_store(const std::string& key, const TuneChoice& c) {
     g_tune_cache[key] = c;
 }
 
-// Times launch(shape, order) for every candidate (one warm-up, then `reps` timed launches) on st and
-// returns the fastest. Synchronises st.
+// Times launch(shape, order, tma) for every candidate (one warm-up, then `reps` timed launches) on st
+// and returns the fastest; tma runs over 0 .. ntma-1. Synchronises st.
 template <class F>
-static int tune_candidates(F&& launch, cudaStream_t st, int reps, TuneChoice* best) {
+static int tune_candidates(F&& launch, cudaStream_t st, int reps, TuneChoice* best, int ntma = 1) {
     cudaEvent_t e0, e1;
     CUDA_TRY(cudaEventCreate(&e0));
     if (cudaEventCreate(&e1) != cudaSuccess) {
@@ -450,10 +454,11 @@ static int tune_candidates(F&& launch, cudaStream_t st, int reps, TuneChoice* be
     int rc = COMPAS_B200_OK;
     best->ms = 3.0e38f;
     for (int sh = 0; sh < kShapes && !rc; ++sh)
-        for (int od = 0; od < kOrders && !rc; ++od) {
-            if ((rc = launch(sh, od))) break;
+        for (int od = 0; od < kOrders * ntma && !rc; ++od) {
+            const int o = od % kOrders, tm = od / kOrders;
+            if ((rc = launch(sh, o, tm))) break;
             cudaEventRecord(e0, st);
-            for (int r = 0; r < reps && !rc; ++r) rc = launch(sh, od);
+            for (int r = 0; r < reps && !rc; ++r) rc = launch(sh, o, tm);
             cudaEventRecord(e1, st);
             if (rc) break;
             cudaError_t e = cudaEventSynchronize(e1);
@@ -466,7 +471,8 @@ static int tune_candidates(F&& launch, cudaStream_t st, int reps, TuneChoice* be
             ms /= reps;
             if (ms < best->ms) {
                 best->shape = sh;
-                best->order = od;
+                best->order = o;
+                best->tma = tm;
                 best->ms = ms;
             }
         }
@@ -483,6 +489,63 @@ static int cached_shape(const compas_b200_parm* p, const compas_b200_geom* g, St
     if (!tune_lookup(tune_key(p, "box", g->n[0], g->n[1], p->dim == 3 ? g->n[2] : 1), &c)) return 0;
     a.order = c.order;
     return c.shape;
+}
+
+// ------------------------------------------------------------------------------------------------
+// TMA tensor maps of a padded state array for the halo-slab staging of the 3D mixed stage kernel
+// (tma.cuh). Encoded with the driver's cuTensorMapEncodeTiled (looked up once through the runtime):
+// dims {PX, PY, PZ, N} of FP64, boxes 10 x 3 x 8 x N (y slabs) and 10 x 8 x 3 x N (z slabs). The
+// slab boxes start at an even x index (16-byte boundary) and at non-negative y and z. Returns false
+// (maps not valid; the kernel then loads the slabs itself) where a rule does not hold: the row
+// stride must be a multiple of 16 bytes (PX even), the array 16-byte aligned, 3D, ng >= 3.
+// ------------------------------------------------------------------------------------------------
+static bool tma_wanted(const compas_b200_parm* p) {
+    return p->tma && p->dim == 3 && p->precision == 1 && !p->thinc &&
+           (p->physics == COMPAS_B200_FIVEEQS || p->physics == COMPAS_B200_SIXEQS);
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
+    static std::mutex mu;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!tried) {
+        tried = true;
+        void* ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+static bool make_tma_maps(const compas_b200_parm* p, const compas_b200_geom* geo, const double* U, TmaMaps* out) {
+    std::memset(out, 0, sizeof(*out));
+    if (!tma_wanted(p) || !U) return false;
+    const Grid g = make_grid(p, geo);
+    if (g.ng < 3 || (g.px % 2) != 0 || (reinterpret_cast<uintptr_t>(U) % 16) != 0) return false;
+    if (g.px > (1LL << 31) || g.pxy / g.px > (1LL << 31) || g.S / g.pxy > (1LL << 31)) return false;
+    auto enc = tma_encoder();
+    if (!enc) return false;
+    const int N = nstate(p);
+    const cuuint64_t dims[4] = {(cuuint64_t)g.px, (cuuint64_t)(g.pxy / g.px), (cuuint64_t)(g.S / g.pxy),
+                                (cuuint64_t)N};
+    const cuuint64_t strides[3] = {(cuuint64_t)g.px * 8, (cuuint64_t)g.pxy * 8, (cuuint64_t)g.S * 8};
+    const cuuint32_t box_y[4] = {(cuuint32_t)kTmaBoxX, 3, (cuuint32_t)kTile3, (cuuint32_t)N};
+    const cuuint32_t box_z[4] = {(cuuint32_t)kTmaBoxX, (cuuint32_t)kTile3, 3, (cuuint32_t)N};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    void* base = const_cast<double*>(U);
+    CUresult r1 = enc(&out->y, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims, strides, box_y, es,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult r2 = enc(&out->z, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims, strides, box_z, es,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    out->valid = (r1 == CUDA_SUCCESS && r2 == CUDA_SUCCESS) ? 1 : 0;
+    return out->valid != 0;
 }
 
 static StageArgs base_args(const compas_b200_parm* p, const compas_b200_geom* g) {
@@ -561,6 +624,8 @@ struct compas_b200_level {
     compas::PfInfo pf_last{};       // counters of the last Phase-Field step
     int shape = 0, order = 0;       // stage-kernel launch shape and tile order (autotuner or forced)
     bool tuned = false, forced = false;
+    compas::TmaMaps maps[3];        // TMA maps of U, U1, U2 (3D mixed form; valid = 0 otherwise)
+    bool use_tma = false;           // stage with the maps (compas_b200.tma = 1; the autotuner may turn it off)
 };
 
 namespace compas {
@@ -654,6 +719,7 @@ int compas_b200_parm_init_nphase(compas_b200_parm* p, int physics, int dim, int 
     p->pf_max_step = 1000000;
     p->pf_tol_rel = 1.0e-10;
     p->autotune = 1;
+    p->tma = 1;
     if (physics != COMPAS_B200_FIVEEQS && physics != COMPAS_B200_SIXEQS && physics != COMPAS_B200_FIVEEQS_NPHASE)
         return fail(COMPAS_B200_EARG, "physics must be FIVEEQS (555), SIXEQS (666) or FIVEEQS_NPHASE (55501)");
     if (dim != 2 && dim != 3) return fail(COMPAS_B200_EARG, "dim must be 2 or 3");
@@ -777,6 +843,12 @@ int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value
             *dk.dst = x;
             return 0;
         }
+    if (k == "compas_b200.tma") {
+        // this engine's own key: stage the 3D mixed form's halo slabs by TMA (1) or plain loads (0)
+        if (!parse_int(value, &ix) || ix < 0 || ix > 1) return bad("0, 1");
+        p->tma = ix;
+        return 0;
+    }
     if (k == "compas_b200.autotune") {
         // this engine's own key: pick the stage kernel's launch shape and tile order by timing
         if (!parse_int(value, &ix) || ix < 0 || ix > 1) return bad("0, 1");
@@ -1128,6 +1200,10 @@ int compas_b200_level_create(const compas_b200_parm* p, const compas_b200_geom* 
         return fail(e == cudaErrorMemoryAllocation ? COMPAS_B200_ENOMEM : COMPAS_B200_ECUDA,
                     std::string("level allocation: ") + cudaGetErrorString(e));
     }
+    make_tma_maps(p, &lv->g, lv->U, &lv->maps[0]);
+    make_tma_maps(p, &lv->g, lv->U1, &lv->maps[1]);
+    make_tma_maps(p, &lv->g, lv->U2, &lv->maps[2]);
+    lv->use_tma = lv->maps[0].valid && lv->maps[1].valid && lv->maps[2].valid;
     if (p->phase_field) {
         std::string msg;
         if ((rc = pf_create(p, &lv->g, &lv->pf, &msg))) {
@@ -1204,11 +1280,11 @@ static int tune_level(compas_b200_level* lv, cudaStream_t st) {
         a.dt = scratch;
         a.cmax = reinterpret_cast<unsigned long long*>(scratch + 1);
         a.err = reinterpret_cast<unsigned int*>(scratch + 2);
-        auto launch = [&](int sh, int od) {
+        auto launch = [&](int sh, int od, int tm) {
             a.order = od;
-            return launch_stage(&lv->p, a, st, 0, sh);
+            return launch_stage(&lv->p, a, st, 0, sh, tm ? &lv->maps[0] : nullptr);
         };
-        const int rc = tune_candidates(launch, st, 2, &c);
+        const int rc = tune_candidates(launch, st, 2, &c, lv->maps[0].valid ? 2 : 1);
         cudaStreamSynchronize(st);
         cudaFree(scratch);
         if (rc) return rc;
@@ -1216,6 +1292,7 @@ static int tune_level(compas_b200_level* lv, cudaStream_t st) {
     }
     lv->shape = c.shape;
     lv->order = c.order;
+    lv->use_tma = c.tma && lv->maps[0].valid;
     lv->tuned = true;
     return COMPAS_B200_OK;
 }
@@ -1251,7 +1328,7 @@ static int enqueue_step(compas_b200_level* lv, cudaStream_t st) {
         a.Us = bufs_in[s];
         a.U0 = lv->U;
         a.Uout = bufs_out[s];
-        if ((rc = launch_stage(p, a, st, 0, lv->shape))) return rc;
+        if ((rc = launch_stage(p, a, st, 0, lv->shape, lv->use_tma ? &lv->maps[s] : nullptr))) return rc;
     }
     step_end_kernel<<<1, 1, 0, st>>>(lv->ctl);
     CUDA_TRY(cudaGetLastError());
@@ -1348,6 +1425,11 @@ int compas_b200_level_kernel(const compas_b200_level* lv, int* shape, int* order
     if (shape) *shape = lv->shape;
     if (order) *order = lv->order;
     return COMPAS_B200_OK;
+}
+
+int compas_b200_level_tma(const compas_b200_level* lv) {
+    if (!lv) return fail(COMPAS_B200_EARG, "null level");
+    return lv->use_tma ? 1 : 0;
 }
 
 int compas_b200_level_set_kernel(compas_b200_level* lv, int shape, int order) {
@@ -1582,7 +1664,7 @@ static int tune_batch(compas_b200_batch* b, cudaStream_t st) {
     const std::string key = tune_key(&b->cases[0].p, "list", tb, nb, 0);
     TuneChoice c;
     if (!tune_lookup(key, &c)) {
-        auto launch = [&](int sh, int od) {
+        auto launch = [&](int sh, int od, int) {
             ListArgs L{b->d_boxes, b->d_nbox, b->d_tile_off, kModeStage, 0, od};
             return launch_list(b->physics, b->dim, b->nphase, b->limiter, b->precision, L, st, sh);
         };

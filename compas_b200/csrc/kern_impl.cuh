@@ -51,8 +51,35 @@ static cudaError_t launch_stage_v(const StageArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+// One box with the y/z halo slabs staged by TMA (3D mixed form; the maps describe a.Us).
+template <class M, int SCHEME, int SH>
+static cudaError_t launch_stage_tma(const StageArgs& a, const TmaMaps& tm, cudaStream_t st) {
+    using S = LaunchShape<M, SH>;
+    using T = TileShape<M, S::TS, S::TS, S::TZ, float, true>;
+    auto kern = stage_kernel_tma<M, SCHEME, true, S::TS, S::TS, S::TZ, S::NT, S::MINB>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    const long long tiles = (long long)((a.g.n[0] + S::TS - 1) / S::TS) * ((a.g.n[1] + S::TS - 1) / S::TS) *
+                            ((a.g.n[2] + S::TZ - 1) / S::TZ);
+    kern<<<(unsigned)tiles, S::NT, T::SMEM, st>>>(a, tm);
+    return cudaGetLastError();
+}
+
 template <class M, int SCHEME, bool MIX>
-static cudaError_t launch_stage_var(const KernelChoice& k, const StageArgs& a, cudaStream_t st) {
+static cudaError_t launch_stage_var(const KernelChoice& k, const StageArgs& a, cudaStream_t st, const TmaMaps* tm) {
+    if constexpr (M::D == 3 && MIX && M::KIND != kModelFiveN) {
+        if (tm && tm->valid && !k.thinc && !k.phase_field) {
+            switch (k.shape) {
+                case 1: return launch_stage_tma<M, SCHEME, 1>(a, *tm, st);
+                case 2: return launch_stage_tma<M, SCHEME, 2>(a, *tm, st);
+                default: return launch_stage_tma<M, SCHEME, 0>(a, *tm, st);
+            }
+        }
+    }
     if constexpr (M::KIND == kModelFiveN) {
         // FIVEEQS_NPHASE: the plain hyperbolic right-hand side only
         if (k.phase_field || k.thinc) return cudaErrorNotSupported;
@@ -72,14 +99,15 @@ static cudaError_t launch_stage_var(const KernelChoice& k, const StageArgs& a, c
 }
 
 template <class M>
-static cudaError_t launch_stage_m(const KernelChoice& k, const StageArgs& a, cudaStream_t st) {
+static cudaError_t launch_stage_m(const KernelChoice& k, const StageArgs& a, cudaStream_t st, const TmaMaps* tm) {
     const bool mix = (k.precision == 1), bounded = (k.limiter == 6);
     if constexpr (M::KIND == kModelFiveN) {
         if (bounded) return cudaErrorNotSupported;
-        return mix ? launch_stage_var<M, 5, true>(k, a, st) : launch_stage_var<M, 5, false>(k, a, st);
+        return mix ? launch_stage_var<M, 5, true>(k, a, st, tm) : launch_stage_var<M, 5, false>(k, a, st, tm);
     } else {
-        if (mix) return bounded ? launch_stage_var<M, 6, true>(k, a, st) : launch_stage_var<M, 5, true>(k, a, st);
-        return bounded ? launch_stage_var<M, 6, false>(k, a, st) : launch_stage_var<M, 5, false>(k, a, st);
+        if (mix)
+            return bounded ? launch_stage_var<M, 6, true>(k, a, st, tm) : launch_stage_var<M, 5, true>(k, a, st, tm);
+        return bounded ? launch_stage_var<M, 6, false>(k, a, st, tm) : launch_stage_var<M, 5, false>(k, a, st, tm);
     }
 }
 
@@ -128,8 +156,9 @@ static cudaError_t launch_list_m(const KernelChoice& k, const ListArgs& L, cudaS
 
 #define COMPAS_DEFINE_LAUNCHERS(name, Model)                                                         \
     namespace compas {                                                                              \
-    cudaError_t launch_stage_##name(const KernelChoice& k, const StageArgs& a, cudaStream_t st) {    \
-        return launch_stage_m<Model>(k, a, st);                                                     \
+    cudaError_t launch_stage_##name(const KernelChoice& k, const StageArgs& a, cudaStream_t st,     \
+                                    const TmaMaps* tm) {                                            \
+        return launch_stage_m<Model>(k, a, st, tm);                                                 \
     }                                                                                               \
     cudaError_t launch_list_##name(const KernelChoice& k, const ListArgs& L, cudaStream_t st) {      \
         return launch_list_m<Model>(k, L, st);                                                      \

@@ -9,6 +9,7 @@ namespace compas {
 
 struct StageArgs;
 struct ListArgs;
+struct TmaMaps;
 
 // Variant of the stage kernel: FiniteVolume.Scheme (5 WENO5, 6 WENO5B), precision (0 FP64, 1 mixed),
 // FiniteVolume.THINC (single-box kernel only), and the Phase-Field regularisation right-hand side
@@ -30,8 +31,9 @@ constexpr int kOrders = 2;
 constexpr int kTile2 = 16;
 constexpr int kTile3 = 8;
 
-#define COMPAS_DECLARE_LAUNCHERS(name)                                                          \
-    cudaError_t launch_stage_##name(const KernelChoice& k, const StageArgs& a, cudaStream_t st); \
+#define COMPAS_DECLARE_LAUNCHERS(name)                                                               \
+    cudaError_t launch_stage_##name(const KernelChoice& k, const StageArgs& a, cudaStream_t st,        \
+                                    const TmaMaps* tm);                                              \
     cudaError_t launch_list_##name(const KernelChoice& k, const ListArgs& L, cudaStream_t st);
 COMPAS_DECLARE_LAUNCHERS(fiveeq2)
 COMPAS_DECLARE_LAUNCHERS(fiveeq3)

@@ -24,6 +24,7 @@
 #include "physics.cuh"
 #include "physics_nphase.cuh"
 #include "relax.cuh"
+#include "tma.cuh"
 
 #include <type_traits>
 
@@ -92,8 +93,10 @@ __device__ __forceinline__ void tile_coords(int w, int ntx, int nty, int ntz, in
     tz = gz * BZ + r / (nx * ny);
 }
 
-// Variants of the stage kernel (the VAR template argument of stage_tile).
-enum { kVarPlain = 0, kVarThinc = 1, kVarPhaseField = 2 };
+// Variants of the stage kernel (the VAR template argument of stage_tile). kVarTma: the plain
+// right-hand side with the y and z halo slabs staged into shared memory by TMA (3D mixed form), each
+// prefetched while the previous direction's faces are computed.
+enum { kVarPlain = 0, kVarThinc = 1, kVarPhaseField = 2, kVarTma = 3 };
 
 }  // namespace compas
 
@@ -102,7 +105,7 @@ enum { kVarPlain = 0, kVarThinc = 1, kVarPhaseField = 2 };
 
 namespace compas {
 
-template <class M, int TX, int TY, int TZ, class PT = double>
+template <class M, int TX, int TY, int TZ, class PT = double, bool TMA = false>
 struct TileShape {
     static constexpr int D = M::D;
     static constexpr int CELLS = TX * TY * TZ;
@@ -118,7 +121,11 @@ struct TileShape {
     // primitives (type PT) of the tile and of one halo slab pair, then the face buffer (FP64)
     static constexpr size_t PBYTES = sizeof(PT) * ((size_t)M::N * CELLS + (size_t)M::N * HALO);
     static constexpr size_t FOFF = (PBYTES + 15) / 16 * 16;
-    static constexpr size_t SMEM = FOFF + sizeof(double) * (size_t)NB * FMAX;
+    static constexpr size_t FEND = FOFF + sizeof(double) * (size_t)NB * FMAX;
+    // TMA staging of one direction's two halo slabs (raw FP64 boxes of kTmaBoxX x 3 x T x N), placed
+    // at the next 128-byte boundary of the (runtime) shared-memory address, hence the 128-byte slack
+    static constexpr size_t SLAB = sizeof(double) * (size_t)kTmaBoxX * 3 * TX * M::N;
+    static constexpr size_t SMEM = TMA ? FEND + 128 + 2 * SLAB : FEND;
 };
 
 template <class M>
@@ -139,15 +146,17 @@ __device__ __forceinline__ void load_cons(double* U, const double* base, const G
 // no non-conservative terms; FIVEEQS).
 // The work of one CTA on tile `tile` of the box described by `a` (tiles numbered x fastest).
 template <class M, int SCHEME, bool MIX, int VAR, int TX, int TY, int TZ, int NT>
-__device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double* smem_d) {
+__device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double* smem_d, const TmaMaps* tm = nullptr) {
     static_assert(TX == TY && (M::D == 2 ? TZ == 1 : TZ == TX), "tiles are cubes (squares in 2D)");
     constexpr bool TH = (VAR == kVarThinc);
     constexpr bool PFX = (VAR == kVarPhaseField);
+    constexpr bool TMA = (VAR == kVarTma);
+    static_assert(!TMA || (M::D == 3 && MIX), "TMA halo staging: the 3D mixed form");
     static_assert(!PFX || M::KIND == kModelFive, "the Phase-Field kernel is the five-equation model's");
     static_assert(M::KIND != kModelFiveN || (SCHEME == 5 && !TH), "FIVEEQS_NPHASE runs WENO5 without THINC");
     constexpr bool NPH = (M::KIND == kModelFiveN);
     using PT = typename std::conditional<MIX, float, double>::type;
-    using T = TileShape<M, TX, TY, TZ, PT>;
+    using T = TileShape<M, TX, TY, TZ, PT, TMA>;
     constexpr int N = M::N, NC = M::NC, D = M::D, NB = T::NB;
     constexpr int CELLS = T::CELLS, HALO = T::HALO, FMAX = T::FMAX;
     constexpr int R = (CELLS + NT - 1) / NT;
@@ -168,6 +177,12 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
     const int k0 = tiz * TZ;
     const int tid = threadIdx.x;
     unsigned int* err = a.err;
+    __shared__ uint64_t tma_bar;
+    double* stg = nullptr;  // TMA staging: low slab, then high slab
+    if constexpr (TMA) {
+        stg = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(smem_d) + T::FEND + 127) & ~uintptr_t(127));
+        if (tid == 0) mbar_init(&tma_bar, 1);  // visible to all after the barrier that ends step 1
+    }
 
     // 1. tile cells and the x-direction halo slabs -> primitives, read as whole rows of TX + 6 cells
     // (coalesced), the tile cells into Pint and the halo cells into the x slabs of Phal
@@ -208,7 +223,42 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
         constexpr int Ad = T::A0;
         constexpr int Ta = TX;
         // 2a. halo slabs of direction d -> primitives (the x slabs came with the rows of step 1)
-        for (int h = (d == 0) ? 6 * Ad : tid; h < 6 * Ad; h += NT) {
+        if constexpr (TMA) {
+            if (d > 0) {
+                // the slabs were staged by TMA during the previous direction's faces (phase d - 1)
+                if (!mbar_wait_bounded(&tma_bar, (unsigned)(d - 1), 1 << 20)) {
+                    flag_error(err, COMPAS_B200_ERR_TIMEOUT);
+                    mbar_wait_bounded(&tma_bar, (unsigned)(d - 1), 1 << 20);
+                }
+                const int offx = (i0 + g.ng) - ((i0 + g.ng - 1) & ~1);
+                for (int h = tid; h < 6 * Ad; h += NT) {
+                    const int slot = h / Ad, t = h % Ad;
+                    const int pos = (slot < 3) ? slot - 3 : Td + slot - 3;
+                    const int ta = t % Ta, tb = t / Ta;
+                    const int b = (slot < 3) ? slot : slot - 3;
+                    const double* sl = stg + ((slot < 3) ? 0 : T::SLAB / sizeof(double));
+                    // box element (x, y, z) of component n: n*(10*3*8) + z*(10*Y) + y*10 + x
+                    const int e0 = (d == 1) ? (ta + offx) + kTmaBoxX * b + kTmaBoxX * 3 * tb
+                                            : (ta + offx) + kTmaBoxX * tb + kTmaBoxX * Ta * b;
+                    int lx, ly, lz;
+                    if (d == 1) { lx = ta; ly = pos; lz = tb; }
+                    else { lx = ta; ly = tb; lz = pos; }
+                    double U[N];
+                    PT W[N];
+                    if (g.padded(i0 + lx, j0 + ly, k0 + lz)) {
+#pragma unroll
+                        for (int n = 0; n < N; ++n) U[n] = sl[n * (kTmaBoxX * 3 * Ta) + e0];
+                        M::cons2prim_f32(W, U, a.e);
+                    } else {
+#pragma unroll
+                        for (int n = 0; n < N; ++n) W[n] = 0;
+                    }
+#pragma unroll
+                    for (int n = 0; n < N; ++n) Phal[n * HALO + slot * T::HS + t] = W[n];
+                }
+            }
+        }
+        for (int h = (d == 0 || TMA) ? 6 * Ad : tid; h < 6 * Ad; h += NT) {
             const int slot = h / Ad, t = h % Ad;
             const int pos = (slot < 3) ? slot - 3 : Td + slot - 3;
             const int ta = t % Ta, tb = t / Ta;
@@ -240,6 +290,23 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
         constexpr int EF = TS + 1;
         const int NF = EF * T::A0;
         const double dxd = (d == 0) ? g.dx[0] : (d == 1 ? g.dx[1] : g.dx[2]);
+        if constexpr (TMA) {
+            // stage the next direction's two halo slabs while this direction's faces are computed;
+            // the staging was last read before the barrier above
+            if (tid == 0 && d + 1 < D) {
+                fence_proxy_async_smem();
+                mbar_arrive_expect_tx(&tma_bar, (unsigned)(2 * T::SLAB));
+                const int xs = (i0 + g.ng - 1) & ~1;  // even: an 8-byte element start on a 16-byte boundary
+                double* hi = stg + T::SLAB / sizeof(double);
+                if (d == 0) {
+                    tma_load_4d(stg, &tm->y, &tma_bar, xs, j0 + g.ng - 3, k0 + g.gz, 0);
+                    tma_load_4d(hi, &tm->y, &tma_bar, xs, j0 + g.ng + TY, k0 + g.gz, 0);
+                } else {
+                    tma_load_4d(stg, &tm->z, &tma_bar, xs, j0 + g.ng, k0 + g.gz - 3, 0);
+                    tma_load_4d(hi, &tm->z, &tma_bar, xs, j0 + g.ng, k0 + g.gz + TZ, 0);
+                }
+            }
+        }
         for (int f = tid; f < NF; f += NT) {
             int fd, ta, tb;
             if (d == 0) {
@@ -538,6 +605,14 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
     if (a.done && *a.done) return;
     extern __shared__ double smem_d[];
     stage_tile<M, SCHEME, MIX, VAR, TX, TY, TZ, NT>(a, blockIdx.x, smem_d);
+}
+
+// One box with the halo slabs staged by TMA (the tensor maps of a.Us are kernel parameters).
+template <class M, int SCHEME, bool MIX, int TX, int TY, int TZ, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) stage_kernel_tma(StageArgs a, const __grid_constant__ TmaMaps tm) {
+    if (a.done && *a.done) return;
+    extern __shared__ __align__(128) double smem_d[];
+    stage_tile<M, SCHEME, MIX, kVarTma, TX, TY, TZ, NT>(a, blockIdx.x, smem_d, &tm);
 }
 
 // ------------------------------------------------------------------------------------------------

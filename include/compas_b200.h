@@ -37,6 +37,7 @@ extern "C" {
 #define COMPAS_B200_ERR_COVOLUME 0x2u     /* NASG 1 - b rho <= 0 (include/EquationOfState_NASG.H:26-32) */
 #define COMPAS_B200_ERR_RELAX_NOROOT 0x4u /* safeguarded relaxation found no root */
 #define COMPAS_B200_ERR_CFL 0x8u          /* non-positive or non-finite time step */
+#define COMPAS_B200_ERR_TIMEOUT 0x10u     /* an asynchronous (TMA) copy did not complete within its bounded wait */
 
 /* ---- models and schemes (the reference's compile-time PHYSICS and run-time keys) ------------ */
 #define COMPAS_B200_FIVEEQS 555 /* include/Macros.H:56 */
@@ -97,6 +98,12 @@ typedef struct compas_b200_parm {
      * launch shape and tile traversal order by timing the candidates on their own data the first
      * time they advance (the result is the same for every candidate) */
     int autotune;
+    /* compas_b200.tma (this engine's key, default 1): levels of the 3D mixed form may stage the y and z
+     * halo slabs of every tile into shared memory by TMA while the previous direction's faces are
+     * computed (needs an even padded row length); the autotuner times both forms and keeps the faster,
+     * a forced kernel (compas_b200_level_set_kernel) uses TMA; 0 always loads them with ordinary loads.
+     * Same results either way. */
+    int tma;
 } compas_b200_parm;
 
 /* One box covering a single-level domain (the valid cells), its ghost width and its boundary codes
@@ -262,6 +269,10 @@ int compas_b200_level_dts(compas_b200_level* lv, double* dts, int n);
  * (compas_b200.autotune = 1), else shape 0 / order 0 or what set_kernel forced. */
 int compas_b200_level_kernel(const compas_b200_level* lv, int* shape, int* order);
 int compas_b200_level_set_kernel(compas_b200_level* lv, int shape, int order);
+
+/* 1 if the level's stage kernel stages the halo slabs by TMA (compas_b200.tma = 1, 3D mixed form, an
+ * even padded row length, and after tuning the faster form), 0 if it loads them with ordinary loads. */
+int compas_b200_level_tma(const compas_b200_level* lv);
 
 /* Kernel launches the library enqueued on this level since upload. */
 long long compas_b200_level_launches(compas_b200_level* lv);

@@ -60,3 +60,10 @@ def test_autotune_key():
     assert cb.make_parm(cb.FIVEEQS, 2, {"compas_b200.autotune": 0}).autotune == 0
     with pytest.raises(cb.CompasError):
         cb.make_parm(cb.FIVEEQS, 2, {"compas_b200.autotune": 2})
+
+
+def test_tma_key():
+    assert cb.make_parm(cb.SIXEQS, 3).tma == 1
+    assert cb.make_parm(cb.SIXEQS, 3, {"compas_b200.tma": 0}).tma == 0
+    with pytest.raises(cb.CompasError):
+        cb.make_parm(cb.SIXEQS, 3, {"compas_b200.tma": 3})

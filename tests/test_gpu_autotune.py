@@ -26,6 +26,7 @@ def _run_forced(fn, kw, precision, steps, shape, order, extra=None):
     info = lv.sync()
     out = lv.download()
     k = lv.kernel()
+    _run_forced.tma = lv.tma()
     lv.close()
     assert info.status == 0 and info.steps == steps
     return cb.valid_view(out, p, g), k
@@ -78,3 +79,23 @@ def test_batch_candidates_give_the_same_bits():
             assert k in CANDIDATES
         for a, r in zip(got, ref):
             assert np.array_equal(a, r), (shape, order)
+
+
+@pytest.mark.parametrize("fn,kw,steps,uses_tma", [
+    (cases.shock_droplet, dict(n=24), 4, True),
+    (cases.shock_droplet, dict(n=21), 3, False),
+    (cases.advected_interface, dict(n=20, dim=3, physics=cb.FIVEEQS), 3, True),
+    (cases.advected_interface, dict(n=16, dim=3, physics=cb.SIXEQS), 3, True),
+], ids=["droplet24", "droplet21_odd_no_tma", "sphere20_five", "sphere16_six"])
+def test_tma_halo_staging_gives_the_same_bits(fn, kw, steps, uses_tma):
+    """The 3D mixed form with the y/z halo slabs staged by TMA equals the plain-load form to the bit,
+    for every launch shape (an odd row length falls back to plain loads)."""
+    outs = {}
+    for tma in (0, 1):
+        for shape in range(3):
+            got, k = _run_forced(fn, kw, "mixed", steps, shape, 0, {"compas_b200.tma": tma})
+            assert _run_forced.tma == (bool(tma) and uses_tma)
+            outs[(tma, shape)] = got
+    ref = outs[(0, 0)]
+    for key, got in outs.items():
+        assert np.array_equal(got, ref), key

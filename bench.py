@@ -363,12 +363,17 @@ def run_triple_point(args):
     return out
 
 
-def run_serving(args):
+def run_serving(args, rank=0, world=1, dist=None):
     """Poisson arrivals of mixed 2D shock-bubble / 3D shock-droplet / 2D three-material triple-point
     solves under an HBM budget, continuous batching, at several arrival rates, against the same
     requests one at a time on the plain FP64 path. The request set (kinds, sizes, steps) is the same at
-    every rate (the seeded draws do not depend on the rate); only the arrival times scale."""
-    from compas_b200 import serving
+    every rate (the seeded draws do not depend on the rate); only the arrival times scale. With several
+    GPUs every rank serves the requests dealt to it (round-robin; no collective on the data path) and
+    rank 0 merges the ranks' time-to-solution records; the sequential baseline is each GPU serving its
+    share one request at a time."""
+    import numpy as np
+
+    from compas_b200 import replicas, serving
 
     def reqs_at(rate):
         return serving.poisson_requests(args.serve_requests, rate, seed=0, sides2d=(128, 512), sides3d=(64, 96),
@@ -376,25 +381,42 @@ def run_serving(args):
 
     rates = [float(x) for x in args.serve_rates.split(",")]
     base = reqs_at(rates[0])
-    service = serving.sequential_service(base, precision="fp64")
+    service = serving.sequential_service(replicas.deal_requests(base, rank, world), precision="fp64")
     kinds = {k: sum(1 for r in base if r.kind == k) for k in serving.KINDS}
     out = {"workload": f"{len(base)} requests {kinds}, Poisson arrivals at each rate (seed 0): 2D FIVEEQS "
                        "shock-bubble 128^2-512^2, 3D SIXEQS shock-droplet 64^3-96^3 and 2D FIVEEQS_NPHASE (NPHASE 3) "
-                       "triple point 224x96-672x288, 100-300 steps each; budget 150 GB; continuous batching in the "
-                       "mixed form vs the same requests one at a time on the plain FP64 path",
+                       "triple point 224x96-672x288, 100-300 steps each; budget 150 GB per GPU; continuous batching "
+                       "in the mixed form vs the same requests one at a time on the plain FP64 path"
+                       + (f"; requests dealt round-robin to {world} GPUs" if world > 1 else ""),
            "rates": {}}
     for rate in rates:
-        reqs = reqs_at(rate)
+        reqs = replicas.deal_requests(reqs_at(rate), rank, world)
         srv = serving.Server(budget_bytes=150e9, precision="mixed", steps_per_iter=4)
         t0 = time.perf_counter()
         done = srv.run(reqs)
         wall = time.perf_counter() - t0
         srv.close()
-        summ = serving.summarize(done, wall)
-        seq = serving.sequential_baseline(reqs, service=service)
+        mine = {"tts": [r.finished - r.arrival for r in done], "work": sum(r.cells * 3 * r.steps for r in done),
+                "wall": wall, "seq_tts": serving.sequential_tts(reqs, service),
+                "seq_busy": sum(service[r.rid] for r in reqs)}
+        allr = replicas.gather(mine, dist)
+        if rank != 0:
+            continue
+        tts = np.concatenate([np.asarray(x["tts"]) for x in allr])
+        seq_tts = np.concatenate([np.asarray(x["seq_tts"]) for x in allr])
+        work = sum(x["work"] for x in allr)
+        wall_max = max(x["wall"] for x in allr)
+        busy_max = max(x["seq_busy"] for x in allr)
+        summ = {"requests": int(tts.size), "p50_tts_s": float(np.percentile(tts, 50)),
+                "p99_tts_s": float(np.percentile(tts, 99)), "mean_tts_s": float(tts.mean()),
+                "cell_updates_per_s_per_stage": work / wall_max, "wall_s": wall_max}
+        seq = {"p50_tts_s": float(np.percentile(seq_tts, 50)), "p99_tts_s": float(np.percentile(seq_tts, 99)),
+               "cell_updates_per_s_per_stage": work / busy_max, "busy_s": busy_max}
         out["rates"][f"{rate:g}/s"] = {
             "continuous_batching_mixed": summ, "sequential_fp64": seq,
             "throughput_ratio": summ["cell_updates_per_s_per_stage"] / seq["cell_updates_per_s_per_stage"]}
+    if rank != 0:
+        return None
     head = out["rates"][f"{args.serve_rate:g}/s"] if f"{args.serve_rate:g}/s" in out["rates"] else \
         next(iter(out["rates"].values()))
     out.update(head)  # the headline rate's figures at the top level
@@ -452,17 +474,13 @@ def run_ours(args, rank, world, dist):
     if args.precision != "both":
         forms = {args.precision: forms[args.precision]}
 
+    from compas_b200 import replicas
+
     def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
+        replicas.barrier(dist, torch.cuda.synchronize)
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, dist, device="cuda")
 
     levels, ms, clks, tuned = {}, {}, [], {}
     for name, p in forms.items():
@@ -493,7 +511,7 @@ def run_ours(args, rank, world, dist):
         tuned[name] = lv.kernel()
     head = "mixed" if "mixed" in forms else "fp64"
     p = forms[head]
-    value = world * cells * 3 * args.steps / (ms[head] / 1e3)
+    value = replicas.whole_job_rate(cells, 3, args.steps, ms[head] / 1e3, world)
 
     # error of the mixed form against the FP64 form after the same warm-up + timed steps
     err = None
@@ -567,7 +585,7 @@ def run_ours(args, rank, world, dist):
         lv.download(out=host_out, stream=stream)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e = world * cells * 3 * args.steps / e2e_s
+    e2e = replicas.whole_job_rate(cells, 3, args.steps, e2e_s, world)
     lv.sync()
     nbytes = int(lv.nbytes)
     for l in levels.values():
@@ -580,12 +598,13 @@ def run_ours(args, rank, world, dist):
                "reasons": sorted(set(r for c in good for r in c["reasons"])),
                "samples": sum(c["samples"] for c in good)}
     line = None
+    # serving runs on every rank (each serves its dealt requests); the rest of the extras on rank 0
+    serving_res = None if args.no_serving else run_serving(args, rank, world, dist)
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu:
             cpu = cpu_baseline(args.cpu_n, args.cpu_steps)
         batched = None if args.no_batched else run_batched(args)
-        serving_res = None if args.no_serving else run_serving(args)
         pf_res = None if args.no_phase_field else run_phase_field(args)
         amr_res = None if args.no_amr else run_amr(args)
         triple_res = None if args.no_triple else run_triple_point(args)
@@ -600,7 +619,7 @@ def run_ours(args, rank, world, dist):
                                           "stage_kernel_autotuned": {
                                               k: {"launch_shape": v[0], "tile_order": ("x fastest", "bricks")[v[1]]}
                                               for k, v in tuned.items()}}),
-            "fp64_plain": ({"value": world * cells * 3 * args.steps / (ms["fp64"] / 1e3),
+            "fp64_plain": ({"value": replicas.whole_job_rate(cells, 3, args.steps, ms["fp64"] / 1e3, world),
                             "ms_per_step": ms["fp64"] / args.steps,
                             "note": "bit-identical to the reference CPU arithmetic"} if "fp64" in ms else None),
             "mixed_error_vs_fp64": err,

@@ -190,6 +190,18 @@ def sequential_service(requests, precision="fp64"):
     return service
 
 
+def sequential_tts(requests, service) -> list:
+    """Time-to-solution of each request served one at a time in arrival order (FIFO, no overlap) with
+    the given service times."""
+    t = 0.0
+    tts = []
+    for r in sorted(requests, key=lambda x: x.arrival):
+        start = max(t, r.arrival)
+        t = start + service[r.rid]
+        tts.append(t - r.arrival)
+    return tts
+
+
 def sequential_baseline(requests, precision="fp64", service=None):
     """The same requests one at a time on a single-case level (FIFO, no overlap): per-request service
     times measured on the GPU (or given), time-to-solution from the arrival times."""

@@ -261,6 +261,8 @@ static Eos make_eos(const compas_b200_parm* p) {
     e.C1 = p->C1; e.C2 = p->C2; e.D1 = p->D1; e.D2 = p->D2;
     e.iA1 = 1.0 / p->A1;
     e.iA2 = 1.0 / p->A2;
+    e.pinf1 = p->B1 / (p->A1 + 1.0);
+    e.pinf2 = p->B2 / (p->A2 + 1.0);
     for (int k = 0; k < kMaxPhases; ++k) {
         e.Ak[k] = p->Ak[k];
         e.Bk[k] = p->Bk[k];

@@ -59,6 +59,7 @@ constexpr int kMaxPhases = COMPAS_B200_MAX_PHASES;
 struct Eos {
     double A1, A2, B1, B2, C1, C2, D1, D2;
     double iA1, iA2;  // 1/A1, 1/A2 (mixed-precision pressure recovery)
+    double pinf1, pinf2;  // B1/(A1 + 1), B2/(A2 + 1) (the relaxation's admissibility check)
     double Ak[kMaxPhases], Bk[kMaxPhases], Ck[kMaxPhases], Dk[kMaxPhases];
 };
 

@@ -143,13 +143,38 @@ __device__ __forceinline__ int relax_safeguarded2(double AlphaR[2], const double
     return kPathSolve;
 }
 
-// Relax the state U of one cell in place (SixEq<D> layout).
-template <int D>
+// Relax the state U of one cell in place (SixEq<D> layout). FAST (the mixed form): the same FP64
+// root solve with the velocities and phase pressures of the entry state formed by multiplying with
+// reciprocals (one division for 1/rho, the precomputed 1/A_k) and one reciprocal for the volume
+// fraction normalisation, instead of the reference's divisions; the plain form (FAST = false) keeps
+// the reference's operations to the bit.
+template <int D, bool FAST = false>
 __device__ __forceinline__ void relax_pressure(double* U, const Eos& e, double trace, unsigned int* err) {
     using M = SixEq<D>;
     constexpr int N = M::N;
     double W[N];
-    M::cons2prim(W, U, e, err);
+    if constexpr (FAST) {
+        const double rho = U[0] + U[1];
+        const double ir = 1.0 / rho;
+        double u[3];
+#pragma unroll
+        for (int d = 0; d < D; ++d) u[d] = U[2 + d] * ir;
+        const double k = ksum<D>(u);
+        const double al1 = U[M::IA], al2 = 1.0 - al1;
+        W[0] = U[0];
+        W[1] = U[1];
+#pragma unroll
+        for (int d = 0; d < D; ++d) W[2 + d] = u[d];
+        W[M::IA] = al1;
+        const double e1 = U[M::IE1] - (0.5 * U[0]) * k;
+        const double e2 = U[M::IE2] - (0.5 * U[1]) * k;
+        if (e.C1 > 0.0) W[M::IE1] = M::phase_p(e1, al1, U[0], e.A1, e.B1, e.C1, e.D1, err);
+        else W[M::IE1] = ((e1 - U[0] * e.D1) - al1 * e.B1) * e.iA1;
+        if (e.C2 > 0.0) W[M::IE2] = M::phase_p(e2, al2, U[1], e.A2, e.B2, e.C2, e.D2, err);
+        else W[M::IE2] = ((e2 - U[1] * e.D2) - al2 * e.B2) * e.iA2;
+    } else {
+        M::cons2prim(W, U, e, err);
+    }
     const double a1r1 = W[0], a2r2 = W[1];
     const double alpha1 = W[M::IA];
     const double alpha2 = 1.0 - alpha1;
@@ -203,15 +228,21 @@ __device__ __forceinline__ void relax_pressure(double* U, const Eos& e, double t
         else if (!isnan(alpha1R) && isnan(alpha2R))
             alpha2R = 1.0 - alpha1R;
         const double sum = alpha1R + alpha2R;
-        alpha1R /= sum;
-        alpha2R /= sum;
+        if constexpr (FAST) {
+            const double is = 1.0 / sum;
+            alpha1R *= is;
+            alpha2R *= is;
+        } else {
+            alpha1R /= sum;
+            alpha2R /= sum;
+        }
         pR = (((A1 * a1p1 + A2 * a2p2) + B1 * (alpha1 - alpha1R)) + B2 * (alpha2 - alpha2R)) /
              (A1 * alpha1R + A2 * alpha2R);
         a1p1R = alpha1R * pR;
         a2p2R = alpha2R * pR;
     }
-    const double pinf_1 = B1 / (A1 + 1.0);
-    const double pinf_2 = B2 / (A2 + 1.0);
+    const double pinf_1 = e.pinf1;  // B1 / (A1 + 1), formed on the host with the same operation
+    const double pinf_2 = e.pinf2;
     double pinf_m = DBL_MAX, pinf_scale = 0.0;
     if (alpha1 > 0.0) { pinf_m = dmin(pinf_m, pinf_1); pinf_scale = dmax(pinf_scale, fabs(pinf_1)); }
     if (alpha2 > 0.0) { pinf_m = dmin(pinf_m, pinf_2); pinf_scale = dmax(pinf_scale, fabs(pinf_2)); }

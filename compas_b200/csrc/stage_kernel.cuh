@@ -569,7 +569,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                     }
                 }
                 if constexpr (M::KIND == kModelSix) {
-                    if (a.relax) relax_pressure<D>(out, a.e, a.trace, err);
+                    if (a.relax) relax_pressure<D, MIX>(out, a.e, a.trace, err);
                 }
                 bool bad = false;
 #pragma unroll

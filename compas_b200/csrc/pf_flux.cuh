@@ -31,7 +31,10 @@ __device__ __forceinline__ double pf_face_gq(const StageArgs& a, int d, int i, i
     return a.gq[d][q];
 }
 
-template <int D>
+// MIX: the mixed form takes the face velocities and pressures from the FP32 primitives (the
+// phase-field flux arithmetic is FP32-grade there; the masses and volume fractions stay the FP64 face
+// states); the plain form converts in FP64 as the reference does.
+template <int D, bool MIX = false>
 __device__ __forceinline__ void pf_face_flux(double* F, const double* UL, const double* UR, double gq, const Eos& e,
                                              unsigned int* err) {
     using M = FiveEq<D>;
@@ -48,8 +51,19 @@ __device__ __forceinline__ void pf_face_flux(double* F, const double* UL, const 
     const double J2 = f_downwind(a2L, a2R, g2) * a1u * g2;
     // mixture fluxes of momentum and energy
     double WL[N], WR[N];
-    M::cons2prim(WL, UL, e, err);
-    M::cons2prim(WR, UR, e, err);
+    if constexpr (MIX) {
+        float wl[N], wr[N];
+        M::cons2prim_f32(wl, UL, e);
+        M::cons2prim_f32(wr, UR, e);
+#pragma unroll
+        for (int n = 0; n < N; ++n) {
+            WL[n] = wl[n];
+            WR[n] = wr[n];
+        }
+    } else {
+        M::cons2prim(WL, UL, e, err);
+        M::cons2prim(WR, UR, e, err);
+    }
     const double Mf = J1r1 + J2r2;
     double ud[3];
 #pragma unroll

@@ -388,7 +388,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                     }
                 }
                 if constexpr (PFX) {
-                    pf_face_flux<D>(F, UL, UR, pf_face_gq(a, d, gi, gj, gk), a.e, err);
+                    pf_face_flux<D, MIX>(F, UL, UR, pf_face_gq(a, d, gi, gj, gk), a.e, err);
                     fnc[0] = 0.0;
                     cm = 0.0;
                 } else {
@@ -437,7 +437,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                 } else {
                     float cmf;
                     if constexpr (PFX) {
-                        pf_face_flux<D>(F, UL, UR, pf_face_gq(a, d, gi, gj, gk), a.e, err);
+                        pf_face_flux<D, MIX>(F, UL, UR, pf_face_gq(a, d, gi, gj, gk), a.e, err);
                         fnc[0] = 0.0;
                         cmf = 0.0f;
                     } else if constexpr (M::KIND == kModelFive) {

@@ -530,7 +530,9 @@ dim3 mg_grid(const PfDims& m) { return dim3((unsigned)((m.n[0] + kRowThreads - 1
 // four launches and four passes over the level by one.
 constexpr int kRbTX = 32, kRbTY = 16, kRbH = 4, kRbPasses = kRbH;
 constexpr int kRbW = kRbTX + 2 * kRbH, kRbHt = kRbTY + 2 * kRbH, kRbCells = kRbW * kRbHt;
-constexpr int kRbThreads = 256;
+// one thread per cell of the tile and its halo: every thread's seven loads are in flight at once
+// (the load phase is latency-bound otherwise), and every pass is one update per thread
+constexpr int kRbThreads = kRbCells;
 constexpr size_t kRbSmem = sizeof(double) * 7 * (size_t)kRbCells + sizeof(unsigned char) * kRbCells;
 
 __global__ void __launch_bounds__(kRbThreads) k_mg_rb4_2d(MgLevel L, int first_color) {

@@ -303,8 +303,11 @@ static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
     if (p->id_limiter != 5 && p->id_limiter != 6)
         return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.Scheme: this build runs WENO5 and WENO5B");
     if (p->id_riemann != 2) return fail(COMPAS_B200_EUNSUPPORTED, "Physics.RiemannSolver: this build runs HLLC");
-    if (p->phase_field && p->physics != COMPAS_B200_FIVEEQS)
-        return fail(COMPAS_B200_EUNSUPPORTED, "PhaseField.phase_field = 1: this engine runs the FIVEEQS Phase-Field step");
+    if (p->phase_field && p->physics == COMPAS_B200_FIVEEQS_NPHASE)
+        return fail(COMPAS_B200_EUNSUPPORTED, "PhaseField.phase_field = 1: this engine runs the FIVEEQS and SIXEQS "
+                                              "Phase-Field step");
+    if (p->physics == COMPAS_B200_FIVEEQS && p->pf_phase2flux != 1)
+        return fail(COMPAS_B200_EUNSUPPORTED, "PhaseField.ID_FluxPhase2Flux: FIVEEQS runs the mixture formulation (1)");
     if (p->phase_field && p->pf_mechanism != 1 && p->pf_mechanism != 3)
         return fail(COMPAS_B200_EUNSUPPORTED, "PhaseField.Mechanism: this engine runs CAC-Adv and ACDI");
     if (p->phase_field && p->pf_explicit_rc && p->pf_mechanism == 1)
@@ -558,6 +561,7 @@ static StageArgs base_args(const compas_b200_parm* p, const compas_b200_geom* g)
     a.id_k = p->source_term;
     a.relax = (p->physics == COMPAS_B200_SIXEQS) ? p->relaxation : 0;
     a.trace = p->relax_trace;
+    a.pf_phasic = (p->pf_phase2flux == 0);
     a.thinc.use_normal = p->thinc_use_normal;
     a.thinc.eps = p->thinc_eps;
     a.thinc.beta = p->thinc_beta;
@@ -715,6 +719,9 @@ int compas_b200_parm_init_nphase(compas_b200_parm* p, int physics, int dim, int 
     // PhaseField_Parameter defaults (include/Physics_PhaseField/PhaseField_Parameter.H:27-50): the
     // inputs default mechanism is CAC-Adv (:52)
     p->pf_mechanism = 1;
+    // PhaseField.ID_FluxPhase2Flux: the mixture formulation, except for the six-equation model whose
+    // Parm.H selects the phasic one (exec/_Tests/Advection/prob/Parm.H:48-50)
+    p->pf_phase2flux = (physics == COMPAS_B200_SIXEQS) ? 0 : 1;
     p->pf_eta_factor = 2.0;
     p->pf_eta_multiplier = 1.0;
     p->pf_cfl = 0.4;
@@ -877,6 +884,15 @@ int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value
     }
     if (k == "PhaseField.phase_field") { if (!parse_int(value, &ix)) return bad("0, 1"); p->phase_field = ix ? 1 : 0; return 0; }
     if (k == "PhaseField.ID_ExplicitRC") { if (!parse_int(value, &ix) || ix < 0 || ix > 1) return bad("0, 1"); p->pf_explicit_rc = ix; return 0; }
+    if (k == "PhaseField.ID_FluxPhase2Flux") {
+        // include/Physics_PhaseField/PhaseField_Parameter.H:53 (0 phasic, 1 mixture formulation)
+        if (!parse_int(value, &ix) || ix < 0 || ix > 1) return bad("0, 1");
+        if (ix == 0 && p->physics != COMPAS_B200_SIXEQS)
+            return fail(COMPAS_B200_EUNSUPPORTED, k + " = 0: this engine runs the phasic formulation for SIXEQS "
+                                                      "(the mixture formulation, 1, for FIVEEQS)");
+        p->pf_phase2flux = ix;
+        return 0;
+    }
     if (k == "PhaseField.max_step") { if (!parse_int(value, &ix)) return bad("an integer"); p->pf_max_step = ix; return 0; }
     {
         struct PKey { const char* name; double* dst; };
@@ -894,8 +910,7 @@ int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value
     // options the engine runs only at their reference defaults (PhaseField_Parameter.H:40-48)
     {
         struct OKey { const char* name; int only; };
-        const OKey okeys[] = {{"PhaseField.ID_Flux", 0}, {"PhaseField.ID_FluxPhase2Flux", 1},
-                              {"PhaseField.ID_Weight", 0}, {"PhaseField.ID_Potential", 0},
+        const OKey okeys[] = {{"PhaseField.ID_Flux", 0}, {"PhaseField.ID_Weight", 0}, {"PhaseField.ID_Potential", 0},
                               {"PhaseField.ID_DegenerateMobility", 0}, {"PhaseField.ID_Formulation", 1},
                               {"PhaseField.Switch_Step", 0}};
         for (const auto& ok : okeys)
@@ -1020,8 +1035,8 @@ int compas_b200_pf_compute_dUdt(const compas_b200_parm* p, const compas_b200_geo
                                 void* stream) {
     int rc = check_args(p, g);
     if (rc) return rc;
-    if (p->physics != COMPAS_B200_FIVEEQS)
-        return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field right-hand side is the FIVEEQS model's");
+    if (p->physics == COMPAS_B200_FIVEEQS_NPHASE)
+        return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field right-hand side is the two-phase models'");
     if (!U || !dUdt || !gq0 || !gq1 || (p->dim == 3 && !gq2)) return fail(COMPAS_B200_EARG, "null argument");
     StageArgs a = base_args(p, g);
     a.Us = U;
@@ -1038,8 +1053,8 @@ int compas_b200_pf_rk3_stage(const compas_b200_parm* p, const compas_b200_geom* 
                              const double* gq1, const double* gq2, unsigned int* err_dev, void* stream) {
     int rc = check_args(p, g);
     if (rc) return rc;
-    if (p->physics != COMPAS_B200_FIVEEQS)
-        return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field right-hand side is the FIVEEQS model's");
+    if (p->physics == COMPAS_B200_FIVEEQS_NPHASE)
+        return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field right-hand side is the two-phase models'");
     if (stage < 0 || stage > 2) return fail(COMPAS_B200_EARG, "stage must be 0, 1 or 2");
     if (!Us || !Unew || !dt_dev || (stage > 0 && !Uold) || !gq0 || !gq1 || (p->dim == 3 && !gq2))
         return fail(COMPAS_B200_EARG, "null argument");
@@ -1061,8 +1076,8 @@ int compas_b200_pf_grad_q(const compas_b200_parm* p, const compas_b200_geom* g, 
                           double* gq0, double* gq1, double* gq2, double* info, void* stream) {
     int rc = check_args(p, g);
     if (rc) return rc;
-    if (p->physics != COMPAS_B200_FIVEEQS)
-        return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field step is the FIVEEQS model's");
+    if (p->physics == COMPAS_B200_FIVEEQS_NPHASE)
+        return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field step is the two-phase models'");
     if (!U || !gq0 || !gq1 || (p->dim == 3 && !gq2)) return fail(COMPAS_B200_EARG, "null argument");
     if (!(dt > 0.0)) return fail(COMPAS_B200_EARG, "dt must be positive");
     compas_b200_geom gg = *g;

@@ -37,7 +37,8 @@ struct LaunchShape {
 template <class M, int SCHEME, bool MIX, int VAR, int SH>
 static cudaError_t launch_stage_v(const StageArgs& a, cudaStream_t st) {
     using S = LaunchShape<M, SH>;
-    using T = TileShape<M, S::TS, S::TS, S::TZ, typename std::conditional<MIX, float, double>::type>;
+    using T = TileShape<M, S::TS, S::TS, S::TZ, typename std::conditional<MIX, float, double>::type, false,
+                        VAR == kVarPhaseField>;
     auto kern = stage_kernel<M, SCHEME, MIX, VAR, S::TS, S::TS, S::TZ, S::NT, S::MINB>;
     static bool attr_set = false;
     if (!attr_set) {
@@ -85,10 +86,7 @@ static cudaError_t launch_stage_var(const KernelChoice& k, const StageArgs& a, c
         if (k.phase_field || k.thinc) return cudaErrorNotSupported;
     } else {
         // the THINC and Phase-Field variants run at shape 0
-        if (k.phase_field) {
-            if constexpr (M::KIND == kModelFive) return launch_stage_v<M, SCHEME, MIX, kVarPhaseField, 0>(a, st);
-            else return cudaErrorNotSupported;
-        }
+        if (k.phase_field) return launch_stage_v<M, SCHEME, MIX, kVarPhaseField, 0>(a, st);
         if (k.thinc) return launch_stage_v<M, SCHEME, MIX, kVarThinc, 0>(a, st);
     }
     switch (k.shape) {

@@ -13,7 +13,7 @@ struct TmaMaps;
 
 // Variant of the stage kernel: FiniteVolume.Scheme (5 WENO5, 6 WENO5B), precision (0 FP64, 1 mixed),
 // FiniteVolume.THINC (single-box kernel only), and the Phase-Field regularisation right-hand side
-// instead of the hyperbolic one (FIVEEQS, single-box kernel only). The N-phase model
+// instead of the hyperbolic one (FIVEEQS and SIXEQS, single-box kernel only). The N-phase model
 // (fiveeqn<dim>_<nphase>) runs WENO5 only.
 struct KernelChoice {
     int limiter;

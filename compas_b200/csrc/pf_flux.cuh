@@ -1,13 +1,21 @@
-// Phase-Field regularisation flux of one face (FIVEEQS, PhaseField.ID_Flux = 0 upwind/downwind,
-// PhaseField.ID_FluxPhase2Flux = 1 mixture formulation) from the reconstructed face states and the
-// face gradient of the regularisation potential Q.
+// Phase-Field regularisation flux of one face from the reconstructed face states and the face gradient
+// of the regularisation potential Q (PhaseField.ID_Flux = 0, upwind/downwind): FIVEEQS in the mixture
+// formulation (PhaseField.ID_FluxPhase2Flux = 1), SIXEQS in the phasic (0) or mixture (1) formulation
+// with the non-conservative face terms of its phase-energy exchange.
 //
-// Reference:
+// Reference (FIVEEQS):
 //   FVM_Conservative2FluxPhaseField_K  include/Operators_Compressible5Eq_PhaseField/FVM_Conservative2FluxPhaseField_K_Compressible5Eq_PhaseField.H:15-69
 //   FluxPhaseField                     include/Physics_Compressible5Eq_PhaseField/FluxPhaseField_Compressible5Eq_PhaseField.H
 //   phase fluxes J_k rho_k, J_k (UD)   include/Physics_Compressible_TwoPhase_PhaseField/FluxPhasePhaseField_UD_Compressible_TwoPhase_PhaseField.H
 //   mixture flux                       include/Physics_Compressible5Eq_PhaseField/FluxPhaseField_Mixture_Compressible5Eq_PhaseField.H
 //   f_Upwind / f_Downwind              include/Operators_FV/f_Upwind.H, f_Downwind.H
+// Reference (SIXEQS):
+//   FVM_Conservative2FluxPhaseField_K  include/Operators_Compressible6Eq_PhaseField/FVM_Conservative2FluxPhaseField_K_Compressible6Eq_PhaseField.H:13-66
+//   FluxPhaseField                     include/Physics_Compressible6Eq_PhaseField/FluxPhaseField_Compressible6Eq_PhaseField.H:10-72
+//   phasic face states                 include/Physics_Compressible6Eq/Conservative2ConservativePhase_Compressible6Eq.H
+//   phase fluxes (UD), FluxNC terms    include/Physics_Compressible6Eq_PhaseField/FluxPhasePhaseField_UD_Compressible6Eq_PhaseField.H
+//   phasic formulation                 include/Physics_Compressible6Eq/VectorPhase2Vector_Compressible6Eq.H
+//   mixture formulation                include/Physics_Compressible6Eq_PhaseField/FluxPhaseField_Mixture_Compressible6Eq_PhaseField.H
 // The flux is stored negated (the face array of PhaseField_ComputeFaceFluxes holds -fhat,
 // source/Class_Compressible_PhaseField.cpp:770-855), so the stage kernel's surface integral applies.
 #pragma once
@@ -82,6 +90,115 @@ __device__ __forceinline__ void pf_face_flux(double* F, const double* UL, const 
     for (int c = 0; c < D; ++c) F[2 + c] = -(Mf * ud[c]);
     F[M::IE] = -(MeK + J1r1e1 + J2r2e2);
     F[M::IA] = -J1;
+}
+
+// SIXEQS: F (stored negated) and the four non-conservative face terms fnc = (J1 rho1, J2 rho2,
+// J1 rho1 EK, J2 rho2 EK). phasic: 1 the phasic formulation (each phase's mass, momentum, energy and
+// volume fraction carried by its own flux), 0 the mixture formulation. MIX as in pf_face_flux: the face
+// velocities and phase pressures come from the FP32 primitives, the masses and volume fraction stay the
+// FP64 face states.
+template <int D, bool MIX = false>
+__device__ __forceinline__ void pf_face_flux_six(double* F, double* fnc, const double* UL, const double* UR, double gq,
+                                                 const Eos& e, int phasic, unsigned int* err) {
+    using M = SixEq<D>;
+    constexpr int N = M::N;
+    double W[2][N];
+    if constexpr (MIX) {
+        float w[N];
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            const double* U = s ? UR : UL;
+            M::cons2prim_f32(w, U, e);
+#pragma unroll
+            for (int n = 0; n < N; ++n) W[s][n] = w[n];
+            W[s][0] = U[0];
+            W[s][1] = U[1];
+            W[s][M::IA] = U[M::IA];
+        }
+    } else {
+        M::cons2prim(W[0], UL, e, err);
+        M::cons2prim(W[1], UR, e, err);
+    }
+    // phasic states of the two sides: alpha_k rho_k, alpha_k rho_k u_d, alpha_k rho_k E_k, alpha_k
+    double r1[2], r2[2], m1[2][3], m2[2][3], E1[2], E2[2], a1[2], a2[2];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        a1[s] = W[s][M::IA];
+        a2[s] = 1.0 - a1[s];
+        r1[s] = W[s][0];
+        r2[s] = W[s][1];
+        const double e1 = M::phase_e(W[s][M::IE1], a1[s], r1[s], e.A1, e.B1, e.C1, e.D1, err);
+        const double e2 = M::phase_e(W[s][M::IE2], a2[s], r2[s], e.A2, e.B2, e.C2, e.D2, err);
+        const double k = ksum<D>(W[s] + 2);
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+            m1[s][c] = r1[s] * W[s][2 + c];
+            m2[s][c] = r2[s] * W[s][2 + c];
+        }
+        E1[s] = e1 + (0.5 * r1[s]) * k;
+        E2[s] = e2 + (0.5 * r2[s]) * k;
+    }
+    // phase fluxes: phase 1 carries Q, phase 2 -Q, each weighted by the upwind volume fraction of the
+    // other phase and the downwind value of the carried quantity
+    const double g1 = gq, g2 = -g1;
+    const double a2u = f_upwind(a2[0], a2[1], g1);
+    const double a1u = f_upwind(a1[0], a1[1], g2);
+    auto j1 = [&](double l, double r) { return f_downwind(l, r, g1) * a2u * g1; };
+    auto j2 = [&](double l, double r) { return f_downwind(l, r, g2) * a1u * g2; };
+    const double J1r1 = j1(r1[0], r1[1]);
+    const double J2r2 = j2(r2[0], r2[1]);
+    // kinetic energy per unit mass of the mixture velocity of the phasic states
+    double uL[3], uR[3];
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+        uL[c] = (m1[0][c] + m2[0][c]) / (r1[0] + r2[0]);
+        uR[c] = (m1[1][c] + m2[1][c]) / (r1[1] + r2[1]);
+    }
+    const double EKL = 0.5 * ksum<D>(uL), EKR = 0.5 * ksum<D>(uR);
+    fnc[0] = J1r1;
+    fnc[1] = J2r2;
+    fnc[2] = j1(r1[0] * EKL, r1[1] * EKR);
+    fnc[3] = j2(r2[0] * EKL, r2[1] * EKR);
+    const double J1 = j1(a1[0], a1[1]);
+    const double J2 = j2(a2[0], a2[1]);
+    F[0] = -J1r1;
+    F[1] = -J2r2;
+    F[M::IA] = -J1;
+    if (phasic) {
+#pragma unroll
+        for (int c = 0; c < D; ++c) F[2 + c] = -(j1(m1[0][c], m1[1][c]) + j2(m2[0][c], m2[1][c]));
+        F[M::IE1] = -j1(E1[0], E1[1]);
+        F[M::IE2] = -j2(E2[0], E2[1]);
+    } else {
+        const double Mf = J1r1 + J2r2;
+        double ud[3];
+#pragma unroll
+        for (int c = 0; c < D; ++c) ud[c] = f_downwind(W[0][2 + c], W[1][2 + c], Mf);
+        const double eK = 0.5 * ksum<D>(ud);
+        const double pL = W[0][M::IE1] + W[0][M::IE2], pR = W[1][M::IE1] + W[1][M::IE2];
+        const double p1 = f_downwind(pL, pR, J1);
+        const double J1phi = (e.C1 > 0.0) ? J1 - e.C1 * J1r1 : J1;
+        const double J1r1e1 = e.A1 * J1phi * p1 + e.B1 * J1phi + e.D1 * J1r1;
+        const double p2 = f_downwind(pL, pR, J2);
+        const double J2phi = (e.C2 > 0.0) ? J2 - e.C2 * J2r2 : J2;
+        const double J2r2e2 = e.A2 * J2phi * p2 + e.B2 * J2phi + e.D2 * J2r2;
+#pragma unroll
+        for (int c = 0; c < D; ++c) F[2 + c] = -(Mf * ud[c]);
+        F[M::IE1] = -(J1r1 * eK + J1r1e1);
+        F[M::IE2] = -(J2r2 * eK + J2r2e2);
+    }
+}
+
+// The Phase-Field face fluxes of model M (F stored negated; fnc the model's NCPF face terms).
+template <class M, bool MIX>
+__device__ __forceinline__ void pf_face_fluxes(double* F, double* fnc, const double* UL, const double* UR, double gq,
+                                               const Eos& e, int phasic, unsigned int* err) {
+    if constexpr (M::KIND == kModelSix) {
+        pf_face_flux_six<M::D, MIX>(F, fnc, UL, UR, gq, e, phasic, err);
+    } else {
+        pf_face_flux<M::D, MIX>(F, UL, UR, gq, e, err);
+        fnc[0] = 0.0;
+    }
 }
 
 }  // namespace compas

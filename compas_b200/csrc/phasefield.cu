@@ -1066,7 +1066,7 @@ int pf_create(const compas_b200_parm* p, const compas_b200_geom* g, PfLevel** ou
     for (int d = 0; d < p->dim; ++d) per[d] = (g->lo_bc[d] == 0);
     pf->m = make_dims(p->dim, g->n, g->dx, per);
     const PfDims& m = pf->m;
-    pf->ia = 3 + p->dim;
+    pf->ia = (p->physics == COMPAS_B200_SIXEQS ? 4 : 3) + p->dim;  // alpha1, the last component
     pf->ung = g->ng;
     pf->ugz = (p->dim == 3) ? g->ng : 0;
     pf->upx = g->n[0] + 2LL * g->ng;

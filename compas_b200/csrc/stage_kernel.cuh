@@ -63,6 +63,7 @@ struct StageArgs {
     double trace;
     Thinc thinc;               // used by the THINC kernels only
     const double* gq[3];       // Phase-Field kernels: face gradients of the potential Q per direction
+    int pf_phasic;             // Phase-Field kernels, six-equation model: 1 phasic, 0 mixture formulation
     int order;                 // tile traversal order (tile_coords): 0 x fastest, 1 bricks of tiles
 };
 
@@ -105,7 +106,8 @@ enum { kVarPlain = 0, kVarThinc = 1, kVarPhaseField = 2, kVarTma = 3 };
 
 namespace compas {
 
-template <class M, int TX, int TY, int TZ, class PT = double, bool TMA = false>
+// PF: the Phase-Field kernel, whose face buffer holds the model's NCPF non-conservative face terms.
+template <class M, int TX, int TY, int TZ, class PT = double, bool TMA = false, bool PF = false>
 struct TileShape {
     static constexpr int D = M::D;
     static constexpr int CELLS = TX * TY * TZ;
@@ -117,7 +119,7 @@ struct TileShape {
     static constexpr int HALO = 6 * HS;
     static constexpr int F0 = (TX + 1) * A0, F1 = (TY + 1) * A1, F2 = (TZ + 1) * A2;
     static constexpr int FMAX = (D == 3) ? (F0 > F1 ? (F0 > F2 ? F0 : F2) : (F1 > F2 ? F1 : F2)) : (F0 > F1 ? F0 : F1);
-    static constexpr int NB = M::N + M::NC;
+    static constexpr int NB = M::N + (PF ? M::NCPF : M::NC);
     // primitives (type PT) of the tile and of one halo slab pair, then the face buffer (FP64)
     static constexpr size_t PBYTES = sizeof(PT) * ((size_t)M::N * CELLS + (size_t)M::N * HALO);
     static constexpr size_t FOFF = (PBYTES + 15) / 16 * 16;
@@ -142,8 +144,8 @@ __device__ __forceinline__ void load_cons(double* U, const double* base, const G
 // relaxation in FP64.
 // VAR: kVarPlain - the hyperbolic right-hand side; kVarThinc - with THINC interface reconstruction
 // (FiniteVolume.THINC = 1); kVarPhaseField - the Phase-Field regularisation right-hand side (the
-// same face states, the regularisation flux of the face gradient a.gq instead of the Riemann flux,
-// no non-conservative terms; FIVEEQS).
+// same face states, the regularisation flux of the face gradient a.gq instead of the Riemann flux;
+// FIVEEQS without non-conservative terms, SIXEQS with its phase-energy exchange).
 // The work of one CTA on tile `tile` of the box described by `a` (tiles numbered x fastest).
 template <class M, int SCHEME, bool MIX, int VAR, int TX, int TY, int TZ, int NT>
 __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double* smem_d, const TmaMaps* tm = nullptr) {
@@ -152,12 +154,12 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
     constexpr bool PFX = (VAR == kVarPhaseField);
     constexpr bool TMA = (VAR == kVarTma);
     static_assert(!TMA || (M::D == 3 && MIX), "TMA halo staging: the 3D mixed form");
-    static_assert(!PFX || M::KIND == kModelFive, "the Phase-Field kernel is the five-equation model's");
+    static_assert(!PFX || M::KIND != kModelFiveN, "the Phase-Field kernel is the two-phase models'");
     static_assert(M::KIND != kModelFiveN || (SCHEME == 5 && !TH), "FIVEEQS_NPHASE runs WENO5 without THINC");
     constexpr bool NPH = (M::KIND == kModelFiveN);
     using PT = typename std::conditional<MIX, float, double>::type;
-    using T = TileShape<M, TX, TY, TZ, PT, TMA>;
-    constexpr int N = M::N, NC = M::NC, D = M::D, NB = T::NB;
+    using T = TileShape<M, TX, TY, TZ, PT, TMA, PFX>;
+    constexpr int N = M::N, NC = PFX ? M::NCPF : M::NC, D = M::D, NB = T::NB;
     constexpr int CELLS = T::CELLS, HALO = T::HALO, FMAX = T::FMAX;
     constexpr int R = (CELLS + NT - 1) / NT;
 
@@ -388,8 +390,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                     }
                 }
                 if constexpr (PFX) {
-                    pf_face_flux<D, MIX>(F, UL, UR, pf_face_gq(a, d, gi, gj, gk), a.e, err);
-                    fnc[0] = 0.0;
+                    pf_face_fluxes<M, MIX>(F, fnc, UL, UR, pf_face_gq(a, d, gi, gj, gk), a.e, a.pf_phasic, err);
                     cm = 0.0;
                 } else {
                     M::hllc(F, fnc, cm, UL, UR, a.e, d, a.id_k, err);
@@ -437,8 +438,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                 } else {
                     float cmf;
                     if constexpr (PFX) {
-                        pf_face_flux<D, MIX>(F, UL, UR, pf_face_gq(a, d, gi, gj, gk), a.e, err);
-                        fnc[0] = 0.0;
+                        pf_face_fluxes<M, MIX>(F, fnc, UL, UR, pf_face_gq(a, d, gi, gj, gk), a.e, a.pf_phasic,
+                                               err);
                         cmf = 0.0f;
                     } else if constexpr (M::KIND == kModelFive) {
                         fiveeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, a.e, d, a.id_k);
@@ -527,7 +528,20 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
 #pragma unroll
             for (int n = 0; n < N; ++n) L[n] = -acc[r][n];
             if constexpr (PFX) {
-                // the Phase-Field step has no non-conservative terms in the five-equation model
+                if constexpr (M::KIND == kModelSix) {
+                    // six-equation: the phase-energy exchange of the regularisation fluxes,
+                    // u . (J_k rho_k . grad u) = div(J_k rho_k EK) - EK div(J_k rho_k)
+                    // (include/Operators_Compressible6Eq_PhaseField/FVM_PhaseField_SurfaceIntegralNC_Compressible6Eq_PhaseField.H:15-85)
+                    const double a1r1 = W[0], a2r2 = W[1];
+                    const double rho = a1r1 + a2r2;
+                    const double EK = 0.5 * ksum<D>(W + 2);
+                    const double vg1 = acc[r][N + 2] - EK * acc[r][N];
+                    const double vg2 = acc[r][N + 3] - EK * acc[r][N + 1];
+                    const double x = (a1r1 / rho) * vg2 - (a2r2 / rho) * vg1;
+                    L[M::IE1] = L[M::IE1] + x;
+                    L[M::IE2] = L[M::IE2] + (-x);
+                }
+                // the five-equation model has no Phase-Field non-conservative terms
                 // (include/Operators_Compressible5Eq_PhaseField/FVM_PhaseField_SurfaceIntegralNC_Compressible5Eq_PhaseField.H)
             } else if constexpr (M::KIND == kModelFive) {
                 // five-equation: alpha1 += phi1 (1 + K1) div u*

@@ -75,10 +75,13 @@ typedef struct compas_b200_parm {
     int precision;
     /* PhaseField.* (include/Physics_PhaseField/PhaseField_Parameter.H:25-117) and LinearSystem.tol_rel
      * (include/Operators_LinearSystem/LinearSystem_Parameter.H:27): the regularisation step after
-     * every hyperbolic step (FIVEEQS) */
+     * every hyperbolic step (FIVEEQS, SIXEQS) */
     int phase_field;          /* PhaseField.phase_field */
     int pf_mechanism;         /* PhaseField.Mechanism: 1 CAC-Adv, 3 ACDI (the reference's ID_Mechanism) */
     int pf_explicit_rc;       /* PhaseField.ID_ExplicitRC: 0 elliptic solve, 1 explicit (flux-based only) */
+    int pf_phase2flux;        /* PhaseField.ID_FluxPhase2Flux: 0 phasic, 1 mixture formulation; default 1
+                               * for FIVEEQS (PhaseField_Parameter.H:53) and 0 for SIXEQS, whose Parm.H
+                               * sets it (exec/_Tests/Advection/prob/Parm.H:48-50); FIVEEQS runs 1 only */
     double pf_lambda;         /* PhaseField.Lambda (<= 0: 1) */
     double pf_eta;            /* PhaseField.Eta (<= 0: Eta_Multiplier x the largest cell size) */
     double pf_eta_factor;     /* PhaseField.Eta_Factor */
@@ -183,7 +186,7 @@ int compas_b200_rk3_stage(const compas_b200_parm* p, const compas_b200_geom* g, 
 int compas_b200_relaxation(const compas_b200_parm* p, const compas_b200_geom* g, double* U, unsigned int* err_dev,
                            void* stream);
 
-/* ---- Phase-Field regularisation (FIVEEQS; PhaseField.phase_field = 1) ---------------------------
+/* ---- Phase-Field regularisation (FIVEEQS, SIXEQS; PhaseField.phase_field = 1) -------------------
  * The level advance runs the Phase-Field step after every hyperbolic step by itself. The entry
  * points below expose its pieces to a host that keeps the reference's Phase-Field loop. Face arrays
  * gq_d are nodal in direction d: (n[0]+(d==0)) x (n[1]+(d==1)) x (n[2]+(d==2)) doubles, x fastest. */
@@ -200,13 +203,17 @@ int compas_b200_pf_grad_q(const compas_b200_parm* p, const compas_b200_geom* g, 
                           double* gq0, double* gq1, double* gq2, double* info, void* stream);
 
 /* Phase-Field right-hand side of the padded state U (ghosts filled) into dUdt: replaces
- * PhaseField_compute_dUdt_FV (source/Class_Compressible_PhaseField.cpp:950-1004). */
+ * PhaseField_compute_dUdt_FV (source/Class_Compressible_PhaseField.cpp:950-1004), SIXEQS with the
+ * phase-energy exchange of PhaseField_FVM_SurfaceIntegral_NC
+ * (include/Operators_Compressible6Eq_PhaseField/FVM_PhaseField_SurfaceIntegralNC_Compressible6Eq_PhaseField.H). */
 int compas_b200_pf_compute_dUdt(const compas_b200_parm* p, const compas_b200_geom* g, const double* U, double* dUdt,
                                 const double* gq0, const double* gq1, const double* gq2, unsigned int* err_dev,
                                 void* stream);
 
 /* One stage of PhaseField_ThirdOrderSSPRK (source/Class_Compressible_PhaseField.cpp:2619-2752): the
- * Phase-Field right-hand side of Us and the stage combination with Uold, dt read from device memory. */
+ * Phase-Field right-hand side of Us and the stage combination with Uold, dt read from device memory;
+ * SIXEQS with Physics.pressure_relaxation relaxes the new state as PhaseField_PostTimeStage does
+ * (source/Class_Compressible6Eq_PhaseField.cpp:61-70). */
 int compas_b200_pf_rk3_stage(const compas_b200_parm* p, const compas_b200_geom* g, int stage, const double* Us,
                              const double* Uold, double* Unew, const double* dt_dev, const double* gq0,
                              const double* gq1, const double* gq2, unsigned int* err_dev, void* stream);

@@ -87,7 +87,7 @@ class PfCase(ctypes.Structure):
         ("mechanism", ctypes.c_int), ("explicit_rc", ctypes.c_int),
         ("lambda_", ctypes.c_double), ("eta", ctypes.c_double), ("eta_factor", ctypes.c_double),
         ("eta_multiplier", ctypes.c_double), ("cfl", ctypes.c_double), ("max_step", ctypes.c_int),
-        ("tol_rel", ctypes.c_double),
+        ("tol_rel", ctypes.c_double), ("phase2flux", ctypes.c_int),
     ]
 
 
@@ -98,6 +98,7 @@ def pf_from(parm, tol_rel=None) -> PfCase:
     q.lambda_, q.eta, q.eta_factor = parm.pf_lambda, parm.pf_eta, parm.pf_eta_factor
     q.eta_multiplier, q.cfl, q.max_step = parm.pf_eta_multiplier, parm.pf_cfl, parm.pf_max_step
     q.tol_rel = parm.pf_tol_rel if tol_rel is None else tol_rel
+    q.phase2flux = parm.pf_phase2flux
     return q
 
 _cache: dict = {}

@@ -70,7 +70,7 @@ int cmp_advance(const cmp_case* c, double* U, int nsteps, double stop_time, doub
 /* Threads the library uses (OpenMP builds); 1 otherwise. */
 int cmp_threads(void);
 
-/* Phase-Field regularisation step (FIVEEQS; PhaseField_Evolve, source/Class_Compressible_PhaseField.cpp:
+/* Phase-Field regularisation step (FIVEEQS, SIXEQS; PhaseField_Evolve, source/Class_Compressible_PhaseField.cpp:
  * 424-595). The reference-header build implements it; the plain-C port returns -2. */
 typedef struct cmp_pf {
     int mechanism;          /* PhaseField ID_Mechanism: 1 CAC-Adv, 3 ACDI (PhaseField_Parameter.H:66-110) */
@@ -82,6 +82,7 @@ typedef struct cmp_pf {
     double cfl;             /* PhaseField.cfl */
     int max_step;           /* PhaseField.max_step */
     double tol_rel;         /* LinearSystem.tol_rel of the elliptic solve */
+    int phase2flux;         /* PhaseField.ID_FluxPhase2Flux: 0 phasic, 1 mixture (PhaseField_Parameter.H:53) */
 } cmp_pf;
 
 /* One Phase-Field step after a hyperbolic step of size dt: mechanism pseudo-time evolution, the

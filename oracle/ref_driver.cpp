@@ -47,6 +47,11 @@
 #include <Operators_FV.H>
 #include <Operators_FD.H>
 #include <Operators_Compressible6Eq.H>
+#include <Physics_PhaseField.H>
+#include <Operators_PhaseField.H>
+#include <Physics_Compressible_TwoPhase_PhaseField.H>
+#include <Physics_Compressible6Eq_PhaseField.H>
+#include <Operators_Compressible6Eq_PhaseField.H>
 #endif
 
 #include "oracle_api.h"
@@ -332,9 +337,9 @@ double est_dt(const cmp_case* c, double cmax) {
     return dt;
 }
 
-#if (PHYSICS == FIVEEQS)
+#if (PHYSICS == FIVEEQS || PHYSICS == SIXEQS)
 // ------------------------------------------------------------------------------------------------
-// Phase-Field regularisation step (FIVEEQS, NPHASE = 1), restating the orchestration of
+// Phase-Field regularisation step (FIVEEQS and SIXEQS, NPHASE = 1), restating the orchestration of
 //   PhaseField_Evolve              source/Class_Compressible_PhaseField.cpp:424-595
 //   PhaseFieldMechanism_Evolve     :596-711
 //   PhaseField_Mechanism (CAC)     :1006-1152, (flux-based) :1155-1232, PhaseField_ACDI :1494-1645
@@ -440,6 +445,7 @@ PfSetup pf_setup(const cmp_case* c, const cmp_pf* pf, const double* U) {
     s.P.Mobility *= 0.5 * s.P.Eta * vmax;  // non-CH mechanisms
     s.P.ID_Mechanism = pf->mechanism;
     s.P.ID_ExplicitRC = pf->explicit_rc;
+    s.P.ID_FluxPhase2Flux = pf->phase2flux;
     s.P.cfl = pf->cfl;
     s.P.max_step = pf->max_step;
     return s;
@@ -779,19 +785,24 @@ void pf_grad_q(const cmp_case* c, const cmp_pf* pf, const PfSetup& S, const doub
     }
 }
 
-// PhaseField_compute_dUdt_FV of a state with filled ghosts: fluxes -fhat on the faces, surface integral.
+// PhaseField_compute_dUdt_FV of a state with filled ghosts (PhaseField_ComputeFaceFluxes :770-855 and
+// PhaseField_FluxDivergence :858-947): fluxes -fhat and the non-conservative terms +fhatNC on the faces,
+// the surface integral, then PhaseField_FVM_SurfaceIntegral_NC (empty for FIVEEQS; the phase-energy
+// exchange for SIXEQS).
 void pf_compute_dudt(const cmp_case* c, const Parm& parm, const double* Ub, const std::vector<FField>& GQ,
                      double* dUdt) {
     Geo g(c);
     auto statein = g.view(const_cast<double*>(Ub), NSTATE);
     auto dudt = g.view(dUdt, NSTATE);
-    std::vector<std::vector<double>> F(AMREX_SPACEDIM);
-    std::vector<amrex::Array4<double>> fa(AMREX_SPACEDIM);
+    std::vector<std::vector<double>> F(AMREX_SPACEDIM), FNC(AMREX_SPACEDIM);
+    std::vector<amrex::Array4<double>> fa(AMREX_SPACEDIM), fnca(AMREX_SPACEDIM);
     amrex::Array4<amrex::Real const> sc = statein;
     for (int d = 0; d < AMREX_SPACEDIM; ++d) {
         const int fx = g.nx + (d == 0), fy = g.ny + (d == 1), fz = g.nz + (d == 2);
         F[d].assign((size_t)fx * fy * fz * NSTATE, 0.0);
         fa[d] = amrex::Array4<double>(F[d].data(), amrex::Dim3{0, 0, 0}, amrex::Dim3{fx, fy, fz}, NSTATE);
+        FNC[d].assign((size_t)fx * fy * fz * NC_TERMS, 0.0);
+        fnca[d] = amrex::Array4<double>(FNC[d].data(), amrex::Dim3{0, 0, 0}, amrex::Dim3{fx, fy, fz}, NC_TERMS);
         const FField& gq = GQ[d];
 #ifdef _OPENMP
 #pragma omp parallel for collapse(2) schedule(static)
@@ -807,11 +818,14 @@ void pf_compute_dudt(const cmp_case* c, const Parm& parm, const double* Ub, cons
                     FVM_Conservative2FluxPhaseField_K(i, j, k, fhat, fhatNC, cmax, sc, grad, parm, c->dx[d], d,
                                                       parm.FiniteVolume_Parm, parm.PhaseField_Parm);
                     for (int n = 0; n < NSTATE; ++n) fa[d](i, j, k, n) = -fhat[n];
+                    for (int n = 0; n < NC_TERMS; ++n) fnca[d](i, j, k, n) = fhatNC[n];
                 }
     }
     amrex::Array4<amrex::Real const> fx_c = fa[0], fy_c = fa[1];
+    amrex::Array4<amrex::Real const> fxnc_c = fnca[0], fync_c = fnca[1];
 #if (AMREX_SPACEDIM == 3)
     amrex::Array4<amrex::Real const> fz_c = fa[2];
+    amrex::Array4<amrex::Real const> fznc_c = fnca[2];
 #endif
     const double dx = c->dx[0], dy = c->dx[1];
 #if (AMREX_SPACEDIM == 3)
@@ -820,6 +834,8 @@ void pf_compute_dudt(const cmp_case* c, const Parm& parm, const double* Ub, cons
     cells(g, [&](int i, int j, int k) {
         for (int n = 0; n < NSTATE; ++n)
             FVM_SurfaceIntegral(i, j, k, n, dudt, statein, AMREX_D_DECL(fx_c, fy_c, fz_c), AMREX_D_DECL(dx, dy, dz));
+        PhaseField_FVM_SurfaceIntegral_NC(i, j, k, dudt, statein, AMREX_D_DECL(fxnc_c, fync_c, fznc_c),
+                                          AMREX_D_DECL(dx, dy, dz), parm);
     });
 }
 
@@ -849,6 +865,7 @@ int pf_advance(const cmp_case* c, const cmp_pf* pf, const PfSetup& S, double* U,
         fill_ghosts(c, Ub.data());
         pf_compute_dudt(c, parm, Ub.data(), GQ, L.data());
         for_valid(g, [&](long long q) { U[q] = 1.0 * Ub[q] + pfdt * L[q]; });
+        relax(c, parm, U);  // PhaseField_PostTimeStage (SIXEQS: Relaxation; nothing for FIVEEQS)
         std::memcpy(Ub.data(), U, tot * sizeof(double));
         fill_ghosts(c, Ub.data());
         pf_compute_dudt(c, parm, Ub.data(), GQ, L.data());
@@ -857,6 +874,7 @@ int pf_advance(const cmp_case* c, const cmp_pf* pf, const PfSetup& S, double* U,
             U[q] = 0.25 * Ub[q] + 0.75 * U0[q];
             U[q] += s2 * L[q];
         });
+        relax(c, parm, U);
         std::memcpy(Ub.data(), U, tot * sizeof(double));
         fill_ghosts(c, Ub.data());
         pf_compute_dudt(c, parm, Ub.data(), GQ, L.data());
@@ -865,6 +883,7 @@ int pf_advance(const cmp_case* c, const cmp_pf* pf, const PfSetup& S, double* U,
             U[q] = a3 * Ub[q] + b3 * U0[q];
             U[q] += s3 * L[q];
         });
+        relax(c, parm, U);
         pft += pfdt;
         ++steps;
         if (pft >= dt - 1.0e-6 * dt) break;
@@ -881,7 +900,7 @@ void pf_step(const cmp_case* c, const cmp_pf* pf, double* U, double dt, double* 
     if (info)
         for (int t = 0; t < 6; ++t) info[t] = loc[t];
 }
-#endif  // PHYSICS == FIVEEQS
+#endif  // PHYSICS == FIVEEQS || PHYSICS == SIXEQS
 
 #if (PHYSICS != FIVEEQS_NPHASE)
 #include "ref_amr.inc"
@@ -970,7 +989,7 @@ int cmp_advance(const cmp_case* c, double* U, int nsteps, double stop_time, doub
 }
 
 int cmp_pf_step(const cmp_case* c, const cmp_pf* pf, double* U, double dt, double* info) {
-#if (PHYSICS == FIVEEQS)
+#if (PHYSICS == FIVEEQS || PHYSICS == SIXEQS)
     return guarded([&] { pf_step(c, pf, U, dt, info); });
 #else
     (void)c; (void)pf; (void)U; (void)dt; (void)info;
@@ -980,7 +999,7 @@ int cmp_pf_step(const cmp_case* c, const cmp_pf* pf, double* U, double dt, doubl
 
 int cmp_pf_grad_q(const cmp_case* c, const cmp_pf* pf, const double* U, double dt, double* gq0, double* gq1,
                   double* gq2, double* info) {
-#if (PHYSICS == FIVEEQS)
+#if (PHYSICS == FIVEEQS || PHYSICS == SIXEQS)
     return guarded([&] {
         PfSetup S = pf_setup(c, pf, U);
         std::vector<FField> GQ;
@@ -997,7 +1016,7 @@ int cmp_pf_grad_q(const cmp_case* c, const cmp_pf* pf, const double* U, double d
 
 int cmp_advance_pf(const cmp_case* c, const cmp_pf* pf, double* U, int nsteps, double stop_time, double* t,
                    double* dts) {
-#if (PHYSICS == FIVEEQS)
+#if (PHYSICS == FIVEEQS || PHYSICS == SIXEQS)
     int taken = 0;
     int rc = guarded([&] {
         Parm parm = make_parm(c);

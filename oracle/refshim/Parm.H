@@ -46,7 +46,12 @@ struct Parm
 {
     Physics_Parameter Physics_Parm;
     FiniteVolume_Parameter FiniteVolume_Parm;
+#if (PHYSICS == SIXEQS)
+    // the six-equation model's Parm.H selects the phasic formulation of the Phase-Field fluxes
+    PhaseField_Parameter PhaseField_Parm{.ID_FluxPhase2Flux = 0};
+#else
     PhaseField_Parameter PhaseField_Parm;
+#endif
 
     int EOS = 1;
 

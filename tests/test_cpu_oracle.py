@@ -181,3 +181,31 @@ def test_amr_oracle_conserves_composite_totals_periodic():
     s1 = [amr.composite_sum(states, boxes, 2, 3, c, cov) for c in range(5)]
     for a, b in zip(s0, s1):
         assert abs(a - b) <= 1e-13 * abs(a)
+
+
+@pytest.mark.parametrize("form", ["0", "1"])
+def test_sixeq_phase_field_oracle_keeps_equilibrium_and_conserves(form):
+    """The six-equation Phase-Field step of the reference-header build (phasic 0 / mixture 1
+    formulation, CAC-Adv with the elliptic solve, relaxation after every stage) keeps a uniform
+    velocity and pressure across the interface and conserves the masses, momenta and total energy."""
+    phys, dim, inputs, geom, U = cases.advected_interface(n=32, dim=2, physics=cb.SIXEQS)
+    p, g = _parm_geom(phys, dim, dict(inputs, **{"PhaseField.phase_field": "1", "LinearSystem.tol_rel": "1e-13",
+                                                 "PhaseField.ID_FluxPhase2Flux": form}), geom)
+    if not have_ref(p.physics, p.dim):
+        pytest.skip("reference-header oracle not built")
+    from oracle.oracle import pf_from
+
+    V0 = cb.valid_view(U, p, g).copy()
+    Oracle("reference", p, g).advance_pf(U, pf_from(p), 3)
+    V = cb.valid_view(U, p, g)
+    rho = V[0] + V[1]
+    u, v = V[2] / rho, V[3] / rho
+    a1 = V[6]
+    k = 0.5 * (u * u + v * v)
+    pres = (V[4] - V[0] * k - a1 * p.B1) / p.A1 + (V[5] - V[1] * k - (1 - a1) * p.B2) / p.A2
+    assert np.max(np.abs(u - 1.0)) < 1e-8 and np.max(np.abs(v - 1.0)) < 1e-8
+    assert np.max(np.abs(pres / 1e5 - 1.0)) < 1e-7
+    for c in range(4):
+        assert abs(V[c].sum() - V0[c].sum()) <= 1e-13 * np.abs(V0[c]).sum(), c
+    E0 = V0[4].sum() + V0[5].sum()
+    assert abs(V[4].sum() + V[5].sum() - E0) <= 1e-12 * abs(E0)

@@ -279,32 +279,60 @@ __global__ void amr_cf_kernel(AmrCfArgs A) {
     }
 }
 
-// FluxRegister::Reflux and, for the five-equation model, RefluxSourceTerms: one thread per coarse cell,
-// its faces in list order
+// FluxRegister::Reflux and RefluxSourceTerms: one thread per coarse cell, its faces in list order.
+// Five-equation model: alpha1 -= xi phi1 (1 + K1) (source/Class_Compressible5Eq_PhaseField.cpp:77-160).
+// Six-equation model (source/Class_Compressible6Eq_PhaseField.cpp:85-195): the refluxed non-conservative
+// face terms give div u, div(u a1p1), div(u a2p2) corrections, applied to the phase energies and alpha1
+// with the primitives of the state before the reflux; with relax set, a cell the reflux changed is
+// relaxed again (RelaxRefluxedCells, :314-349), since the stage relaxation preceded the reflux.
 template <class M>
 __global__ void amr_reflux_kernel(const AmrCf* cf, const int* groups, int ngroups, const double* reg,
-                                  const double* reg_nc, AmrBufs B, int knew, double vol, Eos e, int id_k) {
+                                  const double* reg_nc, AmrBufs B, int knew, double vol, Eos e, int id_k, int relax,
+                                  double trace, unsigned int* err) {
     constexpr int N = M::N, NC = M::NC;
     for (int gi = blockIdx.x * blockDim.x + threadIdx.x; gi < ngroups; gi += gridDim.x * blockDim.x) {
         const int t0 = groups[gi], t1 = groups[gi + 1];
         const AmrCf& f0 = cf[t0];
         double* U = B.p[f0.cbox * 4 + knew];
         const long long S = B.S[f0.cbox];
+        double Uc[N], W[N];
+        for (int c = 0; c < N; ++c) Uc[c] = U[c * S + f0.cq];
+        M::cons2prim(W, Uc, e, nullptr);
         double src = 0.0;
-        if constexpr (NC == 1) {
-            double Uc[N], W[N];
-            for (int c = 0; c < N; ++c) Uc[c] = U[c * S + f0.cq];
-            M::cons2prim(W, Uc, e, nullptr);
-            src = M::kapila_factor(Uc, W, e, id_k, nullptr);
-        }
-        double xs = 0.0;
+        if constexpr (M::KIND == kModelFive) src = M::kapila_factor(Uc, W, e, id_k, nullptr);
+        double xs[NC];
         for (int t = t0; t < t1; ++t) {
             const double mult = cf[t].hi_side ? -1.0 : 1.0;
             for (int c = 0; c < N; ++c) U[c * S + f0.cq] += mult * reg[(long long)t * N + c] / vol;
-            const double xi = mult * reg_nc[(long long)t * NC] / vol;
-            xs = (t == t0) ? xi : xs + xi;
+            for (int c = 0; c < NC; ++c) {
+                const double xi = mult * reg_nc[(long long)t * NC + c] / vol;
+                xs[c] = (t == t0) ? xi : xs[c] + xi;
+            }
         }
-        if constexpr (NC == 1) U[M::IA * S + f0.cq] += -1.0 * (xs * src);
+        if constexpr (M::KIND == kModelFive) {
+            U[M::IA * S + f0.cq] += -1.0 * (xs[0] * src);
+        } else {
+            const double divv = -xs[0], dva1 = -xs[1], dva2 = -xs[2];
+            const double rho = W[0] + W[1];
+            const double vg1 = dva1 - W[M::IE1] * divv;
+            const double vg2 = dva2 - W[M::IE2] * divv;
+            const double x = W[1] / rho * vg1 - W[0] / rho * vg2;
+            U[M::IE1 * S + f0.cq] += x;
+            U[M::IE2 * S + f0.cq] += -x;
+            U[M::IA * S + f0.cq] += W[M::IA] * divv;
+            if (relax) {
+                double v[N];
+                bool changed = false;
+                for (int c = 0; c < N; ++c) {
+                    v[c] = U[c * S + f0.cq];
+                    changed = changed || (v[c] != Uc[c]);
+                }
+                if (changed) {
+                    relax_pressure<M::D>(v, e, trace, err);
+                    for (int c = 0; c < N; ++c) U[c * S + f0.cq] = v[c];
+                }
+            }
+        }
     }
 }
 

@@ -209,3 +209,28 @@ def test_sixeq_phase_field_oracle_keeps_equilibrium_and_conserves(form):
         assert abs(V[c].sum() - V0[c].sum()) <= 1e-13 * np.abs(V0[c]).sum(), c
     E0 = V0[4].sum() + V0[5].sum()
     assert abs(V[4].sum() + V[5].sum() - E0) <= 1e-12 * abs(E0)
+
+
+@pytest.mark.skipif(not have_ref(cb.SIXEQS, 2), reason="reference-header oracle not built here")
+def test_sixeq_amr_oracle_conserves_composite_totals_periodic():
+    """Six-equation multi-level advance of the oracle (flux registers with the three non-conservative
+    face terms, the phase-energy reflux source terms, relaxation of the refluxed cells): the composite
+    masses, momenta and total energy (the sum of the phase energies) are conserved on a periodic square."""
+    from compas_b200 import amr
+
+    kw = dict(n=16, dim=2, physics=cb.SIXEQS)
+    phys, dim, inputs, geom, _ = cases.advected_interface(**kw)
+    p, g = _parm_geom(phys, dim, inputs, geom)
+    boxes = amr.hierarchy((16, 16), 2, [((8, 8, 0), (23, 23, 0))], 8)
+    states = amr.box_states(cases.advected_interface, kw, (16, 16), 2, boxes)
+    cov = amr.covered_mask_fn(boxes, 2)
+
+    def totals(st):
+        s = [amr.composite_sum(st, boxes, 2, 3, c, cov) for c in range(6)]
+        return s[:4] + [s[4] + s[5]]
+
+    s0 = totals(states)
+    Oracle("reference", p, g).amr_advance(boxes, states, 4)
+    s1 = totals(states)
+    for a, b in zip(s0, s1):
+        assert abs(a - b) <= 1e-13 * abs(a)

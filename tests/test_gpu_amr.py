@@ -2,7 +2,8 @@
 (oracle/ref_amr.inc), and its invariants.
 
 Both sides run the same fixed hierarchy (refinement ratio 2, subcycling, flux registers with the
-five-equation non-conservative alpha1 source, average-down), the same coarse-fine interpolation and
+five-equation non-conservative alpha1 source or the six-equation phase-energy and alpha1 terms and the
+relaxation of the refluxed cells, average-down), the same coarse-fine interpolation and
 the reference's own face arithmetic, so the plain FP64 form is compared to the bit (the asserted bound
 is the north star's 1e-11 relative L-infinity per field and box). The coarse-fine operations follow
 AMReX's documented semantics on both sides; AMReX itself is not in the image, so they are not pinned
@@ -82,7 +83,13 @@ def test_one_level_of_boxes_equals_single_box_level():
     (cases.advected_disc, dict(n=32), (32, 32), [((16, 16, 0), (47, 47, 0)), ((40, 40, 0), (87, 87, 0))], 16, 5),
     (cases.advected_interface, dict(n=16, dim=3, physics=cb.FIVEEQS), (16, 16, 16),
      [((8, 8, 8), (23, 23, 23))], 8, 3),
-], ids=["bubble3lev_weno5b", "bubble2lev_weno5", "disc3lev_periodic", "sphere2lev_3d"])
+    (cases.advected_interface, dict(n=16, dim=2, physics=cb.SIXEQS), (16, 16),
+     [((8, 8, 0), (23, 23, 0)), ((24, 24, 0), (39, 39, 0))], 8, 4),
+    (cases.advected_interface, dict(n=16, dim=3, physics=cb.SIXEQS), (16, 16, 16),
+     [((8, 8, 8), (23, 23, 23))], 8, 3),
+    (cases.shock_droplet, dict(n=16), (16, 16, 16), [((8, 8, 8), (23, 23, 23))], 8, 3),
+], ids=["bubble3lev_weno5b", "bubble2lev_weno5", "disc3lev_periodic", "sphere2lev_3d", "sixeq_disc3lev_periodic",
+        "sixeq_sphere2lev_3d", "sixeq_droplet2lev_3d"])
 def test_amr_matches_oracle(case_fn, kw, domain, regions, mgs, steps):
     p, g, dim, boxes, states, got, dts, info, launches = _run(case_fn, kw, domain, regions, mgs, steps)
     assert info.status == 0 and info.steps == steps
@@ -101,6 +108,22 @@ def test_amr_composite_conservation_periodic():
         assert abs(s1 - s0) <= 1e-13 * abs(s0)
 
 
+def test_sixeq_amr_composite_conservation_periodic():
+    kw = dict(n=16, dim=2, physics=cb.SIXEQS)
+    p, g, dim, boxes, states, got, dts, info, _ = _run(
+        cases.advected_interface, kw, (16, 16), [((8, 8, 0), (23, 23, 0)), ((24, 24, 0), (39, 39, 0))], 8, 6)
+    assert info.status == 0
+    cov = amr.covered_mask_fn(boxes, 2)
+
+    def totals(st):
+        s = [amr.composite_sum(st, boxes, 2, 3, c, cov) for c in range(6)]
+        return s[:4] + [s[4] + s[5]]  # masses, momenta, total energy
+
+    for c, (s0, s1) in enumerate(zip(totals(states), totals(got))):
+        print(f"quantity {c}: composite total relative change {abs(s1 - s0) / abs(s0):.1e}")
+        assert abs(s1 - s0) <= 1e-13 * abs(s0)
+
+
 def test_amr_levels_use_one_list_launch_per_stage():
     # 3 levels x (1 + 2 + 4 substeps) x 3 stages of list launches plus fills, faces, reflux and average-down
     p, g, dim, boxes, states, got, dts, info, launches = _run(
@@ -113,9 +136,12 @@ def test_amr_levels_use_one_list_launch_per_stage():
     assert launches < 10 * stage_launches + 20
 
 
-def test_amr_mixed_error_vs_fp64():
-    args = (cases.shock_bubble, dict(nx=64, ny=32, scheme="WENO5B"), (64, 32),
-            [((40, 16, 0), (95, 47, 0)), ((96, 48, 0), (175, 79, 0))], 32, 6)
+@pytest.mark.parametrize("args", [
+    (cases.shock_bubble, dict(nx=64, ny=32, scheme="WENO5B"), (64, 32),
+     [((40, 16, 0), (95, 47, 0)), ((96, 48, 0), (175, 79, 0))], 32, 6),
+    (cases.shock_droplet, dict(n=16), (16, 16, 16), [((8, 8, 8), (23, 23, 23))], 8, 6),
+], ids=["fiveeq_bubble", "sixeq_droplet"])
+def test_amr_mixed_error_vs_fp64(args):
     _, _, dim, boxes, _, a, _, ia, _ = _run(*args, precision="mixed")
     _, _, _, _, _, b, _, ib, _ = _run(*args, precision="fp64")
     assert ia.status == 0 and ib.status == 0
@@ -127,5 +153,5 @@ def test_amr_mixed_error_vs_fp64():
         den += np.abs(Y).reshape(Y.shape[0], -1).sum(axis=1)
     e = num / den
     print("AMR mixed vs FP64 rel L1 per field:", np.array2string(e, precision=2))
-    for c in (0, 1, dim + 3):
+    for c in (0, 1, a[0].shape[0] - 1):  # masses and volume fraction
         assert e[c] <= 1e-5, e

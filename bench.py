@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--pf-steps", type=int, default=10)
     ap.add_argument("--force-kernel", default=None,
                     help="shape,order of the stage kernel instead of the autotuner's pick (profiling)")
+    ap.add_argument("--no-tma", action="store_true", help="stage the halo slabs with ordinary loads (profiling)")
     ap.add_argument("--no-triple", action="store_true")
     ap.add_argument("--triple-m", type=int, default=256, help="triple point side: 7m x 3m cells")
     ap.add_argument("--triple-steps", type=int, default=20)
@@ -229,19 +230,46 @@ def run_phase_field(args):
     import compas_b200 as cb
     from compas_b200 import cases
 
-    stream = torch.cuda.current_stream()
     phys, dim, inputs, geom, U = cases.shock_bubble(nx=2048, ny=1024, xp=torch, device="cuda")
+    workload = ("2D FIVEEQS shock-helium-bubble 2048x1024, WENO5B+HLLC+TVD-RK3, CAC-Adv Phase-Field "
+                "(implicit regularisation potential, Eta_Multiplier 1), reflective top/bottom, outflow left/right")
+    return _phase_field_line(args.pf_steps, phys, dim, inputs, geom, U, workload,
+                             {"PhaseField.phase_field": "1", "PhaseField.Mechanism": "CAC-Adv"})
+
+
+def run_phase_field_sixeq(args):
+    """3D six-equation shock-droplet 128^3 with the explicit ACDI Phase-Field step of the reference's
+    shock-droplet example (Eta_Multiplier 0.5, PhaseField.cfl 0.3, the phasic formulation of the
+    six-equation Parm.H), relaxation after every stage; timed as run_phase_field."""
+    import torch
+
+    from compas_b200 import cases
+
+    phys, dim, inputs, geom, U = cases.shock_droplet(n=128, xp=torch, device="cuda")
+    workload = ("3D SIXEQS shock-droplet 128^3, WENO5+HLLC+TVD-RK3 with relaxation, ACDI Phase-Field (explicit, "
+                "Eta_Multiplier 0.5, cfl 0.3, phasic formulation), outflow on every side")
+    return _phase_field_line(max(2, args.pf_steps // 2), phys, dim, inputs, geom, U, workload,
+                             {"PhaseField.phase_field": "1", "PhaseField.Mechanism": "ACDI",
+                              "PhaseField.ID_ExplicitRC": "1", "PhaseField.Eta_Multiplier": "0.5",
+                              "PhaseField.cfl": "0.3"})
+
+
+def _phase_field_line(K, phys, dim, inputs, geom, U, workload, pf_keys):
+    import torch
+
+    import compas_b200 as cb
+
+    stream = torch.cuda.current_stream()
     g = cb.make_geom(**geom)
-    cells = geom["n"][0] * geom["n"][1]
-    K, W = args.pf_steps, 2
-    out = {"workload": "2D FIVEEQS shock-helium-bubble 2048x1024, WENO5B+HLLC+TVD-RK3, CAC-Adv Phase-Field "
-                       "(implicit regularisation potential, Eta_Multiplier 1), reflective top/bottom, outflow left/right",
-           "cells": cells, "steps": K, "unit": UNIT + " per hyperbolic RK stage (Phase-Field step included)"}
+    cells = geom["n"][0] * geom["n"][1] * (geom["n"][2] if dim == 3 else 1)
+    W = 2
+    out = {"workload": workload, "cells": cells, "steps": K,
+           "unit": UNIT + " per hyperbolic RK stage (Phase-Field step included)"}
     for prec in ("mixed", "fp64"):
         for pf_on in (True, False):
             extra = {"compas_b200.precision": prec}
             if pf_on:
-                extra.update({"PhaseField.phase_field": "1", "PhaseField.Mechanism": "CAC-Adv"})
+                extra.update(pf_keys)
             p = cb.make_parm(phys, dim, dict(inputs, **extra))
             lv = cb.Level(p, g)
             lv.upload(U, stream=stream)
@@ -469,6 +497,8 @@ def run_ours(args, rank, world, dist):
     phys, dim, inputs, geom, U = cases.shock_droplet(n=n, xp=torch, device="cuda")
     g = cb.make_geom(**geom)
     cells = n ** 3
+    if args.no_tma:
+        inputs = dict(inputs, **{"compas_b200.tma": "0"})
     forms = {"mixed": cb.make_parm(phys, dim, dict(inputs, **{"compas_b200.precision": "mixed"})),
              "fp64": cb.make_parm(phys, dim, inputs)}
     if args.precision != "both":
@@ -508,7 +538,7 @@ def run_ours(args, rank, world, dist):
         assert info.steps == info0.steps + args.steps, (info0, info)
         ms[name] = max_over_ranks(t_ms)
         levels[name] = lv
-        tuned[name] = lv.kernel()
+        tuned[name] = lv.kernel() + (lv.tma(),)
     head = "mixed" if "mixed" in forms else "fp64"
     p = forms[head]
     value = replicas.whole_job_rate(cells, 3, args.steps, ms[head] / 1e3, world)
@@ -606,6 +636,7 @@ def run_ours(args, rank, world, dist):
             cpu = cpu_baseline(args.cpu_n, args.cpu_steps)
         batched = None if args.no_batched else run_batched(args)
         pf_res = None if args.no_phase_field else run_phase_field(args)
+        pf6_res = None if args.no_phase_field else run_phase_field_sixeq(args)
         amr_res = None if args.no_amr else run_amr(args)
         triple_res = None if args.no_triple else run_triple_point(args)
         line = {
@@ -617,7 +648,8 @@ def run_ours(args, rank, world, dist):
             "config": workload_config(n, {"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                                           "precision": head,
                                           "stage_kernel_autotuned": {
-                                              k: {"launch_shape": v[0], "tile_order": ("x fastest", "bricks")[v[1]]}
+                                              k: {"launch_shape": v[0], "tile_order": ("x fastest", "bricks")[v[1]],
+                                                  "tma_halo_staging": v[2]}
                                               for k, v in tuned.items()}}),
             "fp64_plain": ({"value": replicas.whole_job_rate(cells, 3, args.steps, ms["fp64"] / 1e3, world),
                             "ms_per_step": ms["fp64"] / args.steps,
@@ -637,6 +669,7 @@ def run_ours(args, rank, world, dist):
             "batched": batched,
             "serving": serving_res,
             "phase_field": pf_res,
+            "phase_field_sixeq": pf6_res,
             "amr": amr_res,
             "triple_point": triple_res,
         }

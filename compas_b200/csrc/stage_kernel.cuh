@@ -669,34 +669,49 @@ __device__ __forceinline__ int find_box(const int* off, int nb, int w) {
     return lo;
 }
 
+// The arguments of the current tile's box live in shared memory: the tile code reads them where it
+// needs them (as the single-box kernel reads its parameters from the constant bank) instead of
+// holding a per-thread copy of the grid and EOS in registers.
 template <class M, int SCHEME, bool MIX, int TX, int TY, int TZ, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) stage_list_kernel(ListArgs L) {
     extern __shared__ double smem_d[];
+    __shared__ StageArgs sa;
+    static_assert(sizeof(Grid) % 8 == 0 && sizeof(Eos) % 8 == 0, "word copies of the grid and EOS");
+    constexpr int GW = sizeof(Grid) / 8, EW = sizeof(Eos) / 8;
+    static_assert(GW + EW <= NT, "one word per thread");
     const int nb = *L.nbox;
     if (nb <= 0) return;
     const int total = L.tile_off[nb];
+    const int tid = threadIdx.x;
     for (int w = blockIdx.x; w < total; w += gridDim.x) {
         const int b = find_box(L.tile_off, nb, w);
         const BoxDesc& B = L.boxes[b];
         if (*B.done) continue;
-        StageArgs a;
-        a.g = B.g;
-        a.e = B.e;
-        a.mode = L.mode;
-        a.stage = L.stage;
-        a.Us = B.U[L.stage];
-        a.U0 = B.U[0];
-        a.Uout = (L.stage == 2 && B.out_last) ? B.out_last : B.U[(L.stage + 1) % 3];
-        a.dt = B.dt;
-        a.done = B.done;
-        a.cmax = B.cmax;
-        a.err = B.err;
-        a.id_k = B.id_k;
-        a.relax = B.relax;
-        a.trace = B.trace;
-        a.order = L.order;
-        __syncthreads();  // the previous tile's readers of shared memory are done
-        stage_tile<M, SCHEME, MIX, kVarPlain, TX, TY, TZ, NT>(a, w - L.tile_off[b], smem_d);
+        __syncthreads();  // the previous tile's readers of shared memory (and of sa) are done
+        if (tid < GW) {
+            reinterpret_cast<unsigned long long*>(&sa.g)[tid] = reinterpret_cast<const unsigned long long*>(&B.g)[tid];
+        } else if (tid < GW + EW) {
+            reinterpret_cast<unsigned long long*>(&sa.e)[tid - GW] =
+                reinterpret_cast<const unsigned long long*>(&B.e)[tid - GW];
+        } else if (tid == GW + EW) {
+            sa.mode = L.mode;
+            sa.stage = L.stage;
+            sa.Us = B.U[L.stage];
+            sa.U0 = B.U[0];
+            sa.Uout = (L.stage == 2 && B.out_last) ? B.out_last : B.U[(L.stage + 1) % 3];
+            sa.dt = B.dt;
+            sa.done = B.done;
+            sa.cmax = B.cmax;
+            sa.err = B.err;
+            sa.id_k = B.id_k;
+            sa.relax = B.relax;
+            sa.trace = B.trace;
+            sa.order = L.order;
+            sa.pf_phasic = 0;
+            for (int d = 0; d < 3; ++d) sa.gq[d] = nullptr;
+        }
+        __syncthreads();
+        stage_tile<M, SCHEME, MIX, kVarPlain, TX, TY, TZ, NT>(sa, w - L.tile_off[b], smem_d);
     }
 }
 

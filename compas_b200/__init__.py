@@ -70,6 +70,7 @@ class Parm(ctypes.Structure):
         ("phase_field", ctypes.c_int),
         ("pf_mechanism", ctypes.c_int),
         ("pf_explicit_rc", ctypes.c_int),
+        ("pf_flux", ctypes.c_int),
         ("pf_phase2flux", ctypes.c_int),
         ("pf_lambda", ctypes.c_double), ("pf_eta", ctypes.c_double),
         ("pf_eta_factor", ctypes.c_double), ("pf_eta_multiplier", ctypes.c_double),

@@ -562,6 +562,7 @@ static StageArgs base_args(const compas_b200_parm* p, const compas_b200_geom* g)
     a.relax = (p->physics == COMPAS_B200_SIXEQS) ? p->relaxation : 0;
     a.trace = p->relax_trace;
     a.pf_phasic = (p->pf_phase2flux == 0);
+    a.pf_hll = (p->pf_flux == 1);
     a.thinc.use_normal = p->thinc_use_normal;
     a.thinc.eps = p->thinc_eps;
     a.thinc.beta = p->thinc_beta;
@@ -884,6 +885,12 @@ int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value
     }
     if (k == "PhaseField.phase_field") { if (!parse_int(value, &ix)) return bad("0, 1"); p->phase_field = ix ? 1 : 0; return 0; }
     if (k == "PhaseField.ID_ExplicitRC") { if (!parse_int(value, &ix) || ix < 0 || ix > 1) return bad("0, 1"); p->pf_explicit_rc = ix; return 0; }
+    if (k == "PhaseField.ID_Flux") {
+        // include/Physics_PhaseField/PhaseField_Parameter.H:52 (0 upwind/downwind, 1 HLL)
+        if (!parse_int(value, &ix) || ix < 0 || ix > 1) return bad("0, 1");
+        p->pf_flux = ix;
+        return 0;
+    }
     if (k == "PhaseField.ID_FluxPhase2Flux") {
         // include/Physics_PhaseField/PhaseField_Parameter.H:53 (0 phasic, 1 mixture formulation)
         if (!parse_int(value, &ix) || ix < 0 || ix > 1) return bad("0, 1");
@@ -910,7 +917,7 @@ int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value
     // options the engine runs only at their reference defaults (PhaseField_Parameter.H:40-48)
     {
         struct OKey { const char* name; int only; };
-        const OKey okeys[] = {{"PhaseField.ID_Flux", 0}, {"PhaseField.ID_Weight", 0}, {"PhaseField.ID_Potential", 0},
+        const OKey okeys[] = {{"PhaseField.ID_Weight", 0}, {"PhaseField.ID_Potential", 0},
                               {"PhaseField.ID_DegenerateMobility", 0}, {"PhaseField.ID_Formulation", 1},
                               {"PhaseField.Switch_Step", 0}};
         for (const auto& ok : okeys)

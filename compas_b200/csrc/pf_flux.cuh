@@ -1,19 +1,24 @@
 // Phase-Field regularisation flux of one face from the reconstructed face states and the face gradient
-// of the regularisation potential Q (PhaseField.ID_Flux = 0, upwind/downwind): FIVEEQS in the mixture
-// formulation (PhaseField.ID_FluxPhase2Flux = 1), SIXEQS in the phasic (0) or mixture (1) formulation
-// with the non-conservative face terms of its phase-energy exchange.
+// of the regularisation potential Q, with the upwind/downwind (PhaseField.ID_Flux = 0) or the HLL (1)
+// phase fluxes: FIVEEQS in the mixture formulation (PhaseField.ID_FluxPhase2Flux = 1), SIXEQS in the
+// phasic (0) or mixture (1) formulation with the non-conservative face terms of its phase-energy
+// exchange.
 //
 // Reference (FIVEEQS):
 //   FVM_Conservative2FluxPhaseField_K  include/Operators_Compressible5Eq_PhaseField/FVM_Conservative2FluxPhaseField_K_Compressible5Eq_PhaseField.H:15-69
 //   FluxPhaseField                     include/Physics_Compressible5Eq_PhaseField/FluxPhaseField_Compressible5Eq_PhaseField.H
 //   phase fluxes J_k rho_k, J_k (UD)   include/Physics_Compressible_TwoPhase_PhaseField/FluxPhasePhaseField_UD_Compressible_TwoPhase_PhaseField.H
 //   mixture flux                       include/Physics_Compressible5Eq_PhaseField/FluxPhaseField_Mixture_Compressible5Eq_PhaseField.H
+//   phase fluxes (HLL)                 include/Physics_Compressible_TwoPhase_PhaseField/FluxPhasePhaseField_HLL_Compressible_TwoPhase_PhaseField.H,
+//                                      ConservativePhase2FluxPhasePhaseField_Compressible_TwoPhase_PhaseField.H
 //   f_Upwind / f_Downwind              include/Operators_FV/f_Upwind.H, f_Downwind.H
 // Reference (SIXEQS):
 //   FVM_Conservative2FluxPhaseField_K  include/Operators_Compressible6Eq_PhaseField/FVM_Conservative2FluxPhaseField_K_Compressible6Eq_PhaseField.H:13-66
 //   FluxPhaseField                     include/Physics_Compressible6Eq_PhaseField/FluxPhaseField_Compressible6Eq_PhaseField.H:10-72
 //   phasic face states                 include/Physics_Compressible6Eq/Conservative2ConservativePhase_Compressible6Eq.H
 //   phase fluxes (UD), FluxNC terms    include/Physics_Compressible6Eq_PhaseField/FluxPhasePhaseField_UD_Compressible6Eq_PhaseField.H
+//   phase fluxes (HLL), FluxNC terms   include/Physics_Compressible6Eq_PhaseField/FluxPhasePhaseField_HLL_Compressible6Eq_PhaseField.H,
+//                                      ConservativePhase2FluxPhasePhaseField_Compressible6Eq_PhaseField.H
 //   phasic formulation                 include/Physics_Compressible6Eq/VectorPhase2Vector_Compressible6Eq.H
 //   mixture formulation                include/Physics_Compressible6Eq_PhaseField/FluxPhaseField_Mixture_Compressible6Eq_PhaseField.H
 // The flux is stored negated (the face array of PhaseField_ComputeFaceFluxes holds -fhat,
@@ -28,6 +33,39 @@ __device__ __forceinline__ double f_upwind(double fL, double fR, double V) {
 __device__ __forceinline__ double f_downwind(double fL, double fR, double V) {
     return (V > 0.0) ? fR : ((V < 0.0) ? fL : 0.5 * (fL + fR));
 }
+
+// HLL phase flux of the Phase-Field step: with the phase velocities V1 = alpha2 G, V2 = -alpha1 G of
+// both sides, Sp = max(0, -V1L, -V2L, -V1R, -V2R) + 1e-10 and Sm = min(...) - 1e-10 (std::max / std::min
+// over the list, first extremum kept), and F = (Sp FL - Sm FR - Sp Sm (CR - CL)) / (Sp - Sm) per phase
+// quantity C with phase flux C V.
+struct PfHll {
+    double V1L, V2L, V1R, V2R, Sp, Sm, SpSm, den;
+    __device__ __forceinline__ PfHll(double a1L, double a1R, double gq) {
+        const double g1 = gq, g2 = -g1;
+        V1L = (1.0 - a1L) * g1;
+        V2L = a1L * g2;
+        V1R = (1.0 - a1R) * g1;
+        V2R = a1R * g2;
+        const double c[4] = {-V1L, -V2L, -V1R, -V2R};
+        double mx = 0.0, mn = 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            mx = (mx < c[i]) ? c[i] : mx;
+            mn = (c[i] < mn) ? c[i] : mn;
+        }
+        Sp = mx + 1.0e-10;
+        Sm = mn - 1.0e-10;
+        SpSm = Sp * Sm;
+        den = Sp - Sm;
+    }
+    // phase 1 (velocity V1) and phase 2 (V2) quantity with states cl, cr
+    __device__ __forceinline__ double p1(double cl, double cr) const {
+        return (Sp * (cl * V1L) - Sm * (cr * V1R) - SpSm * (cr - cl)) / den;
+    }
+    __device__ __forceinline__ double p2(double cl, double cr) const {
+        return (Sp * (cl * V2L) - Sm * (cr * V2R) - SpSm * (cr - cl)) / den;
+    }
+};
 
 // Q gradient of the face of direction d at (i,j,k) (face arrays nodal in d, x fastest).
 __device__ __forceinline__ double pf_face_gq(const StageArgs& a, int d, int i, int j, int k) {
@@ -44,19 +82,28 @@ __device__ __forceinline__ double pf_face_gq(const StageArgs& a, int d, int i, i
 // states); the plain form converts in FP64 as the reference does.
 template <int D, bool MIX = false>
 __device__ __forceinline__ void pf_face_flux(double* F, const double* UL, const double* UR, double gq, const Eos& e,
-                                             unsigned int* err) {
+                                             int hll, unsigned int* err) {
     using M = FiveEq<D>;
     constexpr int N = M::N;
-    // phase fluxes (the two phases carry Q and -Q)
+    // phase fluxes (the two phases carry Q and -Q) of the masses and volume fractions
     const double g1 = gq, g2 = -g1;
     const double a1L = UL[M::IA], a1R = UR[M::IA];
     const double a2L = 1.0 - a1L, a2R = 1.0 - a1R;
-    const double a2u = f_upwind(a2L, a2R, g1);
-    const double a1u = f_upwind(a1L, a1R, g2);
-    const double J1r1 = f_downwind(UL[0], UR[0], g1) * a2u * g1;
-    const double J2r2 = f_downwind(UL[1], UR[1], g2) * a1u * g2;
-    const double J1 = f_downwind(a1L, a1R, g1) * a2u * g1;
-    const double J2 = f_downwind(a2L, a2R, g2) * a1u * g2;
+    double J1r1, J2r2, J1, J2;
+    if (hll) {
+        const PfHll h(a1L, a1R, gq);
+        J1r1 = h.p1(UL[0], UR[0]);
+        J2r2 = h.p2(UL[1], UR[1]);
+        J1 = h.p1(a1L, a1R);
+        J2 = h.p2(a2L, a2R);
+    } else {
+        const double a2u = f_upwind(a2L, a2R, g1);
+        const double a1u = f_upwind(a1L, a1R, g2);
+        J1r1 = f_downwind(UL[0], UR[0], g1) * a2u * g1;
+        J2r2 = f_downwind(UL[1], UR[1], g2) * a1u * g2;
+        J1 = f_downwind(a1L, a1R, g1) * a2u * g1;
+        J2 = f_downwind(a2L, a2R, g2) * a1u * g2;
+    }
     // mixture fluxes of momentum and energy
     double WL[N], WR[N];
     if constexpr (MIX) {
@@ -99,7 +146,7 @@ __device__ __forceinline__ void pf_face_flux(double* F, const double* UL, const 
 // FP64 face states.
 template <int D, bool MIX = false>
 __device__ __forceinline__ void pf_face_flux_six(double* F, double* fnc, const double* UL, const double* UR, double gq,
-                                                 const Eos& e, int phasic, unsigned int* err) {
+                                                 const Eos& e, int phasic, int hll, unsigned int* err) {
     using M = SixEq<D>;
     constexpr int N = M::N;
     double W[2][N];
@@ -138,13 +185,14 @@ __device__ __forceinline__ void pf_face_flux_six(double* F, double* fnc, const d
         E1[s] = e1 + (0.5 * r1[s]) * k;
         E2[s] = e2 + (0.5 * r2[s]) * k;
     }
-    // phase fluxes: phase 1 carries Q, phase 2 -Q, each weighted by the upwind volume fraction of the
-    // other phase and the downwind value of the carried quantity
+    // phase fluxes: phase 1 carries Q, phase 2 -Q; UD: each weighted by the upwind volume fraction of
+    // the other phase and the downwind value of the carried quantity; HLL: PfHll
     const double g1 = gq, g2 = -g1;
     const double a2u = f_upwind(a2[0], a2[1], g1);
     const double a1u = f_upwind(a1[0], a1[1], g2);
-    auto j1 = [&](double l, double r) { return f_downwind(l, r, g1) * a2u * g1; };
-    auto j2 = [&](double l, double r) { return f_downwind(l, r, g2) * a1u * g2; };
+    const PfHll h(a1[0], a1[1], gq);
+    auto j1 = [&](double l, double r) { return hll ? h.p1(l, r) : f_downwind(l, r, g1) * a2u * g1; };
+    auto j2 = [&](double l, double r) { return hll ? h.p2(l, r) : f_downwind(l, r, g2) * a1u * g2; };
     const double J1r1 = j1(r1[0], r1[1]);
     const double J2r2 = j2(r2[0], r2[1]);
     // kinetic energy per unit mass of the mixture velocity of the phasic states
@@ -192,11 +240,11 @@ __device__ __forceinline__ void pf_face_flux_six(double* F, double* fnc, const d
 // The Phase-Field face fluxes of model M (F stored negated; fnc the model's NCPF face terms).
 template <class M, bool MIX>
 __device__ __forceinline__ void pf_face_fluxes(double* F, double* fnc, const double* UL, const double* UR, double gq,
-                                               const Eos& e, int phasic, unsigned int* err) {
+                                               const Eos& e, int phasic, int hll, unsigned int* err) {
     if constexpr (M::KIND == kModelSix) {
-        pf_face_flux_six<M::D, MIX>(F, fnc, UL, UR, gq, e, phasic, err);
+        pf_face_flux_six<M::D, MIX>(F, fnc, UL, UR, gq, e, phasic, hll, err);
     } else {
-        pf_face_flux<M::D, MIX>(F, UL, UR, gq, e, err);
+        pf_face_flux<M::D, MIX>(F, UL, UR, gq, e, hll, err);
         fnc[0] = 0.0;
     }
 }

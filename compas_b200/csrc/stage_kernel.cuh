@@ -64,6 +64,7 @@ struct StageArgs {
     Thinc thinc;               // used by the THINC kernels only
     const double* gq[3];       // Phase-Field kernels: face gradients of the potential Q per direction
     int pf_phasic;             // Phase-Field kernels, six-equation model: 1 phasic, 0 mixture formulation
+    int pf_hll;                // Phase-Field kernels: 1 HLL phase fluxes, 0 upwind/downwind
     int order;                 // tile traversal order (tile_coords): 0 x fastest, 1 bricks of tiles
 };
 
@@ -390,7 +391,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                     }
                 }
                 if constexpr (PFX) {
-                    pf_face_fluxes<M, MIX>(F, fnc, UL, UR, pf_face_gq(a, d, gi, gj, gk), a.e, a.pf_phasic, err);
+                    pf_face_fluxes<M, MIX>(F, fnc, UL, UR, pf_face_gq(a, d, gi, gj, gk), a.e, a.pf_phasic, a.pf_hll,
+                                           err);
                     cm = 0.0;
                 } else {
                     M::hllc(F, fnc, cm, UL, UR, a.e, d, a.id_k, err);
@@ -439,7 +441,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                     float cmf;
                     if constexpr (PFX) {
                         pf_face_fluxes<M, MIX>(F, fnc, UL, UR, pf_face_gq(a, d, gi, gj, gk), a.e, a.pf_phasic,
-                                               err);
+                                               a.pf_hll, err);
                         cmf = 0.0f;
                     } else if constexpr (M::KIND == kModelFive) {
                         fiveeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, a.e, d, a.id_k);
@@ -708,6 +710,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_list_kernel(ListArgs L) {
             sa.trace = B.trace;
             sa.order = L.order;
             sa.pf_phasic = 0;
+            sa.pf_hll = 0;
             for (int d = 0; d < 3; ++d) sa.gq[d] = nullptr;
         }
         __syncthreads();

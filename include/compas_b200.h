@@ -79,6 +79,7 @@ typedef struct compas_b200_parm {
     int phase_field;          /* PhaseField.phase_field */
     int pf_mechanism;         /* PhaseField.Mechanism: 1 CAC-Adv, 3 ACDI (the reference's ID_Mechanism) */
     int pf_explicit_rc;       /* PhaseField.ID_ExplicitRC: 0 elliptic solve, 1 explicit (flux-based only) */
+    int pf_flux;              /* PhaseField.ID_Flux: 0 upwind/downwind, 1 HLL phase fluxes */
     int pf_phase2flux;        /* PhaseField.ID_FluxPhase2Flux: 0 phasic, 1 mixture formulation; default 1
                                * for FIVEEQS (PhaseField_Parameter.H:53) and 0 for SIXEQS, whose Parm.H
                                * sets it (exec/_Tests/Advection/prob/Parm.H:48-50); FIVEEQS runs 1 only */

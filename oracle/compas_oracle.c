@@ -1240,6 +1240,12 @@ int cmp_pf_grad_q(const cmp_case* c, const cmp_pf* pf, const double* U, double d
     (void)c; (void)pf; (void)U; (void)dt; (void)gq0; (void)gq1; (void)gq2; (void)info;
     return -2;
 }
+int cmp_pf_dudt(const cmp_case* c, const cmp_pf* pf, const double* U, const double* gq0, const double* gq1,
+                const double* gq2, double* dUdt) {
+    (void)c; (void)pf; (void)U; (void)gq0; (void)gq1; (void)gq2; (void)dUdt;
+    return -2;
+}
+
 int cmp_advance_pf(const cmp_case* c, const cmp_pf* pf, double* U, int nsteps, double stop_time, double* t,
                    double* dts) {
     (void)c; (void)pf; (void)U; (void)nsteps; (void)stop_time; (void)t; (void)dts;

@@ -67,6 +67,7 @@ _SIGS = {
     "cmp_threads": (ctypes.c_int, []),
     "cmp_pf_step": (ctypes.c_int, [_P, ctypes.c_void_p, _D, ctypes.c_double, _D]),
     "cmp_pf_grad_q": (ctypes.c_int, [_P, ctypes.c_void_p, _D, ctypes.c_double, _D, _D, _D, _D]),
+    "cmp_pf_dudt": (ctypes.c_int, [_P, ctypes.c_void_p, _D, _D, _D, _D, _D]),
     "cmp_advance_pf": (ctypes.c_int, [_P, ctypes.c_void_p, _D, ctypes.c_int, ctypes.c_double,
                                       ctypes.POINTER(ctypes.c_double), _D]),
     "cmp_amr_advance": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
@@ -87,7 +88,7 @@ class PfCase(ctypes.Structure):
         ("mechanism", ctypes.c_int), ("explicit_rc", ctypes.c_int),
         ("lambda_", ctypes.c_double), ("eta", ctypes.c_double), ("eta_factor", ctypes.c_double),
         ("eta_multiplier", ctypes.c_double), ("cfl", ctypes.c_double), ("max_step", ctypes.c_int),
-        ("tol_rel", ctypes.c_double), ("phase2flux", ctypes.c_int),
+        ("tol_rel", ctypes.c_double), ("phase2flux", ctypes.c_int), ("flux", ctypes.c_int),
     ]
 
 
@@ -99,6 +100,7 @@ def pf_from(parm, tol_rel=None) -> PfCase:
     q.eta_multiplier, q.cfl, q.max_step = parm.pf_eta_multiplier, parm.pf_cfl, parm.pf_max_step
     q.tol_rel = parm.pf_tol_rel if tol_rel is None else tol_rel
     q.phase2flux = parm.pf_phase2flux
+    q.flux = parm.pf_flux
     return q
 
 _cache: dict = {}
@@ -240,6 +242,16 @@ class Oracle:
         self._call(self.lib.cmp_pf_grad_q(self._c, self._pf(pf), U.ctypes.data, dt, ptr[0], ptr[1], ptr[2],
                                           info.ctypes.data))
         return out[:dim], info
+
+    def pf_dudt(self, U: np.ndarray, pf, gq) -> np.ndarray:
+        """Phase-Field right-hand side of U (ghosts filled here) for the face gradients gq (one array
+        per direction, as pf_grad_q returns them); padded, valid cells written."""
+        out = np.zeros_like(U)
+        g = [np.ascontiguousarray(x) for x in gq]
+        ptr = [g[d].ctypes.data if d < len(g) else None for d in range(3)]
+        self._call(self.lib.cmp_pf_dudt(self._c, self._pf(pf), U.ctypes.data, ptr[0], ptr[1], ptr[2],
+                                        out.ctypes.data))
+        return out
 
     def advance_pf(self, U: np.ndarray, pf, nsteps: int, stop_time: float = 1e300, t0: float = 0.0):
         t = ctypes.c_double(t0)

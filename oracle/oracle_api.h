@@ -83,6 +83,7 @@ typedef struct cmp_pf {
     int max_step;           /* PhaseField.max_step */
     double tol_rel;         /* LinearSystem.tol_rel of the elliptic solve */
     int phase2flux;         /* PhaseField.ID_FluxPhase2Flux: 0 phasic, 1 mixture (PhaseField_Parameter.H:53) */
+    int flux;               /* PhaseField.ID_Flux: 0 upwind/downwind, 1 HLL (PhaseField_Parameter.H:52) */
 } cmp_pf;
 
 /* One Phase-Field step after a hyperbolic step of size dt: mechanism pseudo-time evolution, the
@@ -98,6 +99,12 @@ int cmp_pf_grad_q(const cmp_case* c, const cmp_pf* pf, const double* U, double d
 
 /* cmp_advance with a Phase-Field step after every hyperbolic step (Evolve, source/
  * Class_Compressible_PhaseField.cpp:171-330). */
+/* The Phase-Field right-hand side (PhaseField_compute_dUdt_FV) of the padded state U, its ghosts filled
+ * here, for given face gradients gq_d of the regularisation potential; dUdt (padded) receives the valid
+ * cells. The reference-header build implements it; the plain-C port returns -2. */
+int cmp_pf_dudt(const cmp_case* c, const cmp_pf* pf, const double* U, const double* gq0, const double* gq1,
+                const double* gq2, double* dUdt);
+
 int cmp_advance_pf(const cmp_case* c, const cmp_pf* pf, double* U, int nsteps, double stop_time, double* t,
                    double* dts);
 

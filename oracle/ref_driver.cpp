@@ -446,6 +446,7 @@ PfSetup pf_setup(const cmp_case* c, const cmp_pf* pf, const double* U) {
     s.P.ID_Mechanism = pf->mechanism;
     s.P.ID_ExplicitRC = pf->explicit_rc;
     s.P.ID_FluxPhase2Flux = pf->phase2flux;
+    s.P.ID_Flux = pf->flux;
     s.P.cfl = pf->cfl;
     s.P.max_step = pf->max_step;
     return s;
@@ -1010,6 +1011,30 @@ int cmp_pf_grad_q(const cmp_case* c, const cmp_pf* pf, const double* U, double d
     });
 #else
     (void)c; (void)pf; (void)U; (void)dt; (void)gq0; (void)gq1; (void)gq2; (void)info;
+    return -2;
+#endif
+}
+
+int cmp_pf_dudt(const cmp_case* c, const cmp_pf* pf, const double* U, const double* gq0, const double* gq1,
+                const double* gq2, double* dUdt) {
+#if (PHYSICS == FIVEEQS || PHYSICS == SIXEQS)
+    return guarded([&] {
+        PfSetup S = pf_setup(c, pf, U);
+        Parm parm = make_parm(c);
+        parm.PhaseField_Parm = S.P;
+        Geo g(c);
+        const double* in[3] = {gq0, gq1, gq2};
+        std::vector<FField> GQ(AMREX_SPACEDIM);
+        for (int d = 0; d < AMREX_SPACEDIM; ++d) {
+            GQ[d] = FField(g, d);
+            std::memcpy(GQ[d].v.data(), in[d], GQ[d].v.size() * sizeof(double));
+        }
+        std::vector<double> Ub(U, U + g.S * NSTATE);
+        fill_ghosts(c, Ub.data());
+        pf_compute_dudt(c, parm, Ub.data(), GQ, dUdt);
+    });
+#else
+    (void)c; (void)pf; (void)U; (void)gq0; (void)gq1; (void)gq2; (void)dUdt;
     return -2;
 #endif
 }

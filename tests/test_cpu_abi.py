@@ -83,6 +83,9 @@ def test_phase_field_formulation_key():
     with pytest.raises(cb.CompasError) as e:
         cb.make_parm(cb.SIXEQS, 2, {"PhaseField.ID_FluxPhase2Flux": 2})
     assert e.value.code == cb.EARG
+    assert cb.make_parm(cb.SIXEQS, 2).pf_flux == 0
+    assert cb.make_parm(cb.SIXEQS, 2, {"PhaseField.ID_Flux": 1}).pf_flux == 1
+    assert cb.make_parm(cb.FIVEEQS, 2, {"PhaseField.ID_Flux": 1}).pf_flux == 1
     with pytest.raises(cb.CompasError) as e:
-        cb.make_parm(cb.SIXEQS, 2, {"PhaseField.ID_Flux": 1})
-    assert e.value.code == cb.EUNSUPPORTED
+        cb.make_parm(cb.FIVEEQS, 2, {"PhaseField.ID_Flux": 2})
+    assert e.value.code == cb.EARG

@@ -183,14 +183,16 @@ def test_amr_oracle_conserves_composite_totals_periodic():
         assert abs(a - b) <= 1e-13 * abs(a)
 
 
-@pytest.mark.parametrize("form", ["0", "1"])
-def test_sixeq_phase_field_oracle_keeps_equilibrium_and_conserves(form):
+@pytest.mark.parametrize("form,flux", [("0", "0"), ("1", "0"), ("0", "1"), ("1", "1")])
+def test_sixeq_phase_field_oracle_keeps_equilibrium_and_conserves(form, flux):
     """The six-equation Phase-Field step of the reference-header build (phasic 0 / mixture 1
-    formulation, CAC-Adv with the elliptic solve, relaxation after every stage) keeps a uniform
+    formulation, upwind/downwind 0 / HLL 1 phase fluxes, CAC-Adv with the elliptic solve, relaxation
+    after every stage) keeps a uniform
     velocity and pressure across the interface and conserves the masses, momenta and total energy."""
     phys, dim, inputs, geom, U = cases.advected_interface(n=32, dim=2, physics=cb.SIXEQS)
     p, g = _parm_geom(phys, dim, dict(inputs, **{"PhaseField.phase_field": "1", "LinearSystem.tol_rel": "1e-13",
-                                                 "PhaseField.ID_FluxPhase2Flux": form}), geom)
+                                                 "PhaseField.ID_FluxPhase2Flux": form, "PhaseField.ID_Flux": flux}),
+                      geom)
     if not have_ref(p.physics, p.dim):
         pytest.skip("reference-header oracle not built")
     from oracle.oracle import pf_from

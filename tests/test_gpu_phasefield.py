@@ -11,9 +11,12 @@ sides, and the maps call atanh / tanh / cosh, which may differ from the host lib
 bit; neither moves the result near the bounds. Cases: CAC-Adv with the implicit approach (the
 configuration of the 2D shock-helium-bubble), ACDI with the explicit and implicit approaches,
 2D and 3D, walls / outflow and periodic sides; the six-equation model in the phasic (its default) and
-the mixture formulation, with the phase-energy exchange and the pressure relaxation after every
+the mixture formulation, upwind/downwind and HLL phase fluxes (PhaseField.ID_Flux), with the
+phase-energy exchange and the pressure relaxation after every
 Phase-Field stage, including the 3D shock-droplet with the explicit ACDI of
-exec/ShockDroplet-AirWater-6Eq/prob/inputs:108-112; conservation; the mixed form's error.
+exec/ShockDroplet-AirWater-6Eq/prob/inputs:108-112; conservation; the mixed form's error; and, for the same face gradients of Q, the Phase-Field
+right-hand side of the FP64 form against the reference headers' to the bit (that check is free of the
+solver tolerance and of the host library's transcendental functions).
 """
 import numpy as np
 import pytest
@@ -58,10 +61,18 @@ CASES = [
                                                                        "PhaseField.ID_FluxPhase2Flux": "1"}),
     (cases.shock_droplet, dict(n=24), {"PhaseField.Mechanism": "ACDI", "PhaseField.ID_ExplicitRC": "1",
                                        "PhaseField.Eta_Multiplier": "0.5", "PhaseField.cfl": "0.3"}),
+    (cases.shock_bubble, dict(nx=64, ny=32, scheme="WENO5B"), {"PhaseField.Mechanism": "CAC-Adv",
+                                                               "PhaseField.ID_Flux": "1"}),
+    (cases.advected_interface, dict(n=32, dim=2, physics=cb.SIXEQS), {"PhaseField.Mechanism": "ACDI",
+                                                                       "PhaseField.ID_ExplicitRC": "1",
+                                                                       "PhaseField.ID_Flux": "1"}),
+    (cases.advected_interface, dict(n=16, dim=3, physics=cb.SIXEQS), {"PhaseField.Mechanism": "CAC-Adv",
+                                                                       "PhaseField.ID_Flux": "1",
+                                                                       "PhaseField.ID_FluxPhase2Flux": "1"}),
 ]
 IDS = ["bubble_cac", "bubble_acdi_explicit", "bubble_acdi_implicit", "disc_cac_periodic", "sphere3d_cac",
        "sphere3d_acdi_explicit", "sixeq_disc_cac_phasic", "sixeq_disc_acdi_mixture", "sixeq_sphere3d_cac_mixture",
-       "sixeq_droplet3d_acdi_phasic"]
+       "sixeq_droplet3d_acdi_phasic", "bubble_cac_hll", "sixeq_disc_acdi_hll_phasic", "sixeq_sphere3d_cac_hll_mixture"]
 
 
 def _need_ref(p):
@@ -210,3 +221,44 @@ def test_phase_field_mixed_error_vs_fp64(physics):
     print("Phase-Field mixed vs FP64 rel L1 per field:", np.array2string(e, precision=2))
     for c in (0, 1, A.shape[0] - 1):  # masses and volume fraction
         assert e[c] <= 1e-5, e
+
+
+RHS_CASES = [
+    (cases.shock_bubble, dict(nx=64, ny=32, scheme="WENO5B"), {}),
+    (cases.shock_bubble, dict(nx=64, ny=32, scheme="WENO5B"), {"PhaseField.ID_Flux": "1"}),
+    (cases.advected_interface, dict(n=12, dim=3, physics=cb.FIVEEQS), {}),
+    (cases.advected_interface, dict(n=32, dim=2, physics=cb.SIXEQS), {}),
+    (cases.advected_interface, dict(n=32, dim=2, physics=cb.SIXEQS), {"PhaseField.ID_FluxPhase2Flux": "1"}),
+    (cases.advected_interface, dict(n=32, dim=2, physics=cb.SIXEQS), {"PhaseField.ID_Flux": "1"}),
+    (cases.advected_interface, dict(n=32, dim=2, physics=cb.SIXEQS), {"PhaseField.ID_Flux": "1",
+                                                                       "PhaseField.ID_FluxPhase2Flux": "1"}),
+    (cases.shock_droplet, dict(n=16), {}),
+    (cases.shock_droplet, dict(n=16), {"PhaseField.ID_Flux": "1", "PhaseField.ID_FluxPhase2Flux": "1"}),
+]
+RHS_IDS = ["bubble_ud", "bubble_hll", "sphere3d_ud", "sixeq_disc_phasic_ud", "sixeq_disc_mixture_ud",
+           "sixeq_disc_phasic_hll", "sixeq_disc_mixture_hll", "sixeq_droplet3d_phasic_ud",
+           "sixeq_droplet3d_mixture_hll"]
+
+
+@pytest.mark.parametrize("fn,kw,extra", RHS_CASES, ids=RHS_IDS)
+def test_phase_field_rhs_bitwise_matches_oracle(fn, kw, extra):
+    """The Phase-Field right-hand side (face states, regularisation flux, surface integral, the
+    six-equation phase-energy exchange) for the same face gradients of Q: the FP64 form equals the
+    reference headers' arithmetic to the bit."""
+    torch = _torch()
+    p, g, U = _case(fn, dict(extra, **{"PhaseField.Mechanism": "CAC-Adv"}), **kw)
+    _need_ref(p)
+    o = Oracle("reference", p, g)
+    A = U.copy()
+    _, dts = o.advance(A, 1)
+    gq, _ = o.pf_grad_q(A, pf_from(p), float(dts[0]))
+    ref = o.pf_dudt(A, pf_from(p), gq)
+    dev = torch.from_numpy(A).cuda()
+    cb.FillPatch(p, g, dev)
+    out = torch.zeros_like(dev)
+    cb.PhaseField_compute_dUdt_FV(p, g, dev, out, [torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in gq])
+    torch.cuda.synchronize()
+    got = cb.valid_view(out.cpu().numpy(), p, g)
+    want = cb.valid_view(ref, p, g)
+    assert np.abs(want).max() > 0.0
+    np.testing.assert_array_equal(got, want)

@@ -263,6 +263,13 @@ static Eos make_eos(const compas_b200_parm* p) {
     e.iA2 = 1.0 / p->A2;
     e.pinf1 = p->B1 / (p->A1 + 1.0);
     e.pinf2 = p->B2 / (p->A2 + 1.0);
+    if (p->source_term == 1) {
+        e.pmin1 = -p->B1 / (p->A1 + 1.0);
+        e.pmin2 = -p->B2 / (p->A2 + 1.0);
+    } else {
+        e.pmin1 = -p->B1 / p->A1;
+        e.pmin2 = -p->B2 / p->A2;
+    }
     for (int k = 0; k < kMaxPhases; ++k) {
         e.Ak[k] = p->Ak[k];
         e.Bk[k] = p->Bk[k];
@@ -306,8 +313,6 @@ static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
     if (p->phase_field && p->physics == COMPAS_B200_FIVEEQS_NPHASE)
         return fail(COMPAS_B200_EUNSUPPORTED, "PhaseField.phase_field = 1: this engine runs the FIVEEQS and SIXEQS "
                                               "Phase-Field step");
-    if (p->physics == COMPAS_B200_FIVEEQS && p->pf_phase2flux != 1)
-        return fail(COMPAS_B200_EUNSUPPORTED, "PhaseField.ID_FluxPhase2Flux: FIVEEQS runs the mixture formulation (1)");
     if (p->phase_field && p->pf_mechanism != 1 && p->pf_mechanism != 3)
         return fail(COMPAS_B200_EUNSUPPORTED, "PhaseField.Mechanism: this engine runs CAC-Adv and ACDI");
     if (p->phase_field && p->pf_explicit_rc && p->pf_mechanism == 1)
@@ -894,9 +899,6 @@ int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value
     if (k == "PhaseField.ID_FluxPhase2Flux") {
         // include/Physics_PhaseField/PhaseField_Parameter.H:53 (0 phasic, 1 mixture formulation)
         if (!parse_int(value, &ix) || ix < 0 || ix > 1) return bad("0, 1");
-        if (ix == 0 && p->physics != COMPAS_B200_SIXEQS)
-            return fail(COMPAS_B200_EUNSUPPORTED, k + " = 0: this engine runs the phasic formulation for SIXEQS "
-                                                      "(the mixture formulation, 1, for FIVEEQS)");
         p->pf_phase2flux = ix;
         return 0;
     }

@@ -1,14 +1,16 @@
 // Phase-Field regularisation flux of one face from the reconstructed face states and the face gradient
 // of the regularisation potential Q, with the upwind/downwind (PhaseField.ID_Flux = 0) or the HLL (1)
-// phase fluxes: FIVEEQS in the mixture formulation (PhaseField.ID_FluxPhase2Flux = 1), SIXEQS in the
-// phasic (0) or mixture (1) formulation with the non-conservative face terms of its phase-energy
-// exchange.
+// phase fluxes, in the phasic (PhaseField.ID_FluxPhase2Flux = 0) or the mixture (1) formulation;
+// SIXEQS with the non-conservative face terms of its phase-energy exchange.
 //
 // Reference (FIVEEQS):
 //   FVM_Conservative2FluxPhaseField_K  include/Operators_Compressible5Eq_PhaseField/FVM_Conservative2FluxPhaseField_K_Compressible5Eq_PhaseField.H:15-69
 //   FluxPhaseField                     include/Physics_Compressible5Eq_PhaseField/FluxPhaseField_Compressible5Eq_PhaseField.H
 //   phase fluxes J_k rho_k, J_k (UD)   include/Physics_Compressible_TwoPhase_PhaseField/FluxPhasePhaseField_UD_Compressible_TwoPhase_PhaseField.H
 //   mixture flux                       include/Physics_Compressible5Eq_PhaseField/FluxPhaseField_Mixture_Compressible5Eq_PhaseField.H
+//   phasic face states                 include/Physics_Compressible5Eq/Conservative2ConservativePhase_Compressible5Eq.H
+//                                      (phase energies from the pressure, clipped at the p_min energies)
+//   phasic formulation                 include/Physics_Compressible5Eq/VectorPhase2Vector_Compressible5Eq.H
 //   phase fluxes (HLL)                 include/Physics_Compressible_TwoPhase_PhaseField/FluxPhasePhaseField_HLL_Compressible_TwoPhase_PhaseField.H,
 //                                      ConservativePhase2FluxPhasePhaseField_Compressible_TwoPhase_PhaseField.H
 //   f_Upwind / f_Downwind              include/Operators_FV/f_Upwind.H, f_Downwind.H
@@ -82,7 +84,7 @@ __device__ __forceinline__ double pf_face_gq(const StageArgs& a, int d, int i, i
 // states); the plain form converts in FP64 as the reference does.
 template <int D, bool MIX = false>
 __device__ __forceinline__ void pf_face_flux(double* F, const double* UL, const double* UR, double gq, const Eos& e,
-                                             int hll, unsigned int* err) {
+                                             int phasic, int hll, unsigned int* err) {
     using M = FiveEq<D>;
     constexpr int N = M::N;
     // phase fluxes (the two phases carry Q and -Q) of the masses and volume fractions
@@ -118,6 +120,50 @@ __device__ __forceinline__ void pf_face_flux(double* F, const double* UL, const 
     } else {
         M::cons2prim(WL, UL, e, err);
         M::cons2prim(WR, UR, e, err);
+    }
+    if (phasic) {
+        // phasic states: alpha_k rho_k e_k from the face pressure, clipped at the energy of p_min_k with
+        // the mixture internal energy kept; alpha_k rho_k u; alpha_k rho_k E_k
+        double m1[2][3], m2[2][3], E1[2], E2[2];
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            const double* U = s ? UR : UL;
+            const double* W = s ? WR : WL;
+            const double r1 = U[0], r2 = U[1], a1 = U[M::IA], a2 = 1.0 - a1, p = W[M::IE];
+            const double phi1 = nasg_phi(a1, r1, e.C1, err), phi2 = nasg_phi(a2, r2, e.C2, err);
+            double e1 = phi1 * e.A1 * p + phi1 * e.B1 + r1 * e.D1;
+            const double e1m = phi1 * e.A1 * e.pmin1 + phi1 * e.B1 + r1 * e.D1;
+            double e2 = phi2 * e.A2 * p + phi2 * e.B2 + r2 * e.D2;
+            const double e2m = phi2 * e.A2 * e.pmin2 + phi2 * e.B2 + r2 * e.D2;
+            const double re = e1 + e2;
+            if (e1 < e1m) {
+                e1 = e1m;
+                e2 = re - e1;
+            } else if (e2 < e2m) {
+                e2 = e2m;
+                e1 = re - e2;
+            }
+            const double k = ksum<D>(W + 2);
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+                m1[s][c] = r1 * W[2 + c];
+                m2[s][c] = r2 * W[2 + c];
+            }
+            E1[s] = e1 + (0.5 * r1) * k;
+            E2[s] = e2 + (0.5 * r2) * k;
+        }
+        const double a2u = f_upwind(a2L, a2R, g1);
+        const double a1u = f_upwind(a1L, a1R, g2);
+        const PfHll h(a1L, a1R, gq);
+        auto j1 = [&](double l, double r) { return hll ? h.p1(l, r) : f_downwind(l, r, g1) * a2u * g1; };
+        auto j2 = [&](double l, double r) { return hll ? h.p2(l, r) : f_downwind(l, r, g2) * a1u * g2; };
+        F[0] = -J1r1;
+        F[1] = -J2r2;
+#pragma unroll
+        for (int c = 0; c < D; ++c) F[2 + c] = -(j1(m1[0][c], m1[1][c]) + j2(m2[0][c], m2[1][c]));
+        F[M::IE] = -(j1(E1[0], E1[1]) + j2(E2[0], E2[1]));
+        F[M::IA] = -J1;
+        return;
     }
     const double Mf = J1r1 + J2r2;
     double ud[3];
@@ -244,7 +290,7 @@ __device__ __forceinline__ void pf_face_fluxes(double* F, double* fnc, const dou
     if constexpr (M::KIND == kModelSix) {
         pf_face_flux_six<M::D, MIX>(F, fnc, UL, UR, gq, e, phasic, hll, err);
     } else {
-        pf_face_flux<M::D, MIX>(F, UL, UR, gq, e, hll, err);
+        pf_face_flux<M::D, MIX>(F, UL, UR, gq, e, phasic, hll, err);
         fnc[0] = 0.0;
     }
 }

@@ -60,6 +60,7 @@ struct Eos {
     double A1, A2, B1, B2, C1, C2, D1, D2;
     double iA1, iA2;  // 1/A1, 1/A2 (mixed-precision pressure recovery)
     double pinf1, pinf2;  // B1/(A1 + 1), B2/(A2 + 1) (the relaxation's admissibility check)
+    double pmin1, pmin2;  // p_min of the two-phase Parm (source/Parm.cpp:164-171): -B/A, or -B/(A + 1) with K
     double Ak[kMaxPhases], Bk[kMaxPhases], Ck[kMaxPhases], Dk[kMaxPhases];
 };
 

@@ -82,7 +82,7 @@ typedef struct compas_b200_parm {
     int pf_flux;              /* PhaseField.ID_Flux: 0 upwind/downwind, 1 HLL phase fluxes */
     int pf_phase2flux;        /* PhaseField.ID_FluxPhase2Flux: 0 phasic, 1 mixture formulation; default 1
                                * for FIVEEQS (PhaseField_Parameter.H:53) and 0 for SIXEQS, whose Parm.H
-                               * sets it (exec/_Tests/Advection/prob/Parm.H:48-50); FIVEEQS runs 1 only */
+                               * sets it (exec/_Tests/Advection/prob/Parm.H:48-50) */
     double pf_lambda;         /* PhaseField.Lambda (<= 0: 1) */
     double pf_eta;            /* PhaseField.Eta (<= 0: Eta_Multiplier x the largest cell size) */
     double pf_eta_factor;     /* PhaseField.Eta_Factor */

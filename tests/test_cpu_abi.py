@@ -72,14 +72,12 @@ def test_tma_key():
 def test_phase_field_formulation_key():
     """PhaseField.ID_FluxPhase2Flux: the mixture formulation by default for FIVEEQS
     (include/Physics_PhaseField/PhaseField_Parameter.H:53), the phasic one for SIXEQS
-    (exec/_Tests/Advection/prob/Parm.H:48-50); SIXEQS takes both, FIVEEQS runs the mixture form only."""
+    (exec/_Tests/Advection/prob/Parm.H:48-50); both models take both."""
     assert cb.make_parm(cb.FIVEEQS, 2).pf_phase2flux == 1
     assert cb.make_parm(cb.SIXEQS, 3).pf_phase2flux == 0
     assert cb.make_parm(cb.SIXEQS, 2, {"PhaseField.ID_FluxPhase2Flux": 1}).pf_phase2flux == 1
     assert cb.make_parm(cb.FIVEEQS, 3, {"PhaseField.ID_FluxPhase2Flux": 1}).pf_phase2flux == 1
-    with pytest.raises(cb.CompasError) as e:
-        cb.make_parm(cb.FIVEEQS, 2, {"PhaseField.ID_FluxPhase2Flux": 0})
-    assert e.value.code == cb.EUNSUPPORTED
+    assert cb.make_parm(cb.FIVEEQS, 2, {"PhaseField.ID_FluxPhase2Flux": 0}).pf_phase2flux == 0
     with pytest.raises(cb.CompasError) as e:
         cb.make_parm(cb.SIXEQS, 2, {"PhaseField.ID_FluxPhase2Flux": 2})
     assert e.value.code == cb.EARG

@@ -11,7 +11,7 @@ sides, and the maps call atanh / tanh / cosh, which may differ from the host lib
 bit; neither moves the result near the bounds. Cases: CAC-Adv with the implicit approach (the
 configuration of the 2D shock-helium-bubble), ACDI with the explicit and implicit approaches,
 2D and 3D, walls / outflow and periodic sides; the six-equation model in the phasic (its default) and
-the mixture formulation, upwind/downwind and HLL phase fluxes (PhaseField.ID_Flux), with the
+the mixture formulation (the five-equation model in both as well), upwind/downwind and HLL phase fluxes (PhaseField.ID_Flux), with the
 phase-energy exchange and the pressure relaxation after every
 Phase-Field stage, including the 3D shock-droplet with the explicit ACDI of
 exec/ShockDroplet-AirWater-6Eq/prob/inputs:108-112; conservation; the mixed form's error; and, for the same face gradients of Q, the Phase-Field
@@ -63,6 +63,8 @@ CASES = [
                                        "PhaseField.Eta_Multiplier": "0.5", "PhaseField.cfl": "0.3"}),
     (cases.shock_bubble, dict(nx=64, ny=32, scheme="WENO5B"), {"PhaseField.Mechanism": "CAC-Adv",
                                                                "PhaseField.ID_Flux": "1"}),
+    (cases.shock_bubble, dict(nx=64, ny=32, scheme="WENO5B"), {"PhaseField.Mechanism": "CAC-Adv",
+                                                               "PhaseField.ID_FluxPhase2Flux": "0"}),
     (cases.advected_interface, dict(n=32, dim=2, physics=cb.SIXEQS), {"PhaseField.Mechanism": "ACDI",
                                                                        "PhaseField.ID_ExplicitRC": "1",
                                                                        "PhaseField.ID_Flux": "1"}),
@@ -72,7 +74,7 @@ CASES = [
 ]
 IDS = ["bubble_cac", "bubble_acdi_explicit", "bubble_acdi_implicit", "disc_cac_periodic", "sphere3d_cac",
        "sphere3d_acdi_explicit", "sixeq_disc_cac_phasic", "sixeq_disc_acdi_mixture", "sixeq_sphere3d_cac_mixture",
-       "sixeq_droplet3d_acdi_phasic", "bubble_cac_hll", "sixeq_disc_acdi_hll_phasic", "sixeq_sphere3d_cac_hll_mixture"]
+       "sixeq_droplet3d_acdi_phasic", "bubble_cac_hll", "bubble_cac_phasic", "sixeq_disc_acdi_hll_phasic", "sixeq_sphere3d_cac_hll_mixture"]
 
 
 def _need_ref(p):
@@ -226,7 +228,11 @@ def test_phase_field_mixed_error_vs_fp64(physics):
 RHS_CASES = [
     (cases.shock_bubble, dict(nx=64, ny=32, scheme="WENO5B"), {}),
     (cases.shock_bubble, dict(nx=64, ny=32, scheme="WENO5B"), {"PhaseField.ID_Flux": "1"}),
+    (cases.shock_bubble, dict(nx=64, ny=32, scheme="WENO5B"), {"PhaseField.ID_FluxPhase2Flux": "0"}),
+    (cases.shock_bubble, dict(nx=64, ny=32, scheme="WENO5B"), {"PhaseField.ID_FluxPhase2Flux": "0",
+                                                               "PhaseField.ID_Flux": "1"}),
     (cases.advected_interface, dict(n=12, dim=3, physics=cb.FIVEEQS), {}),
+    (cases.advected_interface, dict(n=12, dim=3, physics=cb.FIVEEQS), {"PhaseField.ID_FluxPhase2Flux": "0"}),
     (cases.advected_interface, dict(n=32, dim=2, physics=cb.SIXEQS), {}),
     (cases.advected_interface, dict(n=32, dim=2, physics=cb.SIXEQS), {"PhaseField.ID_FluxPhase2Flux": "1"}),
     (cases.advected_interface, dict(n=32, dim=2, physics=cb.SIXEQS), {"PhaseField.ID_Flux": "1"}),
@@ -235,7 +241,7 @@ RHS_CASES = [
     (cases.shock_droplet, dict(n=16), {}),
     (cases.shock_droplet, dict(n=16), {"PhaseField.ID_Flux": "1", "PhaseField.ID_FluxPhase2Flux": "1"}),
 ]
-RHS_IDS = ["bubble_ud", "bubble_hll", "sphere3d_ud", "sixeq_disc_phasic_ud", "sixeq_disc_mixture_ud",
+RHS_IDS = ["bubble_ud", "bubble_hll", "bubble_phasic_ud", "bubble_phasic_hll", "sphere3d_ud", "sphere3d_phasic_ud", "sixeq_disc_phasic_ud", "sixeq_disc_mixture_ud",
            "sixeq_disc_phasic_hll", "sixeq_disc_mixture_hll", "sixeq_droplet3d_phasic_ud",
            "sixeq_droplet3d_mixture_hll"]
 

@@ -134,6 +134,8 @@ _SIGS = {
                                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_uint)]),
     "compas_b200_level_dts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
     "compas_b200_level_launches": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "compas_b200_level_step_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                                   ctypes.c_void_p]),
     "compas_b200_level_pf_substeps": (ctypes.c_longlong, [ctypes.c_void_p]),
     "compas_b200_level_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                                 ctypes.POINTER(ctypes.c_int)]),
@@ -381,6 +383,18 @@ class Level:
             assert U.numel() * 8 == self.nbytes
             _check(lib().compas_b200_level_upload(self._h, U.data_ptr(), 1 if U.is_cuda else 0, t0,
                                                   _stream_ptr(stream)))
+
+    def step_host(self, host_in, host_out, slabs: int = 32, stream=None) -> None:
+        """One step from the padded host state host_in to host_out (pinned torch tensors or numpy
+        arrays), the copies in both directions overlapped with the stages slab by slab."""
+        def ptr(x):
+            if isinstance(x, np.ndarray):
+                assert x.dtype == np.float64 and x.flags.c_contiguous and x.nbytes == self.nbytes
+                return x.ctypes.data
+            assert not x.is_cuda and x.numel() * 8 == self.nbytes
+            return x.data_ptr()
+        _check(lib().compas_b200_level_step_host(self._h, ptr(host_in), ptr(host_out), int(slabs),
+                                                 _stream_ptr(stream)))
 
     def set_state(self, U, stream=None) -> None:
         """Replace the state only (keeps the time and the time-step control)."""

@@ -99,6 +99,19 @@ __host__ __device__ __forceinline__ long long ghost_count(const Grid& g) {
     return 2LL * g.gz * g.pxy + 2LL * g.ng * g.px * g.n[2] + 2LL * g.ng * g.n[1] * g.n[2];
 }
 
+// Ghost cell (i, j, k) of U from the valid cell its coordinates map to, all components.
+__device__ __forceinline__ void fill_cell(double* U, const Grid& g, int N, int D, int m0, const int* lo,
+                                          const int* hi, int i, int j, int k) {
+    const long long dst = g.at(i, j, k);
+    for (int n = 0; n < N; ++n) {
+        int si = i, sj = j, sk = k;
+        double sgn = bc_map(si, g.n[0], lo[0], hi[0], n, 0, D, m0);
+        sgn *= bc_map(sj, g.n[1], lo[1], hi[1], n, 1, D, m0);
+        if (D == 3) sgn *= bc_map(sk, g.n[2], lo[2], hi[2], n, 2, D, m0);
+        U[n * g.S + dst] = sgn * U[n * g.S + g.at(si, sj, sk)];
+    }
+}
+
 // Fill ghost cell number q (enumeration above) of U, all components.
 __device__ __forceinline__ void fill_ghost_cell(double* U, const Grid& g, int N, int D, int m0, const int* lo,
                                                 const int* hi, long long q) {
@@ -131,14 +144,7 @@ __device__ __forceinline__ void fill_ghost_cell(double* U, const Grid& g, int N,
             k = (int)(r / g.n[1]);
             i = (s < g.ng) ? s - g.ng : g.n[0] + (s - g.ng);
         }
-        const long long dst = g.at(i, j, k);
-        for (int n = 0; n < N; ++n) {
-            int si = i, sj = j, sk = k;
-            double sgn = bc_map(si, g.n[0], lo[0], hi[0], n, 0, D, m0);
-            sgn *= bc_map(sj, g.n[1], lo[1], hi[1], n, 1, D, m0);
-            if (D == 3) sgn *= bc_map(sk, g.n[2], lo[2], hi[2], n, 2, D, m0);
-            U[n * g.S + dst] = sgn * U[n * g.S + g.at(si, sj, sk)];
-        }
+        fill_cell(U, g, N, D, m0, lo, hi, i, j, k);
     }
 }
 
@@ -147,6 +153,33 @@ __global__ void fill_boundary_kernel(BcArgs a) {
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
          q += (long long)gridDim.x * blockDim.x)
         fill_ghost_cell(a.U, a.g, a.N, a.D, a.m0, a.lo, a.hi, q);
+}
+
+// The ghost cells of a slab of the padded box: the padded planes (3D: z planes; 2D: y rows) l0 <= l < l1
+// of the slowest direction, in valid coordinates (ghost planes negative or >= n). Every ghost cell
+// maps to the valid cell fill_boundary_kernel maps it to; the slab's own planes hold every source
+// unless the slab direction is periodic.
+__global__ void fill_boundary_slab_kernel(BcArgs a, int l0, int l1) {
+    const Grid& g = a.g;
+    const long long PX = g.px, PY = g.pxy / g.px;
+    const long long unit = (a.D == 3) ? PX * PY : PX;
+    const long long total = (long long)(l1 - l0) * unit;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+         q += (long long)gridDim.x * blockDim.x) {
+        const int l = l0 + (int)(q / unit);
+        const long long r = q % unit;
+        const int i = (int)(r % PX) - g.ng;
+        int j, k;
+        if (a.D == 3) {
+            j = (int)(r / PX) - g.ng;
+            k = l;
+        } else {
+            j = l;
+            k = 0;
+        }
+        const bool valid = i >= 0 && i < g.n[0] && j >= 0 && j < g.n[1] && k >= 0 && k < g.n[2];
+        if (!valid) fill_cell(a.U, g, a.N, a.D, a.m0, a.lo, a.hi, i, j, k);
+    }
 }
 
 template <int D>
@@ -414,6 +447,30 @@ static int launch_fill(const compas_b200_parm* p, const compas_b200_geom* geo, d
     return COMPAS_B200_OK;
 }
 
+// The ghost cells of the slab l0 <= l < l1 (fill_boundary_slab_kernel).
+static int launch_fill_slab(const compas_b200_parm* p, const compas_b200_geom* geo, double* U, int l0, int l1,
+                            cudaStream_t st) {
+    BcArgs b;
+    b.U = U;
+    b.g = make_grid(p, geo);
+    b.N = nstate(p);
+    b.D = p->dim;
+    b.m0 = mom0_of(p->physics, p->nphase);
+    for (int d = 0; d < 3; ++d) {
+        b.lo[d] = geo->lo_bc[d];
+        b.hi[d] = geo->hi_bc[d];
+    }
+    const long long unit = (p->dim == 3) ? b.g.pxy : b.g.px;
+    const long long total = (long long)(l1 - l0) * unit;
+    const int threads = 256;
+    long long blocks = (total + threads - 1) / threads;
+    if (blocks > 148LL * 16) blocks = 148LL * 16;
+    if (blocks < 1) blocks = 1;
+    fill_boundary_slab_kernel<<<(unsigned)blocks, threads, 0, st>>>(b, l0, l1);
+    CUDA_TRY(cudaGetLastError());
+    return COMPAS_B200_OK;
+}
+
 // ------------------------------------------------------------------------------------------------
 // Autotuner: the launch shape (threads per CTA, CTAs per SM; kern_impl.cuh) and the tile traversal
 // order (tile_coords) of the plain stage kernels, picked per model, precision and box size by timing
@@ -638,6 +695,10 @@ struct compas_b200_level {
     bool tuned = false, forced = false;
     compas::TmaMaps maps[3];        // TMA maps of U, U1, U2 (3D mixed form; valid = 0 otherwise)
     bool use_tma = false;           // stage with the maps (compas_b200.tma = 1; the autotuner may turn it off)
+    // host-buffer steps (compas_b200_level_step_host): copy streams and the events that order the slabs
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_done = nullptr;
+    cudaEvent_t ev_in[64] = {}, ev_out[64] = {};
 };
 
 namespace compas {
@@ -1245,6 +1306,18 @@ int compas_b200_level_create(const compas_b200_parm* p, const compas_b200_geom* 
 int compas_b200_level_destroy(compas_b200_level* lv) {
     if (!lv) return COMPAS_B200_OK;
     if (lv->graph) cudaGraphExecDestroy(lv->graph);
+    if (lv->h2d) {
+        cudaStreamSynchronize(lv->h2d);
+        cudaStreamSynchronize(lv->d2h);
+        cudaStreamDestroy(lv->h2d);
+        cudaStreamDestroy(lv->d2h);
+        cudaEventDestroy(lv->ev_start);
+        cudaEventDestroy(lv->ev_done);
+        for (int c = 0; c < 64; ++c) {
+            cudaEventDestroy(lv->ev_in[c]);
+            cudaEventDestroy(lv->ev_out[c]);
+        }
+    }
     cudaFree(lv->U);
     cudaFree(lv->U1);
     cudaFree(lv->U2);
@@ -1443,6 +1516,129 @@ int compas_b200_level_advance(compas_b200_level* lv, int nsteps, double stop_tim
             if ((rc = enqueue_step(lv, st))) return rc;
     }
     lv->launches += 8LL * nsteps;
+    return COMPAS_B200_OK;
+}
+
+// One step from a padded host state to a padded host state. The state moves in slabs of whole tile
+// layers along the slowest direction (z in 3D, y in 2D): slab j is copied in on a copy stream while the
+// stages of earlier slabs run, stage s of slab j runs once stage s-1 has written slabs j-1..j+1 (the
+// stencil reaches 3 cells, a tile layer is 8 or 16), and slab j is copied out on a second copy stream
+// as soon as the last stage has written it, so both copy directions overlap the stages. The kernels and
+// tiles are those of compas_b200_level_advance (tile order 0), so the result is bit-identical to
+// set_state + advance(1) + download. Falls back to that sequence for the first step of a level (the
+// t = 0 wave-speed pass and the autotuner need the whole state), a periodic slab direction, a Phase-Field
+// level or slabs < 2.
+int compas_b200_level_step_host(compas_b200_level* lv, const double* host_in, double* host_out, int slabs,
+                                void* stream) {
+    if (!lv || !host_in || !host_out) return fail(COMPAS_B200_EARG, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const compas_b200_parm* p = &lv->p;
+    const compas_b200_geom* g = &lv->g;
+    const int D = p->dim, sd = D - 1;  // slab direction
+    const int TS = (D == 2) ? kTile2 : kTile3;
+    const int layers = (g->n[sd] + TS - 1) / TS;
+    const int C = std::min(std::min(slabs, layers), 64);
+    const bool tune_pending = p->autotune && !lv->tuned && !lv->forced && !p->thinc;
+    if (lv->pf || lv->need_init || tune_pending || g->lo_bc[sd] == 0 || C < 2) {
+        int rc;
+        if ((rc = compas_b200_level_set_state(lv, host_in, 0, stream))) return rc;
+        if ((rc = compas_b200_level_advance(lv, 1, 1.0e300, 1, stream))) return rc;
+        return compas_b200_level_download(lv, host_out, 0, stream);
+    }
+    if (!lv->h2d) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&lv->h2d, cudaStreamNonBlocking));
+        CUDA_TRY(cudaStreamCreateWithFlags(&lv->d2h, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&lv->ev_start, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&lv->ev_done, cudaEventDisableTiming));
+        for (int c = 0; c < 64; ++c) {
+            CUDA_TRY(cudaEventCreateWithFlags(&lv->ev_in[c], cudaEventDisableTiming));
+            CUDA_TRY(cudaEventCreateWithFlags(&lv->ev_out[c], cudaEventDisableTiming));
+        }
+    }
+    const Grid G = make_grid(p, g);
+    const int gl = (D == 3) ? G.gz : G.ng;                 // ghost planes along the slab direction
+    const long long unit = (D == 3) ? G.pxy : G.px;        // doubles per padded plane of one component
+    const int N = nstate(p);
+    const int layer_tiles = (D == 3) ? ((g->n[0] + TS - 1) / TS) * ((g->n[1] + TS - 1) / TS) : (g->n[0] + TS - 1) / TS;
+    // slab c: tile layers [L0[c], L0[c+1]); valid planes [V0[c], V0[c+1]); padded planes [P0[c], P0[c+1])
+    int L0[65], V0[65], P0[65];
+    for (int c = 0; c <= C; ++c) {
+        L0[c] = (int)((long long)c * layers / C);
+        V0[c] = std::min(L0[c] * TS, g->n[sd]);
+        P0[c] = (c == 0) ? 0 : (c == C ? g->n[sd] + 2 * gl : V0[c] + gl);
+    }
+    auto copy = [&](double* dst, const double* src, int c, cudaMemcpyKind kind, cudaStream_t s) {
+        const size_t off = (size_t)P0[c] * unit;
+        const size_t width = (size_t)(P0[c + 1] - P0[c]) * unit * sizeof(double);
+        return cudaMemcpy2DAsync(dst + off, (size_t)G.S * sizeof(double), src + off, (size_t)G.S * sizeof(double), width,
+                                 (size_t)N, kind, s);
+    };
+    // ghost planes filled with slab c: its own planes, and the domain's ghost planes at the two ends
+    auto fill = [&](double* U, int c) {
+        const int l0 = (c == 0) ? -gl : V0[c];
+        const int l1 = (c == C - 1) ? g->n[sd] + gl : V0[c + 1];
+        return launch_fill_slab(p, g, U, l0, l1, st);
+    };
+    set_time_kernel<<<1, 1, 0, st>>>(lv->ctl, 0.0, 1.0e300, 0);
+    CUDA_TRY(cudaGetLastError());
+    // the copies start after the caller's earlier work on its stream
+    CUDA_TRY(cudaEventRecord(lv->ev_start, st));
+    CUDA_TRY(cudaStreamWaitEvent(lv->h2d, lv->ev_start, 0));
+    CUDA_TRY(cudaStreamWaitEvent(lv->d2h, lv->ev_start, 0));
+    for (int c = 0; c < C; ++c) {
+        CUDA_TRY(copy(lv->U, host_in, c, cudaMemcpyHostToDevice, lv->h2d));
+        CUDA_TRY(cudaEventRecord(lv->ev_in[c], lv->h2d));
+    }
+    StepParams sp;
+    sp.cfl = p->cfl;
+    sp.dx[0] = g->dx[0];
+    sp.dx[1] = g->dx[1];
+    sp.dx[2] = g->dx[2];
+    sp.D = D;
+    sp.limiter = p->change_limiter;
+    sp.dts = lv->dts;
+    sp.dts_cap = lv->dts_cap;
+    step_begin_kernel<<<1, 1, 0, st>>>(lv->ctl, sp);
+    CUDA_TRY(cudaGetLastError());
+    StageArgs a = base_args(p, g);
+    a.mode = kModeStage;
+    a.dt = &lv->ctl->dt;
+    a.done = &lv->ctl->done;
+    a.cmax = &lv->ctl->cmax;
+    a.err = &lv->ctl->err;
+    a.order = 0;
+    double* bufs_in[3] = {lv->U, lv->U1, lv->U2};
+    double* bufs_out[3] = {lv->U1, lv->U2, lv->U};
+    int rc;
+    for (int w = 0; w < C + 3; ++w) {
+        if (w < C) {
+            CUDA_TRY(cudaStreamWaitEvent(st, lv->ev_in[w], 0));
+            if ((rc = fill(lv->U, w))) return rc;
+        }
+        for (int s = 0; s < 3; ++s) {
+            const int c = w - 1 - s;
+            if (c < 0 || c >= C) continue;
+            a.stage = s;
+            a.Us = bufs_in[s];
+            a.U0 = lv->U;
+            a.Uout = bufs_out[s];
+            a.tile_base = L0[c] * layer_tiles;
+            a.tile_count = (L0[c + 1] - L0[c]) * layer_tiles;
+            if ((rc = launch_stage(p, a, st, 0, lv->shape, lv->use_tma ? &lv->maps[s] : nullptr))) return rc;
+            if (s < 2) {
+                if ((rc = fill(bufs_out[s], c))) return rc;
+            } else {
+                CUDA_TRY(cudaEventRecord(lv->ev_out[c], st));
+                CUDA_TRY(cudaStreamWaitEvent(lv->d2h, lv->ev_out[c], 0));
+                CUDA_TRY(copy(host_out, lv->U, c, cudaMemcpyDeviceToHost, lv->d2h));
+            }
+        }
+    }
+    step_end_kernel<<<1, 1, 0, st>>>(lv->ctl);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaEventRecord(lv->ev_done, lv->d2h));
+    CUDA_TRY(cudaStreamWaitEvent(st, lv->ev_done, 0));
+    lv->launches += 3 + 6LL * C;
     return COMPAS_B200_OK;
 }
 

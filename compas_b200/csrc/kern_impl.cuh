@@ -46,8 +46,9 @@ static cudaError_t launch_stage_v(const StageArgs& a, cudaStream_t st) {
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
-    const long long tiles = (long long)((a.g.n[0] + S::TS - 1) / S::TS) * ((a.g.n[1] + S::TS - 1) / S::TS) *
-                            ((a.g.n[2] + S::TZ - 1) / S::TZ);
+    const long long tiles = a.tile_count > 0 ? (long long)a.tile_count
+                                             : (long long)((a.g.n[0] + S::TS - 1) / S::TS) *
+                                                   ((a.g.n[1] + S::TS - 1) / S::TS) * ((a.g.n[2] + S::TZ - 1) / S::TZ);
     kern<<<(unsigned)tiles, S::NT, T::SMEM, st>>>(a);
     return cudaGetLastError();
 }
@@ -64,8 +65,9 @@ static cudaError_t launch_stage_tma(const StageArgs& a, const TmaMaps& tm, cudaS
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
-    const long long tiles = (long long)((a.g.n[0] + S::TS - 1) / S::TS) * ((a.g.n[1] + S::TS - 1) / S::TS) *
-                            ((a.g.n[2] + S::TZ - 1) / S::TZ);
+    const long long tiles = a.tile_count > 0 ? (long long)a.tile_count
+                                             : (long long)((a.g.n[0] + S::TS - 1) / S::TS) *
+                                                   ((a.g.n[1] + S::TS - 1) / S::TS) * ((a.g.n[2] + S::TZ - 1) / S::TZ);
     kern<<<(unsigned)tiles, S::NT, T::SMEM, st>>>(a, tm);
     return cudaGetLastError();
 }

@@ -66,6 +66,8 @@ struct StageArgs {
     int pf_phasic;             // Phase-Field kernels, six-equation model: 1 phasic, 0 mixture formulation
     int pf_hll;                // Phase-Field kernels: 1 HLL phase fluxes, 0 upwind/downwind
     int order;                 // tile traversal order (tile_coords): 0 x fastest, 1 bricks of tiles
+    int tile_base;             // single-box kernels: first tile (order 0) and number of tiles of the launch
+    int tile_count;            // (0: the whole box); a run of whole tile layers is a slab of the box
 };
 
 // Tile coordinates (in tiles) of the w-th CTA of a box of ntx x nty x ntz tiles. order 0: x fastest.
@@ -620,7 +622,7 @@ template <class M, int SCHEME, bool MIX, int VAR, int TX, int TY, int TZ, int NT
 __global__ void __launch_bounds__(NT, MINB) stage_kernel(StageArgs a) {
     if (a.done && *a.done) return;
     extern __shared__ double smem_d[];
-    stage_tile<M, SCHEME, MIX, VAR, TX, TY, TZ, NT>(a, blockIdx.x, smem_d);
+    stage_tile<M, SCHEME, MIX, VAR, TX, TY, TZ, NT>(a, a.tile_base + blockIdx.x, smem_d);
 }
 
 // One box with the halo slabs staged by TMA (the tensor maps of a.Us are kernel parameters).
@@ -628,7 +630,7 @@ template <class M, int SCHEME, bool MIX, int TX, int TY, int TZ, int NT, int MIN
 __global__ void __launch_bounds__(NT, MINB) stage_kernel_tma(StageArgs a, const __grid_constant__ TmaMaps tm) {
     if (a.done && *a.done) return;
     extern __shared__ __align__(128) double smem_d[];
-    stage_tile<M, SCHEME, MIX, kVarTma, TX, TY, TZ, NT>(a, blockIdx.x, smem_d, &tm);
+    stage_tile<M, SCHEME, MIX, kVarTma, TX, TY, TZ, NT>(a, a.tile_base + blockIdx.x, smem_d, &tm);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -709,6 +711,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_list_kernel(ListArgs L) {
             sa.relax = B.relax;
             sa.trace = B.trace;
             sa.order = L.order;
+            sa.tile_base = 0;
+            sa.tile_count = 0;
             sa.pf_phasic = 0;
             sa.pf_hll = 0;
             for (int d = 0; d < 3; ++d) sa.gq[d] = nullptr;

@@ -256,6 +256,18 @@ int compas_b200_level_download(compas_b200_level* lv, double* dst, int is_device
  * control; for callers that hand the state over every step. */
 int compas_b200_level_set_state(compas_b200_level* lv, const double* src, int is_device, void* stream);
 
+/* One coarse step of a host-resident state: replaces ThirdOrderSSPRK on a MultiFab that lives in host
+ * memory (source/Class_Compressible_PhaseField.cpp:3937-4107) for a host that hands the state over every
+ * step. host_in (the state at the start of the step) and host_out (the state after it), both in the
+ * layout above, should be pinned host memory for the copies to run asynchronously; they may be the
+ * same array. The state moves in `slabs` slabs of whole tile layers along the slowest direction, copied
+ * in and out on two copy streams of the level while the stages of neighbouring slabs run, so the copies
+ * in both directions overlap the computation. Bit-identical to set_state + advance(1) + download, which
+ * it falls back to for the level's first step, a periodic slowest direction, a Phase-Field level or
+ * slabs < 2 (at most 64 slabs are used). Completion is ordered on `stream`. */
+int compas_b200_level_step_host(compas_b200_level* lv, const double* host_in, double* host_out, int slabs,
+                                void* stream);
+
 /* Device pointer of the current state (layout above) for callers that keep data on the GPU. */
 double* compas_b200_level_state(compas_b200_level* lv);
 

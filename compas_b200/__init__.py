@@ -55,6 +55,7 @@ class Parm(ctypes.Structure):
         ("C1", ctypes.c_double), ("C2", ctypes.c_double),
         ("D1", ctypes.c_double), ("D2", ctypes.c_double),
         ("id_limiter", ctypes.c_int),
+        ("id_weno", ctypes.c_int),
         ("num_grow", ctypes.c_int),
         ("thinc", ctypes.c_int),
         ("thinc_use_normal", ctypes.c_int),

@@ -74,6 +74,16 @@ static cudaError_t launch_stage_tma(const StageArgs& a, const TmaMaps& tm, cudaS
 
 template <class M, int SCHEME, bool MIX>
 static cudaError_t launch_stage_var(const KernelChoice& k, const StageArgs& a, cudaStream_t st, const TmaMaps* tm) {
+    if constexpr (SCHEME == 2) {
+        // GODUNOV / MUSCL: the plain right-hand side, ordinary halo loads (the tuner's TMA candidate
+        // runs this form too)
+        if (k.phase_field || k.thinc) return cudaErrorNotSupported;
+        switch (k.shape) {
+            case 1: return launch_stage_v<M, 2, MIX, kVarPlain, 1>(a, st);
+            case 2: return launch_stage_v<M, 2, MIX, kVarPlain, 2>(a, st);
+            default: return launch_stage_v<M, 2, MIX, kVarPlain, 0>(a, st);
+        }
+    } else {
     if constexpr (M::D == 3 && MIX && M::KIND != kModelFiveN) {
         if (tm && tm->valid && !k.thinc && !k.phase_field) {
             switch (k.shape) {
@@ -96,11 +106,14 @@ static cudaError_t launch_stage_var(const KernelChoice& k, const StageArgs& a, c
         case 2: return launch_stage_v<M, SCHEME, MIX, kVarPlain, 2>(a, st);
         default: return launch_stage_v<M, SCHEME, MIX, kVarPlain, 0>(a, st);
     }
+    }
 }
 
 template <class M>
 static cudaError_t launch_stage_m(const KernelChoice& k, const StageArgs& a, cudaStream_t st, const TmaMaps* tm) {
     const bool mix = (k.precision == 1), bounded = (k.limiter == 6);
+    if (k.limiter < 5)  // GODUNOV / MUSCL family
+        return mix ? launch_stage_var<M, 2, true>(k, a, st, tm) : launch_stage_var<M, 2, false>(k, a, st, tm);
     if constexpr (M::KIND == kModelFiveN) {
         if (bounded) return cudaErrorNotSupported;
         return mix ? launch_stage_var<M, 5, true>(k, a, st, tm) : launch_stage_var<M, 5, false>(k, a, st, tm);
@@ -142,6 +155,7 @@ static cudaError_t launch_list_s(const KernelChoice& k, const ListArgs& L, cudaS
 
 template <class M>
 static cudaError_t launch_list_m(const KernelChoice& k, const ListArgs& L, cudaStream_t st) {
+    if (k.limiter < 5) return cudaErrorNotSupported;  // the box list runs WENO5 / WENO5B
     if constexpr (M::KIND == kModelFiveN) {
         if (k.limiter == 6) return cudaErrorNotSupported;
         return (k.precision == 1) ? launch_list_s<M, 5, true>(k, L, st) : launch_list_s<M, 5, false>(k, L, st);

@@ -909,6 +909,59 @@ __device__ __forceinline__ float weno5_f32(float f_mm, float f_m, float f_c, flo
     return f_c + __fmaf_rn(w[0], e[0], __fmaf_rn(w[1], e[1], w[2] * e[2]));
 }
 
+// ------------------------------------------------------------------------------------------------
+// GODUNOV and MUSCL face values (FiniteVolume.Scheme = GODUNOV, MUSCL-Minmod / -vanLeer / -Superbee /
+// -MC; ID_Limiter 0..4), in primitive variables like WENO5:
+//   include/Operators_FV/Reconstruction2Face_MUSCL_D.H (slopes (f_c - f_m)/dx, (f_p - f_m)/(2 dx),
+//   (f_p - f_c)/dx), Slope_TVD.H, Limiter_Minmod.H, Limiter_vanLeer.H, Limiter_Superbee.H,
+//   Limiter_MC.H, Reconstruction2Face_Linear.H (f_c + side 0.5 slope dx), Reconstruction2Face_Godunov_D.H
+//   (f_c), include/Tools/Sign.H. std::min / std::max over a list keep the first extremum, as the folds
+//   of dmin / dmax below do.
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ double sign3(double x) { return (x > 0.0) ? 1.0 : ((x < 0.0) ? -1.0 : 0.0); }
+
+__device__ __forceinline__ double tvd_slope(double sm, double sc, double sp, int lim) {
+    if (lim == 1) return dmin(dmax(sm, 0.0), dmax(sp, 0.0)) + dmax(dmin(sm, 0.0), dmin(sp, 0.0));
+    if (lim == 2) return (sm * sp > 0.0) ? 2.0 / (1.0 / sm + 1.0 / sp) : 0.0;
+    if (lim == 3) {
+        const double am = fabs(sm), ap = fabs(sp);
+        return (sign3(sm) + sign3(sp)) * dmin(dmin(am, ap), 0.5 * dmax(am, ap));
+    }
+    // lim == 4: MC(a = sm, b = sp, c = sc)
+    return dmin(dmin(dmax(sc, 0.0), dmax(2.0 * sm, 0.0)), dmax(2.0 * sp, 0.0)) +
+           dmax(dmax(dmin(sc, 0.0), dmin(2.0 * sm, 0.0)), dmin(2.0 * sp, 0.0));
+}
+
+// Face value of the centre cell f_c on its side `side` (+1 right face, -1 left face).
+__device__ __forceinline__ double muscl_face(double f_m, double f_c, double f_p, double dx, int side, int lim) {
+    if (lim == 0) return f_c;
+    const double s_m = (f_c - f_m) / dx;
+    const double s_c = (f_p - f_m) / (2.0 * dx);
+    const double s_p = (f_p - f_c) / dx;
+    const double s = tvd_slope(s_m, s_c, s_p, lim);
+    return f_c + (double)side * 0.5 * s * dx;
+}
+
+// Mixed precision: the limiters are homogeneous of degree one in the slopes, so the FP32 form limits
+// the undivided differences and adds half the limited difference.
+__device__ __forceinline__ float tvd_slope_f32(float sm, float sc, float sp, int lim) {
+    if (lim == 1) return fminf(fmaxf(sm, 0.0f), fmaxf(sp, 0.0f)) + fmaxf(fminf(sm, 0.0f), fminf(sp, 0.0f));
+    if (lim == 2) return (sm * sp > 0.0f) ? 2.0f * sm * sp / (sm + sp) : 0.0f;
+    if (lim == 3) {
+        const float am = fabsf(sm), ap = fabsf(sp);
+        const float sg = ((sm > 0.0f) ? 1.0f : ((sm < 0.0f) ? -1.0f : 0.0f)) + ((sp > 0.0f) ? 1.0f : ((sp < 0.0f) ? -1.0f : 0.0f));
+        return sg * fminf(fminf(am, ap), 0.5f * fmaxf(am, ap));
+    }
+    return fminf(fminf(fmaxf(sc, 0.0f), fmaxf(2.0f * sm, 0.0f)), fmaxf(2.0f * sp, 0.0f)) +
+           fmaxf(fmaxf(fminf(sc, 0.0f), fminf(2.0f * sm, 0.0f)), fminf(2.0f * sp, 0.0f));
+}
+
+__device__ __forceinline__ float muscl_face_f32(float f_m, float f_c, float f_p, int side, int lim) {
+    if (lim == 0) return f_c;
+    const float s = tvd_slope_f32(f_c - f_m, 0.5f * (f_p - f_m), f_p - f_c, lim);
+    return __fmaf_rn((float)side * 0.5f, s, f_c);
+}
+
 __device__ __forceinline__ float bound_min_theta_f32(float f_c, float fL, float fR) {
     const float W = 1.0f / 12.0f;
     const float fC = (f_c - W * fL - W * fR) * (1.0f / (1.0f - 2.0f * W));

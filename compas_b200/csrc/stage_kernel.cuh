@@ -65,6 +65,7 @@ struct StageArgs {
     const double* gq[3];       // Phase-Field kernels: face gradients of the potential Q per direction
     int pf_phasic;             // Phase-Field kernels, six-equation model: 1 phasic, 0 mixture formulation
     int pf_hll;                // Phase-Field kernels: 1 HLL phase fluxes, 0 upwind/downwind
+    int muscl;                 // SCHEME 2: 0 Godunov, 1 minmod, 2 van Leer, 3 superbee, 4 MC (-1 otherwise)
     int order;                 // tile traversal order (tile_coords): 0 x fastest, 1 bricks of tiles
     int tile_base;             // single-box kernels: first tile (order 0) and number of tiles of the launch
     int tile_count;            // (0: the whole box); a run of whole tile layers is a slab of the box
@@ -140,7 +141,8 @@ __device__ __forceinline__ void load_cons(double* U, const double* base, const G
 }
 
 // SCHEME: 5 WENO5 on every primitive variable; 6 WENO5B (bounded masses and volume fractions,
-// plain WENO5 on the velocity and the pressure(s)).
+// plain WENO5 on the velocity and the pressure(s)); 2 GODUNOV / MUSCL in primitive variables, the
+// limiter a.muscl at run time.
 // MIX: false - plain FP64, the reference's arithmetic to the bit; true - mixed precision: the cell
 // primitives are recovered in FP64 (pressure from total energy) and kept in shared memory as FP32,
 // the reconstruction runs in FP32, the Riemann solver, divergence, stage accumulation and
@@ -158,7 +160,9 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
     constexpr bool TMA = (VAR == kVarTma);
     static_assert(!TMA || (M::D == 3 && MIX), "TMA halo staging: the 3D mixed form");
     static_assert(!PFX || M::KIND != kModelFiveN, "the Phase-Field kernel is the two-phase models'");
-    static_assert(M::KIND != kModelFiveN || (SCHEME == 5 && !TH), "FIVEEQS_NPHASE runs WENO5 without THINC");
+    static_assert(M::KIND != kModelFiveN || ((SCHEME == 5 || SCHEME == 2) && !TH),
+                  "FIVEEQS_NPHASE runs WENO5, GODUNOV and MUSCL without THINC");
+    static_assert(SCHEME != 2 || (VAR == kVarPlain && !TH), "GODUNOV / MUSCL: the plain right-hand side");
     constexpr bool NPH = (M::KIND == kModelFiveN);
     using PT = typename std::conditional<MIX, float, double>::type;
     using T = TileShape<M, TX, TY, TZ, PT, TMA, PFX>;
@@ -376,13 +380,24 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                         weno5b_masses(r1, r2, al, 1, WfL[0], WfL[1], WfL[M::IA]);
                         weno5b_masses(r1 + 1, r2 + 1, al + 1, -1, WfR[0], WfR[1], WfR[M::IA]);
                     }
+                    if constexpr (SCHEME == 2) {
+                        const int lim = a.muscl;
 #pragma unroll
-                    for (int n = NB0; n < NB1; ++n) {
-                        const double w0 = smem[off[0] + n * str[0]], w1 = smem[off[1] + n * str[1]];
-                        const double w2 = smem[off[2] + n * str[2]], w3 = smem[off[3] + n * str[3]];
-                        const double w4 = smem[off[4] + n * str[4]], w5 = smem[off[5] + n * str[5]];
-                        WfL[n] = weno5(w0, w1, w2, w3, w4, 1);
-                        WfR[n] = weno5(w1, w2, w3, w4, w5, -1);
+                        for (int n = 0; n < N; ++n) {
+                            const double w1 = smem[off[1] + n * str[1]], w2 = smem[off[2] + n * str[2]];
+                            const double w3 = smem[off[3] + n * str[3]], w4 = smem[off[4] + n * str[4]];
+                            WfL[n] = muscl_face(w1, w2, w3, dxd, 1, lim);
+                            WfR[n] = muscl_face(w2, w3, w4, dxd, -1, lim);
+                        }
+                    } else {
+#pragma unroll
+                        for (int n = NB0; n < NB1; ++n) {
+                            const double w0 = smem[off[0] + n * str[0]], w1 = smem[off[1] + n * str[1]];
+                            const double w2 = smem[off[2] + n * str[2]], w3 = smem[off[3] + n * str[3]];
+                            const double w4 = smem[off[4] + n * str[4]], w5 = smem[off[5] + n * str[5]];
+                            WfL[n] = weno5(w0, w1, w2, w3, w4, 1);
+                            WfR[n] = weno5(w1, w2, w3, w4, w5, -1);
+                        }
                     }
                     M::prim2cons(UL, WfL, a.e, err);
                     M::prim2cons(UR, WfR, a.e, err);
@@ -416,13 +431,24 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                         weno5b_masses_f32(r1, r2, al, 1, wL[0], wL[1], wL[M::IA]);
                         weno5b_masses_f32(r1 + 1, r2 + 1, al + 1, -1, wR[0], wR[1], wR[M::IA]);
                     }
+                    if constexpr (SCHEME == 2) {
+                        const int lim = a.muscl;
 #pragma unroll
-                    for (int n = NB0; n < NB1; ++n) {
-                        const float w0 = smem[off[0] + n * str[0]], w1 = smem[off[1] + n * str[1]];
-                        const float w2 = smem[off[2] + n * str[2]], w3 = smem[off[3] + n * str[3]];
-                        const float w4 = smem[off[4] + n * str[4]], w5 = smem[off[5] + n * str[5]];
-                        wL[n] = weno5_f32(w0, w1, w2, w3, w4, 1);
-                        wR[n] = weno5_f32(w1, w2, w3, w4, w5, -1);
+                        for (int n = 0; n < N; ++n) {
+                            const float w1 = smem[off[1] + n * str[1]], w2 = smem[off[2] + n * str[2]];
+                            const float w3 = smem[off[3] + n * str[3]], w4 = smem[off[4] + n * str[4]];
+                            wL[n] = muscl_face_f32(w1, w2, w3, 1, lim);
+                            wR[n] = muscl_face_f32(w2, w3, w4, -1, lim);
+                        }
+                    } else {
+#pragma unroll
+                        for (int n = NB0; n < NB1; ++n) {
+                            const float w0 = smem[off[0] + n * str[0]], w1 = smem[off[1] + n * str[1]];
+                            const float w2 = smem[off[2] + n * str[2]], w3 = smem[off[3] + n * str[3]];
+                            const float w4 = smem[off[4] + n * str[4]], w5 = smem[off[5] + n * str[5]];
+                            wL[n] = weno5_f32(w0, w1, w2, w3, w4, 1);
+                            wR[n] = weno5_f32(w1, w2, w3, w4, w5, -1);
+                        }
                     }
 #pragma unroll
                     for (int n = 0; n < N; ++n) {

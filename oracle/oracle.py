@@ -39,6 +39,7 @@ class Case(ctypes.Structure):
         ("C1", ctypes.c_double), ("C2", ctypes.c_double),
         ("D1", ctypes.c_double), ("D2", ctypes.c_double),
         ("id_limiter", ctypes.c_int),
+        ("id_weno", ctypes.c_int),
         ("id_riemann", ctypes.c_int),
         ("source_term", ctypes.c_int),
         ("relaxation", ctypes.c_int),
@@ -152,7 +153,7 @@ def case_from(parm, geom) -> Case:
     if parm.dim == 2:
         c.n[2] = 1
     c.ng = geom.ng
-    for k in ("A1", "A2", "B1", "B2", "C1", "C2", "D1", "D2", "id_limiter", "id_riemann", "source_term",
+    for k in ("A1", "A2", "B1", "B2", "C1", "C2", "D1", "D2", "id_limiter", "id_weno", "id_riemann", "source_term",
               "relaxation", "relax_trace", "thinc", "thinc_use_normal", "thinc_eps", "thinc_beta",
               "thinc_normal_threshold", "cfl", "change_limiter"):
         setattr(c, k, getattr(parm, k))

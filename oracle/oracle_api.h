@@ -30,7 +30,8 @@ typedef struct cmp_case {
     int lo_bc[3];       /* COMPAS boundary codes: 0 interior/periodic, 2 outflow, 3 symmetry, */
     int hi_bc[3];       /*   4 slip wall, 5 no-slip wall (docs/user-guide/inputs.md:113-120) */
     double A1, A2, B1, B2, C1, C2, D1, D2;  /* EOS coefficients as source/Parm.cpp:101-188 */
-    int id_limiter;     /* FiniteVolume.Scheme: 5 WENO5, 6 WENO5B (FiniteVolume_Parameter.H:51-147) */
+    int id_limiter;     /* FiniteVolume.Scheme (FiniteVolume_Parameter.H:51-147): with id_weno 1, 5 WENO5, 6 WENO5B; */
+    int id_weno;        /*   with id_weno 0, 0 GODUNOV, 1 MUSCL(-Minmod), 2 -vanLeer, 3 -Superbee, 4 -MC */
     int id_riemann;     /* Physics.RiemannSolver: 0 LLF, 1 HLL, 2 HLLC */
     int source_term;    /* FIVEEQS Physics.source_term (K term): 0 or 1 */
     int relaxation;     /* SIXEQS Physics.pressure_relaxation: 0 or 1 */

@@ -98,14 +98,29 @@ Parm make_parm(const cmp_case* c) {
 #else
     p.A1 = c->A1; p.A2 = c->A2; p.B1 = c->B1; p.B2 = c->B2;
     p.C1 = c->C1; p.C2 = c->C2; p.D1 = c->D1; p.D2 = c->D2;
-    p.p_min = {0.0, 0.0};
+    // source/Parm.cpp:164-171
+    if (c->source_term == 1) {
+        p.p_min = {-c->B1 / (c->A1 + 1.0), -c->B2 / (c->A2 + 1.0)};
+    } else {
+        p.p_min = {-c->B1 / c->A1, -c->B2 / c->A2};
+    }
 #endif
+    // FiniteVolume.Scheme (include/Operators_FV/FiniteVolume_Parameter.H:51-147)
     auto& fv = p.FiniteVolume_Parm;
-    fv.ID_WENO = 1;
+    fv.ID_WENO = c->id_weno;
     fv.ID_Limiter = c->id_limiter;
-    fv.ID_Poly = 4;
-    fv.Num_Grow = 3;
-    fv.Scheme = (c->id_limiter == 6) ? FVReconstruction::WENO_5B : FVReconstruction::WENO_5;
+    if (c->id_weno) {
+        fv.ID_Poly = 4;
+        fv.Num_Grow = 3;
+        fv.Scheme = (c->id_limiter == 6) ? FVReconstruction::WENO_5B : FVReconstruction::WENO_5;
+    } else {
+        fv.ID_Poly = (c->id_limiter == 0) ? 0 : 1;
+        fv.Num_Grow = (c->id_limiter == 0) ? 1 : 2;
+        const FVReconstruction muscl[5] = {FVReconstruction::GODUNOV, FVReconstruction::MUSCL_MM,
+                                           FVReconstruction::MUSCL_VL, FVReconstruction::MUSCL_SB,
+                                           FVReconstruction::MUSCL_MC};
+        fv.Scheme = muscl[c->id_limiter];
+    }
     fv.Quadrature_Weight = 1.0 / 12.0;
     fv.ID_THINC = c->thinc;
     fv.ID_THINC_UseNormal = c->thinc_use_normal;

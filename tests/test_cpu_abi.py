@@ -42,10 +42,18 @@ def test_invalid_inputs_are_errors_not_aborts(key, value):
 
 
 def test_scheme_keys():
-    assert cb.make_parm(cb.FIVEEQS, 2, {"FiniteVolume.Scheme": "WENO5B"}).id_limiter == 6
-    with pytest.raises(cb.CompasError) as e:
-        cb.make_parm(cb.FIVEEQS, 2, {"FiniteVolume.Scheme": "MUSCL"})
-    assert e.value.code == cb.EUNSUPPORTED
+    """FiniteVolume.Scheme to the reference's ID_WENO / ID_Limiter / Num_Grow
+    (include/Operators_FV/FiniteVolume_Parameter.H:51-147)."""
+    p = cb.make_parm(cb.FIVEEQS, 2, {"FiniteVolume.Scheme": "WENO5B"})
+    assert (p.id_weno, p.id_limiter, p.num_grow) == (1, 6, 3)
+    for v, lim, ng in [("GODUNOV", 0, 1), ("MUSCL", 1, 2), ("MUSCL-Minmod", 1, 2), ("MUSCL-vanLeer", 2, 2),
+                       ("MUSCL-Superbee", 3, 2), ("MUSCL-MC", 4, 2)]:
+        p = cb.make_parm(cb.SIXEQS, 3, {"FiniteVolume.Scheme": v})
+        assert (p.id_weno, p.id_limiter, p.num_grow) == (0, lim, ng), v
+    for v in ("WENO3", "WENO3B"):
+        with pytest.raises(cb.CompasError) as e:
+            cb.make_parm(cb.FIVEEQS, 2, {"FiniteVolume.Scheme": v})
+        assert e.value.code == cb.EUNSUPPORTED
 
 
 def test_state_bytes_layout():

@@ -236,3 +236,30 @@ def test_sixeq_amr_oracle_conserves_composite_totals_periodic():
     s1 = totals(states)
     for a, b in zip(s0, s1):
         assert abs(a - b) <= 1e-13 * abs(a)
+
+
+@pytest.mark.parametrize("scheme", ["GODUNOV", "MUSCL", "MUSCL-vanLeer", "MUSCL-Superbee", "MUSCL-MC"])
+def test_muscl_reference_oracle_conserves_and_keeps_equilibrium(scheme):
+    """The reference-header oracle with the GODUNOV / MUSCL reconstructions: conservation on the periodic
+    square and the uniform pressure and velocity across the interface kept (the five-equation
+    primitive-variable reconstruction)."""
+    phys, dim, inputs, geom, U = cases.advected_disc(n=32)
+    p, g = _parm_geom(phys, dim, dict(inputs, **{"FiniteVolume.Scheme": scheme}), geom)
+    if not have_ref(p.physics, p.dim):
+        pytest.skip("reference-header oracle not built")
+    V0 = cb.valid_view(U, p, g).copy()
+    Oracle("reference", p, g).advance(U, 10)
+    V = cb.valid_view(U, p, g)
+    for c in range(5):
+        assert abs(V[c].sum() - V0[c].sum()) <= 1e-13 * np.abs(V0[c]).sum(), c
+    rho = V[0] + V[1]
+    u, v = V[2] / rho, V[3] / rho
+    assert np.max(np.abs(u - 1.0)) < 1e-9 and np.max(np.abs(v - 1.0)) < 1e-9
+
+
+def test_port_rejects_the_muscl_family():
+    """The plain-C restatement covers WENO5 / WENO5B; it refuses the other schemes."""
+    phys, dim, inputs, geom, U = cases.advected_disc(n=16)
+    p, g = _parm_geom(phys, dim, dict(inputs, **{"FiniteVolume.Scheme": "MUSCL-MC"}), geom)
+    with pytest.raises(RuntimeError):
+        Oracle("port", p, g).advance(U, 1)

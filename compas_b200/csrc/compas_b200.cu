@@ -345,7 +345,8 @@ static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
         return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.Scheme: this build runs GODUNOV, MUSCL-*, WENO5 and WENO5B");
     if (!p->id_weno && (p->thinc || p->phase_field))
         return fail(COMPAS_B200_EUNSUPPORTED, "THINC and the Phase-Field step run with WENO5 / WENO5B here");
-    if (p->id_riemann != 2) return fail(COMPAS_B200_EUNSUPPORTED, "Physics.RiemannSolver: this build runs HLLC");
+    if (p->id_riemann < 0 || p->id_riemann > 2)
+        return fail(COMPAS_B200_EUNSUPPORTED, "Physics.RiemannSolver: this build runs LLF, HLL and HLLC");
     if (p->phase_field && p->physics == COMPAS_B200_FIVEEQS_NPHASE)
         return fail(COMPAS_B200_EUNSUPPORTED, "PhaseField.phase_field = 1: this engine runs the FIVEEQS and SIXEQS "
                                               "Phase-Field step");
@@ -625,6 +626,7 @@ static StageArgs base_args(const compas_b200_parm* p, const compas_b200_geom* g)
     a.e = make_eos(p);
     a.id_k = p->source_term;
     a.relax = (p->physics == COMPAS_B200_SIXEQS) ? p->relaxation : 0;
+    a.riemann = p->id_riemann;
     a.trace = p->relax_trace;
     a.pf_phasic = (p->pf_phase2flux == 0);
     a.muscl = p->id_weno ? -1 : p->id_limiter;
@@ -1725,6 +1727,7 @@ static int batch_sync_list(compas_b200_batch* b, cudaStream_t st) {
         }
         B.id_k = c.p.source_term;
         B.relax = (c.p.physics == COMPAS_B200_SIXEQS) ? c.p.relaxation : 0;
+        B.riemann = c.p.id_riemann;
         B.trace = c.p.relax_trace;
         B.tiles = tile_count(b->dim, B.g);
         B.ghosts = ghost_count(B.g);

@@ -66,6 +66,7 @@ struct StageArgs {
     int pf_phasic;             // Phase-Field kernels, six-equation model: 1 phasic, 0 mixture formulation
     int pf_hll;                // Phase-Field kernels: 1 HLL phase fluxes, 0 upwind/downwind
     int muscl;                 // SCHEME 2: 0 Godunov, 1 minmod, 2 van Leer, 3 superbee, 4 MC (-1 otherwise)
+    int riemann;               // Physics.RiemannSolver: 0 LLF, 1 HLL, 2 HLLC
     int order;                 // tile traversal order (tile_coords): 0 x fastest, 1 bricks of tiles
     int tile_base;             // single-box kernels: first tile (order 0) and number of tiles of the launch
     int tile_count;            // (0: the whole box); a run of whole tile layers is a slab of the box
@@ -107,6 +108,73 @@ enum { kVarPlain = 0, kVarThinc = 1, kVarPhaseField = 2, kVarTma = 3 };
 
 #include "thinc.cuh"
 #include "pf_flux.cuh"
+
+namespace compas {
+
+// Local Lax-Friedrichs (hll = 0) and HLL (hll = 1) face fluxes, Physics.RiemannSolver = LLF / HLL, with
+// the face quantities of the non-conservative terms, for the three models:
+//   include/Physics_Compressible5Eq/Riemann_LLF_Compressible5Eq.H, Riemann_HLL_Compressible5Eq.H,
+//   include/Physics_Compressible6Eq/Riemann_LLF_Compressible6Eq.H, Riemann_HLL_Compressible6Eq.H,
+//   include/Physics_Compressible5Eq_NPhase/Riemann_LLF_Compressible5Eq_NPhase.H, Riemann_HLL_...H.
+// LLF: F = (FL + FR - lambda (UR - UL)) / 2, lambda = max(|VL| + cL, |VR| + cR), face velocity the mean;
+// HLL: Sp = max(0, VL + cL, VR + cR), Sm = min(0, VL - cL, VR - cR), F = (Sp FL - Sm FR + Sp Sm (UR - UL))
+// / (Sp - Sm), face velocity (Sp uL - Sm uR) / (Sp - Sm); six-equation: the face values of u alpha_k p_k
+// likewise. cmax = max(cL + |uL|, cR + |uR|).
+template <class M>
+__device__ __forceinline__ void riemann_llf_hll(int hll, double* Fout, double* fnc, double& cmax, const double* UL,
+                                                const double* UR, const Eos& e, int d, int id_k, unsigned int* err) {
+    constexpr int N = M::N, D = M::D;
+    constexpr int IU = M::IM;  // first velocity component of W
+    double WL[N], WR[N];
+    M::cons2prim(WL, UL, e, err);
+    M::cons2prim(WR, UR, e, err);
+    double FL[N], FR[N];
+    M::flux(FL, UL, WL, d);
+    M::flux(FR, UR, WR, d);
+    double cL, cR;
+    if constexpr (M::KIND == kModelSix) {
+        cL = M::sound_speed(WL, e, err);
+        cR = M::sound_speed(WR, e, err);
+    } else {
+        cL = M::sound_speed(WL, e, id_k, err);
+        cR = M::sound_speed(WR, e, id_k, err);
+    }
+    const double VL = pick<D>(WL + IU, d), VR = pick<D>(WR + IU, d);
+    if (!hll) {
+        const double lam = dmax(fabs(VL) + cL, fabs(VR) + cR);
+#pragma unroll
+        for (int i = 0; i < N; ++i) Fout[i] = (FL[i] + FR[i] - lam * (UR[i] - UL[i])) / 2.0;
+        fnc[0] = (VL + VR) / 2.0;
+        if constexpr (M::KIND == kModelSix) {
+            fnc[1] = (VL * WL[M::IE1] + VR * WR[M::IE1]) / 2.0;
+            fnc[2] = (VL * WL[M::IE2] + VR * WR[M::IE2]) / 2.0;
+        }
+    } else {
+        double Sp = 0.0, Sm = 0.0;
+        Sp = (Sp < VL + cL) ? VL + cL : Sp;
+        Sp = (Sp < VR + cR) ? VR + cR : Sp;
+        Sm = (VL - cL < Sm) ? VL - cL : Sm;
+        Sm = (VR - cR < Sm) ? VR - cR : Sm;
+#pragma unroll
+        for (int i = 0; i < N; ++i) Fout[i] = (Sp * FL[i] - Sm * FR[i] + Sp * Sm * (UR[i] - UL[i])) / (Sp - Sm);
+        fnc[0] = (Sp * VL - Sm * VR) / (Sp - Sm);
+        if constexpr (M::KIND == kModelSix) {
+            fnc[1] = (Sp * VL * WL[M::IE1] - Sm * VR * WR[M::IE1]) / (Sp - Sm);
+            fnc[2] = (Sp * VL * WL[M::IE2] - Sm * VR * WR[M::IE2]) / (Sp - Sm);
+        }
+    }
+    cmax = dmax(cL + sqrt(ksum<D>(WL + IU)), cR + sqrt(ksum<D>(WR + IU)));
+}
+
+// Physics.RiemannSolver: 0 LLF, 1 HLL, 2 HLLC (source/Class_Compressible_PhaseField.cpp:92-111).
+template <class M>
+__device__ __forceinline__ void riemann(int id_riemann, double* Fout, double* fnc, double& cmax, const double* UL,
+                                        const double* UR, const Eos& e, int d, int id_k, unsigned int* err) {
+    if (id_riemann == 2) M::hllc(Fout, fnc, cmax, UL, UR, e, d, id_k, err);
+    else riemann_llf_hll<M>(id_riemann, Fout, fnc, cmax, UL, UR, e, d, id_k, err);
+}
+
+}  // namespace compas
 
 namespace compas {
 
@@ -412,7 +480,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                                            err);
                     cm = 0.0;
                 } else {
-                    M::hllc(F, fnc, cm, UL, UR, a.e, d, a.id_k, err);
+                    riemann<M>(a.riemann, F, fnc, cm, UL, UR, a.e, d, a.id_k, err);
                 }
             } else {
                 float wL[N], wR[N];
@@ -464,13 +532,17 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                 }
                 if constexpr (NPH) {
                     // N-phase: FP32 reconstruction, FP64 limiter and Riemann solver
-                    M::hllc(F, fnc, cm, UL, UR, a.e, d, a.id_k, err);
+                    riemann<M>(a.riemann, F, fnc, cm, UL, UR, a.e, d, a.id_k, err);
                 } else {
                     float cmf;
                     if constexpr (PFX) {
                         pf_face_fluxes<M, MIX>(F, fnc, UL, UR, pf_face_gq(a, d, gi, gj, gk), a.e, a.pf_phasic,
                                                a.pf_hll, err);
                         cmf = 0.0f;
+                    } else if (a.riemann != 2) {
+                        double cmd;
+                        riemann_llf_hll<M>(a.riemann, F, fnc, cmd, UL, UR, a.e, d, a.id_k, err);
+                        cmf = (float)cmd;
                     } else if constexpr (M::KIND == kModelFive) {
                         fiveeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, a.e, d, a.id_k);
                     } else {
@@ -675,6 +747,7 @@ struct BoxDesc {
     int lo_bc[3], hi_bc[3];
     int id_k;
     int relax;
+    int riemann;                  // Physics.RiemannSolver of the box's case (0 LLF, 1 HLL, 2 HLLC)
     double trace;
     int tiles;                    // tiles of the box for the kernel's tile shape
     long long ghosts;             // ghost cells of one array of the box
@@ -741,6 +814,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_list_kernel(ListArgs L) {
             sa.tile_count = 0;
             sa.pf_phasic = 0;
             sa.pf_hll = 0;
+            sa.muscl = -1;
+            sa.riemann = B.riemann;
             for (int d = 0; d < 3; ++d) sa.gq[d] = nullptr;
         }
         __syncthreads();

@@ -2,8 +2,8 @@
 MUSCL-Superbee, MUSCL-MC) on the CUDA path against the reference-header oracle: the plain FP64 form
 is compared to the bit over several steps for every limiter (five-equation 2D), the six-equation 3D
 droplet with relaxation, and the N-phase triple point with the scheme of the reference's own example
-(exec/TriplePoint-5Eq-N/prob/inputs: MUSCL-MC, followed by the consistent limiter); and the mixed
-form's error against the FP64 form."""
+(exec/TriplePoint-5Eq-N/prob/inputs: MUSCL-MC, followed by the consistent limiter); the LLF and HLL
+Riemann solvers (Physics.RiemannSolver) likewise; and the mixed form's error against the FP64 form."""
 import numpy as np
 import pytest
 
@@ -95,3 +95,36 @@ def test_triple_point_mixed_error_within_fp64_sensitivity():
           "FP64 sensitivity:", np.array2string(sens, precision=2))
     for k in (0, 1, 2, 6, 7, 8):  # partial densities and volume fractions
         assert e[k] <= 10.0 * sens[k], (e, sens)
+
+
+@pytest.mark.parametrize("solver", ["LLF", "HLL"])
+@pytest.mark.parametrize("fn,kw,scheme,nsteps", [
+    (cases.shock_bubble, dict(nx=48, ny=24, scheme="WENO5B"), "WENO5B", 5),
+    (cases.shock_droplet, dict(n=16), "WENO5", 3),
+    (cases.triple_point, dict(m=12), "MUSCL-MC", 5),
+], ids=["bubble_weno5b", "droplet_weno5", "triple_muscl_mc"])
+def test_llf_hll_bitwise(solver, fn, kw, scheme, nsteps):
+    """Physics.RiemannSolver = LLF and HLL (the five-equation, six-equation and N-phase forms with their
+    face velocities and, for the six-equation model, the face values of u alpha_k p_k), FP64 against the
+    reference headers to the bit."""
+    phys, dim, inputs, geom, U = fn(**kw)
+    p = cb.make_parm(phys, dim, dict(inputs, **{"FiniteVolume.Scheme": scheme, "Physics.RiemannSolver": solver}))
+    g = cb.make_geom(**geom)
+    _bitwise(p, g, U, nsteps)
+
+
+@pytest.mark.parametrize("solver", ["LLF", "HLL"])
+def test_llf_hll_mixed_error_vs_fp64(solver):
+    out = {}
+    for prec in ("fp64", "mixed"):
+        phys, dim, inputs, geom, U = cases.shock_droplet(n=24)
+        p = cb.make_parm(phys, dim, dict(inputs, **{"Physics.RiemannSolver": solver, "compas_b200.precision": prec}))
+        g = cb.make_geom(**geom)
+        got, info, _ = run_gpu(p, g, U, 10)
+        assert info.status == 0
+        out[prec] = cb.valid_view(got, p, g)
+    A, B = out["mixed"], out["fp64"]
+    e = np.array([float(np.abs(A[c] - B[c]).sum() / np.abs(B[c]).sum()) for c in range(A.shape[0])])
+    print(f"{solver} mixed vs FP64 rel L1 per field:", np.array2string(e, precision=2))
+    for c in (0, 1, A.shape[0] - 1):
+        assert e[c] <= 1e-5, e

@@ -944,6 +944,39 @@ __device__ __forceinline__ double muscl_face(double f_m, double f_c, double f_p,
     return f_c + (double)side * 0.5 * s * dx;
 }
 
+// WENO3 face value (FiniteVolume.Scheme = WENO3: include/Operators_FV/WENO3.H, Reconstruction2Face_WENO3_D.H,
+// Reconstruction2Face_WENO.H): two candidates, ratio-form weights with the NaN guard, the weighted sum
+// accumulated from 0.
+__device__ __forceinline__ double weno3_face(double f_m, double f_c, double f_p, int side) {
+    double q0, q1, d0;
+    if (side == 1) {
+        q0 = f_c + 0.5 * (f_c - f_m);
+        q1 = f_c + 0.5 * (f_p - f_c);
+        d0 = 1.0 / 3.0;
+    } else {
+        q0 = f_c - 0.5 * (f_c - f_m);
+        q1 = f_c - 0.5 * (f_p - f_c);
+        d0 = 2.0 / 3.0;
+    }
+    const double d1 = 1.0 - d0;
+    const double IS0 = (f_c - f_m) * (f_c - f_m);
+    const double IS1 = (f_p - f_c) * (f_p - f_c);
+    double IS01 = IS0 / IS1;
+    if (isnan(IS01)) IS01 = 1.0;
+    const double IS10 = 1.0 / IS01;
+    const double w0 = d0 / (d0 + (IS01 * IS01) * d1);
+    const double w1 = d1 / ((IS10 * IS10) * d0 + d1);
+    double f = 0.0;
+    f += w0 * q0;
+    f += w1 * q1;
+    return f;
+}
+
+// Three-cell face values of the stage kernel's SCHEME 2: code 0..4 the GODUNOV / MUSCL family, 10 WENO3.
+__device__ __forceinline__ double face3(double f_m, double f_c, double f_p, double dx, int side, int code) {
+    return (code == 10) ? weno3_face(f_m, f_c, f_p, side) : muscl_face(f_m, f_c, f_p, dx, side, code);
+}
+
 // Mixed precision: the limiters are homogeneous of degree one in the slopes, so the FP32 form limits
 // the undivided differences and adds half the limited difference.
 __device__ __forceinline__ float tvd_slope_f32(float sm, float sc, float sp, int lim) {
@@ -962,6 +995,27 @@ __device__ __forceinline__ float muscl_face_f32(float f_m, float f_c, float f_p,
     if (lim == 0) return f_c;
     const float s = tvd_slope_f32(f_c - f_m, 0.5f * (f_p - f_m), f_p - f_c, lim);
     return __fmaf_rn((float)side * 0.5f, s, f_c);
+}
+
+// WENO3 in FP32 in the correction form of weno5_f32 (f_c plus the weighted corrections), the weights
+// from the ratio of the indicators with one reciprocal.
+__device__ __forceinline__ float weno3_face_f32(float f_m, float f_c, float f_p, int side) {
+    const float a = f_c - f_m, b = f_p - f_c;
+    const float h = (side == 1) ? 0.5f : -0.5f;
+    const float d0 = (side == 1) ? (1.0f / 3.0f) : (2.0f / 3.0f), d1 = 1.0f - d0;
+    const float IS0 = a * a, IS1 = b * b;
+    float w0;
+    if (IS0 == 0.0f && IS1 == 0.0f) w0 = d0;
+    else if (IS1 == 0.0f) w0 = 0.0f;
+    else {
+        const float r = fminf(IS0 / IS1, 1.0e18f);
+        w0 = d0 / __fmaf_rn(r * r, d1, d0);
+    }
+    return f_c + h * __fmaf_rn(w0, a - b, b);
+}
+
+__device__ __forceinline__ float face3_f32(float f_m, float f_c, float f_p, int side, int code) {
+    return (code == 10) ? weno3_face_f32(f_m, f_c, f_p, side) : muscl_face_f32(f_m, f_c, f_p, side, code);
 }
 
 __device__ __forceinline__ float bound_min_theta_f32(float f_c, float fL, float fR) {

@@ -65,7 +65,7 @@ struct StageArgs {
     const double* gq[3];       // Phase-Field kernels: face gradients of the potential Q per direction
     int pf_phasic;             // Phase-Field kernels, six-equation model: 1 phasic, 0 mixture formulation
     int pf_hll;                // Phase-Field kernels: 1 HLL phase fluxes, 0 upwind/downwind
-    int muscl;                 // SCHEME 2: 0 Godunov, 1 minmod, 2 van Leer, 3 superbee, 4 MC (-1 otherwise)
+    int muscl;                 // SCHEME 2: 0 Godunov, 1 minmod, 2 van Leer, 3 superbee, 4 MC, 10 WENO3 (-1 otherwise)
     int riemann;               // Physics.RiemannSolver: 0 LLF, 1 HLL, 2 HLLC
     int order;                 // tile traversal order (tile_coords): 0 x fastest, 1 bricks of tiles
     int tile_base;             // single-box kernels: first tile (order 0) and number of tiles of the launch
@@ -454,8 +454,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                         for (int n = 0; n < N; ++n) {
                             const double w1 = smem[off[1] + n * str[1]], w2 = smem[off[2] + n * str[2]];
                             const double w3 = smem[off[3] + n * str[3]], w4 = smem[off[4] + n * str[4]];
-                            WfL[n] = muscl_face(w1, w2, w3, dxd, 1, lim);
-                            WfR[n] = muscl_face(w2, w3, w4, dxd, -1, lim);
+                            WfL[n] = face3(w1, w2, w3, dxd, 1, lim);
+                            WfR[n] = face3(w2, w3, w4, dxd, -1, lim);
                         }
                     } else {
 #pragma unroll
@@ -505,8 +505,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                         for (int n = 0; n < N; ++n) {
                             const float w1 = smem[off[1] + n * str[1]], w2 = smem[off[2] + n * str[2]];
                             const float w3 = smem[off[3] + n * str[3]], w4 = smem[off[4] + n * str[4]];
-                            wL[n] = muscl_face_f32(w1, w2, w3, 1, lim);
-                            wR[n] = muscl_face_f32(w2, w3, w4, -1, lim);
+                            wL[n] = face3_f32(w1, w2, w3, 1, lim);
+                            wR[n] = face3_f32(w2, w3, w4, -1, lim);
                         }
                     } else {
 #pragma unroll

@@ -109,7 +109,11 @@ Parm make_parm(const cmp_case* c) {
     auto& fv = p.FiniteVolume_Parm;
     fv.ID_WENO = c->id_weno;
     fv.ID_Limiter = c->id_limiter;
-    if (c->id_weno) {
+    if (c->id_weno && c->id_limiter == 3) {
+        fv.ID_Poly = 2;
+        fv.Num_Grow = 2;
+        fv.Scheme = FVReconstruction::WENO_3;
+    } else if (c->id_weno) {
         fv.ID_Poly = 4;
         fv.Num_Grow = 3;
         fv.Scheme = (c->id_limiter == 6) ? FVReconstruction::WENO_5B : FVReconstruction::WENO_5;

@@ -50,10 +50,11 @@ def test_scheme_keys():
                        ("MUSCL-Superbee", 3, 2), ("MUSCL-MC", 4, 2)]:
         p = cb.make_parm(cb.SIXEQS, 3, {"FiniteVolume.Scheme": v})
         assert (p.id_weno, p.id_limiter, p.num_grow) == (0, lim, ng), v
-    for v in ("WENO3", "WENO3B"):
-        with pytest.raises(cb.CompasError) as e:
-            cb.make_parm(cb.FIVEEQS, 2, {"FiniteVolume.Scheme": v})
-        assert e.value.code == cb.EUNSUPPORTED
+    p = cb.make_parm(cb.FIVEEQS, 2, {"FiniteVolume.Scheme": "WENO3"})
+    assert (p.id_weno, p.id_limiter, p.num_grow) == (1, 3, 2)
+    with pytest.raises(cb.CompasError) as e:
+        cb.make_parm(cb.FIVEEQS, 2, {"FiniteVolume.Scheme": "WENO3B"})
+    assert e.value.code == cb.EUNSUPPORTED
 
 
 def test_state_bytes_layout():

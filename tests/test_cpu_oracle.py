@@ -238,7 +238,7 @@ def test_sixeq_amr_oracle_conserves_composite_totals_periodic():
         assert abs(a - b) <= 1e-13 * abs(a)
 
 
-@pytest.mark.parametrize("scheme", ["GODUNOV", "MUSCL", "MUSCL-vanLeer", "MUSCL-Superbee", "MUSCL-MC"])
+@pytest.mark.parametrize("scheme", ["GODUNOV", "MUSCL", "MUSCL-vanLeer", "MUSCL-Superbee", "MUSCL-MC", "WENO3"])
 def test_muscl_reference_oracle_conserves_and_keeps_equilibrium(scheme):
     """The reference-header oracle with the GODUNOV / MUSCL reconstructions: conservation on the periodic
     square and the uniform pressure and velocity across the interface kept (the five-equation

@@ -73,6 +73,8 @@ def box_states(case_fn, kw, domain, dim, boxes, ng=3, xp=None, device=None):
         kw_l = dict(kw)
         if dim == 2 and "nx" in kw:
             kw_l.update(nx=kw["nx"] * scale, ny=kw["ny"] * scale)
+        elif "m" in kw:  # the triple point: 7m x 3m cells
+            kw_l.update(m=kw["m"] * scale)
         else:
             kw_l.update(n=kw["n"] * scale)
         phys, d, inputs, geom, U = case_fn(ng=ng, xp=xp, device=device, **kw_l)

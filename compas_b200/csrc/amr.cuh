@@ -167,12 +167,15 @@ __global__ void amr_bc_kernel(const AmrBc* t, long long n, AmrBufs B, int k, int
 }
 
 // face flux of face (i,j,k) (between cells i-1 and i along d) of a box with ghost-filled data U,
-// by the same sequence of device functions as the stage kernel (stage_kernel.cuh, step 2b)
+// by the same sequence of device functions as the stage kernel (stage_kernel.cuh, step 2b): WENO5 /
+// WENO5B (SCHEME 5 / 6) or the three-cell schemes (SCHEME 2, `code` as StageArgs::muscl), the N-phase
+// consistent limiter, the Riemann solver `id_riemann`
 template <class M, int SCHEME, bool MIX>
 __device__ void amr_face_flux(const double* U, const Grid& g, int d, int i, int j, int k, const Eos& e, int id_k,
-                              double* F, double* fnc, unsigned int* err) {
+                              int code, int id_riemann, double dxd, double* F, double* fnc, unsigned int* err) {
     using PT = typename std::conditional<MIX, float, double>::type;
     constexpr int N = M::N, D = M::D;
+    constexpr bool NPH = (M::KIND == kModelFiveN);
     PT P[6][N];
 #pragma unroll
     for (int s = 0; s < 6; ++s) {
@@ -201,14 +204,26 @@ __device__ void amr_face_flux(const double* U, const Grid& g, int d, int i, int 
             weno5b_masses(r1, r2, al, 1, WfL[0], WfL[1], WfL[M::IA]);
             weno5b_masses(r1 + 1, r2 + 1, al + 1, -1, WfR[0], WfR[1], WfR[M::IA]);
         }
+        if constexpr (SCHEME == 2) {
 #pragma unroll
-        for (int n = NB0; n < NB1; ++n) {
-            WfL[n] = weno5(P[0][n], P[1][n], P[2][n], P[3][n], P[4][n], 1);
-            WfR[n] = weno5(P[1][n], P[2][n], P[3][n], P[4][n], P[5][n], -1);
+            for (int n = 0; n < N; ++n) {
+                WfL[n] = face3(P[1][n], P[2][n], P[3][n], dxd, 1, code);
+                WfR[n] = face3(P[2][n], P[3][n], P[4][n], dxd, -1, code);
+            }
+        } else {
+#pragma unroll
+            for (int n = NB0; n < NB1; ++n) {
+                WfL[n] = weno5(P[0][n], P[1][n], P[2][n], P[3][n], P[4][n], 1);
+                WfR[n] = weno5(P[1][n], P[2][n], P[3][n], P[4][n], P[5][n], -1);
+            }
         }
         M::prim2cons(UL, WfL, e, err);
         M::prim2cons(UR, WfR, e, err);
-        M::hllc(F, fnc, cm, UL, UR, e, d, id_k, err);
+        if constexpr (NPH) {
+            M::consistent_limit(UL, P[2], 1, dxd, 1, e, err);
+            M::consistent_limit(UR, P[3], 1, dxd, -1, e, err);
+        }
+        riemann<M>(id_riemann, F, fnc, cm, UL, UR, e, d, id_k, err);
     } else {
         float wL[N], wR[N];
         if constexpr (SCHEME == 6) {
@@ -222,10 +237,18 @@ __device__ void amr_face_flux(const double* U, const Grid& g, int d, int i, int 
             weno5b_masses_f32(r1, r2, al, 1, wL[0], wL[1], wL[M::IA]);
             weno5b_masses_f32(r1 + 1, r2 + 1, al + 1, -1, wR[0], wR[1], wR[M::IA]);
         }
+        if constexpr (SCHEME == 2) {
 #pragma unroll
-        for (int n = NB0; n < NB1; ++n) {
-            wL[n] = weno5_f32(P[0][n], P[1][n], P[2][n], P[3][n], P[4][n], 1);
-            wR[n] = weno5_f32(P[1][n], P[2][n], P[3][n], P[4][n], P[5][n], -1);
+            for (int n = 0; n < N; ++n) {
+                wL[n] = face3_f32(P[1][n], P[2][n], P[3][n], 1, code);
+                wR[n] = face3_f32(P[2][n], P[3][n], P[4][n], -1, code);
+            }
+        } else {
+#pragma unroll
+            for (int n = NB0; n < NB1; ++n) {
+                wL[n] = weno5_f32(P[0][n], P[1][n], P[2][n], P[3][n], P[4][n], 1);
+                wR[n] = weno5_f32(P[1][n], P[2][n], P[3][n], P[4][n], P[5][n], -1);
+            }
         }
 #pragma unroll
         for (int n = 0; n < N; ++n) {
@@ -234,9 +257,17 @@ __device__ void amr_face_flux(const double* U, const Grid& g, int d, int i, int 
         }
         M::prim2cons(UL, WfL, e, err);
         M::prim2cons(UR, WfR, e, err);
-        float cmf;
-        if constexpr (M::NC == 1) fiveeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, e, d, id_k);
-        else sixeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, e, d);
+        if constexpr (NPH) {
+            M::consistent_limit(UL, P[2], 1, dxd, 1, e, err);
+            M::consistent_limit(UR, P[3], 1, dxd, -1, e, err);
+            riemann<M>(id_riemann, F, fnc, cm, UL, UR, e, d, id_k, err);
+        } else if (id_riemann != 2) {
+            riemann_llf_hll<M>(id_riemann, F, fnc, cm, UL, UR, e, d, id_k, err);
+        } else {
+            float cmf;
+            if constexpr (M::KIND == kModelFive) fiveeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, e, d, id_k);
+            else sixeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, e, d);
+        }
     }
 }
 
@@ -252,6 +283,9 @@ struct AmrCfArgs {
     double dA[3];       // face areas of the level computing the fluxes
     Eos e;
     int id_k;
+    int code;           // three-cell scheme code (SCHEME 2)
+    int id_riemann;     // Physics.RiemannSolver
+    double dx[3];       // cell sizes of the level computing the fluxes
     int role;           // 0: coarse (CrseInit, scale -w), 1: fine (FineAdd, scale w)
 };
 
@@ -261,17 +295,19 @@ __global__ void amr_cf_kernel(AmrCfArgs A) {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < A.n; t += gridDim.x * blockDim.x) {
         const AmrCf& f = A.cf[t];
         const double dA = (f.d == 0) ? A.dA[0] : (f.d == 1 ? A.dA[1] : A.dA[2]);
+        const double dxd = (f.d == 0) ? A.dx[0] : (f.d == 1 ? A.dx[1] : A.dx[2]);
         double F[N], fnc[NC];
         if (A.role == 0) {
             amr_face_flux<M, SCHEME, MIX>(A.B.p[f.cbox * 4 + A.k], A.grids[f.cbox], f.d, f.cface[0], f.cface[1],
-                                          f.cface[2], A.e, A.id_k, F, fnc, nullptr);
+                                          f.cface[2], A.e, A.id_k, A.code, A.id_riemann, dxd, F, fnc, nullptr);
             for (int c = 0; c < N; ++c) A.reg[(long long)t * N + c] += (-A.w) * (F[c] * dA);
             for (int c = 0; c < NC; ++c) A.reg_nc[(long long)t * NC + c] += (-A.w) * (fnc[c] * dA);
         } else {
             const int nf = (M::D == 3) ? 4 : 2;
             for (int a = 0; a < nf; ++a) {
                 amr_face_flux<M, SCHEME, MIX>(A.B.p[f.fbox[a] * 4 + A.k], A.grids[f.fbox[a]], f.d, f.fface[a][0],
-                                              f.fface[a][1], f.fface[a][2], A.e, A.id_k, F, fnc, nullptr);
+                                              f.fface[a][1], f.fface[a][2], A.e, A.id_k, A.code, A.id_riemann, dxd, F,
+                                              fnc, nullptr);
                 for (int c = 0; c < N; ++c) A.reg[(long long)t * N + c] += A.w * (F[c] * dA);
                 for (int c = 0; c < NC; ++c) A.reg_nc[(long long)t * NC + c] += A.w * (fnc[c] * dA);
             }
@@ -299,7 +335,9 @@ __global__ void amr_reflux_kernel(const AmrCf* cf, const int* groups, int ngroup
         for (int c = 0; c < N; ++c) Uc[c] = U[c * S + f0.cq];
         M::cons2prim(W, Uc, e, nullptr);
         double src = 0.0;
+        double srck[(M::KIND == kModelFiveN) ? M::NP : 1];
         if constexpr (M::KIND == kModelFive) src = M::kapila_factor(Uc, W, e, id_k, nullptr);
+        if constexpr (M::KIND == kModelFiveN) M::kapila_factors(srck, W, e, id_k, nullptr);
         double xs[NC];
         for (int t = t0; t < t1; ++t) {
             const double mult = cf[t].hi_side ? -1.0 : 1.0;
@@ -311,6 +349,9 @@ __global__ void amr_reflux_kernel(const AmrCf* cf, const int* groups, int ngroup
         }
         if constexpr (M::KIND == kModelFive) {
             U[M::IA * S + f0.cq] += -1.0 * (xs[0] * src);
+        } else if constexpr (M::KIND == kModelFiveN) {
+            // source/Class_Compressible5Eq_NPhase_PhaseField.cpp:89-110: alpha_k -= xi phi_k (1 + K_k)
+            for (int kk = 0; kk < M::NP; ++kk) U[(M::IA + kk) * S + f0.cq] += -1.0 * (srck[kk] * xs[0]);
         } else {
             const double divv = -xs[0], dva1 = -xs[1], dva2 = -xs[2];
             const double rho = W[0] + W[1];

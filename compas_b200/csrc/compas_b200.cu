@@ -1731,6 +1731,7 @@ static int batch_sync_list(compas_b200_batch* b, cudaStream_t st) {
         B.id_k = c.p.source_term;
         B.relax = (c.p.physics == COMPAS_B200_SIXEQS) ? c.p.relaxation : 0;
         B.riemann = c.p.id_riemann;
+        B.muscl = c.p.id_weno ? (c.p.id_limiter == 3 ? 10 : -1) : c.p.id_limiter;
         B.trace = c.p.relax_trace;
         B.tiles = tile_count(b->dim, B.g);
         B.ghosts = ghost_count(B.g);

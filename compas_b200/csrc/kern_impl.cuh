@@ -155,7 +155,8 @@ static cudaError_t launch_list_s(const KernelChoice& k, const ListArgs& L, cudaS
 
 template <class M>
 static cudaError_t launch_list_m(const KernelChoice& k, const ListArgs& L, cudaStream_t st) {
-    if (k.limiter < 5) return cudaErrorNotSupported;  // the box list runs WENO5 / WENO5B
+    if (k.limiter < 5)  // GODUNOV / MUSCL / WENO3 family
+        return (k.precision == 1) ? launch_list_s<M, 2, true>(k, L, st) : launch_list_s<M, 2, false>(k, L, st);
     if constexpr (M::KIND == kModelFiveN) {
         if (k.limiter == 6) return cudaErrorNotSupported;
         return (k.precision == 1) ? launch_list_s<M, 5, true>(k, L, st) : launch_list_s<M, 5, false>(k, L, st);

@@ -130,6 +130,7 @@ struct FiveEq {
     static constexpr int N = 4 + DIM;
     static constexpr int NC = 1;       // face quantities of the non-conservative terms
     static constexpr int NCPF = 1;     // of the Phase-Field step (none: FluxNC stays 0)
+    static constexpr int NP = 2;        // phases
     static constexpr int IM = 2;        // rho u_d (u_d among the primitives)
     static constexpr int IE = 2 + DIM;  // total energy
     static constexpr int IA = 3 + DIM;  // alpha1
@@ -415,6 +416,7 @@ struct SixEq {
     static constexpr int N = 5 + DIM;
     static constexpr int NC = 3;        // u_n, (u a1p1)_n, (u a2p2)_n
     static constexpr int NCPF = 4;      // Phase-Field step: J1 r1, J2 r2, J1 r1 EK, J2 r2 EK
+    static constexpr int NP = 2;        // phases
     static constexpr int IM = 2;        // rho u_d (u_d among the primitives)
     static constexpr int IE1 = 2 + DIM;
     static constexpr int IE2 = 3 + DIM;

@@ -748,6 +748,7 @@ struct BoxDesc {
     int id_k;
     int relax;
     int riemann;                  // Physics.RiemannSolver of the box's case (0 LLF, 1 HLL, 2 HLLC)
+    int muscl;                    // three-cell scheme code of the box's case (StageArgs::muscl)
     double trace;
     int tiles;                    // tiles of the box for the kernel's tile shape
     long long ghosts;             // ghost cells of one array of the box
@@ -814,7 +815,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_list_kernel(ListArgs L) {
             sa.tile_count = 0;
             sa.pf_phasic = 0;
             sa.pf_hll = 0;
-            sa.muscl = -1;
+            sa.muscl = B.muscl;
             sa.riemann = B.riemann;
             for (int d = 0; d < 3; ++d) sa.gq[d] = nullptr;
         }

@@ -922,9 +922,7 @@ void pf_step(const cmp_case* c, const cmp_pf* pf, double* U, double dt, double* 
 }
 #endif  // PHYSICS == FIVEEQS || PHYSICS == SIXEQS
 
-#if (PHYSICS != FIVEEQS_NPHASE)
 #include "ref_amr.inc"
-#endif
 
 template <class Fn>
 int guarded(Fn&& fn) {
@@ -1098,14 +1096,9 @@ int cmp_advance_pf(const cmp_case* c, const cmp_pf* pf, double* U, int nsteps, d
 
 int cmp_amr_advance(const cmp_case* c, int nlev, const cmp_amr_box* boxes, int nbox, double** U, int nsteps,
                     double stop_time, double* t, double* dts) {
-#if (PHYSICS != FIVEEQS_NPHASE)
     int taken = 0;
     int rc = guarded([&] { taken = amr_advance(c, nlev, boxes, nbox, U, nsteps, stop_time, t, dts); });
     return rc == 0 ? taken : rc;
-#else
-    (void)c; (void)nlev; (void)boxes; (void)nbox; (void)U; (void)nsteps; (void)stop_time; (void)t; (void)dts;
-    return -2;
-#endif
 }
 
 }  // extern "C"

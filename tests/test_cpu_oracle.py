@@ -263,3 +263,24 @@ def test_port_rejects_the_muscl_family():
     p, g = _parm_geom(phys, dim, dict(inputs, **{"FiniteVolume.Scheme": "MUSCL-MC"}), geom)
     with pytest.raises(RuntimeError):
         Oracle("port", p, g).advance(U, 1)
+
+
+@pytest.mark.skipif(not have_ref(cb.FIVEEQS_NPHASE, 2, 3), reason="reference-header oracle not built here")
+def test_nphase_amr_oracle_conserves_masses_and_energy():
+    """N-phase (NPHASE 3) multi-level advance of the oracle on the triple point with the MUSCL-MC of its
+    example (flux registers, the per-phase alpha_k reflux source terms): behind reflecting walls the
+    composite masses and total energy are conserved to round-off."""
+    from compas_b200 import amr
+
+    kw = dict(m=8)
+    phys, dim, inputs, geom, _ = cases.triple_point(**kw)
+    p, g = _parm_geom(phys, dim, dict(inputs, **{"FiniteVolume.Scheme": "MUSCL-MC"}), geom)
+    boxes = amr.hierarchy((56, 24), 2, [((8, 8, 0), (47, 39, 0)), ((24, 24, 0), (71, 55, 0))], 16)
+    states = amr.box_states(cases.triple_point, kw, (56, 24), 2, boxes)
+    cov = amr.covered_mask_fn(boxes, 2)
+    comps = (0, 1, 2, 5)  # the three partial densities, the total energy
+    s0 = [amr.composite_sum(states, boxes, 2, 3, c, cov) for c in comps]
+    Oracle("reference", p, g).amr_advance(boxes, states, 4)
+    s1 = [amr.composite_sum(states, boxes, 2, 3, c, cov) for c in comps]
+    for a, b in zip(s0, s1):
+        assert abs(a - b) <= 1e-13 * abs(a)

@@ -262,7 +262,8 @@ __device__ void amr_face_flux(const double* U, const Grid& g, int d, int i, int 
             M::consistent_limit(UR, P[3], 1, dxd, -1, e, err);
             riemann<M>(id_riemann, F, fnc, cm, UL, UR, e, d, id_k, err);
         } else if (id_riemann != 2) {
-            riemann_llf_hll<M>(id_riemann, F, fnc, cm, UL, UR, e, d, id_k, err);
+            float cmf;
+            llf_hll_mixed<M>(id_riemann, F, fnc, cmf, UL, UR, wL, wR, e, d, id_k);
         } else {
             float cmf;
             if constexpr (M::KIND == kModelFive) fiveeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, e, d, id_k);

@@ -337,27 +337,33 @@ struct FiveEq {
 // primitives (w); the star states and fluxes are assembled in FP64 from the FP64 face states U, so
 // that the large energy (alpha B ~ 1e9) enters only through f*E and stays consistent with the
 // alpha flux f*alpha (the pressure recovered from E - sum alpha_k B_k is not polluted).
+// FP32 sound speeds of the mixed Riemann solvers from FP32 face primitives: five-equation mixture
+// (K = 0: frozen, K = 1: Wood), six-equation frozen.
+template <int DIM>
+__device__ __forceinline__ float fiveeq_c_f32(const float* w, const Eos& e, int id_k) {
+    using M = FiveEq<DIM>;
+    constexpr int IE = M::IE, IA = M::IA;
+    const float p = w[IE], a1 = w[IA], a2 = 1.0f - a1;
+    const float A1 = (float)e.A1, A2 = (float)e.A2, B1 = (float)e.B1, B2 = (float)e.B2;
+    const float r1 = __fdividef(__fmaf_rn(A1 + 1.0f, p, B1), A1);
+    const float r2 = __fdividef(__fmaf_rn(A2 + 1.0f, p, B2), A2);
+    const float ph1 = (e.C1 > 0.0) ? a1 - (float)e.C1 * w[0] : a1;
+    const float ph2 = (e.C2 > 0.0) ? a2 - (float)e.C2 * w[1] : a2;
+    float rc2;
+    if (id_k == 0)
+        rc2 = __fdividef(__fmaf_rn(a1 * A1, r1, (a2 * A2) * r2), __fmaf_rn(ph1, A1, ph2 * A2));
+    else
+        rc2 = __fdividef(1.0f, __fdividef(ph1, r1) + __fdividef(ph2, r2));
+    return sqrtf(fmaxf(rc2, 0.0f) / (w[0] + w[1]));
+}
+
 template <int DIM>
 __device__ __forceinline__ void fiveeq_hllc_mixed(double* Fout, double* fnc, float& cmax, const double* UL,
                                                   const double* UR, const float* wL, const float* wR,
                                                   const Eos& e, int d, int id_k) {
     using M = FiveEq<DIM>;
     constexpr int N = M::N, IE = M::IE, IA = M::IA;
-    auto csound = [&](const float* w) {
-        const float p = w[IE], a1 = w[IA], a2 = 1.0f - a1;
-        const float A1 = (float)e.A1, A2 = (float)e.A2, B1 = (float)e.B1, B2 = (float)e.B2;
-        const float r1 = __fdividef(__fmaf_rn(A1 + 1.0f, p, B1), A1);
-        const float r2 = __fdividef(__fmaf_rn(A2 + 1.0f, p, B2), A2);
-        const float ph1 = (e.C1 > 0.0) ? a1 - (float)e.C1 * w[0] : a1;
-        const float ph2 = (e.C2 > 0.0) ? a2 - (float)e.C2 * w[1] : a2;
-        float rc2;
-        if (id_k == 0)
-            rc2 = __fdividef(__fmaf_rn(a1 * A1, r1, (a2 * A2) * r2), __fmaf_rn(ph1, A1, ph2 * A2));
-        else
-            rc2 = __fdividef(1.0f, __fdividef(ph1, r1) + __fdividef(ph2, r2));
-        return sqrtf(fmaxf(rc2, 0.0f) / (w[0] + w[1]));
-    };
-    const float cL = csound(wL), cR = csound(wR);
+    const float cL = fiveeq_c_f32<DIM>(wL, e, id_k), cR = fiveeq_c_f32<DIM>(wR, e, id_k);
     const float VL = (d == 0) ? wL[2] : ((d == 1 || DIM == 2) ? wL[3] : wL[DIM == 3 ? 4 : 3]);
     const float VR = (d == 0) ? wR[2] : ((d == 1 || DIM == 2) ? wR[3] : wR[DIM == 3 ? 4 : 3]);
     const float pL = wL[IE], pR = wR[IE];
@@ -626,20 +632,24 @@ struct SixEq {
 // star states are written E* = f E + (V alpha p - S* (alpha p)*)/(S* - S), the identity of
 // Riemann_HLLC_Compressible6Eq.H:163-200 with (V - S)/(S* - S) = f, so that E enters only through f.
 template <int DIM>
+__device__ __forceinline__ float sixeq_c_f32(const float* w, const Eos& e) {
+    using M = SixEq<DIM>;
+    constexpr int IE1 = M::IE1, IE2 = M::IE2, IA = M::IA;
+    const float a1 = w[IA];
+    const float xi1 = (e.C1 > 0.0 && a1 > 0.0f) ? 1.0f - (float)e.C1 * __fdividef(w[0], a1) : 1.0f;
+    const float xi2 = (e.C2 > 0.0 && 1.0f - a1 > 0.0f) ? 1.0f - (float)e.C2 * __fdividef(w[1], 1.0f - a1) : 1.0f;
+    const float r1 = __fdividef(__fmaf_rn((float)e.A1 + 1.0f, w[IE1], a1 * (float)e.B1), (float)e.A1 * xi1);
+    const float r2 = __fdividef(__fmaf_rn((float)e.A2 + 1.0f, w[IE2], (1.0f - a1) * (float)e.B2), (float)e.A2 * xi2);
+    return sqrtf(fmaxf(r1 + r2, 0.0f) / (w[0] + w[1]));
+}
+
+template <int DIM>
 __device__ __forceinline__ void sixeq_hllc_mixed(double* Fout, double* fnc, float& cmax, const double* UL,
                                                  const double* UR, const float* wL, const float* wR,
                                                  const Eos& e, int d) {
     using M = SixEq<DIM>;
     constexpr int N = M::N, IE1 = M::IE1, IE2 = M::IE2, IA = M::IA;
-    auto csound = [&](const float* w) {
-        const float a1 = w[IA];
-        const float xi1 = (e.C1 > 0.0 && a1 > 0.0f) ? 1.0f - (float)e.C1 * __fdividef(w[0], a1) : 1.0f;
-        const float xi2 = (e.C2 > 0.0 && 1.0f - a1 > 0.0f) ? 1.0f - (float)e.C2 * __fdividef(w[1], 1.0f - a1) : 1.0f;
-        const float r1 = __fdividef(__fmaf_rn((float)e.A1 + 1.0f, w[IE1], a1 * (float)e.B1), (float)e.A1 * xi1);
-        const float r2 = __fdividef(__fmaf_rn((float)e.A2 + 1.0f, w[IE2], (1.0f - a1) * (float)e.B2), (float)e.A2 * xi2);
-        return sqrtf(fmaxf(r1 + r2, 0.0f) / (w[0] + w[1]));
-    };
-    const float cL = csound(wL), cR = csound(wR);
+    const float cL = sixeq_c_f32<DIM>(wL, e), cR = sixeq_c_f32<DIM>(wR, e);
     const float VL = (d == 0) ? wL[2] : ((d == 1 || DIM == 2) ? wL[3] : wL[DIM == 3 ? 4 : 3]);
     const float VR = (d == 0) ? wR[2] : ((d == 1 || DIM == 2) ? wR[3] : wR[DIM == 3 ? 4 : 3]);
     const float SL = fminf(VL - cL, VR - cR), SR = fmaxf(VL + cL, VR + cR);

@@ -166,6 +166,74 @@ __device__ __forceinline__ void riemann_llf_hll(int hll, double* Fout, double* f
     cmax = dmax(cL + sqrt(ksum<D>(WL + IU)), cR + sqrt(ksum<D>(WR + IU)));
 }
 
+// Mixed precision LLF / HLL of the two-phase models: wave speeds in FP32 from the FP32 face primitives
+// (the sound speeds of the mixed HLLC), the fluxes assembled component by component in FP64 as
+// a FL + b FR + c (UR - UL) (LLF: a = b = 1/2, c = -lambda/2; HLL: a = Sp/(Sp - Sm), b = -Sm/(Sp - Sm),
+// c = Sp Sm/(Sp - Sm)), without per-side flux arrays.
+template <class M>
+__device__ __forceinline__ void llf_hll_mixed(int hll, double* Fout, double* fnc, float& cmax, const double* UL,
+                                              const double* UR, const float* wL, const float* wR, const Eos& e, int d,
+                                              int id_k) {
+    constexpr int N = M::N, D = M::D;
+    constexpr bool SIX = (M::KIND == kModelSix);
+    float cL, cR;
+    if constexpr (SIX) {
+        cL = sixeq_c_f32<D>(wL, e);
+        cR = sixeq_c_f32<D>(wR, e);
+    } else {
+        cL = fiveeq_c_f32<D>(wL, e, id_k);
+        cR = fiveeq_c_f32<D>(wR, e, id_k);
+    }
+    const float VL = (d == 0) ? wL[2] : ((d == 1 || D == 2) ? wL[3] : wL[D == 3 ? 4 : 3]);
+    const float VR = (d == 0) ? wR[2] : ((d == 1 || D == 2) ? wR[3] : wR[D == 3 ? 4 : 3]);
+    double a, b, c;
+    if (!hll) {
+        const float lam = fmaxf(fabsf(VL) + cL, fabsf(VR) + cR);
+        a = 0.5;
+        b = 0.5;
+        c = -0.5 * (double)lam;
+    } else {
+        const double Sp = fmaxf(0.0f, fmaxf(VL + cL, VR + cR)), Sm = fminf(0.0f, fminf(VL - cL, VR - cR));
+        const double inv = 1.0 / (Sp - Sm);
+        a = Sp * inv;
+        b = -Sm * inv;
+        c = (Sp * Sm) * inv;
+    }
+    const double VLd = VL, VRd = VR;
+    double pl[2], pr[2];
+    if constexpr (SIX) {
+        pl[0] = wL[M::IE1]; pl[1] = wL[M::IE2];
+        pr[0] = wR[M::IE1]; pr[1] = wR[M::IE2];
+    } else {
+        pl[0] = wL[M::IE]; pl[1] = 0.0;
+        pr[0] = wR[M::IE]; pr[1] = 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        double fl = UL[i] * VLd, fr = UR[i] * VRd;
+        if (i >= 2 && i < 2 + D && i - 2 == d) {
+            fl += pl[0] + pl[1];
+            fr += pr[0] + pr[1];
+        } else if (SIX && (i == M::IA - 2 || i == M::IA - 1)) {
+            const int k = i - (M::IA - 2);  // phase energies: (alpha_k rho_k E_k + alpha_k p_k) V
+            fl = (UL[i] + pl[k]) * VLd;
+            fr = (UR[i] + pr[k]) * VRd;
+        } else if (!SIX && i == M::IA - 1) {
+            fl = (UL[i] + pl[0]) * VLd;
+            fr = (UR[i] + pr[0]) * VRd;
+        }
+        Fout[i] = a * fl + b * fr + c * (UR[i] - UL[i]);
+    }
+    fnc[0] = a * VLd + b * VRd;
+    if constexpr (SIX) {
+        fnc[1] = a * (VLd * pl[0]) + b * (VRd * pr[0]);
+        fnc[2] = a * (VLd * pl[1]) + b * (VRd * pr[1]);
+    }
+    float kL = wL[2] * wL[2] + wL[3] * wL[3], kR = wR[2] * wR[2] + wR[3] * wR[3];
+    if (D == 3) { kL += wL[4] * wL[4]; kR += wR[4] * wR[4]; }
+    cmax = fmaxf(cL + sqrtf(kL), cR + sqrtf(kR));
+}
+
 // Physics.RiemannSolver: 0 LLF, 1 HLL, 2 HLLC (source/Class_Compressible_PhaseField.cpp:92-111).
 template <class M>
 __device__ __forceinline__ void riemann(int id_riemann, double* Fout, double* fnc, double& cmax, const double* UL,
@@ -540,9 +608,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                                                a.pf_hll, err);
                         cmf = 0.0f;
                     } else if (a.riemann != 2) {
-                        double cmd;
-                        riemann_llf_hll<M>(a.riemann, F, fnc, cmd, UL, UR, a.e, d, a.id_k, err);
-                        cmf = (float)cmd;
+                        llf_hll_mixed<M>(a.riemann, F, fnc, cmf, UL, UR, wL, wR, a.e, d, a.id_k);
                     } else if constexpr (M::KIND == kModelFive) {
                         fiveeq_hllc_mixed<D>(F, fnc, cmf, UL, UR, wL, wR, a.e, d, a.id_k);
                     } else {

@@ -189,11 +189,19 @@ __device__ void amr_face_flux(const double* U, const Grid& g, int d, int i, int 
         else M::cons2prim(P[s], Uc, e, nullptr);
     }
     double WfL[N], WfR[N], UL[N], UR[N];
-    constexpr int NB0 = (SCHEME == 6) ? 2 : 0;
+    constexpr int NB0 = (SCHEME == 6) ? M::IM : 0;
     constexpr int NB1 = (SCHEME == 6) ? M::IA : N;
     double cm;
     if constexpr (!MIX) {
-        if constexpr (SCHEME == 6) {
+        if constexpr (SCHEME == 6 && NPH) {
+            double rf[M::NP], af[M::NP];
+            weno5b_nphase<M::NP, double>([&](int k, int s) { return (double)P[s][k]; },
+                                         [&](int k, int s) { return (double)P[s][M::IA + k]; }, 1, rf, af);
+            for (int k = 0; k < M::NP; ++k) { WfL[k] = rf[k]; WfL[M::IA + k] = af[k]; }
+            weno5b_nphase<M::NP, double>([&](int k, int s) { return (double)P[s + 1][k]; },
+                                         [&](int k, int s) { return (double)P[s + 1][M::IA + k]; }, -1, rf, af);
+            for (int k = 0; k < M::NP; ++k) { WfR[k] = rf[k]; WfR[M::IA + k] = af[k]; }
+        } else if constexpr (SCHEME == 6) {
             double r1[6], r2[6], al[6];
 #pragma unroll
             for (int s = 0; s < 6; ++s) {
@@ -219,14 +227,19 @@ __device__ void amr_face_flux(const double* U, const Grid& g, int d, int i, int 
         }
         M::prim2cons(UL, WfL, e, err);
         M::prim2cons(UR, WfR, e, err);
-        if constexpr (NPH) {
+        if constexpr (NPH && SCHEME != 6) {
             M::consistent_limit(UL, P[2], 1, dxd, 1, e, err);
             M::consistent_limit(UR, P[3], 1, dxd, -1, e, err);
         }
         riemann<M>(id_riemann, F, fnc, cm, UL, UR, e, d, id_k, err);
     } else {
         float wL[N], wR[N];
-        if constexpr (SCHEME == 6) {
+        if constexpr (SCHEME == 6 && NPH) {
+            weno5b_nphase<M::NP, float>([&](int k, int s) { return (float)P[s][k]; },
+                                        [&](int k, int s) { return (float)P[s][M::IA + k]; }, 1, wL, wL + M::IA);
+            weno5b_nphase<M::NP, float>([&](int k, int s) { return (float)P[s + 1][k]; },
+                                        [&](int k, int s) { return (float)P[s + 1][M::IA + k]; }, -1, wR, wR + M::IA);
+        } else if constexpr (SCHEME == 6) {
             float r1[6], r2[6], al[6];
 #pragma unroll
             for (int s = 0; s < 6; ++s) {
@@ -258,8 +271,10 @@ __device__ void amr_face_flux(const double* U, const Grid& g, int d, int i, int 
         M::prim2cons(UL, WfL, e, err);
         M::prim2cons(UR, WfR, e, err);
         if constexpr (NPH) {
-            M::consistent_limit(UL, P[2], 1, dxd, 1, e, err);
-            M::consistent_limit(UR, P[3], 1, dxd, -1, e, err);
+            if constexpr (SCHEME != 6) {
+                M::consistent_limit(UL, P[2], 1, dxd, 1, e, err);
+                M::consistent_limit(UR, P[3], 1, dxd, -1, e, err);
+            }
             riemann<M>(id_riemann, F, fnc, cm, UL, UR, e, d, id_k, err);
         } else if (id_riemann != 2) {
             float cmf;

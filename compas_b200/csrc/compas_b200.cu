@@ -336,9 +336,6 @@ static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
     if (p->physics == COMPAS_B200_FIVEEQS_NPHASE) {
         if (!nphase_built(p->dim, p->nphase))
             return fail(COMPAS_B200_EUNSUPPORTED, "FIVEEQS_NPHASE: this build runs NPHASE 2, 3, 4 in 2D and 3 in 3D");
-        if (p->id_weno && p->id_limiter != 5 && p->id_limiter != 3)
-            return fail(COMPAS_B200_EUNSUPPORTED, "FIVEEQS_NPHASE: this engine runs FiniteVolume.Scheme = WENO5, "
-                                                  "WENO3, GODUNOV and MUSCL-*");
         if (p->thinc) return fail(COMPAS_B200_EUNSUPPORTED, "FIVEEQS_NPHASE: FiniteVolume.THINC is not in this engine");
     }
     if (p->id_weno ? (p->id_limiter != 3 && p->id_limiter != 5 && p->id_limiter != 6)
@@ -1763,8 +1760,8 @@ int compas_b200_batch_create_nphase(int physics, int dim, int nphase, int id_lim
     compas_b200_parm probe;
     int rc = compas_b200_parm_init_nphase(&probe, physics, dim, nphase);
     if (rc) return rc;
-    if (physics == COMPAS_B200_FIVEEQS_NPHASE && (!nphase_built(dim, nphase) || id_limiter != 5))
-        return fail(COMPAS_B200_EUNSUPPORTED, "FIVEEQS_NPHASE batches: WENO5, NPHASE 2, 3, 4 in 2D and 3 in 3D");
+    if (physics == COMPAS_B200_FIVEEQS_NPHASE && !nphase_built(dim, nphase))
+        return fail(COMPAS_B200_EUNSUPPORTED, "FIVEEQS_NPHASE batches: NPHASE 2, 3, 4 in 2D and 3 in 3D");
     if (id_limiter != 5 && id_limiter != 6) return fail(COMPAS_B200_EUNSUPPORTED, "WENO5 (5) or WENO5B (6)");
     if (precision != 0 && precision != 1) return fail(COMPAS_B200_EARG, "precision 0 or 1");
     if (capacity < 1 || capacity > (1 << 20)) return fail(COMPAS_B200_EARG, "capacity out of range");

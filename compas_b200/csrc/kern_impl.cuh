@@ -115,8 +115,8 @@ static cudaError_t launch_stage_m(const KernelChoice& k, const StageArgs& a, cud
     if (k.limiter < 5)  // GODUNOV / MUSCL family
         return mix ? launch_stage_var<M, 2, true>(k, a, st, tm) : launch_stage_var<M, 2, false>(k, a, st, tm);
     if constexpr (M::KIND == kModelFiveN) {
-        if (bounded) return cudaErrorNotSupported;
-        return mix ? launch_stage_var<M, 5, true>(k, a, st, tm) : launch_stage_var<M, 5, false>(k, a, st, tm);
+        if (mix) return bounded ? launch_stage_var<M, 6, true>(k, a, st, tm) : launch_stage_var<M, 5, true>(k, a, st, tm);
+        return bounded ? launch_stage_var<M, 6, false>(k, a, st, tm) : launch_stage_var<M, 5, false>(k, a, st, tm);
     } else {
         if (mix)
             return bounded ? launch_stage_var<M, 6, true>(k, a, st, tm) : launch_stage_var<M, 5, true>(k, a, st, tm);
@@ -158,8 +158,9 @@ static cudaError_t launch_list_m(const KernelChoice& k, const ListArgs& L, cudaS
     if (k.limiter < 5)  // GODUNOV / MUSCL / WENO3 family
         return (k.precision == 1) ? launch_list_s<M, 2, true>(k, L, st) : launch_list_s<M, 2, false>(k, L, st);
     if constexpr (M::KIND == kModelFiveN) {
-        if (k.limiter == 6) return cudaErrorNotSupported;
-        return (k.precision == 1) ? launch_list_s<M, 5, true>(k, L, st) : launch_list_s<M, 5, false>(k, L, st);
+        if (k.precision == 1)
+            return (k.limiter == 6) ? launch_list_s<M, 6, true>(k, L, st) : launch_list_s<M, 5, true>(k, L, st);
+        return (k.limiter == 6) ? launch_list_s<M, 6, false>(k, L, st) : launch_list_s<M, 5, false>(k, L, st);
     } else {
         if (k.precision == 1)
             return (k.limiter == 6) ? launch_list_s<M, 6, true>(k, L, st) : launch_list_s<M, 5, true>(k, L, st);

@@ -1087,4 +1087,82 @@ __device__ __forceinline__ void weno5b_masses_f32(const float* ar1, const float*
     alpha1_f = __fmaf_rn(Th, a1 - al1[2], al1[2]);
 }
 
+// N-phase WENO5B (include/Operators_Compressible5Eq_NPhase/FVM_Reconstruction2Face_Conservative_WENO5B_D_Compressible5Eq_NPhase.H):
+// the steps of weno5b_masses for NP phases whose volume fractions are all state variables. r(k, s) and
+// a(k, s) give alpha_k rho_k and alpha_k of stencil cell s = 0..4 (centre 2); the face values of side
+// `side` go to rf[k], af[k]. PT = double: the reference's arithmetic; PT = float: the mixed form.
+template <int NP, class PT, class FR, class FA>
+__device__ __forceinline__ void weno5b_nphase(FR r, FA a, int side, PT* rf, PT* af) {
+    constexpr bool F32 = std::is_same<PT, float>::value;
+    PT rL[NP], rR[NP], aL[NP], aR[NP];
+    PT sumL = 0, sumR = 0;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+        const PT fr[5] = {r(k, 0), r(k, 1), r(k, 2), r(k, 3), r(k, 4)};
+        const PT fa[5] = {a(k, 0), a(k, 1), a(k, 2), a(k, 3), a(k, 4)};
+        PT th;
+        if constexpr (F32) {
+            float e[3], w[3], ea[3];
+            weno5_f32_parts(fr[0], fr[1], fr[2], fr[3], fr[4], 1, e, w);
+            weno5_f32_parts(fa[0], fa[1], fa[2], fa[3], fa[4], 1, ea, nullptr);
+            rL[k] = fr[2] + __fmaf_rn(w[0], e[0], __fmaf_rn(w[1], e[1], w[2] * e[2]));
+            aL[k] = fa[2] + __fmaf_rn(w[0], ea[0], __fmaf_rn(w[1], ea[1], w[2] * ea[2]));
+            weno5_f32_parts(fr[0], fr[1], fr[2], fr[3], fr[4], -1, e, w);
+            weno5_f32_parts(fa[0], fa[1], fa[2], fa[3], fa[4], -1, ea, nullptr);
+            rR[k] = fr[2] + __fmaf_rn(w[0], e[0], __fmaf_rn(w[1], e[1], w[2] * e[2]));
+            aR[k] = fa[2] + __fmaf_rn(w[0], ea[0], __fmaf_rn(w[1], ea[1], w[2] * ea[2]));
+            th = fminf(bound_min_theta_f32(fr[2], rL[k], rR[k]), bound_min_theta_f32(fa[2], aL[k], aR[k]));
+            rL[k] = __fmaf_rn(th, rL[k] - fr[2], fr[2]);
+            aL[k] = __fmaf_rn(th, aL[k] - fa[2], fa[2]);
+            rR[k] = __fmaf_rn(th, rR[k] - fr[2], fr[2]);
+            aR[k] = __fmaf_rn(th, aR[k] - fa[2], fa[2]);
+        } else {
+            double q[3], w[3], qa[3];
+            weno5_parts(fr[0], fr[1], fr[2], fr[3], fr[4], 1, q, w);
+            rL[k] = weno_sum(q, w);
+            weno5_parts(fa[0], fa[1], fa[2], fa[3], fa[4], 1, qa, nullptr);
+            aL[k] = weno_sum(qa, w);
+            weno5_parts(fr[0], fr[1], fr[2], fr[3], fr[4], -1, q, w);
+            rR[k] = weno_sum(q, w);
+            weno5_parts(fa[0], fa[1], fa[2], fa[3], fa[4], -1, qa, nullptr);
+            aR[k] = weno_sum(qa, w);
+            th = dmin(bound_min_theta(fr[2], rL[k], rR[k]), bound_min_theta(fa[2], aL[k], aR[k]));
+            rL[k] = fr[2] + th * (rL[k] - fr[2]);
+            aL[k] = fa[2] + th * (aL[k] - fa[2]);
+            rR[k] = fr[2] + th * (rR[k] - fr[2]);
+            aR[k] = fa[2] + th * (aR[k] - fa[2]);
+        }
+        sumL += aL[k];
+        sumR += aR[k];
+    }
+    PT Th = 1;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+        const PT rc = r(k, 2), ac = a(k, 2);
+        rL[k] /= sumL;
+        aL[k] /= sumL;
+        rR[k] /= sumR;
+        aR[k] /= sumR;
+        if constexpr (F32) {
+            Th = fminf(Th, fminf(bound_min_theta_f32(rc, rL[k], rR[k]), bound_min_theta_f32(ac, aL[k], aR[k])));
+        } else {
+            const double th_r = bound_min_theta(rc, rL[k], rR[k]);
+            const double th_a = bound_min_theta(ac, aL[k], aR[k]);
+            if (th_r < Th) Th = th_r;  // std::min({Th, th_r, th_a})
+            if (th_a < Th) Th = th_a;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+        const PT rs = (side == 1) ? rL[k] : rR[k], as = (side == 1) ? aL[k] : aR[k];
+        if constexpr (F32) {
+            rf[k] = __fmaf_rn(Th, rs - r(k, 2), r(k, 2));
+            af[k] = __fmaf_rn(Th, as - a(k, 2), a(k, 2));
+        } else {
+            rf[k] = r(k, 2) + Th * (rs - r(k, 2));
+            af[k] = a(k, 2) + Th * (as - a(k, 2));
+        }
+    }
+}
+
 }  // namespace compas

@@ -296,8 +296,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
     constexpr bool TMA = (VAR == kVarTma);
     static_assert(!TMA || (M::D == 3 && MIX), "TMA halo staging: the 3D mixed form");
     static_assert(!PFX || M::KIND != kModelFiveN, "the Phase-Field kernel is the two-phase models'");
-    static_assert(M::KIND != kModelFiveN || ((SCHEME == 5 || SCHEME == 2) && !TH),
-                  "FIVEEQS_NPHASE runs WENO5, GODUNOV and MUSCL without THINC");
+    static_assert(M::KIND != kModelFiveN || !TH, "FIVEEQS_NPHASE runs without THINC");
     static_assert(SCHEME != 2 || (VAR == kVarPlain && !TH), "GODUNOV / MUSCL: the plain right-hand side");
     constexpr bool NPH = (M::KIND == kModelFiveN);
     using PT = typename std::conditional<MIX, float, double>::type;
@@ -496,7 +495,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                 }
             }
             double WfL[N], WfR[N], UL[N], UR[N];
-            constexpr int NB0 = (SCHEME == 6) ? 2 : 0;        // first plainly reconstructed component
+            constexpr int NB0 = (SCHEME == 6) ? M::IM : 0;    // first plainly reconstructed component
             constexpr int NB1 = (SCHEME == 6) ? M::IA : N;    // one past the last
             double F[N], fnc[NC], cm;
             bool thinc_face = false;
@@ -505,7 +504,19 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                                                       UR, err);
             if constexpr (!MIX) {
                 if (!thinc_face) {
-                    if constexpr (SCHEME == 6) {
+                    if constexpr (SCHEME == 6 && NPH) {
+                        double rf[M::NP], af[M::NP];
+                        auto rl = [&](int k, int s) { return (double)smem[off[s] + k * str[s]]; };
+                        auto al_ = [&](int k, int s) { return (double)smem[off[s] + (M::IA + k) * str[s]]; };
+                        weno5b_nphase<M::NP, double>(rl, al_, 1, rf, af);
+#pragma unroll
+                        for (int k = 0; k < M::NP; ++k) { WfL[k] = rf[k]; WfL[M::IA + k] = af[k]; }
+                        auto rr = [&](int k, int s) { return (double)smem[off[s + 1] + k * str[s + 1]]; };
+                        auto ar_ = [&](int k, int s) { return (double)smem[off[s + 1] + (M::IA + k) * str[s + 1]]; };
+                        weno5b_nphase<M::NP, double>(rr, ar_, -1, rf, af);
+#pragma unroll
+                        for (int k = 0; k < M::NP; ++k) { WfR[k] = rf[k]; WfR[M::IA + k] = af[k]; }
+                    } else if constexpr (SCHEME == 6) {
                         double r1[6], r2[6], al[6];
 #pragma unroll
                         for (int s = 0; s < 6; ++s) {
@@ -537,8 +548,9 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                     }
                     M::prim2cons(UL, WfL, a.e, err);
                     M::prim2cons(UR, WfR, a.e, err);
-                    if constexpr (NPH) {
-                        // N-phase WENO5: the consistent limiter about the stencil centres f-1 and f
+                    if constexpr (NPH && SCHEME != 6) {
+                        // N-phase WENO5 / three-cell schemes: the consistent limiter about the stencil
+                        // centres f-1 and f (WENO5B bounds its face values instead)
                         M::consistent_limit(UL, smem + off[2], str[2], dxd, 1, a.e, err);
                         M::consistent_limit(UR, smem + off[3], str[3], dxd, -1, a.e, err);
                     }
@@ -556,7 +568,14 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                     M::cons2prim_f32(wL, UL, a.e);
                     M::cons2prim_f32(wR, UR, a.e);
                 } else {
-                    if constexpr (SCHEME == 6) {
+                    if constexpr (SCHEME == 6 && NPH) {
+                        auto rl = [&](int k, int s) { return (float)smem[off[s] + k * str[s]]; };
+                        auto al_ = [&](int k, int s) { return (float)smem[off[s] + (M::IA + k) * str[s]]; };
+                        weno5b_nphase<M::NP, float>(rl, al_, 1, wL, wL + M::IA);
+                        auto rr = [&](int k, int s) { return (float)smem[off[s + 1] + k * str[s + 1]]; };
+                        auto ar_ = [&](int k, int s) { return (float)smem[off[s + 1] + (M::IA + k) * str[s + 1]]; };
+                        weno5b_nphase<M::NP, float>(rr, ar_, -1, wR, wR + M::IA);
+                    } else if constexpr (SCHEME == 6) {
                         float r1[6], r2[6], al[6];
 #pragma unroll
                         for (int s = 0; s < 6; ++s) {
@@ -593,7 +612,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                     }
                     M::prim2cons(UL, WfL, a.e, err);
                     M::prim2cons(UR, WfR, a.e, err);
-                    if constexpr (NPH) {
+                    if constexpr (NPH && SCHEME != 6) {
                         M::consistent_limit(UL, smem + off[2], str[2], dxd, 1, a.e, err);
                         M::consistent_limit(UR, smem + off[3], str[3], dxd, -1, a.e, err);
                     }

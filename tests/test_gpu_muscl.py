@@ -129,3 +129,34 @@ def test_llf_hll_mixed_error_vs_fp64(solver):
     print(f"{solver} mixed vs FP64 rel L1 per field:", np.array2string(e, precision=2))
     for c in (0, 1, A.shape[0] - 1):
         assert e[c] <= 1e-5, e
+
+
+@pytest.mark.parametrize("fn,kw,nsteps", [
+    (cases.triple_point, dict(m=12), 6),
+    (cases.nphase_bubbles, dict(n=24, nphase=4), 4),
+    (cases.nphase_bubbles, dict(n=10, nphase=3, dim=3), 3),
+], ids=["triple", "bubbles_np4", "bubbles3d_np3"])
+def test_nphase_weno5b_bitwise(fn, kw, nsteps):
+    """FiniteVolume.Scheme = WENO5B for the N-phase model: per-phase bounded reconstruction of alpha_k
+    rho_k and alpha_k with the partial densities' weights, renormalisation, the second limiting pass
+    (FVM_Reconstruction2Face_Conservative_WENO5B_D_Compressible5Eq_NPhase.H), to the bit."""
+    phys, dim, inputs, geom, U = fn(**kw)
+    p = cb.make_parm(phys, dim, dict(inputs, **{"FiniteVolume.Scheme": "WENO5B"}))
+    g = cb.make_geom(**geom)
+    _bitwise(p, g, U, nsteps)
+
+
+def test_nphase_weno5b_mixed_error_vs_fp64():
+    out = {}
+    for prec in ("fp64", "mixed"):
+        phys, dim, inputs, geom, U = cases.nphase_bubbles(n=32, nphase=3)
+        p = cb.make_parm(phys, dim, dict(inputs, **{"FiniteVolume.Scheme": "WENO5B", "compas_b200.precision": prec}))
+        g = cb.make_geom(**geom)
+        got, info, _ = run_gpu(p, g, U, 10)
+        assert info.status == 0
+        out[prec] = cb.valid_view(got, p, g)
+    A, B = out["mixed"], out["fp64"]
+    e = np.array([float(np.abs(A[c] - B[c]).sum() / np.abs(B[c]).sum()) for c in range(A.shape[0])])
+    print("N-phase WENO5B mixed vs FP64 rel L1 per field:", np.array2string(e, precision=2))
+    for c in (0, 1, 2, A.shape[0] - 3, A.shape[0] - 2, A.shape[0] - 1):
+        assert e[c] <= 1e-5, e

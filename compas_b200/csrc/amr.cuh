@@ -195,10 +195,10 @@ __device__ void amr_face_flux(const double* U, const Grid& g, int d, int i, int 
     if constexpr (!MIX) {
         if constexpr (SCHEME == 6 && NPH) {
             double rf[M::NP], af[M::NP];
-            weno5b_nphase<M::NP, double>([&](int k, int s) { return (double)P[s][k]; },
+            bounded_phases<M::NP, 5, double>([&](int k, int s) { return (double)P[s][k]; },
                                          [&](int k, int s) { return (double)P[s][M::IA + k]; }, 1, rf, af);
             for (int k = 0; k < M::NP; ++k) { WfL[k] = rf[k]; WfL[M::IA + k] = af[k]; }
-            weno5b_nphase<M::NP, double>([&](int k, int s) { return (double)P[s + 1][k]; },
+            bounded_phases<M::NP, 5, double>([&](int k, int s) { return (double)P[s + 1][k]; },
                                          [&](int k, int s) { return (double)P[s + 1][M::IA + k]; }, -1, rf, af);
             for (int k = 0; k < M::NP; ++k) { WfR[k] = rf[k]; WfR[M::IA + k] = af[k]; }
         } else if constexpr (SCHEME == 6) {
@@ -218,6 +218,10 @@ __device__ void amr_face_flux(const double* U, const Grid& g, int d, int i, int 
                 WfL[n] = face3(P[1][n], P[2][n], P[3][n], dxd, 1, code);
                 WfR[n] = face3(P[2][n], P[3][n], P[4][n], dxd, -1, code);
             }
+            if (code == 11) {
+                weno3b_faces<M, double>([&](int s, int n) { return P[1 + s][n]; }, 1, WfL);
+                weno3b_faces<M, double>([&](int s, int n) { return P[2 + s][n]; }, -1, WfR);
+            }
         } else {
 #pragma unroll
             for (int n = NB0; n < NB1; ++n) {
@@ -227,7 +231,7 @@ __device__ void amr_face_flux(const double* U, const Grid& g, int d, int i, int 
         }
         M::prim2cons(UL, WfL, e, err);
         M::prim2cons(UR, WfR, e, err);
-        if constexpr (NPH && SCHEME != 6) {
+        if constexpr (NPH && SCHEME != 6) if (SCHEME != 2 || code != 11) {
             M::consistent_limit(UL, P[2], 1, dxd, 1, e, err);
             M::consistent_limit(UR, P[3], 1, dxd, -1, e, err);
         }
@@ -235,9 +239,9 @@ __device__ void amr_face_flux(const double* U, const Grid& g, int d, int i, int 
     } else {
         float wL[N], wR[N];
         if constexpr (SCHEME == 6 && NPH) {
-            weno5b_nphase<M::NP, float>([&](int k, int s) { return (float)P[s][k]; },
+            bounded_phases<M::NP, 5, float>([&](int k, int s) { return (float)P[s][k]; },
                                         [&](int k, int s) { return (float)P[s][M::IA + k]; }, 1, wL, wL + M::IA);
-            weno5b_nphase<M::NP, float>([&](int k, int s) { return (float)P[s + 1][k]; },
+            bounded_phases<M::NP, 5, float>([&](int k, int s) { return (float)P[s + 1][k]; },
                                         [&](int k, int s) { return (float)P[s + 1][M::IA + k]; }, -1, wR, wR + M::IA);
         } else if constexpr (SCHEME == 6) {
             float r1[6], r2[6], al[6];
@@ -256,6 +260,10 @@ __device__ void amr_face_flux(const double* U, const Grid& g, int d, int i, int 
                 wL[n] = face3_f32(P[1][n], P[2][n], P[3][n], 1, code);
                 wR[n] = face3_f32(P[2][n], P[3][n], P[4][n], -1, code);
             }
+            if (code == 11) {
+                weno3b_faces<M, float>([&](int s, int n) { return (float)P[1 + s][n]; }, 1, wL);
+                weno3b_faces<M, float>([&](int s, int n) { return (float)P[2 + s][n]; }, -1, wR);
+            }
         } else {
 #pragma unroll
             for (int n = NB0; n < NB1; ++n) {
@@ -271,7 +279,7 @@ __device__ void amr_face_flux(const double* U, const Grid& g, int d, int i, int 
         M::prim2cons(UL, WfL, e, err);
         M::prim2cons(UR, WfR, e, err);
         if constexpr (NPH) {
-            if constexpr (SCHEME != 6) {
+            if constexpr (SCHEME != 6) if (SCHEME != 2 || code != 11) {
                 M::consistent_limit(UL, P[2], 1, dxd, 1, e, err);
                 M::consistent_limit(UR, P[3], 1, dxd, -1, e, err);
             }

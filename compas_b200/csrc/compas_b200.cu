@@ -338,10 +338,10 @@ static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
             return fail(COMPAS_B200_EUNSUPPORTED, "FIVEEQS_NPHASE: this build runs NPHASE 2, 3, 4 in 2D and 3 in 3D");
         if (p->thinc) return fail(COMPAS_B200_EUNSUPPORTED, "FIVEEQS_NPHASE: FiniteVolume.THINC is not in this engine");
     }
-    if (p->id_weno ? (p->id_limiter != 3 && p->id_limiter != 5 && p->id_limiter != 6)
+    if (p->id_weno ? (p->id_limiter < 3 || p->id_limiter > 6)
                    : (p->id_limiter < 0 || p->id_limiter > 4))
-        return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.Scheme: this build runs GODUNOV, MUSCL-*, WENO3, WENO5 and "
-                                              "WENO5B");
+        return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.Scheme: this build runs GODUNOV, MUSCL-*, WENO3, WENO3B, "
+                                              "WENO5 and WENO5B");
     if (p->id_limiter < 5 && (p->thinc || p->phase_field))
         return fail(COMPAS_B200_EUNSUPPORTED, "THINC and the Phase-Field step run with WENO5 / WENO5B here");
     if (p->id_riemann < 0 || p->id_riemann > 2)
@@ -628,7 +628,7 @@ static StageArgs base_args(const compas_b200_parm* p, const compas_b200_geom* g)
     a.riemann = p->id_riemann;
     a.trace = p->relax_trace;
     a.pf_phasic = (p->pf_phase2flux == 0);
-    a.muscl = p->id_weno ? (p->id_limiter == 3 ? 10 : -1) : p->id_limiter;
+    a.muscl = p->id_weno ? (p->id_limiter == 3 ? 10 : (p->id_limiter == 4 ? 11 : -1)) : p->id_limiter;
     a.pf_hll = (p->pf_flux == 1);
     a.thinc.use_normal = p->thinc_use_normal;
     a.thinc.eps = p->thinc_eps;
@@ -850,9 +850,7 @@ int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value
         if (v == "MUSCL-Superbee") { p->id_limiter = 3; p->id_weno = 0; p->num_grow = 2; return 0; }
         if (v == "MUSCL-MC") { p->id_limiter = 4; p->id_weno = 0; p->num_grow = 2; return 0; }
         if (v == "WENO3") { p->id_limiter = 3; p->id_weno = 1; p->num_grow = 2; return 0; }
-        if (v == "WENO3B")
-            return fail(COMPAS_B200_EUNSUPPORTED, k + " = " + v + " is a valid reference scheme outside this engine "
-                                                  "(GODUNOV, MUSCL-*, WENO3, WENO5, WENO5B)");
+        if (v == "WENO3B") { p->id_limiter = 4; p->id_weno = 1; p->num_grow = 2; return 0; }
         return bad("GODUNOV, MUSCL, MUSCL-Minmod, MUSCL-vanLeer, MUSCL-Superbee, MUSCL-MC, WENO3, WENO3B, WENO5, WENO5B");
     }
     if (k == "FiniteVolume.THINC") { if (!parse_int(value, &ix) || ix < 0 || ix > 1) return bad("0, 1"); p->thinc = ix; return 0; }
@@ -1728,7 +1726,7 @@ static int batch_sync_list(compas_b200_batch* b, cudaStream_t st) {
         B.id_k = c.p.source_term;
         B.relax = (c.p.physics == COMPAS_B200_SIXEQS) ? c.p.relaxation : 0;
         B.riemann = c.p.id_riemann;
-        B.muscl = c.p.id_weno ? (c.p.id_limiter == 3 ? 10 : -1) : c.p.id_limiter;
+        B.muscl = c.p.id_weno ? (c.p.id_limiter == 3 ? 10 : (c.p.id_limiter == 4 ? 11 : -1)) : c.p.id_limiter;
         B.trace = c.p.relax_trace;
         B.tiles = tile_count(b->dim, B.g);
         B.ghosts = ghost_count(B.g);

@@ -796,10 +796,9 @@ __device__ __forceinline__ double weno_sum(const double q[3], const double w[3])
 }
 
 // Positivity limiter of a cell with face values fL (right face) and fR (left face), lower bound 0
-// (Limiter_Bound with ID_BoundType = -1: Limiter_BoundMin.H, fC_QuadratureRule.H; weight 1/12 for
-// the fifth-order polynomial, FiniteVolume_Parameter.H:157-170).
-__device__ __forceinline__ double bound_min_theta(double f_c, double fL, double fR) {
-    const double W = 1.0 / 12.0;
+// (Limiter_Bound with ID_BoundType = -1: Limiter_BoundMin.H, fC_QuadratureRule.H; quadrature weight W:
+// 1/12 for the fifth-order polynomial, 1/6 for the third-order one, FiniteVolume_Parameter.H:157-170).
+__device__ __forceinline__ double bound_min_theta(double f_c, double fL, double fR, double W = 1.0 / 12.0) {
     const double fC = ((f_c - W * fL) - W * fR) / (1.0 - 2.0 * W);
     double mn = fC;  // std::min({fC, fL, fR})
     if (fL < mn) mn = fL;
@@ -959,7 +958,7 @@ __device__ __forceinline__ double muscl_face(double f_m, double f_c, double f_p,
 // WENO3 face value (FiniteVolume.Scheme = WENO3: include/Operators_FV/WENO3.H, Reconstruction2Face_WENO3_D.H,
 // Reconstruction2Face_WENO.H): two candidates, ratio-form weights with the NaN guard, the weighted sum
 // accumulated from 0.
-__device__ __forceinline__ double weno3_face(double f_m, double f_c, double f_p, int side) {
+__device__ __forceinline__ void weno3_qw(double f_m, double f_c, double f_p, int side, double q[2], double w[2]) {
     double q0, q1, d0;
     if (side == 1) {
         q0 = f_c + 0.5 * (f_c - f_m);
@@ -976,17 +975,29 @@ __device__ __forceinline__ double weno3_face(double f_m, double f_c, double f_p,
     double IS01 = IS0 / IS1;
     if (isnan(IS01)) IS01 = 1.0;
     const double IS10 = 1.0 / IS01;
-    const double w0 = d0 / (d0 + (IS01 * IS01) * d1);
-    const double w1 = d1 / ((IS10 * IS10) * d0 + d1);
+    q[0] = q0;
+    q[1] = q1;
+    w[0] = d0 / (d0 + (IS01 * IS01) * d1);
+    w[1] = d1 / ((IS10 * IS10) * d0 + d1);
+}
+
+__device__ __forceinline__ double weno3_sum(const double q[2], const double w[2]) {
     double f = 0.0;
-    f += w0 * q0;
-    f += w1 * q1;
+    f += w[0] * q[0];
+    f += w[1] * q[1];
     return f;
 }
 
-// Three-cell face values of the stage kernel's SCHEME 2: code 0..4 the GODUNOV / MUSCL family, 10 WENO3.
+__device__ __forceinline__ double weno3_face(double f_m, double f_c, double f_p, int side) {
+    double q[2], w[2];
+    weno3_qw(f_m, f_c, f_p, side, q, w);
+    return weno3_sum(q, w);
+}
+
+// Three-cell face values of the stage kernel's SCHEME 2: code 0..4 the GODUNOV / MUSCL family, 10 WENO3,
+// 11 WENO3B (WENO3 here; the masses and volume fractions are bounded afterwards).
 __device__ __forceinline__ double face3(double f_m, double f_c, double f_p, double dx, int side, int code) {
-    return (code == 10) ? weno3_face(f_m, f_c, f_p, side) : muscl_face(f_m, f_c, f_p, dx, side, code);
+    return (code >= 10) ? weno3_face(f_m, f_c, f_p, side) : muscl_face(f_m, f_c, f_p, dx, side, code);
 }
 
 // Mixed precision: the limiters are homogeneous of degree one in the slopes, so the FP32 form limits
@@ -1011,9 +1022,8 @@ __device__ __forceinline__ float muscl_face_f32(float f_m, float f_c, float f_p,
 
 // WENO3 in FP32 in the correction form of weno5_f32 (f_c plus the weighted corrections), the weights
 // from the ratio of the indicators with one reciprocal.
-__device__ __forceinline__ float weno3_face_f32(float f_m, float f_c, float f_p, int side) {
-    const float a = f_c - f_m, b = f_p - f_c;
-    const float h = (side == 1) ? 0.5f : -0.5f;
+// Weight of the left candidate from the undivided differences a = f_c - f_m, b = f_p - f_c.
+__device__ __forceinline__ float weno3_w0_f32(float a, float b, int side) {
     const float d0 = (side == 1) ? (1.0f / 3.0f) : (2.0f / 3.0f), d1 = 1.0f - d0;
     const float IS0 = a * a, IS1 = b * b;
     float w0;
@@ -1023,15 +1033,20 @@ __device__ __forceinline__ float weno3_face_f32(float f_m, float f_c, float f_p,
         const float r = fminf(IS0 / IS1, 1.0e18f);
         w0 = d0 / __fmaf_rn(r * r, d1, d0);
     }
-    return f_c + h * __fmaf_rn(w0, a - b, b);
+    return w0;
+}
+
+__device__ __forceinline__ float weno3_face_f32(float f_m, float f_c, float f_p, int side) {
+    const float a = f_c - f_m, b = f_p - f_c;
+    const float h = (side == 1) ? 0.5f : -0.5f;
+    return f_c + h * __fmaf_rn(weno3_w0_f32(a, b, side), a - b, b);
 }
 
 __device__ __forceinline__ float face3_f32(float f_m, float f_c, float f_p, int side, int code) {
-    return (code == 10) ? weno3_face_f32(f_m, f_c, f_p, side) : muscl_face_f32(f_m, f_c, f_p, side, code);
+    return (code >= 10) ? weno3_face_f32(f_m, f_c, f_p, side) : muscl_face_f32(f_m, f_c, f_p, side, code);
 }
 
-__device__ __forceinline__ float bound_min_theta_f32(float f_c, float fL, float fR) {
-    const float W = 1.0f / 12.0f;
+__device__ __forceinline__ float bound_min_theta_f32(float f_c, float fL, float fR, float W = 1.0f / 12.0f) {
     const float fC = (f_c - W * fL - W * fR) * (1.0f / (1.0f - 2.0f * W));
     float mn = fminf(fC, fminf(fL, fR));
     const float den = f_c - mn;
@@ -1087,21 +1102,49 @@ __device__ __forceinline__ void weno5b_masses_f32(const float* ar1, const float*
     alpha1_f = __fmaf_rn(Th, a1 - al1[2], al1[2]);
 }
 
-// N-phase WENO5B (include/Operators_Compressible5Eq_NPhase/FVM_Reconstruction2Face_Conservative_WENO5B_D_Compressible5Eq_NPhase.H):
-// the steps of weno5b_masses for NP phases whose volume fractions are all state variables. r(k, s) and
-// a(k, s) give alpha_k rho_k and alpha_k of stencil cell s = 0..4 (centre 2); the face values of side
-// `side` go to rf[k], af[k]. PT = double: the reference's arithmetic; PT = float: the mixed form.
-template <int NP, class PT, class FR, class FA>
-__device__ __forceinline__ void weno5b_nphase(FR r, FA a, int side, PT* rf, PT* af) {
+// Bounded WENO face values of NP phases. WENO5B, ORDER 5:
+// include/Operators_Compressible5Eq_NPhase/FVM_Reconstruction2Face_Conservative_WENO5B_D_Compressible5Eq_NPhase.H;
+// WENO3B, ORDER 3: include/Operators_Compressible5Eq/FVM_Reconstruction2Face_Conservative_WENO3B_D_Compressible5Eq.H:95-236,
+// the six-equation and N-phase counterparts (same steps). Per phase: the WENO faces of alpha_k rho_k and of
+// alpha_k (with the weights of alpha_k rho_k), one positivity theta for both; the faces divided by sum alpha_k;
+// one common theta over all phases applied to the face of side `side`. r(k, s) and a(k, s) give alpha_k rho_k
+// and alpha_k of stencil cell s = 0..ORDER-1 (centre ORDER/2); the results go to rf[k], af[k]. PT = double:
+// the reference's arithmetic (quadrature weight 1/12 for ORDER 5, 1/6 for ORDER 3); PT = float: the mixed form.
+template <int NP, int ORDER, class PT, class FR, class FA>
+__device__ __forceinline__ void bounded_phases(FR r, FA a, int side, PT* rf, PT* af) {
     constexpr bool F32 = std::is_same<PT, float>::value;
+    constexpr int C = ORDER / 2;
+    constexpr double W = (ORDER == 5) ? 1.0 / 12.0 : 1.0 / 6.0;
     PT rL[NP], rR[NP], aL[NP], aR[NP];
     PT sumL = 0, sumR = 0;
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
-        const PT fr[5] = {r(k, 0), r(k, 1), r(k, 2), r(k, 3), r(k, 4)};
-        const PT fa[5] = {a(k, 0), a(k, 1), a(k, 2), a(k, 3), a(k, 4)};
+        PT fr[ORDER], fa[ORDER];
+#pragma unroll
+        for (int s = 0; s < ORDER; ++s) {
+            fr[s] = r(k, s);
+            fa[s] = a(k, s);
+        }
         PT th;
-        if constexpr (F32) {
+        if constexpr (F32 && ORDER == 3) {
+            const float ra = fr[1] - fr[0], rb = fr[2] - fr[1], aa = fa[1] - fa[0], ab = fa[2] - fa[1];
+            float w0 = weno3_w0_f32(ra, rb, 1);
+            rL[k] = fr[1] + 0.5f * __fmaf_rn(w0, ra - rb, rb);
+            aL[k] = fa[1] + 0.5f * __fmaf_rn(w0, aa - ab, ab);
+            w0 = weno3_w0_f32(ra, rb, -1);
+            rR[k] = fr[1] - 0.5f * __fmaf_rn(w0, ra - rb, rb);
+            aR[k] = fa[1] - 0.5f * __fmaf_rn(w0, aa - ab, ab);
+        } else if constexpr (!F32 && ORDER == 3) {
+            double q[2], w[2], qa[2], wa[2];
+            weno3_qw(fr[0], fr[1], fr[2], 1, q, w);
+            rL[k] = weno3_sum(q, w);
+            weno3_qw(fa[0], fa[1], fa[2], 1, qa, wa);
+            aL[k] = weno3_sum(qa, w);
+            weno3_qw(fr[0], fr[1], fr[2], -1, q, w);
+            rR[k] = weno3_sum(q, w);
+            weno3_qw(fa[0], fa[1], fa[2], -1, qa, wa);
+            aR[k] = weno3_sum(qa, w);
+        } else if constexpr (F32) {
             float e[3], w[3], ea[3];
             weno5_f32_parts(fr[0], fr[1], fr[2], fr[3], fr[4], 1, e, w);
             weno5_f32_parts(fa[0], fa[1], fa[2], fa[3], fa[4], 1, ea, nullptr);
@@ -1111,11 +1154,6 @@ __device__ __forceinline__ void weno5b_nphase(FR r, FA a, int side, PT* rf, PT* 
             weno5_f32_parts(fa[0], fa[1], fa[2], fa[3], fa[4], -1, ea, nullptr);
             rR[k] = fr[2] + __fmaf_rn(w[0], e[0], __fmaf_rn(w[1], e[1], w[2] * e[2]));
             aR[k] = fa[2] + __fmaf_rn(w[0], ea[0], __fmaf_rn(w[1], ea[1], w[2] * ea[2]));
-            th = fminf(bound_min_theta_f32(fr[2], rL[k], rR[k]), bound_min_theta_f32(fa[2], aL[k], aR[k]));
-            rL[k] = __fmaf_rn(th, rL[k] - fr[2], fr[2]);
-            aL[k] = __fmaf_rn(th, aL[k] - fa[2], fa[2]);
-            rR[k] = __fmaf_rn(th, rR[k] - fr[2], fr[2]);
-            aR[k] = __fmaf_rn(th, aR[k] - fa[2], fa[2]);
         } else {
             double q[3], w[3], qa[3];
             weno5_parts(fr[0], fr[1], fr[2], fr[3], fr[4], 1, q, w);
@@ -1126,11 +1164,20 @@ __device__ __forceinline__ void weno5b_nphase(FR r, FA a, int side, PT* rf, PT* 
             rR[k] = weno_sum(q, w);
             weno5_parts(fa[0], fa[1], fa[2], fa[3], fa[4], -1, qa, nullptr);
             aR[k] = weno_sum(qa, w);
-            th = dmin(bound_min_theta(fr[2], rL[k], rR[k]), bound_min_theta(fa[2], aL[k], aR[k]));
-            rL[k] = fr[2] + th * (rL[k] - fr[2]);
-            aL[k] = fa[2] + th * (aL[k] - fa[2]);
-            rR[k] = fr[2] + th * (rR[k] - fr[2]);
-            aR[k] = fa[2] + th * (aR[k] - fa[2]);
+        }
+        if constexpr (F32) {
+            th = fminf(bound_min_theta_f32(fr[C], rL[k], rR[k], (float)W),
+                       bound_min_theta_f32(fa[C], aL[k], aR[k], (float)W));
+            rL[k] = __fmaf_rn(th, rL[k] - fr[C], fr[C]);
+            aL[k] = __fmaf_rn(th, aL[k] - fa[C], fa[C]);
+            rR[k] = __fmaf_rn(th, rR[k] - fr[C], fr[C]);
+            aR[k] = __fmaf_rn(th, aR[k] - fa[C], fa[C]);
+        } else {
+            th = dmin(bound_min_theta(fr[C], rL[k], rR[k], W), bound_min_theta(fa[C], aL[k], aR[k], W));
+            rL[k] = fr[C] + th * (rL[k] - fr[C]);
+            aL[k] = fa[C] + th * (aL[k] - fa[C]);
+            rR[k] = fr[C] + th * (rR[k] - fr[C]);
+            aR[k] = fa[C] + th * (aR[k] - fa[C]);
         }
         sumL += aL[k];
         sumR += aR[k];
@@ -1138,16 +1185,16 @@ __device__ __forceinline__ void weno5b_nphase(FR r, FA a, int side, PT* rf, PT* 
     PT Th = 1;
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
-        const PT rc = r(k, 2), ac = a(k, 2);
+        const PT rc = r(k, C), ac = a(k, C);
         rL[k] /= sumL;
         aL[k] /= sumL;
         rR[k] /= sumR;
         aR[k] /= sumR;
         if constexpr (F32) {
-            Th = fminf(Th, fminf(bound_min_theta_f32(rc, rL[k], rR[k]), bound_min_theta_f32(ac, aL[k], aR[k])));
+            Th = fminf(Th, fminf(bound_min_theta_f32(rc, rL[k], rR[k], (float)W), bound_min_theta_f32(ac, aL[k], aR[k], (float)W)));
         } else {
-            const double th_r = bound_min_theta(rc, rL[k], rR[k]);
-            const double th_a = bound_min_theta(ac, aL[k], aR[k]);
+            const double th_r = bound_min_theta(rc, rL[k], rR[k], W);
+            const double th_a = bound_min_theta(ac, aL[k], aR[k], W);
             if (th_r < Th) Th = th_r;  // std::min({Th, th_r, th_a})
             if (th_a < Th) Th = th_a;
         }
@@ -1156,11 +1203,11 @@ __device__ __forceinline__ void weno5b_nphase(FR r, FA a, int side, PT* rf, PT* 
     for (int k = 0; k < NP; ++k) {
         const PT rs = (side == 1) ? rL[k] : rR[k], as = (side == 1) ? aL[k] : aR[k];
         if constexpr (F32) {
-            rf[k] = __fmaf_rn(Th, rs - r(k, 2), r(k, 2));
-            af[k] = __fmaf_rn(Th, as - a(k, 2), a(k, 2));
+            rf[k] = __fmaf_rn(Th, rs - r(k, C), r(k, C));
+            af[k] = __fmaf_rn(Th, as - a(k, C), a(k, C));
         } else {
-            rf[k] = r(k, 2) + Th * (rs - r(k, 2));
-            af[k] = a(k, 2) + Th * (as - a(k, 2));
+            rf[k] = r(k, C) + Th * (rs - r(k, C));
+            af[k] = a(k, C) + Th * (as - a(k, C));
         }
     }
 }

@@ -65,7 +65,7 @@ struct StageArgs {
     const double* gq[3];       // Phase-Field kernels: face gradients of the potential Q per direction
     int pf_phasic;             // Phase-Field kernels, six-equation model: 1 phasic, 0 mixture formulation
     int pf_hll;                // Phase-Field kernels: 1 HLL phase fluxes, 0 upwind/downwind
-    int muscl;                 // SCHEME 2: 0 Godunov, 1 minmod, 2 van Leer, 3 superbee, 4 MC, 10 WENO3 (-1 otherwise)
+    int muscl;                 // SCHEME 2: 0 Godunov, 1 minmod, 2 van Leer, 3 superbee, 4 MC, 10 WENO3, 11 WENO3B (-1 otherwise)
     int riemann;               // Physics.RiemannSolver: 0 LLF, 1 HLL, 2 HLLC
     int order;                 // tile traversal order (tile_coords): 0 x fastest, 1 bricks of tiles
     int tile_base;             // single-box kernels: first tile (order 0) and number of tiles of the launch
@@ -235,6 +235,35 @@ __device__ __forceinline__ void llf_hll_mixed(int hll, double* Fout, double* fnc
 }
 
 // Physics.RiemannSolver: 0 LLF, 1 HLL, 2 HLLC (source/Class_Compressible_PhaseField.cpp:92-111).
+// WENO3B (three-cell code 11): the masses and volume fractions of the WENO3 face values Wf replaced by
+// the bounded ones of bounded_phases<., 3>; g(s, n) is primitive n of stencil cell s = 0, 1, 2. The
+// two-phase models bound alpha_2 = 1 - alpha_1 as the second phase
+// (FVM_Reconstruction2Face_Conservative_WENO3B_D_Compressible5Eq.H:48-80).
+template <class M, class PT, class G>
+__device__ __forceinline__ void weno3b_faces(G g, int side, PT* Wf) {
+    PT rf[M::NP], af[M::NP];
+    if constexpr (M::KIND == kModelFiveN) {
+        bounded_phases<M::NP, 3, PT>([&](int k, int s) { return (PT)g(s, k); },
+                                     [&](int k, int s) { return (PT)g(s, M::IA + k); }, side, rf, af);
+#pragma unroll
+        for (int k = 0; k < M::NP; ++k) {
+            Wf[k] = rf[k];
+            Wf[M::IA + k] = af[k];
+        }
+    } else {
+        bounded_phases<2, 3, PT>(
+            [&](int k, int s) { return (PT)g(s, k); },
+            [&](int k, int s) {
+                const PT a1 = (PT)g(s, M::IA);
+                return (k == 0) ? a1 : (PT)1 - a1;
+            },
+            side, rf, af);
+        Wf[0] = rf[0];
+        Wf[1] = rf[1];
+        Wf[M::IA] = af[0];
+    }
+}
+
 template <class M>
 __device__ __forceinline__ void riemann(int id_riemann, double* Fout, double* fnc, double& cmax, const double* UL,
                                         const double* UR, const Eos& e, int d, int id_k, unsigned int* err) {
@@ -508,12 +537,12 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                         double rf[M::NP], af[M::NP];
                         auto rl = [&](int k, int s) { return (double)smem[off[s] + k * str[s]]; };
                         auto al_ = [&](int k, int s) { return (double)smem[off[s] + (M::IA + k) * str[s]]; };
-                        weno5b_nphase<M::NP, double>(rl, al_, 1, rf, af);
+                        bounded_phases<M::NP, 5, double>(rl, al_, 1, rf, af);
 #pragma unroll
                         for (int k = 0; k < M::NP; ++k) { WfL[k] = rf[k]; WfL[M::IA + k] = af[k]; }
                         auto rr = [&](int k, int s) { return (double)smem[off[s + 1] + k * str[s + 1]]; };
                         auto ar_ = [&](int k, int s) { return (double)smem[off[s + 1] + (M::IA + k) * str[s + 1]]; };
-                        weno5b_nphase<M::NP, double>(rr, ar_, -1, rf, af);
+                        bounded_phases<M::NP, 5, double>(rr, ar_, -1, rf, af);
 #pragma unroll
                         for (int k = 0; k < M::NP; ++k) { WfR[k] = rf[k]; WfR[M::IA + k] = af[k]; }
                     } else if constexpr (SCHEME == 6) {
@@ -536,6 +565,12 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                             WfL[n] = face3(w1, w2, w3, dxd, 1, lim);
                             WfR[n] = face3(w2, w3, w4, dxd, -1, lim);
                         }
+                        if (lim == 11) {
+                            weno3b_faces<M, double>([&](int s, int n) { return (double)smem[off[1 + s] + n * str[1 + s]]; },
+                                                    1, WfL);
+                            weno3b_faces<M, double>([&](int s, int n) { return (double)smem[off[2 + s] + n * str[2 + s]]; },
+                                                    -1, WfR);
+                        }
                     } else {
 #pragma unroll
                         for (int n = NB0; n < NB1; ++n) {
@@ -548,7 +583,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                     }
                     M::prim2cons(UL, WfL, a.e, err);
                     M::prim2cons(UR, WfR, a.e, err);
-                    if constexpr (NPH && SCHEME != 6) {
+                    if constexpr (NPH && SCHEME != 6) if (SCHEME != 2 || a.muscl != 11) {
                         // N-phase WENO5 / three-cell schemes: the consistent limiter about the stencil
                         // centres f-1 and f (WENO5B bounds its face values instead)
                         M::consistent_limit(UL, smem + off[2], str[2], dxd, 1, a.e, err);
@@ -571,10 +606,10 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                     if constexpr (SCHEME == 6 && NPH) {
                         auto rl = [&](int k, int s) { return (float)smem[off[s] + k * str[s]]; };
                         auto al_ = [&](int k, int s) { return (float)smem[off[s] + (M::IA + k) * str[s]]; };
-                        weno5b_nphase<M::NP, float>(rl, al_, 1, wL, wL + M::IA);
+                        bounded_phases<M::NP, 5, float>(rl, al_, 1, wL, wL + M::IA);
                         auto rr = [&](int k, int s) { return (float)smem[off[s + 1] + k * str[s + 1]]; };
                         auto ar_ = [&](int k, int s) { return (float)smem[off[s + 1] + (M::IA + k) * str[s + 1]]; };
-                        weno5b_nphase<M::NP, float>(rr, ar_, -1, wR, wR + M::IA);
+                        bounded_phases<M::NP, 5, float>(rr, ar_, -1, wR, wR + M::IA);
                     } else if constexpr (SCHEME == 6) {
                         float r1[6], r2[6], al[6];
 #pragma unroll
@@ -595,6 +630,12 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                             wL[n] = face3_f32(w1, w2, w3, 1, lim);
                             wR[n] = face3_f32(w2, w3, w4, -1, lim);
                         }
+                        if (lim == 11) {
+                            weno3b_faces<M, float>([&](int s, int n) { return (float)smem[off[1 + s] + n * str[1 + s]]; },
+                                                   1, wL);
+                            weno3b_faces<M, float>([&](int s, int n) { return (float)smem[off[2 + s] + n * str[2 + s]]; },
+                                                   -1, wR);
+                        }
                     } else {
 #pragma unroll
                         for (int n = NB0; n < NB1; ++n) {
@@ -612,7 +653,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                     }
                     M::prim2cons(UL, WfL, a.e, err);
                     M::prim2cons(UR, WfR, a.e, err);
-                    if constexpr (NPH && SCHEME != 6) {
+                    if constexpr (NPH && SCHEME != 6) if (SCHEME != 2 || a.muscl != 11) {
                         M::consistent_limit(UL, smem + off[2], str[2], dxd, 1, a.e, err);
                         M::consistent_limit(UR, smem + off[3], str[3], dxd, -1, a.e, err);
                     }

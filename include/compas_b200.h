@@ -56,7 +56,7 @@ typedef struct compas_b200_parm {
     double gamma_1, gamma_2, pinf_1, pinf_2, b_1, b_2, q_1, q_2;
     double A1, A2, B1, B2, C1, C2, D1, D2;
     /* FiniteVolume.* (include/Operators_FV/FiniteVolume_Parameter.H:25-202) */
-    int id_limiter;       /* with id_weno 1: 5 WENO5, 6 WENO5B; with id_weno 0: 0 GODUNOV, 1 MUSCL(-Minmod),
+    int id_limiter;       /* with id_weno 1: 3 WENO3, 4 WENO3B, 5 WENO5, 6 WENO5B; with id_weno 0: 0 GODUNOV, 1 MUSCL(-Minmod),
                            * 2 MUSCL-vanLeer, 3 MUSCL-Superbee, 4 MUSCL-MC (the reference's ID_Limiter) */
     int id_weno;          /* the reference's ID_WENO: 1 for WENO5 / WENO5B, 0 for GODUNOV and MUSCL */
     int num_grow;         /* ghost cells the scheme reads (3 for WENO5/WENO5B) */

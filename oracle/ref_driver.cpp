@@ -109,10 +109,10 @@ Parm make_parm(const cmp_case* c) {
     auto& fv = p.FiniteVolume_Parm;
     fv.ID_WENO = c->id_weno;
     fv.ID_Limiter = c->id_limiter;
-    if (c->id_weno && c->id_limiter == 3) {
+    if (c->id_weno && (c->id_limiter == 3 || c->id_limiter == 4)) {
         fv.ID_Poly = 2;
         fv.Num_Grow = 2;
-        fv.Scheme = FVReconstruction::WENO_3;
+        fv.Scheme = (c->id_limiter == 4) ? FVReconstruction::WENO_3B : FVReconstruction::WENO_3;
     } else if (c->id_weno) {
         fv.ID_Poly = 4;
         fv.Num_Grow = 3;

@@ -52,9 +52,8 @@ def test_scheme_keys():
         assert (p.id_weno, p.id_limiter, p.num_grow) == (0, lim, ng), v
     p = cb.make_parm(cb.FIVEEQS, 2, {"FiniteVolume.Scheme": "WENO3"})
     assert (p.id_weno, p.id_limiter, p.num_grow) == (1, 3, 2)
-    with pytest.raises(cb.CompasError) as e:
-        cb.make_parm(cb.FIVEEQS, 2, {"FiniteVolume.Scheme": "WENO3B"})
-    assert e.value.code == cb.EUNSUPPORTED
+    p = cb.make_parm(cb.FIVEEQS, 2, {"FiniteVolume.Scheme": "WENO3B"})
+    assert (p.id_weno, p.id_limiter, p.num_grow) == (1, 4, 2)
 
 
 def test_state_bytes_layout():

@@ -1,5 +1,5 @@
 """GODUNOV, the MUSCL family and WENO3 (FiniteVolume.Scheme = GODUNOV, MUSCL, MUSCL-Minmod, MUSCL-vanLeer,
-MUSCL-Superbee, MUSCL-MC, WENO3) on the CUDA path against the reference-header oracle: the plain FP64 form
+MUSCL-Superbee, MUSCL-MC, WENO3, WENO3B) on the CUDA path against the reference-header oracle: the plain FP64 form
 is compared to the bit over several steps for every limiter (five-equation 2D), the six-equation 3D
 droplet with relaxation, and the N-phase triple point with the scheme of the reference's own example
 (exec/TriplePoint-5Eq-N/prob/inputs: MUSCL-MC, followed by the consistent limiter); the LLF and HLL
@@ -14,7 +14,7 @@ from oracle.oracle import have_ref
 
 pytestmark = pytest.mark.gpu
 
-SCHEMES = ["GODUNOV", "MUSCL", "MUSCL-vanLeer", "MUSCL-Superbee", "MUSCL-MC", "WENO3"]
+SCHEMES = ["GODUNOV", "MUSCL", "MUSCL-vanLeer", "MUSCL-Superbee", "MUSCL-MC", "WENO3", "WENO3B"]
 
 
 def _run(fn, kw, scheme, nsteps, prec="fp64"):
@@ -42,19 +42,19 @@ def test_fiveeq_2d_bitwise(scheme):
     _bitwise(p, g, U, 6)
 
 
-@pytest.mark.parametrize("scheme", ["MUSCL-MC", "MUSCL-Superbee", "WENO3"])
+@pytest.mark.parametrize("scheme", ["MUSCL-MC", "MUSCL-Superbee", "WENO3", "WENO3B"])
 def test_sixeq_3d_droplet_bitwise(scheme):
     p, g, U = _run(cases.shock_droplet, dict(n=16), scheme, 4)
     _bitwise(p, g, U, 4)
 
 
-@pytest.mark.parametrize("scheme", ["MUSCL-MC", "GODUNOV", "WENO3"])
+@pytest.mark.parametrize("scheme", ["MUSCL-MC", "GODUNOV", "WENO3", "WENO3B"])
 def test_triple_point_bitwise(scheme):
     p, g, U = _run(cases.triple_point, dict(m=12), scheme, 6)
     _bitwise(p, g, U, 6)
 
 
-@pytest.mark.parametrize("scheme", ["MUSCL-MC", "WENO3"])
+@pytest.mark.parametrize("scheme", ["MUSCL-MC", "WENO3", "WENO3B"])
 @pytest.mark.parametrize("fn,kw", [(cases.shock_bubble, dict(nx=64, ny=32, scheme="WENO5")),
                                    (cases.shock_droplet, dict(n=24))], ids=["bubble", "droplet"])
 def test_mixed_error_vs_fp64(fn, kw, scheme):

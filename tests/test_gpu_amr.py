@@ -167,7 +167,12 @@ def test_amr_mixed_error_vs_fp64(args):
      {"Physics.RiemannSolver": "HLL"}),
     (cases.shock_droplet, dict(n=16), (16, 16, 16), [((8, 8, 8), (23, 23, 23))], 8, 3,
      {"FiniteVolume.Scheme": "WENO3", "Physics.RiemannSolver": "LLF"}),
-], ids=["triple_muscl_mc_3lev", "triple_weno5_2lev", "bubble_muscl_mc", "bubble_hll", "droplet_weno3_llf"])
+    (cases.shock_bubble, dict(nx=48, ny=24, scheme="WENO5"), (48, 24), [((24, 8, 0), (71, 39, 0))], 16, 4,
+     {"FiniteVolume.Scheme": "WENO3B"}),
+    (cases.triple_point, dict(m=8), (56, 24), [((16, 12, 0), (47, 35, 0))], 16, 4,
+     {"FiniteVolume.Scheme": "WENO3B"}),
+], ids=["triple_muscl_mc_3lev", "triple_weno5_2lev", "bubble_muscl_mc", "bubble_hll", "droplet_weno3_llf",
+        "bubble_weno3b", "triple_weno3b"])
 def test_amr_schemes_and_nphase_match_oracle(case_fn, kw, domain, regions, mgs, steps, extra):
     """The multi-level advance with the N-phase model (the triple point, as the reference's example runs
     it: MUSCL-MC on a hierarchy), the three-cell schemes and the LLF / HLL Riemann solvers, to the bit."""

@@ -223,16 +223,19 @@ int compas_b200_pf_rk3_stage(const compas_b200_parm* p, const compas_b200_geom* 
 
 /* One TVD-RK3 step of size dt (stages 0-2 with their boundary fills and, for SIXEQS, the pressure
  * relaxation) in place on the caller-owned state U, WITHOUT ALLOCATING ANY DEVICE MEMORY. This entry
- * point has no counterpart in the reference. It is for callers that cannot call cudaMalloc - code
- * running while a CUDA graph is being captured, callers whose memory is owned by another allocator
- * (an AMReX arena, a framework's caching allocator) that must stay the only allocator, or hosts with
- * a fixed memory reservation - which still want a whole step from one call.
+ * point has no counterpart in the reference. It is for callers that cannot call cudaMalloc - hosts
+ * whose device memory is owned by another allocator (an AMReX arena, a framework's caching
+ * allocator) that must stay the only allocator, or hosts with a fixed memory reservation that may
+ * not grow - which still want a whole step from one call.
  *   - The two intermediate stage states live in a file-scope device array of this library,
  *     2 x 16 MiB plus 256 bytes, created on every GPU that loads the library and held until the
  *     process exits. A state (compas_b200_state_bytes) larger than 16 MiB is rejected with
  *     COMPAS_B200_EARG; use compas_b200_level_* for larger boxes.
  *   - The first call on a device looks up that array's device address (cudaGetSymbolAddress) and
- *     caches it, so make the first call on each device before any stream capture.
+ *     caches it for the life of the process, so make the first call on each device before any
+ *     stream capture, and do not use this entry point after a cudaDeviceReset of that device.
+ *   - The stage kernels run with the launch shape a level of the same box size has tuned in this
+ *     process (as compas_b200_rk3_stage does), else the default shape.
  *   - Every call on a device shares the one array and leaves its contents behind; the call rewrites
  *     everything it reads. Calls that overlap on the GPU (other streams, other host threads) race on
  *     it: serialize them.

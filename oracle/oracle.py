@@ -169,8 +169,9 @@ class Oracle:
         """thinc_ulp (port only): move every THINC face value up by one ulp, to measure how strongly
         a case amplifies last-bit differences of exp/log/tanh between math libraries."""
         self.kind = kind
-        self.case = case_from(parm, geom)
-        self.lib = load(kind, parm.physics, parm.dim, getattr(parm, "nphase", 2))
+        # parm: a compas_b200 Parm (with geom), or an oracle Case already filled (oracle.parm)
+        self.case = parm if isinstance(parm, Case) else case_from(parm, geom)
+        self.lib = load(kind, self.case.physics, self.case.dim, self.case.nphase)
         self.thinc_ulp = bool(thinc_ulp)
         if self.thinc_ulp and kind != "port":
             raise ValueError("the one-ulp THINC control exists in the port only")

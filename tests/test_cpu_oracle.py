@@ -284,3 +284,28 @@ def test_nphase_amr_oracle_conserves_masses_and_energy():
     s1 = [amr.composite_sum(states, boxes, 2, 3, c, cov) for c in comps]
     for a, b in zip(s0, s1):
         assert abs(a - b) <= 1e-13 * abs(a)
+
+
+def test_oracle_parm_matches_the_library_parm():
+    """The oracle's own reading of the inputs keys (oracle/parm.py, used by the CPU legs of bench.py
+    so that they load no CUDA library) gives the same oracle Case as the library's Parm."""
+    from oracle.oracle import case_from
+    from oracle.parm import reference_case
+
+    variants = [cases.shock_droplet(n=8), cases.shock_bubble(nx=16, ny=8), cases.advected_disc(n=8)]
+    phys, dim, inputs, geom, _ = cases.shock_bubble(nx=16, ny=8, scheme="MUSCL-MC")
+    variants.append((phys, dim, dict(inputs, **{"Physics.RiemannSolver": "HLL", "run.timestep_change_limiter": 0,
+                                                 "FiniteVolume.THINC": 1, "Physics.source_term": 1}), geom, None))
+    nasg = {"prob.EOS.EOS": 3, "prob.EOS.gamma_1": 1.19, "prob.EOS.gamma_2": 1.19, "prob.EOS.pinf_2": 6.2178e8,
+            "prob.EOS.b_2": 6.7212e-4, "prob.EOS.q_2": -1.177788e6}
+    variants.append((cb.FIVEEQS, 2, nasg, geom, None))
+    for phys, dim, inputs, geom, _ in variants:
+        a = reference_case(phys, dim, inputs, geom)
+        b = case_from(cb.make_parm(phys, dim, inputs), cb.make_geom(**geom))
+        for name, _t in a._fields_:
+            va, vb = getattr(a, name), getattr(b, name)
+            if hasattr(va, "__len__"):
+                va, vb = list(va), list(vb)
+            if name in ("Ak", "Bk", "Ck", "Dk"):
+                continue  # N-phase only
+            assert va == vb, (name, va, vb, inputs)

@@ -1,6 +1,6 @@
 """The allocation-free RK3 step (compas_b200_rk3_step_noalloc), for callers that cannot allocate device
-memory themselves or through the library - inside a CUDA-graph capture, or when another allocator
-must stay the only owner of device memory. It keeps the two intermediate stage states in the
+memory themselves or through the library - when another allocator (an AMReX arena, a framework's
+caching allocator) must stay the only owner of device memory, or the reservation is fixed. It keeps the two intermediate stage states in the
 library's fixed device scratch array, so it is checked here against the existing entry points, which
 take those states from the caller: boundary fill + compas_b200_rk3_stage, three times per step, with
 caller-allocated stage buffers. Two steps in a row, both must agree to the bit (the same kernels run

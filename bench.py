@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--n", type=int, default=256, help="cells per direction of the cube")
     ap.add_argument("--cpu-n", type=int, default=128, help="cube side of the CPU sample")
     ap.add_argument("--cpu-steps", type=int, default=6)
+    ap.add_argument("--error-steps", type=int, default=200,
+                    help="steps after which the mixed form's error against the FP64 form is measured")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
     ap.add_argument("--no-batched", action="store_true")
@@ -65,6 +67,11 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=16)
     ap.add_argument("--serve-rate", type=float, default=16.0, help="headline arrival rate (one of --serve-rates)")
     ap.add_argument("--serve-rates", default="4,16,64", help="arrival rates swept (requests/s)")
+    ap.add_argument("--serve-sizes", default="bench", choices=["bench", "config"],
+                    help="request sizes: 'bench' (reduced: 128-512^2, 64-96^3, 100-300 steps) or 'config' (the "
+                         "serving configuration: 128-1024^2, 64-192^3, triple point 224x96-896x384, 100-2000 steps)")
+    ap.add_argument("--serve-seq-sample", type=int, default=0,
+                    help="time the one-at-a-time baselines over this many steps per request and scale (0: all)")
     return ap.parse_args()
 
 
@@ -170,6 +177,66 @@ def cpu_baseline(n, steps):
     return {"value": val, "unit": UNIT, "cores": o.threads(), "kind": kind,
             "sample": f"{n}^3 cells of the same shock-droplet case, {steps} coarse steps (3 RK stages each) "
                       f"after one untimed step, OpenMP over {o.threads()} host threads, {el:.1f} s"}
+
+
+# Floating-point operations per cell and RK stage executed by the stage kernels of the 256^3
+# shock-droplet (SIXEQS 3D, WENO5 + HLLC + relaxation), from one ncu capture of each form on the
+# 128^3 case (smsp__sass_thread_inst_executed_op_{fadd,fmul,ffma,dadd,dmul,dfma}_pred_on.sum, an FMA
+# counted as 2, summed over the three RK stages and divided by 3 x the cells); the halo cells each
+# tile converts again and the relaxation's iterations are included, as executed.
+STAGE_FLOPS = {"mixed": None, "fp64": None}
+STAGE_FLOPS_SOURCE = "not measured yet"
+
+
+def stage_kernel_times(cb, torch, p, g, lv, stream, cells, N):
+    """Mean CUDA-event duration of the stage kernel of one form over two steps' stages (launched alone,
+    after a warm-up step), with its algorithmic bytes per launch and the boundary-fill time."""
+    shape = cb.padded_shape(p, g)
+    Us = torch.empty(shape, dtype=torch.float64, device="cuda")
+    lv.download(out=Us, stream=stream)
+    cb.FillPatch(p, g, Us, stream=stream)
+    U0 = Us.clone()
+    Un = torch.empty_like(Us)
+    dt_dev = torch.tensor([1e-9], dtype=torch.float64, device="cuda")
+    cmax = torch.zeros(1, dtype=torch.float64, device="cuda")
+    errw = torch.zeros(1, dtype=torch.int32, device="cuda")
+    for s in range(3):
+        cb.ThirdOrderSSPRK_stage(p, g, s, Us, U0, Un, dt_dev, cmax, errw, stream=stream)
+    torch.cuda.synchronize()
+    durs, algo = [], []
+    for _ in range(2):
+        for s in range(3):
+            ea = torch.cuda.Event(enable_timing=True)
+            eb = torch.cuda.Event(enable_timing=True)
+            ea.record(stream)
+            cb.ThirdOrderSSPRK_stage(p, g, s, Us, U0, Un, dt_dev, cmax, errw, stream=stream)
+            eb.record(stream)
+            eb.synchronize()
+            durs.append(ea.elapsed_time(eb) / 1e3)
+            algo.append(cells * N * 8 * (2 if s == 0 else 3))
+    fa = torch.cuda.Event(enable_timing=True)
+    fb = torch.cuda.Event(enable_timing=True)
+    fa.record(stream)
+    cb.FillPatch(p, g, Us, stream=stream)
+    fb.record(stream)
+    fb.synchronize()
+    return {"mean_s": sum(durs) / len(durs), "bytes": sum(algo) / len(algo), "fill_ms": fa.elapsed_time(fb)}
+
+
+def compute_roofline(name, mean_s, cells, fma_peaks):
+    """FP32 and FP64 pipe fractions of one form's stage kernel: executed FLOPs per launch (the frozen
+    per-cell counts) / the launch's mean duration, against the measured FMA throughputs."""
+    fl = STAGE_FLOPS.get(name)
+    out = {"peak_tflops": {k: v / 1e12 for k, v in fma_peaks.items()},
+           "peak_source": "compas_b200_fma_peak: sustained FMA rate of each pipe, measured in this run"}
+    if fl is None:
+        out["note"] = "FLOPs per cell-stage " + STAGE_FLOPS_SOURCE
+        return out
+    for k in ("fp32", "fp64"):
+        ach = fl[k] * cells / mean_s
+        out[k] = {"flops_per_cell_stage": fl[k], "achieved_tflops": ach / 1e12, "frac": ach / fma_peaks[k]}
+    out["flops_source"] = STAGE_FLOPS_SOURCE
+    return out
 
 
 def run_batched(args):
@@ -407,30 +474,44 @@ def run_serving(args, rank=0, world=1, dist=None):
 
     from compas_b200 import replicas, serving
 
+    if args.serve_sizes == "config":
+        sizes = dict(sides2d=(128, 1024), sides3d=(64, 192), sides_triple=(32, 128), steps=(100, 2000))
+        sizes_txt = ("2D FIVEEQS shock-bubble 128^2-1024^2, 3D SIXEQS shock-droplet 64^3-192^3 and 2D FIVEEQS_NPHASE "
+                     "(NPHASE 3) triple point 224x96-896x384, 100-2000 steps each")
+    else:
+        sizes = dict(sides2d=(128, 512), sides3d=(64, 96), sides_triple=(32, 96), steps=(100, 300))
+        sizes_txt = ("2D FIVEEQS shock-bubble 128^2-512^2, 3D SIXEQS shock-droplet 64^3-96^3 and 2D FIVEEQS_NPHASE "
+                     "(NPHASE 3) triple point 224x96-672x288, 100-300 steps each (reduced sizes)")
+
     def reqs_at(rate):
-        return serving.poisson_requests(args.serve_requests, rate, seed=0, sides2d=(128, 512), sides3d=(64, 96),
-                                        sides_triple=(32, 96), steps=(100, 300))
+        return serving.poisson_requests(args.serve_requests, rate, seed=0, **sizes)
 
     rates = [float(x) for x in args.serve_rates.split(",")]
     base = reqs_at(rates[0])
-    service = serving.sequential_service(replicas.deal_requests(base, rank, world), precision="fp64")
+    mine_base = replicas.deal_requests(base, rank, world)
+    sample = args.serve_seq_sample or None
+    service = serving.sequential_service(mine_base, precision="fp64", sample_steps=sample)
+    service_mixed = serving.sequential_service(mine_base, precision="mixed", sample_steps=sample)
     kinds = {k: sum(1 for r in base if r.kind == k) for k in serving.KINDS}
-    out = {"workload": f"{len(base)} requests {kinds}, Poisson arrivals at each rate (seed 0): 2D FIVEEQS "
-                       "shock-bubble 128^2-512^2, 3D SIXEQS shock-droplet 64^3-96^3 and 2D FIVEEQS_NPHASE (NPHASE 3) "
-                       "triple point 224x96-672x288, 100-300 steps each; budget 150 GB per GPU; continuous batching "
-                       "in the mixed form vs the same requests one at a time on the plain FP64 path"
+    out = {"workload": f"{len(base)} requests {kinds}, Poisson arrivals at each rate (seed 0): {sizes_txt}; budget "
+                       "150 GB per GPU; continuous batching in the mixed form vs the same requests one at a time in "
+                       "the mixed form and on the plain FP64 path; initial states built before the clock starts"
+                       + (f"; one-at-a-time service timed over {sample} steps per request and scaled" if sample else "")
                        + (f"; requests dealt round-robin to {world} GPUs" if world > 1 else ""),
            "rates": {}}
     for rate in rates:
         reqs = replicas.deal_requests(reqs_at(rate), rank, world)
         srv = serving.Server(budget_bytes=150e9, precision="mixed", steps_per_iter=4)
+        srv.prepare(reqs)
         t0 = time.perf_counter()
         done = srv.run(reqs)
         wall = time.perf_counter() - t0
         srv.close()
         mine = {"tts": [r.finished - r.arrival for r in done], "work": sum(r.cells * 3 * r.steps for r in done),
                 "wall": wall, "seq_tts": serving.sequential_tts(reqs, service),
-                "seq_busy": sum(service[r.rid] for r in reqs)}
+                "seq_busy": sum(service[r.rid] for r in reqs),
+                "seqm_tts": serving.sequential_tts(reqs, service_mixed),
+                "seqm_busy": sum(service_mixed[r.rid] for r in reqs)}
         allr = replicas.gather(mine, dist)
         if rank != 0:
             continue
@@ -444,8 +525,15 @@ def run_serving(args, rank=0, world=1, dist=None):
                 "cell_updates_per_s_per_stage": work / wall_max, "wall_s": wall_max}
         seq = {"p50_tts_s": float(np.percentile(seq_tts, 50)), "p99_tts_s": float(np.percentile(seq_tts, 99)),
                "cell_updates_per_s_per_stage": work / busy_max, "busy_s": busy_max}
+        seqm_tts = np.concatenate([np.asarray(x["seqm_tts"]) for x in allr])
+        busym_max = max(x["seqm_busy"] for x in allr)
+        seqm = {"p50_tts_s": float(np.percentile(seqm_tts, 50)), "p99_tts_s": float(np.percentile(seqm_tts, 99)),
+                "cell_updates_per_s_per_stage": work / busym_max, "busy_s": busym_max}
         out["rates"][f"{rate:g}/s"] = {
-            "continuous_batching_mixed": summ, "sequential_fp64": seq,
+            "continuous_batching_mixed": summ, "sequential_mixed": seqm, "sequential_fp64": seq,
+            # batching gain (same precision) and the precision gain, separately
+            "batching_gain_vs_sequential_mixed": summ["cell_updates_per_s_per_stage"] / seqm["cell_updates_per_s_per_stage"],
+            "precision_gain_sequential": seqm["cell_updates_per_s_per_stage"] / seq["cell_updates_per_s_per_stage"],
             "throughput_ratio": summ["cell_updates_per_s_per_stage"] / seq["cell_updates_per_s_per_stage"]}
     if rank != 0:
         return None
@@ -540,9 +628,18 @@ def run_ours(args, rank, world, dist):
     p = forms[head]
     value = replicas.whole_job_rate(cells, 3, args.steps, ms[head] / 1e3, world)
 
-    # error of the mixed form against the FP64 form after the same warm-up + timed steps
+    # error of the mixed form against the FP64 form after the configuration's step count (both levels
+    # continue, untimed, from the warm-up + timed steps to --error-steps)
     err = None
     if len(levels) == 2:
+        done = args.warmup + args.steps
+        if args.error_steps > done:
+            for lvx in levels.values():
+                lvx.advance(args.error_steps - done, use_graph=True, stream=stream)
+            torch.cuda.synchronize()
+            for lvx in levels.values():
+                assert lvx.sync().status == 0
+        done = max(done, args.error_steps)
         shape = cb.padded_shape(p, g)
         a = torch.empty(shape, dtype=torch.float64, device="cuda")
         b = torch.empty(shape, dtype=torch.float64, device="cuda")
@@ -552,48 +649,19 @@ def run_ours(args, rank, world, dist):
         va, vb = cb.valid_view(a, p, g), cb.valid_view(b, p, g)
         names = ["a1rho1", "a2rho2", "rho_u", "rho_v", "rho_w", "a1rho1E1", "a2rho2E2", "alpha1"]
         err = {"norm": "relative L1 (sum|mixed - fp64| / sum|fp64|) per field after "
-                       f"{args.warmup + args.steps} steps of the {n}^3 workload",
+                       f"{done} steps of the {n}^3 workload",
                "fields": {nm: float((va[c] - vb[c]).abs().sum() / vb[c].abs().sum()) for c, nm in enumerate(names)},
                "bound": "<= 1e-5 in a1rho1, a2rho2, alpha1"}
         del a, b
 
-    # ---- roofline: the headline stage kernel alone, CUDA events around each launch ----
+    # ---- roofline: each form's stage kernel alone, CUDA events around each launch ----
     N = cb.nstate(p.physics, p.dim)
     shape = cb.padded_shape(p, g)
-    Us = torch.empty(shape, dtype=torch.float64, device="cuda")
-    levels[head].download(out=Us, stream=stream)
-    cb.FillPatch(p, g, Us, stream=stream)
-    U0 = Us.clone()
-    Un = torch.empty_like(Us)
-    dt_dev = torch.tensor([1e-9], dtype=torch.float64, device="cuda")
-    cmax = torch.zeros(1, dtype=torch.float64, device="cuda")
-    errw = torch.zeros(1, dtype=torch.int32, device="cuda")
-    for s in range(3):
-        cb.ThirdOrderSSPRK_stage(p, g, s, Us, U0, Un, dt_dev, cmax, errw, stream=stream)
-    torch.cuda.synchronize()
-    durs, algo = [], []
-    for _ in range(2):
-        for s in range(3):
-            ea = torch.cuda.Event(enable_timing=True)
-            eb = torch.cuda.Event(enable_timing=True)
-            ea.record(stream)
-            cb.ThirdOrderSSPRK_stage(p, g, s, Us, U0, Un, dt_dev, cmax, errw, stream=stream)
-            eb.record(stream)
-            eb.synchronize()
-            durs.append(ea.elapsed_time(eb) / 1e3)
-            algo.append(cells * N * 8 * (2 if s == 0 else 3))
-    fa = torch.cuda.Event(enable_timing=True)
-    fb = torch.cuda.Event(enable_timing=True)
-    fa.record(stream)
-    cb.FillPatch(p, g, Us, stream=stream)
-    fb.record(stream)
-    fb.synchronize()
-    fill_ms = fa.elapsed_time(fb)
-    mean_dur = sum(durs) / len(durs)
-    bytes_per_launch = sum(algo) / len(algo)
+    kern = {name: stage_kernel_times(cb, torch, forms[name], g, levels[name], stream, cells, N) for name in forms}
+    mean_dur, bytes_per_launch, fill_ms = kern[head]["mean_s"], kern[head]["bytes"], kern[head]["fill_ms"]
     achieved = bytes_per_launch / mean_dur / 1e9
     peak, peak_kind = measured_peaks()
-    del Us, U0, Un
+    fma_peaks = {"fp32": cb.fma_peak(False, stream=stream), "fp64": cb.fma_peak(True, stream=stream)}
 
     # ---- e2e: host state in, one step, result out, every step (headline form) ----
     lv = levels[head]
@@ -657,7 +725,15 @@ def run_ours(args, rank, world, dist):
                          "traffic_source": STAGE_TRAFFIC_SOURCE if head == "mixed" else None,
                          "kernel": f"stage_kernel<SixEq<3>, WENO5, {head}> (fused WENO5+HLLC+divergence+RK3+relaxation)",
                          "bytes_per_launch": bytes_per_launch, "mean_launch_ms": mean_dur * 1e3,
-                         "peak_source": f"{peak_kind} HBM copy bandwidth (MEASURED_PEAKS.json)"},
+                         "peak_source": f"{peak_kind} HBM copy bandwidth (MEASURED_PEAKS.json)",
+                         "compute": compute_roofline(head, mean_dur, cells, fma_peaks),
+                         # the plain FP64 form's kernel (bit-identical to the reference arithmetic)
+                         "fp64_form": ({"mean_launch_ms": kern["fp64"]["mean_s"] * 1e3,
+                                        "achieved": kern["fp64"]["bytes"] / kern["fp64"]["mean_s"] / 1e9,
+                                        "frac": kern["fp64"]["bytes"] / kern["fp64"]["mean_s"] / 1e9 / peak,
+                                        "compute": compute_roofline("fp64", kern["fp64"]["mean_s"], cells, fma_peaks),
+                                        "cell_updates_per_s_per_stage": cells / kern["fp64"]["mean_s"]}
+                                       if "fp64" in kern and head != "fp64" else None)},
             "fill_boundary_ms": fill_ms,
             "clocks": clk,
             "cpu_baseline": cpu,

@@ -85,6 +85,8 @@ class Parm(ctypes.Structure):
         ("Ck", ctypes.c_double * MAX_PHASES), ("Dk", ctypes.c_double * MAX_PHASES),
         ("autotune", ctypes.c_int),
         ("tma", ctypes.c_int),
+        ("cv_1", ctypes.c_double),
+        ("cv_2", ctypes.c_double),
     ]
 
 
@@ -113,6 +115,14 @@ _SIGS = {
                                                  ctypes.c_void_p]),
     "compas_b200_compute_dUdt": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_void_p,
                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "compas_b200_nc_terms": (ctypes.c_int, [ctypes.POINTER(Parm)]),
+    "compas_b200_tag_cells": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),
+    "compas_b200_fma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                            ctypes.c_void_p]),
+    "compas_b200_face_fluxes": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_void_p, ctypes.c_int,
+                                               ctypes.c_int, ctypes.c_void_p * 3, ctypes.c_void_p * 3,
+                                               ctypes.c_void_p, ctypes.c_void_p]),
     "compas_b200_rk3_stage": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_int,
                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
@@ -296,6 +306,126 @@ def compute_dUdt_FV(p: Parm, g: Geom, U, dUdt, cmax=None, err=None, stream=None)
     (Compressible_PhaseField::compute_dUdt_FV, source/Class_Compressible_PhaseField.cpp:3472-3537)."""
     _check(lib().compas_b200_compute_dUdt(ctypes.byref(p), ctypes.byref(g), _ptr(U), _ptr(dUdt), _ptr(cmax),
                                           _ptr(err), _stream_ptr(stream)))
+
+
+def fma_peak(fp64: bool, iters: int = 1 << 14, stream=None) -> float:
+    """Measured sustained FMA throughput (FLOP/s) of the FP32 or FP64 pipe of the current GPU."""
+    out = ctypes.c_double()
+    _check(lib().compas_b200_fma_peak(int(bool(fp64)), int(iters), ctypes.byref(out), _stream_ptr(stream)))
+    return out.value
+
+
+class TagCriterion(ctypes.Structure):
+    """ctypes mirror of ``compas_b200_tag_criterion``."""
+
+    _fields_ = [("var", ctypes.c_int), ("derived", ctypes.c_int), ("kind", ctypes.c_int),
+                ("v0", ctypes.c_double), ("v1", ctypes.c_double)]
+
+
+TAG_GRAD, TAG_LESS, TAG_GREATER, TAG_RANGE = 0, 1, 2, 3
+
+# vnamesC / vnamesD of the two-phase models (include/Physics_Compressible5Eq/Variables_Compressible5Eq.H:18-19,
+# include/Physics_Compressible6Eq/Variables_Compressible6Eq.H:18-19)
+_STATE_NAMES = {
+    FIVEEQS: lambda dim: ["a1rho1", "a2rho2", "rho_u", "rho_v", "rho_w"][:2 + dim] + ["rho_E", "a1"],
+    SIXEQS: lambda dim: ["a1rho1", "a2rho2", "rho_u", "rho_v", "rho_w"][:2 + dim] + ["a1rho1E1", "a2rho2E2", "a1"],
+}
+_DERIVED_NAMES = {
+    FIVEEQS: ["a1rho1", "a2rho2", "rho_u", "rho_v", "rho_w", "rho_E", "a1", "rho", "u", "v", "w", "P", "T", "c",
+              "Mach", "vorticity_mag", "q_criterion", "lambda2"],
+    SIXEQS: ["a1rho1", "a2rho2", "rho_u", "rho_v", "rho_w", "a1rho1E1", "a2rho2E2", "a1", "rho", "u", "v", "w", "P",
+             "a1P1", "a2P2", "T", "c", "Mach", "vorticity_mag", "q_criterion", "lambda2"],
+}
+
+
+def tag_variable(physics: int, dim: int, name: str) -> tuple:
+    """(index, derived) of a refinement variable name, state names first (the reference's
+    VariableRegistry, include/Tagging.H:25-76)."""
+    state = _STATE_NAMES[physics](dim)
+    if name in state:
+        return state.index(name), 0
+    derived = _DERIVED_NAMES[physics]
+    if name in derived:
+        return derived.index(name), 1
+    raise CompasError(EARG, f"Unknown refinement variable: {name}")
+
+
+def _floats(v):
+    if isinstance(v, str):
+        return [float(x) for x in v.split()]
+    if isinstance(v, (list, tuple)):
+        return [float(x) for x in v]
+    return [float(v)]
+
+
+def tag_criteria(physics: int, dim: int, inputs: dict, lev: int, max_level: int | None = None) -> list:
+    """The criteria ErrorEst applies on level `lev` from the run.refine.* inputs keys
+    (source/COMPAS.cpp:1473-1532 reads them, :835-905 applies them): run.refine.ref_vars names the
+    variables; run.refine.<name>.grad / value_less / value_greater hold one threshold per level,
+    value_range two, run.refine.<name>.max_level the first level not tagged. max_level is the
+    hierarchy's amr.max_level (default: the inputs key, else lev + 1); a threshold list too short for
+    the levels tagged is an error, as in the reference."""
+    if max_level is None:
+        max_level = int(inputs.get("amr.max_level", lev + 1))
+    names = inputs.get("run.refine.ref_vars", [])
+    names = names.split() if isinstance(names, str) else list(names)
+    out = []
+    for name in names:
+        var, derived = tag_variable(physics, dim, name)
+        vmax = int(inputs.get(f"run.refine.{name}.max_level", 1 << 30))
+        n_tag = max(0, min(vmax, max_level))
+        for opt, kind, per in (("grad", TAG_GRAD, 1), ("value_less", TAG_LESS, 1),
+                               ("value_greater", TAG_GREATER, 1), ("value_range", TAG_RANGE, 2)):
+            key = f"run.refine.{name}.{opt}"
+            if key not in inputs:
+                continue
+            vals = _floats(inputs[key])
+            if len(vals) < per * n_tag:
+                raise CompasError(EARG, f"run.refine.{name}.{opt} has {len(vals)} values, but {per * n_tag} are "
+                                        f"needed to tag levels 0 to {n_tag - 1}")
+            if lev >= vmax:
+                continue
+            c = TagCriterion(var, derived, kind, vals[per * lev], vals[per * lev + 1] if per == 2 else 0.0)
+            out.append(c)
+    return out
+
+
+def tag_cells(p: Parm, g: Geom, U, criteria, tags, stream=None) -> None:
+    """Refinement tags (1 tagged, 0 not) of the valid cells of one box into the device byte array
+    tags (n[0] x n[1] x n[2], x fastest) from the ghost-filled padded state U (ErrorEst,
+    source/COMPAS.cpp:767-932)."""
+    arr = (TagCriterion * max(1, len(criteria)))(*criteria)
+    _check(lib().compas_b200_tag_cells(ctypes.byref(p), ctypes.byref(g), _ptr(U), ctypes.addressof(arr),
+                                       len(criteria), _ptr(tags), _stream_ptr(stream)))
+
+
+FACES_ALL, FACES_BOUNDARY = 0, 1
+
+
+def nc_terms(p: Parm) -> int:
+    """Non-conservative face terms of the model (NC_TERMS: 1 five-equation, 3 six-equation)."""
+    n = lib().compas_b200_nc_terms(ctypes.byref(p))
+    if n <= 0:
+        _check(n)
+    return n
+
+
+def face_shape(p: Parm, g: Geom, d: int, ncomp: int) -> tuple:
+    """Shape (components, z, y, x) of the face array of direction d (a face MultiFab without ghosts)."""
+    n = [g.n[0] + (d == 0), g.n[1] + (d == 1), (g.n[2] + (d == 2)) if p.dim == 3 else 1]
+    return (ncomp, n[2], n[1], n[0])
+
+
+def face_fluxes(p: Parm, g: Geom, Us, flux, flux_nc=None, which=FACES_ALL, area_scaled=True, err=None,
+                stream=None) -> None:
+    """Face fluxes of one box from its ghost-filled stage state for the flux registers, area-scaled as
+    ScaleFaceFluxesByArea (source/Class_Compressible_PhaseField.cpp:3433-3466) unless area_scaled is
+    False; flux[d] / flux_nc[d] are device arrays of face_shape(p, g, d, ...) or None."""
+    fl = (ctypes.c_void_p * 3)(*[_ptr(flux[d]) if flux is not None and d < len(flux) else None for d in range(3)])
+    fn = (ctypes.c_void_p * 3)(*[_ptr(flux_nc[d]) if flux_nc is not None and d < len(flux_nc) else None
+                                 for d in range(3)])
+    _check(lib().compas_b200_face_fluxes(ctypes.byref(p), ctypes.byref(g), _ptr(Us), int(which), int(bool(area_scaled)),
+                                         fl, fn, _ptr(err), _stream_ptr(stream)))
 
 
 def ThirdOrderSSPRK_stage(p: Parm, g: Geom, stage: int, Us, Uold, Unew, dt_dev, cmax=None, err=None,

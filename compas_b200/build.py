@@ -1,9 +1,13 @@
 """Build of the CUDA library libcompas_b200.so (sm_100a) in-tree.
 
 The plain FP64 path must reproduce the reference's CPU arithmetic, so the library is compiled with
-FMA contraction off (-fmad=false) and IEEE division and square root (the nvcc defaults). The stage
-kernels of each model and dimension are separate translation units (csrc/kern_*.cu), compiled in
-parallel and linked with the C-ABI unit (csrc/compas_b200.cu).
+FMA contraction off (-fmad=false) and IEEE division and square root (the nvcc defaults). The mixed
+form keeps contraction off too: its FMAs are written out (__fmaf_rn) where they are wanted, so every
+launch shape of a stage kernel gives the same bits (with contraction on, the compiler contracted the
+launch shapes' instantiations differently, and it measured no faster). The stage kernels of each
+model and dimension are separate translation units per precision form (csrc/kern_<model>.cu plain
+FP64, csrc/kern_<model>_mixed.cu mixed precision), compiled in parallel and linked with the C-ABI
+unit (csrc/compas_b200.cu).
 """
 from __future__ import annotations
 

@@ -309,6 +309,9 @@ static Eos make_eos(const compas_b200_parm* p) {
         e.Ck[k] = p->Ck[k];
         e.Dk[k] = p->Dk[k];
     }
+    e.fA1 = (float)p->A1; e.fA2 = (float)p->A2;
+    e.fB1 = (float)p->B1; e.fB2 = (float)p->B2;
+    e.fC1 = (float)p->C1; e.fC2 = (float)p->C2;
     return e;
 }
 
@@ -649,7 +652,8 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 __global__ void noalloc_set_dt_kernel(double* dt_slot, double dt) { *dt_slot = dt; }
 
-// Device address of g_noalloc_scratch on the current device, looked up once per device.
+// Device address of g_noalloc_scratch on the current device, looked up once per device and kept
+// for the life of the process (a cudaDeviceReset of that device invalidates it).
 static int noalloc_scratch(unsigned char** out) {
     static std::mutex mu;
     static unsigned char* addr[128] = {nullptr};
@@ -673,6 +677,7 @@ static int noalloc_scratch(unsigned char** out) {
 
 #include "batch.cuh"
 #include "amr.cuh"
+#include "tagging.cuh"
 
 // ================================================================================================
 // C ABI
@@ -802,6 +807,8 @@ int compas_b200_parm_init_nphase(compas_b200_parm* p, int physics, int dim, int 
     p->pf_tol_rel = 1.0e-10;
     p->autotune = 1;
     p->tma = 1;
+    p->cv_1 = 1.0;
+    p->cv_2 = 1.0;
     if (physics != COMPAS_B200_FIVEEQS && physics != COMPAS_B200_SIXEQS && physics != COMPAS_B200_FIVEEQS_NPHASE)
         return fail(COMPAS_B200_EARG, "physics must be FIVEEQS (555), SIXEQS (666) or FIVEEQS_NPHASE (55501)");
     if (dim != 2 && dim != 3) return fail(COMPAS_B200_EARG, "dim must be 2 or 3");
@@ -921,6 +928,7 @@ int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value
                           {"prob.EOS.pinf_1", &p->pinf_1},   {"prob.EOS.pinf_2", &p->pinf_2},
                           {"prob.EOS.b_1", &p->b_1},         {"prob.EOS.b_2", &p->b_2},
                           {"prob.EOS.q_1", &p->q_1},         {"prob.EOS.q_2", &p->q_2},
+                          {"prob.EOS.cv_1", &p->cv_1},       {"prob.EOS.cv_2", &p->cv_2},
                           {"run.cfl", &p->cfl}};
     for (const auto& dk : dkeys)
         if (k == dk.name) {
@@ -1257,6 +1265,7 @@ int compas_b200_rk3_step_noalloc(const compas_b200_parm* p, const compas_b200_ge
     a.dt = dt_dev;
     a.cmax = reinterpret_cast<unsigned long long*>(cmax_dev);
     a.err = err_dev;
+    const int shape = cached_shape(p, g, a);  // a host-side cache read: allocates nothing
     double* ins[3] = {U, U1, U2};
     double* outs[3] = {U1, U2, U};
     for (int s = 0; s < 3; ++s) {
@@ -1265,7 +1274,7 @@ int compas_b200_rk3_step_noalloc(const compas_b200_parm* p, const compas_b200_ge
         a.Us = ins[s];
         a.U0 = U;
         a.Uout = outs[s];
-        if ((rc = launch_stage(p, a, st))) return rc;
+        if ((rc = launch_stage(p, a, st, 0, shape))) return rc;
     }
     return COMPAS_B200_OK;
 }
@@ -2032,3 +2041,51 @@ long long compas_b200_batch_launches(compas_b200_batch* b) { return b ? b->launc
 }  // extern "C"
 
 #include "amr_api.inc"
+
+int compas_b200_tag_cells(const compas_b200_parm* p, const compas_b200_geom* g, const double* U,
+                          const compas_b200_tag_criterion* criteria, int ncriteria, unsigned char* tags,
+                          void* stream) {
+    using namespace compas;
+    int rc = check_args(p, g);
+    if (rc) return rc;
+    if (!U || !tags) return fail(COMPAS_B200_EARG, "null state or tag array");
+    if (ncriteria < 0 || ncriteria > kMaxTagCriteria || (ncriteria > 0 && !criteria))
+        return fail(COMPAS_B200_EARG, "between 0 and " + std::to_string(kMaxTagCriteria) + " tagging criteria");
+    if (p->physics == COMPAS_B200_FIVEEQS_NPHASE)
+        return fail(COMPAS_B200_EUNSUPPORTED, "refinement tagging: FIVEEQS and SIXEQS");
+    if (g->ng < 2) return fail(COMPAS_B200_EARG, "refinement tagging needs two ghost cells");
+    const int nderived = (p->physics == COMPAS_B200_SIXEQS) ? 21 : 18;
+    TagArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.U = U;
+    a.g = make_grid(p, g);
+    a.e = make_eos(p);
+    a.cv1 = p->cv_1;
+    a.cv2 = p->cv_2;
+    a.ncrit = ncriteria;
+    a.tags = tags;
+    for (int v = 0; v < ncriteria; ++v) {
+        const compas_b200_tag_criterion& c = criteria[v];
+        if (c.kind < COMPAS_B200_TAG_GRAD || c.kind > COMPAS_B200_TAG_RANGE)
+            return fail(COMPAS_B200_EARG, "tagging criterion kind must be GRAD, LESS, GREATER or RANGE");
+        if (c.var < 0 || c.var >= (c.derived ? nderived : nstate(p)))
+            return fail(COMPAS_B200_EARG, "tagging criterion variable out of range");
+        a.c[v].var = c.var;
+        a.c[v].derived = c.derived ? 1 : 0;
+        a.c[v].kind = c.kind;
+        a.c[v].v0 = c.v0;
+        a.c[v].v1 = c.v1;
+    }
+    const long long n = (long long)a.g.n[0] * a.g.n[1] * a.g.n[2];
+    const unsigned blocks = (unsigned)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148LL * 32));
+    cudaStream_t st = (cudaStream_t)stream;
+    if (p->physics == COMPAS_B200_SIXEQS) {
+        if (p->dim == 2) tag_kernel<SixEq<2>><<<blocks, 256, 0, st>>>(a);
+        else tag_kernel<SixEq<3>><<<blocks, 256, 0, st>>>(a);
+    } else {
+        if (p->dim == 2) tag_kernel<FiveEq<2>><<<blocks, 256, 0, st>>>(a);
+        else tag_kernel<FiveEq<3>><<<blocks, 256, 0, st>>>(a);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return COMPAS_B200_OK;
+}

@@ -1,0 +1,4 @@
+// Stage kernels of the FiveEq<2> model (instantiations and launchers), mixed-precision form.
+#include "kern_impl.cuh"
+
+COMPAS_DEFINE_LAUNCHERS(fiveeq2, FiveEq<2>, 1)

@@ -1,4 +1,4 @@
-// Stage kernels of the FiveEq<3> model (instantiations and launchers).
+// Stage kernels of the FiveEq<3> model (instantiations and launchers), plain FP64 form.
 #include "kern_impl.cuh"
 
-COMPAS_DEFINE_LAUNCHERS(fiveeq3, FiveEq<3>)
+COMPAS_DEFINE_LAUNCHERS(fiveeq3, FiveEq<3>, 0)

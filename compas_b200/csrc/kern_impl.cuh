@@ -109,19 +109,12 @@ static cudaError_t launch_stage_var(const KernelChoice& k, const StageArgs& a, c
     }
 }
 
-template <class M>
+// The kernels of one precision form (MIX); the two forms are separate translation units (built in
+// parallel).
+template <class M, bool MIX>
 static cudaError_t launch_stage_m(const KernelChoice& k, const StageArgs& a, cudaStream_t st, const TmaMaps* tm) {
-    const bool mix = (k.precision == 1), bounded = (k.limiter == 6);
-    if (k.limiter < 5)  // GODUNOV / MUSCL family
-        return mix ? launch_stage_var<M, 2, true>(k, a, st, tm) : launch_stage_var<M, 2, false>(k, a, st, tm);
-    if constexpr (M::KIND == kModelFiveN) {
-        if (mix) return bounded ? launch_stage_var<M, 6, true>(k, a, st, tm) : launch_stage_var<M, 5, true>(k, a, st, tm);
-        return bounded ? launch_stage_var<M, 6, false>(k, a, st, tm) : launch_stage_var<M, 5, false>(k, a, st, tm);
-    } else {
-        if (mix)
-            return bounded ? launch_stage_var<M, 6, true>(k, a, st, tm) : launch_stage_var<M, 5, true>(k, a, st, tm);
-        return bounded ? launch_stage_var<M, 6, false>(k, a, st, tm) : launch_stage_var<M, 5, false>(k, a, st, tm);
-    }
+    if (k.limiter < 5) return launch_stage_var<M, 2, MIX>(k, a, st, tm);  // GODUNOV / MUSCL / WENO3 family
+    return (k.limiter == 6) ? launch_stage_var<M, 6, MIX>(k, a, st, tm) : launch_stage_var<M, 5, MIX>(k, a, st, tm);
 }
 
 // Persistent box-list launch: one resident wave of CTAs walks the tiles of every box.
@@ -153,30 +146,22 @@ static cudaError_t launch_list_s(const KernelChoice& k, const ListArgs& L, cudaS
     }
 }
 
-template <class M>
+template <class M, bool MIX>
 static cudaError_t launch_list_m(const KernelChoice& k, const ListArgs& L, cudaStream_t st) {
-    if (k.limiter < 5)  // GODUNOV / MUSCL / WENO3 family
-        return (k.precision == 1) ? launch_list_s<M, 2, true>(k, L, st) : launch_list_s<M, 2, false>(k, L, st);
-    if constexpr (M::KIND == kModelFiveN) {
-        if (k.precision == 1)
-            return (k.limiter == 6) ? launch_list_s<M, 6, true>(k, L, st) : launch_list_s<M, 5, true>(k, L, st);
-        return (k.limiter == 6) ? launch_list_s<M, 6, false>(k, L, st) : launch_list_s<M, 5, false>(k, L, st);
-    } else {
-        if (k.precision == 1)
-            return (k.limiter == 6) ? launch_list_s<M, 6, true>(k, L, st) : launch_list_s<M, 5, true>(k, L, st);
-        return (k.limiter == 6) ? launch_list_s<M, 6, false>(k, L, st) : launch_list_s<M, 5, false>(k, L, st);
-    }
+    if (k.limiter < 5) return launch_list_s<M, 2, MIX>(k, L, st);  // GODUNOV / MUSCL / WENO3 family
+    return (k.limiter == 6) ? launch_list_s<M, 6, MIX>(k, L, st) : launch_list_s<M, 5, MIX>(k, L, st);
 }
 
 }  // namespace compas
 
-#define COMPAS_DEFINE_LAUNCHERS(name, Model)                                                         \
+// PREC 0: the plain FP64 form (launch_*_<name>_p0), PREC 1: the mixed form (launch_*_<name>_p1).
+#define COMPAS_DEFINE_LAUNCHERS(name, Model, PREC)                                                   \
     namespace compas {                                                                              \
-    cudaError_t launch_stage_##name(const KernelChoice& k, const StageArgs& a, cudaStream_t st,     \
-                                    const TmaMaps* tm) {                                            \
-        return launch_stage_m<Model>(k, a, st, tm);                                                 \
+    cudaError_t launch_stage_##name##_p##PREC(const KernelChoice& k, const StageArgs& a, cudaStream_t st, \
+                                              const TmaMaps* tm) {                                  \
+        return launch_stage_m<Model, PREC == 1>(k, a, st, tm);                                      \
     }                                                                                               \
-    cudaError_t launch_list_##name(const KernelChoice& k, const ListArgs& L, cudaStream_t st) {      \
-        return launch_list_m<Model>(k, L, st);                                                      \
+    cudaError_t launch_list_##name##_p##PREC(const KernelChoice& k, const ListArgs& L, cudaStream_t st) { \
+        return launch_list_m<Model, PREC == 1>(k, L, st);                                           \
     }                                                                                               \
     }

@@ -1,0 +1,4 @@
+// Stage kernels of the SixEq<3> model (instantiations and launchers), mixed-precision form.
+#include "kern_impl.cuh"
+
+COMPAS_DEFINE_LAUNCHERS(sixeq3, SixEq<3>, 1)

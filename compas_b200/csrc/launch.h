@@ -31,10 +31,24 @@ constexpr int kOrders = 2;
 constexpr int kTile2 = 16;
 constexpr int kTile3 = 8;
 
+// Each model's kernels are compiled in two translation units, one per precision form (kern_<name>.cu
+// plain FP64, kern_<name>_mixed.cu mixed precision), built in parallel; launch_*_<name> picks the unit
+// by KernelChoice::precision.
 #define COMPAS_DECLARE_LAUNCHERS(name)                                                               \
-    cudaError_t launch_stage_##name(const KernelChoice& k, const StageArgs& a, cudaStream_t st,        \
-                                    const TmaMaps* tm);                                              \
-    cudaError_t launch_list_##name(const KernelChoice& k, const ListArgs& L, cudaStream_t st);
+    cudaError_t launch_stage_##name##_p0(const KernelChoice& k, const StageArgs& a, cudaStream_t st,   \
+                                         const TmaMaps* tm);                                         \
+    cudaError_t launch_stage_##name##_p1(const KernelChoice& k, const StageArgs& a, cudaStream_t st,   \
+                                         const TmaMaps* tm);                                         \
+    cudaError_t launch_list_##name##_p0(const KernelChoice& k, const ListArgs& L, cudaStream_t st);   \
+    cudaError_t launch_list_##name##_p1(const KernelChoice& k, const ListArgs& L, cudaStream_t st);   \
+    inline cudaError_t launch_stage_##name(const KernelChoice& k, const StageArgs& a, cudaStream_t st, \
+                                           const TmaMaps* tm) {                                      \
+        return (k.precision == 1) ? launch_stage_##name##_p1(k, a, st, tm)                           \
+                                  : launch_stage_##name##_p0(k, a, st, tm);                          \
+    }                                                                                                \
+    inline cudaError_t launch_list_##name(const KernelChoice& k, const ListArgs& L, cudaStream_t st) { \
+        return (k.precision == 1) ? launch_list_##name##_p1(k, L, st) : launch_list_##name##_p0(k, L, st); \
+    }
 COMPAS_DECLARE_LAUNCHERS(fiveeq2)
 COMPAS_DECLARE_LAUNCHERS(fiveeq3)
 COMPAS_DECLARE_LAUNCHERS(sixeq2)

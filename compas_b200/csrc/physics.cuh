@@ -62,6 +62,9 @@ struct Eos {
     double pinf1, pinf2;  // B1/(A1 + 1), B2/(A2 + 1) (the relaxation's admissibility check)
     double pmin1, pmin2;  // p_min of the two-phase Parm (source/Parm.cpp:164-171): -B/A, or -B/(A + 1) with K
     double Ak[kMaxPhases], Bk[kMaxPhases], Ck[kMaxPhases], Dk[kMaxPhases];
+    // FP32 copies (round to nearest) of A, B, C of the two phases for the mixed form's FP32 wave speeds,
+    // so that the face loop converts no coefficients
+    float fA1, fA2, fB1, fB2, fC1, fC2;
 };
 
 // Model families of the stage kernel (the M::KIND of each model struct).
@@ -344,11 +347,11 @@ __device__ __forceinline__ float fiveeq_c_f32(const float* w, const Eos& e, int 
     using M = FiveEq<DIM>;
     constexpr int IE = M::IE, IA = M::IA;
     const float p = w[IE], a1 = w[IA], a2 = 1.0f - a1;
-    const float A1 = (float)e.A1, A2 = (float)e.A2, B1 = (float)e.B1, B2 = (float)e.B2;
+    const float A1 = e.fA1, A2 = e.fA2, B1 = e.fB1, B2 = e.fB2;
     const float r1 = __fdividef(__fmaf_rn(A1 + 1.0f, p, B1), A1);
     const float r2 = __fdividef(__fmaf_rn(A2 + 1.0f, p, B2), A2);
-    const float ph1 = (e.C1 > 0.0) ? a1 - (float)e.C1 * w[0] : a1;
-    const float ph2 = (e.C2 > 0.0) ? a2 - (float)e.C2 * w[1] : a2;
+    const float ph1 = (e.fC1 > 0.0f) ? a1 - e.fC1 * w[0] : a1;
+    const float ph2 = (e.fC2 > 0.0f) ? a2 - e.fC2 * w[1] : a2;
     float rc2;
     if (id_k == 0)
         rc2 = __fdividef(__fmaf_rn(a1 * A1, r1, (a2 * A2) * r2), __fmaf_rn(ph1, A1, ph2 * A2));
@@ -382,7 +385,28 @@ __device__ __forceinline__ void fiveeq_hllc_mixed(double* Fout, double* fnc, flo
     const float eL = (1.0f + fm1L) * dSL * (rhoL * S + __fdividef(pL, gL));
     const float eR = (1.0f + fm1R) * dSR * (rhoR * S + __fdividef(pR, gR));
     const float mL = (1.0f + fm1L) * rhoL * dSL, mR = (1.0f + fm1R) * rhoR * dSR;
-    const float s = (S > 0.0f) ? 1.0f : ((S < 0.0f) ? -1.0f : 0.0f);
+    if (S != 0.0f) {
+        // FP64 assembly of the upwind side K only (left where S > 0): F = F_K + S_K (U*_K - U_K), the
+        // value of the blend below, whose weights are then 1 and 0
+        const bool lt = (S > 0.0f);
+        const double V = lt ? VL : VR, p = lt ? pL : pR, gm = lt ? fm1L : fm1R, Sk = lt ? Sm : Sp;
+        const double en = lt ? eL : eR, mo = lt ? mL : mR;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            const double u = lt ? UL[i] : UR[i];
+            double f = u * V, dd = gm * u;
+            if (i == IE) {
+                f = (u + p) * V;
+                dd += en;
+            } else if (i >= 2 && i < 2 + DIM && i - 2 == d) {
+                f += p;
+                dd += mo;
+            }
+            Fout[i] = fma(Sk, dd, f);
+        }
+        fnc[0] = fma(Sk, gm, V);
+    } else {
+    const float s = 0.0f;
     // FP64 assembly: F = h+ (F_L + S- (U*_L - U_L)) + h- (F_R + S+ (U*_R - U_R))
     const double hp = 0.5 * (1.0 + s), hm = 0.5 * (1.0 - s);
     const double gmL = fm1L, gmR = fm1R, Smd = Sm, Spd = Sp;
@@ -405,6 +429,7 @@ __device__ __forceinline__ void fiveeq_hllc_mixed(double* Fout, double* fnc, flo
         Fout[i] = hp * (fl + Smd * dL) + hm * (fr + Spd * dR);
     }
     fnc[0] = (hp * VLd + hm * VRd) + ((hp * Smd) * gmL + (hm * Spd) * gmR);
+    }
     float kL = wL[2] * wL[2] + wL[3] * wL[3], kR = wR[2] * wR[2] + wR[3] * wR[3];
     if (DIM == 3) { kL += wL[4] * wL[4]; kR += wR[4] * wR[4]; }
     cmax = fmaxf(cL + sqrtf(kL), cR + sqrtf(kR));
@@ -636,10 +661,10 @@ __device__ __forceinline__ float sixeq_c_f32(const float* w, const Eos& e) {
     using M = SixEq<DIM>;
     constexpr int IE1 = M::IE1, IE2 = M::IE2, IA = M::IA;
     const float a1 = w[IA];
-    const float xi1 = (e.C1 > 0.0 && a1 > 0.0f) ? 1.0f - (float)e.C1 * __fdividef(w[0], a1) : 1.0f;
-    const float xi2 = (e.C2 > 0.0 && 1.0f - a1 > 0.0f) ? 1.0f - (float)e.C2 * __fdividef(w[1], 1.0f - a1) : 1.0f;
-    const float r1 = __fdividef(__fmaf_rn((float)e.A1 + 1.0f, w[IE1], a1 * (float)e.B1), (float)e.A1 * xi1);
-    const float r2 = __fdividef(__fmaf_rn((float)e.A2 + 1.0f, w[IE2], (1.0f - a1) * (float)e.B2), (float)e.A2 * xi2);
+    const float xi1 = (e.fC1 > 0.0f && a1 > 0.0f) ? 1.0f - e.fC1 * __fdividef(w[0], a1) : 1.0f;
+    const float xi2 = (e.fC2 > 0.0f && 1.0f - a1 > 0.0f) ? 1.0f - e.fC2 * __fdividef(w[1], 1.0f - a1) : 1.0f;
+    const float r1 = __fdividef(__fmaf_rn(e.fA1 + 1.0f, w[IE1], a1 * e.fB1), e.fA1 * xi1);
+    const float r2 = __fdividef(__fmaf_rn(e.fA2 + 1.0f, w[IE2], (1.0f - a1) * e.fB2), e.fA2 * xi2);
     return sqrtf(fmaxf(r1 + r2, 0.0f) / (w[0] + w[1]));
 }
 
@@ -671,7 +696,34 @@ __device__ __forceinline__ void sixeq_hllc_mixed(double* Fout, double* fnc, floa
     const float tL1 = qL * __fmaf_rn(S * wL[0], gL, a1p1L), tR1 = qR * __fmaf_rn(S * wR[0], gR, a1p1R);
     const float tL2 = qL * __fmaf_rn(S * wL[1], gL, a2p2L), tR2 = qR * __fmaf_rn(S * wR[1], gR, a2p2R);
     const float mL = fL * rhoL * dSL, mR = fR * rhoR * dSR;
-    const float s = (S > 0.0f) ? 1.0f : ((S < 0.0f) ? -1.0f : 0.0f);
+    if (S != 0.0f) {
+        // FP64 assembly of the upwind side K only (left where S > 0): F = F_K + S_K (U*_K - U_K), the
+        // value of the blend below, whose weights are then 1 and 0
+        const bool lt = (S > 0.0f);
+        const double V = lt ? VL : VR, gm = lt ? qL : qR, Sk = lt ? Sm : Sp;
+        const double p1 = lt ? a1p1L : a1p1R, p2 = lt ? a2p2L : a2p2R;
+        const double mo = lt ? mL : mR, t1 = lt ? tL1 : tR1, t2 = lt ? tL2 : tR2;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            const double u = lt ? UL[i] : UR[i];
+            double f = u * V, dd = gm * u;
+            if (i >= 2 && i < 2 + DIM && i - 2 == d) {
+                f += p1 + p2;
+                dd += mo;
+            } else if (i == IE1) {
+                f = (u + p1) * V;
+                dd += t1;
+            } else if (i == IE2) {
+                f = (u + p2) * V;
+                dd += t2;
+            }
+            Fout[i] = fma(Sk, dd, f);
+        }
+        fnc[0] = fma(Sk, gm, V);
+        fnc[1] = fma(Sk, t1, V * p1);
+        fnc[2] = fma(Sk, t2, V * p2);
+    } else {
+    const float s = 0.0f;
     const double hp = 0.5 * (1.0 + s), hm = 0.5 * (1.0 - s);
     const double gmL = qL, gmR = qR, Smd = Sm, Spd = Sp;
     const double VLd = VL, VRd = VR;
@@ -701,6 +753,7 @@ __device__ __forceinline__ void sixeq_hllc_mixed(double* Fout, double* fnc, floa
     fnc[0] = (hp * VLd + hm * VRd) + ((hp * Smd) * gmL + (hm * Spd) * gmR);
     fnc[1] = hp * (VLd * p1L + Smd * (double)tL1) + hm * (VRd * p1R + Spd * (double)tR1);
     fnc[2] = hp * (VLd * p2L + Smd * (double)tL2) + hm * (VRd * p2R + Spd * (double)tR2);
+    }
     float kL = wL[2] * wL[2] + wL[3] * wL[3], kR = wR[2] * wR[2] + wR[3] * wR[3];
     if (DIM == 3) { kL += wL[4] * wL[4]; kR += wR[4] * wR[4]; }
     cmax = fmaxf(cL + sqrtf(kL), cR + sqrtf(kR));

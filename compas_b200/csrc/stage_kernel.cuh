@@ -289,10 +289,20 @@ struct TileShape {
     static constexpr int F0 = (TX + 1) * A0, F1 = (TY + 1) * A1, F2 = (TZ + 1) * A2;
     static constexpr int FMAX = (D == 3) ? (F0 > F1 ? (F0 > F2 ? F0 : F2) : (F1 > F2 ? F1 : F2)) : (F0 > F1 ? F0 : F1);
     static constexpr int NB = M::N + (PF ? M::NCPF : M::NC);
-    // primitives (type PT) of the tile and of one halo slab pair, then the face buffer (FP64)
-    static constexpr size_t PBYTES = sizeof(PT) * ((size_t)M::N * CELLS + (size_t)M::N * HALO);
+    static constexpr size_t FB = sizeof(double) * (size_t)NB * FMAX;  // face buffer (FP64)
+    // Halo slab sets resident at once: D (every direction's slabs converted with the tile in step 1,
+    // one barrier per direction fewer) where the primitives and the face buffer fit two CTAs per SM
+    // (112 KB each), else 1 (the slabs of each direction converted before its faces, into one set).
+    static constexpr size_t kTwoCtaBytes = 112 * 1024;
+    static constexpr size_t pbytes(int nhs) { return sizeof(PT) * (size_t)M::N * (size_t)(CELLS + nhs * HALO); }
+    static constexpr int NHS = (!TMA && (pbytes(D) + 15) / 16 * 16 + FB <= kTwoCtaBytes) ? D : 1;
+    // primitives (type PT): component n of tile cell l at n * CSTR + l, of halo set h, slot s, slab
+    // cell t at n * CSTR + CELLS + h * HALO + s * HS + t (one component stride for tile and halo, so
+    // the stencil loads of a face differ only by compile-time offsets); then the face buffer
+    static constexpr int CSTR = CELLS + NHS * HALO;
+    static constexpr size_t PBYTES = pbytes(NHS);
     static constexpr size_t FOFF = (PBYTES + 15) / 16 * 16;
-    static constexpr size_t FEND = FOFF + sizeof(double) * (size_t)NB * FMAX;
+    static constexpr size_t FEND = FOFF + FB;
     // TMA staging of one direction's two halo slabs (raw FP64 boxes of kTmaBoxX x 3 x T x N), placed
     // at the next 128-byte boundary of the (runtime) shared-memory address, hence the 128-byte slack
     static constexpr size_t SLAB = sizeof(double) * (size_t)kTmaBoxX * 3 * TX * M::N;
@@ -335,8 +345,9 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
     constexpr int R = (CELLS + NT - 1) / NT;
 
     PT* smem = reinterpret_cast<PT*>(smem_d);
-    PT* Pint = smem;
-    PT* Phal = Pint + N * CELLS;
+    PT* Pint = smem;             // tile cells: Pint[n * CSTR + l]
+    PT* Phal = smem + CELLS;     // halo sets: Phal[n * CSTR + h * HALO + slot * HS + t]
+    constexpr int CSTR = T::CSTR, NHS = T::NHS;
     double* Fb = reinterpret_cast<double*>(reinterpret_cast<char*>(smem_d) + T::FOFF);
 
     const Grid& g = a.g;
@@ -358,10 +369,35 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
     }
 
     // 1. tile cells and the x-direction halo slabs -> primitives, read as whole rows of TX + 6 cells
-    // (coalesced), the tile cells into Pint and the halo cells into the x slabs of Phal
+    // (coalesced), the tile cells into Pint and the halo cells into the x slabs of halo set 0; with
+    // NHS = D also the y (and z) halo slabs, into halo sets 1 (and 2), in the same loop
     constexpr int RX = TX + 6;
-    for (int l = tid; l < RX * TY * TZ; l += NT) {
-        const int lx = l % RX - 3, ly = (l / RX) % TY, lz = l / (RX * TY);
+    constexpr int ROWS = RX * TY * TZ;
+    constexpr int A0 = T::A0;
+    constexpr int ITEMS = ROWS + ((NHS == D) ? (D - 1) * 6 * A0 : 0);
+    for (int l = tid; l < ITEMS; l += NT) {
+        int lx, ly, lz, dst;
+        if (l < ROWS) {
+            lx = l % RX - 3;
+            ly = (l / RX) % TY;
+            lz = l / (RX * TY);
+            if (lx >= 0 && lx < TX) {
+                dst = lx + TX * (ly + TY * lz);
+            } else {
+                const int slot = (lx < 0) ? lx + 3 : lx - TX + 3;
+                dst = CELLS + slot * T::HS + (ly + TX * lz);
+            }
+        } else {
+            const int h = l - ROWS;
+            const int dd = 1 + h / (6 * A0);
+            const int hh = h - (dd - 1) * 6 * A0;
+            const int slot = hh / A0, t = hh % A0;
+            const int pos = (slot < 3) ? slot - 3 : TX + slot - 3;
+            const int ta = t % TX, tb = t / TX;
+            if (dd == 1) { lx = ta; ly = pos; lz = tb; }
+            else { lx = ta; ly = tb; lz = pos; }
+            dst = CELLS + dd * T::HALO + slot * T::HS + t;
+        }
         const int i = i0 + lx, j = j0 + ly, k = k0 + lz;
         double U[N];
         PT W[N];
@@ -373,17 +409,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
 #pragma unroll
             for (int n = 0; n < N; ++n) W[n] = 0;
         }
-        int dst;
-        if (lx >= 0 && lx < TX) {
-            dst = lx + TX * (ly + TY * lz);
-        } else {
-            const int slot = (lx < 0) ? lx + 3 : lx - TX + 3;
-            dst = N * CELLS + slot * T::HS + (ly + TX * lz);
-        }
-        PT* out = (dst < N * CELLS) ? Pint + dst : Phal + (dst - N * CELLS);
-        const int stride = (dst < N * CELLS) ? CELLS : HALO;
 #pragma unroll
-        for (int n = 0; n < N; ++n) out[n * stride] = W[n];
+        for (int n = 0; n < N; ++n) smem[n * CSTR + dst] = W[n];
     }
 
     double acc[R][NB];
@@ -398,11 +425,16 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
         // 2a. halo slabs of direction d -> primitives (the x slabs came with the rows of step 1)
         if constexpr (TMA) {
             if (d > 0) {
-                // the slabs were staged by TMA during the previous direction's faces (phase d - 1)
+                // the slabs were staged by TMA during the previous direction's faces (phase d - 1).
+                // A wait that runs out sets the status bit and waits once more (bounded) for the copy
+                // in flight; if that runs out too, the whole CTA leaves the tile without reading the
+                // staging buffer or writing any output (a timed-out tile leaves its cells unwritten)
+                bool lost = false;
                 if (!mbar_wait_bounded(&tma_bar, (unsigned)(d - 1), 1 << 20)) {
                     flag_error(err, COMPAS_B200_ERR_TIMEOUT);
-                    mbar_wait_bounded(&tma_bar, (unsigned)(d - 1), 1 << 20);
+                    lost = !mbar_wait_bounded(&tma_bar, (unsigned)(d - 1), 1 << 20);
                 }
+                if (__syncthreads_or(lost)) return;
                 const int offx = (i0 + g.ng) - ((i0 + g.ng - 1) & ~1);
                 for (int h = tid; h < 6 * Ad; h += NT) {
                     const int slot = h / Ad, t = h % Ad;
@@ -427,11 +459,12 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                         for (int n = 0; n < N; ++n) W[n] = 0;
                     }
 #pragma unroll
-                    for (int n = 0; n < N; ++n) Phal[n * HALO + slot * T::HS + t] = W[n];
+                    for (int n = 0; n < N; ++n) Phal[n * CSTR + slot * T::HS + t] = W[n];
                 }
             }
         }
-        for (int h = (d == 0 || TMA) ? 6 * Ad : tid; h < 6 * Ad; h += NT) {
+        // with one halo set, the slabs of d > 0 are converted here (d = 0 came with the rows of step 1)
+        for (int h = (d == 0 || TMA || NHS == D) ? 6 * Ad : tid; h < 6 * Ad; h += NT) {
             const int slot = h / Ad, t = h % Ad;
             const int pos = (slot < 3) ? slot - 3 : Td + slot - 3;
             const int ta = t % Ta, tb = t / Ta;
@@ -451,8 +484,10 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                 for (int n = 0; n < N; ++n) W[n] = 0;
             }
 #pragma unroll
-            for (int n = 0; n < N; ++n) Phal[n * HALO + slot * T::HS + t] = W[n];
+            for (int n = 0; n < N; ++n) Phal[n * CSTR + slot * T::HS + t] = W[n];
         }
+        // (also the barrier between the previous direction's divergence reads of the face buffer and
+        // this direction's face writes)
         __syncthreads();
 
         // 2b. faces of direction d. Tiles are cubes (squares in 2D) of side TS, so every direction has
@@ -507,7 +542,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                                (D == 2 || (d == 2 ? gk <= g.n[2] : gk < g.n[2]));
             if (!valid) continue;
             const int t = ta + TS * tb;
-            // shared-memory offset and component stride of the six stencil cells f-3 .. f+2
+            // shared-memory offset of the six stencil cells f-3 .. f+2 (component stride CSTR for all)
+            const int hset = (NHS == 1) ? 0 : d;
             int off[6], str[6];
 #pragma unroll
             for (int s = 0; s < 6; ++s) {
@@ -516,12 +552,11 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                     int lx = fx, ly = fy, lz = fz;
                     if (d == 0) lx = pos; else if (d == 1) ly = pos; else lz = pos;
                     off[s] = lx + TX * (ly + TY * lz);
-                    str[s] = CELLS;
                 } else {
                     const int slot = (pos < 0) ? pos + 3 : pos - TS + 3;
-                    off[s] = N * CELLS + slot * T::HS + t;
-                    str[s] = HALO;
+                    off[s] = CELLS + hset * HALO + slot * T::HS + t;
                 }
+                str[s] = CSTR;
             }
             double WfL[N], WfR[N], UL[N], UR[N];
             constexpr int NB0 = (SCHEME == 6) ? M::IM : 0;    // first plainly reconstructed component
@@ -737,7 +772,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                 // masses and volume fraction exactly from the conserved state (FP64); the pressures
                 // of the non-conservative terms from the FP32 tile
 #pragma unroll
-                for (int n = 0; n < N; ++n) W[n] = Pint[n * CELLS + l];
+                for (int n = 0; n < N; ++n) W[n] = Pint[n * CSTR + l];
                 if constexpr (NPH) {
 #pragma unroll
                     for (int k = 0; k < M::NP; ++k) {
@@ -751,7 +786,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                 }
             } else {
 #pragma unroll
-                for (int n = 0; n < N; ++n) W[n] = Pint[n * CELLS + l];
+                for (int n = 0; n < N; ++n) W[n] = Pint[n * CSTR + l];
             }
 #pragma unroll
             for (int n = 0; n < N; ++n) L[n] = -acc[r][n];

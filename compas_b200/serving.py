@@ -103,6 +103,14 @@ class Server:
         for b in self.batches.values():
             b.close()
 
+    def prepare(self, requests):
+        """Build every request's initial state on the device ahead of time (kept on the request), so
+        that run() measures admission, the solves and retirement, not the initial-condition
+        construction."""
+        for r in requests:
+            if getattr(r, "_case", None) is None:
+                r._case = make_case(r, self.precision)
+
     def run(self, requests, clock=None):
         import torch
 
@@ -117,7 +125,8 @@ class Server:
             # admit every arrived request that fits the budget, in arrival order
             while qi < len(pending) and pending[qi].arrival <= now:
                 r = pending[qi]
-                p, g, U = make_case(r, self.precision)
+                prebuilt = getattr(r, "_case", None)
+                p, g, U = prebuilt if prebuilt is not None else make_case(r, self.precision)
                 r.cells = _cells(r)
                 r.bytes = 3 * U.numel() * 8
                 if self.in_use + r.bytes > self.budget and any(active[k] for k in active):
@@ -126,6 +135,7 @@ class Server:
                 r.case_id = self.batches[r.kind].add(p, g, U, max_steps=r.steps)
                 r.admitted = clock() - t0
                 r._pg = (p, g)
+                r._case = None  # the batch holds its own copy
                 self.in_use += r.bytes
                 active[r.kind][r.case_id] = r
                 qi += 1
@@ -167,9 +177,11 @@ def summarize(done, wall_s):
             "mean_tts_s": float(tts.mean()), "cell_updates_per_s_per_stage": work / wall_s, "wall_s": wall_s}
 
 
-def sequential_service(requests, precision="fp64"):
+def sequential_service(requests, precision="fp64", sample_steps=None):
     """Service time of each request alone on a single-case level (device work, after one warm-up
-    step on a separate level), keyed by request id."""
+    step on a separate level), keyed by request id. With sample_steps, a request of more steps is
+    timed over its first sample_steps steps and the time scaled by steps / sample_steps (the cost of a
+    step of a fixed box does not depend on the step)."""
     import torch
 
     service = {}
@@ -181,10 +193,11 @@ def sequential_service(requests, precision="fp64"):
         torch.cuda.synchronize()
         lv2 = Level(p, g)
         lv2.upload(U)
+        k = r.steps if not sample_steps else min(r.steps, int(sample_steps))
         t0 = time.perf_counter()
-        lv2.advance(r.steps)
+        lv2.advance(k)
         lv2.sync()
-        service[r.rid] = time.perf_counter() - t0
+        service[r.rid] = (time.perf_counter() - t0) * (r.steps / k)
         lv.close()
         lv2.close()
     return service

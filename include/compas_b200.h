@@ -110,6 +110,9 @@ typedef struct compas_b200_parm {
      * a forced kernel (compas_b200_level_set_kernel) uses TMA; 0 always loads them with ordinary loads.
      * Same results either way. */
     int tma;
+    /* prob.EOS.cv_1, prob.EOS.cv_2 (default 1): the phases' heat capacities, used by the derived
+     * temperature of the refinement tagging (Conservative2Temperature) */
+    double cv_1, cv_2;
 } compas_b200_parm;
 
 /* One box covering a single-level domain (the valid cells), its ghost width and its boundary codes
@@ -172,6 +175,35 @@ int compas_b200_fill_boundary(const compas_b200_parm* p, const compas_b200_geom*
  * unsigned, may be NULL) is OR-ed with status bits. */
 int compas_b200_compute_dUdt(const compas_b200_parm* p, const compas_b200_geom* g, const double* U, double* dUdt,
                              double* cmax_dev, unsigned int* err_dev, void* stream);
+
+/* Number of non-conservative face terms of the model: 1 for FIVEEQS and FIVEEQS_NPHASE (the face
+ * velocity u*), 3 for SIXEQS (u, u a1p1, u a2p2) - NC_TERMS of include/Macros.H, the component
+ * count of the reference's fluxes_nc (source/Class_Compressible_PhaseField.cpp:3127-3143). */
+int compas_b200_nc_terms(const compas_b200_parm* p);
+
+#define COMPAS_B200_FACES_ALL 0       /* every face of the box */
+#define COMPAS_B200_FACES_BOUNDARY 1  /* the faces on the box boundary: face 0 and face n[d] along d */
+
+/* Face fluxes of one box, for the flux registers of a multi-level host. The fused kernels never
+ * write face fluxes; a host that keeps AMReX's FluxRegister gets them here, recomputed from the same
+ * ghost-filled stage state Us by the same device arithmetic as the stage kernel (FP64 form: the same
+ * bits as the fluxes the stage used). Replaces what ComputeFaceFluxes leaves in `fluxes` and
+ * `fluxes_nc` (source/Class_Compressible_PhaseField.cpp:3151-3301) for the flux registers; with
+ * area_scaled set the values are multiplied by the face area as ScaleFaceFluxesByArea does
+ * (:3433-3466: dy dz, dx dz, dx dy; dz = 1 in 2D), so the host calls CrseInit(flux[d], d, 0, 0, NSTATE,
+ * -dt_lev) and FineAdd(flux[d], d, 0, 0, NSTATE, dt_lev) (and the same on flux_nc with NC_TERMS) as
+ * compute_dUdt_FV does (:3501-3536).
+ *   which: COMPAS_B200_FACES_ALL (CrseInit on a coarse level: coarse-fine faces may lie inside the
+ *          box) or COMPAS_B200_FACES_BOUNDARY (FineAdd: only the box's own boundary faces are read),
+ *          so the fused path keeps its zero face traffic and the registers cost one face pass.
+ *   flux[d]: device face array of direction d, the layout of a face MultiFab with no ghosts
+ *          (surroundingNodes(d)): n[e] + (e == d) faces along each e, nstate components, x fastest;
+ *          flux_nc[d] likewise with compas_b200_nc_terms components. Either may be NULL (not
+ *          written); in BOUNDARY mode only the boundary faces of the arrays are written.
+ * The hyperbolic right-hand side without THINC (EUNSUPPORTED otherwise). */
+int compas_b200_face_fluxes(const compas_b200_parm* p, const compas_b200_geom* g, const double* Us, int which,
+                            int area_scaled, double* const flux[3], double* const flux_nc[3], unsigned int* err_dev,
+                            void* stream);
 
 /* One fused TVD-RK3 stage (stage 0, 1, 2) of ThirdOrderSSPRK
  * (source/Class_Compressible_PhaseField.cpp:3937-4107) followed by PostTimeStage (the SIXEQS
@@ -382,6 +414,44 @@ int compas_b200_amr_sync(compas_b200_amr* A, double* t, int* steps, unsigned int
 /* Level-0 step sizes taken so far (the first n). */
 int compas_b200_amr_dts(const compas_b200_amr* A, double* dts, int n);
 long long compas_b200_amr_launches(const compas_b200_amr* A);
+
+/* ---- refinement tagging (ErrorEst, source/COMPAS.cpp:767-932) ------------------------------------
+ * One criterion of one level, as ErrorEst applies it (include/Tagging.H): the variable is state
+ * component `var` (derived = 0; the names of the model's vnamesC) or derived variable `var`
+ * (derived = 1; the model's vnamesD: FIVEEQS a1rho1 a2rho2 rho_u rho_v rho_w rho_E a1 rho u v w P T c
+ * Mach vorticity_mag q_criterion lambda2; SIXEQS a1rho1 a2rho2 rho_u rho_v rho_w a1rho1E1 a2rho2E2 a1
+ * rho u v w P a1P1 a2P2 T c Mach vorticity_mag q_criterion lambda2), resolved from a name as the
+ * reference's VariableRegistry does (state names first). kind: GRAD (run.refine.<name>.grad of the
+ * level, v0), LESS (value_less, v0), GREATER (value_greater, v0), RANGE (value_range, v0 < x < v1). */
+#define COMPAS_B200_TAG_GRAD 0
+#define COMPAS_B200_TAG_LESS 1
+#define COMPAS_B200_TAG_GREATER 2
+#define COMPAS_B200_TAG_RANGE 3
+#define COMPAS_B200_MAX_TAG_CRITERIA 16
+typedef struct compas_b200_tag_criterion {
+    int var;
+    int derived;
+    int kind;
+    double v0, v1;
+} compas_b200_tag_criterion;
+
+/* Tags of the valid cells of one box: tags (device, n[0] x n[1] x n[2] bytes, x fastest) receive 1
+ * where any criterion holds and 0 elsewhere. U is the padded device state with its ghosts filled
+ * (two ghost layers where a velocity-gradient variable - vorticity_mag, q_criterion, lambda2 - is
+ * tagged by its gradient). criteria is a host array of at most COMPAS_B200_MAX_TAG_CRITERIA entries:
+ * the level's criteria (those whose run.refine.<name>.max_level exceeds the level). Replaces the
+ * tagging loop of COMPAS::ErrorEst for FIVEEQS and SIXEQS; the AMReX host keeps its TagBoxArray
+ * (copy the bytes into it) and its regrid. FIVEEQS_NPHASE: EUNSUPPORTED. */
+int compas_b200_tag_cells(const compas_b200_parm* p, const compas_b200_geom* g, const double* U,
+                          const compas_b200_tag_criterion* criteria, int ncriteria, unsigned char* tags,
+                          void* stream);
+
+/* ---- measurement -------------------------------------------------------------------------------
+ * (no counterpart in the reference) Sustained FMA throughput of the current GPU's FP32 (fp64 = 0)
+ * or FP64 (fp64 = 1) pipe, in floating-point operations per second (one FMA = 2): one warm-up and one
+ * timed launch of iters x 8 independent FMA chains per thread over every SM; synchronises the stream.
+ * The denominators of the stage kernels' compute roofline. */
+int compas_b200_fma_peak(int fp64, int iters, double* flops_per_s, void* stream);
 
 #ifdef __cplusplus
 }

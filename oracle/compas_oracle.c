@@ -1259,3 +1259,11 @@ int cmp_amr_advance(const cmp_case* c, int nlev, const cmp_amr_box* boxes, int n
     (void)c; (void)nlev; (void)boxes; (void)nbox; (void)U; (void)nsteps; (void)stop_time; (void)t; (void)dts;
     return -2;
 }
+
+/* Refinement tags: the reference-header build compiles the reference's own Tagging.H; the port does
+ * not restate them. */
+int cmp_tag(const cmp_case* c, const double* cv, const double* U, const cmp_tag_crit* crit, int ncrit,
+            unsigned char* tags) {
+    (void)c; (void)cv; (void)U; (void)crit; (void)ncrit; (void)tags;
+    return -2;
+}

@@ -73,7 +73,15 @@ _SIGS = {
                                       ctypes.POINTER(ctypes.c_double), _D]),
     "cmp_amr_advance": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
                                        ctypes.c_double, ctypes.POINTER(ctypes.c_double), _D]),
+    "cmp_tag": (ctypes.c_int, [_P, _D, _D, ctypes.c_void_p, ctypes.c_int, _D]),
 }
+
+
+class TagCrit(ctypes.Structure):
+    """ctypes mirror of ``cmp_tag_crit`` (oracle/oracle_api.h)."""
+
+    _fields_ = [("var", ctypes.c_int), ("derived", ctypes.c_int), ("kind", ctypes.c_int),
+                ("v0", ctypes.c_double), ("v1", ctypes.c_double)]
 
 
 class AmrBox(ctypes.Structure):
@@ -283,6 +291,22 @@ class Oracle:
         n = self._call(self.lib.cmp_amr_advance(self._c, nlev, arr, len(boxes), ptrs, nsteps, stop_time,
                                                 ctypes.byref(t), dts.ctypes.data))
         return t.value, dts[:n]
+
+    # ---- refinement tags (reference-header build only) ---------------------------------------------
+    def tag(self, U: np.ndarray, criteria, cv=(1.0, 1.0)) -> np.ndarray:
+        """ErrorEst tags (1/0) of the valid cells, shape (nz, ny, nx), of the ghost-filled padded U for
+        criteria given as (var, derived, kind, v0, v1) tuples."""
+        if self.kind != "reference":
+            raise RuntimeError("tagging is in the reference-header oracle only")
+        c = self.case
+        nz = c.n[2] if c.dim == 3 else 1
+        tags = np.zeros((nz, c.n[1], c.n[0]), dtype=np.uint8)
+        arr = (TagCrit * max(1, len(criteria)))(*[TagCrit(*t) for t in criteria])
+        cvv = np.array(cv, dtype=np.float64)
+        assert U.flags.c_contiguous and U.dtype == np.float64
+        self._call(self.lib.cmp_tag(self._c, cvv.ctypes.data, U.ctypes.data, ctypes.addressof(arr), len(criteria),
+                                    tags.ctypes.data))
+        return tags
 
     def threads(self) -> int:
         return int(self.lib.cmp_threads())

@@ -125,6 +125,24 @@ typedef struct cmp_amr_box {
 int cmp_amr_advance(const cmp_case* c, int nlev, const cmp_amr_box* boxes, int nbox, double** U, int nsteps,
                     double stop_time, double* t, double* dts);
 
+/* Refinement tags of one level (ErrorEst, source/COMPAS.cpp:767-932): for each criterion, the state
+ * component (derived 0) or the derived variable (derived 1, compute_derived_var of the model, into a
+ * scratch array over the valid cells grown by one) is tested with the reference's Tagging.H functions:
+ * kind 0 state_grad (threshold v0), 1 state_value_less (v0), 2 state_value_greater (v0), 3
+ * state_value_range (v0, v1). U is padded with its ghosts filled (two layers where a velocity-gradient
+ * variable is tagged by gradient); tags (valid cells, x fastest) receive 1 where tagged, 0 elsewhere.
+ * cv holds prob.EOS.cv_1, cv_2 (temperature). FIVEEQS and SIXEQS in the reference-header build; the
+ * plain-C port returns -2. */
+typedef struct cmp_tag_crit {
+    int var;
+    int derived;
+    int kind;
+    double v0, v1;
+} cmp_tag_crit;
+
+int cmp_tag(const cmp_case* c, const double* cv, const double* U, const cmp_tag_crit* crit, int ncrit,
+            unsigned char* tags);
+
 #ifdef __cplusplus
 }
 #endif

@@ -54,6 +54,11 @@
 #include <Operators_Compressible6Eq_PhaseField.H>
 #endif
 
+#if (PHYSICS == FIVEEQS || PHYSICS == SIXEQS)
+// ErrorEst's tests (include/Tagging.H); its ProblemICBC.H is the shim's empty stand-in
+#include <Tagging.H>
+#endif
+
 #include "oracle_api.h"
 
 #include <cstring>
@@ -1099,6 +1104,58 @@ int cmp_amr_advance(const cmp_case* c, int nlev, const cmp_amr_box* boxes, int n
     int taken = 0;
     int rc = guarded([&] { taken = amr_advance(c, nlev, boxes, nbox, U, nsteps, stop_time, t, dts); });
     return rc == 0 ? taken : rc;
+}
+
+// ErrorEst of one level (source/COMPAS.cpp:767-932) for the tagging criteria of that level, with the
+// reference's own Tagging.H tests and compute_derived_var; the Derived scratch array covers the
+// valid cells grown by one (ngrow = 1), as ErrorEst's.
+int cmp_tag(const cmp_case* c, const double* cv, const double* U, const cmp_tag_crit* crit, int ncrit,
+            unsigned char* tags) {
+#if (PHYSICS == FIVEEQS || PHYSICS == SIXEQS)
+    try {
+        Geo g(c);
+        Parm parm = make_parm(c);
+        parm.cv_1 = cv[0];
+        parm.cv_2 = cv[1];
+        auto st = g.view(const_cast<double*>(U), NSTATE);
+        amrex::Array4<amrex::Real const> stc(st);
+        std::vector<double> der((size_t)g.S, 0.0);
+        auto dv = g.view(der.data(), 1);
+        std::vector<char> tg((size_t)g.nx * g.ny * g.nz, 0);
+        amrex::Array4<char> tagfab(tg.data(), amrex::Dim3{0, 0, 0}, amrex::Dim3{g.nx, g.ny, g.nz}, 1);
+        const double dx = c->dx[0], dy = c->dx[1], dz = (AMREX_SPACEDIM == 3) ? c->dx[2] : 1.0;
+        const char tagval = 1;
+        const int gz1 = (AMREX_SPACEDIM == 3) ? 1 : 0;
+        for (int v = 0; v < ncrit; ++v) {
+            const cmp_tag_crit& cr = crit[v];
+            amrex::Array4<amrex::Real> varfab = st;
+            int comp = cr.var;
+            if (cr.derived) {
+                for (int k = -gz1; k < g.nz + gz1; ++k)
+                for (int j = -1; j < g.ny + 1; ++j)
+                for (int i = -1; i < g.nx + 1; ++i)
+                    compute_derived_var(i, j, k, cr.var, dx, dy, dz, dv, stc, parm);
+                varfab = dv;
+                comp = 0;
+            }
+            for (int k = 0; k < g.nz; ++k)
+            for (int j = 0; j < g.ny; ++j)
+            for (int i = 0; i < g.nx; ++i) {
+                if (cr.kind == 0) state_grad(i, j, k, comp, tagfab, varfab, cr.v0, tagval);
+                else if (cr.kind == 1) state_value_less(i, j, k, comp, tagfab, varfab, cr.v0, tagval);
+                else if (cr.kind == 2) state_value_greater(i, j, k, comp, tagfab, varfab, cr.v0, tagval);
+                else state_value_range(i, j, k, comp, tagfab, varfab, cr.v0, cr.v1, tagval);
+            }
+        }
+        for (size_t q = 0; q < tg.size(); ++q) tags[q] = (unsigned char)tg[q];
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+#else
+    (void)c; (void)cv; (void)U; (void)crit; (void)ncrit; (void)tags;
+    return -2;
+#endif
 }
 
 }  // extern "C"

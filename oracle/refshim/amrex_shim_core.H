@@ -92,6 +92,10 @@ template <class T, class... Ts>
 constexpr const T& max(const T& a, const T& b, const Ts&... c) { return max(max(a, b), c...); }
 template <class T>
 constexpr T Math_abs(T a) { return std::abs(a); }
+namespace Math {
+template <class T>
+constexpr T abs(T a) { return std::abs(a); }
+}  // namespace Math
 
 [[noreturn]] inline void Abort(const std::string& msg = "") { throw std::runtime_error(msg); }
 [[noreturn]] inline void Abort(const char* msg) { throw std::runtime_error(msg ? msg : ""); }

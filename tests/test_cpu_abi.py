@@ -95,3 +95,16 @@ def test_phase_field_formulation_key():
     with pytest.raises(cb.CompasError) as e:
         cb.make_parm(cb.FIVEEQS, 2, {"PhaseField.ID_Flux": 2})
     assert e.value.code == cb.EARG
+
+
+def test_nc_terms_and_face_shapes():
+    """NC_TERMS of include/Macros.H per model, and the face-array shapes of the flux-register entry
+    point (a face MultiFab without ghosts: one more face than cells along its direction)."""
+    assert cb.nc_terms(cb.make_parm(cb.FIVEEQS, 2, {})) == 1
+    assert cb.nc_terms(cb.make_parm(cb.SIXEQS, 3, {})) == 3
+    assert cb.nc_terms(cb.make_parm(cb.FIVEEQS_NPHASE, 2, {"prob.EOS.gamma": [1.4, 1.5, 1.6]})) == 1
+    p = cb.make_parm(cb.SIXEQS, 3, {})
+    g = cb.make_geom((5, 6, 7), (0.1, 0.1, 0.1))
+    assert cb.face_shape(p, g, 0, 8) == (8, 7, 6, 6)
+    assert cb.face_shape(p, g, 1, 3) == (3, 7, 7, 5)
+    assert cb.face_shape(p, g, 2, 8) == (8, 8, 6, 5)

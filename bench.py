@@ -179,13 +179,17 @@ def cpu_baseline(n, steps):
                       f"after one untimed step, OpenMP over {o.threads()} host threads, {el:.1f} s"}
 
 
-# Floating-point operations per cell and RK stage executed by the stage kernels of the 256^3
-# shock-droplet (SIXEQS 3D, WENO5 + HLLC + relaxation), from one ncu capture of each form on the
-# 128^3 case (smsp__sass_thread_inst_executed_op_{fadd,fmul,ffma,dadd,dmul,dfma}_pred_on.sum, an FMA
-# counted as 2, summed over the three RK stages and divided by 3 x the cells); the halo cells each
-# tile converts again and the relaxation's iterations are included, as executed.
-STAGE_FLOPS = {"mixed": None, "fp64": None}
-STAGE_FLOPS_SOURCE = "not measured yet"
+# Algorithmic floating-point operations per cell and RK stage of the 256^3 shock-droplet (SIXEQS 3D,
+# WENO5 + HLLC + relaxation), a static count of the formulas with each +, -, *, / and sqrt counted as
+# one operation (the per-function table is in DESIGN.md): per face 16 WENO5 calls (79 each), two
+# primitive-to-conservative conversions (30), the HLLC flux with its conversions, fluxes and sound
+# speeds (437); per cell three faces, one cell conversion (30), the divergence (88), the
+# non-conservative terms (14), the stage combination (32 on average) and the closed-form relaxation
+# (118). The mixed form does the WENO5 reconstruction, the wave speeds and the star ratios in FP32 and
+# the conversions, the upwind-side flux assembly, the divergence, the stage and the relaxation in FP64.
+STAGE_FLOPS = {"mixed": {"fp32": 4044, "fp64": 564}, "fp64": {"fp32": 0, "fp64": 5385}}
+STAGE_FLOPS_SOURCE = ("static count of the formulas per cell and RK stage, SIXEQS 3D WENO5+HLLC+relaxation, each "
+                      "+ - * / sqrt = 1 operation")
 
 
 def stage_kernel_times(cb, torch, p, g, lv, stream, cells, N):
@@ -233,6 +237,8 @@ def compute_roofline(name, mean_s, cells, fma_peaks):
         out["note"] = "FLOPs per cell-stage " + STAGE_FLOPS_SOURCE
         return out
     for k in ("fp32", "fp64"):
+        if not fl[k]:
+            continue
         ach = fl[k] * cells / mean_s
         out[k] = {"flops_per_cell_stage": fl[k], "achieved_tflops": ach / 1e12, "frac": ach / fma_peaks[k]}
     out["flops_source"] = STAGE_FLOPS_SOURCE

@@ -87,6 +87,7 @@ class Parm(ctypes.Structure):
         ("tma", ctypes.c_int),
         ("cv_1", ctypes.c_double),
         ("cv_2", ctypes.c_double),
+        ("amr_interp", ctypes.c_int),
     ]
 
 
@@ -116,6 +117,20 @@ _SIGS = {
     "compas_b200_compute_dUdt": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_void_p,
                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "compas_b200_nc_terms": (ctypes.c_int, [ctypes.POINTER(Parm)]),
+    "compas_b200_amr_nbox": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "compas_b200_amr_fill": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "compas_b200_thinc_face_values": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                     ctypes.c_longlong, ctypes.c_void_p, ctypes.c_void_p]),
+    "compas_b200_level_get_control": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                                     ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                                     ctypes.POINTER(ctypes.c_int)]),
+    "compas_b200_level_set_control": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                     ctypes.c_int, ctypes.c_void_p]),
+    "compas_b200_derive": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),
+    "compas_b200_amr_tag": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                           ctypes.c_void_p]),
+    "compas_b200_amr_regrid": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "compas_b200_tag_cells": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_void_p,
                                              ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),
     "compas_b200_fma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
@@ -399,6 +414,24 @@ def tag_cells(p: Parm, g: Geom, U, criteria, tags, stream=None) -> None:
                                        len(criteria), _ptr(tags), _stream_ptr(stream)))
 
 
+def thinc_face_values(beta, sigma, abar, side, out, stream=None) -> None:
+    """THINC face values of alpha1 (the stage kernels' device function) for device arrays of parameters
+    (float64 beta, sigma, abar; int32 side) into the float64 device array out."""
+    _check(lib().compas_b200_thinc_face_values(_ptr(beta), _ptr(sigma), _ptr(abar), _ptr(side), int(out.numel()),
+                                               _ptr(out), _stream_ptr(stream)))
+
+
+def derive(p: Parm, g: Geom, U, names, out, stream=None) -> None:
+    """Plot variables `names` (state or derived names of the model, resolved as tag_variable does) of
+    the valid cells of the ghost-filled padded device state U into the device array out, shape
+    (len(names), nz, ny, nx)."""
+    idx = [tag_variable(p.physics, p.dim, nm) for nm in names]
+    vars_ = (ctypes.c_int * max(1, len(idx)))(*[v for v, _ in idx])
+    der = (ctypes.c_int * max(1, len(idx)))(*[d for _, d in idx])
+    _check(lib().compas_b200_derive(ctypes.byref(p), ctypes.byref(g), _ptr(U), ctypes.addressof(vars_),
+                                    ctypes.addressof(der), len(idx), _ptr(out), _stream_ptr(stream)))
+
+
 FACES_ALL, FACES_BOUNDARY = 0, 1
 
 
@@ -551,6 +584,18 @@ class Level:
     def state_ptr(self) -> int:
         return int(lib().compas_b200_level_state(self._h))
 
+    def get_control(self) -> dict:
+        """Time, previous step size, the last step's largest face wave speed and the step count."""
+        t, dtp, cm, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        _check(lib().compas_b200_level_get_control(self._h, ctypes.byref(t), ctypes.byref(dtp), ctypes.byref(cm),
+                                                   ctypes.byref(n)))
+        return {"t": t.value, "dt_prev": dtp.value, "cmax": cm.value, "steps": n.value}
+
+    def set_control(self, t: float, dt_prev: float, cmax: float, steps: int, stream=None) -> None:
+        """Restore the step control of a checkpoint (the next advance continues the checkpointed run)."""
+        _check(lib().compas_b200_level_set_control(self._h, float(t), float(dt_prev), float(cmax), int(steps),
+                                                   _stream_ptr(stream)))
+
     def advance(self, nsteps: int, stop_time: float = 1.0e300, use_graph: bool = True, stream=None) -> None:
         _check(lib().compas_b200_level_advance(self._h, int(nsteps), float(stop_time), 1 if use_graph else 0,
                                                _stream_ptr(stream)))
@@ -660,6 +705,49 @@ class Amr:
 
     def advance(self, nsteps: int, stop_time: float = 1.0e300, stream=None) -> None:
         _check(lib().compas_b200_amr_advance(self._h, int(nsteps), float(stop_time), _stream_ptr(stream)))
+
+    def level_boxes(self, lev: int) -> list:
+        """Indices (in self.boxes) of the boxes of level lev, in the object's order."""
+        return [b for b, (l, _, _) in enumerate(self.boxes) if l == lev]
+
+    def tag(self, lev: int, criteria, stream=None) -> list:
+        """Refinement tags of level lev (ErrorEst): one uint8 array (nz, ny, nx) per box of the level, in
+        level_boxes order, computed on the device from the state resident there."""
+        import torch
+
+        ids = self.level_boxes(lev)
+        sizes = []
+        for b in ids:
+            _, lo, hi = self.boxes[b]
+            n = [hi[d] - lo[d] + 1 for d in range(3)]
+            sizes.append((n[2] if self.p.dim == 3 else 1, n[1], n[0]))
+        total = sum(int(np.prod(s)) for s in sizes)
+        tags = torch.zeros(max(total, 1), dtype=torch.uint8, device="cuda")
+        arr = (TagCriterion * max(1, len(criteria)))(*criteria)
+        _check(lib().compas_b200_amr_tag(self._h, int(lev), ctypes.addressof(arr), len(criteria), tags.data_ptr(),
+                                         _stream_ptr(stream)))
+        host = tags.cpu().numpy()
+        out, off = [], 0
+        for s in sizes:
+            m = int(np.prod(s))
+            out.append(host[off:off + m].reshape(s))
+            off += m
+        return out
+
+    def fill(self, lev: int, stream=None) -> None:
+        """Ghost cells of every box of level lev at its current time (the FillPatch of a stage)."""
+        _check(lib().compas_b200_amr_fill(self._h, int(lev), _stream_ptr(stream)))
+
+    def regrid(self, boxes, stream=None) -> None:
+        """Replace the boxes of levels >= 1 (level 0 unchanged), the state staying on the device."""
+        arr = (AmrBox * len(boxes))()
+        for b, (lev, lo, hi) in enumerate(boxes):
+            arr[b].lev = lev
+            for d in range(3):
+                arr[b].lo[d] = lo[d]
+                arr[b].hi[d] = hi[d]
+        _check(lib().compas_b200_amr_regrid(self._h, arr, len(boxes), _stream_ptr(stream)))
+        self.boxes = list(boxes)
 
     def sync(self, check: bool = True):
         t, s, st = ctypes.c_double(), ctypes.c_int(), ctypes.c_uint()

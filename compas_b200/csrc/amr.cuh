@@ -125,8 +125,10 @@ __device__ __forceinline__ double amr_coarse(const AmrBufs& B, int cb, long long
     return alpha * B.p[cb * 4 + kold][c * S + cq] + beta * B.p[cb * 4 + knew][c * S + cq];
 }
 
+// pc: amr.Interpolater = pc_interp (the parent's value, AMReX PCInterp); else lincc_interp as restated in the
+// file header
 __global__ void amr_interp_kernel(const AmrInterp* t, long long n, AmrBufs B, int dk, int knew, int kold, int mode,
-                                  double alpha, double beta, int N, int D) {
+                                  double alpha, double beta, int N, int D, int pc) {
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
         const AmrInterp& e = t[q];
         double* dst = B.p[e.db * 4 + dk];
@@ -138,7 +140,7 @@ __global__ void amr_interp_kernel(const AmrInterp* t, long long n, AmrBufs B, in
             };
             const double uc = val(0);
             double u = uc;
-            for (int d = 0; d < D; ++d) {
+            for (int d = 0; d < (pc ? 0 : D); ++d) {
                 const double um = val(1 + 2 * d), up = val(2 + 2 * d);
                 const double dc = 0.5 * (up - um), df = 2.0 * (up - uc), db = 2.0 * (uc - um);
                 double s = 0.0;

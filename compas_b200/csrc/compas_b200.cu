@@ -1009,6 +1009,14 @@ int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value
                 return 0;
             }
     }
+    if (k == "amr.Interpolater") {
+        // source/COMPAS.cpp:1217-1221
+        if (v == "lincc_interp") { p->amr_interp = 0; return 0; }
+        if (v == "pc_interp") { p->amr_interp = 1; return 0; }
+        if (v == "quartic_interp")
+            return fail(COMPAS_B200_EUNSUPPORTED, "amr.Interpolater = quartic_interp is not in this engine");
+        return bad("pc_interp, lincc_interp, quartic_interp");
+    }
     if (k == "run.timestep_change_limiter") { if (!parse_int(value, &ix)) return bad("0, 1"); p->change_limiter = ix ? 1 : 0; return 0; }
     return fail(COMPAS_B200_EARG, "unknown inputs key '" + k + "'");
 }
@@ -2086,6 +2094,101 @@ int compas_b200_tag_cells(const compas_b200_parm* p, const compas_b200_geom* g, 
         if (p->dim == 2) tag_kernel<FiveEq<2>><<<blocks, 256, 0, st>>>(a);
         else tag_kernel<FiveEq<3>><<<blocks, 256, 0, st>>>(a);
     }
+    CUDA_TRY(cudaGetLastError());
+    return COMPAS_B200_OK;
+}
+
+int compas_b200_derive(const compas_b200_parm* p, const compas_b200_geom* g, const double* U, const int* vars,
+                       const int* derived, int nvars, double* out, void* stream) {
+    using namespace compas;
+    int rc = check_args(p, g);
+    if (rc) return rc;
+    if (!U || !out || (nvars > 0 && (!vars || !derived))) return fail(COMPAS_B200_EARG, "null argument");
+    if (nvars < 0 || nvars > kMaxDerive) return fail(COMPAS_B200_EARG, "between 0 and 32 variables");
+    if (p->physics == COMPAS_B200_FIVEEQS_NPHASE)
+        return fail(COMPAS_B200_EUNSUPPORTED, "derived variables: FIVEEQS and SIXEQS");
+    if (g->ng < 2) return fail(COMPAS_B200_EARG, "derived variables need two ghost cells");
+    const int nderived = (p->physics == COMPAS_B200_SIXEQS) ? 21 : 18;
+    DeriveArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.t.U = U;
+    a.t.g = make_grid(p, g);
+    a.t.e = make_eos(p);
+    a.t.cv1 = p->cv_1;
+    a.t.cv2 = p->cv_2;
+    a.nv = nvars;
+    a.out = out;
+    for (int v = 0; v < nvars; ++v) {
+        if (vars[v] < 0 || vars[v] >= (derived[v] ? nderived : nstate(p)))
+            return fail(COMPAS_B200_EARG, "derived variable index out of range");
+        a.var[v] = vars[v];
+        a.derived[v] = derived[v] ? 1 : 0;
+    }
+    const long long n = (long long)a.t.g.n[0] * a.t.g.n[1] * a.t.g.n[2];
+    const unsigned blocks = (unsigned)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148LL * 32));
+    cudaStream_t st = (cudaStream_t)stream;
+    if (p->physics == COMPAS_B200_SIXEQS) {
+        if (p->dim == 2) derive_kernel<SixEq<2>><<<blocks, 256, 0, st>>>(a);
+        else derive_kernel<SixEq<3>><<<blocks, 256, 0, st>>>(a);
+    } else {
+        if (p->dim == 2) derive_kernel<FiveEq<2>><<<blocks, 256, 0, st>>>(a);
+        else derive_kernel<FiveEq<3>><<<blocks, 256, 0, st>>>(a);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return COMPAS_B200_OK;
+}
+
+// ---- step control of a level, for checkpoint and restart ----------------------------------------
+__global__ void set_control_kernel(StepCtl* s, double t, double dt_prev, unsigned long long cmax, int steps) {
+    s->t = t;
+    s->dt = 0.0;
+    s->dt_prev = dt_prev;
+    s->cmax = cmax;
+    s->steps = steps;
+    s->err = 0u;
+    s->done = 0;
+}
+
+int compas_b200_level_get_control(compas_b200_level* lv, double* t, double* dt_prev, double* cmax, int* steps) {
+    if (!lv) return fail(COMPAS_B200_EARG, "null level");
+    CUDA_TRY(cudaDeviceSynchronize());
+    StepCtl h;
+    CUDA_TRY(cudaMemcpy(&h, lv->ctl, sizeof(h), cudaMemcpyDeviceToHost));
+    if (t) *t = h.t;
+    if (dt_prev) *dt_prev = h.dt_prev;
+    if (cmax) std::memcpy(cmax, &h.cmax, sizeof(double));
+    if (steps) *steps = h.steps;
+    return COMPAS_B200_OK;
+}
+
+int compas_b200_level_set_control(compas_b200_level* lv, double t, double dt_prev, double cmax, int steps,
+                                  void* stream) {
+    if (!lv) return fail(COMPAS_B200_EARG, "null level");
+    if (!(cmax >= 0.0) || steps < 0) return fail(COMPAS_B200_EARG, "cmax must be >= 0 and steps >= 0");
+    unsigned long long bits;
+    std::memcpy(&bits, &cmax, sizeof(bits));
+    set_control_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(lv->ctl, t, dt_prev, bits, steps);
+    CUDA_TRY(cudaGetLastError());
+    lv->need_init = false;  // the next step's dt comes from the restored c_max, as in the run checkpointed
+    return COMPAS_B200_OK;
+}
+
+// ---- THINC face values, for the per-face comparison with the reference's host function -------------
+namespace compas {
+__global__ void thinc_face_kernel(const double* beta, const double* sigma, const double* abar, const int* side,
+                                  long long n, double* out) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        out[t] = thinc_alpha_face(beta[t], sigma[t], abar[t], side[t]);
+}
+}  // namespace compas
+
+int compas_b200_thinc_face_values(const double* beta, const double* sigma, const double* abar, const int* side,
+                                  long long n, double* out, void* stream) {
+    using namespace compas;
+    if (n < 0 || (n > 0 && (!beta || !sigma || !abar || !side || !out))) return fail(COMPAS_B200_EARG, "null argument");
+    if (n == 0) return COMPAS_B200_OK;
+    const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 32);
+    thinc_face_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(beta, sigma, abar, side, n, out);
     CUDA_TRY(cudaGetLastError());
     return COMPAS_B200_OK;
 }

@@ -225,3 +225,30 @@ __global__ void tag_kernel(TagArgs A) {
 }
 
 }  // namespace compas
+
+namespace compas {
+
+// Derived variables of the valid cells (the plot variables of the reference's PlotFileMF, computed
+// by compute_derived_var): out[v * cells + t] for variable v and valid cell t (x fastest).
+constexpr int kMaxDerive = 32;
+struct DeriveArgs {
+    TagArgs t;  // state, grid, EOS and heat capacities (no criteria)
+    int nv;
+    int var[kMaxDerive];
+    int derived[kMaxDerive];
+    double* out;
+};
+
+template <class M>
+__global__ void derive_kernel(DeriveArgs A) {
+    const Grid& g = A.t.g;
+    const long long n = (long long)g.n[0] * g.n[1] * g.n[2];
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % g.n[0]);
+        const int j = (int)((t / g.n[0]) % g.n[1]);
+        const int k = (int)(t / ((long long)g.n[0] * g.n[1]));
+        for (int v = 0; v < A.nv; ++v) A.out[v * n + t] = tag_value<M>(A.t, A.var[v], A.derived[v], i, j, k);
+    }
+}
+
+}  // namespace compas

@@ -113,6 +113,9 @@ typedef struct compas_b200_parm {
     /* prob.EOS.cv_1, prob.EOS.cv_2 (default 1): the phases' heat capacities, used by the derived
      * temperature of the refinement tagging (Conservative2Temperature) */
     double cv_1, cv_2;
+    /* amr.Interpolater of the multi-level object's coarse-fine ghost cells and new fine cells
+     * (source/COMPAS.cpp:1217-1221, :1611-1618): 0 lincc_interp (default), 1 pc_interp */
+    int amr_interp;
 } compas_b200_parm;
 
 /* One box covering a single-level domain (the valid cells), its ghost width and its boundary codes
@@ -414,6 +417,31 @@ int compas_b200_amr_sync(compas_b200_amr* A, double* t, int* steps, unsigned int
 /* Level-0 step sizes taken so far (the first n). */
 int compas_b200_amr_dts(const compas_b200_amr* A, double* dts, int n);
 long long compas_b200_amr_launches(const compas_b200_amr* A);
+/* Number of boxes of level lev. */
+int compas_b200_amr_nbox(const compas_b200_amr* A, int lev);
+/* Ghost cells of every box of level lev at its current time (same-level copies, coarse-fine
+ * interpolation, physical boundaries: the FillPatch of a stage), so that compas_b200_amr_download
+ * returns ghost-filled arrays (for plot variables that read neighbours). */
+int compas_b200_amr_fill(compas_b200_amr* A, int lev, void* stream);
+/* New box list for levels 1 .. nlev-1 (the regrid that follows ErrorEst; level 0 must be listed
+ * unchanged, every level keeps at least one box, nesting as for compas_b200_amr_create). The state
+ * stays on the device: a new box takes its valid cells from the old boxes of its level where they
+ * overlap and elsewhere from the cell-conservative linear interpolation of the new coarser level
+ * (the same interpolation as the coarse-fine ghost cells); time, step count and step sizes carry
+ * over. Call between steps; synchronises the stream; A keeps its handle, box indices are the new
+ * list's. */
+int compas_b200_amr_regrid(compas_b200_amr* A, const compas_b200_amr_box* boxes, int nbox, void* stream);
+
+/* Step control of a level, for checkpoint and restart: its time, the previous step size (COMPAS
+ * dt[lev], the 1.1x change limiter's reference), the largest face wave speed of the last step's
+ * stages (the next ComputeDt's input) and the step count. get synchronises the device. After set,
+ * the next advance continues exactly as the checkpointed run would have (no initial wave-speed pass):
+ * a restart from compas_b200_level_set_state + set_control reproduces the uninterrupted run to the
+ * bit. Replaces the time-control part of COMPAS's WriteCheckpointFile / ReadCheckpointFile
+ * (source/COMPAS.cpp:2514-2748). */
+int compas_b200_level_get_control(compas_b200_level* lv, double* t, double* dt_prev, double* cmax, int* steps);
+int compas_b200_level_set_control(compas_b200_level* lv, double t, double dt_prev, double cmax, int steps,
+                                  void* stream);
 
 /* ---- refinement tagging (ErrorEst, source/COMPAS.cpp:767-932) ------------------------------------
  * One criterion of one level, as ErrorEst applies it (include/Tagging.H): the variable is state
@@ -445,6 +473,30 @@ typedef struct compas_b200_tag_criterion {
 int compas_b200_tag_cells(const compas_b200_parm* p, const compas_b200_geom* g, const double* U,
                           const compas_b200_tag_criterion* criteria, int ncriteria, unsigned char* tags,
                           void* stream);
+
+/* Refinement tags of level lev at its current time (ErrorEst, source/COMPAS.cpp:767-932): the
+ * level's ghost cells are filled as for a stage, then every box is tagged as compas_b200_tag_cells
+ * does; tags (device) receives the valid cells of the level's boxes one after the other, in box order,
+ * x fastest within a box. */
+int compas_b200_amr_tag(compas_b200_amr* A, int lev, const compas_b200_tag_criterion* criteria, int ncriteria,
+                        unsigned char* tags, void* stream);
+
+/* Derived variables of the valid cells of one box, for plot files (PlotFileMF with
+ * compute_derived_var, source/COMPAS.cpp:2483-2511): variable v is state component vars[v]
+ * (derived[v] = 0) or the model's derived variable vars[v] (derived[v] = 1, the vnamesD list above);
+ * out (device) receives n[0] x n[1] x n[2] doubles per variable, variable-major, x fastest. U is the
+ * padded state with its ghosts filled (velocity-gradient variables read the neighbours). At most 32
+ * variables; FIVEEQS and SIXEQS. */
+int compas_b200_derive(const compas_b200_parm* p, const compas_b200_geom* g, const double* U, const int* vars,
+                       const int* derived, int nvars, double* out, void* stream);
+
+/* (check entry point) The THINC face value of alpha1 the stage kernels use (the tanh profile of
+ * include/Operators_FV/Reconstruction2Face_THINC_D.H:13-35: steepness beta, sign sigma, cell mean
+ * abar, side 1 the cell's high face, 0 its low face) for n parameter sets in device arrays; it calls
+ * CUDA's exp, log and tanh where the reference's host build calls the C library's, so the two can
+ * differ in the last bits - this entry point lets a test measure that difference face by face. */
+int compas_b200_thinc_face_values(const double* beta, const double* sigma, const double* abar, const int* side,
+                                  long long n, double* out, void* stream);
 
 /* ---- measurement -------------------------------------------------------------------------------
  * (no counterpart in the reference) Sustained FMA throughput of the current GPU's FP32 (fp64 = 0)

@@ -1267,3 +1267,15 @@ int cmp_tag(const cmp_case* c, const double* cv, const double* U, const cmp_tag_
     (void)c; (void)cv; (void)U; (void)crit; (void)ncrit; (void)tags;
     return -2;
 }
+
+int cmp_derive(const cmp_case* c, const double* cv, const double* U, const int* vars, const int* derived, int nvars,
+               double* out) {
+    (void)c; (void)cv; (void)U; (void)vars; (void)derived; (void)nvars; (void)out;
+    return -2;
+}
+
+int cmp_thinc_face(const double* beta, const double* sigma, const double* abar, const int* side, long long n,
+                   double* out) {
+    (void)beta; (void)sigma; (void)abar; (void)side; (void)n; (void)out;
+    return -2;
+}

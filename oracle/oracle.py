@@ -53,6 +53,7 @@ class Case(ctypes.Structure):
         ("nphase", ctypes.c_int),
         ("Ak", ctypes.c_double * 4), ("Bk", ctypes.c_double * 4),
         ("Ck", ctypes.c_double * 4), ("Dk", ctypes.c_double * 4),
+        ("amr_interp", ctypes.c_int),
     ]
 
 
@@ -75,6 +76,23 @@ _SIGS = {
                                        ctypes.c_double, ctypes.POINTER(ctypes.c_double), _D]),
     "cmp_tag": (ctypes.c_int, [_P, _D, _D, ctypes.c_void_p, ctypes.c_int, _D]),
 }
+# bound where the library has them (a library built before they existed still loads)
+_OPTIONAL_SIGS = {
+    "cmp_derive": (ctypes.c_int, [_P, _D, _D, _D, _D, ctypes.c_int, _D]),
+    "cmp_thinc_face": (ctypes.c_int, [_D, _D, _D, _D, ctypes.c_longlong, _D]),
+}
+
+
+def thinc_face_values(beta, sigma, abar, side, physics=SIXEQS, dim=3) -> np.ndarray:
+    """The reference's THINC face value (reference-header build) for numpy parameter arrays."""
+    lib = load("reference", physics, dim)
+    b, s, a = (np.ascontiguousarray(x, dtype=np.float64) for x in (beta, sigma, abar))
+    sd = np.ascontiguousarray(side, dtype=np.int32)
+    out = np.zeros(b.size)
+    rc = lib.cmp_thinc_face(b.ctypes.data, s.ctypes.data, a.ctypes.data, sd.ctypes.data, b.size, out.ctypes.data)
+    if rc < 0:
+        raise RuntimeError("cmp_thinc_face failed")
+    return out
 
 
 class TagCrit(ctypes.Structure):
@@ -145,6 +163,11 @@ def load(kind: str, physics: int, dim: int, nphase: int = 2) -> ctypes.CDLL:
             f = getattr(h, name)
             f.restype = res
             f.argtypes = args
+        for name, (res, args) in _OPTIONAL_SIGS.items():
+            if hasattr(h, name):
+                f = getattr(h, name)
+                f.restype = res
+                f.argtypes = args
         _cache[path] = h
     return _cache[path]
 
@@ -166,6 +189,7 @@ def case_from(parm, geom) -> Case:
               "thinc_normal_threshold", "cfl", "change_limiter"):
         setattr(c, k, getattr(parm, k))
     c.nphase = getattr(parm, "nphase", 2)
+    c.amr_interp = getattr(parm, "amr_interp", 0)
     if parm.physics == FIVEEQS_NPHASE:
         for k in range(4):
             c.Ak[k], c.Bk[k], c.Ck[k], c.Dk[k] = parm.Ak[k], parm.Bk[k], parm.Ck[k], parm.Dk[k]
@@ -307,6 +331,21 @@ class Oracle:
         self._call(self.lib.cmp_tag(self._c, cvv.ctypes.data, U.ctypes.data, ctypes.addressof(arr), len(criteria),
                                     tags.ctypes.data))
         return tags
+
+    def derive(self, U: np.ndarray, vars_derived, cv=(1.0, 1.0)) -> np.ndarray:
+        """Plot variables (var, derived) of the valid cells of the ghost-filled padded U, shape
+        (nvars, nz, ny, nx) (reference-header build only)."""
+        if self.kind != "reference":
+            raise RuntimeError("derived variables are in the reference-header oracle only")
+        c = self.case
+        nz = c.n[2] if c.dim == 3 else 1
+        out = np.zeros((len(vars_derived), nz, c.n[1], c.n[0]))
+        v = np.array([x for x, _ in vars_derived] or [0], dtype=np.int32)
+        dflag = np.array([y for _, y in vars_derived] or [0], dtype=np.int32)
+        cvv = np.array(cv, dtype=np.float64)
+        self._call(self.lib.cmp_derive(self._c, cvv.ctypes.data, U.ctypes.data, v.ctypes.data, dflag.ctypes.data,
+                                       len(vars_derived), out.ctypes.data))
+        return out
 
     def threads(self) -> int:
         return int(self.lib.cmp_threads())

@@ -43,6 +43,7 @@ typedef struct cmp_case {
     int change_limiter; /* run.timestep_change_limiter */
     int nphase;         /* FIVEEQS_NPHASE (55501): phases (the build's NPHASE); 2 otherwise */
     double Ak[4], Bk[4], Ck[4], Dk[4];  /* FIVEEQS_NPHASE EOS coefficients per phase (source/Parm.cpp:185-253) */
+    int amr_interp;     /* amr.Interpolater of the multi-level advance: 0 lincc_interp, 1 pc_interp */
 } cmp_case;
 
 /* Number of conserved components of the case (NSTATE). */
@@ -142,6 +143,18 @@ typedef struct cmp_tag_crit {
 
 int cmp_tag(const cmp_case* c, const double* cv, const double* U, const cmp_tag_crit* crit, int ncrit,
             unsigned char* tags);
+
+/* Plot variables of the valid cells: variable v is state component vars[v] (derived[v] = 0) or the
+ * model's derived variable vars[v] (compute_derived_var, derived[v] = 1); out receives nvars x cells
+ * doubles, variable-major, x fastest. U is padded with its ghosts filled. FIVEEQS and SIXEQS in the
+ * reference-header build; the plain-C port returns -2. */
+int cmp_derive(const cmp_case* c, const double* cv, const double* U, const int* vars, const int* derived, int nvars,
+               double* out);
+
+/* The reference's THINC face value (Reconstruction2Face_THINC_D, include/Operators_FV/
+ * Reconstruction2Face_THINC_D.H:13-35) for n parameter sets. Reference-header build; the port returns -2. */
+int cmp_thinc_face(const double* beta, const double* sigma, const double* abar, const int* side, long long n,
+                   double* out);
 
 #ifdef __cplusplus
 }

@@ -72,4 +72,5 @@ def reference_case(physics: int, dim: int, inputs: dict, geom: dict) -> Case:
     c.cfl = float(g("run.cfl", 0.4))
     c.change_limiter = 1 if int(g("run.timestep_change_limiter", 1)) else 0
     c.nphase = 2
+    c.amr_interp = {"lincc_interp": 0, "pc_interp": 1}[str(g("amr.Interpolater", "lincc_interp"))]
     return c

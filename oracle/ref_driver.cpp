@@ -1158,4 +1158,49 @@ int cmp_tag(const cmp_case* c, const double* cv, const double* U, const cmp_tag_
 #endif
 }
 
+// Plot variables (PlotFileMF with compute_derived_var, source/COMPAS.cpp:2483-2511) of the valid cells.
+int cmp_derive(const cmp_case* c, const double* cv, const double* U, const int* vars, const int* derived, int nvars,
+               double* out) {
+#if (PHYSICS == FIVEEQS || PHYSICS == SIXEQS)
+    try {
+        Geo g(c);
+        Parm parm = make_parm(c);
+        parm.cv_1 = cv[0];
+        parm.cv_2 = cv[1];
+        auto st = g.view(const_cast<double*>(U), NSTATE);
+        amrex::Array4<amrex::Real const> stc(st);
+        std::vector<double> one((size_t)g.S, 0.0);
+        auto ov = g.view(one.data(), 1);
+        const double dx = c->dx[0], dy = c->dx[1], dz = (AMREX_SPACEDIM == 3) ? c->dx[2] : 1.0;
+        const long long cells = (long long)g.nx * g.ny * g.nz;
+        for (int v = 0; v < nvars; ++v)
+            for (int k = 0; k < g.nz; ++k)
+                for (int j = 0; j < g.ny; ++j)
+                    for (int i = 0; i < g.nx; ++i) {
+                        const long long t = ((long long)k * g.ny + j) * g.nx + i;
+                        double val;
+                        if (derived[v]) {
+                            compute_derived_var(i, j, k, vars[v], dx, dy, dz, ov, stc, parm);
+                            val = ov(i, j, k, 0);
+                        } else {
+                            val = st(i, j, k, vars[v]);
+                        }
+                        out[v * cells + t] = val;
+                    }
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+#else
+    (void)c; (void)cv; (void)U; (void)vars; (void)derived; (void)nvars; (void)out;
+    return -2;
+#endif
+}
+
+int cmp_thinc_face(const double* beta, const double* sigma, const double* abar, const int* side, long long n,
+                   double* out) {
+    for (long long t = 0; t < n; ++t) out[t] = Reconstruction2Face_THINC_D(beta[t], sigma[t], abar[t], side[t]);
+    return 0;
+}
+
 }  // extern "C"

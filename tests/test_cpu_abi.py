@@ -108,3 +108,15 @@ def test_nc_terms_and_face_shapes():
     assert cb.face_shape(p, g, 0, 8) == (8, 7, 6, 6)
     assert cb.face_shape(p, g, 1, 3) == (3, 7, 7, 5)
     assert cb.face_shape(p, g, 2, 8) == (8, 8, 6, 5)
+
+
+def test_amr_interpolater_key():
+    """amr.Interpolater: lincc_interp (default) and pc_interp; quartic_interp is refused, an unknown value
+    is an error naming the valid ones (source/COMPAS.cpp:1217-1221)."""
+    assert cb.make_parm(cb.FIVEEQS, 2, {}).amr_interp == 0
+    assert cb.make_parm(cb.FIVEEQS, 2, {"amr.Interpolater": "pc_interp"}).amr_interp == 1
+    with pytest.raises(cb.CompasError) as e:
+        cb.make_parm(cb.FIVEEQS, 2, {"amr.Interpolater": "cubic"})
+    assert "pc_interp, lincc_interp, quartic_interp" in str(e.value)
+    with pytest.raises(cb.CompasError):
+        cb.make_parm(cb.FIVEEQS, 2, {"amr.Interpolater": "quartic_interp"})

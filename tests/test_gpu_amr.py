@@ -171,11 +171,16 @@ def test_amr_mixed_error_vs_fp64(args):
      {"FiniteVolume.Scheme": "WENO3B"}),
     (cases.triple_point, dict(m=8), (56, 24), [((16, 12, 0), (47, 35, 0))], 16, 4,
      {"FiniteVolume.Scheme": "WENO3B"}),
+    (cases.shock_bubble, dict(nx=64, ny=32, scheme="WENO5B"), (64, 32),
+     [((40, 16, 0), (95, 47, 0)), ((96, 48, 0), (175, 79, 0))], 32, 4, {"amr.Interpolater": "pc_interp"}),
+    (cases.shock_droplet, dict(n=16), (16, 16, 16), [((8, 8, 8), (23, 23, 23))], 8, 3,
+     {"amr.Interpolater": "pc_interp"}),
 ], ids=["triple_muscl_mc_3lev", "triple_weno5_2lev", "bubble_muscl_mc", "bubble_hll", "droplet_weno3_llf",
-        "bubble_weno3b", "triple_weno3b"])
+        "bubble_weno3b", "triple_weno3b", "bubble3lev_pc_interp", "droplet2lev_pc_interp"])
 def test_amr_schemes_and_nphase_match_oracle(case_fn, kw, domain, regions, mgs, steps, extra):
     """The multi-level advance with the N-phase model (the triple point, as the reference's example runs
-    it: MUSCL-MC on a hierarchy), the three-cell schemes and the LLF / HLL Riemann solvers, to the bit."""
+    it: MUSCL-MC on a hierarchy), the three-cell schemes, the LLF / HLL Riemann solvers and the
+    piecewise-constant coarse-fine interpolation (amr.Interpolater = pc_interp), to the bit."""
     p, g, dim, boxes, states, got, dts, info, launches = _run(case_fn, kw, domain, regions, mgs, steps, extra)
     assert info.status == 0 and info.steps == steps
     _compare(p, g, dim, boxes, states, got, dts, steps)

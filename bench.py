@@ -145,9 +145,9 @@ def measured_peaks():
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the mixed stage kernel, from
 # one ncu capture of the 128^3 shock-droplet (three launches, one per RK stage, averaged) scaled by the
 # 8x cells of a 256^3 launch; a measured constant, not recomputed by this run.
-STAGE_TRAFFIC_BYTES = 2.90e9
-STAGE_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, mixed stage kernel, 128^3 shock-droplet "
-                        "(mean of the three RK stages), x8 for 256^3")
+STAGE_TRAFFIC_BYTES = 2.99e9
+STAGE_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, mixed stage kernel (TMA form, NT 288), "
+                        "128^3 shock-droplet, mean of the three RK stages (373.7 MB), x8 for 256^3")
 
 
 def _reference_oracle(n):
@@ -190,6 +190,13 @@ def cpu_baseline(n, steps):
 STAGE_FLOPS = {"mixed": {"fp32": 4044, "fp64": 564}, "fp64": {"fp32": 0, "fp64": 5385}}
 STAGE_FLOPS_SOURCE = ("static count of the formulas per cell and RK stage, SIXEQS 3D WENO5+HLLC+relaxation, each "
                       "+ - * / sqrt = 1 operation")
+# Executed floating-point operations per cell and RK stage, from ncu's SASS operation counters
+# (smsp__sass_thread_inst_executed_op_{f,d}{add,mul,fma}_pred_on.sum, FMA = 2) of the 128^3 capture of
+# each form's stage kernel, mean of the three RK stages. They exceed the static counts by the
+# instruction sequences of the divisions and square roots (reciprocal refinement, range checks).
+STAGE_FLOPS_EXECUTED = {"mixed": {"fp32": 3502, "fp64": 1104}, "fp64": {"fp32": 955, "fp64": 17342}}
+STAGE_FLOPS_EXECUTED_SOURCE = ("ncu SASS operation counters (add, mul, fma x2) of the 128^3 stage-kernel capture, "
+                               "mean of the three RK stages")
 
 
 def stage_kernel_times(cb, torch, p, g, lv, stream, cells, N):
@@ -236,12 +243,18 @@ def compute_roofline(name, mean_s, cells, fma_peaks):
     if fl is None:
         out["note"] = "FLOPs per cell-stage " + STAGE_FLOPS_SOURCE
         return out
+    ex = STAGE_FLOPS_EXECUTED.get(name, {})
     for k in ("fp32", "fp64"):
-        if not fl[k]:
+        if not fl[k] and not ex.get(k):
             continue
         ach = fl[k] * cells / mean_s
         out[k] = {"flops_per_cell_stage": fl[k], "achieved_tflops": ach / 1e12, "frac": ach / fma_peaks[k]}
+        if ex.get(k):
+            ache = ex[k] * cells / mean_s
+            out[k].update({"executed_flops_per_cell_stage": ex[k], "executed_tflops": ache / 1e12,
+                           "executed_frac": ache / fma_peaks[k]})
     out["flops_source"] = STAGE_FLOPS_SOURCE
+    out["executed_source"] = STAGE_FLOPS_EXECUTED_SOURCE
     return out
 
 

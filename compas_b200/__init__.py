@@ -25,7 +25,7 @@ MAX_PHASES = 4
 
 OK = 0
 EARG, ECUDA, ENOMEM, ESTATE, EUNSUPPORTED = -1, -2, -3, -4, -5
-ERR_NAN, ERR_COVOLUME, ERR_RELAX_NOROOT, ERR_CFL, ERR_TIMEOUT = 0x1, 0x2, 0x4, 0x8, 0x10
+ERR_NAN, ERR_COVOLUME, ERR_RELAX_NOROOT, ERR_CFL, ERR_TIMEOUT, ERR_BOUND = 0x1, 0x2, 0x4, 0x8, 0x10, 0x20
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libcompas_b200.so")
@@ -88,6 +88,8 @@ class Parm(ctypes.Structure):
         ("cv_1", ctypes.c_double),
         ("cv_2", ctypes.c_double),
         ("amr_interp", ctypes.c_int),
+        ("id_bound", ctypes.c_int),
+        ("id_lambda", ctypes.c_int),
     ]
 
 
@@ -117,6 +119,9 @@ _SIGS = {
     "compas_b200_compute_dUdt": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_void_p,
                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "compas_b200_nc_terms": (ctypes.c_int, [ctypes.POINTER(Parm)]),
+    "compas_b200_energy_bound_min": (ctypes.c_int, [ctypes.POINTER(Parm), ctypes.POINTER(Geom), ctypes.c_void_p,
+                                                    ctypes.c_void_p, ctypes.c_void_p]),
+    "compas_b200_level_bound_restarts": (ctypes.c_longlong, [ctypes.c_void_p]),
     "compas_b200_amr_nbox": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "compas_b200_amr_fill": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "compas_b200_thinc_face_values": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
@@ -443,6 +448,20 @@ def nc_terms(p: Parm) -> int:
     return n
 
 
+def energy_bound_min(p: Parm, g: Geom, U, out=None, stream=None):
+    """Smallest energy bound over the valid cells of the device state U (FIVEEQS): the value the
+    reference's MinEnergyBound (source/Class_Compressible_PhaseField.cpp:3596-3635) checks after every
+    stage under FiniteVolume.ID_Bound = 1. Into the device double `out` when given, else returned."""
+    import torch
+
+    res = out if out is not None else torch.empty(1, dtype=torch.float64, device="cuda")
+    _check(lib().compas_b200_energy_bound_min(ctypes.byref(p), ctypes.byref(g), _ptr(U), _ptr(res),
+                                              _stream_ptr(stream)))
+    if out is None:
+        return float(res.item())
+    return None
+
+
 def face_shape(p: Parm, g: Geom, d: int, ncomp: int) -> tuple:
     """Shape (components, z, y, x) of the face array of direction d (a face MultiFab without ghosts)."""
     n = [g.n[0] + (d == 0), g.n[1] + (d == 1), (g.n[2] + (d == 2)) if p.dim == 3 else 1]
@@ -630,6 +649,10 @@ class Level:
     def tma(self) -> bool:
         """Whether the stage kernel stages its halo slabs by TMA (3D mixed form)."""
         return bool(lib().compas_b200_level_tma(self._h))
+
+    def bound_restarts(self) -> int:
+        """Steps taken again because a stage violated the energy bound (FiniteVolume.ID_Bound = 1)."""
+        return int(lib().compas_b200_level_bound_restarts(self._h))
 
     def pf_substeps(self) -> int:
         """Phase-Field sub-steps taken so far (PhaseField.phase_field = 1)."""

@@ -21,6 +21,7 @@
 #include "launch.h"
 #include "phasefield.h"
 #include "stage_kernel.cuh"
+#include "bound.cuh"
 
 namespace compas {
 
@@ -345,7 +346,7 @@ static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
                    : (p->id_limiter < 0 || p->id_limiter > 4))
         return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.Scheme: this build runs GODUNOV, MUSCL-*, WENO3, WENO3B, "
                                               "WENO5 and WENO5B");
-    if (p->id_limiter < 5 && (p->thinc || p->phase_field))
+    if (p->id_limiter < 5 && !p->id_bound && (p->thinc || p->phase_field))
         return fail(COMPAS_B200_EUNSUPPORTED, "THINC and the Phase-Field step run with WENO5 / WENO5B here");
     if (p->id_riemann < 0 || p->id_riemann > 2)
         return fail(COMPAS_B200_EUNSUPPORTED, "Physics.RiemannSolver: this build runs LLF, HLL and HLLC");
@@ -358,6 +359,19 @@ static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
         return fail(COMPAS_B200_EARG, "non flux-based mechanism can not use the explicit RC approach");
     if (p->precision != 0 && p->precision != 1)
         return fail(COMPAS_B200_EARG, "precision must be 0 (plain FP64) or 1 (mixed)");
+    if (p->id_bound) {
+        // the bound-preserving branch of the flux functor is the five-equation model's
+        // (include/Operators_Compressible5Eq/FVM_Conservative2FluxHyperbolic_K_Compressible5Eq.H:100-152)
+        if (p->physics != COMPAS_B200_FIVEEQS)
+            return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.ID_Bound = 1: this engine runs the bound-preserving "
+                                                  "right-hand side of FIVEEQS");
+        if (p->precision != 0)
+            return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.ID_Bound = 1 runs in plain FP64 (compas_b200.precision = fp64)");
+        if (p->phase_field)
+            return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.ID_Bound = 1 with PhaseField.phase_field = 1 is not in "
+                                                  "this engine");
+        if (p->id_lambda != 0 && p->id_lambda != 1) return fail(COMPAS_B200_EARG, "id_lambda must be 0 or 1");
+    }
     if (g->ng < 3) return fail(COMPAS_B200_EARG, "WENO5 needs ng >= 3 ghost cells");
     for (int d = 0; d < p->dim; ++d) {
         if (g->n[d] < 1) return fail(COMPAS_B200_EARG, "empty box");
@@ -673,6 +687,231 @@ static int noalloc_scratch(unsigned char** out) {
     return COMPAS_B200_OK;
 }
 
+// ------------------------------------------------------------------------------------------------
+// Bound-preserving right-hand side (FiniteVolume.ID_Bound = 1, FIVEEQS): launch helpers of the face
+// pass and the stage update of bound.cuh, and the work arrays of a level.
+// ------------------------------------------------------------------------------------------------
+// Quadrature weight of the limiters: 1/12 with WENO5 / WENO5B (ID_Poly 4), 1/6 otherwise (MUSCLBP's
+// fixed weight; WENO3 / WENO3B run WENO5BP with ID_Poly 2), FiniteVolume_Parameter.H:60-141.
+static double bp_limiter_weight(const compas_b200_parm* p) {
+    return (p->id_weno && p->id_limiter >= 5) ? 1.0 / 12.0 : 1.0 / 6.0;
+}
+// Quadrature_Weight of the CFL speed (FiniteVolume_Parameter.H:161-173): ID_Poly 0 (GODUNOV) 1,
+// 2 (MUSCL family and WENO3 / WENO3B under ID_Bound) 1/6, 4 (WENO5 / WENO5B) 1/12.
+static double bp_cfl_weight(const compas_b200_parm* p) {
+    if (!p->id_weno && p->id_limiter == 0) return 1.0;
+    return (p->id_weno && p->id_limiter >= 5) ? 1.0 / 12.0 : 1.0 / 6.0;
+}
+
+static long long bp_face_count(const compas_b200_geom* g, int D, int d) {
+    long long c = 1;
+    for (int e = 0; e < D; ++e) c *= (long long)g->n[e] + (e == d);
+    return c;
+}
+
+static BpFaceArgs bp_face_args(const compas_b200_parm* p, const compas_b200_geom* g, const double* U, int id_lambda) {
+    BpFaceArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.U = U;
+    a.g = make_grid(p, g);
+    a.e = make_eos(p);
+    a.D = p->dim;
+    a.weno = p->id_weno;
+    a.lim = p->id_weno ? 0 : p->id_limiter;
+    a.id_k = p->source_term;
+    a.id_lambda = id_lambda;
+    a.wb = bp_limiter_weight(p);
+    a.qw = bp_cfl_weight(p);
+    a.which = COMPAS_B200_FACES_ALL;
+    long long tot = 0;
+    for (int d = 0; d < 3; ++d) {
+        a.dx[d] = g->dx[d];
+        a.area[d] = 1.0;
+        a.off[d] = tot;
+        if (d < p->dim) tot += bp_face_count(g, p->dim, d);
+    }
+    a.off[3] = tot;
+    return a;
+}
+
+static int launch_bp_faces(const BpFaceArgs& a, cudaStream_t st) {
+    const long long total = a.off[a.D];
+    if (total == 0) return COMPAS_B200_OK;
+    const unsigned blocks = (unsigned)std::min<long long>((total + 127) / 128, 148LL * 16);
+    if (a.D == 2) bp_face_kernel<2><<<blocks, 128, 0, st>>>(a);
+    else bp_face_kernel<3><<<blocks, 128, 0, st>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    return COMPAS_B200_OK;
+}
+
+static BpUpdateArgs bp_update_args(const compas_b200_parm* p, const compas_b200_geom* g) {
+    BpUpdateArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.g = make_grid(p, g);
+    a.e = make_eos(p);
+    a.D = p->dim;
+    a.id_k = p->source_term;
+    for (int d = 0; d < 3; ++d) a.dx[d] = g->dx[d];
+    return a;
+}
+
+static int launch_bp_update(const BpUpdateArgs& a, cudaStream_t st) {
+    const long long cells = (long long)a.g.n[0] * a.g.n[1] * (a.D == 3 ? a.g.n[2] : 1);
+    const unsigned blocks = (unsigned)std::min<long long>((cells + 127) / 128, 148LL * 16);
+    if (a.D == 2) bp_update_kernel<2><<<blocks, 128, 0, st>>>(a);
+    else bp_update_kernel<3><<<blocks, 128, 0, st>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    return COMPAS_B200_OK;
+}
+
+// Face arrays of one box: N fluxes and the normal face velocity per direction, one allocation.
+struct BpFaces {
+    double* base = nullptr;
+    double* F[3] = {nullptr, nullptr, nullptr};
+    double* V[3] = {nullptr, nullptr, nullptr};
+};
+static long long bp_faces_bytes(const compas_b200_parm* p, const compas_b200_geom* g) {
+    long long b = 0;
+    for (int d = 0; d < p->dim; ++d) b += bp_face_count(g, p->dim, d) * (nstate(p) + 1);
+    return b * (long long)sizeof(double);
+}
+static void bp_faces_carve(const compas_b200_parm* p, const compas_b200_geom* g, double* base, BpFaces* f) {
+    f->base = base;
+    double* q = base;
+    for (int d = 0; d < p->dim; ++d) {
+        const long long c = bp_face_count(g, p->dim, d);
+        f->F[d] = q;
+        q += c * nstate(p);
+        f->V[d] = q;
+        q += c;
+    }
+}
+
+// The face pass and the update of one stage (mode kModeStage or kModeDudt) of a ghost-filled Us.
+static int bp_stage(const compas_b200_parm* p, const compas_b200_geom* g, const BpFaces& f, const double* Us,
+                    const double* U0, double* Uout, int mode, int stage, const double* dt_dev, int id_lambda,
+                    const int* done, const unsigned long long* prev_eb, int nprev, unsigned long long* eb,
+                    unsigned long long* cmax, unsigned int* err, cudaStream_t st) {
+    BpFaceArgs fa = bp_face_args(p, g, Us, id_lambda);
+    for (int d = 0; d < p->dim; ++d) {
+        fa.F[d] = f.F[d];
+        fa.V[d] = f.V[d];
+    }
+    fa.done = done;
+    fa.prev_eb = prev_eb;
+    fa.nprev = nprev;
+    fa.cmax = cmax;
+    fa.err = err;
+    int rc = launch_bp_faces(fa, st);
+    if (rc) return rc;
+    BpUpdateArgs ua = bp_update_args(p, g);
+    ua.Us = Us;
+    ua.U0 = U0;
+    ua.Uout = Uout;
+    ua.mode = mode;
+    ua.stage = stage;
+    ua.dt = dt_dev;
+    for (int d = 0; d < p->dim; ++d) {
+        ua.F[d] = f.F[d];
+        ua.V[d] = f.V[d];
+    }
+    ua.done = done;
+    ua.prev_eb = prev_eb;
+    ua.nprev = nprev;
+    ua.eb = eb;
+    ua.err = err;
+    return launch_bp_update(ua, st);
+}
+
+// Right-hand side or one stage through the drop-in entry points: face arrays from the stream-ordered
+// allocator, released on the same stream.
+static int bp_entry(const compas_b200_parm* p, const compas_b200_geom* g, const double* Us, const double* U0,
+                    double* Uout, int mode, int stage, const double* dt_dev, double* cmax_dev, unsigned int* err_dev,
+                    cudaStream_t st) {
+    compas_b200_geom gg = *g;
+    if (p->dim == 2) gg.n[2] = 1;
+    void* base = nullptr;
+    CUDA_TRY(cudaMallocAsync(&base, (size_t)bp_faces_bytes(p, &gg), st));
+    BpFaces f;
+    bp_faces_carve(p, &gg, static_cast<double*>(base), &f);
+    const int rc = bp_stage(p, &gg, f, Us, U0, Uout, mode, stage, dt_dev, p->id_lambda, nullptr, nullptr, 0, nullptr,
+                            reinterpret_cast<unsigned long long*>(cmax_dev), err_dev, st);
+    const cudaError_t e = cudaFreeAsync(base, st);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(COMPAS_B200_ECUDA, std::string("face scratch release: ") + cudaGetErrorString(e));
+    return COMPAS_B200_OK;
+}
+
+// Work arrays of a bound-preserving level: the state at the start of the step (a step that is taken
+// again starts from it), the face arrays, and the three stages' energy-bound keys.
+struct BpLevel {
+    double* Usave = nullptr;
+    BpFaces faces;
+    unsigned long long* eb = nullptr;
+};
+
+static void bp_destroy(BpLevel* b) {
+    if (!b) return;
+    cudaFree(b->Usave);
+    cudaFree(b->faces.base);
+    cudaFree(b->eb);
+    delete b;
+}
+
+static int bp_create(const compas_b200_parm* p, const compas_b200_geom* g, long long state_bytes, BpLevel** out) {
+    auto* b = new BpLevel();
+    void* base = nullptr;
+    cudaError_t e = cudaMalloc(&b->Usave, state_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&base, bp_faces_bytes(p, g));
+    if (e == cudaSuccess) bp_faces_carve(p, g, static_cast<double*>(base), &b->faces);
+    if (e == cudaSuccess) e = cudaMalloc(&b->eb, 4 * sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        if (!b->faces.base) cudaFree(base);
+        bp_destroy(b);
+        cudaGetLastError();
+        return fail(e == cudaErrorMemoryAllocation ? COMPAS_B200_ENOMEM : COMPAS_B200_ECUDA,
+                    std::string("bound-preserving work arrays: ") + cudaGetErrorString(e));
+    }
+    *out = b;
+    return COMPAS_B200_OK;
+}
+
+// Smallest energy bound of the valid cells (MinEnergyBound) as an ordered key, then as a double.
+template <int D>
+__global__ void __launch_bounds__(128) bp_min_kernel(const double* U, Grid g, Eos e, unsigned long long* key,
+                                                     unsigned int* err) {
+    using M = FiveEq<D>;
+    const long long nx = g.n[0], ny = g.n[1], cells = nx * ny * (D == 3 ? g.n[2] : 1);
+    unsigned long long kmin = ~0ull;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < cells;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % nx), j = (int)((t / nx) % ny), k = (int)(t / (nx * ny));
+        double Uc[M::N];
+        load_cons<M>(Uc, U, g, g.at(i, j, k));
+        const double eb = fiveeq_energy_bound<D>(Uc, e, err);
+        if (!isnan(eb)) {
+            const unsigned long long kk = bp_key(eb);
+            if (kk < kmin) kmin = kk;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long v = __shfl_xor_sync(0xffffffffu, kmin, o);
+        if (v < kmin) kmin = v;
+    }
+    if ((threadIdx.x & 31) == 0 && kmin != ~0ull) atomicMin(key, kmin);
+}
+
+__global__ void bp_key_to_double_kernel(const unsigned long long* key, double* out) {
+    const unsigned long long k = *key;
+    if (k == ~0ull) {
+        *out = __longlong_as_double(0x7ff0000000000000ll);  // +inf: no finite value
+        return;
+    }
+    const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+    *out = __longlong_as_double((long long)b);
+}
+
 }  // namespace compas
 
 #include "batch.cuh"
@@ -701,6 +940,8 @@ struct compas_b200_level {
     compas::PfLevel* pf = nullptr;  // Phase-Field work arrays (PhaseField.phase_field = 1)
     long long pf_substeps = 0;
     compas::PfInfo pf_last{};       // counters of the last Phase-Field step
+    compas::BpLevel* bp = nullptr;  // bound-preserving work arrays (FiniteVolume.ID_Bound = 1)
+    long long bp_restarts = 0;
     int shape = 0, order = 0;       // stage-kernel launch shape and tile order (autotuner or forced)
     bool tuned = false, forced = false;
     compas::TmaMaps maps[3];        // TMA maps of U, U1, U2 (3D mixed form; valid = 0 otherwise)
@@ -809,6 +1050,7 @@ int compas_b200_parm_init_nphase(compas_b200_parm* p, int physics, int dim, int 
     p->tma = 1;
     p->cv_1 = 1.0;
     p->cv_2 = 1.0;
+    p->id_lambda = 1;
     if (physics != COMPAS_B200_FIVEEQS && physics != COMPAS_B200_SIXEQS && physics != COMPAS_B200_FIVEEQS_NPHASE)
         return fail(COMPAS_B200_EARG, "physics must be FIVEEQS (555), SIXEQS (666) or FIVEEQS_NPHASE (55501)");
     if (dim != 2 && dim != 3) return fail(COMPAS_B200_EARG, "dim must be 2 or 3");
@@ -867,7 +1109,7 @@ int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value
     if (k == "FiniteVolume.THINC.NormalThreshold") { if (!parse_double(value, &x)) return bad("a number"); p->thinc_normal_threshold = x; return 0; }
     if (k == "FiniteVolume.ID_Bound") {
         if (!parse_int(value, &ix) || ix < 0 || ix > 1) return bad("0, 1");
-        if (ix == 1) return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.ID_Bound = 1 is outside this engine's hot path");
+        p->id_bound = ix;
         return 0;
     }
     if (k == "Physics.RiemannSolver") {
@@ -1094,6 +1336,8 @@ int compas_b200_compute_dUdt(const compas_b200_parm* p, const compas_b200_geom* 
     int rc = check_args(p, g);
     if (rc) return rc;
     if (!U || !dUdt) return fail(COMPAS_B200_EARG, "null state");
+    if (p->id_bound)
+        return bp_entry(p, g, U, nullptr, dUdt, kModeDudt, 0, nullptr, cmax_dev, err_dev, (cudaStream_t)stream);
     StageArgs a = base_args(p, g);
     a.Us = U;
     a.Uout = dUdt;
@@ -1112,6 +1356,8 @@ int compas_b200_rk3_stage(const compas_b200_parm* p, const compas_b200_geom* g, 
     if (stage < 0 || stage > 2) return fail(COMPAS_B200_EARG, "stage must be 0, 1 or 2");
     if (!Us || !Unew || !dt_dev || (stage > 0 && !Uold)) return fail(COMPAS_B200_EARG, "null argument");
     if (Us == Unew) return fail(COMPAS_B200_EARG, "Unew may not alias Us");
+    if (p->id_bound)
+        return bp_entry(p, g, Us, Uold, Unew, kModeStage, stage, dt_dev, cmax_dev, err_dev, (cudaStream_t)stream);
     StageArgs a = base_args(p, g);
     a.Us = Us;
     a.U0 = Uold;
@@ -1130,6 +1376,8 @@ int compas_b200_pf_compute_dUdt(const compas_b200_parm* p, const compas_b200_geo
                                 void* stream) {
     int rc = check_args(p, g);
     if (rc) return rc;
+    if (p->id_bound)
+        return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field step with FiniteVolume.ID_Bound = 1 is not in this engine");
     if (p->physics == COMPAS_B200_FIVEEQS_NPHASE)
         return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field right-hand side is the two-phase models'");
     if (!U || !dUdt || !gq0 || !gq1 || (p->dim == 3 && !gq2)) return fail(COMPAS_B200_EARG, "null argument");
@@ -1148,6 +1396,8 @@ int compas_b200_pf_rk3_stage(const compas_b200_parm* p, const compas_b200_geom* 
                              const double* gq1, const double* gq2, unsigned int* err_dev, void* stream) {
     int rc = check_args(p, g);
     if (rc) return rc;
+    if (p->id_bound)
+        return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field step with FiniteVolume.ID_Bound = 1 is not in this engine");
     if (p->physics == COMPAS_B200_FIVEEQS_NPHASE)
         return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field right-hand side is the two-phase models'");
     if (stage < 0 || stage > 2) return fail(COMPAS_B200_EARG, "stage must be 0, 1 or 2");
@@ -1171,6 +1421,8 @@ int compas_b200_pf_grad_q(const compas_b200_parm* p, const compas_b200_geom* g, 
                           double* gq0, double* gq1, double* gq2, double* info, void* stream) {
     int rc = check_args(p, g);
     if (rc) return rc;
+    if (p->id_bound)
+        return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field step with FiniteVolume.ID_Bound = 1 is not in this engine");
     if (p->physics == COMPAS_B200_FIVEEQS_NPHASE)
         return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field step is the two-phase models'");
     if (!U || !gq0 || !gq1 || (p->dim == 3 && !gq2)) return fail(COMPAS_B200_EARG, "null argument");
@@ -1252,6 +1504,9 @@ int compas_b200_rk3_step_noalloc(const compas_b200_parm* p, const compas_b200_ge
     int rc = check_args(p, g);
     if (rc) return rc;
     if (!U) return fail(COMPAS_B200_EARG, "null state");
+    if (p->id_bound)
+        return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.ID_Bound = 1 runs on the level API (its steps may be taken "
+                                              "again), not in the allocation-free step");
     if (!(dt > 0.0) || !(dt <= DBL_MAX)) return fail(COMPAS_B200_EARG, "dt must be positive and finite");
     const long long bytes = compas_b200_state_bytes(p, g);
     if (bytes > kNoAllocStateBytes)
@@ -1317,6 +1572,10 @@ int compas_b200_level_create(const compas_b200_parm* p, const compas_b200_geom* 
     make_tma_maps(p, &lv->g, lv->U1, &lv->maps[1]);
     make_tma_maps(p, &lv->g, lv->U2, &lv->maps[2]);
     lv->use_tma = lv->maps[0].valid && lv->maps[1].valid && lv->maps[2].valid;
+    if (p->id_bound && (rc = bp_create(p, &lv->g, lv->bytes, &lv->bp))) {
+        compas_b200_level_destroy(lv);
+        return rc;
+    }
     if (p->phase_field) {
         std::string msg;
         if ((rc = pf_create(p, &lv->g, &lv->pf, &msg))) {
@@ -1350,6 +1609,7 @@ int compas_b200_level_destroy(compas_b200_level* lv) {
     cudaFree(lv->ctl);
     cudaFree(lv->dts);
     pf_destroy(lv->pf);
+    bp_destroy(lv->bp);
     delete lv;
     return COMPAS_B200_OK;
 }
@@ -1423,18 +1683,23 @@ static int tune_level(compas_b200_level* lv, cudaStream_t st) {
 }
 
 // The launches of one coarse step: ComputeDt, then three (fill, stage) pairs, then t += dt.
+static StepParams level_step_params(const compas_b200_level* lv) {
+    StepParams sp;
+    sp.cfl = lv->p.cfl;
+    sp.dx[0] = lv->g.dx[0];
+    sp.dx[1] = lv->g.dx[1];
+    sp.dx[2] = lv->g.dx[2];
+    sp.D = lv->p.dim;
+    sp.limiter = lv->p.change_limiter;
+    sp.dts = lv->dts;
+    sp.dts_cap = lv->dts_cap;
+    return sp;
+}
+
 static int enqueue_step(compas_b200_level* lv, cudaStream_t st) {
     const compas_b200_parm* p = &lv->p;
     const compas_b200_geom* g = &lv->g;
-    StepParams sp;
-    sp.cfl = p->cfl;
-    sp.dx[0] = g->dx[0];
-    sp.dx[1] = g->dx[1];
-    sp.dx[2] = g->dx[2];
-    sp.D = p->dim;
-    sp.limiter = p->change_limiter;
-    sp.dts = lv->dts;
-    sp.dts_cap = lv->dts_cap;
+    const StepParams sp = level_step_params(lv);
     step_begin_kernel<<<1, 1, 0, st>>>(lv->ctl, sp);
     CUDA_TRY(cudaGetLastError());
     StageArgs a = base_args(p, g);
@@ -1460,6 +1725,112 @@ static int enqueue_step(compas_b200_level* lv, cudaStream_t st) {
     return COMPAS_B200_OK;
 }
 
+// ---- bound-preserving level advance (FiniteVolume.ID_Bound = 1) ----------------------------------
+// The step of Evolve with its energy check (source/Class_Compressible_PhaseField.cpp:236-306) and the
+// checks after every stage of ThirdOrderSSPRK (:4014-4030, :4049-4065, :4086-4102). A stage whose new
+// state has a negative energy bound somewhere ends the step: its later launches do nothing, the host
+// reads the three stages' bounds after the step, restores the state the step started from, computes
+// the wave speeds of that state with the general bound (ID_Lambda = 0: CalculateInitialcmax under
+// ID_Return = 1, :4481-4483), the step's dt again (ComputeDt, limited against the failed dt), and
+// takes the step with ID_Lambda = 0. One host synchronisation per step, as the reference's host
+// reductions after every stage need. If the step taken again still violates the bound, the level
+// keeps the state it started from, sets COMPAS_B200_ERR_BOUND and stops (the reference goes on from
+// the violating stage state).
+__global__ void bp_restart_kernel(StepCtl* s, unsigned int err) {
+    s->cmax = 0ull;  // RemakeAllLevelsFromData resets c_max
+    s->err = err;    // the failed attempt's status bits are dropped with its state
+}
+
+__global__ void bp_fail_kernel(StepCtl* s) {
+    s->err |= COMPAS_B200_ERR_BOUND;
+    s->done = 1;
+}
+
+struct BpHostView {
+    StepCtl ctl;
+    unsigned long long eb[3];
+};
+
+static int bp_enqueue_stages(compas_b200_level* lv, int id_lambda, cudaStream_t st) {
+    const compas_b200_parm* p = &lv->p;
+    const compas_b200_geom* g = &lv->g;
+    BpLevel* b = lv->bp;
+    CUDA_TRY(cudaMemsetAsync(b->eb, 0xff, 3 * sizeof(unsigned long long), st));
+    double* in[3] = {lv->U, lv->U1, lv->U2};
+    double* out[3] = {lv->U1, lv->U2, lv->U};
+    for (int s = 0; s < 3; ++s) {
+        int rc;
+        if ((rc = launch_fill(p, g, in[s], st))) return rc;
+        if ((rc = bp_stage(p, g, b->faces, in[s], lv->U, out[s], kModeStage, s, &lv->ctl->dt, id_lambda,
+                           &lv->ctl->done, b->eb, s, b->eb + s, &lv->ctl->cmax, &lv->ctl->err, st)))
+            return rc;
+    }
+    lv->launches += 9;
+    return COMPAS_B200_OK;
+}
+
+static int bp_read(compas_b200_level* lv, BpHostView* h, cudaStream_t st) {
+    CUDA_TRY(cudaMemcpyAsync(&h->ctl, lv->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(h->eb, lv->bp->eb, sizeof(h->eb), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return COMPAS_B200_OK;
+}
+
+static bool bp_violated(const BpHostView& h) {
+    for (int s = 0; s < 3; ++s)
+        if (bp_key_negative(h.eb[s])) return true;
+    return false;
+}
+
+static int bp_advance(compas_b200_level* lv, int nsteps, cudaStream_t st) {
+    const compas_b200_parm* p = &lv->p;
+    const compas_b200_geom* g = &lv->g;
+    const StepParams sp = level_step_params(lv);
+    BpHostView h;
+    int rc;
+    CUDA_TRY(cudaMemcpyAsync(&h.ctl, lv->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    for (int s = 0; s < nsteps && !h.ctl.done; ++s) {
+        const unsigned int err0 = h.ctl.err;
+        step_begin_kernel<<<1, 1, 0, st>>>(lv->ctl, sp);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpyAsync(lv->bp->Usave, lv->U, lv->bytes, cudaMemcpyDeviceToDevice, st));
+        lv->launches += 1;
+        if ((rc = bp_enqueue_stages(lv, 1, st))) return rc;
+        if ((rc = bp_read(lv, &h, st))) return rc;
+        if (h.ctl.done) break;
+        if (bp_violated(h)) {
+            ++lv->bp_restarts;
+            CUDA_TRY(cudaMemcpyAsync(lv->U, lv->bp->Usave, lv->bytes, cudaMemcpyDeviceToDevice, st));
+            bp_restart_kernel<<<1, 1, 0, st>>>(lv->ctl, err0);
+            CUDA_TRY(cudaGetLastError());
+            if ((rc = launch_fill(p, g, lv->U, st))) return rc;
+            BpFaceArgs fa = bp_face_args(p, g, lv->U, 0);
+            fa.cmax = &lv->ctl->cmax;
+            fa.err = &lv->ctl->err;
+            if ((rc = launch_bp_faces(fa, st))) return rc;
+            step_begin_kernel<<<1, 1, 0, st>>>(lv->ctl, sp);
+            CUDA_TRY(cudaGetLastError());
+            lv->launches += 4;
+            if ((rc = bp_enqueue_stages(lv, 0, st))) return rc;
+            if ((rc = bp_read(lv, &h, st))) return rc;
+            if (h.ctl.done) break;
+            if (bp_violated(h)) {
+                CUDA_TRY(cudaMemcpyAsync(lv->U, lv->bp->Usave, lv->bytes, cudaMemcpyDeviceToDevice, st));
+                bp_fail_kernel<<<1, 1, 0, st>>>(lv->ctl);
+                CUDA_TRY(cudaGetLastError());
+                lv->launches += 1;
+                break;
+            }
+        }
+        step_end_kernel<<<1, 1, 0, st>>>(lv->ctl);
+        CUDA_TRY(cudaGetLastError());
+        lv->launches += 1;
+        h.ctl.done = 0;
+    }
+    return COMPAS_B200_OK;
+}
+
 int compas_b200_level_advance(compas_b200_level* lv, int nsteps, double stop_time, int use_graph, void* stream) {
     if (!lv) return fail(COMPAS_B200_EARG, "null level");
     if (nsteps < 0) return fail(COMPAS_B200_EARG, "nsteps must be >= 0");
@@ -1471,16 +1842,25 @@ int compas_b200_level_advance(compas_b200_level* lv, int nsteps, double stop_tim
     if (lv->need_init) {
         // CalculateInitialcmax (source/Class_Compressible_PhaseField.cpp:4501-4605)
         if ((rc = launch_fill(&lv->p, &lv->g, lv->U, st))) return rc;
-        StageArgs a = base_args(&lv->p, &lv->g);
-        a.Us = lv->U;
-        a.mode = kModeCmax;
-        a.cmax = &lv->ctl->cmax;
-        a.err = &lv->ctl->err;
-        if ((rc = launch_stage(&lv->p, a, st))) return rc;
+        if (lv->bp) {
+            // through the bound-preserving branch of the flux functor, ID_Lambda = 1
+            BpFaceArgs fa = bp_face_args(&lv->p, &lv->g, lv->U, 1);
+            fa.cmax = &lv->ctl->cmax;
+            fa.err = &lv->ctl->err;
+            if ((rc = launch_bp_faces(fa, st))) return rc;
+        } else {
+            StageArgs a = base_args(&lv->p, &lv->g);
+            a.Us = lv->U;
+            a.mode = kModeCmax;
+            a.cmax = &lv->ctl->cmax;
+            a.err = &lv->ctl->err;
+            if ((rc = launch_stage(&lv->p, a, st))) return rc;
+        }
         lv->launches += 2;
         lv->need_init = false;
     }
     if (nsteps == 0) return COMPAS_B200_OK;
+    if (lv->bp) return bp_advance(lv, nsteps, st);
     if (lv->p.autotune && !lv->tuned && !lv->forced && !lv->p.thinc) {
         if ((rc = tune_level(lv, st))) return rc;
         if (lv->graph) {
@@ -1565,7 +1945,7 @@ int compas_b200_level_step_host(compas_b200_level* lv, const double* host_in, do
     const int layers = (g->n[sd] + TS - 1) / TS;
     const int C = std::min(std::min(slabs, layers), 64);
     const bool tune_pending = p->autotune && !lv->tuned && !lv->forced && !p->thinc;
-    if (lv->pf || lv->need_init || tune_pending || g->lo_bc[sd] == 0 || C < 2) {
+    if (lv->pf || lv->bp || lv->need_init || tune_pending || g->lo_bc[sd] == 0 || C < 2) {
         int rc;
         if ((rc = compas_b200_level_set_state(lv, host_in, 0, stream))) return rc;
         if ((rc = compas_b200_level_advance(lv, 1, 1.0e300, 1, stream))) return rc;
@@ -1692,6 +2072,30 @@ int compas_b200_level_set_kernel(compas_b200_level* lv, int shape, int order) {
         cudaGraphExecDestroy(lv->graph);
         lv->graph = nullptr;
     }
+    return COMPAS_B200_OK;
+}
+
+long long compas_b200_level_bound_restarts(const compas_b200_level* lv) { return lv ? lv->bp_restarts : 0; }
+
+int compas_b200_energy_bound_min(const compas_b200_parm* p, const compas_b200_geom* g, const double* U,
+                                 double* min_dev, void* stream) {
+    int rc = check_args(p, g);
+    if (rc) return rc;
+    if (!U || !min_dev) return fail(COMPAS_B200_EARG, "null argument");
+    if (p->physics != COMPAS_B200_FIVEEQS)
+        return fail(COMPAS_B200_EUNSUPPORTED, "the energy bound is this engine's for FIVEEQS");
+    cudaStream_t st = (cudaStream_t)stream;
+    const Grid G = make_grid(p, g);
+    const long long cells = (long long)G.n[0] * G.n[1] * (p->dim == 3 ? G.n[2] : 1);
+    const unsigned blocks = (unsigned)std::max<long long>(1, std::min<long long>((cells + 127) / 128, 148LL * 16));
+    // the result slot holds the ordered key of the running minimum, then the value
+    auto* key = reinterpret_cast<unsigned long long*>(min_dev);
+    CUDA_TRY(cudaMemsetAsync(key, 0xff, sizeof(unsigned long long), st));
+    if (p->dim == 2) bp_min_kernel<2><<<blocks, 128, 0, st>>>(U, G, make_eos(p), key, nullptr);
+    else bp_min_kernel<3><<<blocks, 128, 0, st>>>(U, G, make_eos(p), key, nullptr);
+    CUDA_TRY(cudaGetLastError());
+    bp_key_to_double_kernel<<<1, 1, 0, st>>>(key, min_dev);
+    CUDA_TRY(cudaGetLastError());
     return COMPAS_B200_OK;
 }
 
@@ -1835,6 +2239,7 @@ int compas_b200_batch_add(compas_b200_batch* b, const compas_b200_parm* p, const
         (p->physics == COMPAS_B200_FIVEEQS_NPHASE && p->nphase != b->nphase))
         return fail(COMPAS_B200_EARG, "a batch holds cases of one model, dimension, number of phases, scheme and precision");
     if (p->thinc) return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.THINC = 1 runs on the level API, not in a batch");
+    if (p->id_bound) return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.ID_Bound = 1 runs on the level API, not in a batch");
     if (b->free_slots.empty()) return fail(COMPAS_B200_ENOMEM, "batch capacity reached");
     if (max_steps < 0) return fail(COMPAS_B200_EARG, "max_steps must be >= 0");
     cudaStream_t st = (cudaStream_t)stream;

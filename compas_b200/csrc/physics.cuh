@@ -866,8 +866,11 @@ __device__ __forceinline__ double bound_min_theta(double f_c, double fL, double 
 // face `side` (+1 right, -1 left). include/Operators_Compressible5Eq/
 // FVM_Reconstruction2Face_Conservative_WENO5B_D_Compressible5Eq.H:15-320 and the six-equation
 // counterpart (same steps).
-__device__ __forceinline__ void weno5b_masses(const double* ar1, const double* ar2, const double* al1, int side,
-                                              double& a1r1_f, double& a2r2_f, double& alpha1_f) {
+// Both faces of the cell: the right-face values to Wp[0], Wp[1], Wp[ia], the left-face values to
+// Wm[0], Wm[1], Wm[ia]; W the quadrature weight of the positivity limiter (1/12 for WENO5B, 1/6 where
+// the bound-preserving path runs it for a third-order scheme, FiniteVolume_Parameter.H:60-173).
+__device__ __forceinline__ void weno5b_masses_both(const double* ar1, const double* ar2, const double* al1, double W,
+                                                   double* Wp, double* Wm, int ia) {
     double rL[2], rR[2], aL[2], aR[2];
     double sumL = 0.0, sumR = 0.0;
     double ac[2];
@@ -887,8 +890,8 @@ __device__ __forceinline__ void weno5b_masses(const double* ar1, const double* a
         rR[k] = weno_sum(q, w);
         weno5_parts(fa[0], fa[1], fa[2], fa[3], fa[4], -1, qa, nullptr);
         aR[k] = weno_sum(qa, w);
-        const double th_r = bound_min_theta(fr[2], rL[k], rR[k]);
-        const double th_a = bound_min_theta(fa[2], aL[k], aR[k]);
+        const double th_r = bound_min_theta(fr[2], rL[k], rR[k], W);
+        const double th_a = bound_min_theta(fa[2], aL[k], aR[k], W);
         const double th = dmin(th_r, th_a);
         rL[k] = fr[2] + th * (rL[k] - fr[2]);
         aL[k] = fa[2] + th * (aL[k] - fa[2]);
@@ -905,17 +908,27 @@ __device__ __forceinline__ void weno5b_masses(const double* ar1, const double* a
         aL[k] /= sumL;
         rR[k] /= sumR;
         aR[k] /= sumR;
-        const double th_r = bound_min_theta(rc, rL[k], rR[k]);
-        const double th_a = bound_min_theta(ac[k], aL[k], aR[k]);
+        const double th_r = bound_min_theta(rc, rL[k], rR[k], W);
+        const double th_a = bound_min_theta(ac[k], aL[k], aR[k], W);
         if (th_r < Th) Th = th_r;  // std::min({Th, th_r, th_a})
         if (th_a < Th) Th = th_a;
     }
-    const double r1 = (side == 1) ? rL[0] : rR[0];
-    const double r2 = (side == 1) ? rL[1] : rR[1];
-    const double a1 = (side == 1) ? aL[0] : aR[0];
-    a1r1_f = ar1[2] + Th * (r1 - ar1[2]);
-    a2r2_f = ar2[2] + Th * (r2 - ar2[2]);
-    alpha1_f = al1[2] + Th * (a1 - al1[2]);
+    Wp[0] = ar1[2] + Th * (rL[0] - ar1[2]);
+    Wp[1] = ar2[2] + Th * (rL[1] - ar2[2]);
+    Wp[ia] = al1[2] + Th * (aL[0] - al1[2]);
+    Wm[0] = ar1[2] + Th * (rR[0] - ar1[2]);
+    Wm[1] = ar2[2] + Th * (rR[1] - ar2[2]);
+    Wm[ia] = al1[2] + Th * (aR[0] - al1[2]);
+}
+
+__device__ __forceinline__ void weno5b_masses(const double* ar1, const double* ar2, const double* al1, int side,
+                                              double& a1r1_f, double& a2r2_f, double& alpha1_f) {
+    double Wp[3], Wm[3];
+    weno5b_masses_both(ar1, ar2, al1, 1.0 / 12.0, Wp, Wm, 2);
+    const double* Wf = (side == 1) ? Wp : Wm;
+    a1r1_f = Wf[0];
+    a2r2_f = Wf[1];
+    alpha1_f = Wf[2];
 }
 
 // ------------------------------------------------------------------------------------------------

@@ -253,7 +253,25 @@ __device__ __forceinline__ void relax_pressure(double* U, const Eos& e, double t
         W[M::IE1] = a1p1R;
         W[M::IE2] = a2p2R;
         W[M::IA] = alpha1R;
-        M::prim2cons(U, W, e, err);
+        if constexpr (FAST) {
+            // the relaxation moves energy between the phases and leaves the momentum alone: keep the
+            // entry momentum and total energy to the bit (the phase with the larger volume fraction takes
+            // the remainder, as the safeguarded branch below does), so that the reciprocal-based entry
+            // state does not make the total energy drift
+            double mom[D];
+#pragma unroll
+            for (int d = 0; d < D; ++d) mom[d] = U[2 + d];
+            const double E = U[M::IE1] + U[M::IE2];
+            M::prim2cons(U, W, e, err);
+#pragma unroll
+            for (int d = 0; d < D; ++d) U[2 + d] = mom[d];
+            if (alpha1R >= alpha2R)
+                U[M::IE1] = E - U[M::IE2];
+            else
+                U[M::IE2] = E - U[M::IE1];
+        } else {
+            M::prim2cons(U, W, e, err);
+        }
         return;
     }
     double AlphaR[2];

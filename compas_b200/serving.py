@@ -9,7 +9,9 @@ can replay the same requests one at a time on a single-case level for comparison
 
 Request types:
   bubble2d   2D FIVEEQS shock-bubble (WENO5B), side^2 cells
-  droplet3d  3D SIXEQS shock-droplet (WENO5, relaxation), side^3 cells
+  droplet3d  3D SIXEQS shock-droplet (WENO5B, relaxation), side^3 cells: the bounded scheme, because
+             with WENO5 the droplet's volume fraction leaves [0, 1] and the run stops on a NaN after
+             about 700 steps at 112^3 in both precision forms, inside the requests' 100-2000 steps
   triple2d   2D FIVEEQS_NPHASE (NPHASE = 3) triple point on [0,7] x [0,3] (WENO5), 7 side x 3 side cells
 """
 from __future__ import annotations
@@ -23,7 +25,7 @@ from . import FIVEEQS, FIVEEQS_NPHASE, SIXEQS, Batch, Level, make_geom, make_par
 from . import cases as _cases
 
 # kind: (physics, dim, FiniteVolume.Scheme id, NPHASE)
-KINDS = {"bubble2d": (FIVEEQS, 2, 6, 2), "droplet3d": (SIXEQS, 3, 5, 2), "triple2d": (FIVEEQS_NPHASE, 2, 5, 3)}
+KINDS = {"bubble2d": (FIVEEQS, 2, 6, 2), "droplet3d": (SIXEQS, 3, 6, 2), "triple2d": (FIVEEQS_NPHASE, 2, 5, 3)}
 
 
 @dataclass
@@ -57,6 +59,7 @@ def make_case(req: Request, precision: str, device="cuda", xp=None):
         phys, dim, inputs, geom, U = _cases.triple_point(m=req.side, xp=xp, device=device)
     else:
         phys, dim, inputs, geom, U = _cases.shock_droplet(n=req.side, xp=xp, device=device)
+        inputs = dict(inputs, **{"FiniteVolume.Scheme": "WENO5B"})
     inputs = dict(inputs, **{"compas_b200.precision": precision})
     return make_parm(phys, dim, inputs), make_geom(**geom), U
 

@@ -38,6 +38,8 @@ extern "C" {
 #define COMPAS_B200_ERR_RELAX_NOROOT 0x4u /* safeguarded relaxation found no root */
 #define COMPAS_B200_ERR_CFL 0x8u          /* non-positive or non-finite time step */
 #define COMPAS_B200_ERR_TIMEOUT 0x10u     /* an asynchronous (TMA) copy did not complete within its bounded wait */
+#define COMPAS_B200_ERR_BOUND 0x20u       /* FiniteVolume.ID_Bound = 1: the energy bound still failed after the
+                                           * step was taken again with the general wave-speed bound */
 
 /* ---- models and schemes (the reference's compile-time PHYSICS and run-time keys) ------------ */
 #define COMPAS_B200_FIVEEQS 555 /* include/Macros.H:56 */
@@ -116,6 +118,16 @@ typedef struct compas_b200_parm {
     /* amr.Interpolater of the multi-level object's coarse-fine ghost cells and new fine cells
      * (source/COMPAS.cpp:1217-1221, :1611-1618): 0 lincc_interp (default), 1 pc_interp */
     int amr_interp;
+    /* FiniteVolume.ID_Bound (include/Operators_FV/FiniteVolume_Parameter.H:45, :56): 1 the bound-preserving
+     * right-hand side of FIVEEQS (MUSCLBP / WENO5BP face states limited by the energy bound, the HLL
+     * solver with bounded wave speeds) and the level advance's energy check of every stage with the
+     * step taken again on a violation (source/Class_Compressible_PhaseField.cpp:236-306, :3780-3790);
+     * FP64 only. id_lambda is the reference's FiniteVolume_Parm.ID_Lambda (:47, not an inputs key):
+     * 1 (default) the wave speeds from the sound speed, 0 the general bound the driver switches to
+     * for the step it takes again; the level advance switches it by itself, a host that drives the
+     * stage entry points sets it as the reference's Evolve does. */
+    int id_bound;
+    int id_lambda;
 } compas_b200_parm;
 
 /* One box covering a single-level domain (the valid cells), its ghost width and its boundary codes
@@ -175,7 +187,9 @@ int compas_b200_fill_boundary(const compas_b200_parm* p, const compas_b200_geom*
  * (source/Class_Compressible_PhaseField.cpp:3151-3537; include/Classes_Physics/
  * Class_Compressible_PhaseField.H:116-139). cmax_dev (device double, may be NULL) receives
  * max(*cmax_dev, largest face wave speed over the low faces of the valid cells); err_dev (device
- * unsigned, may be NULL) is OR-ed with status bits. */
+ * unsigned, may be NULL) is OR-ed with status bits. With FiniteVolume.ID_Bound = 1 (FIVEEQS) the
+ * bound-preserving right-hand side runs instead (a face pass into stream-ordered scratch face arrays,
+ * then the divergence), its cmax the flux functor's CFL speed of that branch. */
 int compas_b200_compute_dUdt(const compas_b200_parm* p, const compas_b200_geom* g, const double* U, double* dUdt,
                              double* cmax_dev, unsigned int* err_dev, void* stream);
 
@@ -203,10 +217,19 @@ int compas_b200_nc_terms(const compas_b200_parm* p);
  *          (surroundingNodes(d)): n[e] + (e == d) faces along each e, nstate components, x fastest;
  *          flux_nc[d] likewise with compas_b200_nc_terms components. Either may be NULL (not
  *          written); in BOUNDARY mode only the boundary faces of the arrays are written.
- * The hyperbolic right-hand side without THINC (EUNSUPPORTED otherwise). */
+ * The hyperbolic right-hand side without THINC (EUNSUPPORTED otherwise); with FiniteVolume.ID_Bound = 1
+ * the fluxes of the bound-preserving branch. */
 int compas_b200_face_fluxes(const compas_b200_parm* p, const compas_b200_geom* g, const double* Us, int which,
                             int area_scaled, double* const flux[3], double* const flux_nc[3], unsigned int* err_dev,
                             void* stream);
+
+/* Smallest energy bound over the valid cells of U (FIVEEQS): rho E - |rho u|^2 / (2 rho) minus the
+ * internal energy of both phases at their p_min (Conservative2EnergyBound), the value the reference's
+ * MinEnergyBound (source/Class_Compressible_PhaseField.cpp:3596-3635) returns after every stage when
+ * FiniteVolume.ID_Bound = 1; a negative value restarts the step. Written to *min_dev (device double;
+ * +inf for a box without finite values). */
+int compas_b200_energy_bound_min(const compas_b200_parm* p, const compas_b200_geom* g, const double* U,
+                                 double* min_dev, void* stream);
 
 /* One fused TVD-RK3 stage (stage 0, 1, 2) of ThirdOrderSSPRK
  * (source/Class_Compressible_PhaseField.cpp:3937-4107) followed by PostTimeStage (the SIXEQS
@@ -320,6 +343,11 @@ int compas_b200_level_advance(compas_b200_level* lv, int nsteps, double stop_tim
 /* Wait for the level's work; report the time, the number of steps taken since upload and the status
  * word. Returns COMPAS_B200_ESTATE when the status word is non-zero. */
 int compas_b200_level_sync(compas_b200_level* lv, double* t, int* steps, unsigned int* status);
+
+/* FiniteVolume.ID_Bound = 1: how many steps of this level were taken again because a stage state
+ * violated the energy bound (each restart is logged by the reference's Evolve,
+ * source/Class_Compressible_PhaseField.cpp:264-306). Synchronises with the level's last advance. */
+long long compas_b200_level_bound_restarts(const compas_b200_level* lv);
 
 /* Step sizes of the steps taken since upload (up to n values). */
 int compas_b200_level_dts(compas_b200_level* lv, double* dts, int n);

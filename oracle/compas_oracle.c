@@ -1037,8 +1037,16 @@ static void face_flux(const Model* m, const Geo* g, const double* U, int i, int 
     hllc(m, UL, UR, d, F, fnc, cmax);
 }
 
+int cmp_energy_bound_min(const cmp_case* c, const double* U, double* out) {
+    (void)c; (void)U; (void)out;
+    return -2; /* the bound-preserving path is restated in the reference-header oracle only */
+}
+
+int cmp_bound_restarts(void) { return 0; }
+
 int cmp_compute_dudt(const cmp_case* c, const double* U, double* dUdt, double* cmax_out) {
     if (!c->id_weno || c->id_limiter < 5) return -2;  /* the port restates the WENO5 / WENO5B reconstructions only */
+    if (c->id_bound) return -2;
     const Model m = model_of(c);
     const Geo g = geo_of(c);
     const int N = m.N, NC = m.NC, D = m.D;
@@ -1158,7 +1166,7 @@ int cmp_relax(const cmp_case* c, double* U) {
 }
 
 int cmp_rk3_step(const cmp_case* c, double* U, double dt, double* cmax_out) {
-    if (!c->id_weno || c->id_limiter < 5) return -2;
+    if (!c->id_weno || c->id_limiter < 5 || c->id_bound) return -2;
     const Model m = model_of(c);
     const Geo g = geo_of(c);
     const long long tot = g.S * m.N;
@@ -1200,7 +1208,7 @@ int cmp_rk3_step(const cmp_case* c, double* U, double dt, double* cmax_out) {
 }
 
 int cmp_advance(const cmp_case* c, double* U, int nsteps, double stop_time, double* t, double* dts) {
-    if (!c->id_weno || c->id_limiter < 5) return -2;
+    if (!c->id_weno || c->id_limiter < 5 || c->id_bound) return -2;
     const Model m = model_of(c);
     const Geo g = geo_of(c);
     double dt_prev = 1.e100, cmax = 0.0, time = *t;

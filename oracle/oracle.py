@@ -54,6 +54,8 @@ class Case(ctypes.Structure):
         ("Ak", ctypes.c_double * 4), ("Bk", ctypes.c_double * 4),
         ("Ck", ctypes.c_double * 4), ("Dk", ctypes.c_double * 4),
         ("amr_interp", ctypes.c_int),
+        ("id_bound", ctypes.c_int),
+        ("id_lambda", ctypes.c_int),
     ]
 
 
@@ -80,6 +82,8 @@ _SIGS = {
 _OPTIONAL_SIGS = {
     "cmp_derive": (ctypes.c_int, [_P, _D, _D, _D, _D, ctypes.c_int, _D]),
     "cmp_thinc_face": (ctypes.c_int, [_D, _D, _D, _D, ctypes.c_longlong, _D]),
+    "cmp_energy_bound_min": (ctypes.c_int, [_P, _D, ctypes.POINTER(ctypes.c_double)]),
+    "cmp_bound_restarts": (ctypes.c_int, []),
 }
 
 
@@ -190,6 +194,8 @@ def case_from(parm, geom) -> Case:
         setattr(c, k, getattr(parm, k))
     c.nphase = getattr(parm, "nphase", 2)
     c.amr_interp = getattr(parm, "amr_interp", 0)
+    c.id_bound = getattr(parm, "id_bound", 0)
+    c.id_lambda = getattr(parm, "id_lambda", 1)
     if parm.physics == FIVEEQS_NPHASE:
         for k in range(4):
             c.Ak[k], c.Bk[k], c.Ck[k], c.Dk[k] = parm.Ak[k], parm.Bk[k], parm.Ck[k], parm.Dk[k]
@@ -346,6 +352,17 @@ class Oracle:
         self._call(self.lib.cmp_derive(self._c, cvv.ctypes.data, U.ctypes.data, v.ctypes.data, dflag.ctypes.data,
                                        len(vars_derived), out.ctypes.data))
         return out
+
+    # ---- bound-preserving path (FiniteVolume.ID_Bound = 1; reference-header build only) -----------
+    def energy_bound_min(self, U: np.ndarray) -> float:
+        """MinEnergyBound of the valid cells of U."""
+        out = ctypes.c_double()
+        self._call(self.lib.cmp_energy_bound_min(self._c, U.ctypes.data, ctypes.byref(out)))
+        return out.value
+
+    def bound_restarts(self) -> int:
+        """Steps the last advance took again after a failed energy check."""
+        return int(self.lib.cmp_bound_restarts())
 
     def threads(self) -> int:
         return int(self.lib.cmp_threads())

@@ -44,6 +44,10 @@ typedef struct cmp_case {
     int nphase;         /* FIVEEQS_NPHASE (55501): phases (the build's NPHASE); 2 otherwise */
     double Ak[4], Bk[4], Ck[4], Dk[4];  /* FIVEEQS_NPHASE EOS coefficients per phase (source/Parm.cpp:185-253) */
     int amr_interp;     /* amr.Interpolater of the multi-level advance: 0 lincc_interp, 1 pc_interp */
+    int id_bound;       /* FiniteVolume.ID_Bound (FiniteVolume_Parameter.H:45): 1 the bound-preserving branch and
+                         * the energy check of every stage with the step taken again (FIVEEQS) */
+    int id_lambda;      /* FiniteVolume_Parm.ID_Lambda of cmp_compute_dudt / cmp_rk3_step (1 default; the
+                         * advance switches it to 0 for a step it takes again) */
 } cmp_case;
 
 /* Number of conserved components of the case (NSTATE). */
@@ -56,6 +60,11 @@ int cmp_fill_ghosts(const cmp_case* c, double* U);
 /* dUdt (same layout as U; valid cells written) of the state U whose ghosts are filled, and the largest
  * face wave speed over the low faces of the valid cells (the c_max norm of the reference). */
 int cmp_compute_dudt(const cmp_case* c, const double* U, double* dUdt, double* cmax);
+
+/* FiniteVolume.ID_Bound = 1: smallest energy bound over the valid cells of U (MinEnergyBound), and
+ * the number of steps the last cmp_advance took again. */
+int cmp_energy_bound_min(const cmp_case* c, const double* U, double* out);
+int cmp_bound_restarts(void);
 
 /* Pressure relaxation of the valid cells of U in place (SIXEQS; no-op otherwise). */
 int cmp_relax(const cmp_case* c, double* U);

@@ -73,4 +73,7 @@ def reference_case(physics: int, dim: int, inputs: dict, geom: dict) -> Case:
     c.change_limiter = 1 if int(g("run.timestep_change_limiter", 1)) else 0
     c.nphase = 2
     c.amr_interp = {"lincc_interp": 0, "pc_interp": 1}[str(g("amr.Interpolater", "lincc_interp"))]
+    # FiniteVolume.ID_Bound (FiniteVolume_Parameter.H:45, :56); ID_Lambda starts at its default 1 (:47)
+    c.id_bound = int(g("FiniteVolume.ID_Bound", 0))
+    c.id_lambda = 1
     return c

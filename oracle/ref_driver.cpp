@@ -62,6 +62,8 @@
 #include "oracle_api.h"
 
 #include <cstring>
+#include <limits>
+#include <stdexcept>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -130,7 +132,12 @@ Parm make_parm(const cmp_case* c) {
                                            FVReconstruction::MUSCL_MC};
         fv.Scheme = muscl[c->id_limiter];
     }
-    fv.Quadrature_Weight = 1.0 / 12.0;
+    // FiniteVolume.ID_Bound: the MUSCL family runs its bounded form with ID_Poly 2 (:71-112); the
+    // quadrature weight of the bounded branch's CFL speed follows ID_Poly (:161-173)
+    fv.ID_Bound = c->id_bound;
+    fv.ID_Lambda = c->id_lambda;
+    if (c->id_bound && !c->id_weno && c->id_limiter > 0) fv.ID_Poly = 2;
+    fv.Quadrature_Weight = (fv.ID_Poly == 0) ? 1.0 : (fv.ID_Poly == 1) ? 0.5 : (fv.ID_Poly == 2) ? 1.0 / 6.0 : 1.0 / 12.0;
     fv.ID_THINC = c->thinc;
     fv.ID_THINC_UseNormal = c->thinc_use_normal;
     fv.THINC_EPS = c->thinc_eps;
@@ -316,9 +323,41 @@ void for_valid(const Geo& g, F&& f) {
     }
 }
 
+// MinEnergyBound (source/Class_Compressible_PhaseField.cpp:3596-3635): the smallest energy bound of the
+// valid cells through the reference's Conservative2EnergyBound (AMReX's MultiFab::min restated as a
+// running minimum; a NaN bound does not lower it). +inf for the models without the bounded branch.
+double min_energy_bound(const cmp_case* c, const Parm& parm, const double* U) {
+    double mn = std::numeric_limits<double>::infinity();
+#if (PHYSICS == FIVEEQS)
+    Geo g(c);
+    auto a = g.view(const_cast<double*>(U), NSTATE);
+    for (int k = 0; k < g.nz; ++k)
+    for (int j = 0; j < g.ny; ++j)
+    for (int i = 0; i < g.nx; ++i) {
+        amrex::Array<amrex::Real, NSTATE> Cons;
+        for (int n = 0; n < NSTATE; ++n) Cons[n] = a(i, j, k, n);
+        amrex::Real EB;
+        Conservative2EnergyBound(EB, Cons, parm);
+        if (EB < mn) mn = EB;
+    }
+#else
+    (void)c; (void)parm; (void)U;
+#endif
+    return mn;
+}
+
+// The energy check after a stage of ThirdOrderSSPRK under ID_Bound = 1 (:4014-4030): true when the
+// step has to be taken again.
+bool bound_violated(const cmp_case* c, const Parm& parm, const double* U) {
+    return parm.FiniteVolume_Parm.ID_Bound == 1 && min_energy_bound(c, parm, U) < 0;
+}
+
+int g_bound_restarts = 0;
+
 // ThirdOrderSSPRK: the stage combinations as MultiFab::LinComb / Saxpy compute them
-// (dst = a*x + b*y, then dst += a*x), with PostTimeStage (relaxation) after each stage.
-void rk3_step(const cmp_case* c, const Parm& parm, double* U, double dt, double* cmax_out) {
+// (dst = a*x + b*y, then dst += a*x), with PostTimeStage (relaxation) after each stage. Returns 1
+// (U holding the violating stage state) when an energy check fails, 0 otherwise.
+int rk3_step(const cmp_case* c, const Parm& parm, double* U, double dt, double* cmax_out) {
     Geo g(c);
     const long long tot = g.S * NSTATE;
     std::vector<double> U0(U, U + tot), Ub(tot), L(tot, 0.0);
@@ -330,6 +369,7 @@ void rk3_step(const cmp_case* c, const Parm& parm, double* U, double dt, double*
     cm = std::max(cm, cms);
     for_valid(g, [&](long long q) { U[q] = 1.0 * Ub[q] + dt * L[q]; });
     relax(c, parm, U);
+    if (bound_violated(c, parm, U)) return 1;
     // stage 2
     std::memcpy(Ub.data(), U, tot * sizeof(double));
     fill_ghosts(c, Ub.data());
@@ -341,6 +381,7 @@ void rk3_step(const cmp_case* c, const Parm& parm, double* U, double dt, double*
         U[q] += s2 * L[q];
     });
     relax(c, parm, U);
+    if (bound_violated(c, parm, U)) return 1;
     // stage 3
     std::memcpy(Ub.data(), U, tot * sizeof(double));
     fill_ghosts(c, Ub.data());
@@ -352,7 +393,9 @@ void rk3_step(const cmp_case* c, const Parm& parm, double* U, double dt, double*
         U[q] += s3 * L[q];
     });
     relax(c, parm, U);
+    if (bound_violated(c, parm, U)) return 1;
     if (cmax_out) *cmax_out = cm;
+    return 0;
 }
 
 double est_dt(const cmp_case* c, double cmax) {
@@ -973,17 +1016,31 @@ int cmp_relax(const cmp_case* c, double* U) {
 }
 
 int cmp_rk3_step(const cmp_case* c, double* U, double dt, double* cmax) {
+    int violated = 0;
+    const int rc = guarded([&] {
+        Parm parm = make_parm(c);
+        violated = rk3_step(c, parm, U, dt, cmax);
+    });
+    return rc ? rc : violated;
+}
+
+int cmp_energy_bound_min(const cmp_case* c, const double* U, double* out) {
     return guarded([&] {
         Parm parm = make_parm(c);
-        rk3_step(c, parm, U, dt, cmax);
+        *out = min_energy_bound(c, parm, U);
     });
 }
 
+int cmp_bound_restarts(void) { return g_bound_restarts; }
+
 int cmp_advance(const cmp_case* c, double* U, int nsteps, double stop_time, double* t, double* dts) {
     int taken = 0;
+    g_bound_restarts = 0;
     int rc = guarded([&] {
         Parm parm = make_parm(c);
+        parm.FiniteVolume_Parm.ID_Lambda = 1;  // the struct default; the step taken again switches it
         Geo g(c);
+        const long long tot = g.S * NSTATE;
         double dt_prev = 1.e100;  // COMPAS::dt starts at 1e100 (source/COMPAS.cpp:81)
         double cmax = 0.0;
         double time = *t;
@@ -1001,7 +1058,36 @@ int cmp_advance(const cmp_case* c, double* U, int nsteps, double stop_time, doub
             const double eps = 1.0e-3 * dt0;
             if (time + dt0 > stop_time - eps) dt0 = stop_time - time;
             dt_prev = dt0;
-            rk3_step(c, parm, U, dt0, &cmax);
+            std::vector<double> Usave;
+            if (parm.FiniteVolume_Parm.ID_Bound == 1) Usave.assign(U, U + tot);
+            if (rk3_step(c, parm, U, dt0, &cmax)) {
+                // Evolve under ID_Bound = 1 (source/Class_Compressible_PhaseField.cpp:264-306):
+                // RemakeAllLevelsFromData back to the state the step started from, ID_Lambda = 0,
+                // ComputeDt with ID_Return = 1 (CalculateInitialcmax of that state, :4481-4483; the
+                // change limiter against the failed dt), the step again, ID_Lambda = 1
+                ++g_bound_restarts;
+                std::memcpy(U, Usave.data(), sizeof(double) * tot);
+                parm.FiniteVolume_Parm.ID_Lambda = 0;
+                {
+                    std::vector<double> Ub(U, U + tot), L(tot);
+                    fill_ghosts(c, Ub.data());
+                    compute_dudt(c, parm, Ub.data(), L.data(), &cmax);
+                }
+                double dt_re = est_dt(c, cmax);
+                if (time == 0.0) dt_prev = dt_re;
+                if (c->change_limiter && dt_prev > 0.0) dt_re = std::min(dt_re, 1.1 * dt_prev);
+                dt0 = dt_re;
+                const double eps2 = 1.0e-3 * dt0;
+                if (time + dt0 > stop_time - eps2) dt0 = stop_time - time;
+                dt_prev = dt0;
+                const int again = rk3_step(c, parm, U, dt0, &cmax);
+                parm.FiniteVolume_Parm.ID_Lambda = 1;
+                if (again) {
+                    // this engine's convention: the state the step started from is kept and the run stops
+                    std::memcpy(U, Usave.data(), sizeof(double) * tot);
+                    throw std::runtime_error("the energy bound failed again after the step was taken again");
+                }
+            }
             if (dts) dts[step] = dt0;
             time += dt0;
             ++taken;

@@ -115,8 +115,8 @@ def test_shock_droplet_conserves_on_a_periodic_box(precision, scheme):
     err = np.abs(totals(V) - tot0) / scale
     print(f"{precision} {scheme}: periodic shock-droplet 64^3 x 200 steps, relative change of the masses, "
           f"momenta, total energy: {err}; alpha1 in [{V[7].min():.3e}, {V[7].max():.3e}]")
-    assert np.all(err[:5] <= 1e-13), err
-    # the mixed form's total energy moves by ~1.4e-12 over the 200 steps (measured; plain form ~1e-14)
-    assert err[5] <= (1e-13 if precision == "fp64" else 1e-11), err
+    # the mixed relaxation keeps the entry momentum and total energy of a cell to the bit (the larger
+    # phase takes the remainder of the total), so both forms conserve the total energy to round-off
+    assert np.all(err <= 1e-13), err
     if scheme == "WENO5B":
         assert V[7].min() >= 0.0 and V[7].max() <= 1.0

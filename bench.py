@@ -64,13 +64,13 @@ def parse():
     ap.add_argument("--no-triple", action="store_true")
     ap.add_argument("--triple-m", type=int, default=256, help="triple point side: 7m x 3m cells")
     ap.add_argument("--triple-steps", type=int, default=20)
-    ap.add_argument("--serve-requests", type=int, default=16)
+    ap.add_argument("--serve-requests", type=int, default=12)
     ap.add_argument("--serve-rate", type=float, default=16.0, help="headline arrival rate (one of --serve-rates)")
-    ap.add_argument("--serve-rates", default="4,16,64", help="arrival rates swept (requests/s)")
-    ap.add_argument("--serve-sizes", default="bench", choices=["bench", "config"],
-                    help="request sizes: 'bench' (reduced: 128-512^2, 64-96^3, 100-300 steps) or 'config' (the "
-                         "serving configuration: 128-1024^2, 64-192^3, triple point 224x96-896x384, 100-2000 steps)")
-    ap.add_argument("--serve-seq-sample", type=int, default=0,
+    ap.add_argument("--serve-rates", default="4,16", help="arrival rates swept (requests/s)")
+    ap.add_argument("--serve-sizes", default="config", choices=["bench", "config"],
+                    help="request sizes: 'config' (the serving configuration: 128-1024^2, 64-192^3, triple point "
+                         "224x96-896x384, 100-2000 steps) or 'bench' (reduced: 128-512^2, 64-96^3, 100-300 steps)")
+    ap.add_argument("--serve-seq-sample", type=int, default=50,
                     help="time the one-at-a-time baselines over this many steps per request and scale (0: all)")
     return ap.parse_args()
 

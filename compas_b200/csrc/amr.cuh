@@ -7,9 +7,11 @@
 // ThirdOrderSSPRK with flux registers :3937-4107 and :3472-3537, ComputeDt COMPAS.cpp:2249-2303,
 // FillPatch / FillPatchStage COMPAS.cpp:1598-1799 with GetData :1953-1985, AverageDownTo :1549-1558,
 // RefluxLev Class_Compressible5Eq_PhaseField.cpp:77-160. The AMReX operations (FillPatchTwoLevels,
-// lincc_interp, FluxRegister, average_down) follow their documented semantics; lincc_interp is the
-// monotonized-central limited linear interpolation per direction (fine value u_c + sum_d off_d s_d,
-// off_d = -1/4 or +1/4).
+// lincc_interp, FluxRegister, average_down) follow their documented semantics; lincc_interp is AMReX's
+// CellConservativeLinear with linear limiting: per direction the central slopes of all components
+// scaled by one factor shared by the components, the smallest ratio of a component's
+// monotonized-central slope to its central slope (fine value u_c + sum_d off_d slope_d, off_d = -1/4 or
+// +1/4).
 //
 // Layout: every box keeps four padded arrays (two alternating time levels, two stage states); the
 // host builds, once per hierarchy, the tables of where every ghost cell, coarse-fine face and
@@ -126,33 +128,37 @@ __device__ __forceinline__ double amr_coarse(const AmrBufs& B, int cb, long long
 }
 
 // pc: amr.Interpolater = pc_interp (the parent's value, AMReX PCInterp); else lincc_interp as restated in the
-// file header
+// file header: per direction the central slopes of all components, one monotonized-central factor shared
+// by the components, u_f = u_c + sum_d +-1/4 slope_d
 __global__ void amr_interp_kernel(const AmrInterp* t, long long n, AmrBufs B, int dk, int knew, int kold, int mode,
                                   double alpha, double beta, int N, int D, int pc) {
+    constexpr int NMAX = 2 * COMPAS_B200_MAX_PHASES + 4;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
         const AmrInterp& e = t[q];
         double* dst = B.p[e.db * 4 + dk];
         const long long Sd = B.S[e.db];
-        for (int c = 0; c < N; ++c) {
-            auto val = [&](int s) {
-                const double v = amr_coarse(B, e.cb[s], e.cq[s], c, knew, kold, mode, alpha, beta);
-                return ((e.odd[s] >> c) & 1u) ? -1.0 * v : 1.0 * v;
-            };
-            const double uc = val(0);
-            double u = uc;
-            for (int d = 0; d < (pc ? 0 : D); ++d) {
-                const double um = val(1 + 2 * d), up = val(2 + 2 * d);
+        auto val = [&](int s, int c) {
+            const double v = amr_coarse(B, e.cb[s], e.cq[s], c, knew, kold, mode, alpha, beta);
+            return ((e.odd[s] >> c) & 1u) ? -1.0 * v : 1.0 * v;
+        };
+        double u[NMAX];
+        for (int c = 0; c < N; ++c) u[c] = val(0, c);
+        for (int d = 0; d < (pc ? 0 : D); ++d) {
+            double dcs[NMAX];
+            double sf = 1.0;
+            for (int c = 0; c < N; ++c) {
+                const double uc = val(0, c);
+                const double um = val(1 + 2 * d, c), up = val(2 + 2 * d, c);
                 const double dc = 0.5 * (up - um), df = 2.0 * (up - uc), db = 2.0 * (uc - um);
-                double s = 0.0;
-                if (df * db >= 0.0) {
-                    const double m = dmin(fabs(dc), dmin(fabs(df), fabs(db)));
-                    s = (dc >= 0.0) ? m : -m;
-                }
-                const double off = ((e.par >> d) & 1) ? 0.25 : -0.25;
-                u = u + off * s;
+                double sx = (df * db >= 0.0) ? dmin(fabs(df), fabs(db)) : 0.0;
+                sx = copysign(1.0, dc) * dmin(sx, fabs(dc));
+                if (dc != 0.0) sf = dmin(sf, sx / dc);
+                dcs[c] = dc;
             }
-            dst[c * Sd + e.dq] = u;
+            const double off = ((e.par >> d) & 1) ? 0.25 : -0.25;
+            for (int c = 0; c < N; ++c) u[c] = u[c] + off * (dcs[c] * sf);
         }
+        for (int c = 0; c < N; ++c) dst[c * Sd + e.dq] = u[c];
     }
 }
 

@@ -309,6 +309,7 @@ static Eos make_eos(const compas_b200_parm* p) {
         e.Bk[k] = p->Bk[k];
         e.Ck[k] = p->Ck[k];
         e.Dk[k] = p->Dk[k];
+        e.pmink[k] = (p->source_term == 1) ? -p->Bk[k] / (p->Ak[k] + 1.0) : -p->Bk[k] / p->Ak[k];
     }
     e.fA1 = (float)p->A1; e.fA2 = (float)p->A2;
     e.fB1 = (float)p->B1; e.fB2 = (float)p->B2;
@@ -362,9 +363,9 @@ static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
     if (p->id_bound) {
         // the bound-preserving branch of the flux functor is the five-equation model's
         // (include/Operators_Compressible5Eq/FVM_Conservative2FluxHyperbolic_K_Compressible5Eq.H:100-152)
-        if (p->physics != COMPAS_B200_FIVEEQS)
-            return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.ID_Bound = 1: this engine runs the bound-preserving "
-                                                  "right-hand side of FIVEEQS");
+        if (p->physics == COMPAS_B200_SIXEQS)
+            return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.ID_Bound = 1: the bound-preserving right-hand side is "
+                                                  "the five-equation models' (FIVEEQS, FIVEEQS_NPHASE)");
         if (p->precision != 0)
             return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.ID_Bound = 1 runs in plain FP64 (compas_b200.precision = fp64)");
         if (p->phase_field)
@@ -716,6 +717,8 @@ static BpFaceArgs bp_face_args(const compas_b200_parm* p, const compas_b200_geom
     a.g = make_grid(p, g);
     a.e = make_eos(p);
     a.D = p->dim;
+    a.physics = p->physics;
+    a.nphase = p->nphase;
     a.weno = p->id_weno;
     a.lim = p->id_weno ? 0 : p->id_limiter;
     a.id_k = p->source_term;
@@ -735,12 +738,7 @@ static BpFaceArgs bp_face_args(const compas_b200_parm* p, const compas_b200_geom
 }
 
 static int launch_bp_faces(const BpFaceArgs& a, cudaStream_t st) {
-    const long long total = a.off[a.D];
-    if (total == 0) return COMPAS_B200_OK;
-    const unsigned blocks = (unsigned)std::min<long long>((total + 127) / 128, 148LL * 16);
-    if (a.D == 2) bp_face_kernel<2><<<blocks, 128, 0, st>>>(a);
-    else bp_face_kernel<3><<<blocks, 128, 0, st>>>(a);
-    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(launch_bp_faces_model(a, st));
     return COMPAS_B200_OK;
 }
 
@@ -750,17 +748,15 @@ static BpUpdateArgs bp_update_args(const compas_b200_parm* p, const compas_b200_
     a.g = make_grid(p, g);
     a.e = make_eos(p);
     a.D = p->dim;
+    a.physics = p->physics;
+    a.nphase = p->nphase;
     a.id_k = p->source_term;
     for (int d = 0; d < 3; ++d) a.dx[d] = g->dx[d];
     return a;
 }
 
 static int launch_bp_update(const BpUpdateArgs& a, cudaStream_t st) {
-    const long long cells = (long long)a.g.n[0] * a.g.n[1] * (a.D == 3 ? a.g.n[2] : 1);
-    const unsigned blocks = (unsigned)std::min<long long>((cells + 127) / 128, 148LL * 16);
-    if (a.D == 2) bp_update_kernel<2><<<blocks, 128, 0, st>>>(a);
-    else bp_update_kernel<3><<<blocks, 128, 0, st>>>(a);
-    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(launch_bp_update_model(a, st));
     return COMPAS_B200_OK;
 }
 
@@ -876,32 +872,7 @@ static int bp_create(const compas_b200_parm* p, const compas_b200_geom* g, long 
     return COMPAS_B200_OK;
 }
 
-// Smallest energy bound of the valid cells (MinEnergyBound) as an ordered key, then as a double.
-template <int D>
-__global__ void __launch_bounds__(128) bp_min_kernel(const double* U, Grid g, Eos e, unsigned long long* key,
-                                                     unsigned int* err) {
-    using M = FiveEq<D>;
-    const long long nx = g.n[0], ny = g.n[1], cells = nx * ny * (D == 3 ? g.n[2] : 1);
-    unsigned long long kmin = ~0ull;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < cells;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % nx), j = (int)((t / nx) % ny), k = (int)(t / (nx * ny));
-        double Uc[M::N];
-        load_cons<M>(Uc, U, g, g.at(i, j, k));
-        const double eb = fiveeq_energy_bound<D>(Uc, e, err);
-        if (!isnan(eb)) {
-            const unsigned long long kk = bp_key(eb);
-            if (kk < kmin) kmin = kk;
-        }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long v = __shfl_xor_sync(0xffffffffu, kmin, o);
-        if (v < kmin) kmin = v;
-    }
-    if ((threadIdx.x & 31) == 0 && kmin != ~0ull) atomicMin(key, kmin);
-}
-
+// The ordered key of the smallest energy bound (bp_min_kernel) back to a double.
 __global__ void bp_key_to_double_kernel(const unsigned long long* key, double* out) {
     const unsigned long long k = *key;
     if (k == ~0ull) {
@@ -2082,8 +2053,8 @@ int compas_b200_energy_bound_min(const compas_b200_parm* p, const compas_b200_ge
     int rc = check_args(p, g);
     if (rc) return rc;
     if (!U || !min_dev) return fail(COMPAS_B200_EARG, "null argument");
-    if (p->physics != COMPAS_B200_FIVEEQS)
-        return fail(COMPAS_B200_EUNSUPPORTED, "the energy bound is this engine's for FIVEEQS");
+    if (p->physics == COMPAS_B200_SIXEQS)
+        return fail(COMPAS_B200_EUNSUPPORTED, "the energy bound is this engine's for FIVEEQS and FIVEEQS_NPHASE");
     cudaStream_t st = (cudaStream_t)stream;
     const Grid G = make_grid(p, g);
     const long long cells = (long long)G.n[0] * G.n[1] * (p->dim == 3 ? G.n[2] : 1);
@@ -2091,9 +2062,7 @@ int compas_b200_energy_bound_min(const compas_b200_parm* p, const compas_b200_ge
     // the result slot holds the ordered key of the running minimum, then the value
     auto* key = reinterpret_cast<unsigned long long*>(min_dev);
     CUDA_TRY(cudaMemsetAsync(key, 0xff, sizeof(unsigned long long), st));
-    if (p->dim == 2) bp_min_kernel<2><<<blocks, 128, 0, st>>>(U, G, make_eos(p), key, nullptr);
-    else bp_min_kernel<3><<<blocks, 128, 0, st>>>(U, G, make_eos(p), key, nullptr);
-    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(launch_bp_min_model(U, G, make_eos(p), p->dim, p->physics, p->nphase, key, blocks, st));
     bp_key_to_double_kernel<<<1, 1, 0, st>>>(key, min_dev);
     CUDA_TRY(cudaGetLastError());
     return COMPAS_B200_OK;

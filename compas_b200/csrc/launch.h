@@ -10,6 +10,17 @@ namespace compas {
 struct StageArgs;
 struct ListArgs;
 struct TmaMaps;
+struct BpFaceArgs;
+struct BpUpdateArgs;
+struct Grid;
+struct Eos;
+
+// Bound-preserving kernels (FiniteVolume.ID_Bound = 1; kern_bound.cu): the face pass, the stage update
+// and the smallest energy bound, for the model named by physics / nphase (FIVEEQS, FIVEEQS_NPHASE).
+cudaError_t launch_bp_faces_model(const BpFaceArgs& a, cudaStream_t st);
+cudaError_t launch_bp_update_model(const BpUpdateArgs& a, cudaStream_t st);
+cudaError_t launch_bp_min_model(const double* U, const Grid& g, const Eos& e, int dim, int physics, int nphase,
+                                unsigned long long* key, unsigned blocks, cudaStream_t st);
 
 // Variant of the stage kernel: FiniteVolume.Scheme (5 WENO5, 6 WENO5B), precision (0 FP64, 1 mixed),
 // FiniteVolume.THINC (single-box kernel only), and the Phase-Field regularisation right-hand side

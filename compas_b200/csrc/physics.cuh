@@ -62,6 +62,7 @@ struct Eos {
     double pinf1, pinf2;  // B1/(A1 + 1), B2/(A2 + 1) (the relaxation's admissibility check)
     double pmin1, pmin2;  // p_min of the two-phase Parm (source/Parm.cpp:164-171): -B/A, or -B/(A + 1) with K
     double Ak[kMaxPhases], Bk[kMaxPhases], Ck[kMaxPhases], Dk[kMaxPhases];
+    double pmink[kMaxPhases];  // p_min of the N-phase Parm, the same rule per phase (source/Parm.cpp:255-261)
     // FP32 copies (round to nearest) of A, B, C of the two phases for the mixed form's FP32 wave speeds,
     // so that the face loop converts no coefficients
     float fA1, fA2, fB1, fB2, fC1, fC2;
@@ -1176,11 +1177,13 @@ __device__ __forceinline__ void weno5b_masses_f32(const float* ar1, const float*
 // one common theta over all phases applied to the face of side `side`. r(k, s) and a(k, s) give alpha_k rho_k
 // and alpha_k of stencil cell s = 0..ORDER-1 (centre ORDER/2); the results go to rf[k], af[k]. PT = double:
 // the reference's arithmetic (quadrature weight 1/12 for ORDER 5, 1/6 for ORDER 3); PT = float: the mixed form.
+// Wq > 0 replaces the quadrature weight (the bound-preserving path runs the fifth-order stencil with
+// weight 1/6 for WENO3 / WENO3B, FiniteVolume_Parameter.H:114-127).
 template <int NP, int ORDER, class PT, class FR, class FA>
-__device__ __forceinline__ void bounded_phases(FR r, FA a, int side, PT* rf, PT* af) {
+__device__ __forceinline__ void bounded_phases(FR r, FA a, int side, PT* rf, PT* af, double Wq = 0.0) {
     constexpr bool F32 = std::is_same<PT, float>::value;
     constexpr int C = ORDER / 2;
-    constexpr double W = (ORDER == 5) ? 1.0 / 12.0 : 1.0 / 6.0;
+    const double W = (Wq > 0.0) ? Wq : ((ORDER == 5) ? 1.0 / 12.0 : 1.0 / 6.0);
     PT rL[NP], rR[NP], aL[NP], aR[NP];
     PT sumL = 0, sumR = 0;
 #pragma unroll

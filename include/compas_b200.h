@@ -119,10 +119,10 @@ typedef struct compas_b200_parm {
      * (source/COMPAS.cpp:1217-1221, :1611-1618): 0 lincc_interp (default), 1 pc_interp */
     int amr_interp;
     /* FiniteVolume.ID_Bound (include/Operators_FV/FiniteVolume_Parameter.H:45, :56): 1 the bound-preserving
-     * right-hand side of FIVEEQS (MUSCLBP / WENO5BP face states limited by the energy bound, the HLL
-     * solver with bounded wave speeds) and the level advance's energy check of every stage with the
-     * step taken again on a violation (source/Class_Compressible_PhaseField.cpp:236-306, :3780-3790);
-     * FP64 only. id_lambda is the reference's FiniteVolume_Parm.ID_Lambda (:47, not an inputs key):
+     * right-hand side of FIVEEQS and FIVEEQS_NPHASE (MUSCLBP / WENO5BP face states limited by the energy
+     * bound, the HLL solver with bounded wave speeds) and the level advance's energy check of every
+     * stage with the step taken again on a violation (source/Class_Compressible_PhaseField.cpp:236-306,
+     * :3780-3790); FP64 only. id_lambda is the reference's FiniteVolume_Parm.ID_Lambda (:47, not an inputs key):
      * 1 (default) the wave speeds from the sound speed, 0 the general bound the driver switches to
      * for the step it takes again; the level advance switches it by itself, a host that drives the
      * stage entry points sets it as the reference's Evolve does. */
@@ -187,7 +187,7 @@ int compas_b200_fill_boundary(const compas_b200_parm* p, const compas_b200_geom*
  * (source/Class_Compressible_PhaseField.cpp:3151-3537; include/Classes_Physics/
  * Class_Compressible_PhaseField.H:116-139). cmax_dev (device double, may be NULL) receives
  * max(*cmax_dev, largest face wave speed over the low faces of the valid cells); err_dev (device
- * unsigned, may be NULL) is OR-ed with status bits. With FiniteVolume.ID_Bound = 1 (FIVEEQS) the
+ * unsigned, may be NULL) is OR-ed with status bits. With FiniteVolume.ID_Bound = 1 (FIVEEQS, FIVEEQS_NPHASE) the
  * bound-preserving right-hand side runs instead (a face pass into stream-ordered scratch face arrays,
  * then the divergence), its cmax the flux functor's CFL speed of that branch. */
 int compas_b200_compute_dUdt(const compas_b200_parm* p, const compas_b200_geom* g, const double* U, double* dUdt,
@@ -223,8 +223,8 @@ int compas_b200_face_fluxes(const compas_b200_parm* p, const compas_b200_geom* g
                             int area_scaled, double* const flux[3], double* const flux_nc[3], unsigned int* err_dev,
                             void* stream);
 
-/* Smallest energy bound over the valid cells of U (FIVEEQS): rho E - |rho u|^2 / (2 rho) minus the
- * internal energy of both phases at their p_min (Conservative2EnergyBound), the value the reference's
+/* Smallest energy bound over the valid cells of U (FIVEEQS, FIVEEQS_NPHASE): rho E - |rho u|^2 / (2 rho)
+ * minus the internal energy of every phase at its p_min (Conservative2EnergyBound), the value the reference's
  * MinEnergyBound (source/Class_Compressible_PhaseField.cpp:3596-3635) returns after every stage when
  * FiniteVolume.ID_Bound = 1; a negative value restarts the step. Written to *min_dev (device double;
  * +inf for a box without finite values). */

@@ -100,7 +100,8 @@ Parm make_parm(const cmp_case* c) {
     if (c->nphase != NPHASE) amrex::Abort("the case's nphase differs from this build's NPHASE");
     for (int k = 0; k < NPHASE; ++k) {
         p.A[k] = c->Ak[k]; p.B[k] = c->Bk[k]; p.C[k] = c->Ck[k]; p.D[k] = c->Dk[k];
-        p.p_min[k] = 0.0;
+        // source/Parm.cpp:255-261
+        p.p_min[k] = (c->source_term == 1) ? -c->Bk[k] / (c->Ak[k] + 1.0) : -c->Bk[k] / c->Ak[k];
     }
 #else
     p.A1 = c->A1; p.A2 = c->A2; p.B1 = c->B1; p.B2 = c->B2;
@@ -328,7 +329,7 @@ void for_valid(const Geo& g, F&& f) {
 // running minimum; a NaN bound does not lower it). +inf for the models without the bounded branch.
 double min_energy_bound(const cmp_case* c, const Parm& parm, const double* U) {
     double mn = std::numeric_limits<double>::infinity();
-#if (PHYSICS == FIVEEQS)
+#if (PHYSICS == FIVEEQS || PHYSICS == FIVEEQS_NPHASE)
     Geo g(c);
     auto a = g.view(const_cast<double*>(U), NSTATE);
     for (int k = 0; k < g.nz; ++k)

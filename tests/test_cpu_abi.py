@@ -124,7 +124,7 @@ def test_amr_interpolater_key():
 
 def test_bound_preserving_key():
     """FiniteVolume.ID_Bound (FiniteVolume_Parameter.H:45, :56): 0 / 1, ID_Lambda starting at 1; the bounded
-    branch is the five-equation model's, in FP64, on the single-level path (the checks run before any
+    branch is the five-equation models', in FP64, without the Phase-Field step (the checks run before any
     device call, so they hold without a GPU)."""
     p = cb.make_parm(cb.FIVEEQS, 2, {"FiniteVolume.ID_Bound": 1, "FiniteVolume.Scheme": "MUSCL-MC"})
     assert p.id_bound == 1 and p.id_lambda == 1
@@ -134,7 +134,8 @@ def test_bound_preserving_key():
     g = cb.make_geom((16, 16, 1), (0.1, 0.1, 1.0))
     g3 = cb.make_geom((8, 8, 8), (0.1, 0.1, 0.1))
     for phys, dim, extra, geom in [(cb.SIXEQS, 3, {}, g3), (cb.FIVEEQS, 2, {"compas_b200.precision": "mixed"}, g),
-                                   (cb.FIVEEQS_NPHASE, 2, {"prob.EOS.gamma": [1.4, 1.5, 1.6]}, g)]:
+                                   (cb.FIVEEQS_NPHASE, 2, {"prob.EOS.gamma": [1.4, 1.5, 1.6],
+                                                           "PhaseField.phase_field": 1}, g)]:
         q = cb.make_parm(phys, dim, dict({"FiniteVolume.ID_Bound": 1}, **extra))
         with pytest.raises(cb.CompasError) as e:
             cb.Level(q, geom)

@@ -73,7 +73,7 @@ def _stressed_case(dim, scheme, state, seed=7):
 def _dudt_pair(p, g, U):
     import torch
 
-    if not have_ref(p.physics, p.dim):
+    if not have_ref(p.physics, p.dim, p.nphase):
         pytest.skip("reference-header oracle not built")
     Ud = torch.from_numpy(U.copy()).cuda()
     cb.FillPatch(p, g, Ud)
@@ -157,7 +157,7 @@ def test_energy_bound_min_equals_the_reference(dim):
 
 
 def _advance_pair(p, g, U, nsteps):
-    if not have_ref(p.physics, p.dim):
+    if not have_ref(p.physics, p.dim, p.nphase):
         pytest.skip("reference-header oracle not built")
     lv = cb.Level(p, g)
     lv.upload(U)
@@ -228,3 +228,86 @@ def test_advance_without_restarts_equals_the_reference():
     assert info.status == 0 and restarts == restarts_ref == 0
     np.testing.assert_array_equal(dts, dts_ref)
     np.testing.assert_array_equal(cb.valid_view(got, p, g), cb.valid_view(ref, p, g))
+
+
+# ---- FIVEEQS_NPHASE: the reference's N-phase bounded branch (include/Operators_Compressible5Eq_NPhase/
+# FVM_Conservative2FluxHyperbolic_K_Compressible5Eq_NPhase.H, Riemann_HLL_Bound_Compressible5Eq_NPhase.H),
+# its MUSCL states through the consistent limiter, its WENO5B states bounding every phase
+NPHASE_SCHEMES = ["GODUNOV", "MUSCL", "MUSCL-MC", "WENO3B", "WENO5", "WENO5B"]
+NPHASE_CASES = {
+    "triple_point": (cases.triple_point, dict(m=12)),
+    "bubbles2_K": (cases.nphase_bubbles, dict(n=24, nphase=2, source_term=1, velocity=30.0)),
+    "bubbles4_nasg_K": (cases.nphase_bubbles, dict(n=24, nphase=4, eos=3, source_term=1, velocity=30.0)),
+    "bubbles3_3d": (cases.nphase_bubbles, dict(n=12, nphase=3, dim=3, velocity=30.0)),
+    "bubbles3": (cases.nphase_bubbles, dict(n=24, nphase=3, velocity=30.0)),
+}
+
+
+def _nphase(name, scheme, extra=None):
+    fn, kw = NPHASE_CASES[name]
+    phys, dim, inputs, geom, U = fn(**kw, quadrature=False)
+    inp = dict(inputs, **{"FiniteVolume.Scheme": scheme, "FiniteVolume.ID_Bound": 1}, **(extra or {}))
+    p = cb.make_parm(phys, dim, inp)
+    return p, cb.make_geom(**geom), U
+
+
+@pytest.mark.parametrize("scheme", NPHASE_SCHEMES)
+@pytest.mark.parametrize("name", list(NPHASE_CASES))
+@pytest.mark.parametrize("id_lambda", [1, 0])
+def test_nphase_rhs_equals_the_reference(name, scheme, id_lambda):
+    p, g, U = _nphase(name, scheme)
+    if not have_ref(p.physics, p.dim, p.nphase):
+        pytest.skip("reference-header oracle not built")
+    p.id_lambda = id_lambda
+    got, ref, cm, cm_ref, _ = _dudt_pair(p, g, U)
+    np.testing.assert_array_equal(got, ref)
+    assert cm == cm_ref, (cm, cm_ref)
+
+
+def test_nphase_energy_bound_min_equals_the_reference():
+    import torch
+
+    p, g, U = _nphase("bubbles4_nasg_K", "MUSCL")
+    if not have_ref(p.physics, p.dim, p.nphase):
+        pytest.skip("reference-header oracle not built")
+    V = cb.valid_view(U, p, g)
+    V[cb.parm_nstate(p) - p.nphase - 1][..., 5] -= 1e9
+    got = cb.energy_bound_min(p, g, torch.from_numpy(U).cuda())
+    ref = Oracle("reference", p, g).energy_bound_min(U)
+    assert got == ref and got < 0
+
+
+# found with the oracle: 12 steps, one restart each
+NPHASE_RESTARTS = [("triple_point", "WENO5B", "3.0"), ("bubbles3", "MUSCL-MC", "2.8")]
+
+
+@pytest.mark.parametrize("name,scheme,cfl", NPHASE_RESTARTS, ids=[f"{c[0]}-{c[1]}-cfl{c[2]}" for c in NPHASE_RESTARTS])
+def test_nphase_advance_with_restart_equals_the_reference(name, scheme, cfl):
+    p, g, U = _nphase(name, scheme, {"run.cfl": cfl})
+    if not have_ref(p.physics, p.dim, p.nphase):
+        pytest.skip("reference-header oracle not built")
+    got, info, dts, restarts, ref, dts_ref, restarts_ref = _advance_pair(p, g, U, 12)
+    print(f"{name} {scheme} cfl {cfl}: {info.steps} steps, {restarts} restarts (reference {restarts_ref})")
+    assert info.status == 0 and info.steps == 12
+    assert restarts == restarts_ref == 1
+    np.testing.assert_array_equal(dts, dts_ref)
+    np.testing.assert_array_equal(cb.valid_view(got, p, g), cb.valid_view(ref, p, g))
+
+
+def test_nphase_advance_stops_when_the_step_taken_again_fails():
+    p, g, U = _nphase("triple_point", "MUSCL", {"run.cfl": "2.6"})
+    if not have_ref(p.physics, p.dim, p.nphase):
+        pytest.skip("reference-header oracle not built")
+    lv = cb.Level(p, g)
+    lv.upload(U)
+    lv.advance(12)
+    info = lv.sync(check=False)
+    got = lv.download()
+    lv.close()
+    assert info.status & cb.ERR_BOUND and info.steps < 12
+    ref = U.copy()
+    o = Oracle("reference", p, g)
+    o.advance(ref, info.steps)
+    np.testing.assert_array_equal(cb.valid_view(got, p, g), cb.valid_view(ref, p, g))
+    with pytest.raises(RuntimeError):
+        o.advance(U.copy(), info.steps + 1)

@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--batch-steps", type=int, default=10)
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-phase-field", action="store_true")
+    ap.add_argument("--no-phase-field-sixeq", action="store_true", help="only the 2D CAC Phase-Field line")
     ap.add_argument("--no-amr", action="store_true")
     ap.add_argument("--amr-steps", type=int, default=5)
     ap.add_argument("--pf-steps", type=int, default=10)
@@ -716,7 +717,7 @@ def run_ours(args, rank, world, dist):
             cpu = cpu_baseline(args.cpu_n, args.cpu_steps)
         batched = None if args.no_batched else run_batched(args)
         pf_res = None if args.no_phase_field else run_phase_field(args)
-        pf6_res = None if args.no_phase_field else run_phase_field_sixeq(args)
+        pf6_res = None if (args.no_phase_field or args.no_phase_field_sixeq) else run_phase_field_sixeq(args)
         amr_res = None if args.no_amr else run_amr(args)
         triple_res = None if args.no_triple else run_triple_point(args)
         line = {

@@ -21,6 +21,7 @@ import numpy as np
 FIVEEQS = 555
 SIXEQS = 666
 FIVEEQS_NPHASE = 55501
+SIXEQS_IE_NPHASE = 66601
 MAX_PHASES = 4
 
 OK = 0
@@ -243,6 +244,8 @@ def nstate(physics: int, dim: int, nphase: int = 2) -> int:
     """NSTATE of the model (include/Macros.H:73, :89, :114)."""
     if physics == FIVEEQS_NPHASE:
         return 2 * nphase + dim + 1
+    if physics == SIXEQS_IE_NPHASE:
+        return 3 * nphase + dim + 1
     return (4 if physics == FIVEEQS else 5) + dim
 
 
@@ -258,12 +261,14 @@ def _inputs_value(v) -> str:
 
 def make_parm(physics: int, dim: int, inputs: dict | None = None, nphase: int | None = None) -> Parm:
     """A parameter block from reference defaults plus inputs keys, e.g.
-    {"FiniteVolume.Scheme": "WENO5", "prob.EOS.gamma_2": 4.4, "run.cfl": 0.5}; for FIVEEQS_NPHASE the
-    per-phase lists {"prob.EOS.gamma": [1.4, 1.5, 1.5]} and `nphase` (the compile-time NPHASE)."""
+    {"FiniteVolume.Scheme": "WENO5", "prob.EOS.gamma_2": 4.4, "run.cfl": 0.5}; for FIVEEQS_NPHASE and
+    SIXEQS_IE_NPHASE the per-phase lists {"prob.EOS.gamma": [1.4, 1.5, 1.5]} and `nphase` (the
+    compile-time NPHASE)."""
     p = Parm()
     if nphase is None:
         g = (inputs or {}).get("prob.EOS.gamma")
-        nphase = len(g) if physics == FIVEEQS_NPHASE and isinstance(g, (list, tuple)) else 2
+        nphase = (len(g) if physics in (FIVEEQS_NPHASE, SIXEQS_IE_NPHASE) and isinstance(g, (list, tuple))
+                  else 2)
     _check(lib().compas_b200_parm_init_nphase(ctypes.byref(p), physics, dim, int(nphase)))
     for k, v in (inputs or {}).items():
         _check(lib().compas_b200_parm_set(ctypes.byref(p), k.encode(), _inputs_value(v).encode()))

@@ -11,7 +11,7 @@ import math
 
 import numpy as np
 
-from . import FIVEEQS, FIVEEQS_NPHASE, SIXEQS, nstate
+from . import FIVEEQS, FIVEEQS_NPHASE, SIXEQS, SIXEQS_IE_NPHASE, nstate
 
 # Gauss-Legendre nodes and weights on [-1, 1] (4 points, exact to degree 7)
 _GL_X, _GL_W = np.polynomial.legendre.leggauss(4)
@@ -340,6 +340,81 @@ def nphase_bubbles(n=32, nphase=3, dim=2, ng=3, quadrature=True, xp=None, device
     nz = n if dim == 3 else 1
     geom = dict(n=(n, n, nz), dx=dx, ng=ng, lo_bc=(0, 0, 0), hi_bc=(0, 0, 0))
     U = _average(physics, dim, (n, n, nz), dx, (0.0, 0.0, 0.0), pw, ng, quadrature, xp, device, nphase=nphase)
+    return physics, dim, inputs, geom, U
+
+
+def sixn_shock_bubbles(n=32, nphase=2, dim=2, ng=3, quadrature=True, xp=None, device=None, eos=1,
+                       relaxation=1, Ma=1.1, dp=0.0, scheme="MUSCL", riemann="HLLC", trace=0.0):
+    """SIXEQS_IE_NPHASE shock-bubble interaction after exec/ShockBubble-WaterAir-6Eq-Nphase (water
+    and air, pressures scaled by P0 = 101325 Pa and densities by 1000 kg/m^3), on [0, 2] x [0, 1]
+    (x [0, 1] in 3D) with n cells per unit length: water (phase 0, gamma 4.4, pinf 6e8 / P0, rho 1)
+    at p = 1 with a Mach-Ma water shock at x = 0.25 (Rankine-Hugoniot state behind it); an air bubble
+    (phase 1, gamma 1.4, rho 0.001) of radius 0.2 at (0.7, 0.5[, 0.5]); with nphase = 3 a helium
+    bubble (phase 2, gamma 1.667, rho 1.66e-4) of radius 0.15 at (1.3, 0.5[, 0.5]). Every phase
+    keeps a volume fraction of at least 1e-6 (tanh interfaces of width 2 dx, normalised). dp > 0
+    puts the phases out of pressure equilibrium (phase k at p (1 + dp k)), so that the relaxation
+    after each stage has work. eos = 3 adds a NASG covolume (b = 1e-4 for water, q 0). Outflow in x,
+    symmetry at y = 0, outflow at y = 1, periodic in z. Default MUSCL + HLLC with pressure
+    relaxation, cfl 0.3 (the example's inputs)."""
+    xp = _xp_of(xp)
+    physics = SIXEQS_IE_NPHASE
+    h = 1.0 / n
+    dx = (h, h, h if dim == 3 else 1.0)
+    P0 = 101325.0
+    gam = [4.4, 1.4, 1.667][:nphase]
+    pinf = [6.0e8 / P0, 0.0, 0.0][:nphase]
+    rho0 = [1.0, 0.001, 1.66e-4][:nphase]
+    bcov = ([1e-4] + [0.0] * (nphase - 1)) if eos == 3 else [0.0] * nphase
+    A = [1.0 / (g - 1.0) for g in gam]
+    B = [gam[k] * pinf[k] / (gam[k] - 1.0) for k in range(nphase)]
+    rs, us, ps = shock_state(Ma, 0.0, 1.0, rho0[0], gam[0], pinf[0])
+    centres = [(0.7, 0.2), (1.3, 0.15)][:nphase - 1]
+
+    def pw(x, y, z):
+        post = (x < 0.25) * 1.0
+        al = [None] * nphase
+        rest = 1.0
+        for k, (cx, rad) in enumerate(centres):
+            r2 = (x - cx) ** 2 + (y - 0.5) ** 2 + ((z - 0.5) ** 2 if dim == 3 else 0.0)
+            a = _clip(xp, 0.5 * (1.0 + _tanh(xp, (rad - _sqrt(xp, r2)) / (2.0 * h))), 1e-6, 1.0)
+            al[k + 1] = a
+            rest = rest - a
+        al[0] = _clip(xp, rest, 1e-6, 1.0)
+        ssum = 0.0
+        for a in al:
+            ssum = ssum + a
+        al = [a / ssum for a in al]
+        rho_w = rho0[0] + post * (rs - rho0[0])
+        dens = [rho_w] + rho0[1:]
+        ar = [al[k] * dens[k] for k in range(nphase)]
+        rho = 0.0
+        for v in ar:
+            rho = rho + v
+        u = post * us
+        p = 1.0 + post * (ps - 1.0)
+        vel = [u, y * 0.0] + ([z * 0.0] if dim == 3 else [])
+        ke = 0.0
+        for v in vel:
+            ke = ke + v * v
+        are = []
+        rho_e = 0.0
+        for k in range(nphase):
+            pk = p * (1.0 + dp * k)
+            xi = 1.0 - bcov[k] * dens[k]
+            e_k = (A[k] * xi) * (al[k] * pk) + (xi * al[k]) * B[k]
+            are.append(e_k)
+            rho_e = rho_e + e_k
+        return al + ar + are + [rho * v for v in vel] + [rho_e + 0.5 * rho * ke]
+
+    inputs = {"FiniteVolume.Scheme": scheme, "Physics.RiemannSolver": riemann, "prob.EOS.EOS": eos,
+              "prob.EOS.gamma": gam, "prob.EOS.pinf": pinf, "Physics.pressure_relaxation": relaxation,
+              "Physics.pressure_relaxation_trace": trace, "run.cfl": 0.3}
+    if eos == 3:
+        inputs["prob.EOS.b"] = bcov
+        inputs["prob.EOS.q"] = [0.0] * nphase
+    nx, ny, nz = 2 * n, n, (n if dim == 3 else 1)
+    geom = dict(n=(nx, ny, nz), dx=dx, ng=ng, lo_bc=(2, 3, 0), hi_bc=(2, 2, 0))
+    U = _average(physics, dim, (nx, ny, nz), dx, (0.0, 0.0, 0.0), pw, ng, quadrature, xp, device, nphase=nphase)
     return physics, dim, inputs, geom, U
 
 

@@ -320,28 +320,51 @@ static Eos make_eos(const compas_b200_parm* p) {
 // NSTATE (include/Macros.H:73, :89, :114).
 static int nstate_of(int physics, int dim, int nphase) {
     if (physics == COMPAS_B200_FIVEEQS_NPHASE) return 2 * nphase + dim + 1;
+    if (physics == COMPAS_B200_SIXEQS_IE_NPHASE) return 3 * nphase + dim + 1;
     return (physics == COMPAS_B200_FIVEEQS ? 4 : 5) + dim;
 }
 static int nstate(const compas_b200_parm* p) { return nstate_of(p->physics, p->dim, p->nphase); }
 
 // First momentum component (INDEX_MomentumX).
-static int mom0_of(int physics, int nphase) { return physics == COMPAS_B200_FIVEEQS_NPHASE ? nphase : 2; }
+static int mom0_of(int physics, int nphase) {
+    return physics == COMPAS_B200_FIVEEQS_NPHASE ? nphase : (physics == COMPAS_B200_SIXEQS_IE_NPHASE ? 3 * nphase : 2);
+}
+
+// The models with per-phase EOS lists (prob.EOS.gamma, ... with NPHASE values each).
+static bool nphase_model(int physics) {
+    return physics == COMPAS_B200_FIVEEQS_NPHASE || physics == COMPAS_B200_SIXEQS_IE_NPHASE;
+}
 
 // The N-phase kernels this build instantiates.
 static bool nphase_built(int dim, int nphase) {
     return (dim == 2 && nphase >= 2 && nphase <= 4) || (dim == 3 && nphase == 3);
 }
+static bool sixn_built(int dim, int nphase) { return (dim == 2 && (nphase == 2 || nphase == 3)) || (dim == 3 && nphase == 3); }
 
 static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
     if (!p || !g) return fail(COMPAS_B200_EARG, "null parameter or geometry");
     if (p->physics != COMPAS_B200_FIVEEQS && p->physics != COMPAS_B200_SIXEQS &&
-        p->physics != COMPAS_B200_FIVEEQS_NPHASE)
-        return fail(COMPAS_B200_EARG, "physics must be FIVEEQS (555), SIXEQS (666) or FIVEEQS_NPHASE (55501)");
+        p->physics != COMPAS_B200_FIVEEQS_NPHASE && p->physics != COMPAS_B200_SIXEQS_IE_NPHASE)
+        return fail(COMPAS_B200_EARG, "physics must be FIVEEQS (555), SIXEQS (666), FIVEEQS_NPHASE (55501) or "
+                                      "SIXEQS_IE_NPHASE (66601)");
     if (p->dim != 2 && p->dim != 3) return fail(COMPAS_B200_EARG, "dim must be 2 or 3");
     if (p->physics == COMPAS_B200_FIVEEQS_NPHASE) {
         if (!nphase_built(p->dim, p->nphase))
             return fail(COMPAS_B200_EUNSUPPORTED, "FIVEEQS_NPHASE: this build runs NPHASE 2, 3, 4 in 2D and 3 in 3D");
         if (p->thinc) return fail(COMPAS_B200_EUNSUPPORTED, "FIVEEQS_NPHASE: FiniteVolume.THINC is not in this engine");
+    }
+    if (p->physics == COMPAS_B200_SIXEQS_IE_NPHASE) {
+        if (!sixn_built(p->dim, p->nphase))
+            return fail(COMPAS_B200_EUNSUPPORTED, "SIXEQS_IE_NPHASE: this build runs NPHASE 2, 3 in 2D and 3 in 3D");
+        if (p->thinc) return fail(COMPAS_B200_EUNSUPPORTED, "SIXEQS_IE_NPHASE: FiniteVolume.THINC is not in this engine");
+        if (p->precision != 0)
+            return fail(COMPAS_B200_EUNSUPPORTED, "SIXEQS_IE_NPHASE runs in plain FP64 (compas_b200.precision = fp64)");
+        if (p->phase_field)
+            return fail(COMPAS_B200_EUNSUPPORTED, "PhaseField.phase_field = 1: this engine runs the FIVEEQS and SIXEQS "
+                                                  "Phase-Field step");
+        if (p->id_bound)
+            return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.ID_Bound = 1: the bound-preserving right-hand side is "
+                                                  "the five-equation models' (FIVEEQS, FIVEEQS_NPHASE)");
     }
     if (p->id_weno ? (p->id_limiter < 3 || p->id_limiter > 6)
                    : (p->id_limiter < 0 || p->id_limiter > 4))
@@ -421,6 +444,9 @@ static int launch_stage(const compas_b200_parm* p, const StageArgs& a, cudaStrea
         e = (p->dim == 2) ? launch_stage_fiveeq2(k, a, st, tm) : launch_stage_fiveeq3(k, a, st, tm);
     else if (p->physics == COMPAS_B200_SIXEQS)
         e = (p->dim == 2) ? launch_stage_sixeq2(k, a, st, tm) : launch_stage_sixeq3(k, a, st, tm);
+    else if (p->physics == COMPAS_B200_SIXEQS_IE_NPHASE)
+        e = (p->dim == 3) ? launch_stage_sixeqn3_3(k, a, st, tm)
+            : (p->nphase == 2) ? launch_stage_sixeqn2_2(k, a, st, tm) : launch_stage_sixeqn2_3(k, a, st, tm);
     else if (p->dim == 3) e = launch_stage_fiveeqn3_3(k, a, st, tm);
     else e = (p->nphase == 2) ? launch_stage_fiveeqn2_2(k, a, st, tm)
            : (p->nphase == 3) ? launch_stage_fiveeqn2_3(k, a, st, tm) : launch_stage_fiveeqn2_4(k, a, st, tm);
@@ -439,6 +465,9 @@ static int launch_list(int physics, int dim, int nphase, int limiter, int precis
     cudaError_t e;
     if (physics == COMPAS_B200_FIVEEQS) e = (dim == 2) ? launch_list_fiveeq2(k, L, st) : launch_list_fiveeq3(k, L, st);
     else if (physics == COMPAS_B200_SIXEQS) e = (dim == 2) ? launch_list_sixeq2(k, L, st) : launch_list_sixeq3(k, L, st);
+    else if (physics == COMPAS_B200_SIXEQS_IE_NPHASE)
+        e = (dim == 3) ? launch_list_sixeqn3_3(k, L, st)
+            : (nphase == 2) ? launch_list_sixeqn2_2(k, L, st) : launch_list_sixeqn2_3(k, L, st);
     else if (dim == 3) e = launch_list_fiveeqn3_3(k, L, st);
     else e = (nphase == 2) ? launch_list_fiveeqn2_2(k, L, st)
            : (nphase == 3) ? launch_list_fiveeqn2_3(k, L, st) : launch_list_fiveeqn2_4(k, L, st);
@@ -642,7 +671,7 @@ static StageArgs base_args(const compas_b200_parm* p, const compas_b200_geom* g)
     a.g = make_grid(p, g);
     a.e = make_eos(p);
     a.id_k = p->source_term;
-    a.relax = (p->physics == COMPAS_B200_SIXEQS) ? p->relaxation : 0;
+    a.relax = (p->physics == COMPAS_B200_SIXEQS || p->physics == COMPAS_B200_SIXEQS_IE_NPHASE) ? p->relaxation : 0;
     a.riemann = p->id_riemann;
     a.trace = p->relax_trace;
     a.pf_phasic = (p->pf_phase2flux == 0);
@@ -1022,12 +1051,14 @@ int compas_b200_parm_init_nphase(compas_b200_parm* p, int physics, int dim, int 
     p->cv_1 = 1.0;
     p->cv_2 = 1.0;
     p->id_lambda = 1;
-    if (physics != COMPAS_B200_FIVEEQS && physics != COMPAS_B200_SIXEQS && physics != COMPAS_B200_FIVEEQS_NPHASE)
-        return fail(COMPAS_B200_EARG, "physics must be FIVEEQS (555), SIXEQS (666) or FIVEEQS_NPHASE (55501)");
+    if (physics != COMPAS_B200_FIVEEQS && physics != COMPAS_B200_SIXEQS && physics != COMPAS_B200_FIVEEQS_NPHASE &&
+        physics != COMPAS_B200_SIXEQS_IE_NPHASE)
+        return fail(COMPAS_B200_EARG, "physics must be FIVEEQS (555), SIXEQS (666), FIVEEQS_NPHASE (55501) or "
+                                      "SIXEQS_IE_NPHASE (66601)");
     if (dim != 2 && dim != 3) return fail(COMPAS_B200_EARG, "dim must be 2 or 3");
-    if (physics == COMPAS_B200_FIVEEQS_NPHASE && (nphase < 2 || nphase > kMaxPhases))
-        return fail(COMPAS_B200_EARG, "FIVEEQS_NPHASE: nphase must be in [2, " + std::to_string(kMaxPhases) + "]");
-    if (physics != COMPAS_B200_FIVEEQS_NPHASE && nphase != 2)
+    if (nphase_model(physics) && (nphase < 2 || nphase > kMaxPhases))
+        return fail(COMPAS_B200_EARG, "the N-phase models: nphase must be in [2, " + std::to_string(kMaxPhases) + "]");
+    if (!nphase_model(physics) && nphase != 2)
         return fail(COMPAS_B200_EARG, "the two-phase models have nphase = 2");
     return compas_b200_parm_finalize(p);
 }
@@ -1109,7 +1140,7 @@ int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value
         p->eos = ix;
         return 0;
     }
-    if (p->physics == COMPAS_B200_FIVEEQS_NPHASE) {
+    if (nphase_model(p->physics)) {
         // per-phase lists (source/Parm.cpp:66-92): exactly NPHASE values
         struct LKey { const char* name; double* dst; };
         const LKey lkeys[] = {{"prob.EOS.gamma", p->gamma_k}, {"prob.EOS.pinf", p->pinf_k},
@@ -1236,10 +1267,10 @@ int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value
 
 int compas_b200_parm_finalize(compas_b200_parm* p) {
     if (!p) return fail(COMPAS_B200_EARG, "null parm");
-    if (p->physics == COMPAS_B200_FIVEEQS_NPHASE) {
-        // source/Parm.cpp:185-253
+    if (nphase_model(p->physics)) {
+        // source/Parm.cpp:185-253 (FIVEEQS_NPHASE), :364-446 (SIXEQS_IE_NPHASE, the same coefficients)
         const int np = p->nphase;
-        if (np < 2 || np > kMaxPhases) return fail(COMPAS_B200_EARG, "FIVEEQS_NPHASE: nphase out of range");
+        if (np < 2 || np > kMaxPhases) return fail(COMPAS_B200_EARG, "the N-phase models: nphase out of range");
         for (int k = 0; k < np; ++k) {
             if (!(p->gamma_k[k] > 1.0))
                 return fail(COMPAS_B200_EARG, "prob.EOS.EOS requires gamma > 1, but prob.EOS.gamma[" +
@@ -1349,7 +1380,7 @@ int compas_b200_pf_compute_dUdt(const compas_b200_parm* p, const compas_b200_geo
     if (rc) return rc;
     if (p->id_bound)
         return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field step with FiniteVolume.ID_Bound = 1 is not in this engine");
-    if (p->physics == COMPAS_B200_FIVEEQS_NPHASE)
+    if (nphase_model(p->physics))
         return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field right-hand side is the two-phase models'");
     if (!U || !dUdt || !gq0 || !gq1 || (p->dim == 3 && !gq2)) return fail(COMPAS_B200_EARG, "null argument");
     StageArgs a = base_args(p, g);
@@ -1369,7 +1400,7 @@ int compas_b200_pf_rk3_stage(const compas_b200_parm* p, const compas_b200_geom* 
     if (rc) return rc;
     if (p->id_bound)
         return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field step with FiniteVolume.ID_Bound = 1 is not in this engine");
-    if (p->physics == COMPAS_B200_FIVEEQS_NPHASE)
+    if (nphase_model(p->physics))
         return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field right-hand side is the two-phase models'");
     if (stage < 0 || stage > 2) return fail(COMPAS_B200_EARG, "stage must be 0, 1 or 2");
     if (!Us || !Unew || !dt_dev || (stage > 0 && !Uold) || !gq0 || !gq1 || (p->dim == 3 && !gq2))
@@ -1394,7 +1425,7 @@ int compas_b200_pf_grad_q(const compas_b200_parm* p, const compas_b200_geom* g, 
     if (rc) return rc;
     if (p->id_bound)
         return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field step with FiniteVolume.ID_Bound = 1 is not in this engine");
-    if (p->physics == COMPAS_B200_FIVEEQS_NPHASE)
+    if (nphase_model(p->physics))
         return fail(COMPAS_B200_EUNSUPPORTED, "the Phase-Field step is the two-phase models'");
     if (!U || !gq0 || !gq1 || (p->dim == 3 && !gq2)) return fail(COMPAS_B200_EARG, "null argument");
     if (!(dt > 0.0)) return fail(COMPAS_B200_EARG, "dt must be positive");
@@ -2053,7 +2084,7 @@ int compas_b200_energy_bound_min(const compas_b200_parm* p, const compas_b200_ge
     int rc = check_args(p, g);
     if (rc) return rc;
     if (!U || !min_dev) return fail(COMPAS_B200_EARG, "null argument");
-    if (p->physics == COMPAS_B200_SIXEQS)
+    if (p->physics == COMPAS_B200_SIXEQS || p->physics == COMPAS_B200_SIXEQS_IE_NPHASE)
         return fail(COMPAS_B200_EUNSUPPORTED, "the energy bound is this engine's for FIVEEQS and FIVEEQS_NPHASE");
     cudaStream_t st = (cudaStream_t)stream;
     const Grid G = make_grid(p, g);
@@ -2150,6 +2181,8 @@ int compas_b200_batch_create_nphase(int physics, int dim, int nphase, int id_lim
     if (rc) return rc;
     if (physics == COMPAS_B200_FIVEEQS_NPHASE && !nphase_built(dim, nphase))
         return fail(COMPAS_B200_EUNSUPPORTED, "FIVEEQS_NPHASE batches: NPHASE 2, 3, 4 in 2D and 3 in 3D");
+    if (physics == COMPAS_B200_SIXEQS_IE_NPHASE)
+        return fail(COMPAS_B200_EUNSUPPORTED, "SIXEQS_IE_NPHASE runs on the level API, not in a batch");
     if (id_limiter != 5 && id_limiter != 6) return fail(COMPAS_B200_EUNSUPPORTED, "WENO5 (5) or WENO5B (6)");
     if (precision != 0 && precision != 1) return fail(COMPAS_B200_EARG, "precision 0 or 1");
     if (capacity < 1 || capacity > (1 << 20)) return fail(COMPAS_B200_EARG, "capacity out of range");
@@ -2433,7 +2466,7 @@ int compas_b200_tag_cells(const compas_b200_parm* p, const compas_b200_geom* g, 
     if (!U || !tags) return fail(COMPAS_B200_EARG, "null state or tag array");
     if (ncriteria < 0 || ncriteria > kMaxTagCriteria || (ncriteria > 0 && !criteria))
         return fail(COMPAS_B200_EARG, "between 0 and " + std::to_string(kMaxTagCriteria) + " tagging criteria");
-    if (p->physics == COMPAS_B200_FIVEEQS_NPHASE)
+    if (nphase_model(p->physics))
         return fail(COMPAS_B200_EUNSUPPORTED, "refinement tagging: FIVEEQS and SIXEQS");
     if (g->ng < 2) return fail(COMPAS_B200_EARG, "refinement tagging needs two ghost cells");
     const int nderived = (p->physics == COMPAS_B200_SIXEQS) ? 21 : 18;
@@ -2479,7 +2512,7 @@ int compas_b200_derive(const compas_b200_parm* p, const compas_b200_geom* g, con
     if (rc) return rc;
     if (!U || !out || (nvars > 0 && (!vars || !derived))) return fail(COMPAS_B200_EARG, "null argument");
     if (nvars < 0 || nvars > kMaxDerive) return fail(COMPAS_B200_EARG, "between 0 and 32 variables");
-    if (p->physics == COMPAS_B200_FIVEEQS_NPHASE)
+    if (nphase_model(p->physics))
         return fail(COMPAS_B200_EUNSUPPORTED, "derived variables: FIVEEQS and SIXEQS");
     if (g->ng < 2) return fail(COMPAS_B200_EARG, "derived variables need two ghost cells");
     const int nderived = (p->physics == COMPAS_B200_SIXEQS) ? 21 : 18;

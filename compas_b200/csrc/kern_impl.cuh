@@ -93,8 +93,8 @@ static cudaError_t launch_stage_var(const KernelChoice& k, const StageArgs& a, c
             }
         }
     }
-    if constexpr (M::KIND == kModelFiveN) {
-        // FIVEEQS_NPHASE: the plain hyperbolic right-hand side only
+    if constexpr (M::KIND == kModelFiveN || M::KIND == kModelSixN) {
+        // FIVEEQS_NPHASE, SIXEQS_IE_NPHASE: the plain hyperbolic right-hand side only
         if (k.phase_field || k.thinc) return cudaErrorNotSupported;
     } else {
         // the THINC and Phase-Field variants run at shape 0

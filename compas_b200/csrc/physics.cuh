@@ -69,7 +69,7 @@ struct Eos {
 };
 
 // Model families of the stage kernel (the M::KIND of each model struct).
-enum { kModelFive = 0, kModelSix = 1, kModelFiveN = 2 };
+enum { kModelFive = 0, kModelSix = 1, kModelFiveN = 2, kModelSixN = 3 };
 
 // NASG: phi = alpha - b alpha rho (alpha when b = 0); covolume violation 1 - b rho <= 0 is reported
 // through the status word where the reference aborts.

@@ -34,6 +34,7 @@ struct FiveEqN {
     static constexpr int N = 2 * NPH + DIM + 1;
     static constexpr int NC = 1;             // FluxNC[0] = u*_n
     static constexpr int NCPF = 1;           // (no Phase-Field step in this engine)
+    static constexpr int IR = 0;             // alpha_k rho_k at IR + k
     static constexpr int IM = NPH;           // rho u_d (u_d among the primitives)
     static constexpr int IE = NPH + DIM;     // rho E (p among the primitives)
     static constexpr int IA = NPH + DIM + 1; // alpha_1; alpha_k at IA + k

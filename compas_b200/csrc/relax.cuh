@@ -22,15 +22,19 @@ constexpr int kPathModel = 0, kPathSolve = 1, kPathOneActive = 2, kPathNoActive 
 
 __device__ __forceinline__ bool finite_d(double x) { return (x == x) && (fabs(x) <= DBL_MAX); }
 
-// Safeguarded relaxation of two phases: returns the path; AlphaR holds the relaxed volume fractions.
-__device__ __forceinline__ int relax_safeguarded2(double AlphaR[2], const double Alpha[2], const double Alpha_rho[2],
-                                               const double Phi[2], const double Pi[2], const double A[2],
-                                               const double B[2], double trace) {
-    double c[2], dd[2], pinf[2], shift[2] = {0.0, 0.0};
-    bool active[2];
+// Safeguarded relaxation of NP phases (RelaxPressure_Safeguarded<N>): returns the path; AlphaR holds the
+// relaxed volume fractions.
+template <int NP>
+__device__ __forceinline__ int relax_safeguarded(double* AlphaR, const double* Alpha, const double* Alpha_rho,
+                                                const double* Phi, const double* Pi, const double* A,
+                                                const double* B, double trace) {
+    double c[NP], dd[NP], pinf[NP], shift[NP];
+    bool active[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) shift[k] = 0.0;
     int n_active = 0;
     double pinf_m = DBL_MAX;
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < NP; ++k) {
         const double gamma = (A[k] + 1.0) / A[k];
         pinf[k] = B[k] / (A[k] + 1.0);
         c[k] = (Pi[k] + Phi[k] * pinf[k]) / gamma;
@@ -43,19 +47,19 @@ __device__ __forceinline__ int relax_safeguarded2(double AlphaR[2], const double
         }
     }
     double S_passive = 0.0;
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < NP; ++k) {
         AlphaR[k] = Alpha[k];
         if (!active[k]) S_passive += Alpha[k];
     }
     const double V = 1.0 - S_passive;
     if (n_active == 0) return kPathNoActive;
     if (n_active == 1) {
-        for (int k = 0; k < 2; ++k)
+        for (int k = 0; k < NP; ++k)
             if (active[k]) AlphaR[k] = V;
         return kPathOneActive;
     }
     double S = 0.0, Dsum = 0.0, S_Phi = 0.0, S_Pi = 0.0;
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < NP; ++k) {
         if (active[k]) {
             S += Alpha[k];
             Dsum += dd[k];
@@ -69,19 +73,19 @@ __device__ __forceinline__ int relax_safeguarded2(double AlphaR[2], const double
 
     auto g = [&](double x) {
         double r = g_inf;
-        for (int k = 0; k < 2; ++k)
+        for (int k = 0; k < NP; ++k)
             if (active[k]) r += c[k] / (x + shift[k]);
         return r;
     };
     auto g_scale = [&](double x) {
         double r = fabs(g_inf);
-        for (int k = 0; k < 2; ++k)
+        for (int k = 0; k < NP; ++k)
             if (active[k]) r += c[k] / (x + shift[k]);
         return r;
     };
     auto dg = [&](double x) {
         double r = 0.0;
-        for (int k = 0; k < 2; ++k)
+        for (int k = 0; k < NP; ++k)
             if (active[k]) {
                 const double y = x + shift[k];
                 r -= (c[k] / y) / y;
@@ -138,9 +142,16 @@ __device__ __forceinline__ int relax_safeguarded2(double AlphaR[2], const double
             if (step <= kRelaxRelTol * x || fabs(gx) <= kRelaxResTol * g_scale(x)) break;
         }
     }
-    for (int k = 0; k < 2; ++k)
+    for (int k = 0; k < NP; ++k)
         if (active[k]) AlphaR[k] = (Alpha[k] - dd[k]) + c[k] / (x + shift[k]);
     return kPathSolve;
+}
+
+// The two-phase instance (SixEq<D>).
+__device__ __forceinline__ int relax_safeguarded2(double AlphaR[2], const double Alpha[2], const double Alpha_rho[2],
+                                               const double Phi[2], const double Pi[2], const double A[2],
+                                               const double B[2], double trace) {
+    return relax_safeguarded<2>(AlphaR, Alpha, Alpha_rho, Phi, Pi, A, B, trace);
 }
 
 // Relax the state U of one cell in place (SixEq<D> layout). FAST (the mixed form): the same FP64

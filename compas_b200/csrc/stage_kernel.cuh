@@ -24,6 +24,7 @@
 #include "physics.cuh"
 #include "physics_nphase.cuh"
 #include "relax.cuh"
+#include "physics_sixn.cuh"
 #include "tma.cuh"
 
 #include <type_traits>
@@ -132,7 +133,7 @@ __device__ __forceinline__ void riemann_llf_hll(int hll, double* Fout, double* f
     M::flux(FL, UL, WL, d);
     M::flux(FR, UR, WR, d);
     double cL, cR;
-    if constexpr (M::KIND == kModelSix) {
+    if constexpr (M::KIND == kModelSix || M::KIND == kModelSixN) {
         cL = M::sound_speed(WL, e, err);
         cR = M::sound_speed(WR, e, err);
     } else {
@@ -242,12 +243,12 @@ __device__ __forceinline__ void llf_hll_mixed(int hll, double* Fout, double* fnc
 template <class M, class PT, class G>
 __device__ __forceinline__ void weno3b_faces(G g, int side, PT* Wf) {
     PT rf[M::NP], af[M::NP];
-    if constexpr (M::KIND == kModelFiveN) {
-        bounded_phases<M::NP, 3, PT>([&](int k, int s) { return (PT)g(s, k); },
+    if constexpr (M::KIND == kModelFiveN || M::KIND == kModelSixN) {
+        bounded_phases<M::NP, 3, PT>([&](int k, int s) { return (PT)g(s, M::IR + k); },
                                      [&](int k, int s) { return (PT)g(s, M::IA + k); }, side, rf, af);
 #pragma unroll
         for (int k = 0; k < M::NP; ++k) {
-            Wf[k] = rf[k];
+            Wf[M::IR + k] = rf[k];
             Wf[M::IA + k] = af[k];
         }
     } else {
@@ -264,11 +265,28 @@ __device__ __forceinline__ void weno3b_faces(G g, int side, PT* Wf) {
     }
 }
 
+// WENO5B: the components reconstructed with plain WENO5 ([lo, hi)); the masses and volume fractions
+// outside that range are bounded.
+template <class M>
+__host__ __device__ constexpr int weno5b_plain_lo() {
+    if constexpr (M::KIND == kModelSixN) return M::IP;
+    else return M::IM;
+}
+template <class M>
+__host__ __device__ constexpr int weno5b_plain_hi() {
+    if constexpr (M::KIND == kModelSixN) return M::N;
+    else return M::IA;
+}
+
 template <class M>
 __device__ __forceinline__ void riemann(int id_riemann, double* Fout, double* fnc, double& cmax, const double* UL,
                                         const double* UR, const Eos& e, int d, int id_k, unsigned int* err) {
     if (id_riemann == 2) M::hllc(Fout, fnc, cmax, UL, UR, e, d, id_k, err);
-    else riemann_llf_hll<M>(id_riemann, Fout, fnc, cmax, UL, UR, e, d, id_k, err);
+    else if constexpr (M::KIND == kModelSixN) {
+        // the N-phase six-equation LLF takes the face's cmax as its dissipation speed
+        if (id_riemann == 0) M::llf(Fout, fnc, cmax, UL, UR, e, d, err);
+        else riemann_llf_hll<M>(1, Fout, fnc, cmax, UL, UR, e, d, id_k, err);
+    } else riemann_llf_hll<M>(id_riemann, Fout, fnc, cmax, UL, UR, e, d, id_k, err);
 }
 
 }  // namespace compas
@@ -336,8 +354,11 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
     static_assert(!TMA || (M::D == 3 && MIX), "TMA halo staging: the 3D mixed form");
     static_assert(!PFX || M::KIND != kModelFiveN, "the Phase-Field kernel is the two-phase models'");
     static_assert(M::KIND != kModelFiveN || !TH, "FIVEEQS_NPHASE runs without THINC");
+    static_assert(M::KIND != kModelSixN || (VAR == kVarPlain && !MIX),
+                  "SIXEQS_IE_NPHASE: the plain hyperbolic right-hand side in FP64");
     static_assert(SCHEME != 2 || (VAR == kVarPlain && !TH), "GODUNOV / MUSCL: the plain right-hand side");
     constexpr bool NPH = (M::KIND == kModelFiveN);
+    constexpr bool SXN = (M::KIND == kModelSixN);
     using PT = typename std::conditional<MIX, float, double>::type;
     using T = TileShape<M, TX, TY, TZ, PT, TMA, PFX>;
     constexpr int N = M::N, NC = PFX ? M::NCPF : M::NC, D = M::D, NB = T::NB;
@@ -559,8 +580,10 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                 str[s] = CSTR;
             }
             double WfL[N], WfR[N], UL[N], UR[N];
-            constexpr int NB0 = (SCHEME == 6) ? M::IM : 0;    // first plainly reconstructed component
-            constexpr int NB1 = (SCHEME == 6) ? M::IA : N;    // one past the last
+            // first plainly reconstructed component and one past the last (WENO5B: all but the
+            // bounded masses and volume fractions)
+            constexpr int NB0 = (SCHEME == 6) ? weno5b_plain_lo<M>() : 0;
+            constexpr int NB1 = (SCHEME == 6) ? weno5b_plain_hi<M>() : N;
             double F[N], fnc[NC], cm;
             bool thinc_face = false;
             if constexpr (TH)
@@ -568,18 +591,18 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                                                       UR, err);
             if constexpr (!MIX) {
                 if (!thinc_face) {
-                    if constexpr (SCHEME == 6 && NPH) {
+                    if constexpr (SCHEME == 6 && (NPH || SXN)) {
                         double rf[M::NP], af[M::NP];
-                        auto rl = [&](int k, int s) { return (double)smem[off[s] + k * str[s]]; };
+                        auto rl = [&](int k, int s) { return (double)smem[off[s] + (M::IR + k) * str[s]]; };
                         auto al_ = [&](int k, int s) { return (double)smem[off[s] + (M::IA + k) * str[s]]; };
                         bounded_phases<M::NP, 5, double>(rl, al_, 1, rf, af);
 #pragma unroll
-                        for (int k = 0; k < M::NP; ++k) { WfL[k] = rf[k]; WfL[M::IA + k] = af[k]; }
-                        auto rr = [&](int k, int s) { return (double)smem[off[s + 1] + k * str[s + 1]]; };
+                        for (int k = 0; k < M::NP; ++k) { WfL[M::IR + k] = rf[k]; WfL[M::IA + k] = af[k]; }
+                        auto rr = [&](int k, int s) { return (double)smem[off[s + 1] + (M::IR + k) * str[s + 1]]; };
                         auto ar_ = [&](int k, int s) { return (double)smem[off[s + 1] + (M::IA + k) * str[s + 1]]; };
                         bounded_phases<M::NP, 5, double>(rr, ar_, -1, rf, af);
 #pragma unroll
-                        for (int k = 0; k < M::NP; ++k) { WfR[k] = rf[k]; WfR[M::IA + k] = af[k]; }
+                        for (int k = 0; k < M::NP; ++k) { WfR[M::IR + k] = rf[k]; WfR[M::IA + k] = af[k]; }
                     } else if constexpr (SCHEME == 6) {
                         double r1[6], r2[6], al[6];
 #pragma unroll
@@ -621,6 +644,11 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                     if constexpr (NPH && SCHEME != 6) if (SCHEME != 2 || a.muscl != 11) {
                         // N-phase WENO5 / three-cell schemes: the consistent limiter about the stencil
                         // centres f-1 and f (WENO5B bounds its face values instead)
+                        M::consistent_limit(UL, smem + off[2], str[2], dxd, 1, a.e, err);
+                        M::consistent_limit(UR, smem + off[3], str[3], dxd, -1, a.e, err);
+                    }
+                    if constexpr (SXN && SCHEME == 2) if (a.muscl >= 1 && a.muscl < 10) {
+                        // N-phase six-equation: the consistent limiter after MUSCL only
                         M::consistent_limit(UL, smem + off[2], str[2], dxd, 1, a.e, err);
                         M::consistent_limit(UR, smem + off[3], str[3], dxd, -1, a.e, err);
                     }
@@ -816,6 +844,16 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                 M::kapila_factors(fac, W, a.e, a.id_k, err);
 #pragma unroll
                 for (int k = 0; k < M::NP; ++k) L[M::IA + k] = L[M::IA + k] + fac[k] * acc[r][N];
+            } else if constexpr (SXN) {
+                // N-phase six-equation: alpha_k += alpha_k div u*, alpha_k rho_k e_k -= alpha_k p_k div u*
+                // (FVM_SurfaceIntegralNC_Compressible6Eq_IE_NPhase.H; acc holds +div u*, the reference
+                // subtracts alpha_k times its negative)
+                const double divv = acc[r][N];
+#pragma unroll
+                for (int k = 0; k < M::NP; ++k) {
+                    L[M::IA + k] = L[M::IA + k] + W[M::IA + k] * divv;
+                    L[M::IP + k] = L[M::IP + k] - W[M::IP + k] * divv;
+                }
             } else {
                 // six-equation: phase energy exchange and alpha1 div u (FVM_SurfaceIntegralNC_Compressible6Eq.H)
                 const double divv = acc[r][N], dva1 = acc[r][N + 1], dva2 = acc[r][N + 2];
@@ -847,6 +885,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                 }
                 if constexpr (M::KIND == kModelSix) {
                     if (a.relax) relax_pressure<D, MIX>(out, a.e, a.trace, err);
+                } else if constexpr (SXN) {
+                    if (a.relax) M::relax(out, a.e, a.trace, err);
                 }
                 bool bad = false;
 #pragma unroll

@@ -45,13 +45,16 @@ extern "C" {
 #define COMPAS_B200_FIVEEQS 555 /* include/Macros.H:56 */
 #define COMPAS_B200_SIXEQS 666  /* include/Macros.H:57 */
 #define COMPAS_B200_FIVEEQS_NPHASE 55501 /* include/Macros.H:58: N-phase five-equation model */
+#define COMPAS_B200_SIXEQS_IE_NPHASE 66601 /* include/Macros.H:59: N-phase six-equation model, internal-energy
+                                             * form (plain FP64, single-level API; NPHASE 2, 3 in 2D, 3 in 3D) */
 #define COMPAS_B200_MAX_PHASES 4         /* largest NPHASE this build instantiates */
 
 /* Parameters of the hot path: the fields of the reference's `struct Parm`
  * (exec/_Tests/Advection/prob/Parm.H:33-117) that the right-hand side reads, plus the run keys of
  * the level advance. Fill with compas_b200_parm_init, then compas_b200_parm_set per inputs key. */
 typedef struct compas_b200_parm {
-    int physics;          /* COMPAS_B200_FIVEEQS, COMPAS_B200_SIXEQS or COMPAS_B200_FIVEEQS_NPHASE */
+    int physics;          /* COMPAS_B200_FIVEEQS, COMPAS_B200_SIXEQS, COMPAS_B200_FIVEEQS_NPHASE or
+                           * COMPAS_B200_SIXEQS_IE_NPHASE */
     int dim;              /* 2 or 3 (AMREX_SPACEDIM) */
     /* prob.EOS.* (source/Parm.cpp:101-188): raw inputs and the derived partial-form coefficients */
     int eos;              /* 0 ideal gas, 1 stiffened gas, 3 NASG */
@@ -94,9 +97,10 @@ typedef struct compas_b200_parm {
     double pf_cfl;            /* PhaseField.cfl */
     int pf_max_step;          /* PhaseField.max_step */
     double pf_tol_rel;        /* LinearSystem.tol_rel */
-    /* FIVEEQS_NPHASE: the number of phases (the reference's compile-time NPHASE; 2 for the two-phase
-     * models) and the per-phase lists prob.EOS.gamma/pinf/b/q with their partial-form coefficients
-     * (source/Parm.cpp:185-262); the A1..D2 fields above are not used by this model */
+    /* FIVEEQS_NPHASE, SIXEQS_IE_NPHASE: the number of phases (the reference's compile-time NPHASE; 2 for
+     * the two-phase models) and the per-phase lists prob.EOS.gamma/pinf/b/q with their partial-form
+     * coefficients (source/Parm.cpp:185-262, :364-446); the A1..D2 fields above are not used by these
+     * models */
     int nphase;
     double gamma_k[COMPAS_B200_MAX_PHASES], pinf_k[COMPAS_B200_MAX_PHASES];
     double b_k[COMPAS_B200_MAX_PHASES], q_k[COMPAS_B200_MAX_PHASES];
@@ -148,8 +152,9 @@ typedef struct compas_b200_geom {
  * reference's default (include/Macros.H:83-85). */
 int compas_b200_parm_init(compas_b200_parm* p, int physics, int dim);
 
-/* The same with the number of phases of FIVEEQS_NPHASE (2 <= nphase <= COMPAS_B200_MAX_PHASES; this
- * build instantiates the N-phase kernels for nphase 2, 3, 4 in 2D and 3 in 3D). For the two-phase
+/* The same with the number of phases of FIVEEQS_NPHASE or SIXEQS_IE_NPHASE (2 <= nphase <=
+ * COMPAS_B200_MAX_PHASES; this build instantiates the FIVEEQS_NPHASE kernels for nphase 2, 3, 4 in 2D
+ * and 3 in 3D, the SIXEQS_IE_NPHASE kernels for nphase 2, 3 in 2D and 3 in 3D). For the two-phase
  * models nphase must be 2. */
 int compas_b200_parm_init_nphase(compas_b200_parm* p, int physics, int dim, int nphase);
 
@@ -157,7 +162,7 @@ int compas_b200_parm_init_nphase(compas_b200_parm* p, int physics, int dim, int 
  * ("Physics.RiemannSolver", "HLLC"), ("prob.EOS.gamma_2", "4.4"), ("run.cfl", "0.5"). Unknown keys
  * or values return COMPAS_B200_EARG with the valid values in compas_b200_last_error(), where the
  * reference aborts (e.g. include/Operators_FV/FiniteVolume_Parameter.H:143-146). EOS keys take
- * effect at compas_b200_parm_finalize. FIVEEQS_NPHASE takes the per-phase lists
+ * effect at compas_b200_parm_finalize. FIVEEQS_NPHASE and SIXEQS_IE_NPHASE take the per-phase lists
  * ("prob.EOS.gamma", "1.4 1.5 1.5"), "prob.EOS.pinf", "prob.EOS.b", "prob.EOS.q" with exactly
  * nphase values each (source/Parm.cpp:82-92). */
 int compas_b200_parm_set(compas_b200_parm* p, const char* key, const char* value);
@@ -193,7 +198,7 @@ int compas_b200_fill_boundary(const compas_b200_parm* p, const compas_b200_geom*
 int compas_b200_compute_dUdt(const compas_b200_parm* p, const compas_b200_geom* g, const double* U, double* dUdt,
                              double* cmax_dev, unsigned int* err_dev, void* stream);
 
-/* Number of non-conservative face terms of the model: 1 for FIVEEQS and FIVEEQS_NPHASE (the face
+/* Number of non-conservative face terms of the model: 1 for FIVEEQS, FIVEEQS_NPHASE and SIXEQS_IE_NPHASE (the face
  * velocity u*), 3 for SIXEQS (u, u a1p1, u a2p2) - NC_TERMS of include/Macros.H, the component
  * count of the reference's fluxes_nc (source/Class_Compressible_PhaseField.cpp:3127-3143). */
 int compas_b200_nc_terms(const compas_b200_parm* p);

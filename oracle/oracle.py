@@ -22,7 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 PORT_LIB = os.path.join(HERE, "liboracle.so")
 
-FIVEEQS, SIXEQS, FIVEEQS_NPHASE = 555, 666, 55501
+FIVEEQS, SIXEQS, FIVEEQS_NPHASE, SIXEQS_IE_NPHASE = 555, 666, 55501, 66601
 
 
 class Case(ctypes.Structure):
@@ -140,6 +140,8 @@ _cache: dict = {}
 def ref_lib_path(physics: int, dim: int, nphase: int = 2) -> str:
     if physics == FIVEEQS_NPHASE:
         return os.path.join(REF_DIR, f"libref_5eqn{nphase}_{dim}d.so")
+    if physics == SIXEQS_IE_NPHASE:
+        return os.path.join(REF_DIR, f"libref_6eqn{nphase}_{dim}d.so")
     model = "5eq" if physics == FIVEEQS else "6eq"
     return os.path.join(REF_DIR, f"libref_{model}_{dim}d.so")
 
@@ -196,7 +198,7 @@ def case_from(parm, geom) -> Case:
     c.amr_interp = getattr(parm, "amr_interp", 0)
     c.id_bound = getattr(parm, "id_bound", 0)
     c.id_lambda = getattr(parm, "id_lambda", 1)
-    if parm.physics == FIVEEQS_NPHASE:
+    if parm.physics in (FIVEEQS_NPHASE, SIXEQS_IE_NPHASE):
         for k in range(4):
             c.Ak[k], c.Bk[k], c.Ck[k], c.Dk[k] = parm.Ak[k], parm.Bk[k], parm.Ck[k], parm.Dk[k]
     return c

@@ -22,7 +22,8 @@ extern "C" {
 #endif
 
 typedef struct cmp_case {
-    int physics;        /* 555 FIVEEQS, 666 SIXEQS, 55501 FIVEEQS_NPHASE (include/Macros.H:56-59) */
+    int physics;        /* 555 FIVEEQS, 666 SIXEQS, 55501 FIVEEQS_NPHASE, 66601 SIXEQS_IE_NPHASE
+                         * (include/Macros.H:56-59; the last in the reference build only) */
     int dim;            /* 2 or 3 */
     int n[3];           /* valid cells per direction (n[2] = 1 in 2D) */
     int ng;             /* ghost cells (3 for WENO5/WENO5B) */
@@ -34,15 +35,15 @@ typedef struct cmp_case {
     int id_weno;        /*   with id_weno 0, 0 GODUNOV, 1 MUSCL(-Minmod), 2 -vanLeer, 3 -Superbee, 4 -MC */
     int id_riemann;     /* Physics.RiemannSolver: 0 LLF, 1 HLL, 2 HLLC */
     int source_term;    /* FIVEEQS Physics.source_term (K term): 0 or 1 */
-    int relaxation;     /* SIXEQS Physics.pressure_relaxation: 0 or 1 */
-    double relax_trace; /* SIXEQS Physics.pressure_relaxation_trace */
+    int relaxation;     /* SIXEQS, SIXEQS_IE_NPHASE Physics.pressure_relaxation: 0 or 1 */
+    double relax_trace; /* SIXEQS, SIXEQS_IE_NPHASE Physics.pressure_relaxation_trace */
     int thinc;          /* FiniteVolume.THINC: 0 or 1 */
     int thinc_use_normal;
     double thinc_eps, thinc_beta, thinc_normal_threshold;
     double cfl;         /* run.cfl */
     int change_limiter; /* run.timestep_change_limiter */
-    int nphase;         /* FIVEEQS_NPHASE (55501): phases (the build's NPHASE); 2 otherwise */
-    double Ak[4], Bk[4], Ck[4], Dk[4];  /* FIVEEQS_NPHASE EOS coefficients per phase (source/Parm.cpp:185-253) */
+    int nphase;         /* FIVEEQS_NPHASE, SIXEQS_IE_NPHASE: phases (the build's NPHASE); 2 otherwise */
+    double Ak[4], Bk[4], Ck[4], Dk[4];  /* the N-phase models' EOS coefficients per phase (source/Parm.cpp:185-253) */
     int amr_interp;     /* amr.Interpolater of the multi-level advance: 0 lincc_interp, 1 pc_interp */
     int id_bound;       /* FiniteVolume.ID_Bound (FiniteVolume_Parameter.H:45): 1 the bound-preserving branch and
                          * the energy check of every stage with the step taken again (FIVEEQS) */
@@ -66,7 +67,7 @@ int cmp_compute_dudt(const cmp_case* c, const double* U, double* dUdt, double* c
 int cmp_energy_bound_min(const cmp_case* c, const double* U, double* out);
 int cmp_bound_restarts(void);
 
-/* Pressure relaxation of the valid cells of U in place (SIXEQS; no-op otherwise). */
+/* Pressure relaxation of the valid cells of U in place (SIXEQS, SIXEQS_IE_NPHASE; no-op otherwise). */
 int cmp_relax(const cmp_case* c, double* U);
 
 /* One TVD-RK3 step of size dt on U (valid cells in, valid cells out; ghosts are scratch).

@@ -28,6 +28,16 @@
 #include <Operators_FV.H>
 #include <Operators_FD.H>
 #include <Operators_Compressible5Eq_NPhase.H>
+#elif (PHYSICS == SIXEQS_IE_NPHASE)
+#include <Physics_Compressible_NPhase.H>
+#include <Physics_Compressible6Eq_IE_NPhase.H>
+#include <Operators_FV.H>
+#include <Operators_FD.H>
+// the model's operator aggregator also pulls in its Phase-Field flux functor
+#include <Physics_PhaseField.H>
+#include <Physics_Compressible_NPhase_PhaseField.H>
+#include <Physics_Compressible6Eq_IE_NPhase_PhaseField.H>
+#include <Operators_Compressible6Eq_IE_NPhase.H>
 #else
 #include <Physics_Compressible_TwoPhase.H>
 #endif
@@ -96,12 +106,19 @@ struct Geo {
 Parm make_parm(const cmp_case* c) {
     Parm p;
     p.EOS = 1;
-#if (PHYSICS == FIVEEQS_NPHASE)
+#if (PHYSICS == FIVEEQS_NPHASE || PHYSICS == SIXEQS_IE_NPHASE)
     if (c->nphase != NPHASE) amrex::Abort("the case's nphase differs from this build's NPHASE");
     for (int k = 0; k < NPHASE; ++k) {
         p.A[k] = c->Ak[k]; p.B[k] = c->Bk[k]; p.C[k] = c->Ck[k]; p.D[k] = c->Dk[k];
-        // source/Parm.cpp:255-261
+        // source/Parm.cpp:255-261 (FIVEEQS_NPHASE), :446-450 (SIXEQS_IE_NPHASE: -B/(A + 1))
+#if (PHYSICS == SIXEQS_IE_NPHASE)
+        p.p_min[k] = -c->Bk[k] / (c->Ak[k] + 1.0);
+        // the relaxation's NASG branch is taken for EOS = 3 with a covolume or heat of formation
+        // (PressureRelaxation_IsNASG); the EOS 0 and 1 coefficients have C = D = 0
+        if (c->Ck[k] > 0.0 || c->Dk[k] != 0.0) p.EOS = 3;
+#else
         p.p_min[k] = (c->source_term == 1) ? -c->Bk[k] / (c->Ak[k] + 1.0) : -c->Bk[k] / c->Ak[k];
+#endif
     }
 #else
     p.A1 = c->A1; p.A2 = c->A2; p.B1 = c->B1; p.B2 = c->B2;
@@ -151,6 +168,9 @@ Parm make_parm(const cmp_case* c) {
     p.Physics_Parm.pressure_relaxation = c->relaxation;
     p.Physics_Parm.pressure_relaxation_trace = c->relax_trace;
     p.Physics_Parm.relaxation = c->relaxation;
+#elif (PHYSICS == SIXEQS_IE_NPHASE)
+    p.Physics_Parm.pressure_relaxation = c->relaxation;
+    p.Physics_Parm.pressure_relaxation_trace = c->relax_trace;
 #endif
     return p;
 }
@@ -163,6 +183,8 @@ enum { BC_INT = 0, BC_FOEXTRAP = 1, BC_EVEN = 2, BC_ODD = 3 };
 int bc_kind(int code, int n, int d) {
 #if (PHYSICS == FIVEEQS_NPHASE)
     const int m0 = NPHASE;
+#elif (PHYSICS == SIXEQS_IE_NPHASE)
+    const int m0 = 3 * NPHASE;
 #else
     const int m0 = 2;
 #endif
@@ -291,7 +313,30 @@ void compute_dudt(const cmp_case* c, const Parm& parm, const double* U, double* 
 }
 
 void relax(const cmp_case* c, const Parm& parm, double* U) {
-#if (PHYSICS == SIXEQS)
+#if (PHYSICS == SIXEQS_IE_NPHASE)
+    // PostTimeStage -> Relaxation_Pressure -> PressureRelaxationInstantaneous
+    // (source/Class_Compressible6Eq_IE_NPhase_PhaseField.cpp:46-58, :464-472): the reference's cell
+    // function on every valid cell, volume fractions and phase energies written back
+    if (!parm.Physics_Parm.pressure_relaxation) return;
+    const bool NASG = PressureRelaxation_IsNASG(parm);
+    Geo g(c);
+    auto a = g.view(U, NSTATE);
+#ifdef _OPENMP
+#pragma omp parallel for collapse(2) schedule(static)
+#endif
+    for (int k = 0; k < g.nz; ++k)
+    for (int j = 0; j < g.ny; ++j)
+    for (int i = 0; i < g.nx; ++i) {
+        amrex::Array<amrex::Real, NSTATE> Cons, ConsR;
+        for (int n = 0; n < NSTATE; ++n) Cons[n] = a(i, j, k, n);
+        int Iter, Path;
+        PressureRelaxation_Cell(ConsR, Cons, parm, NASG, Iter, Path);
+        for (int ph = 0; ph < NPHASE; ++ph) {
+            a(i, j, k, INDEX_VolumeFraction1 + ph) = ConsR[INDEX_VolumeFraction1 + ph];
+            a(i, j, k, INDEX_Energy1 + ph) = ConsR[INDEX_Energy1 + ph];
+        }
+    }
+#elif (PHYSICS == SIXEQS)
     if (!parm.Physics_Parm.relaxation) return;
     Geo g(c);
     auto a = g.view(U, NSTATE);

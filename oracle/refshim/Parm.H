@@ -1,6 +1,7 @@
 // Test infrastructure (oracle): the per-case parameter struct that the reference's physics headers
 // take as `Parm const&`. Field names and meanings mirror exec/_Tests/Advection/prob/Parm.H:33-117
-// (the two-phase models) and exec/TriplePoint-5Eq-N/prob/Parm.H (FIVEEQS_NPHASE); the linear-solver block is left out because no hyperbolic-path function
+// (the two-phase models), exec/TriplePoint-5Eq-N/prob/Parm.H (FIVEEQS_NPHASE) and
+// exec/ShockBubble-WaterAir-6Eq-Nphase/prob/Parm.H (SIXEQS_IE_NPHASE); the linear-solver block is left out because no hyperbolic-path function
 // reads it. The oracle driver fills the fields directly (the EOS coefficients as source/Parm.cpp:
 // 101-188 computes them), so no ParmParse input is read.
 #ifndef PARM_H_
@@ -16,14 +17,17 @@
 #include <Physics_Parameter_Compressible6Eq.H>
 #elif (PHYSICS == FIVEEQS_NPHASE)
 #include <Physics_Parameter_Compressible5Eq_NPhase.H>
+#elif (PHYSICS == SIXEQS_IE_NPHASE)
+#include <Physics_Parameter_Compressible6Eq_IE_NPhase.H>
 #else
-#error "the oracle build covers FIVEEQS, SIXEQS and FIVEEQS_NPHASE"
+#error "the oracle build covers FIVEEQS, SIXEQS, FIVEEQS_NPHASE and SIXEQS_IE_NPHASE"
 #endif
 #include <FiniteVolume_Parameter.H>
 #include <PhaseField_Parameter.H>
 
-#if (PHYSICS == FIVEEQS_NPHASE)
-// The N-phase model's Parm (exec/TriplePoint-5Eq-N/prob/Parm.H): per-phase EOS arrays.
+#if (PHYSICS == FIVEEQS_NPHASE || PHYSICS == SIXEQS_IE_NPHASE)
+// The N-phase models' Parm (exec/TriplePoint-5Eq-N/prob/Parm.H,
+// exec/ShockBubble-WaterAir-6Eq-Nphase/prob/Parm.H): per-phase EOS arrays.
 struct Parm
 {
     Physics_Parameter Physics_Parm;

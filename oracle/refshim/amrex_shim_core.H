@@ -155,6 +155,27 @@ struct PrintSink {
 inline PrintSink Print(int = 0) { return PrintSink{}; }
 inline PrintSink AllPrint() { return PrintSink{}; }
 
+// Compile-only stand-ins for the host loops over whole MultiFabs that some physics headers define
+// next to their cell functions (e.g. PressureRelaxationInstantaneous of the N-phase six-equation
+// model). The oracle calls the cell functions itself; constructing an MFIter aborts.
+struct Box {};
+class MultiFab;
+class MFIter {
+public:
+    MFIter(const MultiFab&, bool) { Abort("MultiFab loops are not available in the oracle shim"); }
+    bool isValid() const { return false; }
+    MFIter& operator++() { return *this; }
+    Box tilebox() const { return Box{}; }
+};
+class MultiFab {
+public:
+    Array4<Real const> const_array(const MFIter&) const { return Array4<Real const>(); }
+    Array4<Real> array(const MFIter&) { return Array4<Real>(); }
+};
+inline bool TilingIfNotGPU() { return false; }
+template <class F>
+void ParallelFor(const Box&, F&&) {}
+
 }  // namespace amrex
 
 using amrex::operator""_rt;

@@ -143,3 +143,32 @@ def test_bound_preserving_key():
     with pytest.raises(cb.CompasError) as e:
         cb.energy_bound_min(cb.make_parm(cb.SIXEQS, 3, {}), g3, None, out=0)
     assert e.value.code in (cb.EUNSUPPORTED, cb.EARG)
+
+
+def test_sixeqs_ie_nphase_keys():
+    """SIXEQS_IE_NPHASE (include/Macros.H:59): NSTATE = 3 NPHASE + dim + 1, the per-phase EOS lists of
+    the N-phase Parm (source/Parm.cpp:364-446), pressure relaxation keys; the engine runs it in FP64
+    on the single-level API with NPHASE 2, 3 in 2D and 3 in 3D (the checks run before any device call)."""
+    inputs = {"prob.EOS.gamma": [4.4, 1.4, 1.667], "prob.EOS.pinf": [6e8, 0.0, 0.0],
+              "Physics.pressure_relaxation": 1, "Physics.pressure_relaxation_trace": 1e-3,
+              "FiniteVolume.Scheme": "MUSCL"}
+    p = cb.make_parm(cb.SIXEQS_IE_NPHASE, 2, inputs)
+    assert p.nphase == 3 and cb.parm_nstate(p) == 12 and cb.nstate(cb.SIXEQS_IE_NPHASE, 3, 3) == 13
+    assert p.relaxation == 1 and p.relax_trace == 1e-3
+    assert abs(p.Ak[0] - 1.0 / 3.4) < 1e-15 and abs(p.Bk[0] - 4.4 * 6e8 / 3.4) < 1e-6 and p.Bk[1] == 0.0
+    assert cb.nc_terms(p) == 1
+    g = cb.make_geom((16, 16, 1), (0.1, 0.1, 1.0))
+    g3 = cb.make_geom((8, 8, 8), (0.1, 0.1, 0.1))
+    bad = [(2, dict(inputs, **{"compas_b200.precision": "mixed"}), g),
+           (2, dict(inputs, **{"FiniteVolume.THINC": 1, "FiniteVolume.Scheme": "WENO5"}), g),
+           (2, dict(inputs, **{"FiniteVolume.ID_Bound": 1}), g),
+           (2, dict(inputs, **{"prob.EOS.gamma": [1.4] * 4, "prob.EOS.pinf": [0.0] * 4}), g),
+           (3, dict(inputs, **{"prob.EOS.gamma": [1.4] * 2, "prob.EOS.pinf": [0.0] * 2}), g3)]
+    for dim, inp, geom in bad:
+        q = cb.make_parm(cb.SIXEQS_IE_NPHASE, dim, inp)
+        with pytest.raises(cb.CompasError) as e:
+            cb.Level(q, geom)
+        assert e.value.code == cb.EUNSUPPORTED
+    with pytest.raises(cb.CompasError) as e:
+        cb.Batch(cb.SIXEQS_IE_NPHASE, 2, 5, 0, 4, nphase=2)
+    assert e.value.code == cb.EUNSUPPORTED

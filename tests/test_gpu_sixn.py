@@ -1,0 +1,155 @@
+"""The N-phase six-equation model in its internal-energy form (SIXEQS_IE_NPHASE) on the CUDA path
+against the reference's own headers.
+
+The model runs in plain FP64 and reproduces the reference's arithmetic: the phase pressures from the
+phase internal energies, reconstruction in primitive variables (GODUNOV, MUSCL with the consistent
+limiter of volume fractions, partial densities and phase pressures, WENO3, WENO3B, WENO5, WENO5B with
+bounded partial densities and volume fractions), the model's HLLC / HLL / LLF fluxes, the
+non-conservative terms alpha_k div u and alpha_k p_k div u, and the Newton pressure relaxation with its
+safeguarded fallback after every stage. The right-hand side, the face wave speed and whole level
+advances are compared to the bit against the reference-header oracle (oracle/_ref/libref_6eqn*); the
+asserted bound is the north star's 1e-11 relative L-infinity per field. Cases: a Mach 1.1 water shock
+on an air bubble (and a helium bubble with three phases), after the reference's
+ShockBubble-WaterAir-6Eq-Nphase example, in pressure equilibrium and out of it, with the NASG
+covolume, with a trace threshold that sends phases through the safeguarded relaxation, and in 3D.
+"""
+import numpy as np
+import pytest
+import torch
+
+import compas_b200 as cb
+from compas_b200 import cases
+from helpers import rel_linf, run_gpu
+from oracle.oracle import Oracle, have_ref
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-11
+
+SCHEMES = ["GODUNOV", "MUSCL", "MUSCL-vanLeer", "MUSCL-MC", "WENO3", "WENO3B", "WENO5", "WENO5B"]
+RIEMANN = ["HLLC", "HLL", "LLF"]
+
+CASES = {
+    "np2": dict(n=16, nphase=2),
+    "np3_dp": dict(n=16, nphase=3, dp=0.05),
+    "np2_nasg_dp": dict(n=16, nphase=2, eos=3, dp=0.05),
+    "np3_trace": dict(n=16, nphase=3, dp=0.05, trace=1e-3),
+    "np3_3d": dict(n=8, nphase=3, dim=3, dp=0.05),
+}
+
+
+def _case(**kw):
+    phys, dim, inputs, geom, U = cases.sixn_shock_bubbles(**kw)
+    p = cb.make_parm(phys, dim, inputs)
+    g = cb.make_geom(**geom)
+    if not have_ref(p.physics, p.dim, p.nphase):
+        pytest.skip("the SIXEQS_IE_NPHASE oracle is the reference build (oracle/_ref/libref_6eqn*)")
+    return p, g, U
+
+
+def _dudt_pair(p, g, U):
+    o = Oracle("reference", p, g)
+    ref = U.copy()
+    o.fill_ghosts(ref)
+    dref, cref = o.compute_dudt(ref)
+    dev = torch.device("cuda")
+    Ud = torch.from_numpy(ref).to(dev)
+    dU = torch.zeros_like(Ud)
+    cm = torch.zeros(1, dtype=torch.float64, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    cb.compute_dUdt_FV(p, g, Ud, dU, cm, err)
+    torch.cuda.synchronize()
+    return dU.cpu().numpy(), float(cm.item()), int(err.item()), dref, cref
+
+
+@pytest.mark.parametrize("riemann", RIEMANN)
+@pytest.mark.parametrize("scheme", SCHEMES)
+@pytest.mark.parametrize("name", ["np2", "np3_dp", "np3_3d"])
+def test_sixn_dudt_matches_reference(name, scheme, riemann):
+    p, g, U = _case(**CASES[name], scheme=scheme, riemann=riemann)
+    got, cm, err, dref, cref = _dudt_pair(p, g, U)
+    a, b = cb.valid_view(got, p, g), cb.valid_view(dref, p, g)
+    e = rel_linf(a, b)
+    print(f"{name} {scheme} {riemann}: dUdt rel Linf per field {np.array2string(e, precision=2)}; "
+          f"bitwise equal: {np.array_equal(a, b)}; cmax {cm!r} vs {cref!r}")
+    assert err == 0
+    assert np.all(e <= TOL), e
+    assert cm == cref
+
+
+@pytest.mark.parametrize("scheme", ["MUSCL", "WENO5", "WENO5B"])
+def test_sixn_dudt_nasg(scheme):
+    p, g, U = _case(**CASES["np2_nasg_dp"], scheme=scheme)
+    got, cm, err, dref, cref = _dudt_pair(p, g, U)
+    e = rel_linf(cb.valid_view(got, p, g), cb.valid_view(dref, p, g))
+    print(f"NASG {scheme}: rel Linf per field {np.array2string(e, precision=2)}")
+    assert err == 0
+    assert np.all(e <= TOL), e
+    assert cm == cref
+
+
+ADVANCES = [
+    ("np2", "MUSCL", "HLLC", 30),
+    ("np3_dp", "MUSCL", "HLLC", 25),
+    ("np3_dp", "WENO5B", "HLLC", 20),
+    ("np3_dp", "WENO5", "LLF", 20),
+    ("np2_nasg_dp", "MUSCL-MC", "HLL", 20),
+    ("np3_trace", "WENO3B", "HLLC", 20),
+    ("np3_3d", "MUSCL", "HLLC", 6),
+]
+
+
+@pytest.mark.parametrize("name,scheme,riemann,steps", ADVANCES,
+                         ids=[f"{a}-{b}-{c}" for a, b, c, _ in ADVANCES])
+def test_sixn_advance_matches_reference(name, scheme, riemann, steps):
+    """TVD-RK3 steps with the pressure relaxation after every stage and the CFL time step."""
+    p, g, U = _case(**CASES[name], scheme=scheme, riemann=riemann)
+    got, info, dts = run_gpu(p, g, U.copy(), steps)
+    assert info.status == 0 and info.steps == steps
+    ref = U.copy()
+    t, dts_ref = Oracle("reference", p, g).advance(ref, steps)
+    a, b = cb.valid_view(got, p, g), cb.valid_view(ref, p, g)
+    e = rel_linf(a, b)
+    print(f"{name} {scheme} {riemann}, {steps} steps: rel Linf per field {np.array2string(e, precision=2)}; "
+          f"bitwise equal: {np.array_equal(a, b)}")
+    np.testing.assert_array_equal(dts, dts_ref)
+    assert np.all(e <= TOL), e
+
+
+def test_sixn_relaxation_equalises_phase_pressures():
+    """After an advance with relaxation every phase with volume fraction above the trace threshold
+    carries the mixture pressure: alpha_k p_k / alpha_k agrees across the phases."""
+    p, g, U = _case(**CASES["np3_dp"], scheme="MUSCL")
+    got, info, _ = run_gpu(p, g, U.copy(), 5)
+    assert info.status == 0
+    V = cb.valid_view(got, p, g)
+    npk = p.nphase
+    A = np.array(p.Ak[:npk])
+    B = np.array(p.Bk[:npk])
+    al = V[0:npk]
+    are = V[2 * npk:3 * npk]
+    pk = (are - al * B[:, None, None, None]) / (A[:, None, None, None] * al)
+    mask = np.all(al > 1e-3, axis=0)
+    spread = np.max(np.abs(pk[:, mask] - pk[0:1, mask]) / np.abs(pk[0:1, mask]))
+    print(f"largest relative spread of the phase pressures over {int(mask.sum())} mixed cells: {spread:.2e}")
+    assert spread < 1e-9
+    assert np.allclose(al.sum(axis=0), 1.0, atol=1e-12, rtol=0)
+
+
+def test_sixn_conservation():
+    """Masses, momentum and total energy change only through the boundary fluxes: on a periodic
+    box the totals stay to round-off."""
+    phys, dim, inputs, geom, U = cases.sixn_shock_bubbles(n=16, nphase=3, dp=0.05)
+    geom = dict(geom, lo_bc=(0, 0, 0), hi_bc=(0, 0, 0))
+    p = cb.make_parm(phys, dim, inputs)
+    g = cb.make_geom(**geom)
+    got, info, _ = run_gpu(p, g, U.copy(), 20)
+    assert info.status == 0
+    a, b = cb.valid_view(got, p, g), cb.valid_view(U, p, g)
+    npk = p.nphase
+    cons = list(range(npk, 2 * npk)) + list(range(3 * npk, 3 * npk + dim + 1))
+    for c in cons:
+        s0, s1 = float(b[c].sum()), float(a[c].sum())
+        scale = float(np.abs(b[c]).sum())
+        print(f"component {c}: total {s0!r} -> {s1!r}")
+        assert abs(s1 - s0) <= 1e-13 * scale

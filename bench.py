@@ -62,6 +62,9 @@ def parse():
                     help="shape,order of the stage kernel instead of the autotuner's pick (profiling)")
     ap.add_argument("--e2e-slabs", type=int, default=32, help="slabs of the host-buffer step (e2e)")
     ap.add_argument("--no-tma", action="store_true", help="stage the halo slabs with ordinary loads (profiling)")
+    ap.add_argument("--no-sixn", action="store_true")
+    ap.add_argument("--sixn-n", type=int, default=512, help="SIXEQS_IE_NPHASE shock-bubble: 2n x n cells")
+    ap.add_argument("--sixn-steps", type=int, default=20)
     ap.add_argument("--no-triple", action="store_true")
     ap.add_argument("--triple-m", type=int, default=256, help="triple point side: 7m x 3m cells")
     ap.add_argument("--triple-steps", type=int, default=20)
@@ -482,6 +485,67 @@ def run_triple_point(args):
     return out
 
 
+def run_sixn(args):
+    """2D SIXEQS_IE_NPHASE shock-bubble interaction (a Mach 1.1 water shock on an air bubble, with a
+    helium bubble for NPHASE 3) at 2n x n cells, MUSCL (consistent limiter) + HLLC + TVD-RK3 with the
+    Newton pressure relaxation after every stage, plain FP64 (bit-identical to the reference), phases
+    started out of pressure equilibrium; single-box level advance timed with CUDA events. Beside it the
+    reference-header CPU build on the same case for three steps (OpenMP over the host threads)."""
+    import torch
+
+    import compas_b200 as cb
+    from compas_b200 import cases
+    from oracle.oracle import Oracle, case_from, have_ref
+
+    stream = torch.cuda.current_stream()
+    n, K, W = args.sixn_n, args.sixn_steps, 3
+    peak = measured_peaks()[0]
+    out = {}
+    for npk in (2, 3):
+        phys, dim, inputs, geom, U = cases.sixn_shock_bubbles(n=n, nphase=npk, dp=0.05, xp=torch, device="cuda")
+        p = cb.make_parm(phys, dim, inputs)
+        g = cb.make_geom(**geom)
+        cells = geom["n"][0] * geom["n"][1]
+        bytes_cs = cases.algorithmic_bytes_per_cell_stage(phys, dim, npk)
+        lv = cb.Level(p, g)
+        lv.upload(U, stream=stream)
+        lv.advance(W, stream=stream)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        lv.advance(K, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        info = lv.sync()
+        assert info.status == 0
+        lv.close()
+        rate = cells * 3 * K / (ms / 1e3)
+        res = {"workload": f"2D SIXEQS_IE_NPHASE (NPHASE {npk}) shock-bubble {2 * n}x{n}, MUSCL (consistent "
+                           "limiter)+HLLC+TVD-RK3, Newton pressure relaxation after every stage, FP64",
+               "cells": cells, "steps": K, "value": rate, "unit": UNIT, "ms_per_step": ms / K,
+               "algorithmic_bytes_per_cell_stage": bytes_cs,
+               "hbm_frac_of_measured": rate * bytes_cs / 1e9 / peak if peak else None}
+        if not args.no_cpu and have_ref(phys, dim, npk):
+            m = n
+            _, _, _, geom_s, Us = cases.sixn_shock_bubbles(n=m, nphase=npk, dp=0.05)
+            o = Oracle("reference", case_from(p, cb.make_geom(**geom_s)), None)
+            _, dts = o.advance(Us, 1)
+            steps = 3
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                o.rk3_step(Us, float(dts[0]))
+            el = time.perf_counter() - t0
+            cpu = 2 * m * m * 3 * steps / el
+            res["cpu_reference"] = {"value": cpu, "unit": UNIT, "cores": o.threads(), "kind": "reference",
+                                    "sample": f"{2 * m}x{m} cells of the same case, {steps} steps after one untimed "
+                                              f"step, OpenMP over {o.threads()} host threads, {el:.1f} s"}
+            res["speedup_vs_cpu_reference"] = rate / cpu
+        out[f"nphase{npk}"] = res
+    return out
+
+
 def run_serving(args, rank=0, world=1, dist=None):
     """Poisson arrivals of mixed 2D shock-bubble / 3D shock-droplet / 2D three-material triple-point
     solves under an HBM budget, continuous batching, at several arrival rates, against the same
@@ -720,6 +784,7 @@ def run_ours(args, rank, world, dist):
         pf6_res = None if (args.no_phase_field or args.no_phase_field_sixeq) else run_phase_field_sixeq(args)
         amr_res = None if args.no_amr else run_amr(args)
         triple_res = None if args.no_triple else run_triple_point(args)
+        sixn_res = None if args.no_sixn else run_sixn(args)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms[head] / args.steps, "higher_is_better": True,
@@ -763,6 +828,7 @@ def run_ours(args, rank, world, dist):
             "phase_field_sixeq": pf6_res,
             "amr": amr_res,
             "triple_point": triple_res,
+            "sixeqs_ie_nphase": sixn_res,
         }
         if cpu:
             # device-resident speed-up over the reference CPU arithmetic, per precision form; "fp64" is the

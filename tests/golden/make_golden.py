@@ -34,6 +34,10 @@ CASES = {
     "bubbles_nasg_k_5eqn4_2d_24": (cases.nphase_bubbles, dict(n=24, nphase=4, eos=3, source_term=1), 6),
     "bubbles_5eqn2_2d_24": (cases.nphase_bubbles, dict(n=24, nphase=2), 6),
     "bubbles_5eqn3_3d_10": (cases.nphase_bubbles, dict(n=10, nphase=3, dim=3), 3),
+    "shockbubble_6eqn2_2d_24x12": (cases.sixn_shock_bubbles, dict(n=12, nphase=2, dp=0.05), 6),
+    "shockbubbles_nasg_6eqn3_2d_32x16": (cases.sixn_shock_bubbles, dict(n=16, nphase=3, eos=3, dp=0.05,
+                                                                       scheme="WENO5B"), 6),
+    "shockbubbles_6eqn3_3d_16x8x8": (cases.sixn_shock_bubbles, dict(n=8, nphase=3, dim=3, dp=0.05), 3),
 }
 
 

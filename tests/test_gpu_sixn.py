@@ -13,6 +13,10 @@ on an air bubble (and a helium bubble with three phases), after the reference's
 ShockBubble-WaterAir-6Eq-Nphase example, in pressure equilibrium and out of it, with the NASG
 covolume, with a trace threshold that sends phases through the safeguarded relaxation, and in 3D.
 """
+import ast
+import glob
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -36,6 +40,26 @@ CASES = {
     "np3_trace": dict(n=16, nphase=3, dp=0.05, trace=1e-3),
     "np3_3d": dict(n=8, nphase=3, dim=3, dp=0.05),
 }
+
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*_6eqn*.npz")))
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_sixn_matches_reference_golden(path):
+    """Fixtures made by the reference's own SIXEQS_IE_NPHASE headers (tests/golden/make_golden.py)."""
+    z = np.load(path)
+    phys, dim, steps = (int(x) for x in z["physics"])
+    p = cb.make_parm(phys, dim, ast.literal_eval(str(z["inputs"])))
+    g = cb.make_geom(**ast.literal_eval(str(z["geom"])))
+    got, info, dts = run_gpu(p, g, z["U0"].copy(), steps)
+    assert info.status == 0 and info.steps == steps
+    a = cb.valid_view(got, p, g)
+    e = rel_linf(a, z["valid"])
+    print(f"{os.path.basename(path)}: rel Linf per field {np.array2string(e, precision=2)}; "
+          f"bitwise equal: {np.array_equal(a, z['valid'])}")
+    np.testing.assert_array_equal(dts, z["dts"])
+    assert np.all(e <= TOL), e
 
 
 def _case(**kw):

@@ -184,6 +184,7 @@ __device__ void amr_face_flux(const double* U, const Grid& g, int d, int i, int 
     using PT = typename std::conditional<MIX, float, double>::type;
     constexpr int N = M::N, D = M::D;
     constexpr bool NPH = (M::KIND == kModelFiveN);
+    constexpr bool SXN = (M::KIND == kModelSixN);
     PT P[6][N];
 #pragma unroll
     for (int s = 0; s < 6; ++s) {
@@ -197,18 +198,18 @@ __device__ void amr_face_flux(const double* U, const Grid& g, int d, int i, int 
         else M::cons2prim(P[s], Uc, e, nullptr);
     }
     double WfL[N], WfR[N], UL[N], UR[N];
-    constexpr int NB0 = (SCHEME == 6) ? M::IM : 0;
-    constexpr int NB1 = (SCHEME == 6) ? M::IA : N;
+    constexpr int NB0 = (SCHEME == 6) ? weno5b_plain_lo<M>() : 0;
+    constexpr int NB1 = (SCHEME == 6) ? weno5b_plain_hi<M>() : N;
     double cm;
     if constexpr (!MIX) {
-        if constexpr (SCHEME == 6 && NPH) {
+        if constexpr (SCHEME == 6 && (NPH || SXN)) {
             double rf[M::NP], af[M::NP];
-            bounded_phases<M::NP, 5, double>([&](int k, int s) { return (double)P[s][k]; },
+            bounded_phases<M::NP, 5, double>([&](int k, int s) { return (double)P[s][M::IR + k]; },
                                          [&](int k, int s) { return (double)P[s][M::IA + k]; }, 1, rf, af);
-            for (int k = 0; k < M::NP; ++k) { WfL[k] = rf[k]; WfL[M::IA + k] = af[k]; }
-            bounded_phases<M::NP, 5, double>([&](int k, int s) { return (double)P[s + 1][k]; },
+            for (int k = 0; k < M::NP; ++k) { WfL[M::IR + k] = rf[k]; WfL[M::IA + k] = af[k]; }
+            bounded_phases<M::NP, 5, double>([&](int k, int s) { return (double)P[s + 1][M::IR + k]; },
                                          [&](int k, int s) { return (double)P[s + 1][M::IA + k]; }, -1, rf, af);
-            for (int k = 0; k < M::NP; ++k) { WfR[k] = rf[k]; WfR[M::IA + k] = af[k]; }
+            for (int k = 0; k < M::NP; ++k) { WfR[M::IR + k] = rf[k]; WfR[M::IA + k] = af[k]; }
         } else if constexpr (SCHEME == 6) {
             double r1[6], r2[6], al[6];
 #pragma unroll
@@ -240,6 +241,10 @@ __device__ void amr_face_flux(const double* U, const Grid& g, int d, int i, int 
         M::prim2cons(UL, WfL, e, err);
         M::prim2cons(UR, WfR, e, err);
         if constexpr (NPH && SCHEME != 6) if (SCHEME != 2 || code != 11) {
+            M::consistent_limit(UL, P[2], 1, dxd, 1, e, err);
+            M::consistent_limit(UR, P[3], 1, dxd, -1, e, err);
+        }
+        if constexpr (SXN && SCHEME == 2) if (code >= 1 && code < 10) {
             M::consistent_limit(UL, P[2], 1, dxd, 1, e, err);
             M::consistent_limit(UR, P[3], 1, dxd, -1, e, err);
         }
@@ -353,6 +358,9 @@ __global__ void amr_cf_kernel(AmrCfArgs A) {
 // face terms give div u, div(u a1p1), div(u a2p2) corrections, applied to the phase energies and alpha1
 // with the primitives of the state before the reflux; with relax set, a cell the reflux changed is
 // relaxed again (RelaxRefluxedCells, :314-349), since the stage relaxation preceded the reflux.
+// N-phase six-equation model (source/Class_Compressible6Eq_IE_NPhase_PhaseField.cpp:83-181, :302-333):
+// alpha_k -= alpha_k xi, alpha_k rho_k e_k += alpha_k p_k xi with xi the refluxed u* term and the
+// primitives of the state before the reflux; the refluxed cells relaxed again likewise.
 template <class M>
 __global__ void amr_reflux_kernel(const AmrCf* cf, const int* groups, int ngroups, const double* reg,
                                   const double* reg_nc, AmrBufs B, int knew, double vol, Eos e, int id_k, int relax,
@@ -384,6 +392,23 @@ __global__ void amr_reflux_kernel(const AmrCf* cf, const int* groups, int ngroup
         } else if constexpr (M::KIND == kModelFiveN) {
             // source/Class_Compressible5Eq_NPhase_PhaseField.cpp:89-110: alpha_k -= xi phi_k (1 + K_k)
             for (int kk = 0; kk < M::NP; ++kk) U[(M::IA + kk) * S + f0.cq] += -1.0 * (srck[kk] * xs[0]);
+        } else if constexpr (M::KIND == kModelSixN) {
+            for (int kk = 0; kk < M::NP; ++kk) {
+                U[(M::IA + kk) * S + f0.cq] += -W[M::IA + kk] * xs[0];
+                U[(M::IP + kk) * S + f0.cq] += W[M::IP + kk] * xs[0];
+            }
+            if (relax) {
+                double v[N];
+                bool changed = false;
+                for (int c = 0; c < N; ++c) {
+                    v[c] = U[c * S + f0.cq];
+                    changed = changed || (v[c] != Uc[c]);
+                }
+                if (changed) {
+                    M::relax(v, e, trace, err);
+                    for (int c = 0; c < N; ++c) U[c * S + f0.cq] = v[c];
+                }
+            }
         } else {
             const double divv = -xs[0], dva1 = -xs[1], dva2 = -xs[2];
             const double rho = W[0] + W[1];

@@ -2145,7 +2145,7 @@ static int batch_sync_list(compas_b200_batch* b, cudaStream_t st) {
             B.hi_bc[d] = c.g.hi_bc[d];
         }
         B.id_k = c.p.source_term;
-        B.relax = (c.p.physics == COMPAS_B200_SIXEQS) ? c.p.relaxation : 0;
+        B.relax = (c.p.physics == COMPAS_B200_SIXEQS || c.p.physics == COMPAS_B200_SIXEQS_IE_NPHASE) ? c.p.relaxation : 0;
         B.riemann = c.p.id_riemann;
         B.muscl = c.p.id_weno ? (c.p.id_limiter == 3 ? 10 : (c.p.id_limiter == 4 ? 11 : -1)) : c.p.id_limiter;
         B.trace = c.p.relax_trace;
@@ -2181,8 +2181,10 @@ int compas_b200_batch_create_nphase(int physics, int dim, int nphase, int id_lim
     if (rc) return rc;
     if (physics == COMPAS_B200_FIVEEQS_NPHASE && !nphase_built(dim, nphase))
         return fail(COMPAS_B200_EUNSUPPORTED, "FIVEEQS_NPHASE batches: NPHASE 2, 3, 4 in 2D and 3 in 3D");
-    if (physics == COMPAS_B200_SIXEQS_IE_NPHASE)
-        return fail(COMPAS_B200_EUNSUPPORTED, "SIXEQS_IE_NPHASE runs on the level API, not in a batch");
+    if (physics == COMPAS_B200_SIXEQS_IE_NPHASE && !sixn_built(dim, nphase))
+        return fail(COMPAS_B200_EUNSUPPORTED, "SIXEQS_IE_NPHASE batches: NPHASE 2, 3 in 2D and 3 in 3D");
+    if (physics == COMPAS_B200_SIXEQS_IE_NPHASE && precision != 0)
+        return fail(COMPAS_B200_EUNSUPPORTED, "SIXEQS_IE_NPHASE runs in plain FP64 (precision 0)");
     if (id_limiter != 5 && id_limiter != 6) return fail(COMPAS_B200_EUNSUPPORTED, "WENO5 (5) or WENO5B (6)");
     if (precision != 0 && precision != 1) return fail(COMPAS_B200_EARG, "precision 0 or 1");
     if (capacity < 1 || capacity > (1 << 20)) return fail(COMPAS_B200_EARG, "capacity out of range");
@@ -2238,7 +2240,7 @@ int compas_b200_batch_add(compas_b200_batch* b, const compas_b200_parm* p, const
     int rc = check_args(p, g);
     if (rc) return rc;
     if (p->physics != b->physics || p->dim != b->dim || p->id_limiter != b->limiter || p->precision != b->precision ||
-        (p->physics == COMPAS_B200_FIVEEQS_NPHASE && p->nphase != b->nphase))
+        (nphase_model(p->physics) && p->nphase != b->nphase))
         return fail(COMPAS_B200_EARG, "a batch holds cases of one model, dimension, number of phases, scheme and precision");
     if (p->thinc) return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.THINC = 1 runs on the level API, not in a batch");
     if (p->id_bound) return fail(COMPAS_B200_EUNSUPPORTED, "FiniteVolume.ID_Bound = 1 runs on the level API, not in a batch");

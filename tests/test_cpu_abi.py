@@ -170,5 +170,5 @@ def test_sixeqs_ie_nphase_keys():
             cb.Level(q, geom)
         assert e.value.code == cb.EUNSUPPORTED
     with pytest.raises(cb.CompasError) as e:
-        cb.Batch(cb.SIXEQS_IE_NPHASE, 2, 5, 0, 4, nphase=2)
+        cb.Batch(cb.SIXEQS_IE_NPHASE, 2, 5, 1, 4, nphase=2)
     assert e.value.code == cb.EUNSUPPORTED

@@ -177,3 +177,103 @@ def test_sixn_conservation():
         scale = float(np.abs(b[c]).sum())
         print(f"component {c}: total {s0!r} -> {s1!r}")
         assert abs(s1 - s0) <= 1e-13 * scale
+
+
+def test_sixn_batch_equals_level():
+    """Cases of different sizes in one box-list batch give the single-box level's bits."""
+    reqs = [dict(n=8, nphase=2), dict(n=12, nphase=2, dp=0.05), dict(n=16, nphase=2, scheme="WENO5")]
+    b = cb.Batch(cb.SIXEQS_IE_NPHASE, 2, id_limiter=5, precision=0, capacity=4, nphase=2)
+    ids, ins = [], []
+    for kw in reqs:
+        kw = dict(kw, scheme="WENO5")
+        phys, dim, inputs, geom, U = cases.sixn_shock_bubbles(**kw)
+        p, g = cb.make_parm(phys, dim, inputs), cb.make_geom(**geom)
+        ids.append(b.add(p, g, U, max_steps=12))
+        ins.append((p, g, U))
+    b.advance(12)
+    for cid, (p, g, U) in zip(ids, ins):
+        got = b.download(cid)
+        ref, info, _ = run_gpu(p, g, U.copy(), 12)
+        assert np.array_equal(cb.valid_view(got, p, g), cb.valid_view(ref, p, g))
+    b.close()
+
+
+@pytest.mark.parametrize("scheme", ["MUSCL", "WENO5B"])
+def test_sixn_face_flux_divergence_is_the_fused_right_hand_side(scheme):
+    """The area-unscaled face fluxes of compas_b200_face_fluxes difference to the conservative part of
+    the fused right-hand side (masses and momenta) bit for bit."""
+    phys, dim, inputs, geom, U = cases.sixn_shock_bubbles(n=12, nphase=3, dp=0.05, scheme=scheme)
+    p, g = cb.make_parm(phys, dim, inputs), cb.make_geom(**geom)
+    Ud = torch.from_numpy(U).cuda()
+    cb.FillPatch(p, g, Ud)
+    dU = torch.zeros_like(Ud)
+    cb.compute_dUdt_FV(p, g, Ud, dU)
+    N, NC = cb.parm_nstate(p), cb.nc_terms(p)
+    F = [torch.zeros(cb.face_shape(p, g, d, N), dtype=torch.float64, device="cuda") for d in range(dim)]
+    Fn = [torch.zeros(cb.face_shape(p, g, d, NC), dtype=torch.float64, device="cuda") for d in range(dim)]
+    cb.face_fluxes(p, g, Ud, F, Fn, area_scaled=False)
+    torch.cuda.synchronize()
+    F = [f.cpu().numpy() for f in F]
+    acc = None
+    for d in range(dim):
+        df = F[d][:, :, :, 1:] - F[d][:, :, :, :-1] if d == 0 else F[d][:, :, 1:, :] - F[d][:, :, :-1, :]
+        t = df / g.dx[d]
+        acc = t if acc is None else acc + t
+    got = cb.valid_view(dU.cpu().numpy(), p, g)
+    npk = p.nphase
+    for c in list(range(npk, 2 * npk)) + list(range(3 * npk, 3 * npk + dim)):
+        np.testing.assert_array_equal(-acc[c], got[c], err_msg=f"component {c}")
+
+
+def _amr_run(kw, domain, regions, mgs, steps, extra=None):
+    from compas_b200 import amr
+    phys, dim, inputs, geom, _ = cases.sixn_shock_bubbles(**kw)
+    p, g = cb.make_parm(phys, dim, dict(inputs, **(extra or {}))), cb.make_geom(**geom)
+    if not have_ref(p.physics, p.dim, p.nphase):
+        pytest.skip("the SIXEQS_IE_NPHASE oracle is the reference build (oracle/_ref/libref_6eqn*)")
+    boxes = amr.hierarchy(domain, dim, regions, mgs)
+    states = amr.box_states(cases.sixn_shock_bubbles, kw, domain, dim, boxes)
+    A = cb.Amr(p, g, boxes)
+    for b, U in enumerate(states):
+        A.upload(b, U)
+    A.advance(steps)
+    info = A.sync()
+    got = [A.download(b) for b in range(len(boxes))]
+    dts = A.dts(info.steps)
+    A.close()
+    assert info.status == 0 and info.steps == steps
+    ref = [U.copy() for U in states]
+    _, dts_ref = Oracle("reference", p, g).amr_advance(boxes, ref, steps)
+    np.testing.assert_array_equal(dts, dts_ref)
+    ng = geom["ng"]
+    worst = np.zeros(ref[0].shape[0])
+    equal = True
+    for (lev, lo, hi), a, r in zip(boxes, got, ref):
+        if dim == 2:
+            sl = (slice(None), 0, slice(ng, ng + hi[1] - lo[1] + 1), slice(ng, ng + hi[0] - lo[0] + 1))
+        else:
+            sl = (slice(None), slice(ng, ng + hi[2] - lo[2] + 1), slice(ng, ng + hi[1] - lo[1] + 1),
+                  slice(ng, ng + hi[0] - lo[0] + 1))
+        worst = np.maximum(worst, rel_linf(a[sl], r[sl]))
+        equal = equal and np.array_equal(a[sl], r[sl])
+    print(f"{len(boxes)} boxes, {1 + max(b[0] for b in boxes)} levels, {steps} steps: rel Linf per field "
+          f"{np.array2string(worst, precision=2)}; bitwise equal: {equal}")
+    assert np.all(worst <= TOL), worst
+
+
+AMR_CASES = [
+    (dict(n=16, nphase=2, dp=0.05), (32, 16), [((8, 4, 0), (47, 27, 0))], 16, 4, {}),
+    (dict(n=16, nphase=2, dp=0.05), (32, 16), [((8, 4, 0), (47, 27, 0))], 16, 4, {"amr.Interpolater": "pc_interp"}),
+    (dict(n=16, nphase=3, dp=0.05, scheme="WENO5B"), (32, 16),
+     [((8, 4, 0), (55, 27, 0)), ((32, 16, 0), (79, 47, 0))], 16, 3, {}),
+    (dict(n=8, nphase=3, dim=3, dp=0.05), (16, 8, 8), [((8, 4, 4), (23, 11, 11))], 8, 2, {}),
+]
+
+
+@pytest.mark.parametrize("kw,domain,regions,mgs,steps,extra", AMR_CASES,
+                         ids=["np2_muscl_2lev", "np2_muscl_2lev_pc_interp", "np3_weno5b_3lev", "np3_muscl_3d_2lev"])
+def test_sixn_amr_matches_reference(kw, domain, regions, mgs, steps, extra):
+    """The multi-level advance of the model (the reference's ShockBubble-WaterAir-6Eq-Nphase example runs
+    it on a hierarchy): subcycling, flux registers with the alpha_k and alpha_k p_k reflux source terms,
+    the relaxation of the refluxed cells, average-down; to the bit against the oracle's hierarchy driver."""
+    _amr_run(kw, domain, regions, mgs, steps, extra)

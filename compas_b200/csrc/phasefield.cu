@@ -502,10 +502,24 @@ __global__ void k_mg_rb_t(MgLevel L, int color) {
     if (((i + j + k) & 1) != color) return;
     L.x[q] = (L.b[q] + mg_off_t<D>(L, L.x, i, j, k)) * L.idiag[q];
 }
+// the residual of level L and its restriction to level C in one launch over C's cells: each coarse
+// cell averages the residuals b - A x of its 2^D children
 template <int D>
-__global__ void k_mg_residual_t(MgLevel L) {
-    MG_CELL(L.m)
-    L.r[q] = L.b[q] - (L.x[q] / L.idiag[q] - mg_off_t<D>(L, L.x, i, j, k));
+__global__ void k_mg_resrestrict_t(MgLevel L, MgLevel C) {
+    MG_CELL(C.m)
+    const int n0 = L.m.n[0], n1 = L.m.n[1];
+    double s = 0.0;
+#pragma unroll
+    for (int dk = 0; dk < (D == 3 ? 2 : 1); ++dk)
+#pragma unroll
+        for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+            for (int di = 0; di < 2; ++di) {
+                const int fi = 2 * i + di, fj = 2 * j + dj, fk = (D == 3) ? 2 * k + dk : 0;
+                const int fq = fi + n0 * (fj + n1 * fk);
+                s += L.b[fq] - (L.x[fq] / L.idiag[fq] - mg_off_t<D>(L, L.x, fi, fj, fk));
+            }
+    C.b[q] = s / (double)(D == 3 ? 8 : 4);
 }
 template <int D>
 __global__ void k_mg_apply_t(MgLevel L, const double* __restrict__ x, double* __restrict__ y) {
@@ -535,7 +549,11 @@ constexpr int kRbW = kRbTX + 2 * kRbH, kRbHt = kRbTY + 2 * kRbH, kRbCells = kRbW
 constexpr int kRbThreads = kRbCells;
 constexpr size_t kRbSmem = sizeof(double) * 7 * (size_t)kRbCells + sizeof(unsigned char) * kRbCells;
 
-__global__ void __launch_bounds__(kRbThreads) k_mg_rb4_2d(MgLevel L, int first_color) {
+// xmode: 0 starts from L.x; 1 from zero (the first smoothing of a correction, in place of zeroing
+// L.x); 2 from L.x plus the parent's value of the coarser level's x, xc (cn0 columns) - the
+// piecewise-constant prolongation of k_mg_prolong applied as the cells are loaded
+__global__ void __launch_bounds__(kRbThreads) k_mg_rb4_2d(MgLevel L, int first_color, int xmode,
+                                                          const double* __restrict__ xc, int cn0) {
     extern __shared__ double rbs[];
     double* sx = rbs;
     double* sb = sx + kRbCells;
@@ -566,7 +584,12 @@ __global__ void __launch_bounds__(kRbThreads) k_mg_rb4_2d(MgLevel L, int first_c
         unsigned char f = 0;
         if (in) {
             const int q = i + n0 * j;
-            sx[c] = L.x[q];
+            double xv = 0.0;
+            if (xmode != 1) {
+                xv = L.x[q];
+                if (xmode == 2) xv += xc[(i >> 1) + cn0 * (j >> 1)];
+            }
+            sx[c] = xv;
             sb[c] = L.b[q];
             sd[c] = L.idiag[q];
             const int fx = n0 + 1;
@@ -636,20 +659,6 @@ __global__ void k_zero(double* a, long long n) {
     GRID_STRIDE(q, n) a[q] = 0.0;
 }
 
-// coarse rhs = average of the fine residuals of the 2^D children
-__global__ void k_mg_restrict(const double* rf, PfDims f, double* bc, PfDims c) {
-    GRID_STRIDE(q, c.nv) {
-        int I, J, K;
-        vcoord(c, q, I, J, K);
-        double s = 0.0;
-        const int kz = (c.D == 3) ? 2 : 1;
-        for (int dk = 0; dk < kz; ++dk)
-            for (int dj = 0; dj < 2; ++dj)
-                for (int di = 0; di < 2; ++di) s += rf[vidx(f, 2 * I + di, 2 * J + dj, (c.D == 3 ? 2 * K + dk : 0))];
-        bc[q] = s / (double)(c.D == 3 ? 8 : 4);
-    }
-}
-
 // fine x += coarse x of the parent (piecewise-constant prolongation)
 __global__ void k_mg_prolong(const double* xc, PfDims c, double* xf, PfDims f) {
     GRID_STRIDE(q, f.nv) {
@@ -680,13 +689,6 @@ __global__ void k_mg_beta(const double* bf, PfDims f, double* bc, PfDims c, int 
     }
 }
 
-// dot product partials (fixed order); b == nullptr sums a
-__global__ void k_dot(const double* a, const double* b, long long n, double* partial) {
-    double s = 0.0;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
-        s += b ? a[q] * b[q] : a[q];
-    block_sum2(s, 0.0, partial);
-}
 __global__ void k_add_const(double* a, long long n, const double* tot, double scale) {
     const double c = -tot[0] * scale;
     GRID_STRIDE(q, n) a[q] += c;
@@ -880,25 +882,88 @@ __global__ void __launch_bounds__(kBlockThreads) k_mg_vcycle_block(const MgLevel
     for (int q = threadIdx.x; q < (int)levels[l0].m.nv; q += blockDim.x) levels[l0].x[q] = sl[l0].x[q];
 }
 
-// one reduced sum (the first of block_sum2's pair) into *out
-__global__ void k_reduce1(const double* partial, int nb, double* out) {
+// conjugate-gradient scalars kept on the device: cg[0] rz, [1] pAp, [2] alpha, [3] rz_new, [4] beta,
+// [5] the sum of the preconditioned vector (its mean is removed)
+enum CgOp { kCgRz0 = 0, kCgPAp = 1, kCgZsum = 2, kCgRz = 3 };
+
+// true in the block that finishes last (the others' partials are then visible); the counter is
+// reset by that block for the next launch
+__device__ __forceinline__ bool last_block(unsigned int* counter) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    return last;
+}
+
+// the fixed-order sum of the first of each block's pair of partials (block_sum2), by the last block
+__device__ __forceinline__ double sum_partials(const double* partial, int nb) {
     __shared__ double sa[kThreads];
     double a = 0.0;
-    for (int t = threadIdx.x; t < nb; t += kThreads) a += partial[2 * t];
+    for (int t = threadIdx.x; t < nb; t += kThreads) a += __ldcg(partial + 2 * t);
     sa[threadIdx.x] = a;
     __syncthreads();
     for (int s = kThreads / 2; s > 0; s >>= 1) {
         if ((int)threadIdx.x < s) sa[threadIdx.x] += sa[threadIdx.x + s];
         __syncthreads();
     }
-    if (threadIdx.x == 0) *out = sa[0];
+    return sa[0];
 }
 
-// conjugate-gradient scalars kept on the device: cg[0] rz, [1] pAp, [2] alpha, [3] rz_new, [4] beta
-__global__ void k_cg_alpha(double* cg) { cg[2] = (cg[1] > 0.0) ? cg[0] / cg[1] : 0.0; }
-__global__ void k_cg_beta(double* cg) {
-    cg[4] = (cg[0] != 0.0) ? cg[3] / cg[0] : 0.0;
-    cg[0] = cg[3];
+// the scalar update that follows a reduced sum: rz of the start, pAp with alpha = rz / pAp (and the
+// residual maximum cleared for the update that follows), the sum of z, rz_new with beta = rz_new / rz
+__device__ __forceinline__ void cg_finish(double* cg, int op, double tot, unsigned long long* rmax) {
+    if (op == kCgRz0) {
+        cg[0] = tot;
+    } else if (op == kCgPAp) {
+        cg[1] = tot;
+        cg[2] = (cg[1] > 0.0) ? cg[0] / cg[1] : 0.0;
+        *rmax = 0ull;
+    } else if (op == kCgZsum) {
+        cg[5] = tot;
+    } else {
+        cg[3] = tot;
+        cg[4] = (cg[0] != 0.0) ? cg[3] / cg[0] : 0.0;
+        cg[0] = cg[3];
+    }
+}
+
+// A dot product (b == nullptr: the sum of a) and its scalar update in one launch of kRedBlocks
+// blocks: grid-stride per-thread sums reduced per block (block_sum2), then the blocks' partials
+// summed in a fixed order by the last block (a deterministic result)
+__global__ void k_dot_cg(const double* a, const double* b, long long n, double* partial, unsigned int* counter,
+                         double* cg, int op, unsigned long long* rmax) {
+    double s = 0.0;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        s += b ? a[q] * b[q] : a[q];
+    block_sum2(s, 0.0, partial);
+    if (!last_block(counter)) return;
+    const double tot = sum_partials(partial, gridDim.x);
+    if (threadIdx.x == 0) {
+        *counter = 0u;
+        cg_finish(cg, op, tot, rmax);
+    }
+}
+
+// z -= mean(z) (the sum in cg[5]) and the dot product r . z with its scalar update, in one launch of
+// kRedBlocks blocks (the same bits as k_add_const, then k_dot_cg(r, z))
+__global__ void k_center_dot_cg(double* z, const double* r, long long n, double scale, double* partial,
+                                unsigned int* counter, double* cg, int op) {
+    const double c = -cg[5] * scale;
+    double s = 0.0;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const double zq = z[q] + c;
+        z[q] = zq;
+        s += r[q] * zq;
+    }
+    block_sum2(s, 0.0, partial);
+    if (!last_block(counter)) return;
+    const double tot = sum_partials(partial, gridDim.x);
+    if (threadIdx.x == 0) {
+        *counter = 0u;
+        cg_finish(cg, op, tot, nullptr);
+    }
 }
 
 __global__ void k_axpy2(double* x, double* r, const double* p, const double* Ap, long long n, const double* alp,
@@ -950,6 +1015,8 @@ struct PfLevel {
     int mg_block0 = -1;                      // first level of the single-block coarse cycle
     size_t mg_block_smem = 0;                // its shared memory: x, b, r of every level it covers
     double *z = nullptr, *p = nullptr, *Ap = nullptr;
+    double* rhs = nullptr;                   // right-hand side of the elliptic system
+    unsigned int* cnt = nullptr;             // block counter of the one-launch reductions
     double* cg = nullptr;                    // device scalars of the conjugate gradients
     double* qsol = nullptr;                  // solution Q, kept as the next step's starting iterate
     cudaGraphExec_t cg_iter = nullptr;       // one captured iteration (fixed pointers)
@@ -992,16 +1059,16 @@ double read_max(unsigned long long* dev, cudaStream_t st) {
     return v;
 }
 
-// one V-cycle on level l (x_l from its current value, b_l given)
-cudaError_t vcycle(PfLevel* pf, int l, cudaStream_t st) {
+// one V-cycle on level l (b_l given; x_l from zero when x_zero, else from its current value)
+cudaError_t vcycle(PfLevel* pf, int l, cudaStream_t st, bool x_zero) {
     MgLevel& L = pf->mg[l];
     const unsigned nb = blocks_for(L.m.nv);
-    const unsigned nbh = blocks_for((long long)L.m.n[1] * L.m.n[2] * ((L.m.n[0] + 1) / 2));
     const dim3 gg = mg_grid(L.m);
     const bool d3 = (L.m.D == 3);
     // 2D levels of at least 2 halo widths per side: two sweeps per temporally blocked launch
     const bool fused = !d3 && L.rb && L.m.n[0] >= 2 * kRbH && L.m.n[1] >= 2 * kRbH;
-    auto smooth = [&](int sweeps, bool reverse) {
+    // xmode as k_mg_rb4_2d's: 0 from x, 1 from zero, 2 from x plus the prolonged correction of C
+    auto smooth = [&](int sweeps, bool reverse, int xmode, const MgLevel* C) {
         if (fused && sweeps == 2) {
             static bool attr = false;
             if (!attr) {
@@ -1009,9 +1076,12 @@ cudaError_t vcycle(PfLevel* pf, int l, cudaStream_t st) {
                 attr = true;
             }
             const dim3 grid((unsigned)((L.m.n[0] + kRbTX - 1) / kRbTX), (unsigned)((L.m.n[1] + kRbTY - 1) / kRbTY));
-            k_mg_rb4_2d<<<grid, kRbThreads, kRbSmem, st>>>(L, reverse ? 1 : 0);
+            k_mg_rb4_2d<<<grid, kRbThreads, kRbSmem, st>>>(L, reverse ? 1 : 0, xmode, C ? C->x : nullptr,
+                                                           C ? C->m.n[0] : 0);
             return;
         }
+        if (xmode == 1) k_zero<<<nb, kThreads, 0, st>>>(L.x, L.m.nv);
+        else if (xmode == 2) k_mg_prolong<<<nb, kThreads, 0, st>>>(C->x, C->m, L.x, L.m);
         for (int s = 0; s < sweeps; ++s) {
             if (L.rb) {
                 for (int c = 0; c < 2; ++c) {
@@ -1026,31 +1096,29 @@ cudaError_t vcycle(PfLevel* pf, int l, cudaStream_t st) {
             }
         }
     };
-    (void)nbh;
     if (l == pf->mg_block0) {
         static bool attr = false;
         if (!attr) {
             cudaFuncSetAttribute(k_mg_vcycle_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBlockSmemMax);
             attr = true;
         }
+        if (x_zero) k_zero<<<nb, kThreads, 0, st>>>(L.x, L.m.nv);
         k_mg_vcycle_block<<<1, kBlockThreads, pf->mg_block_smem, st>>>(pf->mg_dev, l, (int)pf->mg.size());
         return cudaGetLastError();
     }
     if (l + 1 == (int)pf->mg.size()) {
         // an even number of sweeps alternating the colour order keeps the cycle symmetric
+        if (x_zero) k_zero<<<nb, kThreads, 0, st>>>(L.x, L.m.nv);
         k_mg_coarse<<<1, kThreads, 0, st>>>(L, 16);
         return cudaGetLastError();
     }
-    smooth(2, false);
-    if (d3) k_mg_residual_t<3><<<gg, kRowThreads, 0, st>>>(L);
-    else k_mg_residual_t<2><<<gg, kRowThreads, 0, st>>>(L);
+    smooth(2, false, x_zero ? 1 : 0, nullptr);
     MgLevel& C = pf->mg[l + 1];
-    k_mg_restrict<<<blocks_for(C.m.nv), kThreads, 0, st>>>(L.r, L.m, C.b, C.m);
-    k_zero<<<blocks_for(C.m.nv), kThreads, 0, st>>>(C.x, C.m.nv);
-    cudaError_t e = vcycle(pf, l + 1, st);
+    if (d3) k_mg_resrestrict_t<3><<<mg_grid(C.m), kRowThreads, 0, st>>>(L, C);
+    else k_mg_resrestrict_t<2><<<mg_grid(C.m), kRowThreads, 0, st>>>(L, C);
+    cudaError_t e = vcycle(pf, l + 1, st, true);
     if (e != cudaSuccess) return e;
-    k_mg_prolong<<<nb, kThreads, 0, st>>>(C.x, C.m, L.x, L.m);
-    smooth(2, true);
+    smooth(2, true, 2, &C);
     return cudaGetLastError();
 }
 
@@ -1088,6 +1156,11 @@ int pf_create(const compas_b200_parm* p, const compas_b200_geom* g, PfLevel** ou
         if ((e = dalloc(pf, &pf->J[d], m.nf[d])) || (e = dalloc(pf, &pf->Jhat[d], m.nf[d])) ||
             (e = dalloc(pf, &pf->gq[d], m.nf[d])))
             return fail_out(e);
+    // the conjugate-gradient vectors; z and the residual (mech) double as the finest level's x and b
+    if ((e = dalloc(pf, &pf->z, m.nv)) || (e = dalloc(pf, &pf->p, m.nv)) || (e = dalloc(pf, &pf->Ap, m.nv)) ||
+        (e = dalloc(pf, &pf->rhs, m.nv)) || (e = dalloc(pf, (double**)&pf->cnt, 1)) || (e = dalloc(pf, &pf->cg, 8)) ||
+        (e = dalloc(pf, &pf->qsol, m.nv)))
+        return fail_out(e);
     // multigrid hierarchy
     PfDims lm = m;
     for (int l = 0; l < kMaxLevels; ++l) {
@@ -1098,9 +1171,13 @@ int pf_create(const compas_b200_parm* p, const compas_b200_geom* g, PfLevel** ou
             if (lm.periodic[d] && (lm.n[d] % 2)) L.rb = false;
         for (int d = 0; d < lm.D; ++d)
             if ((e = dalloc(pf, &L.beta[d], lm.nf[d]))) return fail_out(e);
-        if ((e = dalloc(pf, &L.x, lm.nv)) || (e = dalloc(pf, &L.b, lm.nv)) || (e = dalloc(pf, &L.r, lm.nv)) ||
-            (e = dalloc(pf, &L.idiag, lm.nv)))
+        if (l == 0) {
+            L.x = pf->z;
+            L.b = pf->mech;
+        } else if ((e = dalloc(pf, &L.x, lm.nv)) || (e = dalloc(pf, &L.b, lm.nv))) {
             return fail_out(e);
+        }
+        if ((e = dalloc(pf, &L.r, lm.nv)) || (e = dalloc(pf, &L.idiag, lm.nv))) return fail_out(e);
         for (int d = 0; d < lm.D; ++d) L.ih2[d] = 1.0 / (lm.dx[d] * lm.dx[d]);
         pf->mg.push_back(L);
         if (!coarsenable(lm) || lm.nv <= 16) break;
@@ -1125,9 +1202,6 @@ int pf_create(const compas_b200_parm* p, const compas_b200_geom* g, PfLevel** ou
         if ((e = cudaMemcpy(pf->mg_dev, pf->mg.data(), sizeof(MgLevel) * pf->mg.size(), cudaMemcpyHostToDevice)))
             return fail_out(e);
     }
-    if ((e = dalloc(pf, &pf->z, m.nv)) || (e = dalloc(pf, &pf->p, m.nv)) || (e = dalloc(pf, &pf->Ap, m.nv)) ||
-        (e = dalloc(pf, &pf->cg, 8)) || (e = dalloc(pf, &pf->qsol, m.nv)))
-        return fail_out(e);
     *out = pf;
     return COMPAS_B200_OK;
 }
@@ -1213,11 +1287,14 @@ int pf_grad_q(PfLevel* pf, const compas_b200_parm* p, const double* U, double dt
         PF_TRY(cudaGetLastError());
     } else {
         // PhaseField_GradQPF, implicit (:2132-2310): div(beta grad Q) = Div_Jhat
+        // The finest multigrid level reads its right-hand side from the residual r and writes its
+        // solution into z (F.b == r, F.x == z), so the preconditioner z = V(r) needs no copies.
         MgLevel& F = pf->mg[0];
-        k_djhat<<<kRedBlocks, kThreads, 0, st>>>(pf->pfb, pf->pfb0, m, 1.0 / dt, F.b, pf->partial);
+        double* rhs = pf->rhs;
+        k_djhat<<<kRedBlocks, kThreads, 0, st>>>(pf->pfb, pf->pfb0, m, 1.0 / dt, rhs, pf->partial);
         k_reduce2<<<1, kThreads, 0, st>>>(pf->partial, kRedBlocks, pf->tot);
-        k_add_const<<<nbv, kThreads, 0, st>>>(F.b, m.nv, pf->tot, 1.0 / (double)m.nv);  // solvable (zero mean)
-        k_neg<<<nbv, kThreads, 0, st>>>(F.b, m.nv);  // A = -div(beta grad): A Q = -Div_Jhat
+        k_add_const<<<nbv, kThreads, 0, st>>>(rhs, m.nv, pf->tot, 1.0 / (double)m.nv);  // solvable (zero mean)
+        k_neg<<<nbv, kThreads, 0, st>>>(rhs, m.nv);  // A = -div(beta grad): A Q = -Div_Jhat
         for (int d = 0; d < m.D; ++d)
             k_beta<<<blocks_for(m.nf[d]), kThreads, 0, st>>>(pf->pfb0, m, d, eta, eta_f, F.beta[d]);
         for (size_t l = 1; l < pf->mg.size(); ++l)
@@ -1233,50 +1310,42 @@ int pf_grad_q(PfLevel* pf, const compas_b200_parm* p, const double* U, double dt
         // step to the next); the stopping test is the reference's absolute one, max|r| <= tol max|rhs|,
         // so the warm start changes only the number of iterations.
         double* x = pf->qsol;
-        double* r = pf->mech;     // residual (the mechanism's scratch is free here)
+        double* r = pf->mech;     // residual (the mechanism's scratch is free here) == F.b
+        double* z = pf->z;        // preconditioned residual == F.x
         if (m.D == 3) k_mg_apply_t<3><<<mg_grid(F.m), kRowThreads, 0, st>>>(F, x, pf->Ap);
         else k_mg_apply_t<2><<<mg_grid(F.m), kRowThreads, 0, st>>>(F, x, pf->Ap);
-        k_sub<<<nbv, kThreads, 0, st>>>(F.b, pf->Ap, r, m.nv);
+        k_sub<<<nbv, kThreads, 0, st>>>(rhs, pf->Ap, r, m.nv);
         PF_TRY(cudaMemsetAsync(pf->umax, 0, sizeof(unsigned long long), st));
-        k_maxabs<<<nbv, kThreads, 0, st>>>(F.b, m.nv, pf->umax);
+        k_maxabs<<<nbv, kThreads, 0, st>>>(rhs, m.nv, pf->umax);
         const double bnorm = read_max(pf->umax, st);
         PF_TRY(cudaMemsetAsync(pf->umax, 0, sizeof(unsigned long long), st));
         k_maxabs<<<nbv, kThreads, 0, st>>>(r, m.nv, pf->umax);
         const double rnorm0 = read_max(pf->umax, st);
-        auto dot_dev = [&](const double* a, const double* b, double* slot, cudaStream_t s2) {
-            k_dot<<<kRedBlocks, kThreads, 0, s2>>>(a, b, m.nv, pf->partial);
-            k_reduce1<<<1, kThreads, 0, s2>>>(pf->partial, kRedBlocks, slot);
-        };
-        auto precond = [&](const double* in, double* outz, cudaStream_t s2) -> cudaError_t {
-            // z = V(in) with a zero start, made mean-free
-            k_copy<<<nbv, kThreads, 0, s2>>>(in, F.b, m.nv);
-            k_zero<<<nbv, kThreads, 0, s2>>>(F.x, m.nv);
-            cudaError_t e = vcycle(pf, 0, s2);
+        // z = V(r) from a zero start, made mean-free, and r . z with the scalar update `op`
+        auto precond_dot = [&](int op, cudaStream_t s2) -> cudaError_t {
+            cudaError_t e = vcycle(pf, 0, s2, true);
             if (e != cudaSuccess) return e;
-            k_copy<<<nbv, kThreads, 0, s2>>>(F.x, outz, m.nv);
-            dot_dev(outz, nullptr, pf->cg + 5, s2);
-            k_add_const<<<nbv, kThreads, 0, s2>>>(outz, m.nv, pf->cg + 5, 1.0 / (double)m.nv);
+            k_dot_cg<<<kRedBlocks, kThreads, 0, s2>>>(z, nullptr, m.nv, pf->partial, pf->cnt, pf->cg, kCgZsum, nullptr);
+            k_center_dot_cg<<<kRedBlocks, kThreads, 0, s2>>>(z, r, m.nv, 1.0 / (double)m.nv, pf->partial, pf->cnt,
+                                                             pf->cg, op);
             return cudaGetLastError();
         };
         auto iteration = [&](cudaStream_t s2) -> cudaError_t {
             if (m.D == 3) k_mg_apply_t<3><<<mg_grid(F.m), kRowThreads, 0, s2>>>(F, pf->p, pf->Ap);
             else k_mg_apply_t<2><<<mg_grid(F.m), kRowThreads, 0, s2>>>(F, pf->p, pf->Ap);
-            dot_dev(pf->p, pf->Ap, pf->cg + 1, s2);
-            k_cg_alpha<<<1, 1, 0, s2>>>(pf->cg);
-            cudaError_t e = cudaMemsetAsync(pf->umax, 0, sizeof(unsigned long long), s2);
-            if (e != cudaSuccess) return e;
+            // pAp, alpha, and the residual maximum cleared for k_axpy2
+            k_dot_cg<<<kRedBlocks, kThreads, 0, s2>>>(pf->p, pf->Ap, m.nv, pf->partial, pf->cnt, pf->cg, kCgPAp,
+                                                      pf->umax);
             k_axpy2<<<nbv, kThreads, 0, s2>>>(x, r, pf->p, pf->Ap, m.nv, pf->cg + 2, pf->umax);
-            if ((e = precond(r, pf->z, s2)) != cudaSuccess) return e;
-            dot_dev(r, pf->z, pf->cg + 3, s2);
-            k_cg_beta<<<1, 1, 0, s2>>>(pf->cg);
-            k_xpby<<<nbv, kThreads, 0, s2>>>(pf->z, pf->p, m.nv, pf->cg + 4);
+            cudaError_t e = precond_dot(kCgRz, s2);
+            if (e != cudaSuccess) return e;
+            k_xpby<<<nbv, kThreads, 0, s2>>>(z, pf->p, m.nv, pf->cg + 4);
             return cudaGetLastError();
         };
         const double tol = p->pf_tol_rel;
         if (bnorm > 0.0 && rnorm0 > tol * bnorm) {
-            PF_TRY(precond(r, pf->z, st));
-            k_copy<<<nbv, kThreads, 0, st>>>(pf->z, pf->p, m.nv);
-            dot_dev(r, pf->z, pf->cg + 0, st);
+            PF_TRY(precond_dot(kCgRz0, st));
+            k_copy<<<nbv, kThreads, 0, st>>>(z, pf->p, m.nv);
             PF_TRY(cudaGetLastError());
             if (!pf->cg_iter) {
                 cudaStream_t cap;

@@ -20,6 +20,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <utility>
 #include <vector>
 
 #include "physics.cuh"
@@ -536,38 +537,47 @@ constexpr int kRowThreads = 128;
 dim3 mg_grid(const PfDims& m) { return dim3((unsigned)((m.n[0] + kRowThreads - 1) / kRowThreads), (unsigned)m.n[1], (unsigned)m.n[2]); }
 
 // Two red-black Gauss-Seidel sweeps (four colour passes) of a 2D level in ONE launch, by temporal
-// blocking: each CTA loads its kRbTX x kRbTY tile with a halo of kRbH = 4 cells (x, b, 1/diag and
-// the four face coefficients beta_f / h^2 of every cell, periodic sides wrapped) into shared memory
-// and runs the passes there; pass p updates the cells of its colour within kRbH - 1 - p rings of
+// blocking: each CTA loads its kRbTX x kRbTY tile with a halo of kRbH = 4 cells (x into shared memory;
+// b, 1/diag and the four face coefficients beta_f / h^2 of every cell into registers; periodic sides
+// wrapped) and runs the passes there; pass p updates the cells of its colour within kRbH - 1 - p rings of
 // the tile, so after the fourth pass the tile holds exactly what four global passes give (a
 // colour's update reads only the other colour), and only the tile is written back. This replaces
 // four launches and four passes over the level by one.
 constexpr int kRbTX = 32, kRbTY = 16, kRbH = 4, kRbPasses = kRbH;
 constexpr int kRbW = kRbTX + 2 * kRbH, kRbHt = kRbTY + 2 * kRbH, kRbCells = kRbW * kRbHt;
-// one thread per cell of the tile and its halo: every thread's seven loads are in flight at once
-// (the load phase is latency-bound otherwise), and every pass is one update per thread
-constexpr int kRbThreads = kRbCells;
-constexpr size_t kRbSmem = sizeof(double) * 7 * (size_t)kRbCells + sizeof(unsigned char) * kRbCells;
+// two cells of the tile and its halo per thread (cells t and t + kRbThreads): every thread's loads are
+// in flight at once (the load phase is latency-bound otherwise). A cell is always updated by the same
+// thread, so its right-hand side, 1/diagonal, face coefficients and neighbour flags stay in that
+// thread's registers; only x lives in shared memory (neighbours read it), which keeps the passes off
+// the shared-memory instruction limit (one load per neighbour and one store per update)
+constexpr int kRbCellsPerThread = 2;
+constexpr int kRbThreads = kRbCells / kRbCellsPerThread;
+static_assert(kRbThreads * kRbCellsPerThread == kRbCells, "whole cells per thread");
+constexpr size_t kRbSmem = sizeof(double) * (size_t)kRbCells;
 
 // xmode: 0 starts from L.x; 1 from zero (the first smoothing of a correction, in place of zeroing
 // L.x); 2 from L.x plus the parent's value of the coarser level's x, xc (cn0 columns) - the
-// piecewise-constant prolongation of k_mg_prolong applied as the cells are loaded
-__global__ void __launch_bounds__(kRbThreads) k_mg_rb4_2d(MgLevel L, int first_color, int xmode,
-                                                          const double* __restrict__ xc, int cn0) {
-    extern __shared__ double rbs[];
-    double* sx = rbs;
-    double* sb = sx + kRbCells;
-    double* sd = sb + kRbCells;
-    double* cw = sd + kRbCells;  // coefficient of the -x neighbour (beta of the cell's low x face / h^2)
-    double* ce = cw + kRbCells;
-    double* cs = ce + kRbCells;
-    double* cn = cs + kRbCells;
-    unsigned char* flag = reinterpret_cast<unsigned char*>(cn + kRbCells);  // bit0 in domain, bits1-4 nb valid, bit5 colour
+// piecewise-constant prolongation of k_mg_prolong applied as the cells are loaded.
+// The smoothed tile goes to xout, not to L.x: a CTA reads a halo of its neighbours' tiles, which other
+// CTAs (of an earlier wave, when the grid exceeds one) would otherwise have overwritten already.
+__global__ void __launch_bounds__(kRbThreads, 2) k_mg_rb4_2d(MgLevel L, int first_color, int xmode,
+                                                             const double* __restrict__ xc, int cn0,
+                                                             double* __restrict__ xout) {
+    extern __shared__ double sx[];
     const PfDims& m = L.m;
     const int n0 = m.n[0], n1 = m.n[1];
     const int i0 = blockIdx.x * kRbTX - kRbH, j0 = blockIdx.y * kRbTY - kRbH;
     const double ih0 = L.ih2[0], ih1 = L.ih2[1];
-    for (int c = threadIdx.x; c < kRbCells; c += kRbThreads) {
+    // per owned cell: rhs, 1/diag, the coefficients of the -x, +x, -y, +y neighbours (beta_f / h^2),
+    // flags (bit0 in domain, bits1-4 neighbour present, bit5 colour) and its update reach (rings
+    // outside the tile)
+    double rb[kRbCellsPerThread], rd[kRbCellsPerThread], rw[kRbCellsPerThread], re[kRbCellsPerThread];
+    double rs[kRbCellsPerThread], rn[kRbCellsPerThread];
+    unsigned fl[kRbCellsPerThread];
+    int ring[kRbCellsPerThread];
+#pragma unroll
+    for (int u = 0; u < kRbCellsPerThread; ++u) {
+        const int c = threadIdx.x + u * kRbThreads;
         const int lx = c % kRbW, ly = c / kRbW;
         int i = i0 + lx, j = j0 + ly;
         bool in = true;
@@ -581,17 +591,17 @@ __global__ void __launch_bounds__(kRbThreads) k_mg_rb4_2d(MgLevel L, int first_c
             if (m.periodic[1]) j = ((j % n1) + n1) % n1;
             else in = false;
         }
-        unsigned char f = 0;
+        unsigned f = 0;
+        double xv = 0.0;
+        rb[u] = rd[u] = rw[u] = re[u] = rs[u] = rn[u] = 0.0;
         if (in) {
             const int q = i + n0 * j;
-            double xv = 0.0;
             if (xmode != 1) {
                 xv = L.x[q];
                 if (xmode == 2) xv += xc[(i >> 1) + cn0 * (j >> 1)];
             }
-            sx[c] = xv;
-            sb[c] = L.b[q];
-            sd[c] = L.idiag[q];
+            rb[u] = L.b[q];
+            rd[u] = L.idiag[q];
             const int fx = n0 + 1;
             f = 1;
             if (i > 0 || m.periodic[0]) f |= 2;
@@ -599,38 +609,42 @@ __global__ void __launch_bounds__(kRbThreads) k_mg_rb4_2d(MgLevel L, int first_c
             if (j > 0 || m.periodic[1]) f |= 8;
             if (j < n1 - 1 || m.periodic[1]) f |= 16;
             if ((i + j) & 1) f |= 32;
-            cw[c] = L.beta[0][i + fx * j] * ih0;
-            ce[c] = L.beta[0][(i + 1) + fx * j] * ih0;
-            cs[c] = L.beta[1][i + n0 * j] * ih1;
-            cn[c] = L.beta[1][i + n0 * (j + 1)] * ih1;
+            rw[u] = L.beta[0][i + fx * j] * ih0;
+            re[u] = L.beta[0][(i + 1) + fx * j] * ih0;
+            rs[u] = L.beta[1][i + n0 * j] * ih1;
+            rn[u] = L.beta[1][i + n0 * (j + 1)] * ih1;
         }
-        flag[c] = f;
+        sx[c] = xv;
+        fl[u] = f;
+        const int ox = lx - kRbH, oy = ly - kRbH;
+        const int rx = ox < 0 ? -ox : (ox >= kRbTX ? ox - kRbTX + 1 : 0);
+        const int ry = oy < 0 ? -oy : (oy >= kRbTY ? oy - kRbTY + 1 : 0);
+        ring[u] = rx > ry ? rx : ry;
     }
     __syncthreads();
 #pragma unroll 1
     for (int p = 0; p < kRbPasses; ++p) {
-        const int color = first_color ^ (p & 1);
+        const unsigned color = (unsigned)(first_color ^ (p & 1));
         const int reach = kRbH - 1 - p;  // rings of the tile this pass updates
-        for (int c = threadIdx.x; c < kRbCells; c += kRbThreads) {
-            const int lx = c % kRbW - kRbH, ly = c / kRbW - kRbH;
-            const int rx = lx < 0 ? -lx : (lx >= kRbTX ? lx - kRbTX + 1 : 0);
-            const int ry = ly < 0 ? -ly : (ly >= kRbTY ? ly - kRbTY + 1 : 0);
-            const unsigned char f = flag[c];
-            if ((rx > ry ? rx : ry) > reach || !(f & 1) || ((f >> 5) & 1) != color) continue;
+#pragma unroll
+        for (int u = 0; u < kRbCellsPerThread; ++u) {
+            const int c = threadIdx.x + u * kRbThreads;
+            const unsigned f = fl[u];
+            if (ring[u] > reach || !(f & 1) || ((f >> 5) & 1) != color) continue;
             // the neighbours in mg_off_t's order: -x, +x, -y, +y
             double off = 0.0;
-            if (f & 2) off += cw[c] * sx[c - 1];
-            if (f & 4) off += ce[c] * sx[c + 1];
-            if (f & 8) off += cs[c] * sx[c - kRbW];
-            if (f & 16) off += cn[c] * sx[c + kRbW];
-            sx[c] = (sb[c] + off) * sd[c];
+            if (f & 2) off += rw[u] * sx[c - 1];
+            if (f & 4) off += re[u] * sx[c + 1];
+            if (f & 8) off += rs[u] * sx[c - kRbW];
+            if (f & 16) off += rn[u] * sx[c + kRbW];
+            sx[c] = (rb[u] + off) * rd[u];
         }
         __syncthreads();
     }
     for (int c = threadIdx.x; c < kRbTX * kRbTY; c += kRbThreads) {
         const int lx = c % kRbTX, ly = c / kRbTX;
         const int i = blockIdx.x * kRbTX + lx, j = blockIdx.y * kRbTY + ly;
-        if (i < n0 && j < n1) L.x[i + n0 * j] = sx[(lx + kRbH) + kRbW * (ly + kRbH)];
+        if (i < n0 && j < n1) xout[i + n0 * j] = sx[(lx + kRbH) + kRbW * (ly + kRbH)];
     }
 }
 
@@ -729,16 +743,32 @@ constexpr int kBlockCells = 4096;
 constexpr int kBlockThreads = 1024;
 constexpr size_t kBlockSmemMax = 200 * 1024;  // shared memory of the single-block cycle
 
+// Who runs a step of the single-block cycle: the whole block (barriers between steps), or its first
+// warp alone for the smallest levels (warp barriers: a block barrier per step costs more than the
+// step's work there). Either way every cell gets the same updates in the same order.
+struct BlockTeam {
+    __device__ static int id() { return threadIdx.x; }
+    __device__ static int size() { return blockDim.x; }
+    __device__ static void sync() { __syncthreads(); }
+};
+struct WarpTeam {
+    __device__ static int id() { return threadIdx.x & 31; }
+    __device__ static int size() { return 32; }
+    __device__ static void sync() { __syncwarp(); }
+};
+constexpr long long kWarpCells = 128;  // levels of at most this many cells run on one warp
+
 // One red-black colour pass of a 2D level with an even number of columns: each thread takes cells of
 // the colour only (the t-th cell of the colour in row-major order), and the neighbour sum is written
 // out in mg_off's order (-x, +x, -y, +y) with its boundary rules, so the values are mg_off's.
+template <class T>
 __device__ void blk_rb_pass_2d(const MgLevel& L, int color) {
     const PfDims& m = L.m;
     const int n0 = m.n[0], n1 = m.n[1], hw = n0 / 2;
     const int ncol = hw * n1;
     const double ih0 = L.ih2[0], ih1 = L.ih2[1];
     const bool p0 = m.periodic[0], p1 = m.periodic[1];
-    for (int t = threadIdx.x; t < ncol; t += blockDim.x) {
+    for (int t = T::id(); t < ncol; t += T::size()) {
         const int j = t / hw;
         const int i = 2 * (t - j * hw) + ((j + color) & 1);
         const int q = i + n0 * j;
@@ -751,6 +781,7 @@ __device__ void blk_rb_pass_2d(const MgLevel& L, int color) {
     }
 }
 
+template <class T>
 __device__ void blk_smooth(const MgLevel& L, int sweeps, bool reverse) {
     const PfDims& m = L.m;
     const int n = (int)m.nv;
@@ -758,30 +789,80 @@ __device__ void blk_smooth(const MgLevel& L, int sweeps, bool reverse) {
     for (int s = 0; s < sweeps; ++s) {
         if (fast2d) {
             for (int c = 0; c < 2; ++c) {
-                blk_rb_pass_2d(L, reverse ? 1 - c : c);
-                __syncthreads();
+                blk_rb_pass_2d<T>(L, reverse ? 1 - c : c);
+                T::sync();
             }
         } else if (L.rb) {
             for (int c = 0; c < 2; ++c) {
                 const int color = reverse ? 1 - c : c;
-                for (int q = threadIdx.x; q < n; q += blockDim.x) {
+                for (int q = T::id(); q < n; q += T::size()) {
                     const int i = q % m.n[0], r = q / m.n[0];
                     const int j = r % m.n[1], k = r / m.n[1];
                     if (((i + j + k) & 1) != color) continue;
                     L.x[q] = (L.b[q] + mg_off(L, L.x, i, j, k)) * L.idiag[q];
                 }
-                __syncthreads();
+                T::sync();
             }
         } else {
-            for (int q = threadIdx.x; q < n; q += blockDim.x) {
+            for (int q = T::id(); q < n; q += T::size()) {
                 const int i = q % m.n[0], r = q / m.n[0];
                 const int j = r % m.n[1], k = r / m.n[1];
                 L.r[q] = L.x[q] + 0.8 * ((L.b[q] + mg_off(L, L.x, i, j, k)) * L.idiag[q] - L.x[q]);
             }
-            __syncthreads();
-            for (int q = threadIdx.x; q < n; q += blockDim.x) L.x[q] = L.r[q];
-            __syncthreads();
+            T::sync();
+            for (int q = T::id(); q < n; q += T::size()) L.x[q] = L.r[q];
+            T::sync();
         }
+    }
+}
+
+// the downward step at level L: smooth, residual, restriction into C's right-hand side, C's x zeroed
+template <class T>
+__device__ void blk_down(const MgLevel& L, const MgLevel& C) {
+    blk_smooth<T>(L, 2, false);
+    const PfDims& m = L.m;
+    for (int q = T::id(); q < (int)m.nv; q += T::size()) {
+        const int i = q % m.n[0], r = q / m.n[0];
+        const int j = r % m.n[1], k = r / m.n[1];
+        L.r[q] = L.b[q] - (L.x[q] / L.idiag[q] - mg_off(L, L.x, i, j, k));
+    }
+    T::sync();
+    const PfDims& c = C.m;
+    for (int q = T::id(); q < (int)c.nv; q += T::size()) {
+        const int I = q % c.n[0], r = q / c.n[0];
+        const int J = r % c.n[1], K = r / c.n[1];
+        double sacc = 0.0;
+        const int kz = (c.D == 3) ? 2 : 1;
+        for (int dk = 0; dk < kz; ++dk)
+            for (int dj = 0; dj < 2; ++dj)
+                for (int di = 0; di < 2; ++di)
+                    sacc += L.r[(2 * I + di) + m.n[0] * ((2 * J + dj) + m.n[1] * (c.D == 3 ? 2 * K + dk : 0))];
+        C.b[q] = sacc / (double)(c.D == 3 ? 8 : 4);
+        C.x[q] = 0.0;
+    }
+    T::sync();
+}
+
+// the upward step at level L: C's correction prolonged (piecewise constant) onto L, then smoothed
+template <class T>
+__device__ void blk_up(const MgLevel& L, const MgLevel& C) {
+    const PfDims& m = L.m;
+    const PfDims& c = C.m;
+    for (int q = T::id(); q < (int)m.nv; q += T::size()) {
+        const int i = q % m.n[0], r = q / m.n[0];
+        const int j = r % m.n[1], k = r / m.n[1];
+        L.x[q] += C.x[(i / 2) + c.n[0] * ((j / 2) + c.n[1] * (m.D == 3 ? k / 2 : 0))];
+    }
+    T::sync();
+    blk_smooth<T>(L, 2, true);
+}
+
+// the coarsest level: an even number of sweeps alternating the colour order (symmetric)
+template <class T>
+__device__ void blk_coarsest(const MgLevel& L) {
+    for (int s = 0; s < 8; ++s) {
+        blk_smooth<T>(L, 1, false);
+        blk_smooth<T>(L, 1, true);
     }
 }
 
@@ -830,55 +911,21 @@ __global__ void __launch_bounds__(kBlockThreads) k_mg_vcycle_block(const MgLevel
         sl[l0].b[q] = levels[l0].b[q];
     }
     __syncthreads();
-    // down
-    for (int l = l0; l < nl - 1; ++l) {
-        const MgLevel& L = sl[l];
-        const MgLevel& C = sl[l + 1];
-        blk_smooth(L, 2, false);
-        const PfDims& m = L.m;
-        for (int q = threadIdx.x; q < (int)m.nv; q += blockDim.x) {
-            const int i = q % m.n[0], r = q / m.n[0];
-            const int j = r % m.n[1], k = r / m.n[1];
-            L.r[q] = L.b[q] - (L.x[q] / L.idiag[q] - mg_off(L, L.x, i, j, k));
-        }
-        __syncthreads();
-        const PfDims& c = C.m;
-        for (int q = threadIdx.x; q < (int)c.nv; q += blockDim.x) {
-            const int I = q % c.n[0], r = q / c.n[0];
-            const int J = r % c.n[1], K = r / c.n[1];
-            double sacc = 0.0;
-            const int kz = (c.D == 3) ? 2 : 1;
-            for (int dk = 0; dk < kz; ++dk)
-                for (int dj = 0; dj < 2; ++dj)
-                    for (int di = 0; di < 2; ++di)
-                        sacc += L.r[(2 * I + di) + m.n[0] * ((2 * J + dj) + m.n[1] * (c.D == 3 ? 2 * K + dk : 0))];
-            C.b[q] = sacc / (double)(c.D == 3 ? 8 : 4);
-            C.x[q] = 0.0;
-        }
-        __syncthreads();
+    // levels lw .. nl-1 (those of at most kWarpCells cells) run on the first warp alone; lw == nl when
+    // even the coarsest level is larger
+    int lw = nl;
+    while (lw > l0 && sl[lw - 1].m.nv <= kWarpCells) --lw;
+    const int lb = (lw < nl - 1) ? lw : nl - 1;  // the block's downward steps are l0 .. lb-1
+    for (int l = l0; l < lb; ++l) blk_down<BlockTeam>(sl[l], sl[l + 1]);
+    if (lw == nl) {
+        blk_coarsest<BlockTeam>(sl[nl - 1]);
+    } else if (threadIdx.x < 32) {
+        for (int l = lw; l < nl - 1; ++l) blk_down<WarpTeam>(sl[l], sl[l + 1]);
+        blk_coarsest<WarpTeam>(sl[nl - 1]);
+        for (int l = nl - 2; l >= lw; --l) blk_up<WarpTeam>(sl[l], sl[l + 1]);
     }
-    // coarsest: an even number of sweeps alternating the colour order (symmetric)
-    {
-        const MgLevel& L = sl[nl - 1];
-        for (int s = 0; s < 8; ++s) {
-            blk_smooth(L, 1, false);
-            blk_smooth(L, 1, true);
-        }
-    }
-    // up
-    for (int l = nl - 2; l >= l0; --l) {
-        const MgLevel& L = sl[l];
-        const MgLevel& C = sl[l + 1];
-        const PfDims& m = L.m;
-        const PfDims& c = C.m;
-        for (int q = threadIdx.x; q < (int)m.nv; q += blockDim.x) {
-            const int i = q % m.n[0], r = q / m.n[0];
-            const int j = r % m.n[1], k = r / m.n[1];
-            L.x[q] += C.x[(i / 2) + c.n[0] * ((j / 2) + c.n[1] * (m.D == 3 ? k / 2 : 0))];
-        }
-        __syncthreads();
-        blk_smooth(L, 2, true);
-    }
+    __syncthreads();
+    for (int l = lb - 1; l >= l0; --l) blk_up<BlockTeam>(sl[l], sl[l + 1]);
     for (int q = threadIdx.x; q < (int)levels[l0].m.nv; q += blockDim.x) levels[l0].x[q] = sl[l0].x[q];
 }
 
@@ -1076,8 +1123,12 @@ cudaError_t vcycle(PfLevel* pf, int l, cudaStream_t st, bool x_zero) {
                 attr = true;
             }
             const dim3 grid((unsigned)((L.m.n[0] + kRbTX - 1) / kRbTX), (unsigned)((L.m.n[1] + kRbTY - 1) / kRbTY));
+            // out of place into the level's scratch vector r, which then becomes its x (the residual
+            // of a fused 2D level is never stored, so r is free); a V-cycle swaps each level twice,
+            // so every launch of a captured iteration sees the same pointers
             k_mg_rb4_2d<<<grid, kRbThreads, kRbSmem, st>>>(L, reverse ? 1 : 0, xmode, C ? C->x : nullptr,
-                                                           C ? C->m.n[0] : 0);
+                                                           C ? C->m.n[0] : 0, L.r);
+            std::swap(L.x, L.r);
             return;
         }
         if (xmode == 1) k_zero<<<nb, kThreads, 0, st>>>(L.x, L.m.nv);

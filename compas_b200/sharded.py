@@ -276,15 +276,18 @@ class ShardedLevel:
         self.comm.exchange(self.slabs, arrays)
 
     def upload(self, U, t0: float = 0.0) -> None:
-        """Local slabs of the global padded state U (its valid cells; ghosts are filled here), then the
+        """Local slabs of the global padded state U (host numpy or a torch tensor; its valid cells, ghosts
+        are filled here), then the
         initial wave-speed maximum (CalculateInitialcmax, source/Class_Compressible_PhaseField.cpp:4501-4605)."""
         import torch
 
         from . import valid_view
 
         for s, a in zip(self.slabs, self.U):
-            src = np.ascontiguousarray(valid_view(U, self.p, self.g)[s.global_slice(self.g)])
-            valid_view(a, self.p, s.geom).copy_(torch.from_numpy(src))
+            src = valid_view(U, self.p, self.g)[s.global_slice(self.g)]
+            if isinstance(src, np.ndarray):
+                src = torch.from_numpy(np.ascontiguousarray(src))
+            valid_view(a, self.p, s.geom).copy_(src)
         self.t, self.dt_prev, self.steps, self.dts, self.stopped = float(t0), 1.0e100, 0, [], None
         self._fill(self.U)
         for s, a, c, w in zip(self.slabs, self.U, self.cm, self.scratch):

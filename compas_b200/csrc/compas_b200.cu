@@ -357,8 +357,6 @@ static int check_args(const compas_b200_parm* p, const compas_b200_geom* g) {
         if (!sixn_built(p->dim, p->nphase))
             return fail(COMPAS_B200_EUNSUPPORTED, "SIXEQS_IE_NPHASE: this build runs NPHASE 2, 3 in 2D and 3 in 3D");
         if (p->thinc) return fail(COMPAS_B200_EUNSUPPORTED, "SIXEQS_IE_NPHASE: FiniteVolume.THINC is not in this engine");
-        if (p->precision != 0)
-            return fail(COMPAS_B200_EUNSUPPORTED, "SIXEQS_IE_NPHASE runs in plain FP64 (compas_b200.precision = fp64)");
         if (p->phase_field)
             return fail(COMPAS_B200_EUNSUPPORTED, "PhaseField.phase_field = 1: this engine runs the FIVEEQS and SIXEQS "
                                                   "Phase-Field step");
@@ -2183,8 +2181,6 @@ int compas_b200_batch_create_nphase(int physics, int dim, int nphase, int id_lim
         return fail(COMPAS_B200_EUNSUPPORTED, "FIVEEQS_NPHASE batches: NPHASE 2, 3, 4 in 2D and 3 in 3D");
     if (physics == COMPAS_B200_SIXEQS_IE_NPHASE && !sixn_built(dim, nphase))
         return fail(COMPAS_B200_EUNSUPPORTED, "SIXEQS_IE_NPHASE batches: NPHASE 2, 3 in 2D and 3 in 3D");
-    if (physics == COMPAS_B200_SIXEQS_IE_NPHASE && precision != 0)
-        return fail(COMPAS_B200_EUNSUPPORTED, "SIXEQS_IE_NPHASE runs in plain FP64 (precision 0)");
     if (id_limiter != 5 && id_limiter != 6) return fail(COMPAS_B200_EUNSUPPORTED, "WENO5 (5) or WENO5B (6)");
     if (precision != 0 && precision != 1) return fail(COMPAS_B200_EARG, "precision 0 or 1");
     if (capacity < 1 || capacity > (1 << 20)) return fail(COMPAS_B200_EARG, "capacity out of range");

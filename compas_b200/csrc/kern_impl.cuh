@@ -84,7 +84,7 @@ static cudaError_t launch_stage_var(const KernelChoice& k, const StageArgs& a, c
             default: return launch_stage_v<M, 2, MIX, kVarPlain, 0>(a, st);
         }
     } else {
-    if constexpr (M::D == 3 && MIX && M::KIND != kModelFiveN) {
+    if constexpr (M::D == 3 && MIX && M::KIND != kModelFiveN && M::KIND != kModelSixN) {
         if (tm && tm->valid && !k.thinc && !k.phase_field) {
             switch (k.shape) {
                 case 1: return launch_stage_tma<M, SCHEME, 1>(a, *tm, st);

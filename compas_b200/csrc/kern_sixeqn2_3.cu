@@ -1,5 +1,5 @@
 // Stage kernels of the SixEqN<2, 3> model (N-phase six-equation in the internal-energy form, 2D,
-// NPHASE = 3), plain FP64 form (the model's only form).
+// NPHASE = 3), plain FP64 form.
 #include "kern_impl.cuh"
 
 namespace compas {

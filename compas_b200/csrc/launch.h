@@ -68,25 +68,11 @@ COMPAS_DECLARE_LAUNCHERS(fiveeqn2_2)
 COMPAS_DECLARE_LAUNCHERS(fiveeqn2_3)
 COMPAS_DECLARE_LAUNCHERS(fiveeqn2_4)
 COMPAS_DECLARE_LAUNCHERS(fiveeqn3_3)
+// SIXEQS_IE_NPHASE (sixeqn<dim>_<nphase>)
+COMPAS_DECLARE_LAUNCHERS(sixeqn2_2)
+COMPAS_DECLARE_LAUNCHERS(sixeqn2_3)
+COMPAS_DECLARE_LAUNCHERS(sixeqn3_3)
 #undef COMPAS_DECLARE_LAUNCHERS
 
-// Models compiled in the plain FP64 form only (kern_<name>.cu): the mixed form reports
-// cudaErrorNotSupported.
-#define COMPAS_DECLARE_LAUNCHERS_FP64(name)                                                          \
-    cudaError_t launch_stage_##name##_p0(const KernelChoice& k, const StageArgs& a, cudaStream_t st,   \
-                                         const TmaMaps* tm);                                         \
-    cudaError_t launch_list_##name##_p0(const KernelChoice& k, const ListArgs& L, cudaStream_t st);   \
-    inline cudaError_t launch_stage_##name(const KernelChoice& k, const StageArgs& a, cudaStream_t st, \
-                                           const TmaMaps* tm) {                                      \
-        return (k.precision == 0) ? launch_stage_##name##_p0(k, a, st, tm) : cudaErrorNotSupported;  \
-    }                                                                                                \
-    inline cudaError_t launch_list_##name(const KernelChoice& k, const ListArgs& L, cudaStream_t st) { \
-        return (k.precision == 0) ? launch_list_##name##_p0(k, L, st) : cudaErrorNotSupported;        \
-    }
-// SIXEQS_IE_NPHASE (sixeqn<dim>_<nphase>)
-COMPAS_DECLARE_LAUNCHERS_FP64(sixeqn2_2)
-COMPAS_DECLARE_LAUNCHERS_FP64(sixeqn2_3)
-COMPAS_DECLARE_LAUNCHERS_FP64(sixeqn3_3)
-#undef COMPAS_DECLARE_LAUNCHERS_FP64
 
 }  // namespace compas

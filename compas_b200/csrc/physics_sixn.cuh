@@ -67,6 +67,30 @@ struct SixEqN {
         W[IE] = P;
     }
 
+    // Mixed precision: the phase pressures alpha_k p_k from the phase internal energies in FP64 (where the
+    // energy cancels against the B_k term), the velocity by a near-FP64 reciprocal of rho (rcp_mixed), the
+    // primitives rounded once to FP32. The FP32 WENO face states are converted back by prim2cons in FP64.
+    __device__ static __forceinline__ void cons2prim_f32(float* W, const double* U, const Eos& e) {
+        double rho = 0.0;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) rho += U[IR + k];
+        const double ir = rcp_mixed(rho);
+        double P = 0.0;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            const double al = U[IA + k], ar = U[IR + k];
+            const double xi = nasg_xi(al, ar, e.Ck[k], nullptr);
+            const double aps = ((U[IP + k] - ar * e.Dk[k]) - (xi * al) * e.Bk[k]) / (e.Ak[k] * xi);
+            W[IA + k] = (float)al;
+            W[IR + k] = (float)ar;
+            W[IP + k] = (float)aps;
+            P += aps;
+        }
+#pragma unroll
+        for (int d = 0; d < D; ++d) W[IM + d] = (float)(U[IM + d] * ir);
+        W[IE] = (float)P;
+    }
+
     __device__ static __forceinline__ void prim2cons(double* U, const double* W, const Eos& e, unsigned int* err) {
         double rho = 0.0, rho_e = 0.0;
 #pragma unroll

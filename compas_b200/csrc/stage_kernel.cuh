@@ -354,8 +354,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
     static_assert(!TMA || (M::D == 3 && MIX), "TMA halo staging: the 3D mixed form");
     static_assert(!PFX || M::KIND != kModelFiveN, "the Phase-Field kernel is the two-phase models'");
     static_assert(M::KIND != kModelFiveN || !TH, "FIVEEQS_NPHASE runs without THINC");
-    static_assert(M::KIND != kModelSixN || (VAR == kVarPlain && !MIX),
-                  "SIXEQS_IE_NPHASE: the plain hyperbolic right-hand side in FP64");
+    static_assert(M::KIND != kModelSixN || VAR == kVarPlain,
+                  "SIXEQS_IE_NPHASE: the plain hyperbolic right-hand side");
     static_assert(SCHEME != 2 || (VAR == kVarPlain && !TH), "GODUNOV / MUSCL: the plain right-hand side");
     constexpr bool NPH = (M::KIND == kModelFiveN);
     constexpr bool SXN = (M::KIND == kModelSixN);
@@ -666,13 +666,13 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                     M::cons2prim_f32(wL, UL, a.e);
                     M::cons2prim_f32(wR, UR, a.e);
                 } else {
-                    if constexpr (SCHEME == 6 && NPH) {
-                        auto rl = [&](int k, int s) { return (float)smem[off[s] + k * str[s]]; };
+                    if constexpr (SCHEME == 6 && (NPH || SXN)) {
+                        auto rl = [&](int k, int s) { return (float)smem[off[s] + (M::IR + k) * str[s]]; };
                         auto al_ = [&](int k, int s) { return (float)smem[off[s] + (M::IA + k) * str[s]]; };
-                        bounded_phases<M::NP, 5, float>(rl, al_, 1, wL, wL + M::IA);
-                        auto rr = [&](int k, int s) { return (float)smem[off[s + 1] + k * str[s + 1]]; };
+                        bounded_phases<M::NP, 5, float>(rl, al_, 1, wL + M::IR, wL + M::IA);
+                        auto rr = [&](int k, int s) { return (float)smem[off[s + 1] + (M::IR + k) * str[s + 1]]; };
                         auto ar_ = [&](int k, int s) { return (float)smem[off[s + 1] + (M::IA + k) * str[s + 1]]; };
-                        bounded_phases<M::NP, 5, float>(rr, ar_, -1, wR, wR + M::IA);
+                        bounded_phases<M::NP, 5, float>(rr, ar_, -1, wR + M::IR, wR + M::IA);
                     } else if constexpr (SCHEME == 6) {
                         float r1[6], r2[6], al[6];
 #pragma unroll
@@ -720,9 +720,13 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                         M::consistent_limit(UL, smem + off[2], str[2], dxd, 1, a.e, err);
                         M::consistent_limit(UR, smem + off[3], str[3], dxd, -1, a.e, err);
                     }
+                    if constexpr (SXN && SCHEME == 2) if (a.muscl >= 1 && a.muscl < 10) {
+                        M::consistent_limit(UL, smem + off[2], str[2], dxd, 1, a.e, err);
+                        M::consistent_limit(UR, smem + off[3], str[3], dxd, -1, a.e, err);
+                    }
                 }
-                if constexpr (NPH) {
-                    // N-phase: FP32 reconstruction, FP64 limiter and Riemann solver
+                if constexpr (NPH || SXN) {
+                    // N-phase models: FP32 reconstruction, FP64 limiter and Riemann solver
                     riemann<M>(a.riemann, F, fnc, cm, UL, UR, a.e, d, a.id_k, err);
                 } else {
                     float cmf;
@@ -801,10 +805,10 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int tile, double*
                 // of the non-conservative terms from the FP32 tile
 #pragma unroll
                 for (int n = 0; n < N; ++n) W[n] = Pint[n * CSTR + l];
-                if constexpr (NPH) {
+                if constexpr (NPH || SXN) {
 #pragma unroll
                     for (int k = 0; k < M::NP; ++k) {
-                        W[k] = Us[k];
+                        W[M::IR + k] = Us[M::IR + k];
                         W[M::IA + k] = Us[M::IA + k];
                     }
                 } else {

@@ -1,7 +1,7 @@
 """The N-phase six-equation model in its internal-energy form (SIXEQS_IE_NPHASE) on the CUDA path
 against the reference's own headers.
 
-The model runs in plain FP64 and reproduces the reference's arithmetic: the phase pressures from the
+The model's plain FP64 form reproduces the reference's arithmetic: the phase pressures from the
 phase internal energies, reconstruction in primitive variables (GODUNOV, MUSCL with the consistent
 limiter of volume fractions, partial densities and phase pressures, WENO3, WENO3B, WENO5, WENO5B with
 bounded partial densities and volume fractions), the model's HLLC / HLL / LLF fluxes, the
@@ -12,6 +12,9 @@ asserted bound is the north star's 1e-11 relative L-infinity per field. Cases: a
 on an air bubble (and a helium bubble with three phases), after the reference's
 ShockBubble-WaterAir-6Eq-Nphase example, in pressure equilibrium and out of it, with the NASG
 covolume, with a trace threshold that sends phases through the safeguarded relaxation, and in 3D.
+The mixed form (FP32 reconstruction) is held to 1e-5 relative L1 against the FP64 form in the volume
+fractions and phase masses with the WENO schemes (1e-3 with MUSCL, whose discontinuous limiter turns
+rounding into branch flips), and its box-list batch to the bits of its single-box level.
 """
 import ast
 import glob
@@ -277,3 +280,55 @@ def test_sixn_amr_matches_reference(kw, domain, regions, mgs, steps, extra):
     it on a hierarchy): subcycling, flux registers with the alpha_k and alpha_k p_k reflux source terms,
     the relaxation of the refluxed cells, average-down; to the bit against the oracle's hierarchy driver."""
     _amr_run(kw, domain, regions, mgs, steps, extra)
+
+
+def _rel_l1(a, b):
+    return np.array([float(np.abs(a[c] - b[c]).sum()) / max(float(np.abs(b[c]).sum()), 1e-300)
+                     for c in range(a.shape[0])])
+
+
+@pytest.mark.parametrize("kw,steps,bound", [
+    (dict(n=64, nphase=2, scheme="WENO5"), 40, 1e-5),
+    (dict(n=32, nphase=3, dim=3, scheme="WENO5B"), 20, 1e-5),
+    # MUSCL's limiter is discontinuous: FP32 rounding of the slopes flips its branch choices, and the
+    # out-of-equilibrium three-phase bubble carries that further (measured 2.3e-4 after 40 steps)
+    (dict(n=64, nphase=3, dp=0.05, scheme="MUSCL"), 40, 1e-3),
+])
+def test_sixn_mixed_error_vs_fp64(kw, steps, bound):
+    """The mixed form of SIXEQS_IE_NPHASE (FP32 reconstruction of the primitives; FP64 phase-pressure
+    recovery, consistent limiter, Riemann solver, relaxation and stage accumulation): relative L1 error
+    per field against the FP64 form after the stated steps (each form with its own step sizes), bounded
+    on the volume fractions and the phase masses: 1e-5 with the WENO schemes."""
+    phys, dim, inputs, geom, U = cases.sixn_shock_bubbles(**kw)
+    g = cb.make_geom(**geom)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        p = cb.make_parm(phys, dim, dict(inputs, **{"compas_b200.precision": prec}))
+        got, info, _ = run_gpu(p, g, U.copy(), steps)
+        assert info.status == 0 and info.steps == steps
+        out[prec] = cb.valid_view(got, p, g)
+    e = _rel_l1(out["mixed"], out["fp64"])
+    nph = kw["nphase"]
+    print(f"SIXEQS_IE_NPHASE mixed vs FP64 {kw}, {steps} steps: rel L1 per field {np.array2string(e, precision=2)}")
+    assert np.all(e[:2 * nph] <= bound), e  # alpha_k then alpha_k rho_k
+    assert np.all(np.isfinite(out["mixed"]))
+
+
+def test_sixn_mixed_batch_equals_level():
+    """In the mixed form too, cases in one box-list batch give the single-box level's bits."""
+    reqs = [dict(n=8, nphase=2), dict(n=12, nphase=2, dp=0.05), dict(n=16, nphase=2)]
+    b = cb.Batch(cb.SIXEQS_IE_NPHASE, 2, id_limiter=5, precision=1, capacity=4, nphase=2)
+    ids, ins = [], []
+    for kw in reqs:
+        phys, dim, inputs, geom, U = cases.sixn_shock_bubbles(**dict(kw, scheme="WENO5"))
+        p = cb.make_parm(phys, dim, dict(inputs, **{"compas_b200.precision": "mixed"}))
+        g = cb.make_geom(**geom)
+        ids.append(b.add(p, g, U, max_steps=10))
+        ins.append((p, g, U))
+    b.advance(10)
+    for cid, (p, g, U) in zip(ids, ins):
+        got = b.download(cid)
+        ref, info, _ = run_gpu(p, g, U.copy(), 10)
+        assert info.status == 0
+        assert np.array_equal(cb.valid_view(got, p, g), cb.valid_view(ref, p, g))
+    b.close()

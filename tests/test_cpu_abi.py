@@ -159,8 +159,7 @@ def test_sixeqs_ie_nphase_keys():
     assert cb.nc_terms(p) == 1
     g = cb.make_geom((16, 16, 1), (0.1, 0.1, 1.0))
     g3 = cb.make_geom((8, 8, 8), (0.1, 0.1, 0.1))
-    bad = [(2, dict(inputs, **{"compas_b200.precision": "mixed"}), g),
-           (2, dict(inputs, **{"FiniteVolume.THINC": 1, "FiniteVolume.Scheme": "WENO5"}), g),
+    bad = [(2, dict(inputs, **{"FiniteVolume.THINC": 1, "FiniteVolume.Scheme": "WENO5"}), g),
            (2, dict(inputs, **{"FiniteVolume.ID_Bound": 1}), g),
            (2, dict(inputs, **{"prob.EOS.gamma": [1.4] * 4, "prob.EOS.pinf": [0.0] * 4}), g),
            (3, dict(inputs, **{"prob.EOS.gamma": [1.4] * 2, "prob.EOS.pinf": [0.0] * 2}), g3)]
@@ -170,5 +169,5 @@ def test_sixeqs_ie_nphase_keys():
             cb.Level(q, geom)
         assert e.value.code == cb.EUNSUPPORTED
     with pytest.raises(cb.CompasError) as e:
-        cb.Batch(cb.SIXEQS_IE_NPHASE, 2, 5, 1, 4, nphase=2)
+        cb.Batch(cb.SIXEQS_IE_NPHASE, 2, 5, 1, 4, nphase=4)  # NPHASE 4 is not compiled for this model
     assert e.value.code == cb.EUNSUPPORTED
